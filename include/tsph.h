@@ -1,0 +1,241 @@
+/*
+ * tsph.h -- C ABI of the B200 (sm_100a) TensorSPH particle pass.
+ *
+ * Plain pointers and sizes only: every array is caller-owned device memory,
+ * every entry point is stream-ordered on the stream it is given and returns a
+ * status code (TSPH_OK = 0).  Scratch memory is a caller-provided workspace
+ * whose size is queried first; the library itself never allocates device
+ * memory and never frees caller memory.  Entry points that must hand a
+ * data-dependent size back to the host (a pair count, a grid extent, an index
+ * check) synchronise the given stream before returning, exactly where the
+ * reference's PyTorch code synchronises (`int(...)`, `.item()`).
+ *
+ * Dtype codes: TSPH_F32 / TSPH_F64 select the arithmetic of positions and
+ * fields (the reference computes in the dtype of its position tensor).
+ *
+ * The reference (TensorSPH) has no native layer: its "plugin" surface is the
+ * set of Python functions named below, each entry point replaces the pair
+ * arithmetic of one of them (paths are inside the reference project).
+ */
+#ifndef TSPH_H
+#define TSPH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* tsph_stream; /* == cudaStream_t */
+
+enum {
+  TSPH_OK = 0,
+  TSPH_ERR_ARG = 1,         /* bad shape / dtype / parameter            -> ValueError */
+  TSPH_ERR_NONFINITE = 2,   /* non-finite positions                     -> ValueError */
+  TSPH_ERR_CUDA = 3,        /* CUDA runtime error                       -> RuntimeError */
+  TSPH_ERR_WORKSPACE = 4,   /* workspace smaller than queried size      -> RuntimeError */
+  TSPH_ERR_CAPACITY = 5,    /* fixed-capacity structure overflowed      -> RuntimeError */
+  TSPH_ERR_UNSUPPORTED = 6, /* option outside this build                -> NotImplementedError */
+  TSPH_ERR_INDEX = 7,       /* pair index out of range                  -> ValueError */
+  TSPH_ERR_GRID = 8,        /* cell grid extent exceeds 2^31 per axis   -> ValueError */
+  TSPH_ERR_STATE = 9,       /* engine state error (non-finite, stale)   -> FloatingPointError */
+  TSPH_ERR_TIMEOUT = 10     /* bounded device wait gave up              -> RuntimeError */
+};
+
+enum { TSPH_F32 = 0, TSPH_F64 = 1 };
+
+const char* tsph_status_string(int code);
+int tsph_abi_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Linked-cell neighbour search                                             */
+/* replaces neighbor_search.py:44-120 (cell_linked_pairs),                  */
+/*          threed/neighbors3.py:71-142 (periodic_pairs),                   */
+/*          neighbor_search.py:29-41 (brute_force_pairs)                     */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+  int64_t n, dim, dtype, periodic;
+  double cutoff;
+  double box[3];      /* periodic box edges                                   */
+  double width[3];    /* periodic cell width = box / ncell (in dtype)         */
+  int64_t ncell[3];   /* cells per axis (open: max - min + 1)                 */
+  int64_t origin[3];  /* open grid: per-axis minimum of floor(x / cutoff)     */
+  int64_t total_cells;
+  int64_t dense;      /* 1: dense cell table, 0: binary search over runs      */
+  int64_t key_bits;   /* radix-sort width of the row-major cell key           */
+  int64_t workspace_bytes;
+} tsph_grid;
+
+/* Bytes of device scratch tsph_grid_plan needs. */
+int64_t tsph_grid_plan_scratch_bytes(void);
+
+/* Validate positions (finite), read the cell extent of the cloud and size the
+ * workspace (synchronises).  box == NULL: open grid with cell edge = cutoff
+ * and data-dependent origin (neighbor_search.py:63-72); box != NULL (dim
+ * values): periodic grid with ncell = max(3, floor(L / cutoff))
+ * (neighbors3.py:94-97). */
+int tsph_grid_plan(const void* pos, int64_t n, int64_t dim, int64_t dtype, double cutoff,
+                   const double* box, void* scratch, tsph_grid* grid, tsph_stream stream);
+
+/* Cell keys, stable counting (radix) sort by key and the cell-run table.
+ * order_out (nullable, n int64) receives the stable cell order -- the
+ * permutation the reference obtains as argsort(inverse, stable=True). */
+int tsph_grid_build(const void* pos, const tsph_grid* grid, void* ws, int64_t ws_bytes,
+                    int64_t* order_out, tsph_stream stream);
+
+/* Count unordered pairs (i < j, |x_i - x_j|^2 <= cutoff^2) and return on the
+ * host the number whose first index is below row_limit (pair_count) and the
+ * number over all rows (total_count, nullable); synchronises.  Pairs are
+ * sorted by i, so the rows below row_limit are a prefix of the full list --
+ * the fluid_count pruning of PairListCache (neighbor_search.py:208-217). */
+int tsph_pairs_count(const void* pos, const tsph_grid* grid, int64_t row_limit, void* ws,
+                     int64_t ws_bytes, int64_t* pair_count, int64_t* total_count,
+                     tsph_stream stream);
+
+int64_t tsph_pairs_emit_workspace_bytes(int64_t pair_count, int64_t n);
+
+/* Write the lexicographically sorted (pair_count, 2) int64 pair list. */
+int tsph_pairs_emit(const void* pos, const tsph_grid* grid, int64_t row_limit, void* ws,
+                    int64_t ws_bytes, void* emit_ws, int64_t emit_ws_bytes, int64_t* pairs,
+                    int64_t pair_count, tsph_stream stream);
+
+/* O(N^2) reference search, same contract (brute_force_pairs). */
+int64_t tsph_brute_workspace_bytes(int64_t n);
+int tsph_brute_pairs_count(const void* pos, int64_t n, int64_t dim, int64_t dtype, double cutoff,
+                           void* ws, int64_t ws_bytes, int64_t* pair_count, tsph_stream stream);
+int tsph_brute_pairs_emit(const void* pos, int64_t n, int64_t dim, int64_t dtype, double cutoff,
+                          void* ws, int64_t ws_bytes, int64_t* pairs, int64_t pair_count,
+                          tsph_stream stream);
+
+/* max_a |x_a - anchor_a| (minimum image when box != NULL) into *out (device,
+ * one double).  Replaces PairListCache.displacement (neighbor_search.py:
+ * 198-206) and the periodic skin test of threed/solver.py:292-297. */
+int tsph_max_displacement(const void* pos, const void* anchor, int64_t n, int64_t dim,
+                          int64_t dtype, const double* box, double* out, tsph_stream stream);
+
+/* ------------------------------------------------------------------------ */
+/* Pair list -> symmetric gather list (CSR)                                 */
+/* Every pair (i, j) puts j in row i and i in row j; entry = neighbour index */
+/* | (1u << 31 when the row is the pair's second element).  Rows are sorted. */
+/* ------------------------------------------------------------------------ */
+int64_t tsph_csr_workspace_bytes(int64_t npairs, int64_t nrows);
+int tsph_csr_from_pairs(const int64_t* pairs, int64_t npairs, int64_t nrows, int64_t* rowptr,
+                        uint32_t* entries, void* ws, int64_t ws_bytes, tsph_stream stream);
+
+/* ------------------------------------------------------------------------ */
+/* WCSPH pair pass: droplet_impact.py:810-1228 (rhs, 2-D) and                */
+/* dam_break_3d.py:290-422 (rhs_3d).                                        */
+/* ------------------------------------------------------------------------ */
+enum {
+  TSPH_RHS_RENORMALIZE = 1,      /* Config.density_renormalization           */
+  TSPH_RHS_BOUNDARY_DENSITY = 2, /* Config.boundary_consistent_density       */
+  TSPH_RHS_SPLIT = 4,            /* rhs(split=True) / rhs_3d(return_wall_force) */
+  TSPH_RHS_WALL_SELF = 8,        /* walls carry the W(0) self term (3-D)      */
+  TSPH_RHS_WRAP_X = 16           /* periodic x with period wrap_width          */
+};
+
+typedef struct {
+  int64_t dim, dtype, n_fluid, n_wall, flags;
+  int64_t diffusion_form; /* 0 Molteni, 1 Antuono psi                        */
+  double h, sigma, rho0, sound_speed, gamma, gravity, viscosity, wall_friction;
+  double diffusion_scale; /* 2 delta c0 h; 0 disables the diffusive term      */
+  double eigen_floor, dt, wall_mass, wrap_width, lattice_sum;
+} tsph_wcsph_params;
+
+typedef struct {
+  const void* pos;            /* (n, D)                         */
+  const void* vel;            /* (n, D)                         */
+  const void* mass;           /* (n)                            */
+  const void* wall;           /* (nw, D) or NULL                */
+  const void* wall_vel;       /* (nw, D) or NULL (static wall)  */
+  const void* wall_accel;     /* (nw, D) or NULL                */
+  const void* nu_field;       /* (n) or NULL                    */
+  const void* density_offset; /* (n) or NULL                    */
+  const int64_t* rowptr;      /* (n + nw + 1)                   */
+  const uint32_t* entries;    /* CSR entries                    */
+  void* rho;                  /* out (n)                        */
+  void* pressure;             /* out (n)                        */
+  void* acc;                  /* out (n, D)                     */
+  void* reaction;             /* out (nw, D) when SPLIT         */
+  void* face_pressure;        /* out (nw) when SPLIT            */
+} tsph_wcsph_io;
+
+int64_t tsph_wcsph_workspace_bytes(const tsph_wcsph_params* prm);
+int tsph_wcsph_rhs(const tsph_wcsph_params* prm, const tsph_wcsph_io* io, void* ws,
+                   int64_t ws_bytes, tsph_stream stream);
+
+/* ------------------------------------------------------------------------ */
+/* threed operators: threed/operators3.py:212-256 (accelerations), with      */
+/* summation_density :70, diffusion :259, Adami :173, pressure :96 and the   */
+/* renormalised Brookshaw viscosity :116 (order 2 or 4).                     */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  int64_t dtype, n, n_fluid, has_gravity, periodic, renormalise, wall_model, viscous_order,
+      diffusion_form;
+  double h, rho0, sound_speed, gamma, viscosity, diffusion, dt, eigen_floor;
+  double gravity[3];
+  double box[3];
+} tsph_threed_params;
+
+typedef struct {
+  const void* pos; const void* vel; const void* mass; /* (n,3), (n,3), (n) */
+  const int64_t* rowptr; const uint32_t* entries;
+  void* acc; void* rho; void* pressure;               /* (n,3), (n), (n)   */
+} tsph_threed_io;
+
+int64_t tsph_threed_workspace_bytes(const tsph_threed_params* prm);
+int tsph_threed_accelerations(const tsph_threed_params* prm, const tsph_threed_io* io, void* ws,
+                              int64_t ws_bytes, tsph_stream stream);
+
+/* ------------------------------------------------------------------------ */
+/* Particle shifting: particle_shifting.py:93-224 (concentration,            */
+/* concentration_gradient, estimate_reference_concentration, shift_positions)*/
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  int64_t dim, dtype, n;
+  double h, sigma, magnitude, cap, free_surface;
+  double c_reference; /* < 0: the 95th percentile of C (linear interpolation) */
+} tsph_shift_params;
+
+typedef struct {
+  const void* pos; const void* volume;
+  const int64_t* rowptr; const uint32_t* entries;
+  void* out_pos; void* concentration; void* grad; void* normal; void* shift;
+  uint8_t* free_surface; double* c_reference; /* device scalar out */
+} tsph_shift_io;
+
+int64_t tsph_shift_workspace_bytes(const tsph_shift_params* prm);
+int tsph_shift_positions(const tsph_shift_params* prm, const tsph_shift_io* io, void* ws,
+                         int64_t ws_bytes, tsph_stream stream);
+
+/* 95th-percentile style order statistic: linear interpolation of the sorted
+ * values of x (n floats or doubles) at q in [0, 1], into *out (device). */
+int64_t tsph_quantile_workspace_bytes(int64_t n);
+int tsph_quantile(const void* x, int64_t n, int64_t dtype, double q, double* out, void* ws,
+                  int64_t ws_bytes, tsph_stream stream);
+
+/* ------------------------------------------------------------------------ */
+/* Integrators and clamps (FP64 or FP32 state, in place)                    */
+/* droplet_impact.py:1293-1312 apply_boundary, dam_break_3d.py:429-452       */
+/* apply_boundary_3d, kleefsman_obstacle_3d.py:208-266 clamp_out_of_obstacle */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  int64_t dim, dtype, n;
+  double lo[3], hi[3];   /* box clamp                                      */
+  double tolerance;      /* escape tolerance (0.25 dx)                     */
+  int64_t has_obstacle;
+  double ob_lo[3], ob_hi[3], ob_eps;
+} tsph_clamp_params;
+
+/* v += dt a; x += dt v; box clamp; optional obstacle clamp.  Counters:
+ * counters[0] += escapes, counters[1] += obstacle clamps (device int64). */
+int tsph_euler_clamp(const tsph_clamp_params* prm, void* pos, void* vel, const void* acc,
+                     double dt, int64_t* counters, tsph_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TSPH_H */

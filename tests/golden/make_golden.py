@@ -1,0 +1,340 @@
+"""Generate golden input/output fixtures by running the reference TensorSPH.
+
+Run in a checkout that has the reference source tree (not on the GPU host):
+
+    python tests/golden/make_golden.py /path/to/TensorSPH/src
+
+Every case seeds its own ``torch.Generator``; inputs and the reference's
+outputs are stored together in one ``.npz`` per case family, with the torch
+version that produced them.  The committed fixtures are what the oracle and
+the CUDA path are pinned against.
+"""
+from __future__ import annotations
+
+import math
+import sys
+from pathlib import Path
+
+import numpy as np
+import torch
+
+OUT = Path(__file__).resolve().parent
+
+
+def _np(t):
+    return t.detach().cpu().numpy()
+
+
+def capture_order(fn, *args):
+    """Run ``fn`` and record the first stable ``torch.argsort`` it performs.
+
+    ``cell_linked_pairs`` / ``periodic_pairs`` sort the particles by cell with
+    one stable argsort before they expand candidates; that permutation is the
+    cell order the CUDA counting sort must reproduce bit for bit.
+    """
+    seen = []
+    real = torch.argsort
+
+    def spy(*a, **k):
+        out = real(*a, **k)
+        if k.get("stable") and not seen:
+            seen.append(out.clone())
+        return out
+
+    torch.argsort = spy
+    try:
+        result = fn(*args)
+    finally:
+        torch.argsort = real
+    return result, (seen[0] if seen else torch.empty(0, dtype=torch.long))
+
+
+def pairs_cases(ns):
+    data = {}
+    k = 0
+    for dim in (1, 2, 3):
+        for dtype in (torch.float32, torch.float64):
+            for seed in (0, 7):
+                g = torch.Generator().manual_seed(seed + 100 * dim)
+                pos = (4.0 * torch.randn((301, dim), generator=g)).to(dtype)
+                pos[1] = pos[0]
+                pos[2] = pos[0] + 0.25 * torch.nn.functional.one_hot(
+                    torch.tensor(0), num_classes=dim).to(dtype)
+                for cutoff in (0.25, 0.7):
+                    pairs, order = capture_order(ns.cell_linked_pairs, pos, cutoff)
+                    brute = ns.brute_force_pairs(pos, cutoff)
+                    assert torch.equal(pairs, brute)
+                    data[f"c{k}_pos"] = _np(pos)
+                    data[f"c{k}_cutoff"] = np.float64(cutoff)
+                    data[f"c{k}_pairs"] = _np(pairs)
+                    data[f"c{k}_order"] = _np(order)
+                    k += 1
+    # uniform clouds exercise dense cells; lattice points sit exactly at the cutoff
+    for dtype in (torch.float32, torch.float64):
+        g = torch.Generator().manual_seed(21)
+        pos = torch.rand((2000, 2), generator=g).to(dtype)
+        pairs, order = capture_order(ns.cell_linked_pairs, pos, 0.05)
+        data[f"c{k}_pos"], data[f"c{k}_cutoff"] = _np(pos), np.float64(0.05)
+        data[f"c{k}_pairs"], data[f"c{k}_order"] = _np(pairs), _np(order)
+        k += 1
+        xs = torch.arange(20, dtype=dtype) * 0.1
+        gx, gy = torch.meshgrid(xs, xs, indexing="xy")
+        lat = torch.stack((gx.reshape(-1), gy.reshape(-1)), -1)
+        pairs, order = capture_order(ns.cell_linked_pairs, lat, 0.2)
+        data[f"c{k}_pos"], data[f"c{k}_cutoff"] = _np(lat), np.float64(0.2)
+        data[f"c{k}_pairs"], data[f"c{k}_order"] = _np(pairs), _np(order)
+        k += 1
+    clustered = torch.full((30, 2), 2.5, dtype=torch.float64)
+    clustered[0] = torch.tensor([-4.0, 7.0], dtype=torch.float64)
+    pairs, order = capture_order(ns.cell_linked_pairs, clustered, 0.2)
+    data[f"c{k}_pos"], data[f"c{k}_cutoff"] = _np(clustered), np.float64(0.2)
+    data[f"c{k}_pairs"], data[f"c{k}_order"] = _np(pairs), _np(order)
+    k += 1
+    data["count"] = np.int64(k)
+    return data
+
+
+def periodic_cases(n3):
+    data = {}
+    k = 0
+    for dtype in (torch.float32, torch.float64):
+        for seed, npart, cutoff in ((7, 300, 0.12), (3, 800, 0.2)):
+            g = torch.Generator().manual_seed(seed)
+            pos = (torch.rand((npart, 3), generator=g)).to(dtype)
+            pairs, order = capture_order(n3.periodic_pairs, pos, 1.0, cutoff)
+            brute = n3.brute_force_pairs_min_image(pos, 1.0, cutoff)
+            assert torch.equal(pairs, brute)
+            data[f"c{k}_pos"], data[f"c{k}_cutoff"] = _np(pos), np.float64(cutoff)
+            data[f"c{k}_box"] = np.float64(1.0)
+            data[f"c{k}_pairs"], data[f"c{k}_order"] = _np(pairs), _np(order)
+            k += 1
+    data["count"] = np.int64(k)
+    return data
+
+
+def rhs2d_cases(di, db):
+    """2-D ``rhs`` on dam-break states with walls, several option sets."""
+    data = {}
+    k = 0
+    option_sets = [
+        dict(),
+        dict(density_diffusion=0.1),
+        dict(density_diffusion=0.1, density_diffusion_form="antuono", wall_friction=0.5),
+        dict(density_renormalization=True, wall_friction=1.0),
+        dict(boundary_consistent_density=True),
+    ]
+    for dtype in (torch.float32, torch.float64):
+        torch.set_default_dtype(dtype)
+        try:
+            for oi, opts in enumerate(option_sets):
+                cfg = db.DamBreakConfig(dx=0.05, column_width=0.5, column_height=0.6,
+                                        pool_width=1.2, tank_height=0.9, sound_speed=20.0,
+                                        viscosity=1e-3, dt=2e-4, **opts)
+                pos, mass = db.make_column(cfg, torch.device("cpu"))
+                wall = di.wall_lattice(cfg, torch.device("cpu"), top=cfg.tank_top())
+                g = torch.Generator().manual_seed(31 + oi)
+                pos = pos + 0.1 * cfg.dx * torch.randn(pos.shape, generator=g).to(dtype)
+                vel = 0.3 * torch.randn(pos.shape, generator=g).to(dtype)
+                h = cfg.h_factor * cfg.dx
+                all_pos = torch.cat((pos, wall))
+                cache = di.PairListCache(2.0 * h, 0.25 * h, fluid_count=pos.shape[0])
+                pairs, _ = cache.get(all_pos)
+                split = oi in (2, 3)
+                out = di.rhs(pos, vel, mass, cfg, pairs=pairs, wall=wall, dt=cfg.dt,
+                             split=split)
+                data[f"c{k}_pos"], data[f"c{k}_vel"] = _np(pos), _np(vel)
+                data[f"c{k}_mass"], data[f"c{k}_wall"] = _np(mass), _np(wall)
+                data[f"c{k}_pairs"] = _np(pairs)
+                data[f"c{k}_opts"] = np.int64(oi)
+                data[f"c{k}_split"] = np.int64(split)
+                data[f"c{k}_rho"], data[f"c{k}_p"], data[f"c{k}_acc"] = map(_np, out[:3])
+                if split:
+                    data[f"c{k}_reaction"] = _np(out[3]["reaction"])
+                    data[f"c{k}_face_pressure"] = _np(out[3]["face_pressure"])
+                k += 1
+        finally:
+            torch.set_default_dtype(torch.float32)
+    data["count"] = np.int64(k)
+    return data
+
+
+def config1_case(di, db):
+    """One ``rhs`` of the 5,000-particle dam break (dx = 0.02) at rest."""
+    data = {}
+    c0 = 10.0 * math.sqrt(2.0 * 9.81 * 2.0)
+    for tag, dtype in (("f32", torch.float32), ("f64", torch.float64)):
+        torch.set_default_dtype(dtype)
+        try:
+            cfg = db.DamBreakConfig(dx=0.02, column_width=1.0, column_height=2.0,
+                                    pool_width=4.0, tank_height=3.0, sound_speed=c0,
+                                    viscosity=1e-6, max_courant=0.25,
+                                    dt=0.25 * 1.3 * 0.02 / c0, steps=1000, wall_layers=3)
+            pos, mass = db.make_column(cfg, torch.device("cpu"))
+            wall = di.wall_lattice(cfg, torch.device("cpu"), top=cfg.tank_top())
+            h = cfg.h_factor * cfg.dx
+            cache = di.PairListCache(2.0 * h, cfg.pair_skin_factor * h,
+                                     fluid_count=pos.shape[0])
+            pairs, _ = cache.get(torch.cat((pos, wall)))
+            vel = torch.zeros_like(pos)
+            rho, p, acc = di.rhs(pos, vel, mass, cfg, pairs=pairs, wall=wall, dt=cfg.dt)
+            # one semi-implicit Euler step and a second rhs from the moved state
+            vel2 = vel + cfg.dt * acc
+            pos2 = pos + cfg.dt * vel2
+            di.apply_boundary(pos2, vel2, cfg, top=cfg.tank_top())
+            pairs2, rebuilt = cache.get(torch.cat((pos2, wall)))
+            rho2, p2, acc2 = di.rhs(pos2, vel2, mass, cfg, pairs=pairs2, wall=wall, dt=cfg.dt)
+            for name, t in dict(pos=pos, mass=mass, wall=wall, pairs=pairs, rho=rho, p=p,
+                                acc=acc, pos2=pos2, vel2=vel2, rho2=rho2, p2=p2,
+                                acc2=acc2).items():
+                data[f"{tag}_{name}"] = _np(t)
+            data[f"{tag}_rebuilt2"] = np.int64(rebuilt)
+        finally:
+            torch.set_default_dtype(torch.float32)
+    return data
+
+
+def rhs3d_cases(d3, di):
+    data = {}
+    k = 0
+    for dtype in (torch.float32, torch.float64):
+        for opts in (dict(), dict(density_diffusion=0.1, wall_friction=0.3)):
+            torch.set_default_dtype(dtype)
+            try:
+                cfg = d3.DamBreak3DConfig(dx=0.04, tank_height=0.4, tank_depth=0.2,
+                                          column_width=0.2, column_depth=0.2,
+                                          column_height=0.24, pool_width=0.5,
+                                          sound_speed=15.0, viscosity=1e-3, dt=1e-4, **opts)
+                pos, mass = d3.make_column_3d(cfg, torch.device("cpu"), seed=5)
+                wall = d3.wall_lattice_3d(cfg, torch.device("cpu"))
+                g = torch.Generator().manual_seed(9 + k)
+                pos = pos + 0.1 * cfg.dx * torch.randn(pos.shape, generator=g).to(dtype)
+                vel = 0.2 * torch.randn(pos.shape, generator=g).to(dtype)
+                h = cfg.h_factor * cfg.dx
+                cache = di.PairListCache(2.0 * h, 0.25 * h, fluid_count=pos.shape[0])
+                pairs, _ = cache.get(torch.cat((pos, wall)))
+                rho, p, acc, reaction = d3.rhs_3d(pos, vel, mass, cfg, pairs=pairs, wall=wall,
+                                                  dt=cfg.dt, return_wall_force=True)
+                for name, t in dict(pos=pos, vel=vel, mass=mass, wall=wall, pairs=pairs,
+                                    rho=rho, p=p, acc=acc, reaction=reaction).items():
+                    data[f"c{k}_{name}"] = _np(t)
+                data[f"c{k}_diffusion"] = np.float64(cfg.density_diffusion)
+                data[f"c{k}_friction"] = np.float64(cfg.wall_friction)
+                k += 1
+            finally:
+                torch.set_default_dtype(torch.float32)
+    data["count"] = np.int64(k)
+    return data
+
+
+def threed_cases(t3):
+    data = {}
+    k = 0
+    # periodic shear lattice with jitter (config 2 shape, reduced to 12^3)
+    for dtype in (torch.float32, torch.float64):
+        for order in (2, 4):
+            n = 12
+            dx = 1.0 / n
+            h = 1.3 * dx
+            pos = t3.cubic_lattice((n, n, n), dx, dtype=dtype)
+            g = torch.Generator().manual_seed(3 + order)
+            pos = (pos + (torch.rand(pos.shape, generator=g).to(dtype) - 0.5) * 0.02 * dx
+                   ).remainder(1.0)
+            mass = torch.full((pos.shape[0],), t3.calibrated_particle_mass(dx, h, 1000.0),
+                              dtype=dtype)
+            vel = torch.zeros_like(pos)
+            vel[:, 0] = 1e-3 * torch.sin(2 * math.pi * pos[:, 2])
+            pairs = t3.periodic_pairs(pos, 1.0, 2.5 * h)
+            acc, rho, p = t3.accelerations(pos, vel, mass, h, pairs, rho0=1000.0,
+                                           sound_speed=1.0, viscosity=1e-2, box=1.0,
+                                           viscous_order=order)
+            for name, t in dict(pos=pos, vel=vel, mass=mass, pairs=pairs, acc=acc,
+                                rho=rho, p=p).items():
+                data[f"c{k}_{name}"] = _np(t)
+            data[f"c{k}_kind"] = np.int64(0)
+            data[f"c{k}_h"], data[f"c{k}_order"] = np.float64(h), np.int64(order)
+            k += 1
+    # wall-bounded hydrostatic column with Antuono diffusion
+    for dtype in (torch.float32, torch.float64):
+        for form in ("antuono", "molteni"):
+            dx = 0.01
+            h = 1.3 * dx
+            fluid = t3.cubic_lattice((6, 6, 5), dx, origin=(0.02, 0.02, 0.02), dtype=dtype)
+            wall = t3.wall_shell((6, 6, 5), 2, dx, dtype=dtype)
+            pos = torch.cat((fluid, wall))
+            g = torch.Generator().manual_seed(17)
+            pos[: fluid.shape[0]] += 0.05 * dx * torch.randn(fluid.shape, generator=g).to(dtype)
+            mass = torch.full((pos.shape[0],), t3.calibrated_particle_mass(dx, h, 1000.0),
+                              dtype=dtype)
+            vel = 0.05 * torch.randn(pos.shape, generator=g).to(dtype)
+            vel[fluid.shape[0]:] = 0
+            pairs = t3.box_pairs(pos, 2.0 * h)
+            acc, rho, p = t3.accelerations(
+                pos, vel, mass, h, pairs, rho0=1000.0, sound_speed=20.0, viscosity=0.02,
+                gravity=torch.tensor([0.0, 0.0, -9.81], dtype=dtype), n_fluid=fluid.shape[0],
+                density_diffusion=0.1, dt=1e-4, density_diffusion_form=form)
+            for name, t in dict(pos=pos, vel=vel, mass=mass, pairs=pairs, acc=acc,
+                                rho=rho, p=p).items():
+                data[f"c{k}_{name}"] = _np(t)
+            data[f"c{k}_kind"] = np.int64(1 if form == "antuono" else 2)
+            data[f"c{k}_h"], data[f"c{k}_nfluid"] = np.float64(h), np.int64(fluid.shape[0])
+            k += 1
+    data["count"] = np.int64(k)
+    return data
+
+
+def shift_cases(ps, di):
+    data = {}
+    k = 0
+    for dtype in (torch.float32, torch.float64):
+        for dim in (2, 3):
+            g = torch.Generator().manual_seed(40 + dim)
+            side = 14 if dim == 2 else 7
+            dx = 0.05
+            axes = [torch.arange(side, dtype=dtype) * dx for _ in range(dim)]
+            grid = torch.stack(torch.meshgrid(*axes, indexing="ij"), -1).reshape(-1, dim)
+            pos = grid + 0.15 * dx * torch.randn(grid.shape, generator=g).to(dtype)
+            volume = torch.full((pos.shape[0],), dx ** dim, dtype=dtype) * (
+                1.0 + 0.05 * torch.rand((pos.shape[0],), generator=g).to(dtype))
+            h = 1.3 * dx
+            out, state = ps.shift_positions(pos, volume, h, dt=1e-3, v_ref=2.0,
+                                            return_state=True)
+            for name, t in dict(pos=pos, volume=volume, out=out, c=state.concentration,
+                                grad=state.grad_c, shift=state.shift).items():
+                data[f"c{k}_{name}"] = _np(t)
+            data[f"c{k}_h"], data[f"c{k}_cref"] = np.float64(h), np.float64(state.c_reference)
+            k += 1
+    data["count"] = np.int64(k)
+    return data
+
+
+def main(src):
+    sys.path.insert(0, str(src))
+    import tensorsph.neighbor_search as ns
+    import tensorsph.droplet_impact as di
+    import tensorsph.dam_break as db
+    import tensorsph.dam_break_3d as d3
+    import tensorsph.particle_shifting as ps
+    import tensorsph.threed as t3
+    from tensorsph.threed import neighbors3 as n3
+
+    meta = {"torch_version": np.array(torch.__version__)}
+    torch.set_num_threads(1)
+    np.savez_compressed(OUT / "pairs.npz", **pairs_cases(ns), **meta)
+    np.savez_compressed(OUT / "periodic.npz", **periodic_cases(n3), **meta)
+    np.savez_compressed(OUT / "rhs2d.npz", **rhs2d_cases(di, db), **meta)
+    np.savez_compressed(OUT / "config1.npz", **config1_case(di, db), **meta)
+    np.savez_compressed(OUT / "rhs3d.npz", **rhs3d_cases(d3, di), **meta)
+    np.savez_compressed(OUT / "threed.npz", **threed_cases(t3), **meta)
+    np.savez_compressed(OUT / "shift.npz", **shift_cases(ps, di), **meta)
+
+
+RHS2D_OPTION_SETS = [
+    dict(),
+    dict(density_diffusion=0.1),
+    dict(density_diffusion=0.1, density_diffusion_form="antuono", wall_friction=0.5),
+    dict(density_renormalization=True, wall_friction=1.0),
+    dict(boundary_consistent_density=True),
+]
+
+if __name__ == "__main__":
+    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"))

@@ -1,0 +1,149 @@
+"""Pin the numpy oracle against fixtures produced by the reference itself."""
+from types import SimpleNamespace
+
+import numpy as np
+import pytest
+
+from oracle import neighbors as on
+from oracle import pairpass as op
+from tests.golden.make_golden import RHS2D_OPTION_SETS
+
+
+def rel_err(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    scale = max(float(np.abs(b).max()), 1e-300)
+    return float(np.abs(a - b).max()) / scale
+
+
+def test_pairs_and_cell_order_bit_exact(golden):
+    g = golden("pairs")
+    for k in range(int(g["count"])):
+        pos, cutoff = g[f"c{k}_pos"], float(g[f"c{k}_cutoff"])
+        pairs = on.cell_linked_pairs(pos, cutoff)
+        assert np.array_equal(pairs, g[f"c{k}_pairs"]), k
+        *_, order = on.cell_grid(pos, cutoff)
+        assert np.array_equal(order, g[f"c{k}_order"]), k
+        if pos.shape[0] <= 400:
+            assert np.array_equal(on.brute_force_pairs(pos, cutoff), g[f"c{k}_pairs"]), k
+
+
+def test_periodic_pairs_bit_exact(golden):
+    g = golden("periodic")
+    for k in range(int(g["count"])):
+        pos, cutoff = g[f"c{k}_pos"], float(g[f"c{k}_cutoff"])
+        pairs = on.periodic_pairs(pos, float(g[f"c{k}_box"]), cutoff)
+        assert np.array_equal(pairs, g[f"c{k}_pairs"]), k
+        *_, order = on.periodic_grid(pos, float(g[f"c{k}_box"]), cutoff)
+        assert np.array_equal(order, g[f"c{k}_order"]), k
+
+
+def _cfg2d(opts, **kw):
+    base = dict(dx=0.05, h_factor=1.3, rho0=1000.0, sound_speed=20.0, gamma=7.0,
+                gravity=9.81, viscosity=1e-3, dt=2e-4, wall_friction=0.0,
+                density_diffusion=0.0, density_diffusion_form="molteni",
+                density_diffusion_eigenvalue_floor=0.1, density_calibration=True,
+                density_renormalization=False, boundary_consistent_density=False)
+    base.update(kw)
+    base.update(opts)
+    return SimpleNamespace(**base)
+
+
+def test_rhs2d_matches_reference(golden):
+    g = golden("rhs2d")
+    for k in range(int(g["count"])):
+        opts = RHS2D_OPTION_SETS[int(g[f"c{k}_opts"])]
+        cfg = _cfg2d(opts)
+        split = bool(g[f"c{k}_split"])
+        out = op.rhs(g[f"c{k}_pos"], g[f"c{k}_vel"], g[f"c{k}_mass"], cfg,
+                     pairs=g[f"c{k}_pairs"], wall=g[f"c{k}_wall"], dt=cfg.dt, split=split)
+        tol = 1e-12 if g[f"c{k}_pos"].dtype == np.float64 else 2e-5
+        assert rel_err(out[0], g[f"c{k}_rho"]) < tol, k
+        assert rel_err(out[1], g[f"c{k}_p"]) < max(tol, 1e-11) * 50, k
+        assert rel_err(out[2], g[f"c{k}_acc"]) < max(tol, 1e-11) * 50, k
+        if split:
+            assert rel_err(out[3]["reaction"], g[f"c{k}_reaction"]) < max(tol, 1e-11) * 50
+            assert rel_err(out[3]["face_pressure"], g[f"c{k}_face_pressure"]) < max(tol, 1e-11) * 50
+
+
+def test_config1_state_matches_reference(golden):
+    import math
+    g = golden("config1")
+    c0 = 10.0 * math.sqrt(2.0 * 9.81 * 2.0)
+    cfg = _cfg2d({}, dx=0.02, sound_speed=c0, viscosity=1e-6, dt=0.25 * 1.3 * 0.02 / c0)
+    for tag in ("f32", "f64"):
+        pos = g[f"{tag}_pos"]
+        rho, p, acc = op.rhs(pos, np.zeros_like(pos), g[f"{tag}_mass"], cfg,
+                             pairs=g[f"{tag}_pairs"], wall=g[f"{tag}_wall"], dt=cfg.dt)
+        tol = 1e-12 if tag == "f64" else 2e-5
+        assert rel_err(rho, g[f"{tag}_rho"]) < tol
+        assert rel_err(p, g[f"{tag}_p"]) < tol * 50
+        assert rel_err(acc, g[f"{tag}_acc"]) < tol * 50
+
+
+def test_rhs3d_matches_reference(golden):
+    g = golden("rhs3d")
+    for k in range(int(g["count"])):
+        cfg = SimpleNamespace(dx=0.04, h_factor=1.3, rho0=1000.0, sound_speed=15.0, gamma=7.0,
+                              gravity=9.81, viscosity=1e-3, dt=1e-4,
+                              wall_friction=float(g[f"c{k}_friction"]),
+                              density_diffusion=float(g[f"c{k}_diffusion"]),
+                              density_diffusion_form="molteni", density_calibration=True)
+        out = op.rhs_3d(g[f"c{k}_pos"], g[f"c{k}_vel"], g[f"c{k}_mass"], cfg,
+                        pairs=g[f"c{k}_pairs"], wall=g[f"c{k}_wall"], dt=cfg.dt,
+                        return_wall_force=True)
+        tol = 1e-12 if g[f"c{k}_pos"].dtype == np.float64 else 2e-5
+        for got, name in zip(out, ("rho", "p", "acc", "reaction")):
+            assert rel_err(got, g[f"c{k}_{name}"]) < tol * (1 if name == "rho" else 50), (k, name)
+
+
+def test_threed_accelerations_match_reference(golden):
+    g = golden("threed")
+    for k in range(int(g["count"])):
+        kind = int(g[f"c{k}_kind"])
+        pos = g[f"c{k}_pos"]
+        tol = 1e-12 if pos.dtype == np.float64 else 2e-5
+        if kind == 0:
+            acc, rho, p = op.accelerations(pos, g[f"c{k}_vel"], g[f"c{k}_mass"],
+                                           float(g[f"c{k}_h"]), g[f"c{k}_pairs"],
+                                           rho0=1000.0, sound_speed=1.0, viscosity=1e-2,
+                                           box=1.0, viscous_order=int(g[f"c{k}_order"]))
+        else:
+            acc, rho, p = op.accelerations(
+                pos, g[f"c{k}_vel"], g[f"c{k}_mass"], float(g[f"c{k}_h"]), g[f"c{k}_pairs"],
+                rho0=1000.0, sound_speed=20.0, viscosity=0.02,
+                gravity=np.array([0.0, 0.0, -9.81]), n_fluid=int(g[f"c{k}_nfluid"]),
+                density_diffusion=0.1, dt=1e-4,
+                density_diffusion_form="antuono" if kind == 1 else "molteni")
+        assert rel_err(rho, g[f"c{k}_rho"]) < tol, k
+        assert rel_err(p, g[f"c{k}_p"]) < tol * 1e3, k
+        assert rel_err(acc, g[f"c{k}_acc"]) < tol * 1e3, k
+
+
+def test_shift_positions_match_reference(golden):
+    g = golden("shift")
+    for k in range(int(g["count"])):
+        pos = g[f"c{k}_pos"]
+        out, st = op.shift_positions(pos, g[f"c{k}_volume"], float(g[f"c{k}_h"]),
+                                     dt=1e-3, v_ref=2.0)
+        tol = 1e-12 if pos.dtype == np.float64 else 2e-5
+        assert rel_err(st["concentration"], g[f"c{k}_c"]) < tol
+        assert rel_err(st["grad_c"], g[f"c{k}_grad"]) < tol * 100
+        assert abs(st["c_reference"] - float(g[f"c{k}_cref"])) <= 1e-6 * abs(float(g[f"c{k}_cref"]))
+        assert rel_err(st["shift"], g[f"c{k}_shift"]) < tol * 100
+        assert rel_err(out - pos, g[f"c{k}_out"] - pos) < tol * 1e3
+
+
+def test_pair_cache_rebuild_rule():
+    rng = np.random.default_rng(3)
+    pos = rng.random((200, 2))
+    cache = on.PairListCache(0.1, 0.02, fluid_count=150)
+    p1, rebuilt = cache.get(pos)
+    assert rebuilt and cache.rebuilds == 1
+    _, rebuilt = cache.get(pos + 0.006)  # |d| = 0.0085 < skin / 2
+    assert not rebuilt and cache.reuses == 1
+    _, rebuilt = cache.get(pos + 0.02)
+    assert rebuilt and cache.rebuilds == 2
+    assert ((p1[:, 0] < 150) | (p1[:, 1] < 150)).all()
+    with pytest.raises(ValueError):
+        on.PairListCache(0.0, 0.1)
