@@ -81,14 +81,15 @@ class ClampParams(ctypes.Structure):
 
 class EngineParams(ctypes.Structure):
     _fields_ = [(k, c_int64) for k in ("n_fluid", "n_wall", "n_obstacle", "max_neighbors",
-                                       "shift_every")] + \
+                                       "shift_every", "diag_ring", "has_obstacle")] + \
                [(k, c_double) for k in ("dx", "h", "rho0", "sound_speed", "gamma", "gravity",
                                         "viscosity", "wall_friction", "diffusion_scale", "dt",
                                         "wall_mass", "skin")] + \
-               [("box_hi", c_double * 3), ("tolerance", c_double), ("has_obstacle", c_int64),
-                ("ob_lo", c_double * 3), ("ob_hi", c_double * 3), ("ob_eps", c_double),
-                ("shift_strength", c_double), ("shift_limit", c_double),
-                ("shift_free_surface", c_double), ("shift_vref_floor", c_double)]
+               [("box_hi", c_double * 3), ("tolerance", c_double), ("ob_lo", c_double * 3),
+                ("ob_hi", c_double * 3), ("ob_eps", c_double), ("shift_strength", c_double),
+                ("shift_limit", c_double), ("shift_free_surface", c_double),
+                ("shift_vref_floor", c_double), ("grid_lo", c_double * 3),
+                ("grid_hi", c_double * 3)]
 
 
 _SIGNATURES = {
@@ -127,6 +128,15 @@ _SIGNATURES = {
                               c_void_p]),
     "tsph_euler_clamp": (c_int, [POINTER(ClampParams), c_void_p, c_void_p, c_void_p, c_double,
                                  c_void_p, c_void_p]),
+    "tsph_engine_bytes": (c_int64, [POINTER(EngineParams)]),
+    "tsph_engine_create": (c_int, [POINTER(EngineParams), c_void_p, c_int64, c_void_p, c_void_p,
+                                   c_void_p, c_void_p, c_void_p, POINTER(c_void_p)]),
+    "tsph_engine_step": (c_int, [c_void_p, c_int64, c_void_p]),
+    "tsph_engine_step_eager": (c_int, [c_void_p, c_int64, c_void_p]),
+    "tsph_engine_read": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "tsph_engine_diag": (c_int, [c_void_p, c_void_p, c_int64, c_int64, c_void_p]),
+    "tsph_engine_status": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "tsph_engine_destroy": (c_int, [c_void_p]),
 }
 
 EXPORTED = tuple(_SIGNATURES)

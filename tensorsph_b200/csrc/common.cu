@@ -10,7 +10,9 @@ constexpr int kScanItems = 4;
 constexpr int64_t kScanTile = kScanBlock * kScanItems;
 
 template <class TIn>
-__global__ void scan_tile_totals(const TIn* __restrict__ in, int64_t n, int64_t* __restrict__ totals) {
+__global__ void scan_tile_totals(const TIn* __restrict__ in, int64_t n, int64_t* __restrict__ totals,
+                                 const int* __restrict__ enable) {
+  if (enable && !*enable) return;
   const int64_t base = blockIdx.x * kScanTile;
   int64_t local = 0;
 #pragma unroll
@@ -25,7 +27,9 @@ __global__ void scan_tile_totals(const TIn* __restrict__ in, int64_t n, int64_t*
 
 template <class TIn>
 __global__ void scan_tile_apply(const TIn* __restrict__ in, int64_t* __restrict__ out, int64_t n,
-                                const int64_t* __restrict__ offsets, int64_t* __restrict__ grand) {
+                                const int64_t* __restrict__ offsets, int64_t* __restrict__ grand,
+                                const int* __restrict__ enable) {
+  if (enable && !*enable) return;
   const int64_t base = blockIdx.x * kScanTile;
   int64_t vals[kScanItems];
   int64_t local = 0;
@@ -58,37 +62,38 @@ size_t scan_scratch_bytes(int64_t n) {
 
 template <class TIn>
 static int scan_impl(const TIn* in, int64_t* out, int64_t n, int64_t* total, char* scratch,
-                     cudaStream_t s) {
+                     cudaStream_t s, const int* enable) {
   if (n <= 0) {
     if (total) TSPH_CUDA_CHECK(cudaMemsetAsync(total, 0, sizeof(int64_t), s));
     return TSPH_OK;
   }
   const int64_t blocks = (n + kScanTile - 1) / kScanTile;
   if (blocks == 1) {
-    scan_tile_apply<TIn><<<1, kScanBlock, 0, s>>>(in, out, n, nullptr, total);
+    scan_tile_apply<TIn><<<1, kScanBlock, 0, s>>>(in, out, n, nullptr, total, enable);
     TSPH_LAUNCH_CHECK();
     return TSPH_OK;
   }
   int64_t* totals = reinterpret_cast<int64_t*>(scratch);
   int64_t* offsets = reinterpret_cast<int64_t*>(scratch + align_up((blocks + 1) * sizeof(int64_t)));
   char* next = scratch + 2 * align_up((blocks + 1) * sizeof(int64_t));
-  scan_tile_totals<TIn><<<static_cast<unsigned>(blocks), kScanBlock, 0, s>>>(in, n, totals);
+  scan_tile_totals<TIn><<<static_cast<unsigned>(blocks), kScanBlock, 0, s>>>(in, n, totals, enable);
   TSPH_LAUNCH_CHECK();
-  int rc = scan_impl<int64_t>(totals, offsets, blocks, nullptr, next, s);
+  int rc = scan_impl<int64_t>(totals, offsets, blocks, nullptr, next, s, enable);
   if (rc) return rc;
-  scan_tile_apply<TIn><<<static_cast<unsigned>(blocks), kScanBlock, 0, s>>>(in, out, n, offsets, total);
+  scan_tile_apply<TIn><<<static_cast<unsigned>(blocks), kScanBlock, 0, s>>>(in, out, n, offsets, total,
+                                                                            enable);
   TSPH_LAUNCH_CHECK();
   return TSPH_OK;
 }
 
 int exclusive_scan_i64(const int64_t* in, int64_t* out, int64_t n, int64_t* total, void* scratch,
-                       cudaStream_t s) {
-  return scan_impl<int64_t>(in, out, n, total, static_cast<char*>(scratch), s);
+                       cudaStream_t s, const int* enable) {
+  return scan_impl<int64_t>(in, out, n, total, static_cast<char*>(scratch), s, enable);
 }
 
 int exclusive_scan_i32_to_i64(const int32_t* in, int64_t* out, int64_t n, int64_t* total,
-                              void* scratch, cudaStream_t s) {
-  return scan_impl<int32_t>(in, out, n, total, static_cast<char*>(scratch), s);
+                              void* scratch, cudaStream_t s, const int* enable) {
+  return scan_impl<int32_t>(in, out, n, total, static_cast<char*>(scratch), s, enable);
 }
 
 // ------------------------------------------------------------- radix sort ---
@@ -98,7 +103,8 @@ constexpr int kRadixRounds = 8;
 constexpr int64_t kRadixTile = kRadixBlock * kRadixRounds;
 
 __global__ void radix_histogram(const uint64_t* __restrict__ keys, int64_t n, int shift,
-                                int32_t* __restrict__ table, int64_t nblocks) {
+                                int32_t* __restrict__ table, int64_t nblocks, const int* __restrict__ enable) {
+  if (enable && !*enable) return;
   __shared__ int32_t hist[256];
   hist[threadIdx.x] = 0;
   __syncthreads();
@@ -116,7 +122,8 @@ __global__ void radix_histogram(const uint64_t* __restrict__ keys, int64_t n, in
 __global__ void radix_scatter(const uint64_t* __restrict__ keys_in, const int32_t* __restrict__ vals_in,
                               uint64_t* __restrict__ keys_out, int32_t* __restrict__ vals_out,
                               int64_t n, int shift, const int64_t* __restrict__ offsets,
-                              int64_t nblocks) {
+                              int64_t nblocks, const int* __restrict__ enable) {
+  if (enable && !*enable) return;
   __shared__ int32_t warp_cnt[kRadixBlock / 32][256];
   __shared__ int64_t base_off[256];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -164,8 +171,18 @@ size_t radix_scratch_bytes(int64_t n) {
   return align_up(m * sizeof(int32_t)) + align_up(m * sizeof(int64_t)) + scan_scratch_bytes(m);
 }
 
+__global__ void radix_copy_back(const uint64_t* __restrict__ ks, const int32_t* __restrict__ vs,
+                                uint64_t* __restrict__ kd, int32_t* __restrict__ vd, int64_t n,
+                                const int* __restrict__ enable) {
+  if (enable && !*enable) return;
+  for (int64_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    kd[i] = ks[i];
+    vd[i] = vs[i];
+  }
+}
+
 int radix_sort_u64_i32(uint64_t* keys, int32_t* vals, uint64_t* keys_tmp, int32_t* vals_tmp,
-                       int64_t n, int bits, void* scratch, cudaStream_t s) {
+                       int64_t n, int bits, void* scratch, cudaStream_t s, const int* enable) {
   if (n <= 1 || bits <= 0) return TSPH_OK;
   const int64_t nblocks = (n + kRadixTile - 1) / kRadixTile;
   const int64_t m = 256 * nblocks;
@@ -177,19 +194,20 @@ int radix_sort_u64_i32(uint64_t* keys, int32_t* vals, uint64_t* keys_tmp, int32_
   int32_t *va = vals, *vb = vals_tmp;
   int passes = 0;
   for (int shift = 0; shift < bits; shift += 8, ++passes) {
-    radix_histogram<<<static_cast<unsigned>(nblocks), kRadixBlock, 0, s>>>(ka, n, shift, table, nblocks);
+    radix_histogram<<<static_cast<unsigned>(nblocks), kRadixBlock, 0, s>>>(ka, n, shift, table, nblocks,
+                                                                            enable);
     TSPH_LAUNCH_CHECK();
-    int rc = exclusive_scan_i32_to_i64(table, offsets, m, nullptr, scan_sc, s);
+    int rc = exclusive_scan_i32_to_i64(table, offsets, m, nullptr, scan_sc, s, enable);
     if (rc) return rc;
     radix_scatter<<<static_cast<unsigned>(nblocks), kRadixBlock, 0, s>>>(ka, va, kb, vb, n, shift,
-                                                                          offsets, nblocks);
+                                                                          offsets, nblocks, enable);
     TSPH_LAUNCH_CHECK();
     uint64_t* kt = ka; ka = kb; kb = kt;
     int32_t* vt = va; va = vb; vb = vt;
   }
   if (passes & 1) {
-    TSPH_CUDA_CHECK(cudaMemcpyAsync(keys, ka, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
-    TSPH_CUDA_CHECK(cudaMemcpyAsync(vals, va, n * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+    radix_copy_back<<<grid_for(n, 256), 256, 0, s>>>(ka, va, keys, vals, n, enable);
+    TSPH_LAUNCH_CHECK();
   }
   return TSPH_OK;
 }

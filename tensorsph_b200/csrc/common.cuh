@@ -136,16 +136,20 @@ __device__ __forceinline__ T block_exclusive_scan(T v, T* total) {
 // Device-wide exclusive scan of n elements (in place allowed), writing the
 // grand total to *total (device pointer, may be null).  Scratch: scan_scratch_bytes.
 size_t scan_scratch_bytes(int64_t n);
+// `enable` (nullable, device int): every kernel returns at once when *enable
+// is 0, so a fixed launch sequence can be captured in a CUDA graph and the
+// work switched on and off from the device.
 int exclusive_scan_i64(const int64_t* in, int64_t* out, int64_t n, int64_t* total, void* scratch,
-                       cudaStream_t s);
+                       cudaStream_t s, const int* enable = nullptr);
 int exclusive_scan_i32_to_i64(const int32_t* in, int64_t* out, int64_t n, int64_t* total,
-                              void* scratch, cudaStream_t s);
+                              void* scratch, cudaStream_t s, const int* enable = nullptr);
 
 // Stable LSD radix sort of (key, value) by the low `bits` bits of key.
 // keys/vals are sorted in place; tmp buffers of n elements each are needed.
 size_t radix_scratch_bytes(int64_t n);
 int radix_sort_u64_i32(uint64_t* keys, int32_t* vals, uint64_t* keys_tmp, int32_t* vals_tmp,
-                       int64_t n, int bits, void* scratch, cudaStream_t s);
+                       int64_t n, int bits, void* scratch, cudaStream_t s,
+                       const int* enable = nullptr);
 
 // Sort every row segment [rowptr[r], rowptr[r+1]) of `vals` ascending (uint32
 // comparison).  Scratch: segsort_scratch_bytes.

@@ -1,0 +1,1093 @@
+// Device-resident 3-D dam-break engine: the time loop of dam_break_3d.py:623-709
+// (with the obstacle wall force of kleefsman_obstacle_3d.py:644-706 and the
+// optional Lind shift of particle_shifting.py:166-224), one CUDA graph per step.
+//
+// Layout (all in one caller-provided arena, particles in cell order):
+//   pos  double4[N]   x, y, z, mass      fluid [0, nf), walls [nf, N)  (FP64 state)
+//   vel  double4[nf]  FP64 velocity
+//   vr   float4[N]    FP32 velocity + density (walls: 0 velocity, Adami density)
+//   pr   float[N]     pressure;  pq float[N] p / rho^2
+//   nbr  int32[maxnb * N]  k-major neighbour rows (coalesced per k), cnt[N]
+// Pair arithmetic is FP32 with compensated sums; separations are taken in
+// FP64 and rounded once, so a 1 m tank loses no digits against h ~ 1e-2 m.
+//
+// Step (fixed launch sequence, graph-captured):
+//   check/rebuild  skin test -> (cell keys, radix sort, permute, cell table, rows)
+//   E1 density -> E2 diffusion + Tait -> E3 Adami walls -> E4 force
+//   E5 obstacle reaction -> E6 Euler + clamps + meters -> E7 finalize meters
+//   [check/rebuild -> S1 concentration -> S2 gradient -> Q select -> S3 shift]
+// Every rebuild kernel reads the device flag and returns at once when no
+// rebuild is due, so the branch costs a few empty launches, no host sync.
+#include <cmath>
+#include <cstring>
+#include <new>
+
+#include "common.cuh"
+
+namespace tsph {
+namespace {
+
+constexpr int kBlock = 128;
+constexpr int kDiag = 16;
+
+struct Dev {
+  int nf, nw, N, nob, maxnb, shift_every, diag_ring;
+  int ncx, ncy, ncz;
+  double origin[3], cell, rc2, skin_half;
+  double dt, box_hi[3], tol, ob_lo[3], ob_hi[3], ob_eps;
+  int has_ob;
+  double gravity;
+  float h, inv_h, sigma, sig2d, support2, rho0, bulk, gamma, inv_gamma, grav, nu2, nu2f, dscale, dtf,
+      visc_eps, rho_floor, wall_mass;
+  double shift_strength_h_dt, shift_cap, shift_fs, vref_floor;
+  // arrays
+  double4* pos;
+  double4* vel;
+  double4* anchor;
+  int32_t* id;
+  int32_t* wall_id;
+  float4* vr;
+  float* pr;
+  float* pq;
+  float* rho_s;
+  float4* acc;
+  float* conc;
+  float4* gradc;
+  int32_t* nbr;
+  int32_t* cnt;
+  int32_t* ob_rows;
+  int32_t* fstart;
+  int32_t* fend;
+  int32_t* wstart;
+  int32_t* wend;
+  uint64_t* keys;
+  uint64_t* keys_tmp;
+  int32_t* vals;
+  int32_t* vals_tmp;
+  double4* tmp4a;
+  double4* tmp4b;
+  double4* tmp4c;
+  int32_t* tmp_id;
+  // control words
+  int* flag;         // [0] rebuild now, [1] first step, [2] shift this step, [3] shift done
+  unsigned long long* maxbits;  // [0] disp (integrate), [1] disp (shift), [2] rho, [3] speed, [4] front
+  int* status;       // bit 0: neighbour row overflow, bit 1: non-finite state
+  long long* counters;  // [0] escapes [1] clamps [2] rebuilds [3] step [4] max row [5] select k
+  double* partials;  // per-block sums: [blk*8 + 0..7]
+  int nblocks_int;   // blocks of the integrate kernel
+  int nblocks_ob;
+  double* impulse;   // 3
+  double* diag;      // diag_ring * kDiag
+  unsigned int* hist;        // 256
+  unsigned long long* sel;   // [0] prefix [1] value lo bits [2] value hi bits
+  double* cref;
+};
+
+__device__ __forceinline__ float shape(float q) {
+  if (q < 1.f) return 1.f - 1.5f * q * q + 0.75f * q * q * q;
+  if (q < 2.f) {
+    float t = 2.f - q;
+    return 0.25f * t * t * t;
+  }
+  return 0.f;
+}
+__device__ __forceinline__ float dshape(float q) {
+  if (q < 1.f) return -3.f * q + 2.25f * q * q;
+  if (q < 2.f) {
+    float t = 2.f - q;
+    return -0.75f * t * t;
+  }
+  return 0.f;
+}
+
+__device__ __forceinline__ double4 ld4(const double4* p, int i) {
+  const double2* q = reinterpret_cast<const double2*>(p + i);
+  double2 a = q[0], b = q[1];
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+
+__device__ __forceinline__ void st4(double4* p, int i, double4 v) {
+  double2* q = reinterpret_cast<double2*>(p + i);
+  q[0] = make_double2(v.x, v.y);
+  q[1] = make_double2(v.z, v.w);
+}
+
+__device__ __forceinline__ int cell_of(const Dev& e, double x, double y, double z, int& cx, int& cy, int& cz) {
+  cx = static_cast<int>(floor((x - e.origin[0]) / e.cell));
+  cy = static_cast<int>(floor((y - e.origin[1]) / e.cell));
+  cz = static_cast<int>(floor((z - e.origin[2]) / e.cell));
+  cx = cx < 0 ? 0 : (cx >= e.ncx ? e.ncx - 1 : cx);
+  cy = cy < 0 ? 0 : (cy >= e.ncy ? e.ncy - 1 : cy);
+  cz = cz < 0 ? 0 : (cz >= e.ncz ? e.ncz - 1 : cz);
+  return (cx * e.ncy + cy) * e.ncz + cz;
+}
+
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* p, double v) {
+  if (v > 0.0) atomicMax(p, static_cast<unsigned long long>(__double_as_longlong(v)));
+}
+
+__device__ __forceinline__ float tait(const Dev& e, float rho) {
+  float ratio = rho / e.rho0;
+  ratio = ratio > 0.01f ? ratio : 0.01f;
+  float p = e.bulk * (powf(ratio, e.gamma) - 1.f);
+  return p > 0.f ? p : 0.f;
+}
+
+// ------------------------------------------------------------ rebuild ---
+
+__global__ void k_check(Dev e) {
+  if (threadIdx.x || blockIdx.x) return;
+  const double d0 = __longlong_as_double(static_cast<long long>(e.maxbits[0]));
+  const double d1 = __longlong_as_double(static_cast<long long>(e.maxbits[1]));
+  const double d = e.flag[3] ? d1 : d0;
+  const int go = e.flag[1] || d > e.skin_half;
+  e.flag[0] = go;
+  if (go) {
+    e.counters[2] += 1;
+    e.flag[1] = 0;
+  }
+}
+
+__global__ void k_keys(Dev e) {
+  if (!e.flag[0]) return;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    const double4 p = ld4(e.pos, a);
+    int cx, cy, cz;
+    e.keys[a] = static_cast<uint64_t>(cell_of(e, p.x, p.y, p.z, cx, cy, cz));
+    e.vals[a] = a;
+  }
+}
+
+__global__ void k_permute(Dev e) {
+  if (!e.flag[0]) return;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    const int s = e.vals[a];
+    st4(e.tmp4a, a, ld4(e.pos, s));
+    st4(e.tmp4b, a, ld4(e.vel, s));
+    e.tmp_id[a] = e.id[s];
+  }
+}
+
+__global__ void k_permute_back(Dev e) {
+  if (!e.flag[0]) return;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    const double4 p = ld4(e.tmp4a, a);
+    st4(e.pos, a, p);
+    st4(e.anchor, a, p);
+    st4(e.vel, a, ld4(e.tmp4b, a));
+    e.id[a] = e.tmp_id[a];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    e.maxbits[0] = 0;
+    e.maxbits[1] = 0;
+  }
+}
+
+__global__ void k_clear_table(int32_t* start, int32_t* end, int64_t ncells, const int* flag) {
+  if (flag && !flag[0]) return;
+  for (int64_t c = blockIdx.x * blockDim.x + threadIdx.x; c < ncells; c += gridDim.x * blockDim.x) {
+    start[c] = -1;
+    end[c] = -1;
+  }
+}
+
+__global__ void k_fill_table(const uint64_t* __restrict__ keys, int n, int32_t* start, int32_t* end,
+                             const int* flag) {
+  if (flag && !flag[0]) return;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
+    const uint64_t k = keys[a];
+    if (a == 0 || keys[a - 1] != k) start[k] = a;
+    if (a == n - 1 || keys[a + 1] != k) end[k] = a + 1;
+  }
+}
+
+__global__ void k_rows(Dev e) {
+  if (!e.flag[0]) return;
+  int rowmax = 0;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.N; a += gridDim.x * blockDim.x) {
+    const double4 pa = ld4(e.pos, a);
+    int cx, cy, cz;
+    cell_of(e, pa.x, pa.y, pa.z, cx, cy, cz);
+    int count = 0;
+    const bool fluid_row = a < e.nf;
+    for (int dx = -1; dx <= 1; ++dx) {
+      const int x = cx + dx;
+      if (x < 0 || x >= e.ncx) continue;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int y = cy + dy;
+        if (y < 0 || y >= e.ncy) continue;
+        for (int dz = -1; dz <= 1; ++dz) {
+          const int z = cz + dz;
+          if (z < 0 || z >= e.ncz) continue;
+          const int c = (x * e.ncy + y) * e.ncz + z;
+          const int fs = e.fstart[c];
+          if (fs >= 0) {
+            const int fe = e.fend[c];
+            for (int b = fs; b < fe; ++b) {
+              if (b == a) continue;
+              const double4 pb = ld4(e.pos, b);
+              const double ddx = pa.x - pb.x, ddy = pa.y - pb.y, ddz = pa.z - pb.z;
+              if (ddx * ddx + ddy * ddy + ddz * ddz <= e.rc2) {
+                if (count < e.maxnb) e.nbr[static_cast<int64_t>(count) * e.N + a] = b;
+                ++count;
+              }
+            }
+          }
+          if (fluid_row) {
+            const int ws = e.wstart[c];
+            if (ws >= 0) {
+              const int we = e.wend[c];
+              for (int w = ws; w < we; ++w) {
+                const int b = e.nf + w;
+                const double4 pb = ld4(e.pos, b);
+                const double ddx = pa.x - pb.x, ddy = pa.y - pb.y, ddz = pa.z - pb.z;
+                if (ddx * ddx + ddy * ddy + ddz * ddz <= e.rc2) {
+                  if (count < e.maxnb) e.nbr[static_cast<int64_t>(count) * e.N + a] = b;
+                  ++count;
+                }
+              }
+            }
+          }
+        }
+      }
+    }
+    if (count > e.maxnb) atomicOr(e.status, 1);
+    e.cnt[a] = count < e.maxnb ? count : e.maxnb;
+    rowmax = count > rowmax ? count : rowmax;
+  }
+  rowmax = warp_reduce_max(rowmax);
+  if ((threadIdx.x & 31) == 0) atomicMax(&e.counters[4], static_cast<long long>(rowmax));
+}
+
+// ------------------------------------------------------------- physics ---
+
+__device__ __forceinline__ float3 sep(const double4& a, const double4& b) {
+  return make_float3(static_cast<float>(a.x - b.x), static_cast<float>(a.y - b.y),
+                     static_cast<float>(a.z - b.z));
+}
+
+__global__ void k_density(Dev e) {
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    const double4 pa = ld4(e.pos, a);
+    CSum<float> s;
+    s.add(static_cast<float>(pa.w) * e.sigma);
+    const int n = e.cnt[a];
+    for (int k = 0; k < n; ++k) {
+      const int b = e.nbr[static_cast<int64_t>(k) * e.N + a];
+      const double4 pb = ld4(e.pos, b);
+      const float3 d = sep(pa, pb);
+      const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+      if (r2 >= e.support2) continue;
+      const float W = e.sigma * shape(sqrtf(r2) * e.inv_h);
+      s.add(static_cast<float>(pb.w) * W);
+    }
+    float rho = s.value();
+    e.rho_s[a] = rho > e.rho_floor ? rho : e.rho_floor;
+  }
+}
+
+__global__ void k_diffusion_eos(Dev e) {
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    const float ra = e.rho_s[a];
+    float rho = ra;
+    if (e.dscale > 0.f) {
+      const double4 pa = ld4(e.pos, a);
+      CSum<float> rate;
+      const int n = e.cnt[a];
+      for (int k = 0; k < n; ++k) {
+        const int b = e.nbr[static_cast<int64_t>(k) * e.N + a];
+        if (b >= e.nf) continue;
+        const double4 pb = ld4(e.pos, b);
+        const float3 d = sep(pa, pb);
+        const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+        if (r2 >= e.support2) continue;
+        const float r = sqrtf(r2);
+        const float gs = e.sigma * dshape(r * e.inv_h) / (e.h * (r > 1e-12f ? r : 1e-12f));
+        const float radial = -gs * r2;
+        const float rb = e.rho_s[b];
+        const float coupling = (ra - rb) * radial / (r2 + 1e-12f);
+        rate.add((-e.dscale * (static_cast<float>(pb.w) / rb)) * coupling);
+      }
+      rho = ra + e.dtf * rate.value();
+      rho = rho > e.rho_floor ? rho : e.rho_floor;
+    }
+    const float p = tait(e, rho);
+    const double4 v = ld4(e.vel, a);
+    e.vr[a] = make_float4(static_cast<float>(v.x), static_cast<float>(v.y), static_cast<float>(v.z), rho);
+    e.pr[a] = p;
+    e.pq[a] = p / (rho * rho);
+  }
+}
+
+__global__ void k_walls(Dev e) {
+  for (int w = e.nf + blockIdx.x * blockDim.x + threadIdx.x; w < e.N; w += gridDim.x * blockDim.x) {
+    const double4 pw = ld4(e.pos, w);
+    CSum<float> num, den;
+    const int n = e.cnt[w];
+    for (int k = 0; k < n; ++k) {
+      const int f = e.nbr[static_cast<int64_t>(k) * e.N + w];
+      const double4 pf = ld4(e.pos, f);
+      const float3 d = sep(pw, pf);  // r_w - r_f
+      const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+      if (r2 >= e.support2) continue;
+      const float W = e.sigma * shape(sqrtf(r2) * e.inv_h);
+      float src = e.pr[f];
+      if (e.grav != 0.f) src = src + e.vr[f].w * (-e.grav * d.y);
+      num.add(src * W);
+      den.add(W);
+    }
+    const float dd = den.value();
+    float p = num.value() / (dd > 1e-30f ? dd : 1e-30f);
+    p = p > 0.f ? p : 0.f;
+    float rho = e.rho0 * powf(p / e.bulk + 1.f, e.inv_gamma);
+    rho = rho > e.rho0 ? rho : e.rho0;
+    e.vr[w] = make_float4(0.f, 0.f, 0.f, rho);
+    e.pr[w] = p;
+    e.pq[w] = p / (rho * rho);
+  }
+}
+
+__global__ void k_force(Dev e) {
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    const double4 pa = ld4(e.pos, a);
+    const float4 va = e.vr[a];
+    const float Pa = e.pq[a];
+    CSum<float> ax, ay, az;
+    const int n = e.cnt[a];
+    for (int k = 0; k < n; ++k) {
+      const int b = e.nbr[static_cast<int64_t>(k) * e.N + a];
+      const double4 pb = ld4(e.pos, b);
+      const float3 d = sep(pa, pb);
+      const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+      if (r2 >= e.support2) continue;
+      const float r = sqrtf(r2);
+      const float gs = e.sigma * dshape(r * e.inv_h) / (e.h * (r > 1e-12f ? r : 1e-12f));
+      const float4 vb = e.vr[b];
+      const float mb = static_cast<float>(pb.w);
+      const float fp = -mb * (Pa + e.pq[b]) * gs;
+      float fx = fp * d.x, fy = fp * d.y, fz = fp * d.z;
+      const float vs = b < e.nf ? e.nu2 : e.nu2f;
+      if (vs != 0.f) {
+        float lw = -(gs * r2);
+        lw = (lw > 0.f ? lw : 0.f) / (r2 + e.visc_eps);
+        const float coef = -vs * (mb / vb.w * lw);
+        fx += coef * (va.x - vb.x);
+        fy += coef * (va.y - vb.y);
+        fz += coef * (va.z - vb.z);
+      }
+      ax.add(fx);
+      ay.add(fy);
+      az.add(fz);
+    }
+    e.acc[a] = make_float4(ax.value(), ay.value() - e.grav, az.value(), 0.f);
+  }
+}
+
+// Force of the fluid on each obstacle particle (rhs_3d(return_wall_force=True),
+// dam_break_3d.py:412-421), reduced per block in FP64.
+__global__ void k_reaction(Dev e) {
+  __shared__ double part[kBlock / 32][3];
+  double fx = 0, fy = 0, fz = 0;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < e.nob; q += gridDim.x * blockDim.x) {
+    const int w = e.ob_rows[q];
+    const double4 pw = ld4(e.pos, w);
+    const float rw = e.vr[w].w;
+    const float Pw = e.pq[w];
+    const float mw = static_cast<float>(pw.w);
+    CSum<float> rx, ry, rz;
+    const int n = e.cnt[w];
+    for (int k = 0; k < n; ++k) {
+      const int f = e.nbr[static_cast<int64_t>(k) * e.N + w];
+      const double4 pf = ld4(e.pos, f);
+      const float3 d = sep(pw, pf);
+      const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+      if (r2 >= e.support2) continue;
+      const float r = sqrtf(r2);
+      const float gs = e.sigma * dshape(r * e.inv_h) / (e.h * (r > 1e-12f ? r : 1e-12f));
+      const float mf = static_cast<float>(pf.w);
+      const float c = -(mw * mf) * (Pw + e.pq[f]) * gs;
+      float x = c * d.x, y = c * d.y, z = c * d.z;
+      if (e.nu2f != 0.f) {
+        const float4 vf = e.vr[f];
+        float lw = -(gs * r2);
+        lw = (lw > 0.f ? lw : 0.f) / (r2 + e.visc_eps);
+        const float coef = mf * e.nu2f * (mw / rw * lw);
+        x += coef * vf.x;
+        y += coef * vf.y;
+        z += coef * vf.z;
+      }
+      rx.add(x);
+      ry.add(y);
+      rz.add(z);
+    }
+    fx += rx.value();
+    fy += ry.value();
+    fz += rz.value();
+  }
+  fx = warp_reduce_sum(fx);
+  fy = warp_reduce_sum(fy);
+  fz = warp_reduce_sum(fz);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) { part[warp][0] = fx; part[warp][1] = fy; part[warp][2] = fz; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s[3] = {0, 0, 0};
+    for (int w = 0; w < kBlock / 32; ++w)
+      for (int k = 0; k < 3; ++k) s[k] += part[w][k];
+    for (int k = 0; k < 3; ++k) e.partials[static_cast<int64_t>(e.nblocks_int + blockIdx.x) * 8 + k] = s[k];
+  }
+}
+
+// Semi-implicit Euler, box and obstacle clamps, meters (state before the update,
+// as the reference samples it), skin displacement.
+__global__ void k_integrate(Dev e) {
+  __shared__ double part[kBlock / 32][2];
+  double ke = 0, pe = 0, dmax = 0, vmax = 0, xmax = 0;
+  float rmax = 0.f;
+  long long esc = 0, clamps = 0;
+  bool bad = false;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    double4 x = ld4(e.pos, a);
+    double4 v = ld4(e.vel, a);
+    const float4 ac = e.acc[a];
+    const double m = x.w;
+    const double v2 = v.x * v.x + v.y * v.y + v.z * v.z;
+    vmax = fmax(vmax, sqrt(v2));
+    xmax = fmax(xmax, x.x);
+    rmax = fmaxf(rmax, e.vr[a].w);
+    ke += 0.5 * m * v2;
+    pe += m * e.gravity * x.y;
+    v.x += e.dt * static_cast<double>(ac.x);
+    v.y += e.dt * static_cast<double>(ac.y);
+    v.z += e.dt * static_cast<double>(ac.z);
+    x.x += e.dt * v.x;
+    x.y += e.dt * v.y;
+    x.z += e.dt * v.z;
+    double* xs[3] = {&x.x, &x.y, &x.z};
+    double* vs[3] = {&v.x, &v.y, &v.z};
+    bool out_any = false;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double hi = e.box_hi[k];
+      const double xv = *xs[k];
+      const bool out = xv < -e.tol || xv > hi + e.tol;
+      *xs[k] = xv < 0.0 ? 0.0 : (xv > hi ? hi : xv);
+      if (out) { *vs[k] = 0.0; out_any = true; }
+    }
+    esc += out_any;
+    if (e.has_ob) {
+      const bool inside = x.x > e.ob_lo[0] && x.x < e.ob_hi[0] && x.y > e.ob_lo[1] && x.y < e.ob_hi[1] &&
+                          x.z > e.ob_lo[2] && x.z < e.ob_hi[2];
+      if (inside) {
+        double best = x.x - e.ob_lo[0];
+        int which = 0;
+        for (int f = 1; f < 6; ++f) {
+          const int k = f >> 1;
+          const double dist = (f & 1) ? e.ob_hi[k] - *xs[k] : *xs[k] - e.ob_lo[k];
+          if (dist < best) { best = dist; which = f; }
+        }
+        const int k = which >> 1;
+        *xs[k] = (which & 1) ? e.ob_hi[k] + e.ob_eps : e.ob_lo[k] - e.ob_eps;
+        *vs[k] = 0.0;
+        ++clamps;
+      }
+    }
+    if (!isfinite(x.x) || !isfinite(x.y) || !isfinite(x.z) || !isfinite(v.x) || !isfinite(v.y) ||
+        !isfinite(v.z))
+      bad = true;
+    st4(e.pos, a, x);
+    st4(e.vel, a, v);
+    const double4 an = ld4(e.anchor, a);
+    const double ex = x.x - an.x, ey = x.y - an.y, ez = x.z - an.z;
+    dmax = fmax(dmax, sqrt(ex * ex + ey * ey + ez * ez));
+  }
+  dmax = warp_reduce_max(dmax);
+  vmax = warp_reduce_max(vmax);
+  xmax = warp_reduce_max(xmax);
+  rmax = warp_reduce_max(rmax);
+  ke = warp_reduce_sum(ke);
+  pe = warp_reduce_sum(pe);
+  esc = warp_reduce_sum(esc);
+  clamps = warp_reduce_sum(clamps);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    atomic_max_nonneg(&e.maxbits[0], dmax);
+    atomic_max_nonneg(&e.maxbits[3], vmax);
+    atomic_max_nonneg(&e.maxbits[4], xmax);
+    atomic_max_nonneg(&e.maxbits[2], static_cast<double>(rmax));
+    if (esc) atomicAdd(reinterpret_cast<unsigned long long*>(&e.counters[0]), static_cast<unsigned long long>(esc));
+    if (clamps) atomicAdd(reinterpret_cast<unsigned long long*>(&e.counters[1]), static_cast<unsigned long long>(clamps));
+    part[warp][0] = ke;
+    part[warp][1] = pe;
+  }
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(e.status, 2);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s0 = 0, s1 = 0;
+    for (int w = 0; w < kBlock / 32; ++w) { s0 += part[w][0]; s1 += part[w][1]; }
+    e.partials[static_cast<int64_t>(blockIdx.x) * 8 + 0] = s0;
+    e.partials[static_cast<int64_t>(blockIdx.x) * 8 + 1] = s1;
+  }
+}
+
+__global__ void k_finalize(Dev e) {
+  if (threadIdx.x || blockIdx.x) return;
+  double ke = 0, pe = 0, f[3] = {0, 0, 0};
+  for (int b = 0; b < e.nblocks_int; ++b) {
+    ke += e.partials[static_cast<int64_t>(b) * 8];
+    pe += e.partials[static_cast<int64_t>(b) * 8 + 1];
+  }
+  for (int b = 0; b < e.nblocks_ob; ++b)
+    for (int k = 0; k < 3; ++k) f[k] += e.partials[static_cast<int64_t>(e.nblocks_int + b) * 8 + k];
+  const long long step = e.counters[3];
+  double* row = e.diag + (step % e.diag_ring) * kDiag;
+  row[0] = __longlong_as_double(static_cast<long long>(e.maxbits[2]));
+  row[1] = __longlong_as_double(static_cast<long long>(e.maxbits[3]));
+  row[2] = __longlong_as_double(static_cast<long long>(e.maxbits[4]));
+  row[3] = f[0];
+  row[4] = f[1];
+  row[5] = f[2];
+  row[6] = ke;
+  row[7] = pe;
+  row[8] = static_cast<double>(e.counters[0]);
+  row[9] = static_cast<double>(e.counters[1]);
+  row[10] = static_cast<double>(e.counters[2]);
+  row[11] = static_cast<double>(e.counters[4]);
+  row[12] = static_cast<double>(step);
+  row[13] = static_cast<double>(*e.status);
+  for (int k = 0; k < 3; ++k) e.impulse[k] += f[k] * e.dt;
+  row[14] = e.impulse[0];
+  row[15] = e.cref[0];
+  // the speed of this step is the shift's reference speed
+  e.cref[1] = __longlong_as_double(static_cast<long long>(e.maxbits[3]));
+  e.maxbits[2] = e.maxbits[3] = e.maxbits[4] = 0;
+  e.counters[3] = step + 1;
+  e.flag[2] = e.shift_every > 0 && step > 0 && (step % e.shift_every) == 0;
+  e.flag[3] = 0;
+}
+
+// ------------------------------------------------------------- shifting ---
+
+__global__ void k_concentration(Dev e) {
+  if (!e.flag[2]) return;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    const double4 pa = ld4(e.pos, a);
+    CSum<float> s;
+    s.add(static_cast<float>(pa.w) / e.vr[a].w * e.sig2d);
+    const int n = e.cnt[a];
+    for (int k = 0; k < n; ++k) {
+      const int b = e.nbr[static_cast<int64_t>(k) * e.N + a];
+      if (b >= e.nf) continue;
+      const double4 pb = ld4(e.pos, b);
+      const float3 d = sep(pa, pb);
+      const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+      if (r2 >= e.support2) continue;
+      s.add(static_cast<float>(pb.w) / e.vr[b].w * (e.sig2d * shape(sqrtf(r2) * e.inv_h)));
+    }
+    e.conc[a] = s.value();
+  }
+}
+
+__global__ void k_conc_gradient(Dev e) {
+  if (!e.flag[2]) return;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    const double4 pa = ld4(e.pos, a);
+    const float ca = e.conc[a];
+    CSum<float> gx, gy, gz;
+    const int n = e.cnt[a];
+    for (int k = 0; k < n; ++k) {
+      const int b = e.nbr[static_cast<int64_t>(k) * e.N + a];
+      if (b >= e.nf) continue;
+      const double4 pb = ld4(e.pos, b);
+      const float3 d = sep(pa, pb);
+      const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+      if (r2 >= e.support2) continue;
+      const float r = sqrtf(r2);
+      const float gs = e.sig2d * dshape(r * e.inv_h) / (e.h * (r > 1e-12f ? r : 1e-12f));
+      const float c = static_cast<float>(pb.w) / e.vr[b].w * (e.conc[b] - ca) * gs;
+      gx.add(c * d.x);
+      gy.add(c * d.y);
+      gz.add(c * d.z);
+    }
+    e.gradc[a] = make_float4(gx.value(), gy.value(), gz.value(), 0.f);
+  }
+}
+
+__device__ __forceinline__ uint32_t fkey(float v) {
+  uint32_t b = __float_as_uint(v);
+  return (b >> 31) ? ~b : (b | 0x80000000u);
+}
+
+// Radix select of the k-th smallest concentration, one 8-bit digit per pass.
+__global__ void k_select_hist(Dev e, int shift) {
+  if (!e.flag[2]) return;
+  __shared__ unsigned int h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const uint32_t prefix = static_cast<uint32_t>(e.sel[0]);
+  const int hs = shift + 8;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    const uint32_t k = fkey(e.conc[a]);
+    if (hs >= 32 || (k >> hs) == (prefix >> hs)) atomicAdd(&h[(k >> shift) & 255u], 1u);
+  }
+  __syncthreads();
+  if (h[threadIdx.x]) atomicAdd(&e.hist[threadIdx.x], h[threadIdx.x]);
+}
+
+__global__ void k_select_pick(Dev e, int shift, long long rank, int which) {
+  if (!e.flag[2] || threadIdx.x || blockIdx.x) return;
+  if (shift == 24) {
+    e.sel[0] = 0;
+    e.counters[5] = rank;
+  }
+  long long k = e.counters[5];
+  int d = 0;
+  for (; d < 255; ++d) {
+    if (k < static_cast<long long>(e.hist[d])) break;
+    k -= e.hist[d];
+  }
+  e.sel[0] |= static_cast<unsigned long long>(d) << shift;
+  e.counters[5] = k;
+  for (int i = 0; i < 256; ++i) e.hist[i] = 0;
+  if (shift == 0) {
+    const uint32_t key = static_cast<uint32_t>(e.sel[0]);
+    const uint32_t b = (key >> 31) ? (key & 0x7fffffffu) : ~key;
+    e.sel[1 + which] = static_cast<unsigned long long>(__double_as_longlong(static_cast<double>(__uint_as_float(b))));
+  }
+}
+
+__global__ void k_select_finish(Dev e, double w) {
+  if (!e.flag[2] || threadIdx.x || blockIdx.x) return;
+  const double a = __longlong_as_double(static_cast<long long>(e.sel[1]));
+  const double b = __longlong_as_double(static_cast<long long>(e.sel[2]));
+  e.cref[0] = w < 0.5 ? a + w * (b - a) : b - (b - a) * (1.0 - w);
+  e.maxbits[1] = 0;
+}
+
+__global__ void k_shift_apply(Dev e) {
+  if (!e.flag[2]) return;
+  const double cref = e.cref[0];
+  const float thresh = static_cast<float>(e.shift_fs * cref);
+  const double vref = fmax(e.cref[1], e.vref_floor);
+  const float mag = static_cast<float>(e.shift_strength_h_dt * vref);
+  const float cap = static_cast<float>(e.shift_cap);
+  double dmax = 0;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    const float4 g = e.gradc[a];
+    float sx = -mag * g.x, sy = -mag * g.y, sz = -mag * g.z;
+    if (cref > 0.0 && e.conc[a] < thresh) {
+      const float nrm = sqrtf(g.x * g.x + g.y * g.y + g.z * g.z);
+      if (nrm > 1e-30f) {
+        const float nx = -g.x / nrm, ny = -g.y / nrm, nz = -g.z / nrm;
+        const float dot = sx * nx + sy * ny + sz * nz;
+        sx -= dot * nx;
+        sy -= dot * ny;
+        sz -= dot * nz;
+      }
+    }
+    const float m = sqrtf(sx * sx + sy * sy + sz * sz);
+    if (m > cap) {
+      const float s = cap / m;
+      sx *= s;
+      sy *= s;
+      sz *= s;
+    }
+    double4 x = ld4(e.pos, a);
+    x.x += sx;
+    x.y += sy;
+    x.z += sz;
+    st4(e.pos, a, x);
+    const double4 an = ld4(e.anchor, a);
+    const double ex = x.x - an.x, ey = x.y - an.y, ez = x.z - an.z;
+    dmax = fmax(dmax, sqrt(ex * ex + ey * ey + ez * ez));
+  }
+  dmax = warp_reduce_max(dmax);
+  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&e.maxbits[1], dmax);
+  if (blockIdx.x == 0 && threadIdx.x == 0) e.flag[3] = 1;
+}
+
+// ----------------------------------------------------------------- init ---
+
+__global__ void k_init_fluid(Dev e, const double* __restrict__ x, const double* __restrict__ v,
+                             const double* __restrict__ m) {
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    st4(e.pos, a, make_double4(x[3 * a], x[3 * a + 1], x[3 * a + 2], m[a]));
+    st4(e.vel, a, make_double4(v[3 * a], v[3 * a + 1], v[3 * a + 2], 0.0));
+    e.id[a] = a;
+  }
+}
+
+__global__ void k_wall_keys(Dev e, const double* __restrict__ w) {
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nw; a += gridDim.x * blockDim.x) {
+    int cx, cy, cz;
+    e.keys[a] = static_cast<uint64_t>(cell_of(e, w[3 * a], w[3 * a + 1], w[3 * a + 2], cx, cy, cz));
+    e.vals[a] = a;
+  }
+}
+
+__global__ void k_wall_place(Dev e, const double* __restrict__ w) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < e.nw; s += gridDim.x * blockDim.x) {
+    const int o = e.vals[s];
+    st4(e.pos, e.nf + s, make_double4(w[3 * o], w[3 * o + 1], w[3 * o + 2], static_cast<double>(e.wall_mass)));
+    e.wall_id[s] = o;
+    if (o >= e.nw - e.nob) e.ob_rows[o - (e.nw - e.nob)] = e.nf + s;
+  }
+}
+
+__global__ void k_read(Dev e, double* __restrict__ x, double* __restrict__ v, double* __restrict__ rho,
+                       double* __restrict__ p) {
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    const int o = e.id[a];
+    const double4 xa = ld4(e.pos, a), va = ld4(e.vel, a);
+    if (x) { x[3 * o] = xa.x; x[3 * o + 1] = xa.y; x[3 * o + 2] = xa.z; }
+    if (v) { v[3 * o] = va.x; v[3 * o + 1] = va.y; v[3 * o + 2] = va.z; }
+    if (rho) rho[o] = e.vr[a].w;
+    if (p) p[o] = e.pr[a];
+  }
+}
+
+}  // namespace
+}  // namespace tsph
+
+struct tsph_engine {
+  tsph::Dev d;
+  tsph_engine_params prm;
+  char* arena;
+  int64_t ncells;
+  char* radix_scratch;
+  int key_bits;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t captured_on = nullptr;
+};
+
+namespace tsph {
+namespace {
+
+struct Plan {
+  int64_t N, ncells;
+  int ncx, ncy, ncz;
+  double cell;
+  int nblocks_int, nblocks_ob;
+};
+
+Plan make_plan(const tsph_engine_params& p) {
+  Plan q{};
+  q.N = p.n_fluid + p.n_wall;
+  q.cell = 2.0 * p.h + p.skin;
+  q.ncx = static_cast<int>(std::ceil((p.grid_hi[0] - p.grid_lo[0]) / q.cell)) + 1;
+  q.ncy = static_cast<int>(std::ceil((p.grid_hi[1] - p.grid_lo[1]) / q.cell)) + 1;
+  q.ncz = static_cast<int>(std::ceil((p.grid_hi[2] - p.grid_lo[2]) / q.cell)) + 1;
+  q.ncells = static_cast<int64_t>(q.ncx) * q.ncy * q.ncz;
+  q.nblocks_int = static_cast<int>(grid_for(p.n_fluid, kBlock));
+  q.nblocks_ob = static_cast<int>(grid_for(std::max<int64_t>(p.n_obstacle, 1), kBlock));
+  return q;
+}
+
+// Carve the arena; with base == nullptr only the size is computed.
+size_t carve(const tsph_engine_params& p, const Plan& q, Dev* d, char* base, char** radix_scratch) {
+  size_t used = 0;
+  auto take = [&](size_t bytes) -> void* {
+    void* ptr = base ? base + used : nullptr;
+    used += align_up(bytes);
+    return ptr;
+  };
+  const int64_t nf = p.n_fluid, N = q.N;
+  const int64_t nsort = std::max<int64_t>(nf, p.n_wall);
+  Dev t{};
+  t.pos = static_cast<double4*>(take(N * sizeof(double4)));
+  t.vel = static_cast<double4*>(take(nf * sizeof(double4)));
+  t.anchor = static_cast<double4*>(take(nf * sizeof(double4)));
+  t.id = static_cast<int32_t*>(take(nf * sizeof(int32_t)));
+  t.wall_id = static_cast<int32_t*>(take(std::max<int64_t>(p.n_wall, 1) * sizeof(int32_t)));
+  t.vr = static_cast<float4*>(take(N * sizeof(float4)));
+  t.pr = static_cast<float*>(take(N * sizeof(float)));
+  t.pq = static_cast<float*>(take(N * sizeof(float)));
+  t.rho_s = static_cast<float*>(take(nf * sizeof(float)));
+  t.acc = static_cast<float4*>(take(nf * sizeof(float4)));
+  t.conc = static_cast<float*>(take(nf * sizeof(float)));
+  t.gradc = static_cast<float4*>(take(nf * sizeof(float4)));
+  t.nbr = static_cast<int32_t*>(take(static_cast<size_t>(p.max_neighbors) * N * sizeof(int32_t)));
+  t.cnt = static_cast<int32_t*>(take(N * sizeof(int32_t)));
+  t.ob_rows = static_cast<int32_t*>(take(std::max<int64_t>(p.n_obstacle, 1) * sizeof(int32_t)));
+  t.fstart = static_cast<int32_t*>(take(q.ncells * sizeof(int32_t)));
+  t.fend = static_cast<int32_t*>(take(q.ncells * sizeof(int32_t)));
+  t.wstart = static_cast<int32_t*>(take(q.ncells * sizeof(int32_t)));
+  t.wend = static_cast<int32_t*>(take(q.ncells * sizeof(int32_t)));
+  t.keys = static_cast<uint64_t*>(take(nsort * sizeof(uint64_t)));
+  t.keys_tmp = static_cast<uint64_t*>(take(nsort * sizeof(uint64_t)));
+  t.vals = static_cast<int32_t*>(take(nsort * sizeof(int32_t)));
+  t.vals_tmp = static_cast<int32_t*>(take(nsort * sizeof(int32_t)));
+  t.tmp4a = static_cast<double4*>(take(nf * sizeof(double4)));
+  t.tmp4b = static_cast<double4*>(take(nf * sizeof(double4)));
+  t.tmp4c = nullptr;
+  t.tmp_id = static_cast<int32_t*>(take(nf * sizeof(int32_t)));
+  t.flag = static_cast<int*>(take(16 * sizeof(int)));
+  t.maxbits = static_cast<unsigned long long*>(take(8 * sizeof(unsigned long long)));
+  t.status = static_cast<int*>(take(sizeof(int)));
+  t.counters = static_cast<long long*>(take(8 * sizeof(long long)));
+  t.partials = static_cast<double*>(take(static_cast<size_t>(q.nblocks_int + q.nblocks_ob) * 8 * sizeof(double)));
+  t.impulse = static_cast<double*>(take(4 * sizeof(double)));
+  t.diag = static_cast<double*>(take(static_cast<size_t>(p.diag_ring) * kDiag * sizeof(double)));
+  t.hist = static_cast<unsigned int*>(take(256 * sizeof(unsigned int)));
+  t.sel = static_cast<unsigned long long*>(take(4 * sizeof(unsigned long long)));
+  t.cref = static_cast<double*>(take(4 * sizeof(double)));
+  char* rs = static_cast<char*>(take(radix_scratch_bytes(nsort)));
+  if (radix_scratch) *radix_scratch = rs;
+  if (d) *d = t;
+  return used + 256;
+}
+
+int enqueue_rebuild(tsph_engine* E, cudaStream_t s) {
+  Dev& d = E->d;
+  const unsigned g = grid_for(d.nf, kBlock);
+  k_check<<<1, 32, 0, s>>>(d);
+  k_keys<<<g, kBlock, 0, s>>>(d);
+  TSPH_LAUNCH_CHECK();
+  int rc = radix_sort_u64_i32(d.keys, d.vals, d.keys_tmp, d.vals_tmp, d.nf, E->key_bits, E->radix_scratch, s,
+                              d.flag);
+  if (rc) return rc;
+  k_permute<<<g, kBlock, 0, s>>>(d);
+  k_permute_back<<<g, kBlock, 0, s>>>(d);
+  k_clear_table<<<grid_for(E->ncells, 256), 256, 0, s>>>(d.fstart, d.fend, E->ncells, d.flag);
+  k_fill_table<<<g, kBlock, 0, s>>>(d.keys, d.nf, d.fstart, d.fend, d.flag);
+  k_rows<<<grid_for(d.N, kBlock), kBlock, 0, s>>>(d);
+  TSPH_LAUNCH_CHECK();
+  return TSPH_OK;
+}
+
+int enqueue_step(tsph_engine* E, cudaStream_t s) {
+  Dev& d = E->d;
+  int rc = enqueue_rebuild(E, s);
+  if (rc) return rc;
+  const unsigned g = grid_for(d.nf, kBlock);
+  k_density<<<g, kBlock, 0, s>>>(d);
+  k_diffusion_eos<<<g, kBlock, 0, s>>>(d);
+  if (d.nw) k_walls<<<grid_for(d.nw, kBlock), kBlock, 0, s>>>(d);
+  k_force<<<g, kBlock, 0, s>>>(d);
+  k_reaction<<<d.nblocks_ob, kBlock, 0, s>>>(d);
+  TSPH_CUDA_CHECK(cudaMemsetAsync(d.maxbits, 0, 2 * sizeof(unsigned long long), s));
+  k_integrate<<<d.nblocks_int, kBlock, 0, s>>>(d);
+  k_finalize<<<1, 32, 0, s>>>(d);
+  TSPH_LAUNCH_CHECK();
+  if (d.shift_every > 0) {
+    rc = enqueue_rebuild(E, s);
+    if (rc) return rc;
+    k_concentration<<<g, kBlock, 0, s>>>(d);
+    k_conc_gradient<<<g, kBlock, 0, s>>>(d);
+    const double pos = 0.95 * static_cast<double>(d.nf - 1);
+    const long long lo = static_cast<long long>(std::floor(pos)), hi = static_cast<long long>(std::ceil(pos));
+    const unsigned gs = grid_for(d.nf, 256, 148 * 4);
+    for (int which = 0; which < 2; ++which) {
+      for (int shift = 24; shift >= 0; shift -= 8) {
+        k_select_hist<<<gs, 256, 0, s>>>(d, shift);
+        k_select_pick<<<1, 32, 0, s>>>(d, shift, which == 0 ? lo : hi, which);
+      }
+    }
+    k_select_finish<<<1, 32, 0, s>>>(d, pos - static_cast<double>(lo));
+    k_shift_apply<<<g, kBlock, 0, s>>>(d);
+    TSPH_LAUNCH_CHECK();
+  }
+  return TSPH_OK;
+}
+
+}  // namespace
+}  // namespace tsph
+
+using namespace tsph;
+
+extern "C" {
+
+int64_t tsph_engine_bytes(const tsph_engine_params* prm) {
+  if (!prm || prm->n_fluid <= 0 || prm->n_wall < 0 || prm->max_neighbors <= 0) return -1;
+  Plan q = make_plan(*prm);
+  return static_cast<int64_t>(carve(*prm, q, nullptr, nullptr, nullptr));
+}
+
+int tsph_engine_create(const tsph_engine_params* prm, void* arena, int64_t arena_bytes, const double* x,
+                       const double* v, const double* mass, const double* wall, tsph_stream stream,
+                       tsph_engine** out) {
+  if (!prm || !out || !arena) return TSPH_ERR_ARG;
+  if (prm->n_fluid <= 0 || prm->n_wall < 0 || prm->n_obstacle < 0 || prm->n_obstacle > prm->n_wall ||
+      prm->n_fluid + prm->n_wall >= (int64_t(1) << 31) || prm->max_neighbors <= 0 || prm->diag_ring <= 0)
+    return TSPH_ERR_ARG;
+  if (arena_bytes < tsph_engine_bytes(prm)) return TSPH_ERR_WORKSPACE;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  tsph_engine* E = new (std::nothrow) tsph_engine();
+  if (!E) return TSPH_ERR_ARG;
+  E->prm = *prm;
+  E->arena = static_cast<char*>(arena);
+  Plan q = make_plan(*prm);
+  E->ncells = q.ncells;
+  carve(*prm, q, &E->d, E->arena, &E->radix_scratch);
+  int bits = 0;
+  while ((int64_t(1) << bits) < q.ncells) ++bits;
+  E->key_bits = bits;
+  Dev& d = E->d;
+  d.nf = static_cast<int>(prm->n_fluid);
+  d.nw = static_cast<int>(prm->n_wall);
+  d.N = static_cast<int>(q.N);
+  d.nob = static_cast<int>(prm->n_obstacle);
+  d.maxnb = static_cast<int>(prm->max_neighbors);
+  d.shift_every = static_cast<int>(prm->shift_every);
+  d.diag_ring = static_cast<int>(prm->diag_ring);
+  d.ncx = q.ncx; d.ncy = q.ncy; d.ncz = q.ncz;
+  for (int k = 0; k < 3; ++k) {
+    d.origin[k] = prm->grid_lo[k];
+    d.box_hi[k] = prm->box_hi[k];
+    d.ob_lo[k] = prm->ob_lo[k];
+    d.ob_hi[k] = prm->ob_hi[k];
+  }
+  d.cell = q.cell;
+  const double rc = 2.0 * prm->h + prm->skin;
+  d.rc2 = rc * rc;
+  d.skin_half = 0.5 * prm->skin;
+  d.dt = prm->dt;
+  d.tol = prm->tolerance;
+  d.ob_eps = prm->ob_eps;
+  d.has_ob = static_cast<int>(prm->has_obstacle);
+  d.gravity = prm->gravity;
+  d.h = static_cast<float>(prm->h);
+  d.inv_h = static_cast<float>(1.0 / prm->h);
+  d.sigma = static_cast<float>(1.0 / (M_PI * prm->h * prm->h * prm->h));
+  d.sig2d = static_cast<float>(10.0 / (7.0 * M_PI * prm->h * prm->h));
+  d.support2 = static_cast<float>(4.0 * prm->h * prm->h);
+  d.rho0 = static_cast<float>(prm->rho0);
+  d.bulk = static_cast<float>(prm->rho0 * prm->sound_speed * prm->sound_speed / prm->gamma);
+  d.gamma = static_cast<float>(prm->gamma);
+  d.inv_gamma = static_cast<float>(1.0 / prm->gamma);
+  d.grav = static_cast<float>(prm->gravity);
+  d.nu2 = static_cast<float>(2.0 * prm->viscosity);
+  d.nu2f = static_cast<float>(2.0 * prm->viscosity * prm->wall_friction);
+  d.dscale = static_cast<float>(prm->diffusion_scale);
+  d.dtf = static_cast<float>(prm->dt);
+  d.visc_eps = static_cast<float>(0.01 * prm->h * prm->h);
+  d.rho_floor = static_cast<float>(0.1 * prm->rho0);
+  d.wall_mass = static_cast<float>(prm->wall_mass);
+  d.shift_strength_h_dt = prm->shift_strength * prm->h * prm->dt;
+  d.shift_cap = prm->shift_limit * prm->h;
+  d.shift_fs = prm->shift_free_surface;
+  d.vref_floor = prm->shift_vref_floor;
+  d.nblocks_int = q.nblocks_int;
+  d.nblocks_ob = q.nblocks_ob;
+
+  int rc_ = TSPH_OK;
+  do {
+    if (cudaMemsetAsync(d.flag, 0, 16 * sizeof(int), s) != cudaSuccess ||
+        cudaMemsetAsync(d.maxbits, 0, 8 * sizeof(unsigned long long), s) != cudaSuccess ||
+        cudaMemsetAsync(d.status, 0, sizeof(int), s) != cudaSuccess ||
+        cudaMemsetAsync(d.counters, 0, 8 * sizeof(long long), s) != cudaSuccess ||
+        cudaMemsetAsync(d.impulse, 0, 4 * sizeof(double), s) != cudaSuccess ||
+        cudaMemsetAsync(d.hist, 0, 256 * sizeof(unsigned int), s) != cudaSuccess ||
+        cudaMemsetAsync(d.cref, 0, 4 * sizeof(double), s) != cudaSuccess ||
+        cudaMemsetAsync(d.diag, 0, static_cast<size_t>(d.diag_ring) * kDiag * sizeof(double), s) != cudaSuccess ||
+        cudaMemsetAsync(d.cnt, 0, static_cast<size_t>(d.N) * sizeof(int32_t), s) != cudaSuccess) {
+      rc_ = TSPH_ERR_CUDA;
+      break;
+    }
+    const int one = 1;
+    if (cudaMemcpyAsync(d.flag + 1, &one, sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess) {
+      rc_ = TSPH_ERR_CUDA;
+      break;
+    }
+    k_init_fluid<<<grid_for(d.nf, kBlock), kBlock, 0, s>>>(d, x, v, mass);
+    if (d.nw) {
+      k_wall_keys<<<grid_for(d.nw, kBlock), kBlock, 0, s>>>(d, wall);
+      rc_ = radix_sort_u64_i32(d.keys, d.vals, d.keys_tmp, d.vals_tmp, d.nw, E->key_bits, E->radix_scratch, s);
+      if (rc_) break;
+      k_wall_place<<<grid_for(d.nw, kBlock), kBlock, 0, s>>>(d, wall);
+      k_clear_table<<<grid_for(E->ncells, 256), 256, 0, s>>>(d.wstart, d.wend, E->ncells, nullptr);
+      k_fill_table<<<grid_for(d.nw, kBlock), kBlock, 0, s>>>(d.keys, d.nw, d.wstart, d.wend, nullptr);
+    } else {
+      k_clear_table<<<grid_for(E->ncells, 256), 256, 0, s>>>(d.wstart, d.wend, E->ncells, nullptr);
+    }
+    if (cudaGetLastError() != cudaSuccess) rc_ = TSPH_ERR_CUDA;
+  } while (0);
+  // Positions arrive in the caller's (host) byte order and may be pageable:
+  // make sure the copies above finished before the caller's buffers go away.
+  if (rc_ == TSPH_OK && cudaStreamSynchronize(s) != cudaSuccess) rc_ = TSPH_ERR_CUDA;
+  if (rc_) {
+    delete E;
+    return rc_;
+  }
+  *out = E;
+  return TSPH_OK;
+}
+
+int tsph_engine_step(tsph_engine* E, int64_t steps, tsph_stream stream) {
+  if (!E || steps < 0) return TSPH_ERR_ARG;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (!E->exec || E->captured_on != s) {
+    if (E->exec) { cudaGraphExecDestroy(E->exec); E->exec = nullptr; }
+    if (E->graph) { cudaGraphDestroy(E->graph); E->graph = nullptr; }
+    TSPH_CUDA_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_step(E, s);
+    cudaGraph_t g = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(s, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (ce != cudaSuccess) return TSPH_ERR_CUDA;
+    E->graph = g;
+    TSPH_CUDA_CHECK(cudaGraphInstantiate(&E->exec, g, 0));
+    E->captured_on = s;
+  }
+  for (int64_t i = 0; i < steps; ++i) TSPH_CUDA_CHECK(cudaGraphLaunch(E->exec, s));
+  return TSPH_OK;
+}
+
+int tsph_engine_step_eager(tsph_engine* E, int64_t steps, tsph_stream stream) {
+  if (!E || steps < 0) return TSPH_ERR_ARG;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  for (int64_t i = 0; i < steps; ++i) {
+    int rc = enqueue_step(E, s);
+    if (rc) return rc;
+  }
+  return TSPH_OK;
+}
+
+int tsph_engine_read(tsph_engine* E, double* x, double* v, double* rho, double* p, tsph_stream stream) {
+  if (!E) return TSPH_ERR_ARG;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  k_read<<<grid_for(E->d.nf, 256), 256, 0, s>>>(E->d, x, v, rho, p);
+  TSPH_LAUNCH_CHECK();
+  return TSPH_OK;
+}
+
+int tsph_engine_diag(tsph_engine* E, double* out, int64_t first, int64_t count, tsph_stream stream) {
+  if (!E || count < 0 || count > E->d.diag_ring) return TSPH_ERR_ARG;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  for (int64_t i = 0; i < count; ++i) {
+    const int64_t slot = (first + i) % E->d.diag_ring;
+    TSPH_CUDA_CHECK(cudaMemcpyAsync(out + i * kDiag, E->d.diag + slot * kDiag, kDiag * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, s));
+  }
+  return TSPH_OK;
+}
+
+int tsph_engine_status(tsph_engine* E, int64_t* counters, tsph_stream stream) {
+  if (!E || !counters) return TSPH_ERR_ARG;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  long long c[8];
+  int st = 0;
+  TSPH_CUDA_CHECK(cudaMemcpyAsync(c, E->d.counters, sizeof(c), cudaMemcpyDeviceToHost, s));
+  TSPH_CUDA_CHECK(cudaMemcpyAsync(&st, E->d.status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  TSPH_CUDA_CHECK(cudaStreamSynchronize(s));
+  for (int k = 0; k < 6; ++k) counters[k] = c[k];
+  counters[6] = st;
+  counters[7] = 0;
+  if (st & 2) return TSPH_ERR_STATE;
+  if (st & 1) return TSPH_ERR_CAPACITY;
+  return TSPH_OK;
+}
+
+int tsph_engine_destroy(tsph_engine* E) {
+  if (!E) return TSPH_OK;
+  if (E->exec) cudaGraphExecDestroy(E->exec);
+  if (E->graph) cudaGraphDestroy(E->graph);
+  delete E;
+  return TSPH_OK;
+}
+
+}  // extern "C"
