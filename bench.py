@@ -1,0 +1,320 @@
+"""Benchmark: fluid particle-updates/s of the 3-D dam break with a box obstacle.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Workload (one case per GPU; with N > 1 every rank runs its own replica, weak
+scaling, no collective on the data path): fluid block 1.2 x 1.0 x 0.55 m at
+dx = 0.0069 m (1,968,048 fluid particles) in a 3.2 x 1.0 x 1.0 m tank with
+three wall layers and a 0.16 x 0.16 x 0.4 m obstacle (776k wall particles),
+h = 1.3 dx, Tait rho0 = 1000, gamma = 7, c0 = 10 sqrt(2 g 0.55), Molteni
+diffusion delta = 0.1, Lind shifting every step, CFL 0.25; FP32 pair
+arithmetic with FP64 positions, velocities and meters.  A step is one
+graph-captured engine step (skin test and device-side rebuild, density,
+diffusion + EOS, Adami walls, force, obstacle force, Euler + clamps, shift).
+
+One JSON line on rank 0.  ``value`` is device-timed (CUDA events on the
+engine stream, max over ranks); ``e2e`` is the same metric through the public
+API from pinned host memory: engine creation from the host lattice (H2D), the
+K steps with one device->host read of the step's meter row per step, and the
+final state back to the host.  ``--impl reference`` times the CPU oracle port
+of the same algorithm (numpy, one core) on a 4x coarser rung of the same case.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+from pathlib import Path
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+ALGO_BYTES_FORCE = 52      # per fluid particle: pos+mass 16, vel+rho 16, p/rho^2 4 in; acc 16 out
+ALGO_BYTES_STEP = 244      # per fluid update, compulsory bytes of the whole step (3-D plain path)
+FLOPS_PER_PAIR_FORCE = 60  # kernel + pressure + viscosity per in-support pair
+CANDIDATE_FLOPS = 10       # separation + radius test per listed neighbour
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--dx", type=float, default=0.0069)
+    ap.add_argument("--shift-every", type=int, default=1)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-sample-steps", type=int, default=6)
+    return ap.parse_args()
+
+
+def peaks():
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        data = json.loads(path.read_text())
+        return float(data["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic_per_fluid_particle():
+    """DRAM bytes per fluid particle of one force launch, from the committed ncu summary."""
+    path = ROOT / "profiles" / "engine_force_dam_break_3d.md"
+    if not path.exists():
+        return None
+    for line in path.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_fluid_particle:"):
+            return float(line.split(":", 1)[1].strip())
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.index)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        rows = [r.split(",") for r in out.strip().splitlines() if r.strip()]
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for name, val in zip(names, r[5:9]):
+                if val.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def cpu_baseline(dx, steps, shift_every):
+    """Oracle port (numpy, 1 core): rhs_3d + Euler + clamps, skin-cached pairs."""
+    import numpy as np
+    from oracle import neighbors as on
+    from oracle import pairpass as op
+    from tensorsph_b200.engine import DamBreak3DEngine, obstacle_case
+    cfg, ob = obstacle_case(dx=dx)
+    x, m, w, _ = DamBreak3DEngine.build_host_state(cfg, ob)
+    x, m, w = x.numpy(), m.numpy(), w.numpy()
+    n = x.shape[0]
+    v = np.zeros_like(x)
+    h = cfg.h_factor * cfg.dx
+    skin = cfg.pair_skin_factor * h
+    box = np.array([cfg.pool_width, cfg.tank_height, cfg.tank_depth])
+    anchor, pairs = None, None
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        allp = np.concatenate((x, w))
+        if anchor is None or np.sqrt(((x - anchor) ** 2).sum(1)).max() > 0.5 * skin:
+            pairs = on.cell_linked_pairs_batched(allp, 2.0 * h + skin)
+            pairs = pairs[pairs[:, 0] < n]
+            anchor = x.copy()
+        rho, p, acc, react = op.rhs_3d(x, v, m, cfg, pairs=pairs, wall=w, dt=cfg.dt,
+                                       return_wall_force=True)
+        v = v + cfg.dt * acc
+        x = x + cfg.dt * v
+        out = (x < -0.25 * cfg.dx) | (x > box + 0.25 * cfg.dx)
+        x = np.clip(x, 0.0, box)
+        v[out] = 0.0
+        if shift_every:
+            vol = m / rho
+            x, _ = op.shift_positions(x, vol, h, dt=cfg.dt,
+                                      v_ref=max(float(np.sqrt((v * v).sum(1)).max()),
+                                                0.05 * cfg.sound_speed))
+    elapsed = time.perf_counter() - t0
+    return n * steps / elapsed, n, elapsed
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    coarse = args.dx * 4.0
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        for _ in range(max(args.warmup, 0) and 1):
+            cpu_baseline(coarse, 1, args.shift_every)
+        value, n, elapsed = cpu_baseline(coarse, max(args.steps // 20, 2), args.shift_every)
+        line = {"metric": "particle-updates/s", "value": value, "unit": "fluid particle-updates/s",
+                "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded lattice)",
+                "config": {"workload": f"3-D dam break with obstacle, CPU oracle port on the "
+                           f"dx={coarse:g} rung ({n} fluid)"},
+                "cpu_baseline": {"value": value, "unit": "fluid particle-updates/s", "cores": 1,
+                                 "kind": "port",
+                                 "sample": f"{max(args.steps // 20, 2)} steps of the dx={coarse:g} "
+                                           f"rung ({n} fluid), {elapsed:.1f} s"},
+                "e2e": {"value": value, "unit": "fluid particle-updates/s",
+                        "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    from tensorsph_b200.engine import DamBreak3DEngine, obstacle_case
+
+    cfg, obstacle = obstacle_case(dx=args.dx)
+    host = DamBreak3DEngine.build_host_state(cfg, obstacle)
+    eng = DamBreak3DEngine(cfg, obstacle=obstacle, shift_every=args.shift_every,
+                           host_state=host, diag_ring=max(args.steps + args.warmup + 64, 256),
+                           device=dev)
+    nf, nw = eng.n_fluid, eng.n_wall
+    eng.step(max(args.warmup, 1))
+    torch.cuda.synchronize(dev)
+    eng.status()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier()
+    torch.cuda.synchronize(dev)
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    start.record(eng.stream)
+    eng.step(args.steps)
+    stop.record(eng.stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    clocks = sampler.stop()
+    ms = start.elapsed_time(stop)
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t)
+    status = eng.status()
+    ms_step = ms / args.steps
+    value = nf * args.steps * world / (ms / 1e3)
+    kernels_per_step = eng.graph_kernels()
+
+    stage = {}
+    for _ in range(3):
+        for k, v in eng.step_timed().items():
+            stage.setdefault(k, []).append(v)
+    stage = {k: statistics.median(v) for k, v in stage.items()}
+    t_force = stage["force"] / 1e3
+    peak, peak_kind = peaks()
+    achieved = ALGO_BYTES_FORCE * nf / t_force / 1e9
+    traffic_pp = ncu_traffic_per_fluid_particle()
+    diag = eng.diagnostics(eng.steps_done - 1, 1).cpu()[0]
+    eng.close()
+    del eng
+
+    e2e = None
+    if not args.no_e2e:
+        x, m, w, n_ob = host
+        pinned = tuple(t.pin_memory() for t in (x, m, w))
+        rows = torch.empty((args.steps, 16), dtype=torch.float64).pin_memory()
+        final = torch.empty((nf, 3), dtype=torch.float64).pin_memory()
+        barrier()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        e = DamBreak3DEngine(cfg, obstacle=obstacle, shift_every=args.shift_every,
+                             host_state=(pinned[0], pinned[1], pinned[2], n_ob),
+                             diag_ring=args.steps + 8, device=dev)
+        for k in range(args.steps):
+            e.step(1)
+            with torch.cuda.stream(e.stream):
+                rows[k].copy_(e.diagnostics(k, 1)[0], non_blocking=True)
+        xs = e.state()[0]
+        with torch.cuda.stream(e.stream):
+            final.copy_(xs, non_blocking=True)
+        torch.cuda.synchronize(dev)
+        t_e2e = time.perf_counter() - t0
+        barrier()
+        if dist is not None:
+            t = torch.tensor([t_e2e], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            t_e2e = float(t)
+        e.close()
+        state_bytes = (x.numel() + m.numel() + w.numel()) * 8
+        e2e = {"value": nf * args.steps * world / t_e2e, "unit": "fluid particle-updates/s",
+               "h2d_bytes_per_step": state_bytes / args.steps,
+               "d2h_bytes_per_step": 16 * 8 + nf * 3 * 8 / args.steps,
+               "scope": "engine creation from pinned host lattices + K steps with a per-step "
+                        "meter-row read + final positions read, wall clock"}
+
+    cpu = None
+    if rank == 0 and world == 1 and args.cpu_sample_steps > 0:
+        v_cpu, n_cpu, t_cpu = cpu_baseline(4.0 * args.dx, args.cpu_sample_steps, args.shift_every)
+        cpu = {"value": v_cpu, "unit": "fluid particle-updates/s", "cores": 1, "kind": "port",
+               "sample": f"{args.cpu_sample_steps} steps of the dx={4.0 * args.dx:g} rung "
+                         f"({n_cpu} fluid), {t_cpu:.1f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": "particle-updates/s", "value": value, "unit": "fluid particle-updates/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded lattice, no dataset)",
+            "config": {"workload": "3-D dam break with box obstacle: 1.2x1.0x0.55 m fluid in a "
+                                   "3.2x1.0x1.0 m tank, obstacle 0.16x0.16x0.4 m, dx="
+                                   f"{args.dx:g}", "fluid_particles": nf, "wall_particles": nw,
+                       "shift_every": args.shift_every, "density_diffusion": 0.1,
+                       "pairs": "FP32 pair arithmetic, FP64 positions/velocities/meters",
+                       "l2": "working set (state + neighbour rows) > 126 MB L2, no flush",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "roofline": {"bound": "hbm", "kernel": "k_force", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None if traffic_pp is None else traffic_pp * nf,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                         "algorithmic_bytes_per_launch": ALGO_BYTES_FORCE * nf,
+                         "launch_ms": stage["force"],
+                         "step_hbm_frac": ALGO_BYTES_STEP * nf / (ms_step / 1e3) / 1e9 / peak},
+            "stage_ms": stage,
+            "clocks": clocks,
+            "gpu_launches": kernels_per_step * args.steps,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "engine": {"rebuilds": status["rebuilds"], "escapes": status["escapes"],
+                       "obstacle_clamps": status["clamps"], "longest_row": status["row_max"],
+                       "last_rho_max": float(diag[0]), "last_speed_max": float(diag[1]),
+                       "kernels_per_step": kernels_per_step},
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

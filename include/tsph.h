@@ -275,6 +275,15 @@ int tsph_engine_create(const tsph_engine_params* prm, void* arena, int64_t arena
 int tsph_engine_step(tsph_engine* engine, int64_t steps, tsph_stream stream);
 /* Same steps launched kernel by kernel (no graph). */
 int tsph_engine_step_eager(tsph_engine* engine, int64_t steps, tsph_stream stream);
+/* One step launched kernel by kernel with an event after each stage; the
+ * stage times (ms) go to stage_ms[0..*stages) on the host (synchronises).
+ * Stages: rebuild, density, diffusion+EOS, walls, force, reaction,
+ * integrate+meters, then with shifting: shift rebuild, concentration,
+ * gradient, reference select, apply. */
+int tsph_engine_step_timed(tsph_engine* engine, tsph_stream stream, float* stage_ms,
+                           int64_t* stages);
+/* Number of kernel nodes in the captured step graph (host; after a step). */
+int tsph_engine_graph_kernels(tsph_engine* engine, int64_t* kernels);
 /* Fluid state in the caller's original particle order (device, nullable). */
 int tsph_engine_read(tsph_engine* engine, double* x, double* v, double* rho, double* p,
                      tsph_stream stream);

@@ -207,3 +207,41 @@ class PairListCache:
             return pairs, True
         self.reuses += 1
         return self._pairs, False
+
+
+def cell_linked_pairs_batched(pos, cutoff):
+    """Same pairs as :func:`cell_linked_pairs`, candidate expansion done in one
+    batched pass (the structure of neighbor_search.py:80-120: every particle
+    queries its 3^D neighbour cells through a sorted key table).  Used where
+    the oracle has to run at tens of thousands of particles (CPU baseline)."""
+    pos = _check(pos, cutoff)
+    n, dim = pos.shape
+    if n < 2:
+        return _empty()
+    cells, keys, extent, strides, order = cell_grid(pos, cutoff)
+    sorted_keys = keys[order]
+    uniq, first = np.unique(sorted_keys, return_index=True)
+    counts = np.diff(np.append(first, n))
+    c2 = pos.dtype.type(float(cutoff) ** 2)
+    ii, jj = [], []
+    for off in product((-1, 0, 1), repeat=dim):
+        nb = cells + np.asarray(off, dtype=np.int64)
+        inside = np.all((nb >= 0) & (nb < extent), axis=1)
+        nkey = nb @ strides
+        slot = np.clip(np.searchsorted(uniq, nkey), 0, uniq.size - 1)
+        found = inside & (uniq[slot] == nkey)
+        src = np.nonzero(found)[0]
+        if src.size == 0:
+            continue
+        occ = counts[slot[src]]
+        starts = first[slot[src]]
+        rep = np.repeat(src, occ)
+        within = np.arange(occ.sum()) - np.repeat(np.cumsum(occ) - occ, occ)
+        j = order[np.repeat(starts, occ) + within]
+        keep = rep < j
+        rep, j = rep[keep], j[keep]
+        d2 = squared_distance(pos[rep] - pos[j])
+        keep = d2 <= c2
+        ii.append(rep[keep])
+        jj.append(j[keep])
+    return _finish(ii, jj)

@@ -133,6 +133,9 @@ _SIGNATURES = {
                                    c_void_p, c_void_p, c_void_p, POINTER(c_void_p)]),
     "tsph_engine_step": (c_int, [c_void_p, c_int64, c_void_p]),
     "tsph_engine_step_eager": (c_int, [c_void_p, c_int64, c_void_p]),
+    "tsph_engine_step_timed": (c_int, [c_void_p, c_void_p, POINTER(ctypes.c_float),
+                                       POINTER(c_int64)]),
+    "tsph_engine_graph_kernels": (c_int, [c_void_p, POINTER(c_int64)]),
     "tsph_engine_read": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "tsph_engine_diag": (c_int, [c_void_p, c_void_p, c_int64, c_int64, c_void_p]),
     "tsph_engine_status": (c_int, [c_void_p, c_void_p, c_void_p]),

@@ -856,25 +856,45 @@ int enqueue_rebuild(tsph_engine* E, cudaStream_t s) {
   return TSPH_OK;
 }
 
-int enqueue_step(tsph_engine* E, cudaStream_t s) {
+// Stage marks: when `marks` is non-null an event is recorded after each stage
+// (rebuild, density, diffusion+EOS, walls, force, reaction, integrate+meters,
+// shift rebuild, concentration, gradient, select, apply).
+constexpr int kStages = 12;
+
+int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr) {
   Dev& d = E->d;
+  int stage = 0;
+  auto mark = [&]() {
+    if (marks) cudaEventRecord(marks[stage], s);
+    ++stage;
+  };
   int rc = enqueue_rebuild(E, s);
   if (rc) return rc;
+  mark();
   const unsigned g = grid_for(d.nf, kBlock);
   k_density<<<g, kBlock, 0, s>>>(d);
+  mark();
   k_diffusion_eos<<<g, kBlock, 0, s>>>(d);
+  mark();
   if (d.nw) k_walls<<<grid_for(d.nw, kBlock), kBlock, 0, s>>>(d);
+  mark();
   k_force<<<g, kBlock, 0, s>>>(d);
+  mark();
   k_reaction<<<d.nblocks_ob, kBlock, 0, s>>>(d);
+  mark();
   TSPH_CUDA_CHECK(cudaMemsetAsync(d.maxbits, 0, 2 * sizeof(unsigned long long), s));
   k_integrate<<<d.nblocks_int, kBlock, 0, s>>>(d);
   k_finalize<<<1, 32, 0, s>>>(d);
   TSPH_LAUNCH_CHECK();
+  mark();
   if (d.shift_every > 0) {
     rc = enqueue_rebuild(E, s);
     if (rc) return rc;
+    mark();
     k_concentration<<<g, kBlock, 0, s>>>(d);
+    mark();
     k_conc_gradient<<<g, kBlock, 0, s>>>(d);
+    mark();
     const double pos = 0.95 * static_cast<double>(d.nf - 1);
     const long long lo = static_cast<long long>(std::floor(pos)), hi = static_cast<long long>(std::ceil(pos));
     const unsigned gs = grid_for(d.nf, 256, 148 * 4);
@@ -885,8 +905,10 @@ int enqueue_step(tsph_engine* E, cudaStream_t s) {
       }
     }
     k_select_finish<<<1, 32, 0, s>>>(d, pos - static_cast<double>(lo));
+    mark();
     k_shift_apply<<<g, kBlock, 0, s>>>(d);
     TSPH_LAUNCH_CHECK();
+    mark();
   }
   return TSPH_OK;
 }
@@ -1044,6 +1066,46 @@ int tsph_engine_step_eager(tsph_engine* E, int64_t steps, tsph_stream stream) {
     int rc = enqueue_step(E, s);
     if (rc) return rc;
   }
+  return TSPH_OK;
+}
+
+int tsph_engine_step_timed(tsph_engine* E, tsph_stream stream, float* stage_ms, int64_t* stages) {
+  if (!E || !stage_ms || !stages) return TSPH_ERR_ARG;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  cudaEvent_t ev[kStages + 1];
+  for (int i = 0; i <= kStages; ++i) TSPH_CUDA_CHECK(cudaEventCreate(&ev[i]));
+  TSPH_CUDA_CHECK(cudaEventRecord(ev[0], s));
+  int rc = enqueue_step(E, s, ev + 1);
+  const int n = E->d.shift_every > 0 ? kStages : 7;
+  if (rc == TSPH_OK) {
+    if (cudaEventSynchronize(ev[n]) != cudaSuccess) rc = TSPH_ERR_CUDA;
+    for (int i = 0; i < n && rc == TSPH_OK; ++i)
+      if (cudaEventElapsedTime(&stage_ms[i], ev[i], ev[i + 1]) != cudaSuccess) rc = TSPH_ERR_CUDA;
+  }
+  for (int i = 0; i <= kStages; ++i) cudaEventDestroy(ev[i]);
+  *stages = n;
+  return rc;
+}
+
+int tsph_engine_graph_kernels(tsph_engine* E, int64_t* kernels) {
+  if (!E || !kernels) return TSPH_ERR_ARG;
+  *kernels = 0;
+  if (!E->graph) return TSPH_ERR_ARG;
+  size_t count = 0;
+  TSPH_CUDA_CHECK(cudaGraphGetNodes(E->graph, nullptr, &count));
+  cudaGraphNode_t* nodes = new (std::nothrow) cudaGraphNode_t[count];
+  if (!nodes) return TSPH_ERR_ARG;
+  if (cudaGraphGetNodes(E->graph, nodes, &count) != cudaSuccess) {
+    delete[] nodes;
+    return TSPH_ERR_CUDA;
+  }
+  int64_t k = 0;
+  for (size_t i = 0; i < count; ++i) {
+    cudaGraphNodeType t;
+    if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++k;
+  }
+  delete[] nodes;
+  *kernels = k;
   return TSPH_OK;
 }
 

@@ -220,6 +220,26 @@ class DamBreak3DEngine:
             for t in tensors:
                 t.record_stream(cur)
 
+    STAGES = ("rebuild", "density", "diffusion_eos", "walls", "force", "reaction",
+              "integrate", "shift_rebuild", "concentration", "gradient", "select", "shift_apply")
+
+    def step_timed(self) -> dict:
+        """One eager step with CUDA events between stages; ``{stage: ms}``."""
+        self.stream.wait_stream(torch.cuda.current_stream(self.device))
+        ms = (ctypes.c_float * 12)()
+        n = ctypes.c_int64(0)
+        _lib.check(_lib.lib().tsph_engine_step_timed(self._handle, self.stream.cuda_stream, ms,
+                                                     ctypes.byref(n)), "tsph_engine_step_timed")
+        self.steps_done += 1
+        return {self.STAGES[i]: float(ms[i]) for i in range(n.value)}
+
+    def graph_kernels(self) -> int:
+        """Kernel launches in one captured step (the step graph's kernel nodes)."""
+        k = ctypes.c_int64(0)
+        _lib.check(_lib.lib().tsph_engine_graph_kernels(self._handle, ctypes.byref(k)),
+                   "tsph_engine_graph_kernels")
+        return int(k.value)
+
     def diagnostics(self, first: int, count: int) -> torch.Tensor:
         """Per-step meter rows ``(count, 16)`` (fields in ``DIAG_FIELDS``)."""
         with torch.cuda.stream(self.stream):

@@ -24,6 +24,7 @@ def test_pairs_and_cell_order_bit_exact(golden):
         assert np.array_equal(pairs, g[f"c{k}_pairs"]), k
         *_, order = on.cell_grid(pos, cutoff)
         assert np.array_equal(order, g[f"c{k}_order"]), k
+        assert np.array_equal(on.cell_linked_pairs_batched(pos, cutoff), g[f"c{k}_pairs"]), k
         if pos.shape[0] <= 400:
             assert np.array_equal(on.brute_force_pairs(pos, cutoff), g[f"c{k}_pairs"]), k
 
