@@ -439,111 +439,126 @@ __global__ void k_reaction(Dev e) {
 }
 
 // Semi-implicit Euler, box and obstacle clamps, meters (state before the update,
-// as the reference samples it), skin displacement.
+// as the reference samples it), skin displacement.  Per-block partials only:
+// [0] kinetic [1] potential [2] max displacement [3] max speed [4] max front
+// [5] max density [6] escapes [7] obstacle clamps; k_finalize reduces them.
 __global__ void k_integrate(Dev e) {
-  __shared__ double part[kBlock / 32][2];
-  double ke = 0, pe = 0, dmax = 0, vmax = 0, xmax = 0;
-  float rmax = 0.f;
-  long long esc = 0, clamps = 0;
+  __shared__ double part[kBlock / 32][8];
+  double acc8[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   bool bad = false;
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
-    double4 x = ld4(e.pos, a);
-    double4 v = ld4(e.vel, a);
+    const double4 x0 = ld4(e.pos, a);
+    const double4 v0 = ld4(e.vel, a);
     const float4 ac = e.acc[a];
-    const double m = x.w;
-    const double v2 = v.x * v.x + v.y * v.y + v.z * v.z;
-    vmax = fmax(vmax, sqrt(v2));
-    xmax = fmax(xmax, x.x);
-    rmax = fmaxf(rmax, e.vr[a].w);
-    ke += 0.5 * m * v2;
-    pe += m * e.gravity * x.y;
-    v.x += e.dt * static_cast<double>(ac.x);
-    v.y += e.dt * static_cast<double>(ac.y);
-    v.z += e.dt * static_cast<double>(ac.z);
-    x.x += e.dt * v.x;
-    x.y += e.dt * v.y;
-    x.z += e.dt * v.z;
-    double* xs[3] = {&x.x, &x.y, &x.z};
-    double* vs[3] = {&v.x, &v.y, &v.z};
+    const double m = x0.w;
+    const double v2 = v0.x * v0.x + v0.y * v0.y + v0.z * v0.z;
+    acc8[0] += 0.5 * m * v2;
+    acc8[1] += m * e.gravity * x0.y;
+    acc8[3] = fmax(acc8[3], sqrt(v2));
+    acc8[4] = fmax(acc8[4], x0.x);
+    acc8[5] = fmax(acc8[5], static_cast<double>(e.vr[a].w));
+    double v[3] = {v0.x + e.dt * static_cast<double>(ac.x), v0.y + e.dt * static_cast<double>(ac.y),
+                   v0.z + e.dt * static_cast<double>(ac.z)};
+    double x[3] = {x0.x + e.dt * v[0], x0.y + e.dt * v[1], x0.z + e.dt * v[2]};
     bool out_any = false;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       const double hi = e.box_hi[k];
-      const double xv = *xs[k];
-      const bool out = xv < -e.tol || xv > hi + e.tol;
-      *xs[k] = xv < 0.0 ? 0.0 : (xv > hi ? hi : xv);
-      if (out) { *vs[k] = 0.0; out_any = true; }
-    }
-    esc += out_any;
-    if (e.has_ob) {
-      const bool inside = x.x > e.ob_lo[0] && x.x < e.ob_hi[0] && x.y > e.ob_lo[1] && x.y < e.ob_hi[1] &&
-                          x.z > e.ob_lo[2] && x.z < e.ob_hi[2];
-      if (inside) {
-        double best = x.x - e.ob_lo[0];
-        int which = 0;
-        for (int f = 1; f < 6; ++f) {
-          const int k = f >> 1;
-          const double dist = (f & 1) ? e.ob_hi[k] - *xs[k] : *xs[k] - e.ob_lo[k];
-          if (dist < best) { best = dist; which = f; }
-        }
-        const int k = which >> 1;
-        *xs[k] = (which & 1) ? e.ob_hi[k] + e.ob_eps : e.ob_lo[k] - e.ob_eps;
-        *vs[k] = 0.0;
-        ++clamps;
+      const bool out = x[k] < -e.tol || x[k] > hi + e.tol;
+      x[k] = x[k] < 0.0 ? 0.0 : (x[k] > hi ? hi : x[k]);
+      if (out) {
+        v[k] = 0.0;
+        out_any = true;
       }
     }
-    if (!isfinite(x.x) || !isfinite(x.y) || !isfinite(x.z) || !isfinite(v.x) || !isfinite(v.y) ||
-        !isfinite(v.z))
+    acc8[6] += out_any ? 1.0 : 0.0;
+    if (e.has_ob && x[0] > e.ob_lo[0] && x[0] < e.ob_hi[0] && x[1] > e.ob_lo[1] && x[1] < e.ob_hi[1] &&
+        x[2] > e.ob_lo[2] && x[2] < e.ob_hi[2]) {
+      double best = x[0] - e.ob_lo[0];
+      int which = 0;
+#pragma unroll
+      for (int f = 1; f < 6; ++f) {
+        const int k = f >> 1;
+        const double dist = (f & 1) ? e.ob_hi[k] - x[k] : x[k] - e.ob_lo[k];
+        if (dist < best) {
+          best = dist;
+          which = f;
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        if (k == (which >> 1)) {
+          x[k] = (which & 1) ? e.ob_hi[k] + e.ob_eps : e.ob_lo[k] - e.ob_eps;
+          v[k] = 0.0;
+        }
+      }
+      acc8[7] += 1.0;
+    }
+    if (!isfinite(x[0]) || !isfinite(x[1]) || !isfinite(x[2]) || !isfinite(v[0]) || !isfinite(v[1]) ||
+        !isfinite(v[2]))
       bad = true;
-    st4(e.pos, a, x);
-    st4(e.vel, a, v);
+    st4(e.pos, a, make_double4(x[0], x[1], x[2], m));
+    st4(e.vel, a, make_double4(v[0], v[1], v[2], 0.0));
     const double4 an = ld4(e.anchor, a);
-    const double ex = x.x - an.x, ey = x.y - an.y, ez = x.z - an.z;
-    dmax = fmax(dmax, sqrt(ex * ex + ey * ey + ez * ez));
+    const double ex = x[0] - an.x, ey = x[1] - an.y, ez = x[2] - an.z;
+    acc8[2] = fmax(acc8[2], sqrt(ex * ex + ey * ey + ez * ez));
   }
-  dmax = warp_reduce_max(dmax);
-  vmax = warp_reduce_max(vmax);
-  xmax = warp_reduce_max(xmax);
-  rmax = warp_reduce_max(rmax);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const bool is_max = k >= 2 && k <= 5;
+    acc8[k] = is_max ? warp_reduce_max(acc8[k]) : warp_reduce_sum(acc8[k]);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0)
+    for (int k = 0; k < 8; ++k) part[warp][k] = acc8[k];
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(e.status, 2);
+  __syncthreads();
+  if (threadIdx.x < 8) {
+    const int k = threadIdx.x;
+    const bool is_max = k >= 2 && k <= 5;
+    double r = part[0][k];
+    for (int w = 1; w < kBlock / 32; ++w) r = is_max ? fmax(r, part[w][k]) : r + part[w][k];
+    e.partials[static_cast<int64_t>(blockIdx.x) * 8 + k] = r;
+  }
+}
+
+// One warp reduces the per-block partials in a fixed order (deterministic).
+__global__ void k_finalize(Dev e) {
+  if (blockIdx.x) return;
+  const int lane = threadIdx.x;
+  double ke = 0, pe = 0, dmax = 0, vmax = 0, xmax = 0, rmax = 0, esc = 0, clamps = 0;
+  double f[3] = {0, 0, 0};
+  for (int b = lane; b < e.nblocks_int; b += 32) {
+    const double* q = e.partials + static_cast<int64_t>(b) * 8;
+    ke += q[0];
+    pe += q[1];
+    dmax = fmax(dmax, q[2]);
+    vmax = fmax(vmax, q[3]);
+    xmax = fmax(xmax, q[4]);
+    rmax = fmax(rmax, q[5]);
+    esc += q[6];
+    clamps += q[7];
+  }
+  for (int b = lane; b < e.nblocks_ob; b += 32)
+    for (int k = 0; k < 3; ++k) f[k] += e.partials[static_cast<int64_t>(e.nblocks_int + b) * 8 + k];
   ke = warp_reduce_sum(ke);
   pe = warp_reduce_sum(pe);
   esc = warp_reduce_sum(esc);
   clamps = warp_reduce_sum(clamps);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0) {
-    atomic_max_nonneg(&e.maxbits[0], dmax);
-    atomic_max_nonneg(&e.maxbits[3], vmax);
-    atomic_max_nonneg(&e.maxbits[4], xmax);
-    atomic_max_nonneg(&e.maxbits[2], static_cast<double>(rmax));
-    if (esc) atomicAdd(reinterpret_cast<unsigned long long*>(&e.counters[0]), static_cast<unsigned long long>(esc));
-    if (clamps) atomicAdd(reinterpret_cast<unsigned long long*>(&e.counters[1]), static_cast<unsigned long long>(clamps));
-    part[warp][0] = ke;
-    part[warp][1] = pe;
-  }
-  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(e.status, 2);
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s0 = 0, s1 = 0;
-    for (int w = 0; w < kBlock / 32; ++w) { s0 += part[w][0]; s1 += part[w][1]; }
-    e.partials[static_cast<int64_t>(blockIdx.x) * 8 + 0] = s0;
-    e.partials[static_cast<int64_t>(blockIdx.x) * 8 + 1] = s1;
-  }
-}
-
-__global__ void k_finalize(Dev e) {
-  if (threadIdx.x || blockIdx.x) return;
-  double ke = 0, pe = 0, f[3] = {0, 0, 0};
-  for (int b = 0; b < e.nblocks_int; ++b) {
-    ke += e.partials[static_cast<int64_t>(b) * 8];
-    pe += e.partials[static_cast<int64_t>(b) * 8 + 1];
-  }
-  for (int b = 0; b < e.nblocks_ob; ++b)
-    for (int k = 0; k < 3; ++k) f[k] += e.partials[static_cast<int64_t>(e.nblocks_int + b) * 8 + k];
+  dmax = warp_reduce_max(dmax);
+  vmax = warp_reduce_max(vmax);
+  xmax = warp_reduce_max(xmax);
+  rmax = warp_reduce_max(rmax);
+  for (int k = 0; k < 3; ++k) f[k] = warp_reduce_sum(f[k]);
+  if (lane) return;
+  e.counters[0] += static_cast<long long>(esc);
+  e.counters[1] += static_cast<long long>(clamps);
+  e.maxbits[0] = static_cast<unsigned long long>(__double_as_longlong(dmax));
   const long long step = e.counters[3];
   double* row = e.diag + (step % e.diag_ring) * kDiag;
-  row[0] = __longlong_as_double(static_cast<long long>(e.maxbits[2]));
-  row[1] = __longlong_as_double(static_cast<long long>(e.maxbits[3]));
-  row[2] = __longlong_as_double(static_cast<long long>(e.maxbits[4]));
+  row[0] = rmax;
+  row[1] = vmax;
+  row[2] = xmax;
   row[3] = f[0];
   row[4] = f[1];
   row[5] = f[2];
@@ -559,8 +574,7 @@ __global__ void k_finalize(Dev e) {
   row[14] = e.impulse[0];
   row[15] = e.cref[0];
   // the speed of this step is the shift's reference speed
-  e.cref[1] = __longlong_as_double(static_cast<long long>(e.maxbits[3]));
-  e.maxbits[2] = e.maxbits[3] = e.maxbits[4] = 0;
+  e.cref[1] = vmax;
   e.counters[3] = step + 1;
   e.flag[2] = e.shift_every > 0 && step > 0 && (step % e.shift_every) == 0;
   e.flag[3] = 0;
@@ -701,9 +715,16 @@ __global__ void k_shift_apply(Dev e) {
     const double ex = x.x - an.x, ey = x.y - an.y, ez = x.z - an.z;
     dmax = fmax(dmax, sqrt(ex * ex + ey * ey + ez * ez));
   }
+  __shared__ double part[kBlock / 32];
   dmax = warp_reduce_max(dmax);
-  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&e.maxbits[1], dmax);
-  if (blockIdx.x == 0 && threadIdx.x == 0) e.flag[3] = 1;
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = dmax;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r = part[0];
+    for (int w = 1; w < kBlock / 32; ++w) r = fmax(r, part[w]);
+    atomic_max_nonneg(&e.maxbits[1], r);
+    if (blockIdx.x == 0) e.flag[3] = 1;
+  }
 }
 
 // ----------------------------------------------------------------- init ---
