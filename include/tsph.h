@@ -166,6 +166,26 @@ int64_t tsph_wcsph_workspace_bytes(const tsph_wcsph_params* prm);
 int tsph_wcsph_rhs(const tsph_wcsph_params* prm, const tsph_wcsph_io* io, void* ws,
                    int64_t ws_bytes, tsph_stream stream);
 
+/* tsph_wcsph_rhs without a workspace argument: this entry point allocates no
+ * device memory.  It has no counterpart in the reference (whose pair pass
+ * allocates freely through PyTorch).  It exists for callers that cannot call
+ * cudaMalloc at the point where they need the pair pass -- a host framework
+ * that owns the whole GPU memory pool, or a real-time loop that reserves its
+ * memory once up front -- and that still own their input and output buffers.
+ *
+ * Its scratch is a fixed 16 MiB array inside the library's device image
+ * (every GPU that loads the library holds it until the process exits).  Calls
+ * whose tsph_wcsph_workspace_bytes exceeds 16 MiB are rejected with
+ * TSPH_ERR_CAPACITY before any GPU work: about 300,000 particles (fluid +
+ * wall) in FP32, 150,000 in FP64.  The first call on a device looks up the
+ * array's device address (with that device current), so make that first call
+ * before any stream capture; the stream must belong to the current device.
+ * Every call shares the one array and leaves its contents behind: calls that
+ * overlap on the GPU (other streams, other threads, the same device) race on
+ * it, so serialise them.  No part of the array has to start at zero. */
+int tsph_wcsph_rhs_noalloc(const tsph_wcsph_params* prm, const tsph_wcsph_io* io,
+                           tsph_stream stream);
+
 /* ------------------------------------------------------------------------ */
 /* threed operators: threed/operators3.py:212-256 (accelerations), with      */
 /* summation_density :70, diffusion :259, Adami :173, pressure :96 and the   */

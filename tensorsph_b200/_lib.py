@@ -117,6 +117,7 @@ _SIGNATURES = {
     "tsph_wcsph_workspace_bytes": (c_int64, [POINTER(WcsphParams)]),
     "tsph_wcsph_rhs": (c_int, [POINTER(WcsphParams), POINTER(WcsphIO), c_void_p, c_int64,
                                c_void_p]),
+    "tsph_wcsph_rhs_noalloc": (c_int, [POINTER(WcsphParams), POINTER(WcsphIO), c_void_p]),
     "tsph_threed_workspace_bytes": (c_int64, [POINTER(ThreedParams)]),
     "tsph_threed_accelerations": (c_int, [POINTER(ThreedParams), POINTER(ThreedIO), c_void_p,
                                           c_int64, c_void_p]),

@@ -14,6 +14,7 @@
 //                       - sum 2 nu blend (v_a - v_b) (m_b / rho_b) L_ab + g   fluid rows
 //   K6 reaction   force of the fluid on each wall particle (split / 3-D)    wall rows
 #include <cmath>
+#include <mutex>
 
 #include "common.cuh"
 #include "fpmath.cuh"
@@ -547,3 +548,44 @@ int tsph_wcsph_rhs(const tsph_wcsph_params* prm, const tsph_wcsph_io* io, void* 
 }
 
 }  // extern "C"
+
+// ------------------------------------------------ allocation-free variant ---
+//
+// Scratch of tsph_wcsph_rhs_noalloc: one fixed array in the library's own
+// device image, so a call needs no allocation at all.  Every GPU that loads
+// the library holds these 16 MiB until the process exits.  Host code must not
+// hand `g_rhs_noalloc_scratch` itself to a kernel (on the host it names a
+// host-side stand-in, not device memory): the device address comes from
+// cudaGetSymbolAddress, taken once per device with that device current.
+static constexpr int64_t kNoAllocScratchBytes = int64_t(16) << 20;
+static __device__ __align__(256) unsigned char g_rhs_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+constexpr int kMaxDevices = 128;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[kMaxDevices] = {};
+}  // namespace
+
+extern "C" int tsph_wcsph_rhs_noalloc(const tsph_wcsph_params* prm, const tsph_wcsph_io* io,
+                                      tsph_stream stream) {
+  if (!prm || !io) return TSPH_ERR_ARG;
+  const int64_t need = tsph_wcsph_workspace_bytes(prm);
+  if (need < 0) return TSPH_ERR_ARG;
+  if (need > kNoAllocScratchBytes) return TSPH_ERR_CAPACITY;
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return TSPH_ERR_CUDA;
+  void* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    scratch = g_noalloc_ptr[dev];
+    if (!scratch) {
+      if (cudaGetSymbolAddress(&scratch, g_rhs_noalloc_scratch) != cudaSuccess || !scratch)
+        return TSPH_ERR_CUDA;
+      g_noalloc_ptr[dev] = scratch;
+    }
+  }
+  // Nothing in the scratch needs to start at zero: every byte the rhs kernels
+  // read was written earlier in the same call, so stale contents of a
+  // previous call are never seen.
+  return tsph_wcsph_rhs(prm, io, scratch, need, stream);
+}
