@@ -2,14 +2,22 @@
 // (with the obstacle wall force of kleefsman_obstacle_3d.py:644-706 and the
 // optional Lind shift of particle_shifting.py:166-224), one CUDA graph per step.
 //
-// Layout (all in one caller-provided arena, particles in cell order):
-//   pos  double4[N]   x, y, z, mass      fluid [0, nf), walls [nf, N)  (FP64 state)
-//   vel  double4[nf]  FP64 velocity
-//   vr   float4[N]    FP32 velocity + density (walls: 0 velocity, Adami density)
-//   pr   float[N]     pressure;  pq float[N] p / rho^2
-//   nbr  int32[maxnb * N]  k-major neighbour rows (coalesced per k), cnt[N]
-// Pair arithmetic is FP32 with compensated sums; separations are taken in
-// FP64 and rounded once, so a 1 m tank loses no digits against h ~ 1e-2 m.
+// Layout (one caller-provided arena; particles in cell order, fluid rows
+// [0, nf) re-sorted at every rebuild, wall rows [nf, N) sorted once):
+//   pos  double4[N]  x, y, z, mass -- FP64 state (integration, list builds)
+//   lp   float4[N]   position relative to the particle's home cell + mass;
+//                    the home cell is its cell at the last rebuild
+//   vb   float4[N]   FP32 velocity + volume m/rho (walls: 0 + m/rho_w)
+//   pr, rho, pq      float[N] pressure, density, p/rho^2
+//   nbr  uint32[maxnb * N]  k-major rows (thread a reads nbr[k*N + a],
+//                    coalesced); entry = neighbour << 5 | cell-offset code
+// A pair separation is (l_a - l_b) - (c_b - c_a) * cell: exact to the FP32
+// rounding of the two local coordinates (~1e-9 m here), so the FP32 pair
+// arithmetic loses nothing against the FP64 positions.
+//
+// Gather loops take kBatch neighbours per iteration without branches, so
+// several independent loads are in flight per thread; each batch's partial
+// sums enter a Neumaier-compensated FP32 accumulator.
 //
 // Step (fixed launch sequence, graph-captured):
 //   check/rebuild  skin test -> (cell keys, radix sort, permute, cell table, rows)
@@ -29,6 +37,8 @@ namespace {
 
 constexpr int kBlock = 128;
 constexpr int kDiag = 16;
+constexpr int kBatch = 4;
+constexpr int kMaxFinalBlocks = 148 * 8;
 
 struct Dev {
   int nf, nw, N, nob, maxnb, shift_every, diag_ring;
@@ -37,23 +47,26 @@ struct Dev {
   double dt, box_hi[3], tol, ob_lo[3], ob_hi[3], ob_eps;
   int has_ob;
   double gravity;
-  float h, inv_h, sigma, sig2d, support2, rho0, bulk, gamma, inv_gamma, grav, nu2, nu2f, dscale, dtf,
-      visc_eps, rho_floor, wall_mass;
+  float cellf, h, inv_h, sigma, sig2d, support2, rho0, bulk, gamma, inv_gamma, grav, nu2, nu2f, dscale,
+      dtf, visc_eps, rho_floor, wall_mass;
   double shift_strength_h_dt, shift_cap, shift_fs, vref_floor;
   // arrays
   double4* pos;
   double4* vel;
   double4* anchor;
+  float4* lp;
+  int32_t* home;
   int32_t* id;
   int32_t* wall_id;
-  float4* vr;
+  float4* vb;
   float* pr;
+  float* rho;
   float* pq;
-  float* rho_s;
+  float2* rs;
   float4* acc;
   float* conc;
   float4* gradc;
-  int32_t* nbr;
+  uint32_t* nbr;
   int32_t* cnt;
   int32_t* ob_rows;
   int32_t* fstart;
@@ -66,11 +79,10 @@ struct Dev {
   int32_t* vals_tmp;
   double4* tmp4a;
   double4* tmp4b;
-  double4* tmp4c;
   int32_t* tmp_id;
   // control words
   int* flag;         // [0] rebuild now, [1] first step, [2] shift this step, [3] shift done
-  unsigned long long* maxbits;  // [0] disp (integrate), [1] disp (shift), [2] rho, [3] speed, [4] front
+  unsigned long long* maxbits;  // [0] disp (integrate), [1] disp (shift)
   int* status;       // bit 0: neighbour row overflow, bit 1: non-finite state
   long long* counters;  // [0] escapes [1] clamps [2] rebuilds [3] step [4] max row [5] select k
   double* partials;  // per-block sums: [blk*8 + 0..7]
@@ -80,24 +92,20 @@ struct Dev {
   double* diag;      // diag_ring * kDiag
   unsigned int* hist;        // 256
   unsigned long long* sel;   // [0] prefix [1] value lo bits [2] value hi bits
-  double* cref;
+  double* cref;      // [0] c_ref, [1] max speed of the step
 };
 
 __device__ __forceinline__ float shape(float q) {
-  if (q < 1.f) return 1.f - 1.5f * q * q + 0.75f * q * q * q;
-  if (q < 2.f) {
-    float t = 2.f - q;
-    return 0.25f * t * t * t;
-  }
-  return 0.f;
+  const float t = 2.f - q;
+  const float far = 0.25f * t * t * t;
+  const float near = 1.f - 1.5f * q * q + 0.75f * q * q * q;
+  return q < 1.f ? near : (q < 2.f ? far : 0.f);
 }
 __device__ __forceinline__ float dshape(float q) {
-  if (q < 1.f) return -3.f * q + 2.25f * q * q;
-  if (q < 2.f) {
-    float t = 2.f - q;
-    return -0.75f * t * t;
-  }
-  return 0.f;
+  const float t = 2.f - q;
+  const float far = -0.75f * t * t;
+  const float near = -3.f * q + 2.25f * q * q;
+  return q < 1.f ? near : (q < 2.f ? far : 0.f);
 }
 
 __device__ __forceinline__ double4 ld4(const double4* p, int i) {
@@ -122,6 +130,26 @@ __device__ __forceinline__ int cell_of(const Dev& e, double x, double y, double 
   return (cx * e.ncy + cy) * e.ncz + cz;
 }
 
+// Position relative to the origin of cell `key`; the cell origin uses the
+// FP32-rounded cell size so that (c_a - c_b) * cellf is exact in FP32.
+__device__ __forceinline__ float4 local_of(const Dev& e, int key, double x, double y, double z, double m) {
+  const int cz = key % e.ncz;
+  const int cy = (key / e.ncz) % e.ncy;
+  const int cx = key / (e.ncz * e.ncy);
+  const double cs = static_cast<double>(e.cellf);
+  return make_float4(static_cast<float>(x - (e.origin[0] + cx * cs)),
+                     static_cast<float>(y - (e.origin[1] + cy * cs)),
+                     static_cast<float>(z - (e.origin[2] + cz * cs)), static_cast<float>(m));
+}
+
+// Cell-offset table in shared memory: code = (dx+1)*9 + (dy+1)*3 + (dz+1)
+// for dx, dy, dz = c_b - c_a; entry = (c_b - c_a) * cell.
+__device__ __forceinline__ void fill_offsets(float4* tab, float cellf) {
+  for (int c = threadIdx.x; c < 27; c += blockDim.x)
+    tab[c] = make_float4((c / 9 - 1) * cellf, ((c / 3) % 3 - 1) * cellf, (c % 3 - 1) * cellf, 0.f);
+  __syncthreads();
+}
+
 __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* p, double v) {
   if (v > 0.0) atomicMax(p, static_cast<unsigned long long>(__double_as_longlong(v)));
 }
@@ -131,6 +159,50 @@ __device__ __forceinline__ float tait(const Dev& e, float rho) {
   ratio = ratio > 0.01f ? ratio : 0.01f;
   float p = e.bulk * (powf(ratio, e.gamma) - 1.f);
   return p > 0.f ? p : 0.f;
+}
+
+// Kernel arguments from r^2 with one reciprocal square root: q = r / h and
+// 1/r, so that gs = sigma f'(q) / (h r) needs no division (grad_a W = d * gs);
+// at r = 0, f'(0) = 0 and 1/r is taken as 0.
+struct Radial {
+  float r, q, inv_r;
+};
+__device__ __forceinline__ Radial radial(float r2, float inv_h) {
+  Radial o;
+  o.inv_r = r2 > 1e-24f ? rsqrtf(r2) : 0.f;
+  o.r = r2 * o.inv_r;
+  o.q = o.r * inv_h;
+  return o;
+}
+
+// separation x_a - x_b = (l_a - l_b) - (c_b - c_a) * cell for a neighbour
+// entry whose offset-table row is `off` = (c_b - c_a) * cell
+__device__ __forceinline__ float3 sep(const float4& la, const float4& lb, const float4& off) {
+  return make_float3((la.x - lb.x) - off.x, (la.y - lb.y) - off.y, (la.z - lb.z) - off.z);
+}
+
+// Walk row a in batches: `body(entry, j)` for j in batch; loads of the batch
+// are issued before any use.
+template <class Body>
+__device__ __forceinline__ void walk_row(const Dev& e, int a, Body&& body) {
+  const int n = e.cnt[a];
+  const uint32_t* row = e.nbr + a;
+  int k = 0;
+  for (; k + kBatch <= n; k += kBatch) {
+    uint32_t ent[kBatch];
+#pragma unroll
+    for (int j = 0; j < kBatch; ++j) ent[j] = row[static_cast<int64_t>(k + j) * e.N];
+    body(ent);
+  }
+  if (k < n) {
+    uint32_t ent[kBatch];
+#pragma unroll
+    for (int j = 0; j < kBatch; ++j) {
+      // pad with a harmless self entry whose contribution is masked out
+      ent[j] = (k + j < n) ? row[static_cast<int64_t>(k + j) * e.N] : 0xffffffffu;
+    }
+    body(ent);
+  }
 }
 
 // ------------------------------------------------------------ rebuild ---
@@ -172,10 +244,13 @@ __global__ void k_permute_back(Dev e) {
   if (!e.flag[0]) return;
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
     const double4 p = ld4(e.tmp4a, a);
+    const int key = static_cast<int>(e.keys[a]);
     st4(e.pos, a, p);
     st4(e.anchor, a, p);
     st4(e.vel, a, ld4(e.tmp4b, a));
     e.id[a] = e.tmp_id[a];
+    e.home[a] = key;
+    e.lp[a] = local_of(e, key, p.x, p.y, p.z, p.w);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     e.maxbits[0] = 0;
@@ -201,13 +276,16 @@ __global__ void k_fill_table(const uint64_t* __restrict__ keys, int n, int32_t* 
   }
 }
 
+// Neighbour rows at the list cutoff (2h + skin) in FP64, for every particle;
+// wall rows keep fluid neighbours only (they feed the Adami extrapolation and
+// the obstacle reaction).
 __global__ void k_rows(Dev e) {
   if (!e.flag[0]) return;
   int rowmax = 0;
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.N; a += gridDim.x * blockDim.x) {
     const double4 pa = ld4(e.pos, a);
-    int cx, cy, cz;
-    cell_of(e, pa.x, pa.y, pa.z, cx, cy, cz);
+    const int key_a = e.home[a];
+    const int cz = key_a % e.ncz, cy = (key_a / e.ncz) % e.ncy, cx = key_a / (e.ncz * e.ncy);
     int count = 0;
     const bool fluid_row = a < e.nf;
     for (int dx = -1; dx <= 1; ++dx) {
@@ -220,6 +298,7 @@ __global__ void k_rows(Dev e) {
           const int z = cz + dz;
           if (z < 0 || z >= e.ncz) continue;
           const int c = (x * e.ncy + y) * e.ncz + z;
+          const uint32_t code = static_cast<uint32_t>((dx + 1) * 9 + (dy + 1) * 3 + (dz + 1));
           const int fs = e.fstart[c];
           if (fs >= 0) {
             const int fe = e.fend[c];
@@ -228,7 +307,8 @@ __global__ void k_rows(Dev e) {
               const double4 pb = ld4(e.pos, b);
               const double ddx = pa.x - pb.x, ddy = pa.y - pb.y, ddz = pa.z - pb.z;
               if (ddx * ddx + ddy * ddy + ddz * ddz <= e.rc2) {
-                if (count < e.maxnb) e.nbr[static_cast<int64_t>(count) * e.N + a] = b;
+                if (count < e.maxnb)
+                  e.nbr[static_cast<int64_t>(count) * e.N + a] = (static_cast<uint32_t>(b) << 5) | code;
                 ++count;
               }
             }
@@ -242,7 +322,8 @@ __global__ void k_rows(Dev e) {
                 const double4 pb = ld4(e.pos, b);
                 const double ddx = pa.x - pb.x, ddy = pa.y - pb.y, ddz = pa.z - pb.z;
                 if (ddx * ddx + ddy * ddy + ddz * ddz <= e.rc2) {
-                  if (count < e.maxnb) e.nbr[static_cast<int64_t>(count) * e.N + a] = b;
+                  if (count < e.maxnb)
+                    e.nbr[static_cast<int64_t>(count) * e.N + a] = (static_cast<uint32_t>(b) << 5) | code;
                   ++count;
                 }
               }
@@ -261,165 +342,192 @@ __global__ void k_rows(Dev e) {
 
 // ------------------------------------------------------------- physics ---
 
-__device__ __forceinline__ float3 sep(const double4& a, const double4& b) {
-  return make_float3(static_cast<float>(a.x - b.x), static_cast<float>(a.y - b.y),
-                     static_cast<float>(a.z - b.z));
-}
-
-__global__ void k_density(Dev e) {
+__global__ void __launch_bounds__(kBlock) k_density(Dev e) {
+  __shared__ float4 tab[27];
+  fill_offsets(tab, e.cellf);
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
-    const double4 pa = ld4(e.pos, a);
+    const float4 la = e.lp[a];
     CSum<float> s;
-    s.add(static_cast<float>(pa.w) * e.sigma);
-    const int n = e.cnt[a];
-    for (int k = 0; k < n; ++k) {
-      const int b = e.nbr[static_cast<int64_t>(k) * e.N + a];
-      const double4 pb = ld4(e.pos, b);
-      const float3 d = sep(pa, pb);
-      const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
-      if (r2 >= e.support2) continue;
-      const float W = e.sigma * shape(sqrtf(r2) * e.inv_h);
-      s.add(static_cast<float>(pb.w) * W);
-    }
+    s.add(la.w * e.sigma);
+    walk_row(e, a, [&](const uint32_t* ent) {
+      float part = 0.f;
+#pragma unroll
+      for (int j = 0; j < kBatch; ++j) {
+        const bool ok = ent[j] != 0xffffffffu;
+        const int b = ok ? static_cast<int>(ent[j] >> 5) : a;
+        const float4 lb = e.lp[b];
+        const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u]);
+        const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+        const float W = e.sigma * shape(radial(r2, e.inv_h).q);
+        part += ok ? lb.w * W : 0.f;
+      }
+      s.add(part);
+    });
     float rho = s.value();
-    e.rho_s[a] = rho > e.rho_floor ? rho : e.rho_floor;
+    rho = rho > e.rho_floor ? rho : e.rho_floor;
+    e.rs[a] = make_float2(rho, la.w / rho);
   }
 }
 
-__global__ void k_diffusion_eos(Dev e) {
+__global__ void __launch_bounds__(kBlock) k_diffusion_eos(Dev e) {
+  __shared__ float4 tab[27];
+  fill_offsets(tab, e.cellf);
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
-    const float ra = e.rho_s[a];
-    float rho = ra;
+    const float2 ra = e.rs[a];
+    float rho = ra.x;
     if (e.dscale > 0.f) {
-      const double4 pa = ld4(e.pos, a);
+      const float4 la = e.lp[a];
       CSum<float> rate;
-      const int n = e.cnt[a];
-      for (int k = 0; k < n; ++k) {
-        const int b = e.nbr[static_cast<int64_t>(k) * e.N + a];
-        if (b >= e.nf) continue;
-        const double4 pb = ld4(e.pos, b);
-        const float3 d = sep(pa, pb);
-        const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
-        if (r2 >= e.support2) continue;
-        const float r = sqrtf(r2);
-        const float gs = e.sigma * dshape(r * e.inv_h) / (e.h * (r > 1e-12f ? r : 1e-12f));
-        const float radial = -gs * r2;
-        const float rb = e.rho_s[b];
-        const float coupling = (ra - rb) * radial / (r2 + 1e-12f);
-        rate.add((-e.dscale * (static_cast<float>(pb.w) / rb)) * coupling);
-      }
-      rho = ra + e.dtf * rate.value();
+      walk_row(e, a, [&](const uint32_t* ent) {
+        float part = 0.f;
+#pragma unroll
+        for (int j = 0; j < kBatch; ++j) {
+          const int b = ent[j] != 0xffffffffu ? static_cast<int>(ent[j] >> 5) : a;
+          const bool ok = ent[j] != 0xffffffffu && b < e.nf;
+          const int bf = ok ? b : a;
+          const float4 lb = e.lp[bf];
+          const float2 rb = e.rs[bf];
+          const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u]);
+          const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+          const Radial R = radial(r2, e.inv_h);
+          const float gs = e.sigma * dshape(R.q) * e.inv_h * R.inv_r;
+          const float coupling = (ra.x - rb.x) * (-gs * r2) * __frcp_rn(r2 + 1e-12f);
+          part += ok ? (-e.dscale * rb.y) * coupling : 0.f;
+        }
+        rate.add(part);
+      });
+      rho = ra.x + e.dtf * rate.value();
       rho = rho > e.rho_floor ? rho : e.rho_floor;
     }
     const float p = tait(e, rho);
     const double4 v = ld4(e.vel, a);
-    e.vr[a] = make_float4(static_cast<float>(v.x), static_cast<float>(v.y), static_cast<float>(v.z), rho);
+    const float m = e.lp[a].w;
+    e.vb[a] = make_float4(static_cast<float>(v.x), static_cast<float>(v.y), static_cast<float>(v.z), m / rho);
+    e.rho[a] = rho;
     e.pr[a] = p;
     e.pq[a] = p / (rho * rho);
   }
 }
 
-__global__ void k_walls(Dev e) {
-  for (int w = e.nf + blockIdx.x * blockDim.x + threadIdx.x; w < e.N; w += gridDim.x * blockDim.x) {
-    const double4 pw = ld4(e.pos, w);
+__global__ void __launch_bounds__(kBlock) k_walls(Dev e) {
+  __shared__ float4 tab[27];
+  fill_offsets(tab, e.cellf);
+  for (int a = e.nf + blockIdx.x * blockDim.x + threadIdx.x; a < e.N; a += gridDim.x * blockDim.x) {
+    const float4 la = e.lp[a];
     CSum<float> num, den;
-    const int n = e.cnt[w];
-    for (int k = 0; k < n; ++k) {
-      const int f = e.nbr[static_cast<int64_t>(k) * e.N + w];
-      const double4 pf = ld4(e.pos, f);
-      const float3 d = sep(pw, pf);  // r_w - r_f
-      const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
-      if (r2 >= e.support2) continue;
-      const float W = e.sigma * shape(sqrtf(r2) * e.inv_h);
-      float src = e.pr[f];
-      if (e.grav != 0.f) src = src + e.vr[f].w * (-e.grav * d.y);
-      num.add(src * W);
-      den.add(W);
-    }
+    walk_row(e, a, [&](const uint32_t* ent) {
+      float pn = 0.f, pd = 0.f;
+#pragma unroll
+      for (int j = 0; j < kBatch; ++j) {
+        const bool ok = ent[j] != 0xffffffffu;
+        const int f = ok ? static_cast<int>(ent[j] >> 5) : 0;
+        const float4 lf = e.lp[f];
+        const float3 d = sep(la, lf, tab[ok ? (ent[j] & 31u) : 13u]);  // r_w - r_f
+        const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+        const float W = ok ? e.sigma * shape(radial(r2, e.inv_h).q) : 0.f;
+        float src = e.pr[f];
+        if (e.grav != 0.f) src = src + e.rho[f] * (-e.grav * d.y);
+        pn += src * W;
+        pd += W;
+      }
+      num.add(pn);
+      den.add(pd);
+    });
     const float dd = den.value();
     float p = num.value() / (dd > 1e-30f ? dd : 1e-30f);
     p = p > 0.f ? p : 0.f;
     float rho = e.rho0 * powf(p / e.bulk + 1.f, e.inv_gamma);
     rho = rho > e.rho0 ? rho : e.rho0;
-    e.vr[w] = make_float4(0.f, 0.f, 0.f, rho);
-    e.pr[w] = p;
-    e.pq[w] = p / (rho * rho);
+    e.vb[a] = make_float4(0.f, 0.f, 0.f, la.w / rho);
+    e.rho[a] = rho;
+    e.pr[a] = p;
+    e.pq[a] = p / (rho * rho);
   }
 }
 
-__global__ void k_force(Dev e) {
+__global__ void __launch_bounds__(kBlock) k_force(Dev e) {
+  __shared__ float4 tab[27];
+  fill_offsets(tab, e.cellf);
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
-    const double4 pa = ld4(e.pos, a);
-    const float4 va = e.vr[a];
+    const float4 la = e.lp[a];
+    const float4 va = e.vb[a];
     const float Pa = e.pq[a];
     CSum<float> ax, ay, az;
-    const int n = e.cnt[a];
-    for (int k = 0; k < n; ++k) {
-      const int b = e.nbr[static_cast<int64_t>(k) * e.N + a];
-      const double4 pb = ld4(e.pos, b);
-      const float3 d = sep(pa, pb);
-      const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
-      if (r2 >= e.support2) continue;
-      const float r = sqrtf(r2);
-      const float gs = e.sigma * dshape(r * e.inv_h) / (e.h * (r > 1e-12f ? r : 1e-12f));
-      const float4 vb = e.vr[b];
-      const float mb = static_cast<float>(pb.w);
-      const float fp = -mb * (Pa + e.pq[b]) * gs;
-      float fx = fp * d.x, fy = fp * d.y, fz = fp * d.z;
-      const float vs = b < e.nf ? e.nu2 : e.nu2f;
-      if (vs != 0.f) {
-        float lw = -(gs * r2);
-        lw = (lw > 0.f ? lw : 0.f) / (r2 + e.visc_eps);
-        const float coef = -vs * (mb / vb.w * lw);
-        fx += coef * (va.x - vb.x);
-        fy += coef * (va.y - vb.y);
-        fz += coef * (va.z - vb.z);
+    walk_row(e, a, [&](const uint32_t* ent) {
+      float px = 0.f, py = 0.f, pz = 0.f;
+#pragma unroll
+      for (int j = 0; j < kBatch; ++j) {
+        const bool ok = ent[j] != 0xffffffffu;
+        const int b = ok ? static_cast<int>(ent[j] >> 5) : a;
+        const float4 lb = e.lp[b];
+        const float4 vb = e.vb[b];
+        const float Pb = e.pq[b];
+        const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u]);
+        const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+        const Radial R = radial(r2, e.inv_h);
+        float gs = e.sigma * dshape(R.q) * e.inv_h * R.inv_r;
+        gs = ok ? gs : 0.f;
+        const float fp = -lb.w * (Pa + Pb) * gs;
+        const float vs = b < e.nf ? e.nu2 : e.nu2f;
+        const float lw = fmaxf(-gs * r2, 0.f) * __frcp_rn(r2 + e.visc_eps);
+        const float coef = -vs * (vb.w * lw);
+        px += fp * d.x + coef * (va.x - vb.x);
+        py += fp * d.y + coef * (va.y - vb.y);
+        pz += fp * d.z + coef * (va.z - vb.z);
       }
-      ax.add(fx);
-      ay.add(fy);
-      az.add(fz);
-    }
+      ax.add(px);
+      ay.add(py);
+      az.add(pz);
+    });
     e.acc[a] = make_float4(ax.value(), ay.value() - e.grav, az.value(), 0.f);
   }
 }
 
 // Force of the fluid on each obstacle particle (rhs_3d(return_wall_force=True),
 // dam_break_3d.py:412-421), reduced per block in FP64.
-__global__ void k_reaction(Dev e) {
+__global__ void __launch_bounds__(kBlock) k_reaction(Dev e) {
+  __shared__ float4 tab[27];
   __shared__ double part[kBlock / 32][3];
+  fill_offsets(tab, e.cellf);
   double fx = 0, fy = 0, fz = 0;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < e.nob; q += gridDim.x * blockDim.x) {
     const int w = e.ob_rows[q];
-    const double4 pw = ld4(e.pos, w);
-    const float rw = e.vr[w].w;
+    const float4 lw_ = e.lp[w];
     const float Pw = e.pq[w];
-    const float mw = static_cast<float>(pw.w);
+    const float mw = lw_.w;
+    const float Vw = e.vb[w].w;
     CSum<float> rx, ry, rz;
-    const int n = e.cnt[w];
-    for (int k = 0; k < n; ++k) {
-      const int f = e.nbr[static_cast<int64_t>(k) * e.N + w];
-      const double4 pf = ld4(e.pos, f);
-      const float3 d = sep(pw, pf);
-      const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
-      if (r2 >= e.support2) continue;
-      const float r = sqrtf(r2);
-      const float gs = e.sigma * dshape(r * e.inv_h) / (e.h * (r > 1e-12f ? r : 1e-12f));
-      const float mf = static_cast<float>(pf.w);
-      const float c = -(mw * mf) * (Pw + e.pq[f]) * gs;
-      float x = c * d.x, y = c * d.y, z = c * d.z;
-      if (e.nu2f != 0.f) {
-        const float4 vf = e.vr[f];
-        float lw = -(gs * r2);
-        lw = (lw > 0.f ? lw : 0.f) / (r2 + e.visc_eps);
-        const float coef = mf * e.nu2f * (mw / rw * lw);
-        x += coef * vf.x;
-        y += coef * vf.y;
-        z += coef * vf.z;
+    walk_row(e, w, [&](const uint32_t* ent) {
+      float px = 0.f, py = 0.f, pz = 0.f;
+#pragma unroll
+      for (int j = 0; j < kBatch; ++j) {
+        const bool ok = ent[j] != 0xffffffffu;
+        const int f = ok ? static_cast<int>(ent[j] >> 5) : 0;
+        const float4 lf = e.lp[f];
+        const float3 d = sep(lw_, lf, tab[ok ? (ent[j] & 31u) : 13u]);
+        const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+        const Radial R = radial(r2, e.inv_h);
+        float gs = e.sigma * dshape(R.q) * e.inv_h * R.inv_r;
+        gs = ok ? gs : 0.f;
+        const float mf = lf.w;
+        const float c = -(mw * mf) * (Pw + e.pq[f]) * gs;
+        float x = c * d.x, y = c * d.y, z = c * d.z;
+        if (e.nu2f != 0.f) {
+          const float4 vf = e.vb[f];
+          const float lwt = fmaxf(-gs * r2, 0.f) * __frcp_rn(r2 + e.visc_eps);
+          const float coef = mf * e.nu2f * (Vw * lwt);
+          x += coef * vf.x;
+          y += coef * vf.y;
+          z += coef * vf.z;
+        }
+        px += x;
+        py += y;
+        pz += z;
       }
-      rx.add(x);
-      ry.add(y);
-      rz.add(z);
-    }
+      rx.add(px);
+      ry.add(py);
+      rz.add(pz);
+    });
     fx += rx.value();
     fy += ry.value();
     fz += rz.value();
@@ -437,7 +545,6 @@ __global__ void k_reaction(Dev e) {
     for (int k = 0; k < 3; ++k) e.partials[static_cast<int64_t>(e.nblocks_int + blockIdx.x) * 8 + k] = s[k];
   }
 }
-
 // Semi-implicit Euler, box and obstacle clamps, meters (state before the update,
 // as the reference samples it), skin displacement.  Per-block partials only:
 // [0] kinetic [1] potential [2] max displacement [3] max speed [4] max front
@@ -456,7 +563,7 @@ __global__ void k_integrate(Dev e) {
     acc8[1] += m * e.gravity * x0.y;
     acc8[3] = fmax(acc8[3], sqrt(v2));
     acc8[4] = fmax(acc8[4], x0.x);
-    acc8[5] = fmax(acc8[5], static_cast<double>(e.vr[a].w));
+    acc8[5] = fmax(acc8[5], static_cast<double>(e.rho[a]));
     double v[3] = {v0.x + e.dt * static_cast<double>(ac.x), v0.y + e.dt * static_cast<double>(ac.y),
                    v0.z + e.dt * static_cast<double>(ac.z)};
     double x[3] = {x0.x + e.dt * v[0], x0.y + e.dt * v[1], x0.z + e.dt * v[2]};
@@ -499,6 +606,7 @@ __global__ void k_integrate(Dev e) {
       bad = true;
     st4(e.pos, a, make_double4(x[0], x[1], x[2], m));
     st4(e.vel, a, make_double4(v[0], v[1], v[2], 0.0));
+    e.lp[a] = local_of(e, e.home[a], x[0], x[1], x[2], m);
     const double4 an = ld4(e.anchor, a);
     const double ex = x[0] - an.x, ey = x[1] - an.y, ez = x[2] - an.z;
     acc8[2] = fmax(acc8[2], sqrt(ex * ex + ey * ey + ez * ez));
@@ -582,51 +690,67 @@ __global__ void k_finalize(Dev e) {
 
 // ------------------------------------------------------------- shifting ---
 
-__global__ void k_concentration(Dev e) {
+__global__ void __launch_bounds__(kBlock) k_concentration(Dev e) {
   if (!e.flag[2]) return;
+  __shared__ float4 tab[27];
+  fill_offsets(tab, e.cellf);
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
-    const double4 pa = ld4(e.pos, a);
+    const float4 la = e.lp[a];
     CSum<float> s;
-    s.add(static_cast<float>(pa.w) / e.vr[a].w * e.sig2d);
-    const int n = e.cnt[a];
-    for (int k = 0; k < n; ++k) {
-      const int b = e.nbr[static_cast<int64_t>(k) * e.N + a];
-      if (b >= e.nf) continue;
-      const double4 pb = ld4(e.pos, b);
-      const float3 d = sep(pa, pb);
-      const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
-      if (r2 >= e.support2) continue;
-      s.add(static_cast<float>(pb.w) / e.vr[b].w * (e.sig2d * shape(sqrtf(r2) * e.inv_h)));
-    }
+    s.add(e.vb[a].w * e.sig2d);
+    walk_row(e, a, [&](const uint32_t* ent) {
+      float part = 0.f;
+#pragma unroll
+      for (int j = 0; j < kBatch; ++j) {
+        const int b0 = ent[j] != 0xffffffffu ? static_cast<int>(ent[j] >> 5) : a;
+        const bool ok = ent[j] != 0xffffffffu && b0 < e.nf;
+        const int b = ok ? b0 : a;
+        const float4 lb = e.lp[b];
+        const float Vb = e.vb[b].w;
+        const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u]);
+        const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+        part += ok ? Vb * (e.sig2d * shape(radial(r2, e.inv_h).q)) : 0.f;
+      }
+      s.add(part);
+    });
     e.conc[a] = s.value();
   }
 }
 
-__global__ void k_conc_gradient(Dev e) {
+__global__ void __launch_bounds__(kBlock) k_conc_gradient(Dev e) {
   if (!e.flag[2]) return;
+  __shared__ float4 tab[27];
+  fill_offsets(tab, e.cellf);
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
-    const double4 pa = ld4(e.pos, a);
+    const float4 la = e.lp[a];
     const float ca = e.conc[a];
     CSum<float> gx, gy, gz;
-    const int n = e.cnt[a];
-    for (int k = 0; k < n; ++k) {
-      const int b = e.nbr[static_cast<int64_t>(k) * e.N + a];
-      if (b >= e.nf) continue;
-      const double4 pb = ld4(e.pos, b);
-      const float3 d = sep(pa, pb);
-      const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
-      if (r2 >= e.support2) continue;
-      const float r = sqrtf(r2);
-      const float gs = e.sig2d * dshape(r * e.inv_h) / (e.h * (r > 1e-12f ? r : 1e-12f));
-      const float c = static_cast<float>(pb.w) / e.vr[b].w * (e.conc[b] - ca) * gs;
-      gx.add(c * d.x);
-      gy.add(c * d.y);
-      gz.add(c * d.z);
-    }
+    walk_row(e, a, [&](const uint32_t* ent) {
+      float px = 0.f, py = 0.f, pz = 0.f;
+#pragma unroll
+      for (int j = 0; j < kBatch; ++j) {
+        const int b0 = ent[j] != 0xffffffffu ? static_cast<int>(ent[j] >> 5) : a;
+        const bool ok = ent[j] != 0xffffffffu && b0 < e.nf;
+        const int b = ok ? b0 : a;
+        const float4 lb = e.lp[b];
+        const float Vb = e.vb[b].w;
+        const float cb = e.conc[b];
+        const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u]);
+        const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+        const Radial R = radial(r2, e.inv_h);
+        const float gs = e.sig2d * dshape(R.q) * e.inv_h * R.inv_r;
+        const float c = ok ? Vb * (cb - ca) * gs : 0.f;
+        px += c * d.x;
+        py += c * d.y;
+        pz += c * d.z;
+      }
+      gx.add(px);
+      gy.add(py);
+      gz.add(pz);
+    });
     e.gradc[a] = make_float4(gx.value(), gy.value(), gz.value(), 0.f);
   }
 }
-
 __device__ __forceinline__ uint32_t fkey(float v) {
   uint32_t b = __float_as_uint(v);
   return (b >> 31) ? ~b : (b | 0x80000000u);
@@ -711,6 +835,7 @@ __global__ void k_shift_apply(Dev e) {
     x.y += sy;
     x.z += sz;
     st4(e.pos, a, x);
+    e.lp[a] = local_of(e, e.home[a], x.x, x.y, x.z, x.w);
     const double4 an = ld4(e.anchor, a);
     const double ex = x.x - an.x, ey = x.y - an.y, ez = x.z - an.z;
     dmax = fmax(dmax, sqrt(ex * ex + ey * ey + ez * ez));
@@ -749,7 +874,11 @@ __global__ void k_wall_keys(Dev e, const double* __restrict__ w) {
 __global__ void k_wall_place(Dev e, const double* __restrict__ w) {
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < e.nw; s += gridDim.x * blockDim.x) {
     const int o = e.vals[s];
-    st4(e.pos, e.nf + s, make_double4(w[3 * o], w[3 * o + 1], w[3 * o + 2], static_cast<double>(e.wall_mass)));
+    const int key = static_cast<int>(e.keys[s]);
+    const double m = static_cast<double>(e.wall_mass);
+    st4(e.pos, e.nf + s, make_double4(w[3 * o], w[3 * o + 1], w[3 * o + 2], m));
+    e.home[e.nf + s] = key;
+    e.lp[e.nf + s] = local_of(e, key, w[3 * o], w[3 * o + 1], w[3 * o + 2], m);
     e.wall_id[s] = o;
     if (o >= e.nw - e.nob) e.ob_rows[o - (e.nw - e.nob)] = e.nf + s;
   }
@@ -762,7 +891,7 @@ __global__ void k_read(Dev e, double* __restrict__ x, double* __restrict__ v, do
     const double4 xa = ld4(e.pos, a), va = ld4(e.vel, a);
     if (x) { x[3 * o] = xa.x; x[3 * o + 1] = xa.y; x[3 * o + 2] = xa.z; }
     if (v) { v[3 * o] = va.x; v[3 * o + 1] = va.y; v[3 * o + 2] = va.z; }
-    if (rho) rho[o] = e.vr[a].w;
+    if (rho) rho[o] = e.rho[a];
     if (p) p[o] = e.pr[a];
   }
 }
@@ -800,7 +929,7 @@ Plan make_plan(const tsph_engine_params& p) {
   q.ncy = static_cast<int>(std::ceil((p.grid_hi[1] - p.grid_lo[1]) / q.cell)) + 1;
   q.ncz = static_cast<int>(std::ceil((p.grid_hi[2] - p.grid_lo[2]) / q.cell)) + 1;
   q.ncells = static_cast<int64_t>(q.ncx) * q.ncy * q.ncz;
-  q.nblocks_int = static_cast<int>(grid_for(p.n_fluid, kBlock));
+  q.nblocks_int = static_cast<int>(grid_for(p.n_fluid, kBlock, kMaxFinalBlocks));
   q.nblocks_ob = static_cast<int>(grid_for(std::max<int64_t>(p.n_obstacle, 1), kBlock));
   return q;
 }
@@ -819,16 +948,19 @@ size_t carve(const tsph_engine_params& p, const Plan& q, Dev* d, char* base, cha
   t.pos = static_cast<double4*>(take(N * sizeof(double4)));
   t.vel = static_cast<double4*>(take(nf * sizeof(double4)));
   t.anchor = static_cast<double4*>(take(nf * sizeof(double4)));
+  t.lp = static_cast<float4*>(take(N * sizeof(float4)));
+  t.home = static_cast<int32_t*>(take(N * sizeof(int32_t)));
   t.id = static_cast<int32_t*>(take(nf * sizeof(int32_t)));
   t.wall_id = static_cast<int32_t*>(take(std::max<int64_t>(p.n_wall, 1) * sizeof(int32_t)));
-  t.vr = static_cast<float4*>(take(N * sizeof(float4)));
+  t.vb = static_cast<float4*>(take(N * sizeof(float4)));
   t.pr = static_cast<float*>(take(N * sizeof(float)));
+  t.rho = static_cast<float*>(take(N * sizeof(float)));
   t.pq = static_cast<float*>(take(N * sizeof(float)));
-  t.rho_s = static_cast<float*>(take(nf * sizeof(float)));
+  t.rs = static_cast<float2*>(take(nf * sizeof(float2)));
   t.acc = static_cast<float4*>(take(nf * sizeof(float4)));
   t.conc = static_cast<float*>(take(nf * sizeof(float)));
   t.gradc = static_cast<float4*>(take(nf * sizeof(float4)));
-  t.nbr = static_cast<int32_t*>(take(static_cast<size_t>(p.max_neighbors) * N * sizeof(int32_t)));
+  t.nbr = static_cast<uint32_t*>(take(static_cast<size_t>(p.max_neighbors) * N * sizeof(uint32_t)));
   t.cnt = static_cast<int32_t*>(take(N * sizeof(int32_t)));
   t.ob_rows = static_cast<int32_t*>(take(std::max<int64_t>(p.n_obstacle, 1) * sizeof(int32_t)));
   t.fstart = static_cast<int32_t*>(take(q.ncells * sizeof(int32_t)));
@@ -841,7 +973,6 @@ size_t carve(const tsph_engine_params& p, const Plan& q, Dev* d, char* base, cha
   t.vals_tmp = static_cast<int32_t*>(take(nsort * sizeof(int32_t)));
   t.tmp4a = static_cast<double4*>(take(nf * sizeof(double4)));
   t.tmp4b = static_cast<double4*>(take(nf * sizeof(double4)));
-  t.tmp4c = nullptr;
   t.tmp_id = static_cast<int32_t*>(take(nf * sizeof(int32_t)));
   t.flag = static_cast<int*>(take(16 * sizeof(int)));
   t.maxbits = static_cast<unsigned long long*>(take(8 * sizeof(unsigned long long)));
@@ -951,8 +1082,9 @@ int tsph_engine_create(const tsph_engine_params* prm, void* arena, int64_t arena
                        const double* v, const double* mass, const double* wall, tsph_stream stream,
                        tsph_engine** out) {
   if (!prm || !out || !arena) return TSPH_ERR_ARG;
+  // row entries pack the neighbour index into 27 bits
   if (prm->n_fluid <= 0 || prm->n_wall < 0 || prm->n_obstacle < 0 || prm->n_obstacle > prm->n_wall ||
-      prm->n_fluid + prm->n_wall >= (int64_t(1) << 31) || prm->max_neighbors <= 0 || prm->diag_ring <= 0)
+      prm->n_fluid + prm->n_wall >= (int64_t(1) << 27) || prm->max_neighbors <= 0 || prm->diag_ring <= 0)
     return TSPH_ERR_ARG;
   if (arena_bytes < tsph_engine_bytes(prm)) return TSPH_ERR_WORKSPACE;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
@@ -982,6 +1114,7 @@ int tsph_engine_create(const tsph_engine_params* prm, void* arena, int64_t arena
     d.ob_hi[k] = prm->ob_hi[k];
   }
   d.cell = q.cell;
+  d.cellf = static_cast<float>(q.cell);
   const double rc = 2.0 * prm->h + prm->skin;
   d.rc2 = rc * rc;
   d.skin_half = 0.5 * prm->skin;
