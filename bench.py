@@ -50,6 +50,12 @@ def parse():
     ap.add_argument("--shift-every", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=6)
+    ap.add_argument("--ensemble-cases", type=int, default=256)
+    ap.add_argument("--ensemble-steps", type=int, default=100)
+    ap.add_argument("--plain-steps", type=int, default=20)
+    ap.add_argument("--serve-requests", type=int, default=32)
+    ap.add_argument("--serve-time-scale", type=float, default=0.01)
+    ap.add_argument("--serve-budget-gb", type=float, default=150.0)
     return ap.parse_args()
 
 
@@ -151,6 +157,50 @@ def cpu_baseline(dx, steps, shift_every):
                                                 0.05 * cfg.sound_speed))
     elapsed = time.perf_counter() - t0
     return n * steps / elapsed, n, elapsed
+
+
+def ensemble_leg(args, dev):
+    """Batched droplet ensemble vs the same cases one at a time (both device
+    timed); block size and skin chosen by the autotuner on a 32-case sample."""
+    from tensorsph_b200 import ensemble as en
+    draws = en.draw_ensemble(args.ensemble_cases, seed=0)
+    tune = en.autotune(draws[:32], steps=20, warmup=5, device=dev)
+    best = tune["best"]
+    specs = en.ensemble_specs(draws, skin_factor=best["skin_factor"])
+    batched = en.run_batched(specs, args.ensemble_steps, block=best["block"], device=dev)
+    plain = en.run_plain(specs, args.plain_steps, block=128, device=dev)
+    return {"workload": f"{len(specs)} independent 2-D droplet impacts (R~U[0.02,0.08] m, dx=R/20, "
+                        "depth~U[2R,6R], width 8R, U~U[1,5] m/s, seed 0), surface tension off",
+            "fluid_particles": batched["fluid"],
+            "batched_updates_per_s": batched["updates_per_s"],
+            "batched_ms_per_step": 1e3 * batched["seconds"] / batched["steps"],
+            "plain_updates_per_s": plain["updates_per_s"],
+            "speedup_vs_plain": batched["updates_per_s"] / plain["updates_per_s"],
+            "kernels_per_step": batched["kernels_per_step"], "failed_cases": batched["failed_cases"],
+            "autotune": {"best": best, "trials": len(tune["trials"])},
+            "steps": {"batched": batched["steps"], "plain_per_case": plain["steps"]}}
+
+
+def serving_leg(args, dev):
+    """Continuous-batching server vs serial single-case runs of one seeded stream."""
+    from tensorsph_b200 import serving as sv
+    reqs = sv.request_stream(args.serve_requests, rate=20.0, seed=0,
+                             time_scale=args.serve_time_scale)
+    srv = sv.Server(budget_bytes=args.serve_budget_gb * 1e9, device=dev)
+    served = srv.serve(reqs)
+    engine_gb = srv.engine_bytes / 1e9
+    srv.close()
+    serial = sv.run_serial(sv.request_stream(args.serve_requests, rate=20.0, seed=0,
+                                             time_scale=args.serve_time_scale), device=dev)
+    return {"workload": f"{args.serve_requests} requests, Poisson 20/s (seed 0), types "
+                        f"{list(sv.CASE_TYPES)}, fluid log-uniform [1e3, 2e6], simulated time "
+                        f"U[0.1, 1.0] s x {args.serve_time_scale:g}",
+            "budget_gb": args.serve_budget_gb, "engine_gb": engine_gb,
+            "batched": {"updates_per_s": served["updates_per_s"], "wall_s": served["wall_s"],
+                        "latency_s": served["latency_s"]},
+            "serial": {"updates_per_s": serial["updates_per_s"], "wall_s": serial["wall_s"],
+                       "latency_s": serial["latency_s"]},
+            "throughput_vs_serial": served["updates_per_s"] / serial["updates_per_s"]}
 
 
 def main():
@@ -281,6 +331,18 @@ def main():
                "sample": f"{args.cpu_sample_steps} steps of the dx={4.0 * args.dx:g} rung "
                          f"({n_cpu} fluid), {t_cpu:.1f} s"}
 
+    extra = {}
+    if rank == 0 and world == 1:
+        for name, leg, on in (("ensemble", ensemble_leg, args.ensemble_cases > 0),
+                              ("serving", serving_leg, args.serve_requests > 0)):
+            if not on:
+                continue
+            try:
+                extra[name] = leg(args, dev)
+            except Exception as exc:  # reported, never hides the headline
+                extra[name] = {"error": f"{type(exc).__name__}: {exc}"}
+            torch.cuda.empty_cache()
+
     if rank == 0:
         line = {
             "metric": "particle-updates/s", "value": value, "unit": "fluid particle-updates/s",
@@ -311,6 +373,7 @@ def main():
                        "last_rho_max": float(diag[0]), "last_speed_max": float(diag[1]),
                        "kernels_per_step": kernels_per_step},
         }
+        line.update(extra)
         print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()

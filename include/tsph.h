@@ -255,43 +255,65 @@ int tsph_euler_clamp(const tsph_clamp_params* prm, void* pos, void* vel, const v
                      double dt, int64_t* counters, tsph_stream stream);
 
 /* ------------------------------------------------------------------------ */
-/* Device-resident 3-D dam-break engine (one GPU, one CUDA graph per step). */
-/* Replaces the step loop of dam_break_3d.py:623-709 and of                  */
-/* kleefsman_obstacle_3d.py:644-706: PairListCache.get + rhs_3d(return_wall_ */
-/* force) + semi-implicit Euler + box and obstacle clamps, with the obstacle */
-/* force summed over the obstacle rows, and optionally the Lind shift of     */
-/* particle_shifting.py:166-224 every shift_every steps (as dam_break.py:    */
-/* 424-433 does in 2-D).  FP64 positions, velocities and meters; FP32 pair   */
-/* arithmetic with compensated sums.                                          */
+/* Multi-case device engine (one GPU, one CUDA graph per step for all cases). */
+/* Replaces the step loops of dam_break.py:374-440 (2-D), dam_break_3d.py:    */
+/* 623-709 and kleefsman_obstacle_3d.py:644-706 (3-D): PairListCache.get +   */
+/* rhs / rhs_3d(return_wall_force) + semi-implicit Euler + box and obstacle  */
+/* clamps, with the obstacle force summed over the obstacle rows, and for a  */
+/* batch of one case optionally the Lind shift of particle_shifting.py:      */
+/* 166-224 every shift_every steps (dam_break.py:424-433).  FP64 positions,  */
+/* velocities and meters; FP32 pair arithmetic with compensated sums.        */
+/*                                                                            */
+/* An engine is a fixed arena sized by its capacities; cases are admitted    */
+/* and retired while it runs, each with its own physics, grid, time step and  */
+/* meters, and each evolves bit for bit the same whatever else is batched.   */
+/* All calls on one engine must use one stream.                              */
 /* ------------------------------------------------------------------------ */
 typedef struct {
-  int64_t n_fluid, n_wall, n_obstacle; /* obstacle rows are the last n_obstacle walls */
-  int64_t max_neighbors;               /* neighbour-row capacity (overflow -> status) */
-  int64_t shift_every;                 /* 0 disables shifting                       */
-  int64_t diag_ring;                   /* rows kept in the per-step meter ring      */
-  int64_t has_obstacle;
-  double dx, h, rho0, sound_speed, gamma, gravity, viscosity, wall_friction;
-  double diffusion_scale;              /* 2 delta c0 h (Molteni); 0 disables         */
-  double dt, wall_mass, skin;          /* skin = pair_skin_factor * h               */
-  double box_hi[3];                    /* fluid clamp box [0, box_hi]               */
-  double tolerance;                    /* escape tolerance, 0.25 dx                 */
-  double ob_lo[3], ob_hi[3], ob_eps;   /* obstacle box and exit offset              */
-  double shift_strength, shift_limit, shift_free_surface, shift_vref_floor;
-  double grid_lo[3], grid_hi[3];       /* bounds of every particle (cell grid)      */
+  int64_t max_fluid, max_wall, max_obstacle; /* particle capacities (sum < 2^27)   */
+  int64_t max_cells;                          /* cell capacity over all cases       */
+  int64_t max_cases;                          /* case slots                         */
+  int64_t max_neighbors;                      /* neighbour-row capacity             */
+  int64_t diag_ring;                          /* meter rows kept per case           */
 } tsph_engine_params;
+
+typedef struct {
+  int64_t dim;                         /* 2 or 3 (2-D: z = 0, one cell layer)        */
+  int64_t n_fluid, n_wall, n_obstacle; /* obstacle rows are the last n_obstacle walls */
+  int64_t shift_every;                 /* 0 disables shifting (batch of one only)    */
+  int64_t has_obstacle;                /* 3-D box obstacle clamp                     */
+  double h, rho0, sound_speed, gamma, gravity, viscosity, wall_friction;
+  double diffusion_scale;              /* 2 delta c0 h (Molteni); 0 disables         */
+  double dt, wall_mass, skin;          /* skin = pair_skin_factor * h                */
+  double box_hi[3];                    /* fluid clamp box [0, box_hi]                */
+  double tolerance;                    /* escape tolerance, 0.25 dx                  */
+  double ob_lo[3], ob_hi[3], ob_eps;   /* obstacle box and exit offset               */
+  double shift_strength, shift_limit, shift_free_surface, shift_vref_floor;
+  double grid_lo[3], grid_hi[3];       /* bounds every particle stays in (cell grid) */
+} tsph_case_params;
 
 typedef struct tsph_engine tsph_engine; /* opaque host handle */
 
 int64_t tsph_engine_bytes(const tsph_engine_params* prm);
-/* Build the engine in `arena` (tsph_engine_bytes bytes of device memory) from
- * device arrays x, v (n_fluid, 3) FP64, mass (n_fluid) FP64 and wall
- * (n_wall, 3) FP64; synchronises once.  The handle owns no device memory. */
+/* Cells the case's grid takes from max_cells (-1 for invalid parameters). */
+int64_t tsph_engine_case_cells(const tsph_case_params* prm);
+/* Build an empty engine in `arena` (tsph_engine_bytes bytes of device
+ * memory); synchronises once.  The handle owns no device memory. */
 int tsph_engine_create(const tsph_engine_params* prm, void* arena, int64_t arena_bytes,
-                       const double* x, const double* v, const double* mass, const double* wall,
                        tsph_stream stream, tsph_engine** out);
-/* Advance `steps` steps: the first call captures one step as a CUDA graph on
- * `stream` (which must not be the legacy default stream); later calls replay
- * it.  No host synchronisation. */
+/* Admit a case from device arrays x, v (n_fluid, dim) FP64, mass (n_fluid)
+ * FP64 and wall (n_wall, dim) FP64; *case_id receives its slot.  Returns
+ * TSPH_ERR_CAPACITY when a capacity would be exceeded (nothing changes) and
+ * TSPH_ERR_UNSUPPORTED for a shifting case in a non-empty batch.
+ * Synchronises; the step graph is re-captured at the next step. */
+int tsph_engine_add_case(tsph_engine* engine, const tsph_case_params* prm, const double* x,
+                         const double* v, const double* mass, const double* wall,
+                         tsph_stream stream, int64_t* case_id);
+/* Retire a case and compact the others (synchronises). */
+int tsph_engine_remove_case(tsph_engine* engine, int64_t case_id, tsph_stream stream);
+/* Advance every case `steps` steps: the first call after a change of the
+ * batch captures one step as a CUDA graph on `stream` (which must not be the
+ * legacy default stream); later calls replay it.  No host synchronisation. */
 int tsph_engine_step(tsph_engine* engine, int64_t steps, tsph_stream stream);
 /* Same steps launched kernel by kernel (no graph). */
 int tsph_engine_step_eager(tsph_engine* engine, int64_t steps, tsph_stream stream);
@@ -304,19 +326,26 @@ int tsph_engine_step_timed(tsph_engine* engine, tsph_stream stream, float* stage
                            int64_t* stages);
 /* Number of kernel nodes in the captured step graph (host; after a step). */
 int tsph_engine_graph_kernels(tsph_engine* engine, int64_t* kernels);
-/* Fluid state in the caller's original particle order (device, nullable). */
-int tsph_engine_read(tsph_engine* engine, double* x, double* v, double* rho, double* p,
-                     tsph_stream stream);
-/* Copy `count` per-step meter rows (16 doubles each: max rho, max |v|, front x,
- * obstacle force xyz, kinetic and potential energy, escapes, clamps, rebuilds,
- * longest row, step, status, obstacle impulse x, c_ref) starting at step
- * `first` into `out` (device). */
-int tsph_engine_diag(tsph_engine* engine, double* out, int64_t first, int64_t count,
-                     tsph_stream stream);
-/* Counters (escapes, clamps, rebuilds, steps, longest row, -, status, -) to the
- * host; synchronises.  Returns TSPH_ERR_STATE on a non-finite state and
- * TSPH_ERR_CAPACITY when a neighbour row overflowed. */
-int tsph_engine_status(tsph_engine* engine, int64_t* counters, tsph_stream stream);
+/* Fluid state of one case in its original particle order, (n_fluid, dim)
+ * FP64 (device, nullable). */
+int tsph_engine_read(tsph_engine* engine, int64_t case_id, double* x, double* v, double* rho,
+                     double* p, tsph_stream stream);
+/* Copy `count` per-step meter rows of one case (16 doubles each: max rho,
+ * max |v|, front x, obstacle force xyz, kinetic and potential energy,
+ * escapes, clamps, rebuilds, longest row, step, status, obstacle impulse x,
+ * c_ref) starting at its step `first` into `out` (device). */
+int tsph_engine_diag(tsph_engine* engine, int64_t case_id, double* out, int64_t first,
+                     int64_t count, tsph_stream stream);
+/* Counters of one case (escapes, clamps, rebuilds, steps, longest row, -,
+ * status, -) to the host; synchronises.  Returns TSPH_ERR_STATE on a
+ * non-finite state and TSPH_ERR_CAPACITY when a neighbour row overflowed. */
+int tsph_engine_status(tsph_engine* engine, int64_t case_id, int64_t* counters,
+                       tsph_stream stream);
+/* Threads per block of the pair kernels: 64, 128 (default) or 256.  A tuning
+ * knob (results do not depend on it); the step graph is re-captured. */
+int tsph_engine_set_block(tsph_engine* engine, int64_t threads);
+/* Occupancy (fluid rows, wall rows, obstacle rows, cells, cases) (host). */
+int tsph_engine_usage(const tsph_engine* engine, int64_t* usage);
 int tsph_engine_destroy(tsph_engine* engine);
 
 #ifdef __cplusplus

@@ -80,9 +80,14 @@ class ClampParams(ctypes.Structure):
 
 
 class EngineParams(ctypes.Structure):
-    _fields_ = [(k, c_int64) for k in ("n_fluid", "n_wall", "n_obstacle", "max_neighbors",
-                                       "shift_every", "diag_ring", "has_obstacle")] + \
-               [(k, c_double) for k in ("dx", "h", "rho0", "sound_speed", "gamma", "gravity",
+    _fields_ = [(k, c_int64) for k in ("max_fluid", "max_wall", "max_obstacle", "max_cells",
+                                       "max_cases", "max_neighbors", "diag_ring")]
+
+
+class CaseParams(ctypes.Structure):
+    _fields_ = [(k, c_int64) for k in ("dim", "n_fluid", "n_wall", "n_obstacle", "shift_every",
+                                       "has_obstacle")] + \
+               [(k, c_double) for k in ("h", "rho0", "sound_speed", "gamma", "gravity",
                                         "viscosity", "wall_friction", "diffusion_scale", "dt",
                                         "wall_mass", "skin")] + \
                [("box_hi", c_double * 3), ("tolerance", c_double), ("ob_lo", c_double * 3),
@@ -130,16 +135,22 @@ _SIGNATURES = {
     "tsph_euler_clamp": (c_int, [POINTER(ClampParams), c_void_p, c_void_p, c_void_p, c_double,
                                  c_void_p, c_void_p]),
     "tsph_engine_bytes": (c_int64, [POINTER(EngineParams)]),
-    "tsph_engine_create": (c_int, [POINTER(EngineParams), c_void_p, c_int64, c_void_p, c_void_p,
-                                   c_void_p, c_void_p, c_void_p, POINTER(c_void_p)]),
+    "tsph_engine_case_cells": (c_int64, [POINTER(CaseParams)]),
+    "tsph_engine_create": (c_int, [POINTER(EngineParams), c_void_p, c_int64, c_void_p, c_void_p]),
+    "tsph_engine_add_case": (c_int, [c_void_p, POINTER(CaseParams), c_void_p, c_void_p, c_void_p,
+                                     c_void_p, c_void_p, POINTER(c_int64)]),
+    "tsph_engine_remove_case": (c_int, [c_void_p, c_int64, c_void_p]),
     "tsph_engine_step": (c_int, [c_void_p, c_int64, c_void_p]),
     "tsph_engine_step_eager": (c_int, [c_void_p, c_int64, c_void_p]),
     "tsph_engine_step_timed": (c_int, [c_void_p, c_void_p, POINTER(ctypes.c_float),
                                        POINTER(c_int64)]),
     "tsph_engine_graph_kernels": (c_int, [c_void_p, POINTER(c_int64)]),
-    "tsph_engine_read": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
-    "tsph_engine_diag": (c_int, [c_void_p, c_void_p, c_int64, c_int64, c_void_p]),
-    "tsph_engine_status": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "tsph_engine_read": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p,
+                                 c_void_p]),
+    "tsph_engine_diag": (c_int, [c_void_p, c_int64, c_void_p, c_int64, c_int64, c_void_p]),
+    "tsph_engine_status": (c_int, [c_void_p, c_int64, c_void_p, c_void_p]),
+    "tsph_engine_usage": (c_int, [c_void_p, c_void_p]),
+    "tsph_engine_set_block": (c_int, [c_void_p, c_int64]),
     "tsph_engine_destroy": (c_int, [c_void_p]),
 }
 

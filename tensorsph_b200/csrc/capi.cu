@@ -3,7 +3,7 @@
 
 extern "C" {
 
-int tsph_abi_version(void) { return 1; }
+int tsph_abi_version(void) { return 2; }
 
 const char* tsph_status_string(int code) {
   switch (code) {

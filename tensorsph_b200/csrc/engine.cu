@@ -1,63 +1,93 @@
-// Device-resident 3-D dam-break engine: the time loop of dam_break_3d.py:623-709
-// (with the obstacle wall force of kleefsman_obstacle_3d.py:644-706 and the
-// optional Lind shift of particle_shifting.py:166-224), one CUDA graph per step.
+// Multi-case device engine: the WCSPH time loop of dam_break.py:374-440 (2-D),
+// dam_break_3d.py:623-709 and kleefsman_obstacle_3d.py:644-706 (3-D) for any
+// number of independent cases packed into one particle set and advanced by one
+// CUDA graph per step; a single-case batch can add the Lind shift of
+// particle_shifting.py:166-224.
 //
-// Layout (one caller-provided arena; particles in cell order, fluid rows
-// [0, nf) re-sorted at every rebuild, wall rows [nf, N) sorted once):
-//   pos  double4[N]  x, y, z, mass -- FP64 state (integration, list builds)
-//   lp   float4[N]   position relative to the particle's home cell + mass;
-//                    the home cell is its cell at the last rebuild
-//   vb   float4[N]   FP32 velocity + volume m/rho (walls: 0 + m/rho_w)
-//   pr, rho, pq      float[N] pressure, density, p/rho^2
-//   nbr  uint32[maxnb * N]  k-major rows (thread a reads nbr[k*N + a],
-//                    coalesced); entry = neighbour << 5 | cell-offset code
-// A pair separation is (l_a - l_b) - (c_b - c_a) * cell: exact to the FP32
-// rounding of the two local coordinates (~1e-9 m here), so the FP32 pair
-// arithmetic loses nothing against the FP64 positions.
+// Packing.  Fluid rows [0, nf) and wall rows [NF, NF + nw) (NF = fluid
+// capacity) hold the cases as contiguous blocks in case order, each block in
+// the cell order of its own grid.  Every case has its own parameters (h, c0,
+// dt, box, obstacle ...), its own cell grid and a range [key_off, key_off +
+// ncells) of one global cell-key space, so one radix sort orders every block
+// at once and no cell is shared by two cases.  A 2-D case is a 3-D case with
+// z = 0 and one cell layer.
 //
-// Gather loops take kBatch neighbours per iteration without branches, so
-// several independent loads are in flight per thread; each batch's partial
-// sums enter a Neumaier-compensated FP32 accumulator.
+// Per particle (sorted order):
+//   pos  double4  x, y, z, mass -- FP64 state (integration, list builds)
+//   lp   float4   position relative to its home cell (its cell at its case's
+//                 last rebuild) + mass; a pair separation is
+//                 (l_a - l_b) - (c_b - c_a) * cell, exact to the FP32 rounding
+//                 of the two local coordinates
+//   vb   float4   FP32 velocity + volume m/rho;  pr, rho, pq = p/rho^2
+//   nbr  uint32[maxnb][rows] k-major rows (thread a reads nbr[k*rows + a]),
+//        entry = row index << 5 | cell-offset code (dx+1)*9 + (dy+1)*3 + (dz+1)
+// Each case rebuilds its rows only when its own particles leave its own skin
+// and the order of its block depends on its own particles only, so a case
+// evolves bit for bit the same alone or batched with others.  Retiring a case
+// moves the later blocks down and shifts their row entries and cell keys.
 //
 // Step (fixed launch sequence, graph-captured):
-//   check/rebuild  skin test -> (cell keys, radix sort, permute, cell table, rows)
+//   per-case skin test -> [keys, radix sort, permute, cell table, rows]
 //   E1 density -> E2 diffusion + Tait -> E3 Adami walls -> E4 force
-//   E5 obstacle reaction -> E6 Euler + clamps + meters -> E7 finalize meters
-//   [check/rebuild -> S1 concentration -> S2 gradient -> Q select -> S3 shift]
-// Every rebuild kernel reads the device flag and returns at once when no
-// rebuild is due, so the branch costs a few empty launches, no host sync.
+//   E5 obstacle reaction -> E6 Euler + clamps + meters -> E7 per-case meter rows
+//   [one shifting case: skin test -> S1 concentration -> S2 gradient ->
+//    Q 95th-percentile select -> S3 shift]
+// Rebuild kernels read a device flag and return at once when no case is due.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include "common.cuh"
 
 namespace tsph {
 namespace {
 
-constexpr int kBlock = 128;
+constexpr int kBlock = 128;     // default threads per block of the pair kernels
+constexpr int kMaxBlock = 256;  // largest block the kernels are built for
 constexpr int kDiag = 16;
 constexpr int kBatch = 4;
-constexpr int kMaxFinalBlocks = 148 * 8;
+constexpr uint32_t kPad = 0xffffffffu;
+constexpr int64_t kMaxRows = (int64_t(1) << 27) - 1;  // row index in 27 bits
+
+struct CaseDev {
+  double origin[3];
+  double cell, rc2, skin_half;
+  double dt, gravity, box_hi[3], tol, ob_lo[3], ob_hi[3], ob_eps;
+  double shift_strength_h_dt, shift_cap, shift_fs, vref_floor;
+  int ncx, ncy, ncz, key_off;
+  int fluid_begin, n_fluid, wall_begin, n_wall;
+  int ob_begin, n_ob, has_ob, shift_every;
+  float cellf, inv_h, sigma, sig2d, rho0, bulk, gamma, inv_gamma;
+  float grav, nu2, nu2f, dscale, dtf, visc_eps, rho_floor, wall_mass;
+};
+
+struct CaseCtl {
+  int rebuild, first, shift_now, shift_done;
+  int status, active, pad0, pad1;
+  unsigned long long disp[2];  // max |x - anchor| (double bits): [0] Euler, [1] shift
+  unsigned long long rho_max, speed_max, front_max, row_max;
+  double ke, pe;
+  double force[3], impulse[3];
+  unsigned long long escapes, clamps, rebuilds, steps;
+  double cref[2];  // [0] c_ref of the last shift, [1] max speed of the step
+};
 
 struct Dev {
-  int nf, nw, N, nob, maxnb, shift_every, diag_ring;
-  int ncx, ncy, ncz;
-  double origin[3], cell, rc2, skin_half;
-  double dt, box_hi[3], tol, ob_lo[3], ob_hi[3], ob_eps;
-  int has_ob;
-  double gravity;
-  float cellf, h, inv_h, sigma, sig2d, support2, rho0, bulk, gamma, inv_gamma, grav, nu2, nu2f, dscale,
-      dtf, visc_eps, rho_floor, wall_mass;
-  double shift_strength_h_dt, shift_cap, shift_fs, vref_floor;
-  // arrays
+  int nf, nw, NF, n_slots, maxnb, diag_ring, n_ob, shift_slot, one_slot, pad_;
+  int64_t rows;  // NF + wall capacity: the row stride of nbr
+  CaseDev one;   // the case of a batch of one (kernel-parameter copy)
+  const CaseDev* cases;
+  CaseCtl* ctl;
+  double* diag;
   double4* pos;
   double4* vel;
   double4* anchor;
   float4* lp;
   int32_t* home;
   int32_t* id;
-  int32_t* wall_id;
+  int32_t* cid;
   float4* vb;
   float* pr;
   float* rho;
@@ -80,20 +110,14 @@ struct Dev {
   double4* tmp4a;
   double4* tmp4b;
   int32_t* tmp_id;
-  // control words
-  int* flag;         // [0] rebuild now, [1] first step, [2] shift this step, [3] shift done
-  unsigned long long* maxbits;  // [0] disp (integrate), [1] disp (shift)
-  int* status;       // bit 0: neighbour row overflow, bit 1: non-finite state
-  long long* counters;  // [0] escapes [1] clamps [2] rebuilds [3] step [4] max row [5] select k
-  double* partials;  // per-block sums: [blk*8 + 0..7]
-  int nblocks_int;   // blocks of the integrate kernel
-  int nblocks_ob;
-  double* impulse;   // 3
-  double* diag;      // diag_ring * kDiag
-  unsigned int* hist;        // 256
-  unsigned long long* sel;   // [0] prefix [1] value lo bits [2] value hi bits
-  double* cref;      // [0] c_ref, [1] max speed of the step
+  int* any_rebuild;
+  int* status;
+  unsigned int* hist;
+  unsigned long long* sel;
+  long long* sel_k;
 };
+
+// ------------------------------------------------------------- helpers ---
 
 __device__ __forceinline__ float shape(float q) {
   const float t = 2.f - q;
@@ -108,130 +132,160 @@ __device__ __forceinline__ float dshape(float q) {
   return q < 1.f ? near : (q < 2.f ? far : 0.f);
 }
 
-__device__ __forceinline__ double4 ld4(const double4* p, int i) {
+// q = r / h and 1/r from r^2 with one reciprocal square root (1/r = 0 at
+// r = 0, where f'(0) = 0), so that grad_a W = d * sigma f'(q) / (h r) needs no
+// division.
+struct Radial {
+  float q, inv_r;
+};
+__device__ __forceinline__ Radial radial(float r2, float inv_h) {
+  Radial o;
+  o.inv_r = r2 > 1e-24f ? rsqrtf(r2) : 0.f;
+  o.q = r2 * o.inv_r * inv_h;
+  return o;
+}
+
+__device__ __forceinline__ double4 ld4(const double4* p, int64_t i) {
   const double2* q = reinterpret_cast<const double2*>(p + i);
   double2 a = q[0], b = q[1];
   return make_double4(a.x, a.y, b.x, b.y);
 }
 
-__device__ __forceinline__ void st4(double4* p, int i, double4 v) {
+__device__ __forceinline__ void st4(double4* p, int64_t i, double4 v) {
   double2* q = reinterpret_cast<double2*>(p + i);
   q[0] = make_double2(v.x, v.y);
   q[1] = make_double2(v.z, v.w);
 }
 
-__device__ __forceinline__ int cell_of(const Dev& e, double x, double y, double z, int& cx, int& cy, int& cz) {
-  cx = static_cast<int>(floor((x - e.origin[0]) / e.cell));
-  cy = static_cast<int>(floor((y - e.origin[1]) / e.cell));
-  cz = static_cast<int>(floor((z - e.origin[2]) / e.cell));
-  cx = cx < 0 ? 0 : (cx >= e.ncx ? e.ncx - 1 : cx);
-  cy = cy < 0 ? 0 : (cy >= e.ncy ? e.ncy - 1 : cy);
-  cz = cz < 0 ? 0 : (cz >= e.ncz ? e.ncz - 1 : cz);
-  return (cx * e.ncy + cy) * e.ncz + cz;
+__device__ __forceinline__ int local_cell(const CaseDev& c, double x, double y, double z) {
+  int cx = static_cast<int>(floor((x - c.origin[0]) / c.cell));
+  int cy = static_cast<int>(floor((y - c.origin[1]) / c.cell));
+  int cz = static_cast<int>(floor((z - c.origin[2]) / c.cell));
+  cx = cx < 0 ? 0 : (cx >= c.ncx ? c.ncx - 1 : cx);
+  cy = cy < 0 ? 0 : (cy >= c.ncy ? c.ncy - 1 : cy);
+  cz = cz < 0 ? 0 : (cz >= c.ncz ? c.ncz - 1 : cz);
+  return (cx * c.ncy + cy) * c.ncz + cz;
 }
 
-// Position relative to the origin of cell `key`; the cell origin uses the
-// FP32-rounded cell size so that (c_a - c_b) * cellf is exact in FP32.
-__device__ __forceinline__ float4 local_of(const Dev& e, int key, double x, double y, double z, double m) {
-  const int cz = key % e.ncz;
-  const int cy = (key / e.ncz) % e.ncy;
-  const int cx = key / (e.ncz * e.ncy);
-  const double cs = static_cast<double>(e.cellf);
-  return make_float4(static_cast<float>(x - (e.origin[0] + cx * cs)),
-                     static_cast<float>(y - (e.origin[1] + cy * cs)),
-                     static_cast<float>(z - (e.origin[2] + cz * cs)), static_cast<float>(m));
+// Position relative to the origin of the case's cell `local_key`; the cell
+// origin uses the FP32-rounded cell size so that (c_b - c_a) * cellf is exact.
+__device__ __forceinline__ float4 local_of(const CaseDev& c, int local_key, double x, double y, double z,
+                                           double m) {
+  const int cz = local_key % c.ncz;
+  const int cy = (local_key / c.ncz) % c.ncy;
+  const int cx = local_key / (c.ncz * c.ncy);
+  const double cs = static_cast<double>(c.cellf);
+  return make_float4(static_cast<float>(x - (c.origin[0] + cx * cs)),
+                     static_cast<float>(y - (c.origin[1] + cy * cs)),
+                     static_cast<float>(z - (c.origin[2] + cz * cs)), static_cast<float>(m));
 }
 
-// Cell-offset table in shared memory: code = (dx+1)*9 + (dy+1)*3 + (dz+1)
-// for dx, dy, dz = c_b - c_a; entry = (c_b - c_a) * cell.
-__device__ __forceinline__ void fill_offsets(float4* tab, float cellf) {
+// Unit cell offsets (c_b - c_a) per entry code, in shared memory; the
+// separation is (l_a - l_b) - u * cell with u * cell exact, so one FMA per
+// axis gives the same bits as a subtraction of a precomputed offset.
+__device__ __forceinline__ void fill_units(float4* tab) {
   for (int c = threadIdx.x; c < 27; c += blockDim.x)
-    tab[c] = make_float4((c / 9 - 1) * cellf, ((c / 3) % 3 - 1) * cellf, (c % 3 - 1) * cellf, 0.f);
+    tab[c] = make_float4(static_cast<float>(c / 9 - 1), static_cast<float>((c / 3) % 3 - 1),
+                         static_cast<float>(c % 3 - 1), 0.f);
   __syncthreads();
+}
+
+__device__ __forceinline__ float3 sep(const float4& la, const float4& lb, const float4& u, float cellf) {
+  return make_float3(fmaf(-u.x, cellf, la.x - lb.x), fmaf(-u.y, cellf, la.y - lb.y),
+                     fmaf(-u.z, cellf, la.z - lb.z));
 }
 
 __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* p, double v) {
   if (v > 0.0) atomicMax(p, static_cast<unsigned long long>(__double_as_longlong(v)));
 }
 
-__device__ __forceinline__ float tait(const Dev& e, float rho) {
-  float ratio = rho / e.rho0;
+__device__ __forceinline__ float tait(float rho, float rho0, float bulk, float gamma) {
+  float ratio = rho / rho0;
   ratio = ratio > 0.01f ? ratio : 0.01f;
-  float p = e.bulk * (powf(ratio, e.gamma) - 1.f);
+  float p = bulk * (powf(ratio, gamma) - 1.f);
   return p > 0.f ? p : 0.f;
 }
 
-// Kernel arguments from r^2 with one reciprocal square root: q = r / h and
-// 1/r, so that gs = sigma f'(q) / (h r) needs no division (grad_a W = d * gs);
-// at r = 0, f'(0) = 0 and 1/r is taken as 0.
-struct Radial {
-  float r, q, inv_r;
-};
-__device__ __forceinline__ Radial radial(float r2, float inv_h) {
-  Radial o;
-  o.inv_r = r2 > 1e-24f ? rsqrtf(r2) : 0.f;
-  o.r = r2 * o.inv_r;
-  o.q = o.r * inv_h;
-  return o;
-}
-
-// separation x_a - x_b = (l_a - l_b) - (c_b - c_a) * cell for a neighbour
-// entry whose offset-table row is `off` = (c_b - c_a) * cell
-__device__ __forceinline__ float3 sep(const float4& la, const float4& lb, const float4& off) {
-  return make_float3((la.x - lb.x) - off.x, (la.y - lb.y) - off.y, (la.z - lb.z) - off.z);
-}
-
-// Walk row a in batches: `body(entry, j)` for j in batch; loads of the batch
-// are issued before any use.
+// Walk row a in batches of kBatch entries (padded with kPad); the loads of a
+// batch are all issued before any use.
 template <class Body>
-__device__ __forceinline__ void walk_row(const Dev& e, int a, Body&& body) {
+__device__ __forceinline__ void walk_row(const Dev& e, int64_t a, Body&& body) {
   const int n = e.cnt[a];
   const uint32_t* row = e.nbr + a;
   int k = 0;
   for (; k + kBatch <= n; k += kBatch) {
     uint32_t ent[kBatch];
 #pragma unroll
-    for (int j = 0; j < kBatch; ++j) ent[j] = row[static_cast<int64_t>(k + j) * e.N];
+    for (int j = 0; j < kBatch; ++j) ent[j] = row[static_cast<int64_t>(k + j) * e.rows];
     body(ent);
   }
   if (k < n) {
     uint32_t ent[kBatch];
 #pragma unroll
-    for (int j = 0; j < kBatch; ++j) {
-      // pad with a harmless self entry whose contribution is masked out
-      ent[j] = (k + j < n) ? row[static_cast<int64_t>(k + j) * e.N] : 0xffffffffu;
-    }
+    for (int j = 0; j < kBatch; ++j) ent[j] = (k + j < n) ? row[static_cast<int64_t>(k + j) * e.rows] : kPad;
     body(ent);
   }
 }
 
+// Block-wide sum or max of v, returned to every thread.
+template <bool kMax>
+__device__ __forceinline__ double block_reduce(double v, double* red) {
+  v = kMax ? warp_reduce_max(v) : warp_reduce_sum(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double r = red[0];
+  for (int k = 1; k < static_cast<int>(blockDim.x >> 5); ++k) r = kMax ? fmax(r, red[k]) : r + red[k];
+  __syncthreads();
+  return r;
+}
+
+// Parameters of the case of row a: from the kernel-parameter copy when the
+// batch holds one case (no dependent load), else from the case table.
+template <bool kOne>
+__device__ __forceinline__ const CaseDev& case_of(const Dev& e, int64_t a) {
+  if (kOne) return e.one;
+  return e.cases[e.cid[a]];
+}
+
 // ------------------------------------------------------------ rebuild ---
 
-__global__ void k_check(Dev e) {
-  if (threadIdx.x || blockIdx.x) return;
-  const double d0 = __longlong_as_double(static_cast<long long>(e.maxbits[0]));
-  const double d1 = __longlong_as_double(static_cast<long long>(e.maxbits[1]));
-  const double d = e.flag[3] ? d1 : d0;
-  const int go = e.flag[1] || d > e.skin_half;
-  e.flag[0] = go;
-  if (go) {
-    e.counters[2] += 1;
-    e.flag[1] = 0;
+__global__ void k_check(Dev e, int shift_pass) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= e.n_slots) return;
+  CaseCtl& t = e.ctl[c];
+  if (!t.active) {
+    t.rebuild = 0;
+    return;
   }
+  const double d = __longlong_as_double(static_cast<long long>(t.shift_done ? t.disp[1] : t.disp[0]));
+  const int go = t.first || d > e.cases[c].skin_half;
+  t.rebuild = go;
+  if (go) {
+    t.rebuilds += 1;
+    t.first = 0;
+    atomicOr(e.any_rebuild, 1);
+  }
+  (void)shift_pass;
 }
 
 __global__ void k_keys(Dev e) {
-  if (!e.flag[0]) return;
+  if (!*e.any_rebuild) return;
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
-    const double4 p = ld4(e.pos, a);
-    int cx, cy, cz;
-    e.keys[a] = static_cast<uint64_t>(cell_of(e, p.x, p.y, p.z, cx, cy, cz));
+    const int c = e.cid[a];
+    int key = e.home[a];
+    if (e.ctl[c].rebuild) {
+      const CaseDev& C = e.cases[c];
+      const double4 p = ld4(e.pos, a);
+      key = C.key_off + local_cell(C, p.x, p.y, p.z);
+    }
+    e.keys[a] = static_cast<uint64_t>(key);
     e.vals[a] = a;
   }
 }
 
 __global__ void k_permute(Dev e) {
-  if (!e.flag[0]) return;
+  if (!*e.any_rebuild) return;
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
     const int s = e.vals[a];
     st4(e.tmp4a, a, ld4(e.pos, s));
@@ -240,9 +294,14 @@ __global__ void k_permute(Dev e) {
   }
 }
 
+// Only the blocks of rebuilding cases change: every other block is already in
+// home-key order, which the stable sort keeps.
 __global__ void k_permute_back(Dev e) {
-  if (!e.flag[0]) return;
+  if (!*e.any_rebuild) return;
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    const int c = e.cid[a];
+    if (!e.ctl[c].rebuild) continue;
+    const CaseDev& C = e.cases[c];
     const double4 p = ld4(e.tmp4a, a);
     const int key = static_cast<int>(e.keys[a]);
     st4(e.pos, a, p);
@@ -250,80 +309,85 @@ __global__ void k_permute_back(Dev e) {
     st4(e.vel, a, ld4(e.tmp4b, a));
     e.id[a] = e.tmp_id[a];
     e.home[a] = key;
-    e.lp[a] = local_of(e, key, p.x, p.y, p.z, p.w);
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    e.maxbits[0] = 0;
-    e.maxbits[1] = 0;
+    e.lp[a] = local_of(C, key - C.key_off, p.x, p.y, p.z, p.w);
   }
 }
 
 __global__ void k_clear_table(int32_t* start, int32_t* end, int64_t ncells, const int* flag) {
-  if (flag && !flag[0]) return;
+  if (flag && !*flag) return;
   for (int64_t c = blockIdx.x * blockDim.x + threadIdx.x; c < ncells; c += gridDim.x * blockDim.x) {
     start[c] = -1;
     end[c] = -1;
   }
 }
 
-__global__ void k_fill_table(const uint64_t* __restrict__ keys, int n, int32_t* start, int32_t* end,
-                             const int* flag) {
-  if (flag && !flag[0]) return;
+// Cell runs of a key-sorted array: [start, end) per key; `base` offsets the
+// stored values.
+__global__ void k_fill_table(const int32_t* __restrict__ home, const uint64_t* __restrict__ keys, int n,
+                             int32_t* start, int32_t* end, const int* flag) {
+  if (flag && !*flag) return;
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
-    const uint64_t k = keys[a];
-    if (a == 0 || keys[a - 1] != k) start[k] = a;
-    if (a == n - 1 || keys[a + 1] != k) end[k] = a + 1;
+    const int64_t k = keys ? static_cast<int64_t>(keys[a]) : home[a];
+    const int64_t prev = a == 0 ? -1 : (keys ? static_cast<int64_t>(keys[a - 1]) : home[a - 1]);
+    const int64_t next = a == n - 1 ? -1 : (keys ? static_cast<int64_t>(keys[a + 1]) : home[a + 1]);
+    if (prev != k) start[k] = a;
+    if (next != k) end[k] = a + 1;
   }
 }
 
-// Neighbour rows at the list cutoff (2h + skin) in FP64, for every particle;
-// wall rows keep fluid neighbours only (they feed the Adami extrapolation and
-// the obstacle reaction).
+// Rows at the list cutoff (2h + skin) with FP64 distances, for the rows of
+// rebuilding cases; wall rows keep fluid neighbours only (they feed the Adami
+// extrapolation and the obstacle reaction).
 __global__ void k_rows(Dev e) {
-  if (!e.flag[0]) return;
-  int rowmax = 0;
-  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.N; a += gridDim.x * blockDim.x) {
+  if (!*e.any_rebuild) return;
+  const int total = e.nf + e.nw;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const int64_t a = t < e.nf ? t : e.NF + (t - e.nf);
+    const int c = e.cid[a];
+    CaseCtl& ctl = e.ctl[c];
+    if (!ctl.rebuild) continue;
+    const CaseDev& C = e.cases[c];
     const double4 pa = ld4(e.pos, a);
-    const int key_a = e.home[a];
-    const int cz = key_a % e.ncz, cy = (key_a / e.ncz) % e.ncy, cx = key_a / (e.ncz * e.ncy);
+    const int key_a = e.home[a] - C.key_off;
+    const int cz = key_a % C.ncz, cy = (key_a / C.ncz) % C.ncy, cx = key_a / (C.ncz * C.ncy);
+    const bool fluid_row = t < e.nf;
+    const double rc2 = C.rc2;
     int count = 0;
-    const bool fluid_row = a < e.nf;
     for (int dx = -1; dx <= 1; ++dx) {
       const int x = cx + dx;
-      if (x < 0 || x >= e.ncx) continue;
+      if (x < 0 || x >= C.ncx) continue;
       for (int dy = -1; dy <= 1; ++dy) {
         const int y = cy + dy;
-        if (y < 0 || y >= e.ncy) continue;
+        if (y < 0 || y >= C.ncy) continue;
         for (int dz = -1; dz <= 1; ++dz) {
           const int z = cz + dz;
-          if (z < 0 || z >= e.ncz) continue;
-          const int c = (x * e.ncy + y) * e.ncz + z;
+          if (z < 0 || z >= C.ncz) continue;
+          const int cell = C.key_off + (x * C.ncy + y) * C.ncz + z;
           const uint32_t code = static_cast<uint32_t>((dx + 1) * 9 + (dy + 1) * 3 + (dz + 1));
-          const int fs = e.fstart[c];
+          const int fs = e.fstart[cell];
           if (fs >= 0) {
-            const int fe = e.fend[c];
+            const int fe = e.fend[cell];
             for (int b = fs; b < fe; ++b) {
               if (b == a) continue;
               const double4 pb = ld4(e.pos, b);
               const double ddx = pa.x - pb.x, ddy = pa.y - pb.y, ddz = pa.z - pb.z;
-              if (ddx * ddx + ddy * ddy + ddz * ddz <= e.rc2) {
-                if (count < e.maxnb)
-                  e.nbr[static_cast<int64_t>(count) * e.N + a] = (static_cast<uint32_t>(b) << 5) | code;
+              if (ddx * ddx + ddy * ddy + ddz * ddz <= rc2) {
+                if (count < e.maxnb) e.nbr[static_cast<int64_t>(count) * e.rows + a] = (static_cast<uint32_t>(b) << 5) | code;
                 ++count;
               }
             }
           }
           if (fluid_row) {
-            const int ws = e.wstart[c];
+            const int ws = e.wstart[cell];
             if (ws >= 0) {
-              const int we = e.wend[c];
+              const int we = e.wend[cell];
               for (int w = ws; w < we; ++w) {
-                const int b = e.nf + w;
+                const int64_t b = e.NF + w;
                 const double4 pb = ld4(e.pos, b);
                 const double ddx = pa.x - pb.x, ddy = pa.y - pb.y, ddz = pa.z - pb.z;
-                if (ddx * ddx + ddy * ddy + ddz * ddz <= e.rc2) {
+                if (ddx * ddx + ddy * ddy + ddz * ddz <= rc2) {
                   if (count < e.maxnb)
-                    e.nbr[static_cast<int64_t>(count) * e.N + a] = (static_cast<uint32_t>(b) << 5) | code;
+                    e.nbr[static_cast<int64_t>(count) * e.rows + a] = (static_cast<uint32_t>(b) << 5) | code;
                   ++count;
                 }
               }
@@ -332,101 +396,132 @@ __global__ void k_rows(Dev e) {
         }
       }
     }
-    if (count > e.maxnb) atomicOr(e.status, 1);
+    if (count > e.maxnb) {
+      atomicOr(e.status, 1);
+      atomicOr(&ctl.status, 1);
+    }
     e.cnt[a] = count < e.maxnb ? count : e.maxnb;
-    rowmax = count > rowmax ? count : rowmax;
+    atomicMax(&ctl.row_max, static_cast<unsigned long long>(count));
   }
-  rowmax = warp_reduce_max(rowmax);
-  if ((threadIdx.x & 31) == 0) atomicMax(&e.counters[4], static_cast<long long>(rowmax));
+}
+
+__global__ void k_rebuilt(Dev e) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= e.n_slots || !e.ctl[c].rebuild) return;
+  e.ctl[c].disp[0] = 0;
+  e.ctl[c].disp[1] = 0;
+}
+
+// Per-case step start: clear the per-step meters.
+__global__ void k_step_begin(Dev e) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= e.n_slots) return;
+  CaseCtl& t = e.ctl[c];
+  t.rho_max = t.speed_max = t.front_max = 0;
+  t.ke = t.pe = 0;
+  t.force[0] = t.force[1] = t.force[2] = 0;
+  t.disp[0] = 0;
 }
 
 // ------------------------------------------------------------- physics ---
 
-__global__ void __launch_bounds__(kBlock) k_density(Dev e) {
+template <bool kOne>
+__global__ void __launch_bounds__(kMaxBlock) k_density(const __grid_constant__ Dev e) {
   __shared__ float4 tab[27];
-  fill_offsets(tab, e.cellf);
+  fill_units(tab);
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    const CaseDev& C = case_of<kOne>(e, a);
+    const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, floor_ = C.rho_floor;
     const float4 la = e.lp[a];
     CSum<float> s;
-    s.add(la.w * e.sigma);
+    s.add(la.w * sigma);
     walk_row(e, a, [&](const uint32_t* ent) {
       float part = 0.f;
 #pragma unroll
       for (int j = 0; j < kBatch; ++j) {
-        const bool ok = ent[j] != 0xffffffffu;
+        const bool ok = ent[j] != kPad;
         const int b = ok ? static_cast<int>(ent[j] >> 5) : a;
         const float4 lb = e.lp[b];
-        const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u]);
+        const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u], cellf);
         const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
-        const float W = e.sigma * shape(radial(r2, e.inv_h).q);
+        const float W = sigma * shape(radial(r2, inv_h).q);
         part += ok ? lb.w * W : 0.f;
       }
       s.add(part);
     });
     float rho = s.value();
-    rho = rho > e.rho_floor ? rho : e.rho_floor;
+    rho = rho > floor_ ? rho : floor_;
     e.rs[a] = make_float2(rho, la.w / rho);
   }
 }
 
-__global__ void __launch_bounds__(kBlock) k_diffusion_eos(Dev e) {
+template <bool kOne>
+__global__ void __launch_bounds__(kMaxBlock) k_diffusion_eos(const __grid_constant__ Dev e) {
   __shared__ float4 tab[27];
-  fill_offsets(tab, e.cellf);
+  fill_units(tab);
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    const CaseDev& C = case_of<kOne>(e, a);
     const float2 ra = e.rs[a];
+    const float4 la = e.lp[a];
     float rho = ra.x;
-    if (e.dscale > 0.f) {
-      const float4 la = e.lp[a];
+    const float dscale = C.dscale;
+    if (dscale > 0.f) {
+      const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf;
+      const int NF = e.NF;
       CSum<float> rate;
       walk_row(e, a, [&](const uint32_t* ent) {
         float part = 0.f;
 #pragma unroll
         for (int j = 0; j < kBatch; ++j) {
-          const int b = ent[j] != 0xffffffffu ? static_cast<int>(ent[j] >> 5) : a;
-          const bool ok = ent[j] != 0xffffffffu && b < e.nf;
-          const int bf = ok ? b : a;
-          const float4 lb = e.lp[bf];
-          const float2 rb = e.rs[bf];
-          const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u]);
+          const int b0 = ent[j] != kPad ? static_cast<int>(ent[j] >> 5) : a;
+          const bool ok = ent[j] != kPad && b0 < NF;
+          const int b = ok ? b0 : a;
+          const float4 lb = e.lp[b];
+          const float2 rb = e.rs[b];
+          const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u], cellf);
           const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
-          const Radial R = radial(r2, e.inv_h);
-          const float gs = e.sigma * dshape(R.q) * e.inv_h * R.inv_r;
+          const Radial R = radial(r2, inv_h);
+          const float gs = sigma * dshape(R.q) * inv_h * R.inv_r;
           const float coupling = (ra.x - rb.x) * (-gs * r2) * __frcp_rn(r2 + 1e-12f);
-          part += ok ? (-e.dscale * rb.y) * coupling : 0.f;
+          part += ok ? (-dscale * rb.y) * coupling : 0.f;
         }
         rate.add(part);
       });
-      rho = ra.x + e.dtf * rate.value();
-      rho = rho > e.rho_floor ? rho : e.rho_floor;
+      rho = ra.x + C.dtf * rate.value();
+      rho = rho > C.rho_floor ? rho : C.rho_floor;
     }
-    const float p = tait(e, rho);
+    const float p = tait(rho, C.rho0, C.bulk, C.gamma);
     const double4 v = ld4(e.vel, a);
-    const float m = e.lp[a].w;
-    e.vb[a] = make_float4(static_cast<float>(v.x), static_cast<float>(v.y), static_cast<float>(v.z), m / rho);
+    e.vb[a] = make_float4(static_cast<float>(v.x), static_cast<float>(v.y), static_cast<float>(v.z), la.w / rho);
     e.rho[a] = rho;
     e.pr[a] = p;
     e.pq[a] = p / (rho * rho);
   }
 }
 
-__global__ void __launch_bounds__(kBlock) k_walls(Dev e) {
+template <bool kOne>
+__global__ void __launch_bounds__(kMaxBlock) k_walls(const __grid_constant__ Dev e) {
   __shared__ float4 tab[27];
-  fill_offsets(tab, e.cellf);
-  for (int a = e.nf + blockIdx.x * blockDim.x + threadIdx.x; a < e.N; a += gridDim.x * blockDim.x) {
+  fill_units(tab);
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < e.nw; t += gridDim.x * blockDim.x) {
+    const int64_t a = e.NF + t;
+    const CaseDev& C = case_of<kOne>(e, a);
+    const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, grav = C.grav;
+    const int f0 = C.fluid_begin;
     const float4 la = e.lp[a];
     CSum<float> num, den;
     walk_row(e, a, [&](const uint32_t* ent) {
       float pn = 0.f, pd = 0.f;
 #pragma unroll
       for (int j = 0; j < kBatch; ++j) {
-        const bool ok = ent[j] != 0xffffffffu;
-        const int f = ok ? static_cast<int>(ent[j] >> 5) : 0;
+        const bool ok = ent[j] != kPad;
+        const int f = ok ? static_cast<int>(ent[j] >> 5) : f0;
         const float4 lf = e.lp[f];
-        const float3 d = sep(la, lf, tab[ok ? (ent[j] & 31u) : 13u]);  // r_w - r_f
+        const float3 d = sep(la, lf, tab[ok ? (ent[j] & 31u) : 13u], cellf);  // r_w - r_f
         const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
-        const float W = ok ? e.sigma * shape(radial(r2, e.inv_h).q) : 0.f;
+        const float W = ok ? sigma * shape(radial(r2, inv_h).q) : 0.f;
         float src = e.pr[f];
-        if (e.grav != 0.f) src = src + e.rho[f] * (-e.grav * d.y);
+        if (grav != 0.f) src = src + e.rho[f] * (-grav * d.y);
         pn += src * W;
         pd += W;
       }
@@ -436,8 +531,8 @@ __global__ void __launch_bounds__(kBlock) k_walls(Dev e) {
     const float dd = den.value();
     float p = num.value() / (dd > 1e-30f ? dd : 1e-30f);
     p = p > 0.f ? p : 0.f;
-    float rho = e.rho0 * powf(p / e.bulk + 1.f, e.inv_gamma);
-    rho = rho > e.rho0 ? rho : e.rho0;
+    float rho = C.rho0 * powf(p / C.bulk + 1.f, C.inv_gamma);
+    rho = rho > C.rho0 ? rho : C.rho0;
     e.vb[a] = make_float4(0.f, 0.f, 0.f, la.w / rho);
     e.rho[a] = rho;
     e.pr[a] = p;
@@ -445,10 +540,15 @@ __global__ void __launch_bounds__(kBlock) k_walls(Dev e) {
   }
 }
 
-__global__ void __launch_bounds__(kBlock) k_force(Dev e) {
+template <bool kOne>
+__global__ void __launch_bounds__(kMaxBlock) k_force(const __grid_constant__ Dev e) {
   __shared__ float4 tab[27];
-  fill_offsets(tab, e.cellf);
+  fill_units(tab);
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    const CaseDev& C = case_of<kOne>(e, a);
+    const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, nu2 = C.nu2, nu2f = C.nu2f,
+                eta2 = C.visc_eps;
+    const int NF = e.NF;
     const float4 la = e.lp[a];
     const float4 va = e.vb[a];
     const float Pa = e.pq[a];
@@ -457,19 +557,19 @@ __global__ void __launch_bounds__(kBlock) k_force(Dev e) {
       float px = 0.f, py = 0.f, pz = 0.f;
 #pragma unroll
       for (int j = 0; j < kBatch; ++j) {
-        const bool ok = ent[j] != 0xffffffffu;
+        const bool ok = ent[j] != kPad;
         const int b = ok ? static_cast<int>(ent[j] >> 5) : a;
         const float4 lb = e.lp[b];
         const float4 vb = e.vb[b];
         const float Pb = e.pq[b];
-        const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u]);
+        const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u], cellf);
         const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
-        const Radial R = radial(r2, e.inv_h);
-        float gs = e.sigma * dshape(R.q) * e.inv_h * R.inv_r;
+        const Radial R = radial(r2, inv_h);
+        float gs = sigma * dshape(R.q) * inv_h * R.inv_r;
         gs = ok ? gs : 0.f;
         const float fp = -lb.w * (Pa + Pb) * gs;
-        const float vs = b < e.nf ? e.nu2 : e.nu2f;
-        const float lw = fmaxf(-gs * r2, 0.f) * __frcp_rn(r2 + e.visc_eps);
+        const float vs = b < NF ? nu2 : nu2f;
+        const float lw = fmaxf(-gs * r2, 0.f) * __frcp_rn(r2 + eta2);
         const float coef = -vs * (vb.w * lw);
         px += fp * d.x + coef * (va.x - vb.x);
         py += fp * d.y + coef * (va.y - vb.y);
@@ -479,19 +579,31 @@ __global__ void __launch_bounds__(kBlock) k_force(Dev e) {
       ay.add(py);
       az.add(pz);
     });
-    e.acc[a] = make_float4(ax.value(), ay.value() - e.grav, az.value(), 0.f);
+    e.acc[a] = make_float4(ax.value(), ay.value() - C.grav, az.value(), 0.f);
   }
 }
 
 // Force of the fluid on each obstacle particle (rhs_3d(return_wall_force=True),
-// dam_break_3d.py:412-421), reduced per block in FP64.
-__global__ void __launch_bounds__(kBlock) k_reaction(Dev e) {
+// dam_break_3d.py:412-421), summed per case in FP64.  Obstacle rows are grouped
+// by case, so a block whose rows all belong to one case adds one total.
+__global__ void __launch_bounds__(kMaxBlock) k_reaction(Dev e) {
   __shared__ float4 tab[27];
-  __shared__ double part[kBlock / 32][3];
-  fill_offsets(tab, e.cellf);
-  double fx = 0, fy = 0, fz = 0;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < e.nob; q += gridDim.x * blockDim.x) {
-    const int w = e.ob_rows[q];
+  __shared__ double red[kMaxBlock / 32];
+  fill_units(tab);
+  const int q0 = blockIdx.x * blockDim.x;
+  if (q0 >= e.n_ob) return;
+  const int q = q0 + threadIdx.x;
+  const int last = min(q0 + static_cast<int>(blockDim.x), e.n_ob) - 1;
+  const int cb = e.cid[e.ob_rows[q0]];
+  const bool uniform = cb == e.cid[e.ob_rows[last]];
+  int c = -1;
+  double f[3] = {0, 0, 0};
+  if (q < e.n_ob) {
+    const int64_t w = e.ob_rows[q];
+    c = e.cid[w];
+    const CaseDev& C = e.cases[c];
+    const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, nu2f = C.nu2f, eta2 = C.visc_eps;
+    const int f0 = C.fluid_begin;
     const float4 lw_ = e.lp[w];
     const float Pw = e.pq[w];
     const float mw = lw_.w;
@@ -501,21 +613,21 @@ __global__ void __launch_bounds__(kBlock) k_reaction(Dev e) {
       float px = 0.f, py = 0.f, pz = 0.f;
 #pragma unroll
       for (int j = 0; j < kBatch; ++j) {
-        const bool ok = ent[j] != 0xffffffffu;
-        const int f = ok ? static_cast<int>(ent[j] >> 5) : 0;
-        const float4 lf = e.lp[f];
-        const float3 d = sep(lw_, lf, tab[ok ? (ent[j] & 31u) : 13u]);
+        const bool ok = ent[j] != kPad;
+        const int fi = ok ? static_cast<int>(ent[j] >> 5) : f0;
+        const float4 lf = e.lp[fi];
+        const float3 d = sep(lw_, lf, tab[ok ? (ent[j] & 31u) : 13u], cellf);
         const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
-        const Radial R = radial(r2, e.inv_h);
-        float gs = e.sigma * dshape(R.q) * e.inv_h * R.inv_r;
+        const Radial R = radial(r2, inv_h);
+        float gs = sigma * dshape(R.q) * inv_h * R.inv_r;
         gs = ok ? gs : 0.f;
         const float mf = lf.w;
-        const float c = -(mw * mf) * (Pw + e.pq[f]) * gs;
-        float x = c * d.x, y = c * d.y, z = c * d.z;
-        if (e.nu2f != 0.f) {
-          const float4 vf = e.vb[f];
-          const float lwt = fmaxf(-gs * r2, 0.f) * __frcp_rn(r2 + e.visc_eps);
-          const float coef = mf * e.nu2f * (Vw * lwt);
+        const float cc = -(mw * mf) * (Pw + e.pq[fi]) * gs;
+        float x = cc * d.x, y = cc * d.y, z = cc * d.z;
+        if (nu2f != 0.f) {
+          const float4 vf = e.vb[fi];
+          const float lwt = fmaxf(-gs * r2, 0.f) * __frcp_rn(r2 + eta2);
+          const float coef = mf * nu2f * (Vw * lwt);
           x += coef * vf.x;
           y += coef * vf.y;
           z += coef * vf.z;
@@ -528,188 +640,180 @@ __global__ void __launch_bounds__(kBlock) k_reaction(Dev e) {
       ry.add(py);
       rz.add(pz);
     });
-    fx += rx.value();
-    fy += ry.value();
-    fz += rz.value();
+    f[0] = rx.value();
+    f[1] = ry.value();
+    f[2] = rz.value();
   }
-  fx = warp_reduce_sum(fx);
-  fy = warp_reduce_sum(fy);
-  fz = warp_reduce_sum(fz);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0) { part[warp][0] = fx; part[warp][1] = fy; part[warp][2] = fz; }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s[3] = {0, 0, 0};
-    for (int w = 0; w < kBlock / 32; ++w)
-      for (int k = 0; k < 3; ++k) s[k] += part[w][k];
-    for (int k = 0; k < 3; ++k) e.partials[static_cast<int64_t>(e.nblocks_int + blockIdx.x) * 8 + k] = s[k];
+  if (uniform) {
+    for (int k = 0; k < 3; ++k) {
+      const double s = block_reduce<false>(f[k], red);
+      if (threadIdx.x == 0) atomicAdd(&e.ctl[cb].force[k], s);
+    }
+  } else if (c >= 0) {
+    for (int k = 0; k < 3; ++k) atomicAdd(&e.ctl[c].force[k], f[k]);
   }
 }
-// Semi-implicit Euler, box and obstacle clamps, meters (state before the update,
-// as the reference samples it), skin displacement.  Per-block partials only:
-// [0] kinetic [1] potential [2] max displacement [3] max speed [4] max front
-// [5] max density [6] escapes [7] obstacle clamps; k_finalize reduces them.
-__global__ void k_integrate(Dev e) {
-  __shared__ double part[kBlock / 32][8];
-  double acc8[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  bool bad = false;
-  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+
+// Semi-implicit Euler, box and obstacle clamps, per-case meters (of the state
+// before the update, as the reference samples them) and the skin displacement.
+template <bool kOne>
+__global__ void __launch_bounds__(kMaxBlock) k_integrate(const __grid_constant__ Dev e) {
+  __shared__ double red[kMaxBlock / 32];
+  const int a0 = blockIdx.x * blockDim.x;
+  if (a0 >= e.nf) return;
+  const int a = a0 + threadIdx.x;
+  const int cb = kOne ? e.one_slot : e.cid[a0];
+  const bool uniform = kOne || cb == e.cid[min(a0 + static_cast<int>(blockDim.x), e.nf) - 1];
+  int c = -1;
+  double ke = 0, pe = 0, dmax = 0, vmax = 0, xmax = 0, rmax = 0;
+  if (a < e.nf) {
+    c = kOne ? cb : e.cid[a];
+    const CaseDev& C = case_of<kOne>(e, a);
     const double4 x0 = ld4(e.pos, a);
     const double4 v0 = ld4(e.vel, a);
     const float4 ac = e.acc[a];
     const double m = x0.w;
+    const double dt = C.dt;
     const double v2 = v0.x * v0.x + v0.y * v0.y + v0.z * v0.z;
-    acc8[0] += 0.5 * m * v2;
-    acc8[1] += m * e.gravity * x0.y;
-    acc8[3] = fmax(acc8[3], sqrt(v2));
-    acc8[4] = fmax(acc8[4], x0.x);
-    acc8[5] = fmax(acc8[5], static_cast<double>(e.rho[a]));
-    double v[3] = {v0.x + e.dt * static_cast<double>(ac.x), v0.y + e.dt * static_cast<double>(ac.y),
-                   v0.z + e.dt * static_cast<double>(ac.z)};
-    double x[3] = {x0.x + e.dt * v[0], x0.y + e.dt * v[1], x0.z + e.dt * v[2]};
-    bool out_any = false;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const double hi = e.box_hi[k];
-      const bool out = x[k] < -e.tol || x[k] > hi + e.tol;
-      x[k] = x[k] < 0.0 ? 0.0 : (x[k] > hi ? hi : x[k]);
-      if (out) {
-        v[k] = 0.0;
-        out_any = true;
-      }
-    }
-    acc8[6] += out_any ? 1.0 : 0.0;
-    if (e.has_ob && x[0] > e.ob_lo[0] && x[0] < e.ob_hi[0] && x[1] > e.ob_lo[1] && x[1] < e.ob_hi[1] &&
-        x[2] > e.ob_lo[2] && x[2] < e.ob_hi[2]) {
-      double best = x[0] - e.ob_lo[0];
+    ke = 0.5 * m * v2;
+    pe = m * C.gravity * x0.y;
+    vmax = sqrt(v2);
+    xmax = x0.x;
+    rmax = static_cast<double>(e.rho[a]);
+    double vx = v0.x + dt * static_cast<double>(ac.x), vy = v0.y + dt * static_cast<double>(ac.y),
+           vz = v0.z + dt * static_cast<double>(ac.z);
+    double px = x0.x + dt * vx, py = x0.y + dt * vy, pz = x0.z + dt * vz;
+    const bool ox = px < -C.tol || px > C.box_hi[0] + C.tol;
+    const bool oy = py < -C.tol || py > C.box_hi[1] + C.tol;
+    const bool oz = pz < -C.tol || pz > C.box_hi[2] + C.tol;
+    px = px < 0.0 ? 0.0 : (px > C.box_hi[0] ? C.box_hi[0] : px);
+    py = py < 0.0 ? 0.0 : (py > C.box_hi[1] ? C.box_hi[1] : py);
+    pz = pz < 0.0 ? 0.0 : (pz > C.box_hi[2] ? C.box_hi[2] : pz);
+    vx = ox ? 0.0 : vx;
+    vy = oy ? 0.0 : vy;
+    vz = oz ? 0.0 : vz;
+    if (ox || oy || oz) atomicAdd(&e.ctl[c].escapes, 1ull);
+    if (C.has_ob && px > C.ob_lo[0] && px < C.ob_hi[0] && py > C.ob_lo[1] && py < C.ob_hi[1] &&
+        pz > C.ob_lo[2] && pz < C.ob_hi[2]) {
+      // exit through the nearest face (first minimum, as argmin)
+      const double dist[6] = {px - C.ob_lo[0], C.ob_hi[0] - px, py - C.ob_lo[1],
+                              C.ob_hi[1] - py, pz - C.ob_lo[2], C.ob_hi[2] - pz};
       int which = 0;
+      double best = dist[0];
 #pragma unroll
       for (int f = 1; f < 6; ++f) {
-        const int k = f >> 1;
-        const double dist = (f & 1) ? e.ob_hi[k] - x[k] : x[k] - e.ob_lo[k];
-        if (dist < best) {
-          best = dist;
+        if (dist[f] < best) {
+          best = dist[f];
           which = f;
         }
       }
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        if (k == (which >> 1)) {
-          x[k] = (which & 1) ? e.ob_hi[k] + e.ob_eps : e.ob_lo[k] - e.ob_eps;
-          v[k] = 0.0;
-        }
+      const double to = (which & 1) ? C.ob_eps : -C.ob_eps;
+      if (which < 2) {
+        px = ((which & 1) ? C.ob_hi[0] : C.ob_lo[0]) + to;
+        vx = 0.0;
+      } else if (which < 4) {
+        py = ((which & 1) ? C.ob_hi[1] : C.ob_lo[1]) + to;
+        vy = 0.0;
+      } else {
+        pz = ((which & 1) ? C.ob_hi[2] : C.ob_lo[2]) + to;
+        vz = 0.0;
       }
-      acc8[7] += 1.0;
+      atomicAdd(&e.ctl[c].clamps, 1ull);
     }
-    if (!isfinite(x[0]) || !isfinite(x[1]) || !isfinite(x[2]) || !isfinite(v[0]) || !isfinite(v[1]) ||
-        !isfinite(v[2]))
-      bad = true;
+    if (!isfinite(px) || !isfinite(py) || !isfinite(pz) || !isfinite(vx) || !isfinite(vy) || !isfinite(vz)) {
+      atomicOr(e.status, 2);
+      atomicOr(&e.ctl[c].status, 2);
+    }
+    const double x[3] = {px, py, pz};
+    const double v[3] = {vx, vy, vz};
     st4(e.pos, a, make_double4(x[0], x[1], x[2], m));
     st4(e.vel, a, make_double4(v[0], v[1], v[2], 0.0));
-    e.lp[a] = local_of(e, e.home[a], x[0], x[1], x[2], m);
+    e.lp[a] = local_of(C, e.home[a] - C.key_off, x[0], x[1], x[2], m);
     const double4 an = ld4(e.anchor, a);
     const double ex = x[0] - an.x, ey = x[1] - an.y, ez = x[2] - an.z;
-    acc8[2] = fmax(acc8[2], sqrt(ex * ex + ey * ey + ez * ez));
+    dmax = sqrt(ex * ex + ey * ey + ez * ez);
   }
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    const bool is_max = k >= 2 && k <= 5;
-    acc8[k] = is_max ? warp_reduce_max(acc8[k]) : warp_reduce_sum(acc8[k]);
+  if (uniform) {
+    ke = block_reduce<false>(ke, red);
+    pe = block_reduce<false>(pe, red);
+    dmax = block_reduce<true>(dmax, red);
+    vmax = block_reduce<true>(vmax, red);
+    xmax = block_reduce<true>(xmax, red);
+    rmax = block_reduce<true>(rmax, red);
+    c = threadIdx.x == 0 ? cb : -1;
   }
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0)
-    for (int k = 0; k < 8; ++k) part[warp][k] = acc8[k];
-  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(e.status, 2);
-  __syncthreads();
-  if (threadIdx.x < 8) {
-    const int k = threadIdx.x;
-    const bool is_max = k >= 2 && k <= 5;
-    double r = part[0][k];
-    for (int w = 1; w < kBlock / 32; ++w) r = is_max ? fmax(r, part[w][k]) : r + part[w][k];
-    e.partials[static_cast<int64_t>(blockIdx.x) * 8 + k] = r;
+  if (c >= 0) {
+    CaseCtl& t = e.ctl[c];
+    atomicAdd(&t.ke, ke);
+    atomicAdd(&t.pe, pe);
+    atomic_max_nonneg(&t.disp[0], dmax);
+    atomic_max_nonneg(&t.speed_max, vmax);
+    atomic_max_nonneg(&t.front_max, xmax);
+    atomic_max_nonneg(&t.rho_max, rmax);
   }
 }
 
-// One warp reduces the per-block partials in a fixed order (deterministic).
+// Per-case meter row: max rho, max |v|, front x, obstacle force xyz, kinetic
+// and potential energy, escapes, clamps, rebuilds, longest row, step, status,
+// obstacle impulse x, c_ref.
 __global__ void k_finalize(Dev e) {
-  if (blockIdx.x) return;
-  const int lane = threadIdx.x;
-  double ke = 0, pe = 0, dmax = 0, vmax = 0, xmax = 0, rmax = 0, esc = 0, clamps = 0;
-  double f[3] = {0, 0, 0};
-  for (int b = lane; b < e.nblocks_int; b += 32) {
-    const double* q = e.partials + static_cast<int64_t>(b) * 8;
-    ke += q[0];
-    pe += q[1];
-    dmax = fmax(dmax, q[2]);
-    vmax = fmax(vmax, q[3]);
-    xmax = fmax(xmax, q[4]);
-    rmax = fmax(rmax, q[5]);
-    esc += q[6];
-    clamps += q[7];
-  }
-  for (int b = lane; b < e.nblocks_ob; b += 32)
-    for (int k = 0; k < 3; ++k) f[k] += e.partials[static_cast<int64_t>(e.nblocks_int + b) * 8 + k];
-  ke = warp_reduce_sum(ke);
-  pe = warp_reduce_sum(pe);
-  esc = warp_reduce_sum(esc);
-  clamps = warp_reduce_sum(clamps);
-  dmax = warp_reduce_max(dmax);
-  vmax = warp_reduce_max(vmax);
-  xmax = warp_reduce_max(xmax);
-  rmax = warp_reduce_max(rmax);
-  for (int k = 0; k < 3; ++k) f[k] = warp_reduce_sum(f[k]);
-  if (lane) return;
-  e.counters[0] += static_cast<long long>(esc);
-  e.counters[1] += static_cast<long long>(clamps);
-  e.maxbits[0] = static_cast<unsigned long long>(__double_as_longlong(dmax));
-  const long long step = e.counters[3];
-  double* row = e.diag + (step % e.diag_ring) * kDiag;
-  row[0] = rmax;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= e.n_slots) return;
+  CaseCtl& t = e.ctl[c];
+  if (!t.active) return;
+  const CaseDev& C = e.cases[c];
+  const unsigned long long step = t.steps;
+  double* row = e.diag + (static_cast<int64_t>(c) * e.diag_ring + static_cast<int64_t>(step % e.diag_ring)) * kDiag;
+  const double vmax = __longlong_as_double(static_cast<long long>(t.speed_max));
+  row[0] = __longlong_as_double(static_cast<long long>(t.rho_max));
   row[1] = vmax;
-  row[2] = xmax;
-  row[3] = f[0];
-  row[4] = f[1];
-  row[5] = f[2];
-  row[6] = ke;
-  row[7] = pe;
-  row[8] = static_cast<double>(e.counters[0]);
-  row[9] = static_cast<double>(e.counters[1]);
-  row[10] = static_cast<double>(e.counters[2]);
-  row[11] = static_cast<double>(e.counters[4]);
+  row[2] = __longlong_as_double(static_cast<long long>(t.front_max));
+  for (int k = 0; k < 3; ++k) {
+    row[3 + k] = t.force[k];
+    t.impulse[k] += t.force[k] * C.dt;
+  }
+  row[6] = t.ke;
+  row[7] = t.pe;
+  row[8] = static_cast<double>(t.escapes);
+  row[9] = static_cast<double>(t.clamps);
+  row[10] = static_cast<double>(t.rebuilds);
+  row[11] = static_cast<double>(t.row_max);
   row[12] = static_cast<double>(step);
-  row[13] = static_cast<double>(*e.status);
-  for (int k = 0; k < 3; ++k) e.impulse[k] += f[k] * e.dt;
-  row[14] = e.impulse[0];
-  row[15] = e.cref[0];
-  // the speed of this step is the shift's reference speed
-  e.cref[1] = vmax;
-  e.counters[3] = step + 1;
-  e.flag[2] = e.shift_every > 0 && step > 0 && (step % e.shift_every) == 0;
-  e.flag[3] = 0;
+  row[13] = static_cast<double>(t.status);
+  row[14] = t.impulse[0];
+  row[15] = t.cref[0];
+  t.cref[1] = vmax;  // the shift's reference speed
+  t.steps = step + 1;
+  t.shift_now = C.shift_every > 0 && step > 0 && (step % static_cast<unsigned long long>(C.shift_every)) == 0;
+  t.shift_done = 0;
 }
 
 // ------------------------------------------------------------- shifting ---
+// One case (slot e.shift_slot) owns every fluid row when shifting runs.
 
-__global__ void __launch_bounds__(kBlock) k_concentration(Dev e) {
-  if (!e.flag[2]) return;
+__global__ void __launch_bounds__(kMaxBlock) k_concentration(Dev e) {
+  if (!e.ctl[e.shift_slot].shift_now) return;
   __shared__ float4 tab[27];
-  fill_offsets(tab, e.cellf);
+  fill_units(tab);
+  const CaseDev& C = e.cases[e.shift_slot];
+  const float sig2d = C.sig2d, inv_h = C.inv_h, cellf = C.cellf;
+  const int NF = e.NF;
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
     const float4 la = e.lp[a];
     CSum<float> s;
-    s.add(e.vb[a].w * e.sig2d);
+    s.add(e.vb[a].w * sig2d);
     walk_row(e, a, [&](const uint32_t* ent) {
       float part = 0.f;
 #pragma unroll
       for (int j = 0; j < kBatch; ++j) {
-        const int b0 = ent[j] != 0xffffffffu ? static_cast<int>(ent[j] >> 5) : a;
-        const bool ok = ent[j] != 0xffffffffu && b0 < e.nf;
+        const int b0 = ent[j] != kPad ? static_cast<int>(ent[j] >> 5) : a;
+        const bool ok = ent[j] != kPad && b0 < NF;
         const int b = ok ? b0 : a;
         const float4 lb = e.lp[b];
         const float Vb = e.vb[b].w;
-        const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u]);
+        const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u], cellf);
         const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
-        part += ok ? Vb * (e.sig2d * shape(radial(r2, e.inv_h).q)) : 0.f;
+        part += ok ? Vb * (sig2d * shape(radial(r2, inv_h).q)) : 0.f;
       }
       s.add(part);
     });
@@ -717,10 +821,13 @@ __global__ void __launch_bounds__(kBlock) k_concentration(Dev e) {
   }
 }
 
-__global__ void __launch_bounds__(kBlock) k_conc_gradient(Dev e) {
-  if (!e.flag[2]) return;
+__global__ void __launch_bounds__(kMaxBlock) k_conc_gradient(Dev e) {
+  if (!e.ctl[e.shift_slot].shift_now) return;
   __shared__ float4 tab[27];
-  fill_offsets(tab, e.cellf);
+  fill_units(tab);
+  const CaseDev& C = e.cases[e.shift_slot];
+  const float sig2d = C.sig2d, inv_h = C.inv_h, cellf = C.cellf;
+  const int NF = e.NF;
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
     const float4 la = e.lp[a];
     const float ca = e.conc[a];
@@ -729,20 +836,20 @@ __global__ void __launch_bounds__(kBlock) k_conc_gradient(Dev e) {
       float px = 0.f, py = 0.f, pz = 0.f;
 #pragma unroll
       for (int j = 0; j < kBatch; ++j) {
-        const int b0 = ent[j] != 0xffffffffu ? static_cast<int>(ent[j] >> 5) : a;
-        const bool ok = ent[j] != 0xffffffffu && b0 < e.nf;
+        const int b0 = ent[j] != kPad ? static_cast<int>(ent[j] >> 5) : a;
+        const bool ok = ent[j] != kPad && b0 < NF;
         const int b = ok ? b0 : a;
         const float4 lb = e.lp[b];
         const float Vb = e.vb[b].w;
         const float cb = e.conc[b];
-        const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u]);
+        const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u], cellf);
         const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
-        const Radial R = radial(r2, e.inv_h);
-        const float gs = e.sig2d * dshape(R.q) * e.inv_h * R.inv_r;
-        const float c = ok ? Vb * (cb - ca) * gs : 0.f;
-        px += c * d.x;
-        py += c * d.y;
-        pz += c * d.z;
+        const Radial R = radial(r2, inv_h);
+        const float gs = sig2d * dshape(R.q) * inv_h * R.inv_r;
+        const float cc = ok ? Vb * (cb - ca) * gs : 0.f;
+        px += cc * d.x;
+        py += cc * d.y;
+        pz += cc * d.z;
       }
       gx.add(px);
       gy.add(py);
@@ -751,6 +858,7 @@ __global__ void __launch_bounds__(kBlock) k_conc_gradient(Dev e) {
     e.gradc[a] = make_float4(gx.value(), gy.value(), gz.value(), 0.f);
   }
 }
+
 __device__ __forceinline__ uint32_t fkey(float v) {
   uint32_t b = __float_as_uint(v);
   return (b >> 31) ? ~b : (b | 0x80000000u);
@@ -758,7 +866,7 @@ __device__ __forceinline__ uint32_t fkey(float v) {
 
 // Radix select of the k-th smallest concentration, one 8-bit digit per pass.
 __global__ void k_select_hist(Dev e, int shift) {
-  if (!e.flag[2]) return;
+  if (!e.ctl[e.shift_slot].shift_now) return;
   __shared__ unsigned int h[256];
   h[threadIdx.x] = 0;
   __syncthreads();
@@ -773,19 +881,19 @@ __global__ void k_select_hist(Dev e, int shift) {
 }
 
 __global__ void k_select_pick(Dev e, int shift, long long rank, int which) {
-  if (!e.flag[2] || threadIdx.x || blockIdx.x) return;
+  if (!e.ctl[e.shift_slot].shift_now || threadIdx.x || blockIdx.x) return;
   if (shift == 24) {
     e.sel[0] = 0;
-    e.counters[5] = rank;
+    *e.sel_k = rank;
   }
-  long long k = e.counters[5];
+  long long k = *e.sel_k;
   int d = 0;
   for (; d < 255; ++d) {
     if (k < static_cast<long long>(e.hist[d])) break;
     k -= e.hist[d];
   }
   e.sel[0] |= static_cast<unsigned long long>(d) << shift;
-  e.counters[5] = k;
+  *e.sel_k = k;
   for (int i = 0; i < 256; ++i) e.hist[i] = 0;
   if (shift == 0) {
     const uint32_t key = static_cast<uint32_t>(e.sel[0]);
@@ -794,21 +902,25 @@ __global__ void k_select_pick(Dev e, int shift, long long rank, int which) {
   }
 }
 
+// torch.quantile's linear interpolation, computed as torch.lerp does it
 __global__ void k_select_finish(Dev e, double w) {
-  if (!e.flag[2] || threadIdx.x || blockIdx.x) return;
+  if (!e.ctl[e.shift_slot].shift_now || threadIdx.x || blockIdx.x) return;
   const double a = __longlong_as_double(static_cast<long long>(e.sel[1]));
   const double b = __longlong_as_double(static_cast<long long>(e.sel[2]));
-  e.cref[0] = w < 0.5 ? a + w * (b - a) : b - (b - a) * (1.0 - w);
-  e.maxbits[1] = 0;
+  e.ctl[e.shift_slot].cref[0] = w < 0.5 ? a + w * (b - a) : b - (b - a) * (1.0 - w);
+  e.ctl[e.shift_slot].disp[1] = 0;
 }
 
-__global__ void k_shift_apply(Dev e) {
-  if (!e.flag[2]) return;
-  const double cref = e.cref[0];
-  const float thresh = static_cast<float>(e.shift_fs * cref);
-  const double vref = fmax(e.cref[1], e.vref_floor);
-  const float mag = static_cast<float>(e.shift_strength_h_dt * vref);
-  const float cap = static_cast<float>(e.shift_cap);
+__global__ void __launch_bounds__(kMaxBlock) k_shift_apply(Dev e) {
+  CaseCtl& t = e.ctl[e.shift_slot];
+  if (!t.shift_now) return;
+  __shared__ double red[kMaxBlock / 32];
+  const CaseDev& C = e.cases[e.shift_slot];
+  const double cref = t.cref[0];
+  const float thresh = static_cast<float>(C.shift_fs * cref);
+  const double vref = fmax(t.cref[1], C.vref_floor);
+  const float mag = static_cast<float>(C.shift_strength_h_dt * vref);
+  const float cap = static_cast<float>(C.shift_cap);
   double dmax = 0;
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
     const float4 g = e.gradc[a];
@@ -835,66 +947,113 @@ __global__ void k_shift_apply(Dev e) {
     x.y += sy;
     x.z += sz;
     st4(e.pos, a, x);
-    e.lp[a] = local_of(e, e.home[a], x.x, x.y, x.z, x.w);
+    e.lp[a] = local_of(C, e.home[a] - C.key_off, x.x, x.y, x.z, x.w);
     const double4 an = ld4(e.anchor, a);
     const double ex = x.x - an.x, ey = x.y - an.y, ez = x.z - an.z;
     dmax = fmax(dmax, sqrt(ex * ex + ey * ey + ez * ez));
   }
-  __shared__ double part[kBlock / 32];
-  dmax = warp_reduce_max(dmax);
-  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = dmax;
-  __syncthreads();
+  dmax = block_reduce<true>(dmax, red);
   if (threadIdx.x == 0) {
-    double r = part[0];
-    for (int w = 1; w < kBlock / 32; ++w) r = fmax(r, part[w]);
-    atomic_max_nonneg(&e.maxbits[1], r);
-    if (blockIdx.x == 0) e.flag[3] = 1;
+    atomic_max_nonneg(&t.disp[1], dmax);
+    if (blockIdx.x == 0) t.shift_done = 1;
   }
 }
 
-// ----------------------------------------------------------------- init ---
+// ----------------------------------------------------- admission, retire ---
 
-__global__ void k_init_fluid(Dev e, const double* __restrict__ x, const double* __restrict__ v,
-                             const double* __restrict__ m) {
-  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
-    st4(e.pos, a, make_double4(x[3 * a], x[3 * a + 1], x[3 * a + 2], m[a]));
-    st4(e.vel, a, make_double4(v[3 * a], v[3 * a + 1], v[3 * a + 2], 0.0));
-    e.id[a] = a;
+__global__ void k_place_fluid(Dev e, int begin, int n, int slot, int dim, const double* __restrict__ x,
+                              const double* __restrict__ v, const double* __restrict__ m) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int a = begin + i;
+    const double z = dim == 3 ? x[3 * i + 2] : 0.0;
+    const double vz = dim == 3 ? v[3 * i + 2] : 0.0;
+    const double4 p = make_double4(x[dim * i], x[dim * i + 1], z, m[i]);
+    st4(e.pos, a, p);
+    st4(e.anchor, a, p);
+    st4(e.vel, a, make_double4(v[dim * i], v[dim * i + 1], vz, 0.0));
+    e.id[a] = i;
+    e.cid[a] = slot;
+    e.home[a] = 0;
+    e.cnt[a] = 0;
+    e.rho[a] = 0.f;
+    e.pr[a] = 0.f;
   }
 }
 
-__global__ void k_wall_keys(Dev e, const double* __restrict__ w) {
-  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nw; a += gridDim.x * blockDim.x) {
-    int cx, cy, cz;
-    e.keys[a] = static_cast<uint64_t>(cell_of(e, w[3 * a], w[3 * a + 1], w[3 * a + 2], cx, cy, cz));
-    e.vals[a] = a;
+__global__ void k_wall_keys(Dev e, int n, int slot, int dim, const double* __restrict__ w) {
+  const CaseDev& C = e.cases[slot];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double z = dim == 3 ? w[3 * i + 2] : 0.0;
+    e.keys[i] = static_cast<uint64_t>(C.key_off + local_cell(C, w[dim * i], w[dim * i + 1], z));
+    e.vals[i] = i;
   }
 }
 
-__global__ void k_wall_place(Dev e, const double* __restrict__ w) {
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < e.nw; s += gridDim.x * blockDim.x) {
+__global__ void k_place_walls(Dev e, int begin, int n, int slot, int dim, const double* __restrict__ w,
+                              int ob_begin, int n_ob) {
+  const CaseDev& C = e.cases[slot];
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
     const int o = e.vals[s];
     const int key = static_cast<int>(e.keys[s]);
-    const double m = static_cast<double>(e.wall_mass);
-    st4(e.pos, e.nf + s, make_double4(w[3 * o], w[3 * o + 1], w[3 * o + 2], m));
-    e.home[e.nf + s] = key;
-    e.lp[e.nf + s] = local_of(e, key, w[3 * o], w[3 * o + 1], w[3 * o + 2], m);
-    e.wall_id[s] = o;
-    if (o >= e.nw - e.nob) e.ob_rows[o - (e.nw - e.nob)] = e.nf + s;
+    const int64_t a = static_cast<int64_t>(e.NF) + begin + s;
+    const double m = static_cast<double>(C.wall_mass);
+    const double z = dim == 3 ? w[3 * o + 2] : 0.0;
+    st4(e.pos, a, make_double4(w[dim * o], w[dim * o + 1], z, m));
+    e.home[a] = key;
+    e.cid[a] = slot;
+    e.cnt[a] = 0;
+    e.lp[a] = local_of(C, key - C.key_off, w[dim * o], w[dim * o + 1], z, m);
+    if (o >= n - n_ob) e.ob_rows[ob_begin + (o - (n - n_ob))] = static_cast<int>(a);
   }
 }
 
-__global__ void k_read(Dev e, double* __restrict__ x, double* __restrict__ v, double* __restrict__ rho,
-                       double* __restrict__ p) {
-  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+// After a retire moved the later blocks down by (df fluid, dw wall) rows:
+// shift their row entries, home keys and obstacle rows.
+__global__ void k_remap(Dev e, int fluid_from, int wall_from, int df, int dw, int dkeys, int ob_from) {
+  const int nfl = e.nf - fluid_from, nwl = e.nw - wall_from;
+  const int total = nfl + nwl;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const int64_t a = t < nfl ? fluid_from + t : static_cast<int64_t>(e.NF) + wall_from + (t - nfl);
+    e.home[a] -= dkeys;
+    const int n = e.cnt[a];
+    for (int k = 0; k < n; ++k) {
+      uint32_t& ent = e.nbr[static_cast<int64_t>(k) * e.rows + a];
+      const uint32_t b = ent >> 5;
+      const uint32_t nb = b < static_cast<uint32_t>(e.NF) ? b - df : b - dw;
+      ent = (nb << 5) | (ent & 31u);
+    }
+  }
+  for (int q = ob_from + blockIdx.x * blockDim.x + threadIdx.x; q < e.n_ob; q += gridDim.x * blockDim.x)
+    e.ob_rows[q] -= dw;
+}
+
+__global__ void k_read(Dev e, int begin, int n, int dim, double* __restrict__ x, double* __restrict__ v,
+                       double* __restrict__ rho, double* __restrict__ p) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int a = begin + i;
     const int o = e.id[a];
     const double4 xa = ld4(e.pos, a), va = ld4(e.vel, a);
-    if (x) { x[3 * o] = xa.x; x[3 * o + 1] = xa.y; x[3 * o + 2] = xa.z; }
-    if (v) { v[3 * o] = va.x; v[3 * o + 1] = va.y; v[3 * o + 2] = va.z; }
+    if (x) {
+      x[dim * o] = xa.x;
+      x[dim * o + 1] = xa.y;
+      if (dim == 3) x[3 * o + 2] = xa.z;
+    }
+    if (v) {
+      v[dim * o] = va.x;
+      v[dim * o + 1] = va.y;
+      if (dim == 3) v[3 * o + 2] = va.z;
+    }
     if (rho) rho[o] = e.rho[a];
     if (p) p[o] = e.pr[a];
   }
 }
+
+struct CaseHost {
+  CaseDev dev;
+  tsph_case_params prm;
+  int64_t ncells;
+  int slot;
+};
 
 }  // namespace
 }  // namespace tsph
@@ -902,10 +1061,13 @@ __global__ void k_read(Dev e, double* __restrict__ x, double* __restrict__ v, do
 struct tsph_engine {
   tsph::Dev d;
   tsph_engine_params prm;
-  char* arena;
-  int64_t ncells;
-  char* radix_scratch;
-  int key_bits;
+  char* arena = nullptr;
+  tsph::CaseDev* cases_dev = nullptr;
+  char* radix_scratch = nullptr;
+  std::vector<tsph::CaseHost> order;  // active cases in block order
+  std::vector<int> free_slots;
+  int64_t total_cells = 0;
+  int block = tsph::kBlock;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaStream_t captured_on = nullptr;
@@ -914,96 +1076,109 @@ struct tsph_engine {
 namespace tsph {
 namespace {
 
-struct Plan {
-  int64_t N, ncells;
-  int ncx, ncy, ncz;
-  double cell;
-  int nblocks_int, nblocks_ob;
-};
-
-Plan make_plan(const tsph_engine_params& p) {
-  Plan q{};
-  q.N = p.n_fluid + p.n_wall;
-  q.cell = 2.0 * p.h + p.skin;
-  q.ncx = static_cast<int>(std::ceil((p.grid_hi[0] - p.grid_lo[0]) / q.cell)) + 1;
-  q.ncy = static_cast<int>(std::ceil((p.grid_hi[1] - p.grid_lo[1]) / q.cell)) + 1;
-  q.ncz = static_cast<int>(std::ceil((p.grid_hi[2] - p.grid_lo[2]) / q.cell)) + 1;
-  q.ncells = static_cast<int64_t>(q.ncx) * q.ncy * q.ncz;
-  q.nblocks_int = static_cast<int>(grid_for(p.n_fluid, kBlock, kMaxFinalBlocks));
-  q.nblocks_ob = static_cast<int>(grid_for(std::max<int64_t>(p.n_obstacle, 1), kBlock));
-  return q;
-}
-
 // Carve the arena; with base == nullptr only the size is computed.
-size_t carve(const tsph_engine_params& p, const Plan& q, Dev* d, char* base, char** radix_scratch) {
+size_t carve(const tsph_engine_params& p, Dev* d, char* base, CaseDev** cases, char** radix_scratch) {
   size_t used = 0;
   auto take = [&](size_t bytes) -> void* {
     void* ptr = base ? base + used : nullptr;
     used += align_up(bytes);
     return ptr;
   };
-  const int64_t nf = p.n_fluid, N = q.N;
-  const int64_t nsort = std::max<int64_t>(nf, p.n_wall);
+  const int64_t NF = p.max_fluid, NW = std::max<int64_t>(p.max_wall, 1), N = NF + NW;
+  const int64_t nsort = std::max(NF, NW);
   Dev t{};
+  t.rows = N;
   t.pos = static_cast<double4*>(take(N * sizeof(double4)));
-  t.vel = static_cast<double4*>(take(nf * sizeof(double4)));
-  t.anchor = static_cast<double4*>(take(nf * sizeof(double4)));
+  t.vel = static_cast<double4*>(take(NF * sizeof(double4)));
+  t.anchor = static_cast<double4*>(take(NF * sizeof(double4)));
   t.lp = static_cast<float4*>(take(N * sizeof(float4)));
   t.home = static_cast<int32_t*>(take(N * sizeof(int32_t)));
-  t.id = static_cast<int32_t*>(take(nf * sizeof(int32_t)));
-  t.wall_id = static_cast<int32_t*>(take(std::max<int64_t>(p.n_wall, 1) * sizeof(int32_t)));
+  t.id = static_cast<int32_t*>(take(NF * sizeof(int32_t)));
+  t.cid = static_cast<int32_t*>(take(N * sizeof(int32_t)));
   t.vb = static_cast<float4*>(take(N * sizeof(float4)));
   t.pr = static_cast<float*>(take(N * sizeof(float)));
   t.rho = static_cast<float*>(take(N * sizeof(float)));
   t.pq = static_cast<float*>(take(N * sizeof(float)));
-  t.rs = static_cast<float2*>(take(nf * sizeof(float2)));
-  t.acc = static_cast<float4*>(take(nf * sizeof(float4)));
-  t.conc = static_cast<float*>(take(nf * sizeof(float)));
-  t.gradc = static_cast<float4*>(take(nf * sizeof(float4)));
+  t.rs = static_cast<float2*>(take(NF * sizeof(float2)));
+  t.acc = static_cast<float4*>(take(NF * sizeof(float4)));
+  t.conc = static_cast<float*>(take(NF * sizeof(float)));
+  t.gradc = static_cast<float4*>(take(NF * sizeof(float4)));
   t.nbr = static_cast<uint32_t*>(take(static_cast<size_t>(p.max_neighbors) * N * sizeof(uint32_t)));
   t.cnt = static_cast<int32_t*>(take(N * sizeof(int32_t)));
-  t.ob_rows = static_cast<int32_t*>(take(std::max<int64_t>(p.n_obstacle, 1) * sizeof(int32_t)));
-  t.fstart = static_cast<int32_t*>(take(q.ncells * sizeof(int32_t)));
-  t.fend = static_cast<int32_t*>(take(q.ncells * sizeof(int32_t)));
-  t.wstart = static_cast<int32_t*>(take(q.ncells * sizeof(int32_t)));
-  t.wend = static_cast<int32_t*>(take(q.ncells * sizeof(int32_t)));
+  t.ob_rows = static_cast<int32_t*>(take(std::max<int64_t>(p.max_obstacle, 1) * sizeof(int32_t)));
+  t.fstart = static_cast<int32_t*>(take(p.max_cells * sizeof(int32_t)));
+  t.fend = static_cast<int32_t*>(take(p.max_cells * sizeof(int32_t)));
+  t.wstart = static_cast<int32_t*>(take(p.max_cells * sizeof(int32_t)));
+  t.wend = static_cast<int32_t*>(take(p.max_cells * sizeof(int32_t)));
   t.keys = static_cast<uint64_t*>(take(nsort * sizeof(uint64_t)));
   t.keys_tmp = static_cast<uint64_t*>(take(nsort * sizeof(uint64_t)));
   t.vals = static_cast<int32_t*>(take(nsort * sizeof(int32_t)));
   t.vals_tmp = static_cast<int32_t*>(take(nsort * sizeof(int32_t)));
-  t.tmp4a = static_cast<double4*>(take(nf * sizeof(double4)));
-  t.tmp4b = static_cast<double4*>(take(nf * sizeof(double4)));
-  t.tmp_id = static_cast<int32_t*>(take(nf * sizeof(int32_t)));
-  t.flag = static_cast<int*>(take(16 * sizeof(int)));
-  t.maxbits = static_cast<unsigned long long*>(take(8 * sizeof(unsigned long long)));
+  t.tmp4a = static_cast<double4*>(take(nsort * sizeof(double4)));
+  t.tmp4b = static_cast<double4*>(take(nsort * sizeof(double4)));
+  t.tmp_id = static_cast<int32_t*>(take(nsort * sizeof(int32_t)));
+  t.ctl = static_cast<CaseCtl*>(take(p.max_cases * sizeof(CaseCtl)));
+  t.diag = static_cast<double*>(take(static_cast<size_t>(p.max_cases) * p.diag_ring * kDiag * sizeof(double)));
+  t.any_rebuild = static_cast<int*>(take(sizeof(int)));
   t.status = static_cast<int*>(take(sizeof(int)));
-  t.counters = static_cast<long long*>(take(8 * sizeof(long long)));
-  t.partials = static_cast<double*>(take(static_cast<size_t>(q.nblocks_int + q.nblocks_ob) * 8 * sizeof(double)));
-  t.impulse = static_cast<double*>(take(4 * sizeof(double)));
-  t.diag = static_cast<double*>(take(static_cast<size_t>(p.diag_ring) * kDiag * sizeof(double)));
   t.hist = static_cast<unsigned int*>(take(256 * sizeof(unsigned int)));
   t.sel = static_cast<unsigned long long*>(take(4 * sizeof(unsigned long long)));
-  t.cref = static_cast<double*>(take(4 * sizeof(double)));
+  t.sel_k = static_cast<long long*>(take(sizeof(long long)));
+  CaseDev* cd = static_cast<CaseDev*>(take(p.max_cases * sizeof(CaseDev)));
   char* rs = static_cast<char*>(take(radix_scratch_bytes(nsort)));
+  if (cases) *cases = cd;
   if (radix_scratch) *radix_scratch = rs;
   if (d) *d = t;
   return used + 256;
 }
 
-int enqueue_rebuild(tsph_engine* E, cudaStream_t s) {
+int key_bits(int64_t cells) {
+  int bits = 1;
+  while ((int64_t(1) << bits) < cells) ++bits;
+  return bits;
+}
+
+void invalidate_graph(tsph_engine* E) {
+  if (E->exec) cudaGraphExecDestroy(E->exec);
+  if (E->graph) cudaGraphDestroy(E->graph);
+  E->exec = nullptr;
+  E->graph = nullptr;
+  E->captured_on = nullptr;
+}
+
+bool shifting(const tsph_engine* E) { return E->order.size() == 1 && E->order[0].prm.shift_every > 0; }
+
+// Per-batch fields of the kernel parameters: the shifting slot and, for a
+// batch of one, the case itself.
+void batch_changed(tsph_engine* E) {
+  Dev& d = E->d;
+  d.shift_slot = shifting(E) ? E->order[0].slot : 0;
+  if (E->order.size() == 1) {
+    d.one = E->order[0].dev;
+    d.one_slot = E->order[0].slot;
+  } else {
+    d.one = CaseDev{};
+    d.one_slot = 0;
+  }
+}
+
+int enqueue_rebuild(tsph_engine* E, cudaStream_t s, int pass) {
   Dev& d = E->d;
   const unsigned g = grid_for(d.nf, kBlock);
-  k_check<<<1, 32, 0, s>>>(d);
+  const unsigned gc = grid_for(d.n_slots, 128);
+  TSPH_CUDA_CHECK(cudaMemsetAsync(d.any_rebuild, 0, sizeof(int), s));
+  k_check<<<gc, 128, 0, s>>>(d, pass);
   k_keys<<<g, kBlock, 0, s>>>(d);
   TSPH_LAUNCH_CHECK();
-  int rc = radix_sort_u64_i32(d.keys, d.vals, d.keys_tmp, d.vals_tmp, d.nf, E->key_bits, E->radix_scratch, s,
-                              d.flag);
+  int rc = radix_sort_u64_i32(d.keys, d.vals, d.keys_tmp, d.vals_tmp, d.nf, key_bits(E->total_cells),
+                              E->radix_scratch, s, d.any_rebuild);
   if (rc) return rc;
   k_permute<<<g, kBlock, 0, s>>>(d);
   k_permute_back<<<g, kBlock, 0, s>>>(d);
-  k_clear_table<<<grid_for(E->ncells, 256), 256, 0, s>>>(d.fstart, d.fend, E->ncells, d.flag);
-  k_fill_table<<<g, kBlock, 0, s>>>(d.keys, d.nf, d.fstart, d.fend, d.flag);
-  k_rows<<<grid_for(d.N, kBlock), kBlock, 0, s>>>(d);
+  k_clear_table<<<grid_for(E->total_cells, 256), 256, 0, s>>>(d.fstart, d.fend, E->total_cells, d.any_rebuild);
+  k_fill_table<<<g, kBlock, 0, s>>>(nullptr, d.keys, d.nf, d.fstart, d.fend, d.any_rebuild);
+  k_rows<<<grid_for(d.nf + d.nw, kBlock), kBlock, 0, s>>>(d);
+  k_rebuilt<<<gc, 128, 0, s>>>(d);
   TSPH_LAUNCH_CHECK();
   return TSPH_OK;
 }
@@ -1020,32 +1195,36 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr) {
     if (marks) cudaEventRecord(marks[stage], s);
     ++stage;
   };
-  int rc = enqueue_rebuild(E, s);
+  if (d.nf == 0) return TSPH_OK;
+  int rc = enqueue_rebuild(E, s, 0);
   if (rc) return rc;
+  const unsigned gc = grid_for(d.n_slots, 128);
+  k_step_begin<<<gc, 128, 0, s>>>(d);
   mark();
-  const unsigned g = grid_for(d.nf, kBlock);
-  k_density<<<g, kBlock, 0, s>>>(d);
+  const int B = E->block;
+  const unsigned g = grid_for(d.nf, B);
+  const bool one = E->order.size() == 1;
+  (one ? k_density<true> : k_density<false>)<<<g, B, 0, s>>>(d);
   mark();
-  k_diffusion_eos<<<g, kBlock, 0, s>>>(d);
+  (one ? k_diffusion_eos<true> : k_diffusion_eos<false>)<<<g, B, 0, s>>>(d);
   mark();
-  if (d.nw) k_walls<<<grid_for(d.nw, kBlock), kBlock, 0, s>>>(d);
+  if (d.nw) (one ? k_walls<true> : k_walls<false>)<<<grid_for(d.nw, B), B, 0, s>>>(d);
   mark();
-  k_force<<<g, kBlock, 0, s>>>(d);
+  (one ? k_force<true> : k_force<false>)<<<g, B, 0, s>>>(d);
   mark();
-  k_reaction<<<d.nblocks_ob, kBlock, 0, s>>>(d);
+  if (d.n_ob) k_reaction<<<static_cast<unsigned>((d.n_ob + B - 1) / B), B, 0, s>>>(d);
   mark();
-  TSPH_CUDA_CHECK(cudaMemsetAsync(d.maxbits, 0, 2 * sizeof(unsigned long long), s));
-  k_integrate<<<d.nblocks_int, kBlock, 0, s>>>(d);
-  k_finalize<<<1, 32, 0, s>>>(d);
+  (one ? k_integrate<true> : k_integrate<false>)<<<static_cast<unsigned>((d.nf + B - 1) / B), B, 0, s>>>(d);
+  k_finalize<<<gc, 128, 0, s>>>(d);
   TSPH_LAUNCH_CHECK();
   mark();
-  if (d.shift_every > 0) {
-    rc = enqueue_rebuild(E, s);
+  if (shifting(E)) {
+    rc = enqueue_rebuild(E, s, 1);
     if (rc) return rc;
     mark();
-    k_concentration<<<g, kBlock, 0, s>>>(d);
+    k_concentration<<<g, B, 0, s>>>(d);
     mark();
-    k_conc_gradient<<<g, kBlock, 0, s>>>(d);
+    k_conc_gradient<<<g, B, 0, s>>>(d);
     mark();
     const double pos = 0.95 * static_cast<double>(d.nf - 1);
     const long long lo = static_cast<long long>(std::floor(pos)), hi = static_cast<long long>(std::ceil(pos));
@@ -1058,11 +1237,103 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr) {
     }
     k_select_finish<<<1, 32, 0, s>>>(d, pos - static_cast<double>(lo));
     mark();
-    k_shift_apply<<<g, kBlock, 0, s>>>(d);
+    k_shift_apply<<<g, B, 0, s>>>(d);
     TSPH_LAUNCH_CHECK();
     mark();
   }
   return TSPH_OK;
+}
+
+CaseDev make_case_dev(const tsph_case_params& p, int64_t* ncells) {
+  CaseDev c{};
+  const double cell = 2.0 * p.h + p.skin;
+  c.cell = cell;
+  c.cellf = static_cast<float>(cell);
+  for (int k = 0; k < 3; ++k) c.origin[k] = p.grid_lo[k];
+  const int64_t nx = static_cast<int64_t>(std::ceil((p.grid_hi[0] - p.grid_lo[0]) / cell)) + 1;
+  const int64_t ny = static_cast<int64_t>(std::ceil((p.grid_hi[1] - p.grid_lo[1]) / cell)) + 1;
+  const int64_t nz = p.dim == 3 ? static_cast<int64_t>(std::ceil((p.grid_hi[2] - p.grid_lo[2]) / cell)) + 1 : 1;
+  if (p.dim == 2) c.origin[2] = -0.5 * cell;
+  *ncells = nx * ny * nz;
+  c.ncx = static_cast<int>(nx);
+  c.ncy = static_cast<int>(ny);
+  c.ncz = static_cast<int>(nz);
+  c.rc2 = cell * cell;
+  c.skin_half = 0.5 * p.skin;
+  c.dt = p.dt;
+  c.gravity = p.gravity;
+  for (int k = 0; k < 3; ++k) {
+    c.box_hi[k] = (p.dim == 2 && k == 2) ? 0.0 : p.box_hi[k];
+    c.ob_lo[k] = p.ob_lo[k];
+    c.ob_hi[k] = p.ob_hi[k];
+  }
+  c.tol = p.tolerance;
+  c.ob_eps = p.ob_eps;
+  c.has_ob = (p.has_obstacle && p.dim == 3) ? 1 : 0;
+  c.shift_every = static_cast<int>(p.shift_every);
+  c.shift_strength_h_dt = p.shift_strength * p.h * p.dt;
+  c.shift_cap = p.shift_limit * p.h;
+  c.shift_fs = p.shift_free_surface;
+  c.vref_floor = p.shift_vref_floor;
+  c.inv_h = static_cast<float>(1.0 / p.h);
+  c.sigma = static_cast<float>(p.dim == 3 ? 1.0 / (M_PI * p.h * p.h * p.h) : 10.0 / (7.0 * M_PI * p.h * p.h));
+  c.sig2d = static_cast<float>(10.0 / (7.0 * M_PI * p.h * p.h));
+  c.rho0 = static_cast<float>(p.rho0);
+  c.bulk = static_cast<float>(p.rho0 * p.sound_speed * p.sound_speed / p.gamma);
+  c.gamma = static_cast<float>(p.gamma);
+  c.inv_gamma = static_cast<float>(1.0 / p.gamma);
+  c.grav = static_cast<float>(p.gravity);
+  c.nu2 = static_cast<float>(2.0 * p.viscosity);
+  c.nu2f = static_cast<float>(2.0 * p.viscosity * p.wall_friction);
+  c.dscale = static_cast<float>(p.diffusion_scale);
+  c.dtf = static_cast<float>(p.dt);
+  c.visc_eps = static_cast<float>(0.01 * p.h * p.h);
+  c.rho_floor = static_cast<float>(0.1 * p.rho0);
+  c.wall_mass = static_cast<float>(p.wall_mass);
+  return c;
+}
+
+bool case_params_ok(const tsph_case_params* p) {
+  if (!p || (p->dim != 2 && p->dim != 3) || p->n_fluid <= 0 || p->n_wall < 0 || p->n_obstacle < 0 ||
+      p->n_obstacle > p->n_wall || p->shift_every < 0)
+    return false;
+  if (!(p->h > 0) || !(p->dt > 0) || !(p->skin >= 0) || !(p->rho0 > 0) || !(p->gamma > 0) ||
+      !(p->sound_speed > 0))
+    return false;
+  for (int k = 0; k < p->dim; ++k)
+    if (!(p->grid_hi[k] >= p->grid_lo[k]) || !std::isfinite(p->grid_lo[k]) || !std::isfinite(p->grid_hi[k]))
+      return false;
+  return true;
+}
+
+// Move rows [src, src + n) to [dst, dst + n) (dst < src, may overlap) through
+// a staging buffer.
+int move_down(void* base, size_t elem, int64_t dst, int64_t src, int64_t n, void* stage, size_t stage_bytes,
+              cudaStream_t s) {
+  if (n <= 0 || dst == src) return TSPH_OK;
+  char* b = static_cast<char*>(base);
+  const int64_t chunk = std::max<int64_t>(1, static_cast<int64_t>(stage_bytes / elem));
+  for (int64_t off = 0; off < n; off += chunk) {
+    const int64_t m = std::min(chunk, n - off);
+    TSPH_CUDA_CHECK(cudaMemcpyAsync(stage, b + (src + off) * elem, m * elem, cudaMemcpyDeviceToDevice, s));
+    TSPH_CUDA_CHECK(cudaMemcpyAsync(b + (dst + off) * elem, stage, m * elem, cudaMemcpyDeviceToDevice, s));
+  }
+  return TSPH_OK;
+}
+
+int refresh_wall_table(tsph_engine* E, cudaStream_t s) {
+  Dev& d = E->d;
+  if (E->total_cells > 0)
+    k_clear_table<<<grid_for(E->total_cells, 256), 256, 0, s>>>(d.wstart, d.wend, E->total_cells, nullptr);
+  if (d.nw) k_fill_table<<<grid_for(d.nw, 256), 256, 0, s>>>(d.home + d.NF, nullptr, d.nw, d.wstart, d.wend, nullptr);
+  TSPH_LAUNCH_CHECK();
+  return TSPH_OK;
+}
+
+const CaseHost* find_case(const tsph_engine* E, int64_t id) {
+  for (const CaseHost& c : E->order)
+    if (c.slot == id) return &c;
+  return nullptr;
 }
 
 }  // namespace
@@ -1073,129 +1344,194 @@ using namespace tsph;
 extern "C" {
 
 int64_t tsph_engine_bytes(const tsph_engine_params* prm) {
-  if (!prm || prm->n_fluid <= 0 || prm->n_wall < 0 || prm->max_neighbors <= 0) return -1;
-  Plan q = make_plan(*prm);
-  return static_cast<int64_t>(carve(*prm, q, nullptr, nullptr, nullptr));
+  if (!prm || prm->max_fluid <= 0 || prm->max_wall < 0 || prm->max_obstacle < 0 || prm->max_neighbors <= 0 ||
+      prm->max_cases <= 0 || prm->max_cells <= 0 || prm->diag_ring <= 0)
+    return -1;
+  return static_cast<int64_t>(carve(*prm, nullptr, nullptr, nullptr, nullptr));
 }
 
-int tsph_engine_create(const tsph_engine_params* prm, void* arena, int64_t arena_bytes, const double* x,
-                       const double* v, const double* mass, const double* wall, tsph_stream stream,
+int64_t tsph_engine_case_cells(const tsph_case_params* prm) {
+  if (!case_params_ok(prm)) return -1;
+  int64_t n = 0;
+  make_case_dev(*prm, &n);
+  return n;
+}
+
+int tsph_engine_create(const tsph_engine_params* prm, void* arena, int64_t arena_bytes, tsph_stream stream,
                        tsph_engine** out) {
   if (!prm || !out || !arena) return TSPH_ERR_ARG;
-  // row entries pack the neighbour index into 27 bits
-  if (prm->n_fluid <= 0 || prm->n_wall < 0 || prm->n_obstacle < 0 || prm->n_obstacle > prm->n_wall ||
-      prm->n_fluid + prm->n_wall >= (int64_t(1) << 27) || prm->max_neighbors <= 0 || prm->diag_ring <= 0)
+  const int64_t bytes = tsph_engine_bytes(prm);
+  if (bytes < 0 || prm->max_fluid + std::max<int64_t>(prm->max_wall, 1) > kMaxRows ||
+      prm->max_cells >= (int64_t(1) << 31) || prm->max_obstacle > prm->max_wall)
     return TSPH_ERR_ARG;
-  if (arena_bytes < tsph_engine_bytes(prm)) return TSPH_ERR_WORKSPACE;
+  if (arena_bytes < bytes) return TSPH_ERR_WORKSPACE;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   tsph_engine* E = new (std::nothrow) tsph_engine();
   if (!E) return TSPH_ERR_ARG;
   E->prm = *prm;
   E->arena = static_cast<char*>(arena);
-  Plan q = make_plan(*prm);
-  E->ncells = q.ncells;
-  carve(*prm, q, &E->d, E->arena, &E->radix_scratch);
-  int bits = 0;
-  while ((int64_t(1) << bits) < q.ncells) ++bits;
-  E->key_bits = bits;
+  carve(*prm, &E->d, E->arena, &E->cases_dev, &E->radix_scratch);
   Dev& d = E->d;
-  d.nf = static_cast<int>(prm->n_fluid);
-  d.nw = static_cast<int>(prm->n_wall);
-  d.N = static_cast<int>(q.N);
-  d.nob = static_cast<int>(prm->n_obstacle);
+  d.NF = static_cast<int>(prm->max_fluid);
+  d.nf = d.nw = d.n_ob = 0;
+  d.n_slots = static_cast<int>(prm->max_cases);
   d.maxnb = static_cast<int>(prm->max_neighbors);
-  d.shift_every = static_cast<int>(prm->shift_every);
   d.diag_ring = static_cast<int>(prm->diag_ring);
-  d.ncx = q.ncx; d.ncy = q.ncy; d.ncz = q.ncz;
-  for (int k = 0; k < 3; ++k) {
-    d.origin[k] = prm->grid_lo[k];
-    d.box_hi[k] = prm->box_hi[k];
-    d.ob_lo[k] = prm->ob_lo[k];
-    d.ob_hi[k] = prm->ob_hi[k];
-  }
-  d.cell = q.cell;
-  d.cellf = static_cast<float>(q.cell);
-  const double rc = 2.0 * prm->h + prm->skin;
-  d.rc2 = rc * rc;
-  d.skin_half = 0.5 * prm->skin;
-  d.dt = prm->dt;
-  d.tol = prm->tolerance;
-  d.ob_eps = prm->ob_eps;
-  d.has_ob = static_cast<int>(prm->has_obstacle);
-  d.gravity = prm->gravity;
-  d.h = static_cast<float>(prm->h);
-  d.inv_h = static_cast<float>(1.0 / prm->h);
-  d.sigma = static_cast<float>(1.0 / (M_PI * prm->h * prm->h * prm->h));
-  d.sig2d = static_cast<float>(10.0 / (7.0 * M_PI * prm->h * prm->h));
-  d.support2 = static_cast<float>(4.0 * prm->h * prm->h);
-  d.rho0 = static_cast<float>(prm->rho0);
-  d.bulk = static_cast<float>(prm->rho0 * prm->sound_speed * prm->sound_speed / prm->gamma);
-  d.gamma = static_cast<float>(prm->gamma);
-  d.inv_gamma = static_cast<float>(1.0 / prm->gamma);
-  d.grav = static_cast<float>(prm->gravity);
-  d.nu2 = static_cast<float>(2.0 * prm->viscosity);
-  d.nu2f = static_cast<float>(2.0 * prm->viscosity * prm->wall_friction);
-  d.dscale = static_cast<float>(prm->diffusion_scale);
-  d.dtf = static_cast<float>(prm->dt);
-  d.visc_eps = static_cast<float>(0.01 * prm->h * prm->h);
-  d.rho_floor = static_cast<float>(0.1 * prm->rho0);
-  d.wall_mass = static_cast<float>(prm->wall_mass);
-  d.shift_strength_h_dt = prm->shift_strength * prm->h * prm->dt;
-  d.shift_cap = prm->shift_limit * prm->h;
-  d.shift_fs = prm->shift_free_surface;
-  d.vref_floor = prm->shift_vref_floor;
-  d.nblocks_int = q.nblocks_int;
-  d.nblocks_ob = q.nblocks_ob;
-
-  int rc_ = TSPH_OK;
-  do {
-    if (cudaMemsetAsync(d.flag, 0, 16 * sizeof(int), s) != cudaSuccess ||
-        cudaMemsetAsync(d.maxbits, 0, 8 * sizeof(unsigned long long), s) != cudaSuccess ||
-        cudaMemsetAsync(d.status, 0, sizeof(int), s) != cudaSuccess ||
-        cudaMemsetAsync(d.counters, 0, 8 * sizeof(long long), s) != cudaSuccess ||
-        cudaMemsetAsync(d.impulse, 0, 4 * sizeof(double), s) != cudaSuccess ||
-        cudaMemsetAsync(d.hist, 0, 256 * sizeof(unsigned int), s) != cudaSuccess ||
-        cudaMemsetAsync(d.cref, 0, 4 * sizeof(double), s) != cudaSuccess ||
-        cudaMemsetAsync(d.diag, 0, static_cast<size_t>(d.diag_ring) * kDiag * sizeof(double), s) != cudaSuccess ||
-        cudaMemsetAsync(d.cnt, 0, static_cast<size_t>(d.N) * sizeof(int32_t), s) != cudaSuccess) {
-      rc_ = TSPH_ERR_CUDA;
-      break;
-    }
-    const int one = 1;
-    if (cudaMemcpyAsync(d.flag + 1, &one, sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess) {
-      rc_ = TSPH_ERR_CUDA;
-      break;
-    }
-    k_init_fluid<<<grid_for(d.nf, kBlock), kBlock, 0, s>>>(d, x, v, mass);
-    if (d.nw) {
-      k_wall_keys<<<grid_for(d.nw, kBlock), kBlock, 0, s>>>(d, wall);
-      rc_ = radix_sort_u64_i32(d.keys, d.vals, d.keys_tmp, d.vals_tmp, d.nw, E->key_bits, E->radix_scratch, s);
-      if (rc_) break;
-      k_wall_place<<<grid_for(d.nw, kBlock), kBlock, 0, s>>>(d, wall);
-      k_clear_table<<<grid_for(E->ncells, 256), 256, 0, s>>>(d.wstart, d.wend, E->ncells, nullptr);
-      k_fill_table<<<grid_for(d.nw, kBlock), kBlock, 0, s>>>(d.keys, d.nw, d.wstart, d.wend, nullptr);
-    } else {
-      k_clear_table<<<grid_for(E->ncells, 256), 256, 0, s>>>(d.wstart, d.wend, E->ncells, nullptr);
-    }
-    if (cudaGetLastError() != cudaSuccess) rc_ = TSPH_ERR_CUDA;
-  } while (0);
-  // Positions arrive in the caller's (host) byte order and may be pageable:
-  // make sure the copies above finished before the caller's buffers go away.
-  if (rc_ == TSPH_OK && cudaStreamSynchronize(s) != cudaSuccess) rc_ = TSPH_ERR_CUDA;
-  if (rc_) {
+  d.shift_slot = 0;
+  d.one_slot = 0;
+  d.cases = E->cases_dev;
+  for (int64_t c = prm->max_cases - 1; c >= 0; --c) E->free_slots.push_back(static_cast<int>(c));
+  if (cudaMemsetAsync(d.ctl, 0, prm->max_cases * sizeof(CaseCtl), s) != cudaSuccess ||
+      cudaMemsetAsync(d.status, 0, sizeof(int), s) != cudaSuccess ||
+      cudaMemsetAsync(d.hist, 0, 256 * sizeof(unsigned int), s) != cudaSuccess ||
+      cudaMemsetAsync(E->cases_dev, 0, prm->max_cases * sizeof(CaseDev), s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess) {
     delete E;
-    return rc_;
+    return TSPH_ERR_CUDA;
   }
   *out = E;
+  return TSPH_OK;
+}
+
+int tsph_engine_add_case(tsph_engine* E, const tsph_case_params* p, const double* x, const double* v,
+                         const double* mass, const double* wall, tsph_stream stream, int64_t* case_id) {
+  if (!E || !x || !v || !mass || !case_id || !case_params_ok(p) || (p->n_wall > 0 && !wall)) return TSPH_ERR_ARG;
+  // shifting needs the whole batch (its reference concentration is a global quantile)
+  if (p->shift_every > 0 && !E->order.empty()) return TSPH_ERR_UNSUPPORTED;
+  if (shifting(E)) return TSPH_ERR_UNSUPPORTED;
+  if (E->free_slots.empty()) return TSPH_ERR_CAPACITY;
+  Dev& d = E->d;
+  int64_t ncells = 0;
+  CaseDev c = make_case_dev(*p, &ncells);
+  if (d.nf + p->n_fluid > E->prm.max_fluid || d.nw + p->n_wall > E->prm.max_wall ||
+      d.n_ob + p->n_obstacle > E->prm.max_obstacle || E->total_cells + ncells > E->prm.max_cells)
+    return TSPH_ERR_CAPACITY;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const int slot = E->free_slots.back();
+  c.key_off = static_cast<int>(E->total_cells);
+  c.fluid_begin = d.nf;
+  c.n_fluid = static_cast<int>(p->n_fluid);
+  c.wall_begin = d.nw;
+  c.n_wall = static_cast<int>(p->n_wall);
+  c.ob_begin = d.n_ob;
+  c.n_ob = static_cast<int>(p->n_obstacle);
+  TSPH_CUDA_CHECK(cudaMemcpyAsync(E->cases_dev + slot, &c, sizeof(CaseDev), cudaMemcpyHostToDevice, s));
+  CaseCtl ctl{};
+  ctl.first = 1;
+  ctl.active = 1;
+  TSPH_CUDA_CHECK(cudaMemcpyAsync(d.ctl + slot, &ctl, sizeof(CaseCtl), cudaMemcpyHostToDevice, s));
+  TSPH_CUDA_CHECK(cudaMemsetAsync(d.diag + static_cast<int64_t>(slot) * d.diag_ring * kDiag, 0,
+                                  static_cast<size_t>(d.diag_ring) * kDiag * sizeof(double), s));
+  const int dim = static_cast<int>(p->dim);
+  k_place_fluid<<<grid_for(p->n_fluid, kBlock), kBlock, 0, s>>>(d, d.nf, static_cast<int>(p->n_fluid), slot, dim,
+                                                                 x, v, mass);
+  TSPH_LAUNCH_CHECK();
+  if (p->n_wall > 0) {
+    k_wall_keys<<<grid_for(p->n_wall, kBlock), kBlock, 0, s>>>(d, static_cast<int>(p->n_wall), slot, dim, wall);
+    TSPH_LAUNCH_CHECK();
+    int rc = radix_sort_u64_i32(d.keys, d.vals, d.keys_tmp, d.vals_tmp, p->n_wall,
+                                key_bits(E->total_cells + ncells), E->radix_scratch, s);
+    if (rc) return rc;
+    k_place_walls<<<grid_for(p->n_wall, kBlock), kBlock, 0, s>>>(d, d.nw, static_cast<int>(p->n_wall), slot, dim,
+                                                                  wall, d.n_ob, static_cast<int>(p->n_obstacle));
+    TSPH_LAUNCH_CHECK();
+  }
+  CaseHost h{};
+  h.dev = c;
+  h.prm = *p;
+  h.ncells = ncells;
+  h.slot = slot;
+  E->order.push_back(h);
+  E->free_slots.pop_back();
+  E->total_cells += ncells;
+  d.nf += static_cast<int>(p->n_fluid);
+  d.nw += static_cast<int>(p->n_wall);
+  d.n_ob += static_cast<int>(p->n_obstacle);
+  batch_changed(E);
+  int rc = refresh_wall_table(E, s);
+  if (rc) return rc;
+  invalidate_graph(E);
+  // the caller's buffers may be released as soon as this returns
+  TSPH_CUDA_CHECK(cudaStreamSynchronize(s));
+  *case_id = slot;
+  return TSPH_OK;
+}
+
+int tsph_engine_remove_case(tsph_engine* E, int64_t case_id, tsph_stream stream) {
+  if (!E) return TSPH_ERR_ARG;
+  size_t idx = 0;
+  while (idx < E->order.size() && E->order[idx].slot != case_id) ++idx;
+  if (idx == E->order.size()) return TSPH_ERR_ARG;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  Dev& d = E->d;
+  const CaseHost gone = E->order[idx];
+  const int64_t fb = gone.dev.fluid_begin, nfc = gone.dev.n_fluid, fe = fb + nfc;
+  const int64_t wb = gone.dev.wall_begin, nwc = gone.dev.n_wall, we = wb + nwc;
+  const int64_t ob = gone.dev.ob_begin, nob = gone.dev.n_ob;
+  const int64_t ftail = d.nf - fe, wtail = d.nw - we, otail = d.n_ob - (ob + nob);
+  const int64_t W0 = d.NF;
+  void* stage = d.tmp4a;
+  const size_t stage_bytes = static_cast<size_t>(std::max(E->prm.max_fluid, std::max<int64_t>(E->prm.max_wall, 1))) *
+                             sizeof(double4);
+  struct Arr {
+    void* p;
+    size_t e;
+  };
+  const Arr fluid_arrays[] = {{d.pos, sizeof(double4)}, {d.vel, sizeof(double4)}, {d.anchor, sizeof(double4)},
+                              {d.lp, sizeof(float4)},   {d.home, sizeof(int32_t)}, {d.id, sizeof(int32_t)},
+                              {d.cid, sizeof(int32_t)}, {d.vb, sizeof(float4)},    {d.pr, sizeof(float)},
+                              {d.rho, sizeof(float)},   {d.pq, sizeof(float)},     {d.rs, sizeof(float2)},
+                              {d.acc, sizeof(float4)},  {d.cnt, sizeof(int32_t)}};
+  const Arr wall_arrays[] = {{d.pos, sizeof(double4)}, {d.lp, sizeof(float4)}, {d.home, sizeof(int32_t)},
+                             {d.cid, sizeof(int32_t)},  {d.vb, sizeof(float4)}, {d.pr, sizeof(float)},
+                             {d.rho, sizeof(float)},    {d.pq, sizeof(float)},  {d.cnt, sizeof(int32_t)}};
+  int rc = TSPH_OK;
+  for (const Arr& a : fluid_arrays)
+    if ((rc = move_down(a.p, a.e, fb, fe, ftail, stage, stage_bytes, s))) return rc;
+  for (const Arr& a : wall_arrays)
+    if ((rc = move_down(a.p, a.e, W0 + wb, W0 + we, wtail, stage, stage_bytes, s))) return rc;
+  for (int k = 0; k < d.maxnb; ++k) {
+    uint32_t* col = d.nbr + static_cast<int64_t>(k) * d.rows;
+    if ((rc = move_down(col, sizeof(uint32_t), fb, fe, ftail, stage, stage_bytes, s))) return rc;
+    if ((rc = move_down(col, sizeof(uint32_t), W0 + wb, W0 + we, wtail, stage, stage_bytes, s))) return rc;
+  }
+  if ((rc = move_down(d.ob_rows, sizeof(int32_t), ob, ob + nob, otail, stage, stage_bytes, s))) return rc;
+  CaseCtl off{};
+  TSPH_CUDA_CHECK(cudaMemcpyAsync(d.ctl + gone.slot, &off, sizeof(CaseCtl), cudaMemcpyHostToDevice, s));
+  // later cases move down in rows and keys
+  E->order.erase(E->order.begin() + static_cast<int64_t>(idx));
+  for (size_t k = idx; k < E->order.size(); ++k) {
+    CaseDev& c = E->order[k].dev;
+    c.fluid_begin -= static_cast<int>(nfc);
+    c.wall_begin -= static_cast<int>(nwc);
+    c.ob_begin -= static_cast<int>(nob);
+    c.key_off -= static_cast<int>(gone.ncells);
+    TSPH_CUDA_CHECK(cudaMemcpyAsync(E->cases_dev + E->order[k].slot, &c, sizeof(CaseDev), cudaMemcpyHostToDevice, s));
+  }
+  d.nf -= static_cast<int>(nfc);
+  d.nw -= static_cast<int>(nwc);
+  d.n_ob -= static_cast<int>(nob);
+  E->total_cells -= gone.ncells;
+  if (ftail + wtail + otail > 0) {
+    k_remap<<<grid_for(ftail + wtail + otail, kBlock), kBlock, 0, s>>>(
+        d, static_cast<int>(fb), static_cast<int>(wb), static_cast<int>(nfc), static_cast<int>(nwc),
+        static_cast<int>(gone.ncells), static_cast<int>(ob));
+    TSPH_LAUNCH_CHECK();
+  }
+  E->free_slots.push_back(gone.slot);
+  batch_changed(E);
+  if ((rc = refresh_wall_table(E, s))) return rc;
+  invalidate_graph(E);
+  TSPH_CUDA_CHECK(cudaStreamSynchronize(s));
   return TSPH_OK;
 }
 
 int tsph_engine_step(tsph_engine* E, int64_t steps, tsph_stream stream) {
   if (!E || steps < 0) return TSPH_ERR_ARG;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (E->order.empty()) return TSPH_OK;
   if (!E->exec || E->captured_on != s) {
-    if (E->exec) { cudaGraphExecDestroy(E->exec); E->exec = nullptr; }
-    if (E->graph) { cudaGraphDestroy(E->graph); E->graph = nullptr; }
+    invalidate_graph(E);
     TSPH_CUDA_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     int rc = enqueue_step(E, s);
     cudaGraph_t g = nullptr;
@@ -1225,12 +1561,13 @@ int tsph_engine_step_eager(tsph_engine* E, int64_t steps, tsph_stream stream) {
 
 int tsph_engine_step_timed(tsph_engine* E, tsph_stream stream, float* stage_ms, int64_t* stages) {
   if (!E || !stage_ms || !stages) return TSPH_ERR_ARG;
+  if (E->order.empty()) return TSPH_ERR_ARG;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   cudaEvent_t ev[kStages + 1];
   for (int i = 0; i <= kStages; ++i) TSPH_CUDA_CHECK(cudaEventCreate(&ev[i]));
   TSPH_CUDA_CHECK(cudaEventRecord(ev[0], s));
   int rc = enqueue_step(E, s, ev + 1);
-  const int n = E->d.shift_every > 0 ? kStages : 7;
+  const int n = shifting(E) ? kStages : 7;
   if (rc == TSPH_OK) {
     if (cudaEventSynchronize(ev[n]) != cudaSuccess) rc = TSPH_ERR_CUDA;
     for (int i = 0; i < n && rc == TSPH_OK; ++i)
@@ -1247,61 +1584,88 @@ int tsph_engine_graph_kernels(tsph_engine* E, int64_t* kernels) {
   if (!E->graph) return TSPH_ERR_ARG;
   size_t count = 0;
   TSPH_CUDA_CHECK(cudaGraphGetNodes(E->graph, nullptr, &count));
-  cudaGraphNode_t* nodes = new (std::nothrow) cudaGraphNode_t[count];
-  if (!nodes) return TSPH_ERR_ARG;
-  if (cudaGraphGetNodes(E->graph, nodes, &count) != cudaSuccess) {
-    delete[] nodes;
-    return TSPH_ERR_CUDA;
-  }
+  std::vector<cudaGraphNode_t> nodes(count);
+  TSPH_CUDA_CHECK(cudaGraphGetNodes(E->graph, nodes.data(), &count));
   int64_t k = 0;
   for (size_t i = 0; i < count; ++i) {
     cudaGraphNodeType t;
     if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++k;
   }
-  delete[] nodes;
   *kernels = k;
   return TSPH_OK;
 }
 
-int tsph_engine_read(tsph_engine* E, double* x, double* v, double* rho, double* p, tsph_stream stream) {
+int tsph_engine_read(tsph_engine* E, int64_t case_id, double* x, double* v, double* rho, double* p,
+                     tsph_stream stream) {
   if (!E) return TSPH_ERR_ARG;
+  const CaseHost* c = find_case(E, case_id);
+  if (!c) return TSPH_ERR_ARG;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  k_read<<<grid_for(E->d.nf, 256), 256, 0, s>>>(E->d, x, v, rho, p);
+  k_read<<<grid_for(c->dev.n_fluid, 256), 256, 0, s>>>(E->d, c->dev.fluid_begin, c->dev.n_fluid,
+                                                      static_cast<int>(c->prm.dim), x, v, rho, p);
   TSPH_LAUNCH_CHECK();
   return TSPH_OK;
 }
 
-int tsph_engine_diag(tsph_engine* E, double* out, int64_t first, int64_t count, tsph_stream stream) {
-  if (!E || count < 0 || count > E->d.diag_ring) return TSPH_ERR_ARG;
+int tsph_engine_diag(tsph_engine* E, int64_t case_id, double* out, int64_t first, int64_t count,
+                     tsph_stream stream) {
+  if (!E || count < 0 || count > E->d.diag_ring || first < 0) return TSPH_ERR_ARG;
+  if (!find_case(E, case_id)) return TSPH_ERR_ARG;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  for (int64_t i = 0; i < count; ++i) {
-    const int64_t slot = (first + i) % E->d.diag_ring;
-    TSPH_CUDA_CHECK(cudaMemcpyAsync(out + i * kDiag, E->d.diag + slot * kDiag, kDiag * sizeof(double),
+  const double* ring = E->d.diag + case_id * E->d.diag_ring * kDiag;
+  int64_t done = 0;
+  while (done < count) {
+    const int64_t slot = (first + done) % E->d.diag_ring;
+    const int64_t run = std::min(count - done, E->d.diag_ring - slot);
+    TSPH_CUDA_CHECK(cudaMemcpyAsync(out + done * kDiag, ring + slot * kDiag, run * kDiag * sizeof(double),
                                     cudaMemcpyDeviceToDevice, s));
+    done += run;
   }
   return TSPH_OK;
 }
 
-int tsph_engine_status(tsph_engine* E, int64_t* counters, tsph_stream stream) {
+int tsph_engine_status(tsph_engine* E, int64_t case_id, int64_t* counters, tsph_stream stream) {
   if (!E || !counters) return TSPH_ERR_ARG;
+  if (!find_case(E, case_id)) return TSPH_ERR_ARG;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  long long c[8];
-  int st = 0;
-  TSPH_CUDA_CHECK(cudaMemcpyAsync(c, E->d.counters, sizeof(c), cudaMemcpyDeviceToHost, s));
-  TSPH_CUDA_CHECK(cudaMemcpyAsync(&st, E->d.status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CaseCtl t;
+  TSPH_CUDA_CHECK(cudaMemcpyAsync(&t, E->d.ctl + case_id, sizeof(CaseCtl), cudaMemcpyDeviceToHost, s));
   TSPH_CUDA_CHECK(cudaStreamSynchronize(s));
-  for (int k = 0; k < 6; ++k) counters[k] = c[k];
-  counters[6] = st;
+  counters[0] = static_cast<int64_t>(t.escapes);
+  counters[1] = static_cast<int64_t>(t.clamps);
+  counters[2] = static_cast<int64_t>(t.rebuilds);
+  counters[3] = static_cast<int64_t>(t.steps);
+  counters[4] = static_cast<int64_t>(t.row_max);
+  counters[5] = 0;
+  counters[6] = t.status;
   counters[7] = 0;
-  if (st & 2) return TSPH_ERR_STATE;
-  if (st & 1) return TSPH_ERR_CAPACITY;
+  if (t.status & 2) return TSPH_ERR_STATE;
+  if (t.status & 1) return TSPH_ERR_CAPACITY;
+  return TSPH_OK;
+}
+
+int tsph_engine_usage(const tsph_engine* E, int64_t* usage) {
+  if (!E || !usage) return TSPH_ERR_ARG;
+  usage[0] = E->d.nf;
+  usage[1] = E->d.nw;
+  usage[2] = E->d.n_ob;
+  usage[3] = E->total_cells;
+  usage[4] = static_cast<int64_t>(E->order.size());
+  return TSPH_OK;
+}
+
+int tsph_engine_set_block(tsph_engine* E, int64_t threads) {
+  if (!E || (threads != 64 && threads != 128 && threads != 256)) return TSPH_ERR_ARG;
+  if (threads != E->block) {
+    E->block = static_cast<int>(threads);
+    invalidate_graph(E);
+  }
   return TSPH_OK;
 }
 
 int tsph_engine_destroy(tsph_engine* E) {
   if (!E) return TSPH_OK;
-  if (E->exec) cudaGraphExecDestroy(E->exec);
-  if (E->graph) cudaGraphDestroy(E->graph);
+  invalidate_graph(E);
   delete E;
   return TSPH_OK;
 }

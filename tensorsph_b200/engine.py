@@ -1,16 +1,23 @@
-"""Device-resident 3-D dam-break engine (``csrc/engine.cu``) and its case drivers.
+"""Device-resident multi-case engine (``csrc/engine.cu``) and its case drivers.
 
-``DamBreak3DEngine`` owns one GPU-resident case: FP64 positions, velocities
-and meters, cell-sorted particles, a skin-cached neighbour list rebuilt on the
-device, and one CUDA graph per step (rebuild check, density, Molteni
-diffusion, Tait, Adami walls, force, obstacle reaction, semi-implicit Euler
-with the box and obstacle clamps, optional Lind shift).
+``BatchEngine`` owns a fixed block of HBM (its capacities) in which any number
+of independent cases live at once: each case keeps FP64 positions, velocities
+and meters, cell-sorted particles and a skin-cached neighbour list on the
+device, and one CUDA graph advances every case by one step (skin test and
+rebuild, density, Molteni diffusion, Tait, Adami walls, force, obstacle
+reaction, semi-implicit Euler with the box and obstacle clamps).  Cases are
+admitted and retired while the others keep running; a case evolves bit for
+bit the same alone or in a batch.
 
-``run_case`` is the drop-in for ``tensorsph.dam_break_3d.run_case``
-(dam_break_3d.py:569-734) and returns the same ``DamBreak3DRun`` record;
-``obstacle_case`` builds the 3-D dam break with a box obstacle of the
-headline benchmark (fluid 1.2 x 1.0 x 0.55 m in a 3.2 x 1.0 x 1.0 m tank,
-obstacle 0.16 x 0.16 x 0.4 m).
+``CaseSpec`` is one case ready for admission; ``dam_break_3d_case`` and
+``dam_break_2d_case`` build it from the reference configurations.
+
+``DamBreak3DEngine`` is the single-case engine (with the optional Lind shift)
+and ``run_case`` / ``run_dam_break_2d`` are the drop-ins for
+``tensorsph.dam_break_3d.run_case`` (dam_break_3d.py:569-734) and
+``tensorsph.dam_break.run_case`` (dam_break.py:319-460).  ``obstacle_case``
+builds the 3-D dam break with a box obstacle (fluid 1.2 x 1.0 x 0.55 m in a
+3.2 x 1.0 x 1.0 m tank, obstacle 0.16 x 0.16 x 0.4 m).
 """
 from __future__ import annotations
 
@@ -23,8 +30,11 @@ import torch
 from . import _lib
 from .dam_break_3d import DamBreak3DConfig, make_column_3d, mass_3d, wall_lattice_3d
 
-__all__ = ["DamBreak3DEngine", "DamBreak3DRun", "obstacle_case", "obstacle_lattice_3d",
-           "run_case", "DIAG_FIELDS"]
+__all__ = ["BatchEngine", "CaseSpec", "DamBreak3DEngine", "DamBreak3DRun", "dam_break_2d_case",
+           "dam_break_3d_case", "droplet_impact_case", "engine_bytes", "obstacle_case", "obstacle_lattice_3d",
+           "run_case", "run_dam_break_2d", "DIAG_FIELDS"]
+
+MAX_ROWS = (1 << 27) - 1   # fluid + wall rows of one engine (27-bit row index)
 
 DIAG_FIELDS = ("rho_max", "speed_max", "front", "force_x", "force_y", "force_z", "kinetic",
                "potential", "escapes", "clamps", "rebuilds", "row_max", "step", "status",
@@ -86,6 +96,379 @@ def obstacle_case(dx: float = 0.0069, *, viscosity: float = 1.0e-6, density_diff
     return cfg, (lo, hi)
 
 
+# ------------------------------------------------------------------ cases --
+
+@dataclass
+class CaseSpec:
+    """One case ready for admission: parameters plus its host arrays (FP64).
+
+    ``wall`` holds the static wall particles with the obstacle particles, if
+    any, as its last ``n_obstacle`` rows (the order of the reference's
+    ``torch.cat((wall, obstacle))``)."""
+
+    params: _lib.CaseParams
+    x: torch.Tensor
+    v: torch.Tensor
+    mass: torch.Tensor
+    wall: torch.Tensor
+    label: str = ""
+
+    @property
+    def dim(self) -> int:
+        return int(self.params.dim)
+
+    @property
+    def n_fluid(self) -> int:
+        return int(self.params.n_fluid)
+
+    @property
+    def n_wall(self) -> int:
+        return int(self.params.n_wall)
+
+    @property
+    def n_obstacle(self) -> int:
+        return int(self.params.n_obstacle)
+
+    @property
+    def dt(self) -> float:
+        return float(self.params.dt)
+
+    def cells(self) -> int:
+        n = _lib.lib().tsph_engine_case_cells(ctypes.byref(self.params))
+        if n < 0:
+            raise ValueError("invalid case parameters")
+        return int(n)
+
+
+def _case_params(*, dim, n_fluid, n_wall, n_obstacle, cfg, h, wall_mass, box_hi, lo, hi,
+                 shift_every=0, obstacle=None):
+    if cfg.density_diffusion > 0.0 and cfg.density_diffusion_form != "molteni":
+        raise NotImplementedError("the device engine implements the 'molteni' diffusion form only")
+    p = _lib.CaseParams()
+    p.dim, p.n_fluid, p.n_wall, p.n_obstacle = dim, n_fluid, n_wall, n_obstacle
+    p.shift_every = int(shift_every)
+    p.has_obstacle = 1 if obstacle is not None else 0
+    p.h, p.rho0, p.sound_speed, p.gamma = h, cfg.rho0, cfg.sound_speed, cfg.gamma
+    p.gravity, p.viscosity, p.wall_friction = cfg.gravity, cfg.viscosity, cfg.wall_friction
+    p.diffusion_scale = (2.0 * cfg.density_diffusion * cfg.sound_speed * cfg.h_factor * cfg.dx
+                         if cfg.density_diffusion > 0.0 else 0.0)
+    p.dt = cfg.dt
+    p.wall_mass = wall_mass
+    p.skin = cfg.pair_skin_factor * h
+    for k in range(3):
+        p.box_hi[k] = box_hi[k]
+    p.tolerance = 0.25 * cfg.dx
+    if obstacle is not None:
+        for k in range(3):
+            p.ob_lo[k], p.ob_hi[k] = obstacle[0][k], obstacle[1][k]
+        p.ob_eps = 0.01 * cfg.dx
+    p.shift_strength = getattr(cfg, "shift_strength", 1.0)
+    p.shift_limit = getattr(cfg, "shift_limit", 0.25)
+    p.shift_free_surface = 0.95
+    p.shift_vref_floor = 0.05 * cfg.sound_speed
+    margin = 2.0 * cfg.dx
+    for k in range(3):
+        if k < dim:
+            p.grid_lo[k] = min(lo[k], 0.0) - margin
+            p.grid_hi[k] = max(hi[k], box_hi[k]) + margin
+    return p
+
+
+def dam_break_3d_host_state(cfg: DamBreak3DConfig, obstacle=None, seed=None):
+    """Host lattices of a 3-D case: fluid (FP64), masses, walls (+ obstacle
+    particles last) and the obstacle particle count."""
+    saved = torch.get_default_dtype()
+    torch.set_default_dtype(torch.float64)
+    try:
+        x, mass = make_column_3d(cfg, "cpu", seed=seed)
+        wall = wall_lattice_3d(cfg, "cpu")
+        n_ob = 0
+        if obstacle is not None:
+            ob = obstacle_lattice_3d(obstacle[0], obstacle[1], cfg.dx)
+            n_ob = ob.shape[0]
+            wall = torch.cat((wall, ob))
+            clamp_out_of_obstacle_host(x, obstacle[0], obstacle[1], 0.01 * cfg.dx)
+    finally:
+        torch.set_default_dtype(saved)
+    return x.double(), mass.double(), wall.double(), n_ob
+
+
+def dam_break_3d_case(cfg: DamBreak3DConfig, *, obstacle=None, shift_every: int = 0, seed=None,
+                      host_state=None, velocity=None, label: str = "") -> CaseSpec:
+    """The 3-D dam break of ``tensorsph.dam_break_3d`` (optionally with the box
+    obstacle of kleefsman_obstacle_3d.py) as a ``CaseSpec``."""
+    if host_state is None:
+        host_state = dam_break_3d_host_state(cfg, obstacle, seed)
+    x, mass, wall, n_ob = host_state
+    x = x.double().contiguous()
+    wall = wall.double().contiguous()
+    h = cfg.h_factor * cfg.dx
+    box = (cfg.pool_width, cfg.tank_top(), cfg.tank_depth)
+    allpos = torch.cat((x, wall)) if wall.shape[0] else x
+    p = _case_params(dim=3, n_fluid=x.shape[0], n_wall=wall.shape[0], n_obstacle=n_ob, cfg=cfg, h=h,
+                     wall_mass=mass_3d(cfg.dx, cfg.h_factor, cfg.rho0, cfg.density_calibration),
+                     box_hi=box, lo=allpos.min(dim=0).values.tolist(),
+                     hi=allpos.max(dim=0).values.tolist(), shift_every=shift_every,
+                     obstacle=obstacle)
+    v = torch.zeros_like(x) if velocity is None else velocity.double().contiguous()
+    return CaseSpec(p, x, v, mass.double().contiguous(), wall, label or "dam_break_3d")
+
+
+def dam_break_2d_case(cfg, *, shift_every: int = 0, velocity=None, label: str = "") -> CaseSpec:
+    """The 2-D dam break of ``tensorsph.dam_break`` (dam_break.py:319-340 set-up:
+    ``make_column`` and ``wall_lattice`` up to ``tank_top``) as a ``CaseSpec``."""
+    from .dam_break import make_column, validate_case
+    from .droplet_impact import lattice_mass_unit, wall_lattice
+    validate_case(cfg)
+    if cfg.density_renormalization or cfg.boundary_consistent_density:
+        raise NotImplementedError("density_renormalization and boundary_consistent_density are "
+                                  "not part of the device engine")
+    x, mass = make_column(cfg, "cpu")
+    wall = wall_lattice(cfg, "cpu", top=cfg.tank_top())
+    x = x.double().contiguous()
+    wall = wall.double().contiguous()
+    h = cfg.h_factor * cfg.dx
+    box = (cfg.pool_width, cfg.tank_top(), 0.0)
+    allpos = torch.cat((x, wall))
+    p = _case_params(dim=2, n_fluid=x.shape[0], n_wall=wall.shape[0], n_obstacle=0, cfg=cfg, h=h,
+                     wall_mass=lattice_mass_unit(cfg), box_hi=box,
+                     lo=allpos.min(dim=0).values.tolist(), hi=allpos.max(dim=0).values.tolist(),
+                     shift_every=shift_every)
+    v = torch.zeros_like(x) if velocity is None else velocity.double().contiguous()
+    return CaseSpec(p, x, v, mass.double().contiguous(), wall, label or "dam_break_2d")
+
+
+def droplet_impact_case(cfg, *, drop_speed: float = 0.0, label: str = "") -> CaseSpec:
+    """The 2-D droplet impact of ``tensorsph.droplet_impact`` (pool plus
+    circular drop from ``make_particles``, walls from ``wall_lattice`` up to
+    ``domain_top``, droplet_impact.py:666-760) as a ``CaseSpec``; the drop
+    starts with the downward speed ``drop_speed`` (the reference drops it from
+    rest).  Surface tension is not part of the device engine."""
+    from .droplet_impact import domain_top, lattice_mass_unit, make_particles, validate_config, wall_lattice
+    validate_config(cfg)
+    if cfg.surface_tension_coefficient > 0.0:
+        raise NotImplementedError("surface tension is not part of the device engine")
+    if cfg.density_renormalization or cfg.boundary_consistent_density:
+        raise NotImplementedError("density_renormalization and boundary_consistent_density are "
+                                  "not part of the device engine")
+    x, mass = make_particles(cfg, "cpu")
+    wall = wall_lattice(cfg, "cpu")
+    x = x.double().contiguous()
+    wall = wall.double().contiguous()
+    n_pool = int(((x[:, 1] <= cfg.pool_depth)).sum())
+    v = torch.zeros_like(x)
+    v[n_pool:, 1] = -float(drop_speed)
+    h = cfg.h_factor * cfg.dx
+    top = domain_top(cfg)
+    allpos = torch.cat((x, wall))
+    p = _case_params(dim=2, n_fluid=x.shape[0], n_wall=wall.shape[0], n_obstacle=0, cfg=cfg, h=h,
+                     wall_mass=lattice_mass_unit(cfg), box_hi=(cfg.pool_width, top, 0.0),
+                     lo=allpos.min(dim=0).values.tolist(), hi=allpos.max(dim=0).values.tolist())
+    return CaseSpec(p, x, v, mass.double().contiguous(), wall, label or "droplet_impact")
+
+
+# ------------------------------------------------------------------ engine --
+
+def _engine_params(max_fluid, max_wall, max_obstacle, max_cells, max_cases, max_neighbors,
+                   diag_ring) -> _lib.EngineParams:
+    prm = _lib.EngineParams()
+    prm.max_fluid, prm.max_wall, prm.max_obstacle = int(max_fluid), int(max_wall), int(max_obstacle)
+    prm.max_cells, prm.max_cases = int(max_cells), int(max_cases)
+    prm.max_neighbors, prm.diag_ring = int(max_neighbors), int(diag_ring)
+    return prm
+
+
+def engine_bytes(*, max_fluid, max_wall, max_obstacle=0, max_cells, max_cases=1,
+                 max_neighbors=160, diag_ring=1024) -> int:
+    """Device bytes of an engine with these capacities (its HBM footprint)."""
+    prm = _engine_params(max_fluid, max_wall, max_obstacle, max_cells, max_cases, max_neighbors,
+                         diag_ring)
+    n = _lib.lib().tsph_engine_bytes(ctypes.byref(prm))
+    if n <= 0:
+        raise ValueError("invalid engine capacities")
+    return int(n)
+
+
+class BatchEngine:
+    """Fixed-capacity device engine holding any number of independent cases."""
+
+    def __init__(self, *, max_fluid: int, max_wall: int, max_obstacle: int = 0, max_cells: int,
+                 max_cases: int = 1, max_neighbors: int = 160, diag_ring: int = 1024,
+                 device: torch.device | None = None):
+        dev = device or _lib.cuda_device()
+        self.device = dev
+        self.stream = torch.cuda.Stream(device=dev)
+        self.capacity = dict(max_fluid=int(max_fluid), max_wall=int(max_wall),
+                             max_obstacle=int(max_obstacle), max_cells=int(max_cells),
+                             max_cases=int(max_cases), max_neighbors=int(max_neighbors),
+                             diag_ring=int(diag_ring))
+        self.params = _engine_params(max_fluid, max_wall, max_obstacle, max_cells, max_cases,
+                                     max_neighbors, diag_ring)
+        L = _lib.lib()
+        nbytes = L.tsph_engine_bytes(ctypes.byref(self.params))
+        if nbytes <= 0:
+            raise ValueError("invalid engine capacities")
+        self.nbytes = int(nbytes)
+        self._handle = ctypes.c_void_p(None)
+        self.stream.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(self.stream):
+            self.arena = torch.empty(self.nbytes, dtype=torch.uint8, device=dev)
+        _lib.check(L.tsph_engine_create(ctypes.byref(self.params), self.arena.data_ptr(), self.nbytes,
+                                        self.stream.cuda_stream, ctypes.byref(self._handle)),
+                   "tsph_engine_create")
+        self.cases: dict[int, CaseSpec] = {}
+        self.steps_of: dict[int, int] = {}
+
+    # ----------------------------------------------------------- admission --
+    def usage(self) -> dict:
+        u = (ctypes.c_int64 * 5)()
+        _lib.check(_lib.lib().tsph_engine_usage(self._handle, u), "tsph_engine_usage")
+        return dict(fluid=u[0], wall=u[1], obstacle=u[2], cells=u[3], cases=u[4])
+
+    def fits(self, spec: CaseSpec) -> bool:
+        """Whether ``spec`` fits in the free capacity right now."""
+        u = self.usage()
+        c = self.capacity
+        return (u["cases"] < c["max_cases"] and u["fluid"] + spec.n_fluid <= c["max_fluid"]
+                and u["wall"] + spec.n_wall <= c["max_wall"]
+                and u["obstacle"] + spec.n_obstacle <= c["max_obstacle"]
+                and u["cells"] + spec.cells() <= c["max_cells"])
+
+    def add(self, spec: CaseSpec) -> int:
+        """Admit a case; returns its id.  Raises RuntimeError when it does not fit."""
+        L = _lib.lib()
+        cid = ctypes.c_int64(-1)
+        self.stream.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(self.stream):
+            X = spec.x.to(self.device, torch.float64).contiguous()
+            V = spec.v.to(self.device, torch.float64).contiguous()
+            M = spec.mass.to(self.device, torch.float64).contiguous()
+            W = spec.wall.to(self.device, torch.float64).contiguous() if spec.n_wall else None
+        rc = L.tsph_engine_add_case(self._handle, ctypes.byref(spec.params), X.data_ptr(),
+                                    V.data_ptr(), M.data_ptr(), W.data_ptr() if W is not None else None,
+                                    self.stream.cuda_stream, ctypes.byref(cid))
+        if rc == _lib.ERR_CAPACITY:
+            raise RuntimeError("the case does not fit in the engine's free capacity")
+        _lib.check(rc, "tsph_engine_add_case")
+        self.cases[cid.value] = spec
+        self.steps_of[cid.value] = 0
+        return int(cid.value)
+
+    def remove(self, case_id: int) -> None:
+        _lib.check(_lib.lib().tsph_engine_remove_case(self._handle, int(case_id),
+                                                      self.stream.cuda_stream),
+                   "tsph_engine_remove_case")
+        self.cases.pop(case_id, None)
+        self.steps_of.pop(case_id, None)
+
+    # ------------------------------------------------------------ stepping --
+    def set_block(self, threads: int) -> None:
+        """Threads per block of the pair kernels (64, 128 or 256): a tuning knob."""
+        _lib.check(_lib.lib().tsph_engine_set_block(self._handle, int(threads)),
+                   "tsph_engine_set_block")
+
+    def step(self, steps: int = 1, graph: bool = True) -> None:
+        """Advance every case ``steps`` steps on the engine's stream (no host
+        synchronisation)."""
+        self.stream.wait_stream(torch.cuda.current_stream(self.device))
+        L = _lib.lib()
+        fn = L.tsph_engine_step if graph else L.tsph_engine_step_eager
+        _lib.check(fn(self._handle, int(steps), self.stream.cuda_stream), "tsph_engine_step")
+        for k in self.steps_of:
+            self.steps_of[k] += int(steps)
+
+    def _hand_over(self, *tensors):
+        """Make the caller's current stream wait for the engine stream, so the
+        returned tensors are safe to use there."""
+        cur = torch.cuda.current_stream(self.device)
+        if cur != self.stream:
+            cur.wait_stream(self.stream)
+            for t in tensors:
+                t.record_stream(cur)
+
+    STAGES = ("rebuild", "density", "diffusion_eos", "walls", "force", "reaction",
+              "integrate", "shift_rebuild", "concentration", "gradient", "select", "shift_apply")
+
+    def step_timed(self) -> dict:
+        """One eager step with CUDA events between stages; ``{stage: ms}``."""
+        self.stream.wait_stream(torch.cuda.current_stream(self.device))
+        ms = (ctypes.c_float * 12)()
+        n = ctypes.c_int64(0)
+        _lib.check(_lib.lib().tsph_engine_step_timed(self._handle, self.stream.cuda_stream, ms,
+                                                     ctypes.byref(n)), "tsph_engine_step_timed")
+        for k in self.steps_of:
+            self.steps_of[k] += 1
+        return {self.STAGES[i]: float(ms[i]) for i in range(n.value)}
+
+    def graph_kernels(self) -> int:
+        """Kernel launches in one captured step (the step graph's kernel nodes)."""
+        k = ctypes.c_int64(0)
+        _lib.check(_lib.lib().tsph_engine_graph_kernels(self._handle, ctypes.byref(k)),
+                   "tsph_engine_graph_kernels")
+        return int(k.value)
+
+    # -------------------------------------------------------------- output --
+    def diagnostics(self, case_id: int, first: int, count: int) -> torch.Tensor:
+        """Per-step meter rows ``(count, 16)`` of one case (``DIAG_FIELDS``)."""
+        with torch.cuda.stream(self.stream):
+            out = torch.empty((count, 16), dtype=torch.float64, device=self.device)
+        _lib.check(_lib.lib().tsph_engine_diag(self._handle, int(case_id), out.data_ptr(),
+                                               int(first), int(count), self.stream.cuda_stream),
+                   "tsph_engine_diag")
+        self._hand_over(out)
+        return out
+
+    def read(self, case_id: int):
+        """``(x, v, rho, p)`` of one case's fluid in its original order (device)."""
+        spec = self.cases[case_id]
+        n, dim = spec.n_fluid, spec.dim
+        with torch.cuda.stream(self.stream):
+            x = torch.empty((n, dim), dtype=torch.float64, device=self.device)
+            v = torch.empty_like(x)
+            rho = torch.empty(n, dtype=torch.float64, device=self.device)
+            p = torch.empty_like(rho)
+        _lib.check(_lib.lib().tsph_engine_read(self._handle, int(case_id), x.data_ptr(),
+                                               v.data_ptr(), rho.data_ptr(), p.data_ptr(),
+                                               self.stream.cuda_stream), "tsph_engine_read")
+        self._hand_over(x, v, rho, p)
+        return x, v, rho, p
+
+    def status(self, case_id: int) -> dict:
+        buf = (ctypes.c_int64 * 8)()
+        rc = _lib.lib().tsph_engine_status(self._handle, int(case_id), buf, self.stream.cuda_stream)
+        out = dict(escapes=buf[0], clamps=buf[1], rebuilds=buf[2], steps=buf[3], row_max=buf[4],
+                   status=buf[6])
+        if rc == _lib.ERR_CAPACITY:
+            raise RuntimeError(f"neighbour row capacity exceeded (longest row {buf[4]}); "
+                               "raise max_neighbors")
+        _lib.check(rc, "tsph_engine_status")
+        return out
+
+    def close(self) -> None:
+        if self._handle is not None and self._handle.value:
+            torch.cuda.synchronize(self.device)
+            _lib.lib().tsph_engine_destroy(self._handle)
+            self._handle = ctypes.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def capacity_for(specs, *, max_neighbors: int = 160, diag_ring: int = 1024, cases: int | None = None):
+    """Capacities that hold every case of ``specs`` at once."""
+    specs = list(specs)
+    return dict(max_fluid=sum(s.n_fluid for s in specs), max_wall=max(1, sum(s.n_wall for s in specs)),
+                max_obstacle=sum(s.n_obstacle for s in specs),
+                max_cells=sum(s.cells() for s in specs),
+                max_cases=cases if cases is not None else len(specs),
+                max_neighbors=max_neighbors, diag_ring=diag_ring)
+
+
+# ------------------------------------------------------- single-case engine --
+
 @dataclass
 class DamBreak3DRun:
     """Run record with the fields of the reference ``DamBreak3DRun`` that the
@@ -116,176 +499,39 @@ class DamBreak3DRun:
         return self.final_mass - self.initial_mass
 
 
-class DamBreak3DEngine:
-    """One device-resident 3-D dam-break case."""
+class DamBreak3DEngine(BatchEngine):
+    """One device-resident 3-D dam-break case (a batch of one, sized to it)."""
 
     def __init__(self, cfg: DamBreak3DConfig, *, obstacle=None, shift_every: int = 0,
                  seed: int | None = None, max_neighbors: int = 160, diag_ring: int = 8192,
                  device: torch.device | None = None, host_state=None):
-        dev = device or _lib.cuda_device()
+        spec = dam_break_3d_case(cfg, obstacle=obstacle, shift_every=shift_every, seed=seed,
+                                 host_state=host_state)
+        super().__init__(**capacity_for([spec], max_neighbors=max_neighbors, diag_ring=diag_ring),
+                         device=device)
         self.cfg = cfg
-        self.device = dev
-        self.stream = torch.cuda.Stream(device=dev)
-        h = cfg.h_factor * cfg.dx
-        if host_state is None:
-            host_state = self.build_host_state(cfg, obstacle, seed)
-        x, mass, wall, n_ob = host_state
-        self.n_fluid, self.n_wall, self.n_obstacle = x.shape[0], wall.shape[0], n_ob
-        prm = _lib.EngineParams()
-        prm.n_fluid, prm.n_wall, prm.n_obstacle = self.n_fluid, self.n_wall, n_ob
-        prm.max_neighbors, prm.shift_every, prm.diag_ring = max_neighbors, shift_every, diag_ring
-        prm.has_obstacle = 1 if obstacle is not None else 0
-        prm.dx, prm.h, prm.rho0 = cfg.dx, h, cfg.rho0
-        prm.sound_speed, prm.gamma, prm.gravity = cfg.sound_speed, cfg.gamma, cfg.gravity
-        prm.viscosity, prm.wall_friction = cfg.viscosity, cfg.wall_friction
-        if cfg.density_diffusion > 0.0 and cfg.density_diffusion_form != "molteni":
-            raise ValueError("the 3-D pass implements the 'molteni' diffusion form only")
-        prm.diffusion_scale = (2.0 * cfg.density_diffusion * cfg.sound_speed * cfg.h_factor
-                               * cfg.dx if cfg.density_diffusion > 0.0 else 0.0)
-        prm.dt = cfg.dt
-        prm.wall_mass = mass_3d(cfg.dx, cfg.h_factor, cfg.rho0, cfg.density_calibration)
-        prm.skin = cfg.pair_skin_factor * h
-        for k, v in enumerate((cfg.pool_width, cfg.tank_top(), cfg.tank_depth)):
-            prm.box_hi[k] = v
-        prm.tolerance = 0.25 * cfg.dx
-        if obstacle is not None:
-            for k in range(3):
-                prm.ob_lo[k], prm.ob_hi[k] = obstacle[0][k], obstacle[1][k]
-            prm.ob_eps = 0.01 * cfg.dx
-        prm.shift_strength = getattr(cfg, "shift_strength", 1.0)
-        prm.shift_limit = getattr(cfg, "shift_limit", 0.25)
-        prm.shift_free_surface = 0.95
-        prm.shift_vref_floor = 0.05 * cfg.sound_speed
-        allpos = torch.cat((x, wall)) if self.n_wall else x
-        lo = allpos.min(dim=0).values.tolist()
-        hi = allpos.max(dim=0).values.tolist()
-        for k in range(3):
-            prm.grid_lo[k] = min(lo[k], 0.0) - 2.0 * cfg.dx
-            prm.grid_hi[k] = max(hi[k], prm.box_hi[k]) + 2.0 * cfg.dx
-        self.params = prm
-        L = _lib.lib()
-        nbytes = L.tsph_engine_bytes(ctypes.byref(prm))
-        if nbytes <= 0:
-            raise ValueError("invalid engine parameters")
-        self._handle = ctypes.c_void_p(None)
-        with torch.cuda.stream(self.stream):
-            self.arena = torch.empty(nbytes, dtype=torch.uint8, device=dev)
-            X = x.to(dev, torch.float64, non_blocking=True).contiguous()
-            V = torch.zeros_like(X)
-            M = mass.to(dev, torch.float64, non_blocking=True).contiguous()
-            Wl = wall.to(dev, torch.float64, non_blocking=True).contiguous()
-            _lib.check(L.tsph_engine_create(ctypes.byref(prm), self.arena.data_ptr(), nbytes,
-                                            X.data_ptr(), V.data_ptr(), M.data_ptr(),
-                                            Wl.data_ptr() if self.n_wall else None,
-                                            self.stream.cuda_stream, ctypes.byref(self._handle)),
-                       "tsph_engine_create")
-        self.initial_mass = float(mass.sum())
-        self.initial_pe = float((mass * cfg.gravity * x[:, 1]).sum())
-        self.steps_done = 0
-        self.state_bytes = (X.numel() + M.numel() + Wl.numel()) * 8
+        self.spec = spec
+        self.n_fluid, self.n_wall, self.n_obstacle = spec.n_fluid, spec.n_wall, spec.n_obstacle
+        self.case_id = self.add(spec)
+        self.initial_mass = float(spec.mass.sum())
+        self.initial_pe = float((spec.mass * cfg.gravity * spec.x[:, 1]).sum())
+        self.state_bytes = (spec.x.numel() + spec.mass.numel() + spec.wall.numel()) * 8
 
-    @staticmethod
-    def build_host_state(cfg, obstacle=None, seed=None):
-        """Host lattices of the case: fluid (FP64), masses, walls (+ obstacle last)."""
-        saved = torch.get_default_dtype()
-        torch.set_default_dtype(torch.float64)
-        try:
-            x, mass = make_column_3d(cfg, "cpu", seed=seed)
-            wall = wall_lattice_3d(cfg, "cpu")
-            n_ob = 0
-            if obstacle is not None:
-                ob = obstacle_lattice_3d(obstacle[0], obstacle[1], cfg.dx)
-                n_ob = ob.shape[0]
-                wall = torch.cat((wall, ob))
-                clamp_out_of_obstacle_host(x, obstacle[0], obstacle[1], 0.01 * cfg.dx)
-        finally:
-            torch.set_default_dtype(saved)
-        return x.double(), mass.double(), wall.double(), n_ob
+    @property
+    def steps_done(self) -> int:
+        return self.steps_of.get(self.case_id, 0)
 
-    # ------------------------------------------------------------ stepping --
-    def step(self, steps: int = 1, graph: bool = True) -> None:
-        """Advance ``steps`` steps on the engine's stream (no host synchronisation)."""
-        self.stream.wait_stream(torch.cuda.current_stream(self.device))
-        L = _lib.lib()
-        fn = L.tsph_engine_step if graph else L.tsph_engine_step_eager
-        _lib.check(fn(self._handle, int(steps), self.stream.cuda_stream), "tsph_engine_step")
-        self.steps_done += int(steps)
+    build_host_state = staticmethod(dam_break_3d_host_state)
 
-    def _hand_over(self, *tensors):
-        """Make the caller's current stream wait for the engine stream, so the
-        returned tensors are safe to use there."""
-        cur = torch.cuda.current_stream(self.device)
-        if cur != self.stream:
-            cur.wait_stream(self.stream)
-            for t in tensors:
-                t.record_stream(cur)
-
-    STAGES = ("rebuild", "density", "diffusion_eos", "walls", "force", "reaction",
-              "integrate", "shift_rebuild", "concentration", "gradient", "select", "shift_apply")
-
-    def step_timed(self) -> dict:
-        """One eager step with CUDA events between stages; ``{stage: ms}``."""
-        self.stream.wait_stream(torch.cuda.current_stream(self.device))
-        ms = (ctypes.c_float * 12)()
-        n = ctypes.c_int64(0)
-        _lib.check(_lib.lib().tsph_engine_step_timed(self._handle, self.stream.cuda_stream, ms,
-                                                     ctypes.byref(n)), "tsph_engine_step_timed")
-        self.steps_done += 1
-        return {self.STAGES[i]: float(ms[i]) for i in range(n.value)}
-
-    def graph_kernels(self) -> int:
-        """Kernel launches in one captured step (the step graph's kernel nodes)."""
-        k = ctypes.c_int64(0)
-        _lib.check(_lib.lib().tsph_engine_graph_kernels(self._handle, ctypes.byref(k)),
-                   "tsph_engine_graph_kernels")
-        return int(k.value)
-
-    def diagnostics(self, first: int, count: int) -> torch.Tensor:
-        """Per-step meter rows ``(count, 16)`` (fields in ``DIAG_FIELDS``)."""
-        with torch.cuda.stream(self.stream):
-            out = torch.empty((count, 16), dtype=torch.float64, device=self.device)
-        _lib.check(_lib.lib().tsph_engine_diag(self._handle, out.data_ptr(), int(first),
-                                               int(count), self.stream.cuda_stream),
-                   "tsph_engine_diag")
-        self._hand_over(out)
-        return out
+    def diagnostics(self, first: int, count: int) -> torch.Tensor:  # type: ignore[override]
+        return super().diagnostics(self.case_id, first, count)
 
     def state(self):
         """``(x, v, rho, p)`` of the fluid in the original particle order (device)."""
-        n = self.n_fluid
-        with torch.cuda.stream(self.stream):
-            x = torch.empty((n, 3), dtype=torch.float64, device=self.device)
-            v = torch.empty_like(x)
-            rho = torch.empty(n, dtype=torch.float64, device=self.device)
-            p = torch.empty_like(rho)
-        _lib.check(_lib.lib().tsph_engine_read(self._handle, x.data_ptr(), v.data_ptr(),
-                                               rho.data_ptr(), p.data_ptr(),
-                                               self.stream.cuda_stream), "tsph_engine_read")
-        self._hand_over(x, v, rho, p)
-        return x, v, rho, p
+        return self.read(self.case_id)
 
-    def status(self) -> dict:
-        buf = (ctypes.c_int64 * 8)()
-        rc = _lib.lib().tsph_engine_status(self._handle, buf, self.stream.cuda_stream)
-        out = dict(escapes=buf[0], clamps=buf[1], rebuilds=buf[2], steps=buf[3], row_max=buf[4],
-                   status=buf[6])
-        if rc == _lib.ERR_CAPACITY:
-            raise RuntimeError(f"neighbour row capacity exceeded (longest row {buf[4]}); "
-                               "raise max_neighbors")
-        _lib.check(rc, "tsph_engine_status")
-        return out
-
-    def close(self) -> None:
-        if self._handle is not None and self._handle.value:
-            torch.cuda.synchronize(self.device)
-            _lib.lib().tsph_engine_destroy(self._handle)
-            self._handle = ctypes.c_void_p(None)
-
-    def __del__(self):
-        try:
-            self.close()
-        except Exception:
-            pass
+    def status(self) -> dict:  # type: ignore[override]
+        return super().status(self.case_id)
 
 
 def run_case(cfg: DamBreak3DConfig, pair_skin_factor: float | None = None, snapshot_times=None,
@@ -311,7 +557,6 @@ def run_case(cfg: DamBreak3DConfig, pair_skin_factor: float | None = None, snaps
         diag = eng.diagnostics(0, cfg.steps).cpu()
         x, v, rho, p = eng.state()
     st = eng.status()
-    # the reference samples the state at step == cfg.steps too: one more rhs
     sample = [k for k in range(cfg.steps) if k % cfg.output_every == 0]
     times = [k * cfg.dt for k in sample]
     xs = x.cpu()
@@ -327,8 +572,61 @@ def run_case(cfg: DamBreak3DConfig, pair_skin_factor: float | None = None, snaps
         initial_energy=eng.initial_pe, steps_taken=cfg.steps, simulated_time=cfg.steps * cfg.dt,
         obstacle_force=diag[:, 3:6].tolist(), obstacle_impulse=[float(diag[-1, 14])] if cfg.steps else [],
         obstacle_clamps=int(st["clamps"]))
-    masses = DamBreak3DEngine.build_host_state(cfg, obstacle, seed)[1]
+    masses = eng.spec.mass
     run.final_energy = float(0.5 * (masses[:, None] * vs.square()).sum()
                              + (masses * cfg.gravity * xs[:, 1]).sum())
+    eng.close()
+    return run
+
+
+@dataclass
+class DamBreakRun:
+    """The fields of the reference 2-D ``DamBreakRun`` (dam_break.py:250-280)
+    that the device loop measures."""
+
+    times: list
+    front: list
+    kinetic_energy: list
+    potential_energy: list
+    mass: float
+    escaped: int
+    rebuilds: int
+    max_speed: float
+    max_density_compression: float
+    final_positions: torch.Tensor
+    steps_taken: int = 0
+    simulated_time: float = 0.0
+
+
+def run_dam_break_2d(cfg, *, max_neighbors: int = 64) -> DamBreakRun:
+    """Integrate the 2-D dam break (dam_break.py:319-460 with the pair cache,
+    fixed dt, no shifting) on the GPU and return the measured trajectory."""
+    if cfg.adaptive_dt:
+        raise NotImplementedError("adaptive_dt is not supported by the device engine")
+    if cfg.tvc_every:
+        raise NotImplementedError("transport-velocity correction is not part of the device engine")
+    spec = dam_break_2d_case(cfg, shift_every=cfg.shift_every)
+    eng = BatchEngine(**capacity_for([spec], max_neighbors=max_neighbors,
+                                     diag_ring=max(cfg.steps + 1, 1)))
+    cid = eng.add(spec)
+    eng.step(cfg.steps)
+    with torch.cuda.stream(eng.stream):
+        x = eng.read(cid)[0].cpu()
+    # the reference evaluates the right-hand side once more at step == steps
+    # to record the final meters, without integrating it
+    eng.step(1)
+    with torch.cuda.stream(eng.stream):
+        diag = eng.diagnostics(cid, 0, cfg.steps + 1).cpu()
+    st = eng.status(cid)
+    sample = [k for k in range(cfg.steps + 1) if k % cfg.output_every == 0 or k == cfg.steps]
+    run = DamBreakRun(times=[k * cfg.dt for k in sample], front=[float(diag[k, 2]) for k in sample],
+                      kinetic_energy=[float(diag[k, 6]) for k in sample],
+                      potential_energy=[float(diag[k, 7]) for k in sample],
+                      mass=float(spec.mass.sum()), escaped=int(st["escapes"]),
+                      rebuilds=int(st["rebuilds"]),
+                      max_speed=float(diag[:, 1].max()),
+                      max_density_compression=float(diag[:, 0].max()) / cfg.rho0 - 1.0,
+                      final_positions=x, steps_taken=cfg.steps,
+                      simulated_time=cfg.steps * cfg.dt)
     eng.close()
     return run

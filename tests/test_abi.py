@@ -4,6 +4,7 @@ No compute call is made (there is no GPU here); these tests pin the boundary
 between ``include/tsph.h``, the built library and the ctypes binding.
 """
 import ctypes
+import math
 import re
 from pathlib import Path
 
@@ -47,12 +48,34 @@ def test_ctypes_binding_covers_header():
 
 
 def test_pure_host_entry_points(library):
-    assert library.tsph_abi_version() == 1
+    assert library.tsph_abi_version() == 2
     assert library.tsph_status_string(0) == b"ok"
     assert b"finite" in library.tsph_status_string(2)
     assert library.tsph_grid_plan_scratch_bytes() >= 64
     assert library.tsph_pairs_emit_workspace_bytes(100, 10) >= 400
     assert library.tsph_csr_workspace_bytes(100, 10) > 0
+
+
+def test_engine_sizing_is_host_only(library):
+    """Engine footprint and per-case cell counts need no GPU (admission control)."""
+    import ctypes
+    from tensorsph_b200 import _lib
+    prm = _lib.EngineParams(max_fluid=1000, max_wall=500, max_obstacle=0, max_cells=4096,
+                            max_cases=4, max_neighbors=64, diag_ring=8)
+    small = library.tsph_engine_bytes(ctypes.byref(prm))
+    prm.max_fluid = 2000
+    assert library.tsph_engine_bytes(ctypes.byref(prm)) > small > 1000 * 64 * 4
+    prm.max_cases = 0
+    assert library.tsph_engine_bytes(ctypes.byref(prm)) == -1
+    c = _lib.CaseParams(dim=2, n_fluid=10, n_wall=0, h=0.013, rho0=1000.0, sound_speed=20.0,
+                        gamma=7.0, dt=1e-4, skin=0.0)
+    c.grid_lo[0], c.grid_lo[1] = -0.1, -0.1
+    c.grid_hi[0], c.grid_hi[1] = 0.9, 0.4
+    cell = 2 * 0.013
+    nx, ny = math.ceil(1.0 / cell) + 1, math.ceil(0.5 / cell) + 1
+    assert library.tsph_engine_case_cells(ctypes.byref(c)) == nx * ny
+    c.n_fluid = 0
+    assert library.tsph_engine_case_cells(ctypes.byref(c)) == -1
 
 
 def test_struct_sizes_match_header():
@@ -64,6 +87,8 @@ def test_struct_sizes_match_header():
     assert ctypes.sizeof(_lib.ThreedParams) == 8 * (9 + 8 + 6)
     assert ctypes.sizeof(_lib.ShiftParams) == 8 * 9
     assert ctypes.sizeof(_lib.ClampParams) == 8 * (3 + 3 + 3 + 1 + 1 + 3 + 3 + 1)
+    assert ctypes.sizeof(_lib.EngineParams) == 8 * 7
+    assert ctypes.sizeof(_lib.CaseParams) == 8 * (6 + 11 + 3 + 1 + 3 + 3 + 1 + 4 + 3 + 3)
 
 
 def test_product_path_fails_loudly_without_gpu():

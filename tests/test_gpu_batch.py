@@ -1,0 +1,212 @@
+"""The multi-case engine: 2-D cases against the FP64 oracle, and every case
+bit for bit the same alone and batched with others admitted and retired
+around it (continuous batching).
+
+Tolerances of the FP32 pair pass against the FP64 oracle are those of the 3-D
+engine test: density |d rho| / rho0 < 2e-6, pressure |d p| / B < 2e-5,
+velocity after one step |d v| / max|v| < 2e-4.  Alone against batched, the
+state (positions, velocities, density, pressure) must be bitwise equal; the
+energy meters are FP64 sums accumulated with atomics, equal to 1e-12.
+"""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import pairpass as op
+from oracle.neighbors import cell_linked_pairs
+
+pytestmark = pytest.mark.gpu
+
+
+def small_2d(dx=0.02, height=0.4, width=0.2, pool=0.6, diffusion=0.1):
+    from tensorsph_b200.dam_break import DamBreakConfig
+    c0 = 10.0 * math.sqrt(2.0 * 9.81 * height)
+    h = 1.3 * dx
+    return DamBreakConfig(dx=dx, column_width=width, column_height=height, pool_width=pool,
+                          tank_height=height * 1.5, sound_speed=c0, viscosity=1e-3,
+                          dt=0.25 * h / c0, max_courant=0.25, density_diffusion=diffusion,
+                          wall_friction=0.3, steps=10, output_every=5)
+
+
+def small_3d(dx=0.02, obstacle=True):
+    from tensorsph_b200.dam_break_3d import DamBreak3DConfig
+    c0 = 10.0 * math.sqrt(2.0 * 9.81 * 0.24)
+    h = 1.3 * dx
+    cfg = DamBreak3DConfig(dx=dx, pool_width=0.5, tank_depth=0.2, tank_height=0.4,
+                           column_width=0.2, column_depth=0.2, column_height=0.24,
+                           sound_speed=c0, viscosity=1e-3, dt=0.25 * h / c0,
+                           density_diffusion=0.1, wall_friction=0.3, steps=12, output_every=4)
+    ob = ((0.22, 0.0, 0.04), (0.30, 0.08, 0.16)) if obstacle else None
+    return cfg, ob
+
+
+def oracle_2d_steps(cfg, x, mass, wall, steps):
+    x = x.copy()
+    v = np.zeros_like(x)
+    out = []
+    box = np.array([cfg.pool_width, cfg.tank_top()])
+    tol = 0.25 * cfg.dx
+    for _ in range(steps):
+        h = cfg.h_factor * cfg.dx
+        pairs = cell_linked_pairs(np.concatenate((x, wall)), 2.0 * h)
+        rho, p, acc = op.rhs(x, v, mass, cfg, pairs=pairs, wall=wall, dt=cfg.dt)
+        out.append((rho, p, acc))
+        v = v + cfg.dt * acc
+        x = x + cfg.dt * v
+        out_mask = (x < -tol) | (x > box + tol)
+        x = np.clip(x, 0.0, box)
+        v[out_mask] = 0.0
+    return out, x, v
+
+
+def engine_for(specs, **kw):
+    from tensorsph_b200.engine import BatchEngine, capacity_for
+    return BatchEngine(**capacity_for(specs, **kw))
+
+
+def test_2d_case_matches_fp64_oracle(gpu):
+    from tensorsph_b200.engine import dam_break_2d_case
+    cfg = small_2d()
+    spec = dam_break_2d_case(cfg)
+    eng = engine_for([spec], max_neighbors=64, diag_ring=32)
+    cid = eng.add(spec)
+    steps = 6
+    x, m, w = spec.x.numpy(), spec.mass.numpy(), spec.wall.numpy()
+    ref, xr, vr = oracle_2d_steps(cfg, x, m, w, steps)
+    eng.step(1)
+    ex, ev, erho, ep = [t.cpu().numpy() for t in eng.read(cid)]
+    bulk = cfg.rho0 * cfg.sound_speed ** 2 / cfg.gamma
+    rho0, p0, acc0 = ref[0]
+    assert np.abs(erho - rho0).max() / cfg.rho0 < 2e-6
+    assert np.abs(ep - p0).max() / bulk < 2e-5
+    v1 = cfg.dt * acc0
+    assert np.abs(ev - v1).max() / np.abs(v1).max() < 2e-4
+    eng.step(steps - 1)
+    ex, ev, _, _ = [t.cpu().numpy() for t in eng.read(cid)]
+    assert np.abs(ex - xr).max() < 1e-6 * cfg.dx * steps
+    assert np.abs(ev - vr).max() / max(np.abs(vr).max(), 1e-12) < 5e-4
+    diag = eng.diagnostics(cid, 0, steps).cpu().numpy()
+    for k in range(steps):
+        assert diag[k, 0] == pytest.approx(ref[k][0].max(), rel=2e-6)
+    st = eng.status(cid)
+    assert st["steps"] == steps and st["status"] == 0 and st["escapes"] == 0
+    eng.close()
+
+
+def _alone(spec, steps, **kw):
+    eng = engine_for([spec], **kw)
+    cid = eng.add(spec)
+    eng.step(steps)
+    out = [t.cpu() for t in eng.read(cid)]
+    diag = eng.diagnostics(cid, 0, steps).cpu()
+    eng.close()
+    return out, diag
+
+
+def _assert_same(a, b, diag_a, diag_b):
+    for u, w in zip(a, b):
+        assert torch.equal(u, w)
+    # maxima are order independent: exact; FP64 atomic sums: 1e-12
+    assert torch.equal(diag_a[:, [0, 1, 2, 8, 9, 10, 11, 12, 13]], diag_b[:, [0, 1, 2, 8, 9, 10, 11, 12, 13]])
+    torch.testing.assert_close(diag_a[:, [6, 7]], diag_b[:, [6, 7]], rtol=1e-12, atol=1e-12)
+
+
+def test_case_is_the_same_alone_and_in_a_changing_batch(gpu):
+    from tensorsph_b200.engine import dam_break_2d_case, dam_break_3d_case
+    cfg_a, ob = small_3d()
+    a = dam_break_3d_case(cfg_a, obstacle=ob)
+    b = dam_break_2d_case(small_2d())
+    cfg_c, _ = small_3d(dx=0.025, obstacle=False)
+    c = dam_break_3d_case(cfg_c)
+    d = dam_break_2d_case(small_2d(dx=0.025, height=0.3, width=0.3, pool=0.8, diffusion=0.0))
+    kw = dict(max_neighbors=160, diag_ring=64)
+    eng = engine_for([a, b, c, d], **kw)
+    ia = eng.add(a)
+    eng.step(3)
+    ib = eng.add(b)
+    eng.step(4)
+    ic = eng.add(c)
+    eng.step(2)
+    eng.remove(ia)                       # a: 9 steps, retired from the front
+    idd = eng.add(d)                     # d takes the freed slot, placed last
+    eng.step(5)
+    got_b = [t.cpu() for t in eng.read(ib)]  # b: 11 steps
+    diag_b = eng.diagnostics(ib, 0, 11).cpu()
+    eng.remove(ib)
+    eng.step(3, graph=False)             # the eager path too
+    got_c = [t.cpu() for t in eng.read(ic)]  # c: 10 steps
+    got_d = [t.cpu() for t in eng.read(idd)]  # d: 8 steps
+    diag_c = eng.diagnostics(ic, 0, 10).cpu()
+    diag_d = eng.diagnostics(idd, 0, 8).cpu()
+    assert eng.status(ic)["steps"] == 10 and eng.status(idd)["steps"] == 8
+    eng.close()
+    for spec, steps, got, diag in ((b, 11, got_b, diag_b), (c, 10, got_c, diag_c), (d, 8, got_d, diag_d)):
+        ref, ref_diag = _alone(spec, steps, **kw)
+        _assert_same(got, ref, diag, ref_diag)
+
+
+def test_admission_respects_capacity(gpu):
+    from tensorsph_b200.engine import BatchEngine, capacity_for, dam_break_2d_case
+    b = dam_break_2d_case(small_2d())
+    cap = capacity_for([b], max_neighbors=64, diag_ring=16, cases=2)
+    eng = BatchEngine(**cap)
+    i = eng.add(b)
+    assert not eng.fits(b)               # the fluid capacity is taken
+    with pytest.raises(RuntimeError):
+        eng.add(b)
+    eng.step(2)
+    eng.remove(i)
+    assert eng.fits(b) and eng.usage()["cases"] == 0
+    j = eng.add(b)
+    eng.step(4)
+    got = [t.cpu() for t in eng.read(j)]
+    eng.close()
+    ref, _ = _alone(b, 4, max_neighbors=64, diag_ring=16)
+    for u, w in zip(got, ref):
+        assert torch.equal(u, w)
+
+
+def test_run_dam_break_2d_record(gpu):
+    from tensorsph_b200.engine import run_dam_break_2d
+    cfg = small_2d()
+    run = run_dam_break_2d(cfg)
+    assert run.steps_taken == cfg.steps
+    assert len(run.times) == 3
+    assert run.escaped == 0
+    assert run.front[0] == pytest.approx(0.19, abs=1e-6)   # FP32 lattice (default dtype)
+    assert np.isfinite(run.final_positions.numpy()).all()
+
+
+def test_served_results_equal_alone(gpu):
+    """Continuous batching: requests admitted and retired while others run give
+    the same final state as each request run alone."""
+    from tensorsph_b200 import serving as sv
+    reqs = sv.request_stream(6, rate=200.0, seed=3, n_min=800, n_max=6000, time_scale=0.004)
+    srv = sv.Server(budget_bytes=0.25e9, max_cases=4, max_neighbors=160)
+    out = srv.serve(reqs, max_chunk=7, keep_results=True)
+    srv.close()
+    assert out["requests"] == 6 and all(r.finished > r.arrival for r in reqs)
+    alone = sv.run_serial(sv.request_stream(6, rate=200.0, seed=3, n_min=800, n_max=6000,
+                                            time_scale=0.004), keep_results=True)
+    for rid, got in out["results"].items():
+        for u, w in zip(got, alone["results"][rid]):
+            assert torch.equal(u, w), rid
+
+
+def test_droplet_ensemble_batched_equals_plain(gpu):
+    from tensorsph_b200 import ensemble as en
+    from tensorsph_b200.engine import BatchEngine, capacity_for
+    specs = en.ensemble_specs(en.draw_ensemble(5, seed=1))
+    eng = BatchEngine(**capacity_for(specs, max_neighbors=64, diag_ring=8))
+    eng.set_block(64)
+    ids = [eng.add(s) for s in specs]
+    eng.step(6)
+    got = [[t.cpu() for t in eng.read(i)] for i in ids]
+    eng.close()
+    for spec, g in zip(specs, got):
+        ref, _ = _alone(spec, 6, max_neighbors=64, diag_ring=8)
+        for u, w in zip(g, ref):
+            assert torch.equal(u, w)
+        assert float(g[1][:, 1].min()) < -0.9   # the drop keeps its impact speed
