@@ -53,9 +53,11 @@ def parse():
     ap.add_argument("--ensemble-cases", type=int, default=256)
     ap.add_argument("--ensemble-steps", type=int, default=100)
     ap.add_argument("--plain-steps", type=int, default=20)
-    ap.add_argument("--serve-requests", type=int, default=32)
-    ap.add_argument("--serve-time-scale", type=float, default=0.01)
+    ap.add_argument("--serve-requests", type=int, default=48)
+    ap.add_argument("--serve-time-scale", type=float, default=0.05)
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
+    ap.add_argument("--shear-n", type=int, default=64)
+    ap.add_argument("--shear-steps", type=int, default=2000)
     return ap.parse_args()
 
 
@@ -203,6 +205,35 @@ def serving_leg(args, dev):
             "throughput_vs_serial": served["updates_per_s"] / serial["updates_per_s"]}
 
 
+def shear_leg(args, dev):
+    """Triply periodic shear decay u_x = 1e-3 sin(2 pi z), n^3 jittered lattice,
+    nu = 1e-2, c0 = 1: FP32 (compensated) and FP64 runs of the same driver;
+    decay rates against nu k^2 and the FP32 density field against FP64."""
+    import torch
+    from tensorsph_b200.threed.shear import run_shear_decay
+    out = {"workload": f"{args.shear_n}^3 periodic shear decay, u_x=1e-3 sin(2 pi z), nu=1e-2, "
+                       f"c0=1, h=1.3dx, jitter 0.01dx (seed 0), {args.shear_steps} KDK steps"}
+    runs = {}
+    for name, dtype in (("fp32", torch.float32), ("fp64", torch.float64)):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        r = run_shear_decay(n=args.shear_n, steps=args.shear_steps, dtype=dtype, device=dev)
+        torch.cuda.synchronize(dev)
+        wall = time.perf_counter() - t0
+        runs[name] = r
+        out[name] = {"fit_rate": r.fit_rate, "analytic_rate": r.analytic_rate,
+                     "rate_rel_error": r.rate_error, "pair_rebuilds": r.pair_rebuilds,
+                     "ms_per_step": 1e3 * wall / args.shear_steps,
+                     "updates_per_s": args.shear_n ** 3 * args.shear_steps / wall,
+                     "momentum_final_over_scale": r.diagnostics[-1]["momentum_magnitude"]
+                     / r.momentum_scale}
+    a, b = runs["fp32"], runs["fp64"]
+    out["rate_rel_diff_fp32_vs_fp64"] = (a.fit_rate - b.fit_rate) / b.fit_rate
+    out["density_max_abs_diff_over_rho0"] = float(
+        (a.final_density.double() - b.final_density).abs().max()) / 1000.0
+    return out
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -334,7 +365,8 @@ def main():
     extra = {}
     if rank == 0 and world == 1:
         for name, leg, on in (("ensemble", ensemble_leg, args.ensemble_cases > 0),
-                              ("serving", serving_leg, args.serve_requests > 0)):
+                              ("serving", serving_leg, args.serve_requests > 0),
+                              ("shear", shear_leg, args.shear_steps > 0)):
             if not on:
                 continue
             try:

@@ -254,6 +254,47 @@ typedef struct {
 int tsph_euler_clamp(const tsph_clamp_params* prm, void* pos, void* vel, const void* acc,
                      double dt, int64_t* counters, tsph_stream stream);
 
+/* Half kick v += (dt/2) a, and with drift != 0 also the drift
+ * x = remainder(x + dt v, box) (box: dim edges, NULL for no wrap) -- the
+ * kick-drift-kick halves of threed/solver.py:287-299, in the input dtype. */
+int tsph_kick_drift(void* pos, void* vel, const void* acc, int64_t n, int64_t dim, int64_t dtype,
+                    double dt, int64_t drift, const double* box, tsph_stream stream);
+
+/* ------------------------------------------------------------------------ */
+/* Conservation meters: threed/conservation.py:41-121 (diagnostics) as one   */
+/* FP64 device reduction, deterministic (fixed-order block partials).        */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  int64_t dim, dtype, n;
+  int64_t periodic;          /* circular centre of mass in box (conservation.py:88) */
+  double rho0, sound_speed, gamma;
+  double origin[3];          /* angular-momentum origin                           */
+  double box[3];             /* periodic box edges                                */
+} tsph_meter_params;
+
+typedef struct {
+  const void* pos;           /* (n, dim)                                          */
+  const void* vel;           /* (n, dim)                                          */
+  const void* mass;          /* (n)                                               */
+  const void* rho;           /* (n) or NULL (internal energy 0)                   */
+  double* out;               /* device, 13 doubles: mass, momentum xyz, angular   */
+                             /* momentum xyz (2-D: z only), kinetic, internal and */
+                             /* total energy, centre of mass xyz                  */
+} tsph_meter_io;
+
+int64_t tsph_meters_workspace_bytes(void);
+int tsph_meters(const tsph_meter_params* prm, const tsph_meter_io* io, void* ws, int64_t ws_bytes,
+                tsph_stream stream);
+/* Shear-mode amplitude of v_x (positions and velocities (n, 3)): mode 0
+ * 4 <v_x sin(k y) sin(k z)> (operators3.py:401-408), mode 1 2 <v_x sin(k z)>,
+ * FP64, into *out (device); workspace tsph_meters_workspace_bytes. */
+int tsph_mode_amplitude(const void* pos, const void* vel, int64_t n, int64_t dtype, double wavenumber,
+                        int64_t mode, void* ws, int64_t ws_bytes, double* out, tsph_stream stream);
+/* Per-particle Tait internal energy (conservation.py:71-85) in the input
+ * dtype, computed in FP64. */
+int tsph_internal_energy(const void* rho, int64_t n, int64_t dtype, double rho0, double sound_speed,
+                         double gamma, void* out, tsph_stream stream);
+
 /* ------------------------------------------------------------------------ */
 /* Multi-case device engine (one GPU, one CUDA graph per step for all cases). */
 /* Replaces the step loops of dam_break.py:374-440 (2-D), dam_break_3d.py:    */

@@ -79,6 +79,16 @@ class ClampParams(ctypes.Structure):
                 ("ob_eps", c_double)]
 
 
+class MeterParams(ctypes.Structure):
+    _fields_ = [(k, c_int64) for k in ("dim", "dtype", "n", "periodic")] + \
+               [(k, c_double) for k in ("rho0", "sound_speed", "gamma")] + \
+               [("origin", c_double * 3), ("box", c_double * 3)]
+
+
+class MeterIO(ctypes.Structure):
+    _fields_ = [(k, c_void_p) for k in ("pos", "vel", "mass", "rho", "out")]
+
+
 class EngineParams(ctypes.Structure):
     _fields_ = [(k, c_int64) for k in ("max_fluid", "max_wall", "max_obstacle", "max_cells",
                                        "max_cases", "max_neighbors", "diag_ring")]
@@ -134,6 +144,14 @@ _SIGNATURES = {
                               c_void_p]),
     "tsph_euler_clamp": (c_int, [POINTER(ClampParams), c_void_p, c_void_p, c_void_p, c_double,
                                  c_void_p, c_void_p]),
+    "tsph_meters_workspace_bytes": (c_int64, []),
+    "tsph_meters": (c_int, [POINTER(MeterParams), POINTER(MeterIO), c_void_p, c_int64, c_void_p]),
+    "tsph_mode_amplitude": (c_int, [c_void_p, c_void_p, c_int64, c_int64, c_double, c_int64,
+                                    c_void_p, c_int64, c_void_p, c_void_p]),
+    "tsph_kick_drift": (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_int64, c_double,
+                                c_int64, c_void_p, c_void_p]),
+    "tsph_internal_energy": (c_int, [c_void_p, c_int64, c_int64, c_double, c_double, c_double,
+                                     c_void_p, c_void_p]),
     "tsph_engine_bytes": (c_int64, [POINTER(EngineParams)]),
     "tsph_engine_case_cells": (c_int64, [POINTER(CaseParams)]),
     "tsph_engine_create": (c_int, [POINTER(EngineParams), c_void_p, c_int64, c_void_p, c_void_p]),

@@ -32,7 +32,7 @@ __all__ = [
     "calibrated_particle_mass", "lattice_mass_unit", "cell_centres", "pool_lattice",
     "make_particles", "wall_lattice", "wall_mass", "drop_wall_wall_pairs", "rhs",
     "symmetric_rows", "boundary_box", "apply_boundary", "domain_top",
-    "PairListCache", "cell_linked_pairs",
+    "PairListCache", "cell_linked_pairs", "density_from_neighbor_pairs",
 ]
 
 VISCOUS_LAPLACIAN_FACTOR = 2.0
@@ -341,6 +341,28 @@ def drop_wall_wall_pairs(pairs: torch.Tensor, fluid_count: int) -> torch.Tensor:
 
 
 # ----------------------------------------------------------- gather rows ---
+
+def density_from_neighbor_pairs(pos, mass, h: float, pairs=None):
+    """Density summation over an unordered pair list with each particle's self
+    term (droplet_impact.py:761-788), 2-D cubic normalisation as the reference
+    uses in any dimension.  On the GPU it is the shift kernel's concentration
+    sum with the masses as weights."""
+    if pos.ndim != 2 or mass.ndim != 1 or mass.shape[0] != pos.shape[0]:
+        raise ValueError("pos must be (N, D) and mass must be (N,)")
+    if pos.device != mass.device:
+        raise ValueError("pos and mass must be on the same device")
+    if not pos.is_floating_point() or not mass.is_floating_point():
+        raise TypeError("pos and mass must be floating-point tensors")
+    if not math.isfinite(float(h)) or h <= 0:
+        raise ValueError("h must be finite and positive")
+    if pairs is not None:
+        if pairs.ndim != 2 or pairs.shape[1] != 2 or pairs.dtype != torch.long:
+            raise ValueError("pairs must be a long tensor with shape (pair_count, 2)")
+        if pairs.device != pos.device:
+            raise ValueError("pairs and pos must be on the same device")
+    from .particle_shifting import concentration
+    return concentration(pos, mass.to(pos.dtype), float(h), pairs=pairs)
+
 
 def symmetric_rows(pairs: torch.Tensor, nrows: int):
     """Turn a ``(P, 2)`` pair list (CUDA) into row-sorted symmetric gather rows."""

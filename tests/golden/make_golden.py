@@ -307,7 +307,60 @@ def shift_cases(ps, di):
     return data
 
 
-def main(src):
+def meters_cases(cons, di):
+    """Conservation ledger rows (threed/conservation.py) and the pair-list
+    density summation (droplet_impact.py:761-788) on seeded clouds."""
+    data = {}
+    k = 0
+    for dtype in (torch.float32, torch.float64):
+        for dim, box in ((3, None), (3, 0.5), (2, None)):
+            g = torch.Generator().manual_seed(60 + k)
+            n = 500
+            pos = (0.5 * torch.rand((n, dim), generator=g)).to(dtype)
+            vel = (0.1 * torch.randn((n, dim), generator=g)).to(dtype)
+            mass = (1.0 + 0.1 * torch.rand((n,), generator=g)).to(dtype)
+            rho = (1000.0 * (1.0 + 0.01 * torch.randn((n,), generator=g))).to(dtype)
+            if dim == 3:
+                row = cons.diagnostics(pos, vel, mass, rho, rho0=1000.0, sound_speed=20.0,
+                                       gamma=7.0, periodic_box=box)
+                for key in ("mass", "kinetic_energy", "internal_energy", "total_energy"):
+                    data[f"c{k}_ledger_{key}"] = np.float64(row[key])
+                for key in ("momentum", "angular_momentum", "centre_of_mass"):
+                    data[f"c{k}_ledger_{key}"] = np.asarray(row[key], dtype=np.float64)
+                data[f"c{k}_e"] = _np(cons.internal_energy(rho, 1000.0, 20.0, 7.0))
+            data[f"c{k}_box"] = np.float64(-1.0 if box is None else box)
+            h = 0.03
+            pairs = di.cell_linked_pairs(pos, 2.0 * h)
+            data[f"c{k}_rho_pairs"] = _np(di.density_from_neighbor_pairs(pos, mass, h, pairs))
+            for name, t in dict(pos=pos, vel=vel, mass=mass, rho=rho).items():
+                data[f"c{k}_{name}"] = _np(t)
+            data[f"c{k}_dim"] = np.int64(dim)
+            k += 1
+    data["count"] = np.int64(k)
+    return data
+
+
+def shear_cases(sv):
+    """Short runs of the reference double-shear decay (threed/solver.py:211)."""
+    data = {}
+    k = 0
+    for dtype in (torch.float64, torch.float32):
+        r = sv.run_shear_wave(n=12, steps=40, sample_every=10, dtype=dtype)
+        data[f"c{k}_times"] = np.asarray(r.times, dtype=np.float64)
+        data[f"c{k}_amplitudes"] = np.asarray(r.amplitudes, dtype=np.float64)
+        data[f"c{k}_fit_rate"] = np.float64(r.fit_rate)
+        data[f"c{k}_kinetic"] = np.asarray([d["kinetic_energy"] for d in r.diagnostics])
+        data[f"c{k}_total"] = np.asarray([d["total_energy"] for d in r.diagnostics])
+        data[f"c{k}_momentum"] = np.asarray([d["momentum"] for d in r.diagnostics])
+        data[f"c{k}_pairs_last"] = np.int64(r.pairs_last)
+        data[f"c{k}_rebuilds"] = np.int64(r.pair_rebuilds)
+        data[f"c{k}_dtype"] = np.array(str(dtype))
+        k += 1
+    data["count"] = np.int64(k)
+    return data
+
+
+def main(src, families=None):
     sys.path.insert(0, str(src))
     import tensorsph.neighbor_search as ns
     import tensorsph.droplet_impact as di
@@ -316,16 +369,24 @@ def main(src):
     import tensorsph.particle_shifting as ps
     import tensorsph.threed as t3
     from tensorsph.threed import neighbors3 as n3
+    from tensorsph.threed import conservation as cons
+    from tensorsph.threed import solver as sv
 
     meta = {"torch_version": np.array(torch.__version__)}
     torch.set_num_threads(1)
-    np.savez_compressed(OUT / "pairs.npz", **pairs_cases(ns), **meta)
-    np.savez_compressed(OUT / "periodic.npz", **periodic_cases(n3), **meta)
-    np.savez_compressed(OUT / "rhs2d.npz", **rhs2d_cases(di, db), **meta)
-    np.savez_compressed(OUT / "config1.npz", **config1_case(di, db), **meta)
-    np.savez_compressed(OUT / "rhs3d.npz", **rhs3d_cases(d3, di), **meta)
-    np.savez_compressed(OUT / "threed.npz", **threed_cases(t3), **meta)
-    np.savez_compressed(OUT / "shift.npz", **shift_cases(ps, di), **meta)
+    makers = {
+        "pairs": lambda: pairs_cases(ns),
+        "periodic": lambda: periodic_cases(n3),
+        "rhs2d": lambda: rhs2d_cases(di, db),
+        "config1": lambda: config1_case(di, db),
+        "rhs3d": lambda: rhs3d_cases(d3, di),
+        "threed": lambda: threed_cases(t3),
+        "shift": lambda: shift_cases(ps, di),
+        "meters": lambda: meters_cases(cons, di),
+        "shear": lambda: shear_cases(sv),
+    }
+    for name in families or makers:
+        np.savez_compressed(OUT / f"{name}.npz", **makers[name](), **meta)
 
 
 RHS2D_OPTION_SETS = [
@@ -337,4 +398,5 @@ RHS2D_OPTION_SETS = [
 ]
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"))
+    # make_golden.py [SRC] [FAMILY ...]: regenerate the named families (default all)
+    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"), sys.argv[2:] or None)
