@@ -207,17 +207,21 @@ def serving_leg(args, dev):
 
 def shear_leg(args, dev):
     """Triply periodic shear decay u_x = 1e-3 sin(2 pi z), n^3 jittered lattice,
-    nu = 1e-2, c0 = 1: FP32 (compensated) and FP64 runs of the same driver;
-    decay rates against nu k^2 and the FP32 density field against FP64."""
+    nu = 1e-2, c0 = 1: the same driver with FP32 (compensated) pair arithmetic on
+    an FP64 state ("fp32"), everything in FP32 ("fp32_state_fp32") and all FP64;
+    decay rates against nu k^2 and the FP32 density fields against FP64."""
     import torch
     from tensorsph_b200.threed.shear import run_shear_decay
     out = {"workload": f"{args.shear_n}^3 periodic shear decay, u_x=1e-3 sin(2 pi z), nu=1e-2, "
                        f"c0=1, h=1.3dx, jitter 0.01dx (seed 0), {args.shear_steps} KDK steps"}
     runs = {}
-    for name, dtype in (("fp32", torch.float32), ("fp64", torch.float64)):
+    for name, dtype, state in (("fp32", torch.float32, torch.float64),
+                               ("fp32_state_fp32", torch.float32, torch.float32),
+                               ("fp64", torch.float64, torch.float64)):
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
-        r = run_shear_decay(n=args.shear_n, steps=args.shear_steps, dtype=dtype, device=dev)
+        r = run_shear_decay(n=args.shear_n, steps=args.shear_steps, dtype=dtype, state_dtype=state,
+                            device=dev)
         torch.cuda.synchronize(dev)
         wall = time.perf_counter() - t0
         runs[name] = r
@@ -227,10 +231,12 @@ def shear_leg(args, dev):
                      "updates_per_s": args.shear_n ** 3 * args.shear_steps / wall,
                      "momentum_final_over_scale": r.diagnostics[-1]["momentum_magnitude"]
                      / r.momentum_scale}
-    a, b = runs["fp32"], runs["fp64"]
-    out["rate_rel_diff_fp32_vs_fp64"] = (a.fit_rate - b.fit_rate) / b.fit_rate
-    out["density_max_abs_diff_over_rho0"] = float(
-        (a.final_density.double() - b.final_density).abs().max()) / 1000.0
+    b = runs["fp64"]
+    for name in ("fp32", "fp32_state_fp32"):
+        a = runs[name]
+        out[name]["rate_rel_diff_vs_fp64"] = (a.fit_rate - b.fit_rate) / b.fit_rate
+        out[name]["density_max_abs_diff_over_rho0"] = float(
+            (a.final_density.double() - b.final_density).abs().max()) / 1000.0
     return out
 
 

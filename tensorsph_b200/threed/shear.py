@@ -119,10 +119,16 @@ class ShearWaveResult:
 
 
 def _integrate(pos, vel, mass, *, box, h, nu, rho0, sound_speed, gamma, dt, steps, sample_every,
-               skin_factor, renormalise, viscous_order, wavenumber, mode, result):
+               skin_factor, renormalise, viscous_order, wavenumber, mode, result, pair_dtype=None):
+    """KDK loop.  The state (pos, vel) stays in its own dtype; with
+    ``pair_dtype`` set (FP32 on an FP64 state) the operator pass runs on a
+    rounded copy of the state each step and its accelerations are applied in
+    the state's precision."""
     dev = pos.device
     n = pos.shape[0]
-    dtype = pos.dtype
+    dtype = pos.dtype if pair_dtype is None else pair_dtype
+    mixed = dtype != pos.dtype
+    mass_p = mass.to(dtype)
     cutoff = 2.0 * h * (1.0 + skin_factor)
     skin = cutoff - 2.0 * h
     boxes = [float(box)] * 3
@@ -145,27 +151,36 @@ def _integrate(pos, vel, mass, *, box, h, nu, rho0, sound_speed, gamma, dt, step
     acc = torch.empty((n, 3), dtype=dtype, device=dev)
     rho = torch.empty(n, dtype=dtype, device=dev)
     prs = torch.empty(n, dtype=dtype, device=dev)
-    _run_rows(prm, pos, vel, mass, rowptr, entries, acc, rho, prs)
+    acc_state = torch.empty((n, 3), dtype=pos.dtype, device=dev) if mixed else acc
+
+    def operator_pass():
+        if mixed:
+            _run_rows(prm, pos.to(dtype), vel.to(dtype), mass_p, rowptr, entries, acc, rho, prs)
+            acc_state.copy_(acc)
+        else:
+            _run_rows(prm, pos, vel, mass_p, rowptr, entries, acc, rho, prs)
+
+    operator_pass()
     for k in range(steps + 1):
         if k % sample_every == 0:
             result.times.append(k * dt)
             result.amplitudes.append(mode_amplitude(pos, vel, wavenumber, mode))
             result.diagnostics.append(conservation.diagnostics(
-                pos, vel, mass, rho, rho0=rho0, sound_speed=sound_speed, gamma=gamma,
-                periodic_box=box))
+                pos, vel, mass, rho.to(pos.dtype), rho0=rho0, sound_speed=sound_speed,
+                gamma=gamma, periodic_box=box))
         if k == steps:
             break
-        _lib.check(L.tsph_kick_drift(pos.data_ptr(), vel.data_ptr(), acc.data_ptr(), n, 3,
-                                     _lib.dtype_code(dtype), float(dt), 1, box_arr, s),
+        _lib.check(L.tsph_kick_drift(pos.data_ptr(), vel.data_ptr(), acc_state.data_ptr(), n, 3,
+                                     _lib.dtype_code(pos.dtype), float(dt), 1, box_arr, s),
                    "tsph_kick_drift")
         moved = float(max_displacement(pos, reference, box=boxes))
         if 2.0 * moved > skin:
             npairs, rowptr, entries = build(pos)
             reference.copy_(pos)
             rebuilds += 1
-        _run_rows(prm, pos, vel, mass, rowptr, entries, acc, rho, prs)
-        _lib.check(L.tsph_kick_drift(None, vel.data_ptr(), acc.data_ptr(), n, 3,
-                                     _lib.dtype_code(dtype), float(dt), 0, None, s),
+        operator_pass()
+        _lib.check(L.tsph_kick_drift(None, vel.data_ptr(), acc_state.data_ptr(), n, 3,
+                                     _lib.dtype_code(pos.dtype), float(dt), 0, None, s),
                    "tsph_kick_drift")
     result.pairs_last = int(npairs)
     result.pair_rebuilds = rebuilds
@@ -220,10 +235,13 @@ def run_shear_decay(*, n: int = 64, box: float = 1.0, h_factor: float = 1.3, amp
                     gamma: float = 7.0, steps: int = 2000, dt: float | None = None,
                     jitter: float = 0.01, seed: int = 0, sample_every: int = 20,
                     skin_factor: float = 0.25, renormalise: bool = True, viscous_order: int = 2,
-                    dtype=torch.float32, device=None) -> ShearWaveResult:
+                    dtype=torch.float32, state_dtype=torch.float64,
+                    device=None) -> ShearWaveResult:
     """u_x = A sin(2 pi z / L) on an n^3 lattice with a seeded uniform jitter of
     +-jitter dx, minimum-image pairs, KDK at acoustic CFL 0.25; the mode decays
-    as exp(-nu k^2 t)."""
+    as exp(-nu k^2 t).  ``dtype`` is the pair arithmetic, ``state_dtype`` the
+    positions, velocities and integration (FP64 by default: FP32 pairs on an
+    FP64 state)."""
     dx = box / n
     h = h_factor * dx
     k = 2.0 * math.pi / box
@@ -244,7 +262,9 @@ def run_shear_decay(*, n: int = 64, box: float = 1.0, h_factor: float = 1.3, amp
     result.momentum_scale = float((mass.unsqueeze(-1) * vel.abs()).sum())
     result.analytic_rate = nu * k * k
     dev = device or _lib.cuda_device()
-    return _integrate(pos.to(dev, dtype), vel.to(dev, dtype), mass.to(dev, dtype), box=box, h=h,
+    sd = state_dtype if state_dtype is not None else dtype
+    return _integrate(pos.to(dev, sd), vel.to(dev, sd), mass.to(dev, sd), box=box, h=h,
                       nu=nu, rho0=rho0, sound_speed=sound_speed, gamma=gamma, dt=dt, steps=steps,
                       sample_every=sample_every, skin_factor=skin_factor, renormalise=renormalise,
-                      viscous_order=viscous_order, wavenumber=k, mode=1, result=result)
+                      viscous_order=viscous_order, wavenumber=k, mode=1, result=result,
+                      pair_dtype=dtype)

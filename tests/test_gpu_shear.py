@@ -37,10 +37,13 @@ def test_shear_wave_matches_reference(golden, gpu):
 def test_single_mode_decay_fp32_matches_fp64(gpu):
     from tensorsph_b200.threed.shear import run_shear_decay
     kw = dict(n=24, steps=300, sample_every=30, amplitude=1e-3, nu=1e-2, sound_speed=1.0)
-    a = run_shear_decay(dtype=torch.float32, **kw)
+    a = run_shear_decay(dtype=torch.float32, **kw)      # FP32 pairs on an FP64 state
     b = run_shear_decay(dtype=torch.float64, **kw)
     assert abs(a.fit_rate - b.fit_rate) <= 1e-3 * abs(b.fit_rate)
     drho = (a.final_density.double() - b.final_density).abs().max().item()
     assert drho / 1000.0 < 1e-5
-    # momentum stays at round-off of the momentum the flow carries
-    assert b.diagnostics[-1]["momentum_magnitude"] <= 1e-10 * b.momentum_scale
+    # the jittered lattice starts with a small momentum; its drift stays at
+    # round-off of the momentum the flow carries
+    p0 = np.asarray(b.diagnostics[0]["momentum"])
+    p1 = np.asarray(b.diagnostics[-1]["momentum"])
+    assert np.abs(p1 - p0).max() <= 1e-10 * b.momentum_scale
