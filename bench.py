@@ -172,7 +172,7 @@ def ensemble_leg(args, dev):
     batched = en.run_batched(specs, args.ensemble_steps, block=best["block"], device=dev)
     plain = en.run_plain(specs, args.plain_steps, block=128, device=dev)
     return {"workload": f"{len(specs)} independent 2-D droplet impacts (R~U[0.02,0.08] m, dx=R/20, "
-                        "depth~U[2R,6R], width 8R, U~U[1,5] m/s, seed 0), surface tension off",
+                        "depth~U[2R,6R], width 8R, U~U[1,5] m/s, seed 0), CSF sigma=0.0728 N/m",
             "fluid_particles": batched["fluid"],
             "batched_updates_per_s": batched["updates_per_s"],
             "batched_ms_per_step": 1e3 * batched["seconds"] / batched["steps"],

@@ -331,6 +331,7 @@ typedef struct {
   double ob_lo[3], ob_hi[3], ob_eps;   /* obstacle box and exit offset               */
   double shift_strength, shift_limit, shift_free_surface, shift_vref_floor;
   double grid_lo[3], grid_hi[3];       /* bounds every particle stays in (cell grid) */
+  double surface_tension;              /* CSF coefficient sigma (2-D cases); 0 = off  */
 } tsph_case_params;
 
 typedef struct tsph_engine tsph_engine; /* opaque host handle */

@@ -61,6 +61,10 @@ struct CaseDev {
   int ob_begin, n_ob, has_ob, shift_every;
   float cellf, inv_h, sigma, sig2d, rho0, bulk, gamma, inv_gamma;
   float grav, nu2, nu2f, dscale, dtf, visc_eps, rho_floor, wall_mass;
+  int csf;                 // CSF surface tension on (2-D)
+  float sigma_st, h, vol_scale;  // surface tension coefficient, h, 1 / rho0
+  int stencil_cells;       // cells each side covering the 4h fit stencil
+  float stencil2;          // (4h)^2
 };
 
 struct CaseCtl {
@@ -72,6 +76,12 @@ struct CaseCtl {
   double force[3], impulse[3];
   unsigned long long escapes, clamps, rebuilds, steps;
   double cref[2];  // [0] c_ref of the last shift, [1] max speed of the step
+  // CSF per-step reductions: max |grad c| (float bits), max |det| of the fit
+  // (double bits), median |det M| selection state
+  unsigned int csf_gmax, csf_prefix;
+  long long csf_rank;
+  unsigned long long csf_fmax;
+  float csf_med, pad2;
 };
 
 struct Dev {
@@ -96,6 +106,15 @@ struct Dev {
   float4* acc;
   float* conc;
   float4* gradc;
+  float4* csA;       // CSF: colour, M00, M01, M11
+  float4* csB;       // CSF: grad c x, y, |grad c|, |det M|
+  float2* csN0;      // CSF: raw normal
+  float2* csN1;      // CSF: normal after one Shepard pass
+  float2* csN;       // CSF: final normal
+  float4* csK;       // CSF: kappa_mls, fit b, fit a, |det fit|
+  float2* st;        // CSF: surface-tension acceleration
+  unsigned int* csf_hist;  // [n_slots][256] median-select histograms
+  int has_csf;
   uint32_t* nbr;
   int32_t* cnt;
   int32_t* ob_rows;
@@ -579,7 +598,13 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(const __grid_constant__ Dev
       ay.add(py);
       az.add(pz);
     });
-    e.acc[a] = make_float4(ax.value(), ay.value() - C.grav, az.value(), 0.f);
+    float sx = 0.f, sy = 0.f;
+    if (C.csf) {
+      const float2 st = e.st[a];
+      sx = st.x;
+      sy = st.y;
+    }
+    e.acc[a] = make_float4(ax.value() + sx, (ay.value() + sy) - C.grav, az.value(), 0.f);
   }
 }
 
@@ -652,6 +677,432 @@ __global__ void __launch_bounds__(kMaxBlock) k_reaction(Dev e) {
   } else if (c >= 0) {
     for (int k = 0; k < 3; ++k) atomicAdd(&e.ctl[c].force[k], f[k]);
   }
+}
+
+
+// ------------------------------------------------------------------ CSF ---
+// Consistent CSF surface tension (csf_consistent.py:262-446) with the
+// quadratic curvature fit (csf_curvature.py:78-166), fluid rows of 2-D cases
+// with csf on:
+//   Q1 colour c and MLS matrix M over the 2h rows (fluid neighbours)
+//   Q2 per-case median |det M| (radix select over the case's rows)
+//   Q3 grad c = M'^-T sum V (c_b - c_a) grad W, raw normal, max |grad c|
+//   Q4, Q5 two Shepard passes of the normal (self term in the denominator)
+//   Q6 kappa_mls = trace(S M'^-1)
+//   Q7 quadratic interface fit over the 4h stencil from the cell table
+//   Q8 kappa, delta_s with the flat mask, a = -sigma kappa delta_s n / rho
+// Pair sums in compensated FP32 on the exact local separations; the 2x2 and
+// 3x3 solves and the fit moments in FP64.
+
+// Per-case max of a non-negative float (block total when the block is one case).
+__device__ __forceinline__ void case_max_float(const Dev& e, int c, int cb, bool uniform, float v,
+                                               unsigned int CaseCtl::*field, float* red) {
+  if (uniform) {
+    const float m = warp_reduce_max(v);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      float t = red[0];
+      for (int w = 1; w < static_cast<int>(blockDim.x >> 5); ++w) t = fmaxf(t, red[w]);
+      if (t > 0.f) atomicMax(&(e.ctl[cb].*field), __float_as_uint(t));
+    }
+    __syncthreads();
+  } else if (c >= 0 && v > 0.f) {
+    atomicMax(&(e.ctl[c].*field), __float_as_uint(v));
+  }
+}
+
+__global__ void __launch_bounds__(kMaxBlock) k_csf_colour(const __grid_constant__ Dev e) {
+  __shared__ float4 tab[27];
+  fill_units(tab);
+  const int NF = e.NF;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    const CaseDev& C = e.cases[e.cid[a]];
+    if (!C.csf) continue;
+    const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, vs = C.vol_scale;
+    const float4 la = e.lp[a];
+    CSum<float> c, m00, m01, m11;
+    c.add((la.w * vs) * sigma);
+    walk_row(e, a, [&](const uint32_t* ent) {
+      float pc = 0.f, p00 = 0.f, p01 = 0.f, p11 = 0.f;
+#pragma unroll
+      for (int j = 0; j < kBatch; ++j) {
+        const int b0 = ent[j] != kPad ? static_cast<int>(ent[j] >> 5) : a;
+        const bool ok = ent[j] != kPad && b0 < NF;
+        const int b = ok ? b0 : a;
+        const float4 lb = e.lp[b];
+        const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u], cellf);
+        const float r2 = d.x * d.x + d.y * d.y;
+        const Radial R = radial(r2, inv_h);
+        const float vb = ok ? lb.w * vs : 0.f;
+        pc += vb * (sigma * shape(R.q));
+        const float g = -vb * (sigma * dshape(R.q) * inv_h * R.inv_r);  // -V_b gs
+        p00 += g * (d.x * d.x);
+        p01 += g * (d.x * d.y);
+        p11 += g * (d.y * d.y);
+      }
+      c.add(pc);
+      m00.add(p00);
+      m01.add(p01);
+      m11.add(p11);
+    });
+    float cv = c.value();
+    cv = cv < 0.f ? 0.f : (cv > 1.f ? 1.f : cv);
+    const float a00 = m00.value(), a01 = m01.value(), a11 = m11.value();
+    const double det = static_cast<double>(a00) * a11 - static_cast<double>(a01) * a01;
+    e.csA[a] = make_float4(cv, a00, a01, a11);
+    e.csB[a] = make_float4(0.f, 0.f, 0.f, static_cast<float>(fabs(det)));
+  }
+}
+
+// Q2: per-case radix select of the lower median of |det M| (torch.median),
+// one 8-bit digit per pass from the top; keys are the non-negative float bits.
+__global__ void k_csf_hist(const __grid_constant__ Dev e, int shift) {
+  __shared__ unsigned int h[256];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0;
+  __syncthreads();
+  const int a0 = blockIdx.x * blockDim.x;
+  const int last = min(a0 + static_cast<int>(blockDim.x), e.nf) - 1;
+  const int cb = a0 < e.nf ? e.cid[a0] : 0;
+  const bool uniform = a0 < e.nf && cb == e.cid[last];
+  const int a = a0 + threadIdx.x;
+  if (a < e.nf) {
+    const int c = e.cid[a];
+    if (e.cases[c].csf) {
+      const uint32_t key = __float_as_uint(e.csB[a].w);
+      const uint32_t prefix = e.ctl[c].csf_prefix;
+      const int hs = shift + 8;
+      if (hs >= 32 || (key >> hs) == (prefix >> hs)) {
+        const uint32_t digit = (key >> shift) & 255u;
+        if (uniform)
+          atomicAdd(&h[digit], 1u);
+        else
+          atomicAdd(&e.csf_hist[c * 256 + digit], 1u);
+      }
+    }
+  }
+  __syncthreads();
+  if (uniform)
+    for (int i = threadIdx.x; i < 256; i += blockDim.x)
+      if (h[i]) atomicAdd(&e.csf_hist[cb * 256 + i], h[i]);
+}
+
+__global__ void k_csf_pick(const __grid_constant__ Dev e, int shift) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= e.n_slots) return;
+  CaseCtl& t = e.ctl[c];
+  const CaseDev& C = e.cases[c];
+  unsigned int* h = e.csf_hist + c * 256;
+  if (!t.active || !C.csf) return;
+  if (shift == 24) {
+    t.csf_prefix = 0;
+    t.csf_rank = (C.n_fluid - 1) / 2;
+  }
+  long long k = t.csf_rank;
+  int d = 0;
+  for (; d < 255; ++d) {
+    if (k < static_cast<long long>(h[d])) break;
+    k -= h[d];
+  }
+  t.csf_prefix |= static_cast<unsigned int>(d) << shift;
+  t.csf_rank = k;
+  for (int i = 0; i < 256; ++i) h[i] = 0;
+  if (shift == 0) t.csf_med = __uint_as_float(t.csf_prefix);
+}
+
+// M' = M, or the identity where |det M| <= 1e-4 median |det M| (csf_consistent.py:106-113)
+__device__ __forceinline__ void csf_matrix(const Dev& e, int c, const float4& A, float detabs, double& p, double& q,
+                                           double& r) {
+  const float med = e.ctl[c].csf_med;
+  const float scale = med > 1e-30f ? med : 1e-30f;
+  if (detabs > 1e-4f * scale) {
+    p = A.y;
+    q = A.z;
+    r = A.w;
+  } else {
+    p = 1.0;
+    q = 0.0;
+    r = 1.0;
+  }
+}
+
+__global__ void __launch_bounds__(kMaxBlock) k_csf_grad(const __grid_constant__ Dev e) {
+  __shared__ float4 tab[27];
+  __shared__ float red[kMaxBlock / 32];
+  fill_units(tab);
+  const int a0 = blockIdx.x * blockDim.x;
+  if (a0 >= e.nf) return;
+  const int NF = e.NF;
+  const int a = a0 + threadIdx.x;
+  const int cb = e.cid[a0];
+  const bool uniform = cb == e.cid[min(a0 + static_cast<int>(blockDim.x), e.nf) - 1];
+  int c = -1;
+  float mag = 0.f;
+  if (a < e.nf) {
+    c = e.cid[a];
+    const CaseDev& C = e.cases[c];
+    if (C.csf) {
+      const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, vs = C.vol_scale;
+      const float4 la = e.lp[a];
+      const float4 A = e.csA[a];
+      CSum<float> gx, gy;
+      walk_row(e, a, [&](const uint32_t* ent) {
+        float px = 0.f, py = 0.f;
+#pragma unroll
+        for (int j = 0; j < kBatch; ++j) {
+          const int b0 = ent[j] != kPad ? static_cast<int>(ent[j] >> 5) : a;
+          const bool ok = ent[j] != kPad && b0 < NF;
+          const int b = ok ? b0 : a;
+          const float4 lb = e.lp[b];
+          const float cbv = e.csA[b].x;
+          const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u], cellf);
+          const Radial R = radial(d.x * d.x + d.y * d.y, inv_h);
+          const float gs = sigma * dshape(R.q) * inv_h * R.inv_r;
+          const float w = ok ? (lb.w * vs) * (cbv - A.x) * gs : 0.f;
+          px += w * d.x;
+          py += w * d.y;
+        }
+        gx.add(px);
+        gy.add(py);
+      });
+      double p, q, r;
+      csf_matrix(e, c, A, e.csB[a].w, p, q, r);
+      const double det = p * r - q * q;
+      const double rx = gx.value(), ry = gy.value();
+      const float g0 = static_cast<float>((r * rx - q * ry) / det);
+      const float g1 = static_cast<float>((p * ry - q * rx) / det);
+      mag = sqrtf(g0 * g0 + g1 * g1);
+      const float4 B = e.csB[a];
+      e.csB[a] = make_float4(g0, g1, mag, B.w);
+      e.csN0[a] = mag > 1e-12f ? make_float2(-g0 / mag, -g1 / mag) : make_float2(0.f, 0.f);
+    } else {
+      c = -1;
+    }
+  }
+  // every thread of the block reaches this barrier (the early return above is per block)
+  const bool all = __syncthreads_and(c >= 0 || a >= e.nf);
+  case_max_float(e, c, cb, uniform && all, mag, &CaseCtl::csf_gmax, red);
+}
+
+// Q4 / Q5: one Shepard pass of the normal field; the second pass also
+// renormalises on the interface (|grad c| > 1e-12, csf_consistent.py:320-330).
+template <bool kFinal>
+__global__ void __launch_bounds__(kMaxBlock) k_csf_smooth(const __grid_constant__ Dev e) {
+  __shared__ float4 tab[27];
+  fill_units(tab);
+  const int NF = e.NF;
+  const float2* __restrict__ src = kFinal ? e.csN1 : e.csN0;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    const CaseDev& C = e.cases[e.cid[a]];
+    if (!C.csf) continue;
+    const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, vs = C.vol_scale;
+    const float4 la = e.lp[a];
+    CSum<float> nx, ny, den;
+    den.add((la.w * vs) * sigma);
+    walk_row(e, a, [&](const uint32_t* ent) {
+      float px = 0.f, py = 0.f, pd = 0.f;
+#pragma unroll
+      for (int j = 0; j < kBatch; ++j) {
+        const int b0 = ent[j] != kPad ? static_cast<int>(ent[j] >> 5) : a;
+        const bool ok = ent[j] != kPad && b0 < NF;
+        const int b = ok ? b0 : a;
+        const float4 lb = e.lp[b];
+        const float2 nb = src[b];
+        const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u], cellf);
+        const float w = ok ? (lb.w * vs) * (sigma * shape(radial(d.x * d.x + d.y * d.y, inv_h).q)) : 0.f;
+        px += w * nb.x;
+        py += w * nb.y;
+        pd += w;
+      }
+      nx.add(px);
+      ny.add(py);
+      den.add(pd);
+    });
+    float dd = den.value();
+    dd = dd > 1e-30f ? dd : 1e-30f;
+    const float sx = nx.value() / dd, sy = ny.value() / dd;
+    if (!kFinal) {
+      e.csN1[a] = make_float2(sx, sy);
+    } else {
+      const float mag = e.csB[a].z;
+      float2 out = e.csN0[a];
+      if (mag > 1e-12f) {
+        float nrm = sqrtf(sx * sx + sy * sy);
+        nrm = nrm > 1e-12f ? nrm : 1e-12f;
+        out = make_float2(sx / nrm, sy / nrm);
+      }
+      e.csN[a] = out;
+    }
+  }
+}
+
+// Q6: kappa_mls = trace(S M'^-1), S = sum V_b (n_b - n_a) (x) grad_a W
+__global__ void __launch_bounds__(kMaxBlock) k_csf_div(const __grid_constant__ Dev e) {
+  __shared__ float4 tab[27];
+  fill_units(tab);
+  const int NF = e.NF;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    const int c = e.cid[a];
+    const CaseDev& C = e.cases[c];
+    if (!C.csf) continue;
+    const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, vs = C.vol_scale;
+    const float4 la = e.lp[a];
+    const float2 na = e.csN[a];
+    CSum<float> s00, s01, s10, s11;
+    walk_row(e, a, [&](const uint32_t* ent) {
+      float q00 = 0.f, q01 = 0.f, q10 = 0.f, q11 = 0.f;
+#pragma unroll
+      for (int j = 0; j < kBatch; ++j) {
+        const int b0 = ent[j] != kPad ? static_cast<int>(ent[j] >> 5) : a;
+        const bool ok = ent[j] != kPad && b0 < NF;
+        const int b = ok ? b0 : a;
+        const float4 lb = e.lp[b];
+        const float2 nb = e.csN[b];
+        const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u], cellf);
+        const Radial R = radial(d.x * d.x + d.y * d.y, inv_h);
+        const float gs = ok ? (lb.w * vs) * (sigma * dshape(R.q) * inv_h * R.inv_r) : 0.f;
+        const float g0 = gs * d.x, g1 = gs * d.y;
+        const float dn0 = nb.x - na.x, dn1 = nb.y - na.y;
+        q00 += dn0 * g0;
+        q01 += dn0 * g1;
+        q10 += dn1 * g0;
+        q11 += dn1 * g1;
+      }
+      s00.add(q00);
+      s01.add(q01);
+      s10.add(q10);
+      s11.add(q11);
+    });
+    double p, q, r;
+    csf_matrix(e, c, e.csA[a], e.csB[a].w, p, q, r);
+    const double det = p * r - q * q;
+    // M'^-1 = [r -q; -q p] / det; trace(S M'^-1)
+    const double k = (s00.value() * r - s01.value() * q - s10.value() * q + s11.value() * p) / det;
+    float4 K = e.csK[a];
+    K.x = static_cast<float>(k);
+    e.csK[a] = K;
+  }
+}
+
+// Q7: weighted fit v = c + b u + a u^2 in the frame (t, n) of row a over the
+// fluid particles within 4h (cells within stencil_cells of the home cell),
+// weights w_b = |grad c|_b / max |grad c| (= delta_s / max delta_s).
+__global__ void __launch_bounds__(kMaxBlock) k_csf_fit(const __grid_constant__ Dev e) {
+  const int a0 = blockIdx.x * blockDim.x;
+  if (a0 >= e.nf) return;
+  const int a = a0 + threadIdx.x;
+  const int cb = e.cid[a0];
+  const bool uniform = cb == e.cid[min(a0 + static_cast<int>(blockDim.x), e.nf) - 1];
+  int c = -1;
+  double detabs = 0.0;
+  if (a < e.nf) {
+    c = e.cid[a];
+    const CaseDev& C = e.cases[c];
+    if (C.csf) {
+      const float gmax = __uint_as_float(e.ctl[c].csf_gmax);
+      const float inv_g = 1.f / (gmax > 1e-30f ? gmax : 1e-30f);
+      const float4 la = e.lp[a];
+      const float2 na = e.csN[a];
+      const float tx = -na.y, ty = na.x;
+      const float cellf = C.cellf, st2 = C.stencil2;
+      const int key = e.home[a] - C.key_off;
+      const int cy = (key / C.ncz) % C.ncy, cx = key / (C.ncz * C.ncy);
+      const int sc = C.stencil_cells;
+      double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      for (int dx = -sc; dx <= sc; ++dx) {
+        const int x = cx + dx;
+        if (x < 0 || x >= C.ncx) continue;
+        for (int dy = -sc; dy <= sc; ++dy) {
+          const int y = cy + dy;
+          if (y < 0 || y >= C.ncy) continue;
+          const int cell = C.key_off + (x * C.ncy + y) * C.ncz;
+          const int fs = e.fstart[cell];
+          if (fs < 0) continue;
+          const int fe = e.fend[cell];
+          const float ox = static_cast<float>(dx), oy = static_cast<float>(dy);
+          for (int b = fs; b < fe; ++b) {
+            if (b == a) continue;
+            const float4 lb = e.lp[b];
+            const float ddx = fmaf(-ox, cellf, la.x - lb.x), ddy = fmaf(-oy, cellf, la.y - lb.y);
+            if (ddx * ddx + ddy * ddy > st2) continue;
+            float w = e.csB[b].z * inv_g;
+            w = w < 0.f ? 0.f : (w > 1.f ? 1.f : w);
+            const double u = static_cast<double>(-(ddx * tx + ddy * ty));
+            const double v = static_cast<double>(-(ddx * na.x + ddy * na.y));
+            const double uu = u * u;
+            s[0] += w;
+            s[1] += w * u;
+            s[2] += w * v;
+            s[3] += w * uu;
+            s[4] += w * u * v;
+            s[5] += w * uu * u;
+            s[6] += w * uu * v;
+            s[7] += w * uu * uu;
+          }
+        }
+      }
+      float wa = e.csB[a].z * inv_g;
+      wa = wa < 0.f ? 0.f : (wa > 1.f ? 1.f : wa);
+      s[0] += wa;
+      // [s0 s1 s3; s1 s3 s5; s3 s5 s7] (c, b, a) = (s2, s4, s6)
+      const double m00 = s[0], m01 = s[1], m02 = s[3], m11 = s[3], m12 = s[5], m22 = s[7];
+      const double c0 = m11 * m22 - m12 * m12, c1 = m01 * m22 - m12 * m02, c2 = m01 * m12 - m11 * m02;
+      const double det = m00 * c0 - m01 * c1 + m02 * c2;
+      const double r0 = s[2], r1 = s[4], r2 = s[6];
+      // Cramer's rule for the second and third unknowns
+      const double detb = m00 * (r1 * m22 - m12 * r2) - r0 * (m01 * m22 - m12 * m02) + m02 * (m01 * r2 - r1 * m02);
+      const double deta = m00 * (m11 * r2 - r1 * m12) - m01 * (m01 * r2 - r1 * m02) + r0 * (m01 * m12 - m11 * m02);
+      detabs = fabs(det);
+      float kfit = 0.f;
+      if (det != 0.0) {
+        const double bb = detb / det, aa = deta / det;
+        kfit = static_cast<float>(-2.0 * aa / pow(1.0 + bb * bb, 1.5));
+      }
+      float4 K = e.csK[a];
+      K.y = kfit;
+      K.z = wa;
+      K.w = static_cast<float>(detabs);
+      e.csK[a] = K;
+    } else {
+      c = -1;
+    }
+  }
+  __shared__ double red[kMaxBlock / 32];
+  const bool all = __syncthreads_and(c >= 0 || a >= e.nf);
+  if (uniform && all) {
+    const double m = block_reduce<true>(detabs, red);
+    if (threadIdx.x == 0) atomic_max_nonneg(&e.ctl[cb].csf_fmax, m);
+  } else if (c >= 0) {
+    atomic_max_nonneg(&e.ctl[c].csf_fmax, detabs);
+  }
+}
+
+// Q8: kappa (fit where active and regular, else kappa_mls), delta_s = 2|grad c|
+// with the flat mask, a = -sigma kappa delta_s n / rho
+__global__ void k_csf_final(const __grid_constant__ Dev e) {
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    const int c = e.cid[a];
+    const CaseDev& C = e.cases[c];
+    if (!C.csf) continue;
+    const CaseCtl& t = e.ctl[c];
+    const float4 K = e.csK[a];
+    const double det_max = ::fmax(__longlong_as_double(static_cast<long long>(t.csf_fmax)), 1e-30);
+    const bool ok = K.z > 0.05f && static_cast<double>(K.w) > 1e-6 * det_max;
+    const float kappa = ok ? K.y : K.x;
+    const float mag = e.csB[a].z;
+    const float gmax = __uint_as_float(t.csf_gmax);
+    const float ds = mag <= 1e-3f * gmax ? 0.f : 2.f * mag;
+    const float2 n = e.csN[a];
+    const float f = -C.sigma_st * kappa * ds / e.rho[a];
+    e.st[a] = make_float2(f * n.x, f * n.y);
+  }
+}
+
+__global__ void k_csf_clear(Dev e) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= e.n_slots) return;
+  e.ctl[c].csf_gmax = 0;
+  e.ctl[c].csf_fmax = 0;
 }
 
 // Semi-implicit Euler, box and obstacle clamps, per-case meters (of the state
@@ -1103,6 +1554,14 @@ size_t carve(const tsph_engine_params& p, Dev* d, char* base, CaseDev** cases, c
   t.acc = static_cast<float4*>(take(NF * sizeof(float4)));
   t.conc = static_cast<float*>(take(NF * sizeof(float)));
   t.gradc = static_cast<float4*>(take(NF * sizeof(float4)));
+  t.csA = static_cast<float4*>(take(NF * sizeof(float4)));
+  t.csB = static_cast<float4*>(take(NF * sizeof(float4)));
+  t.csN0 = static_cast<float2*>(take(NF * sizeof(float2)));
+  t.csN1 = static_cast<float2*>(take(NF * sizeof(float2)));
+  t.csN = static_cast<float2*>(take(NF * sizeof(float2)));
+  t.csK = static_cast<float4*>(take(NF * sizeof(float4)));
+  t.st = static_cast<float2*>(take(NF * sizeof(float2)));
+  t.csf_hist = static_cast<unsigned int*>(take(static_cast<size_t>(p.max_cases) * 256 * sizeof(unsigned int)));
   t.nbr = static_cast<uint32_t*>(take(static_cast<size_t>(p.max_neighbors) * N * sizeof(uint32_t)));
   t.cnt = static_cast<int32_t*>(take(N * sizeof(int32_t)));
   t.ob_rows = static_cast<int32_t*>(take(std::max<int64_t>(p.max_obstacle, 1) * sizeof(int32_t)));
@@ -1153,6 +1612,8 @@ bool shifting(const tsph_engine* E) { return E->order.size() == 1 && E->order[0]
 void batch_changed(tsph_engine* E) {
   Dev& d = E->d;
   d.shift_slot = shifting(E) ? E->order[0].slot : 0;
+  d.has_csf = 0;
+  for (const CaseHost& c : E->order) d.has_csf |= c.dev.csf;
   if (E->order.size() == 1) {
     d.one = E->order[0].dev;
     d.one_slot = E->order[0].slot;
@@ -1209,6 +1670,22 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr) {
   (one ? k_diffusion_eos<true> : k_diffusion_eos<false>)<<<g, B, 0, s>>>(d);
   mark();
   if (d.nw) (one ? k_walls<true> : k_walls<false>)<<<grid_for(d.nw, B), B, 0, s>>>(d);
+  if (d.has_csf) {
+    const unsigned gf = static_cast<unsigned>((d.nf + B - 1) / B);
+    k_csf_clear<<<gc, 128, 0, s>>>(d);
+    k_csf_colour<<<g, B, 0, s>>>(d);
+    for (int shift = 24; shift >= 0; shift -= 8) {
+      k_csf_hist<<<gf, B, 0, s>>>(d, shift);
+      k_csf_pick<<<gc, 128, 0, s>>>(d, shift);
+    }
+    k_csf_grad<<<gf, B, 0, s>>>(d);
+    k_csf_smooth<false><<<g, B, 0, s>>>(d);
+    k_csf_smooth<true><<<g, B, 0, s>>>(d);
+    k_csf_div<<<g, B, 0, s>>>(d);
+    k_csf_fit<<<gf, B, 0, s>>>(d);
+    k_csf_final<<<g, B, 0, s>>>(d);
+    TSPH_LAUNCH_CHECK();
+  }
   mark();
   (one ? k_force<true> : k_force<false>)<<<g, B, 0, s>>>(d);
   mark();
@@ -1290,6 +1767,12 @@ CaseDev make_case_dev(const tsph_case_params& p, int64_t* ncells) {
   c.visc_eps = static_cast<float>(0.01 * p.h * p.h);
   c.rho_floor = static_cast<float>(0.1 * p.rho0);
   c.wall_mass = static_cast<float>(p.wall_mass);
+  c.csf = (p.surface_tension > 0.0 && p.dim == 2) ? 1 : 0;
+  c.sigma_st = static_cast<float>(p.surface_tension);
+  c.h = static_cast<float>(p.h);
+  c.vol_scale = static_cast<float>(1.0 / p.rho0);
+  c.stencil_cells = static_cast<int>(std::ceil((4.0 * p.h + p.skin) / cell));
+  c.stencil2 = static_cast<float>(16.0 * p.h * p.h);
   return c;
 }
 
@@ -1521,6 +2004,11 @@ int tsph_engine_remove_case(tsph_engine* E, int64_t case_id, tsph_stream stream)
   E->free_slots.push_back(gone.slot);
   batch_changed(E);
   if ((rc = refresh_wall_table(E, s))) return rc;
+  // the fluid cell table (read by the CSF fit between rebuilds) follows the keys
+  if (E->total_cells > 0)
+    k_clear_table<<<grid_for(E->total_cells, 256), 256, 0, s>>>(d.fstart, d.fend, E->total_cells, nullptr);
+  if (d.nf) k_fill_table<<<grid_for(d.nf, 256), 256, 0, s>>>(d.home, nullptr, d.nf, d.fstart, d.fend, nullptr);
+  TSPH_LAUNCH_CHECK();
   invalidate_graph(E);
   TSPH_CUDA_CHECK(cudaStreamSynchronize(s));
   return TSPH_OK;

@@ -243,11 +243,16 @@ def droplet_impact_case(cfg, *, drop_speed: float = 0.0, label: str = "") -> Cas
     circular drop from ``make_particles``, walls from ``wall_lattice`` up to
     ``domain_top``, droplet_impact.py:666-760) as a ``CaseSpec``; the drop
     starts with the downward speed ``drop_speed`` (the reference drops it from
-    rest).  Surface tension is not part of the device engine."""
+    rest).  ``surface_tension_coefficient > 0`` turns on the consistent CSF
+    force with the quadratic curvature fit (csf_consistent.py:384-446)."""
     from .droplet_impact import domain_top, lattice_mass_unit, make_particles, validate_config, wall_lattice
     validate_config(cfg)
     if cfg.surface_tension_coefficient > 0.0:
-        raise NotImplementedError("surface tension is not part of the device engine")
+        if (cfg.csf_scheme != "consistent" or cfg.csf_curvature != "fit_quadratic"
+                or cfg.csf_delta_normalization != "legacy" or cfg.contact_angle is not None):
+            raise NotImplementedError("the device engine implements the consistent CSF scheme "
+                                      "with the fit_quadratic curvature, legacy delta_s and no "
+                                      "contact angle")
     if cfg.density_renormalization or cfg.boundary_consistent_density:
         raise NotImplementedError("density_renormalization and boundary_consistent_density are "
                                   "not part of the device engine")
@@ -264,6 +269,7 @@ def droplet_impact_case(cfg, *, drop_speed: float = 0.0, label: str = "") -> Cas
     p = _case_params(dim=2, n_fluid=x.shape[0], n_wall=wall.shape[0], n_obstacle=0, cfg=cfg, h=h,
                      wall_mass=lattice_mass_unit(cfg), box_hi=(cfg.pool_width, top, 0.0),
                      lo=allpos.min(dim=0).values.tolist(), hi=allpos.max(dim=0).values.tolist())
+    p.surface_tension = float(cfg.surface_tension_coefficient)
     return CaseSpec(p, x, v, mass.double().contiguous(), wall, label or "droplet_impact")
 
 

@@ -4,8 +4,10 @@ An ensemble draws its cases from one seed: drop radius R ~ U[0.02, 0.08] m at
 dx = R / 20, pool depth ~ U[2R, 6R], pool width 8R and impact speed
 U ~ U[1, 5] m/s (rho0 = 1000).  Every case gets c0 = 10 max(U, sqrt(2 g d))
 (Mach <= 0.1) and dt at acoustic CFL 0.25; the rest is the reference
-``Config`` (droplet_impact.py:55-269).  With dx tied to R the particle count
-depends on the depth ratio only: 7.7k (pool 2R) to 20.5k (pool 6R) fluid.
+``Config`` (droplet_impact.py:55-269) with CSF surface tension sigma =
+0.0728 N/m (consistent scheme, quadratic curvature fit).  With dx tied to R
+the particle count depends on the depth ratio only: 7.7k (pool 2R) to 20.5k
+(pool 6R) fluid.
 
 ``run_batched`` advances all cases in one engine (one CUDA graph per step for
 the whole ensemble); ``run_plain`` runs the same cases one at a time, each in
@@ -48,19 +50,20 @@ def draw_ensemble(n: int = 256, seed: int = 0) -> list[DropletDraw]:
 
 
 def droplet_config(draw: DropletDraw, *, skin_factor: float = 0.25, courant: float = 0.25,
-                   viscosity: float = 1.0e-6) -> Config:
+                   viscosity: float = 1.0e-6, surface_tension: float = 0.0728) -> Config:
     dx = draw.radius / 20.0
     c0 = 10.0 * max(draw.speed, math.sqrt(2.0 * 9.81 * draw.depth))
     h = 1.3 * dx
     return Config(dx=dx, pool_width=8.0 * draw.radius, pool_depth=draw.depth,
                   drop_radius=draw.radius, drop_center_y=draw.depth + draw.radius + 1.5 * dx,
                   sound_speed=c0, viscosity=viscosity, dt=courant * h / c0, max_courant=courant,
-                  pair_skin_factor=skin_factor, surface_tension_coefficient=0.0)
+                  pair_skin_factor=skin_factor, surface_tension_coefficient=surface_tension)
 
 
-def ensemble_specs(draws, *, skin_factor: float = 0.25) -> list[CaseSpec]:
-    return [droplet_impact_case(droplet_config(d, skin_factor=skin_factor), drop_speed=d.speed,
-                                label=f"droplet R={d.radius:.4f}") for d in draws]
+def ensemble_specs(draws, *, skin_factor: float = 0.25, surface_tension: float = 0.0728) -> list[CaseSpec]:
+    return [droplet_impact_case(droplet_config(d, skin_factor=skin_factor,
+                                               surface_tension=surface_tension),
+                                drop_speed=d.speed, label=f"droplet R={d.radius:.4f}") for d in draws]
 
 
 def _timed_steps(eng: BatchEngine, steps: int) -> float:

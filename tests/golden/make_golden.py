@@ -360,6 +360,47 @@ def shear_cases(sv):
     return data
 
 
+def csf_cases(ca, di):
+    """Surface-tension acceleration and fields of the consistent CSF scheme
+    (csf_consistent.py:384-446, fit_quadratic curvature) on a lattice drop, a
+    jittered drop and a drop above a pool, and one full ``rhs`` with it."""
+    data = {}
+    k = 0
+    for dtype in (torch.float64, torch.float32):
+        for kind in ("drop", "jitter", "pool"):
+            g = torch.Generator().manual_seed(80 + k)
+            dx = 0.002
+            h = 1.3 * dx
+            if kind == "pool":
+                cfg = di.Config(dx=dx, pool_width=0.08, pool_depth=0.02, drop_radius=0.01,
+                                drop_center_y=0.035)
+                pos, mass = di.make_particles(cfg, "cpu")
+                pos, mass = pos.to(dtype), mass.to(dtype)
+            else:
+                ax = (torch.arange(-12, 13, dtype=torch.float64) * dx)
+                gx, gy = torch.meshgrid(ax, ax, indexing="xy")
+                pts = torch.stack((gx.reshape(-1), gy.reshape(-1)), -1)
+                pts = pts[torch.linalg.vector_norm(pts, dim=1) <= 10.5 * dx]
+                if kind == "jitter":
+                    pts = pts + 0.05 * dx * torch.randn(pts.shape, generator=g, dtype=torch.float64)
+                pos = (pts + 0.05).to(dtype)
+                mass = torch.full((pos.shape[0],), 1000.0 * dx * dx, dtype=dtype)
+            rho = (1000.0 * (1.0 + 0.002 * torch.randn((pos.shape[0],), generator=g,
+                                                        dtype=torch.float64))).to(dtype)
+            pairs = di.cell_linked_pairs(pos, 2.0 * h)
+            acc, st = ca.surface_tension_acceleration(pos, rho, mass, pairs, h, 0.0728, rho0=1000.0,
+                                                      curvature_scheme="fit_quadratic",
+                                                      delta_normalization="legacy")
+            for name, t in dict(pos=pos, mass=mass, rho=rho, acc=acc, color=st.color,
+                                grad_c=st.grad_c, normal=st.normal, kappa=st.kappa,
+                                delta_s=st.delta_s).items():
+                data[f"c{k}_{name}"] = _np(t)
+            data[f"c{k}_h"] = np.float64(h)
+            k += 1
+    data["count"] = np.int64(k)
+    return data
+
+
 def main(src, families=None):
     sys.path.insert(0, str(src))
     import tensorsph.neighbor_search as ns
@@ -371,6 +412,7 @@ def main(src, families=None):
     from tensorsph.threed import neighbors3 as n3
     from tensorsph.threed import conservation as cons
     from tensorsph.threed import solver as sv
+    import tensorsph.csf_consistent as ca
 
     meta = {"torch_version": np.array(torch.__version__)}
     torch.set_num_threads(1)
@@ -384,6 +426,7 @@ def main(src, families=None):
         "shift": lambda: shift_cases(ps, di),
         "meters": lambda: meters_cases(cons, di),
         "shear": lambda: shear_cases(sv),
+        "csf": lambda: csf_cases(ca, di),
     }
     for name in families or makers:
         np.savez_compressed(OUT / f"{name}.npz", **makers[name](), **meta)

@@ -177,3 +177,26 @@ def test_meters_oracle_matches_reference(golden):
         dens = om.density_from_neighbor_pairs(pos, mass, 0.03, pairs)
         ref = g[f"c{k}_rho_pairs"]
         assert np.abs(dens - ref).max() <= (2e-6 if fp32 else 1e-12) * np.abs(ref).max(), k
+
+
+def test_csf_oracle_matches_reference(golden):
+    """The oracle's consistent CSF (fit_quadratic curvature) against the
+    reference's own FP64 output; fields compared where they carry force
+    (delta_s > 0: interior normals are round-off directions)."""
+    from oracle import csf
+    g = golden("csf")
+    for k in range(int(g["count"])):
+        pos = g[f"c{k}_pos"]
+        if pos.dtype != np.float64:
+            continue
+        acc, st = csf.surface_tension_acceleration(pos, g[f"c{k}_rho"], g[f"c{k}_mass"],
+                                                   float(g[f"c{k}_h"]), 0.0728, 1000.0)
+        ref = g[f"c{k}_acc"]
+        assert np.abs(acc - ref).max() <= 1e-10 * np.abs(ref).max(), k
+        live = g[f"c{k}_delta_s"] > 0
+        for name in ("color", "grad_c", "delta_s"):
+            r = g[f"c{k}_{name}"]
+            assert np.abs(st[name] - r).max() <= 1e-12 * max(np.abs(r).max(), 1.0), (k, name)
+        for name in ("normal", "kappa"):
+            r = g[f"c{k}_{name}"][live]
+            assert np.abs(st[name][live] - r).max() <= 1e-8 * np.abs(r).max(), (k, name)
