@@ -62,9 +62,9 @@ struct CaseDev {
   float cellf, inv_h, sigma, sig2d, rho0, bulk, gamma, inv_gamma;
   float grav, nu2, nu2f, dscale, dtf, visc_eps, rho_floor, wall_mass;
   int csf;                 // CSF surface tension on (2-D)
-  float sigma_st, h, vol_scale;  // surface tension coefficient, h, 1 / rho0
   int stencil_cells;       // cells each side covering the 4h fit stencil
-  float stencil2;          // (4h)^2
+  double sigma_st, h_d, sigma2d_d, vol_scale;  // CSF: sigma, h, 10/(7 pi h^2), 1/rho0
+  double stencil2;         // (4h)^2
 };
 
 struct CaseCtl {
@@ -78,10 +78,10 @@ struct CaseCtl {
   double cref[2];  // [0] c_ref of the last shift, [1] max speed of the step
   // CSF per-step reductions: max |grad c| (float bits), max |det| of the fit
   // (double bits), median |det M| selection state
-  unsigned int csf_gmax, csf_prefix;
+  unsigned long long csf_gmax, csf_prefix;
   long long csf_rank;
   unsigned long long csf_fmax;
-  float csf_med, pad2;
+  double csf_med;
 };
 
 struct Dev {
@@ -106,12 +106,12 @@ struct Dev {
   float4* acc;
   float* conc;
   float4* gradc;
-  float4* csA;       // CSF: colour, M00, M01, M11
-  float4* csB;       // CSF: grad c x, y, |grad c|, |det M|
-  float2* csN0;      // CSF: raw normal
-  float2* csN1;      // CSF: normal after one Shepard pass
-  float2* csN;       // CSF: final normal
-  float4* csK;       // CSF: kappa_mls, fit b, fit a, |det fit|
+  double4* csA;      // CSF: colour, M00, M01, M11
+  double4* csB;      // CSF: grad c x, y, |grad c|, |det M|
+  double2* csN0;     // CSF: raw normal
+  double2* csN1;     // CSF: normal after one Shepard pass
+  double2* csN;      // CSF: final normal
+  double4* csK;      // CSF: kappa_mls, kappa_fit, own fit weight, |det fit|
   float2* st;        // CSF: surface-tension acceleration
   unsigned int* csf_hist;  // [n_slots][256] median-select histograms
   int has_csf;
@@ -691,72 +691,80 @@ __global__ void __launch_bounds__(kMaxBlock) k_reaction(Dev e) {
 //   Q6 kappa_mls = trace(S M'^-1)
 //   Q7 quadratic interface fit over the 4h stencil from the cell table
 //   Q8 kappa, delta_s with the flat mask, a = -sigma kappa delta_s n / rho
-// Pair sums in compensated FP32 on the exact local separations; the 2x2 and
-// 3x3 solves and the fit moments in FP64.
+// The operator differentiates the colour twice and divides by |grad c|, so
+// FP32 cancellation in c_b - c_a (c ~ 1) reaches the force at the 1e-3 level;
+// these passes therefore run in FP64 on the FP64 positions.
 
-// Per-case max of a non-negative float (block total when the block is one case).
-__device__ __forceinline__ void case_max_float(const Dev& e, int c, int cb, bool uniform, float v,
-                                               unsigned int CaseCtl::*field, float* red) {
+__device__ __forceinline__ double shape_d(double q) {
+  const double t = 2.0 - q;
+  return q < 1.0 ? 1.0 - 1.5 * q * q + 0.75 * q * q * q : (q < 2.0 ? 0.25 * t * t * t : 0.0);
+}
+__device__ __forceinline__ double dshape_d(double q) {
+  const double t = 2.0 - q;
+  return q < 1.0 ? -3.0 * q + 2.25 * q * q : (q < 2.0 ? -0.75 * t * t : 0.0);
+}
+
+// W and grad_a W = d * gs for the separation d = x_a - x_b (2-D cubic spline,
+// gradient scale with r clamped to 1e-12 as the reference's kernel does)
+struct KD {
+  double w, gs;
+};
+__device__ __forceinline__ KD kernel_d(double dx, double dy, const CaseDev& C) {
+  const double r = sqrt(dx * dx + dy * dy);
+  const double q = r / C.h_d;
+  KD k;
+  k.w = C.sigma2d_d * shape_d(q);
+  k.gs = C.sigma2d_d * dshape_d(q) / (C.h_d * fmax(r, 1e-12));
+  return k;
+}
+
+// Loop the fluid neighbours b of fluid row a (2h rows; walls skipped).
+template <class Body>
+__device__ __forceinline__ void fluid_row(const Dev& e, int a, Body&& body) {
+  const int n = e.cnt[a];
+  const uint32_t* row = e.nbr + a;
+  for (int k = 0; k < n; ++k) {
+    const uint32_t b = row[static_cast<int64_t>(k) * e.rows] >> 5;
+    if (b < static_cast<uint32_t>(e.NF)) body(static_cast<int>(b));
+  }
+}
+
+// Per-case max of a non-negative double (block total when the block is one case).
+__device__ __forceinline__ void case_max_double(const Dev& e, int c, int cb, bool uniform, double v,
+                                                unsigned long long CaseCtl::*field, double* red) {
   if (uniform) {
-    const float m = warp_reduce_max(v);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      float t = red[0];
-      for (int w = 1; w < static_cast<int>(blockDim.x >> 5); ++w) t = fmaxf(t, red[w]);
-      if (t > 0.f) atomicMax(&(e.ctl[cb].*field), __float_as_uint(t));
-    }
-    __syncthreads();
-  } else if (c >= 0 && v > 0.f) {
-    atomicMax(&(e.ctl[c].*field), __float_as_uint(v));
+    const double m = block_reduce<true>(v, red);
+    if (threadIdx.x == 0) atomic_max_nonneg(&(e.ctl[cb].*field), m);
+  } else if (c >= 0) {
+    atomic_max_nonneg(&(e.ctl[c].*field), v);
   }
 }
 
 __global__ void __launch_bounds__(kMaxBlock) k_csf_colour(const __grid_constant__ Dev e) {
-  __shared__ float4 tab[27];
-  fill_units(tab);
-  const int NF = e.NF;
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
     const CaseDev& C = e.cases[e.cid[a]];
     if (!C.csf) continue;
-    const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, vs = C.vol_scale;
-    const float4 la = e.lp[a];
-    CSum<float> c, m00, m01, m11;
-    c.add((la.w * vs) * sigma);
-    walk_row(e, a, [&](const uint32_t* ent) {
-      float pc = 0.f, p00 = 0.f, p01 = 0.f, p11 = 0.f;
-#pragma unroll
-      for (int j = 0; j < kBatch; ++j) {
-        const int b0 = ent[j] != kPad ? static_cast<int>(ent[j] >> 5) : a;
-        const bool ok = ent[j] != kPad && b0 < NF;
-        const int b = ok ? b0 : a;
-        const float4 lb = e.lp[b];
-        const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u], cellf);
-        const float r2 = d.x * d.x + d.y * d.y;
-        const Radial R = radial(r2, inv_h);
-        const float vb = ok ? lb.w * vs : 0.f;
-        pc += vb * (sigma * shape(R.q));
-        const float g = -vb * (sigma * dshape(R.q) * inv_h * R.inv_r);  // -V_b gs
-        p00 += g * (d.x * d.x);
-        p01 += g * (d.x * d.y);
-        p11 += g * (d.y * d.y);
-      }
-      c.add(pc);
-      m00.add(p00);
-      m01.add(p01);
-      m11.add(p11);
+    const double4 pa = ld4(e.pos, a);
+    double c = pa.w * C.vol_scale * C.sigma2d_d, m00 = 0.0, m01 = 0.0, m11 = 0.0;
+    fluid_row(e, a, [&](int b) {
+      const double4 pb = ld4(e.pos, b);
+      const double dx = pa.x - pb.x, dy = pa.y - pb.y;
+      const KD k = kernel_d(dx, dy, C);
+      const double vb = pb.w * C.vol_scale;
+      c += vb * k.w;
+      const double g = -vb * k.gs;  // M += V_b (-d) (x) (d gs)
+      m00 += g * (dx * dx);
+      m01 += g * (dx * dy);
+      m11 += g * (dy * dy);
     });
-    float cv = c.value();
-    cv = cv < 0.f ? 0.f : (cv > 1.f ? 1.f : cv);
-    const float a00 = m00.value(), a01 = m01.value(), a11 = m11.value();
-    const double det = static_cast<double>(a00) * a11 - static_cast<double>(a01) * a01;
-    e.csA[a] = make_float4(cv, a00, a01, a11);
-    e.csB[a] = make_float4(0.f, 0.f, 0.f, static_cast<float>(fabs(det)));
+    c = c < 0.0 ? 0.0 : (c > 1.0 ? 1.0 : c);
+    e.csA[a] = make_double4(c, m00, m01, m11);
+    e.csB[a] = make_double4(0.0, 0.0, 0.0, fabs(m00 * m11 - m01 * m01));
   }
 }
 
 // Q2: per-case radix select of the lower median of |det M| (torch.median),
-// one 8-bit digit per pass from the top; keys are the non-negative float bits.
+// 8 bits per pass from the top of the non-negative double's bit pattern.
 __global__ void k_csf_hist(const __grid_constant__ Dev e, int shift) {
   __shared__ unsigned int h[256];
   for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0;
@@ -769,11 +777,11 @@ __global__ void k_csf_hist(const __grid_constant__ Dev e, int shift) {
   if (a < e.nf) {
     const int c = e.cid[a];
     if (e.cases[c].csf) {
-      const uint32_t key = __float_as_uint(e.csB[a].w);
-      const uint32_t prefix = e.ctl[c].csf_prefix;
+      const unsigned long long key = static_cast<unsigned long long>(__double_as_longlong(e.csB[a].w));
+      const unsigned long long prefix = e.ctl[c].csf_prefix;
       const int hs = shift + 8;
-      if (hs >= 32 || (key >> hs) == (prefix >> hs)) {
-        const uint32_t digit = (key >> shift) & 255u;
+      if (hs >= 64 || (key >> hs) == (prefix >> hs)) {
+        const unsigned int digit = static_cast<unsigned int>((key >> shift) & 255u);
         if (uniform)
           atomicAdd(&h[digit], 1u);
         else
@@ -794,7 +802,7 @@ __global__ void k_csf_pick(const __grid_constant__ Dev e, int shift) {
   const CaseDev& C = e.cases[c];
   unsigned int* h = e.csf_hist + c * 256;
   if (!t.active || !C.csf) return;
-  if (shift == 24) {
+  if (shift == 56) {
     t.csf_prefix = 0;
     t.csf_rank = (C.n_fluid - 1) / 2;
   }
@@ -804,18 +812,17 @@ __global__ void k_csf_pick(const __grid_constant__ Dev e, int shift) {
     if (k < static_cast<long long>(h[d])) break;
     k -= h[d];
   }
-  t.csf_prefix |= static_cast<unsigned int>(d) << shift;
+  t.csf_prefix |= static_cast<unsigned long long>(d) << shift;
   t.csf_rank = k;
   for (int i = 0; i < 256; ++i) h[i] = 0;
-  if (shift == 0) t.csf_med = __uint_as_float(t.csf_prefix);
+  if (shift == 0) t.csf_med = __longlong_as_double(static_cast<long long>(t.csf_prefix));
 }
 
 // M' = M, or the identity where |det M| <= 1e-4 median |det M| (csf_consistent.py:106-113)
-__device__ __forceinline__ void csf_matrix(const Dev& e, int c, const float4& A, float detabs, double& p, double& q,
-                                           double& r) {
-  const float med = e.ctl[c].csf_med;
-  const float scale = med > 1e-30f ? med : 1e-30f;
-  if (detabs > 1e-4f * scale) {
+__device__ __forceinline__ void csf_matrix(const Dev& e, int c, const double4& A, double detabs, double& p,
+                                           double& q, double& r) {
+  const double scale = fmax(e.ctl[c].csf_med, 1e-30);
+  if (detabs > 1e-4 * scale) {
     p = A.y;
     q = A.z;
     r = A.w;
@@ -827,109 +834,73 @@ __device__ __forceinline__ void csf_matrix(const Dev& e, int c, const float4& A,
 }
 
 __global__ void __launch_bounds__(kMaxBlock) k_csf_grad(const __grid_constant__ Dev e) {
-  __shared__ float4 tab[27];
-  __shared__ float red[kMaxBlock / 32];
-  fill_units(tab);
+  __shared__ double red[kMaxBlock / 32];
   const int a0 = blockIdx.x * blockDim.x;
   if (a0 >= e.nf) return;
-  const int NF = e.NF;
   const int a = a0 + threadIdx.x;
   const int cb = e.cid[a0];
   const bool uniform = cb == e.cid[min(a0 + static_cast<int>(blockDim.x), e.nf) - 1];
   int c = -1;
-  float mag = 0.f;
+  double mag = 0.0;
   if (a < e.nf) {
     c = e.cid[a];
     const CaseDev& C = e.cases[c];
     if (C.csf) {
-      const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, vs = C.vol_scale;
-      const float4 la = e.lp[a];
-      const float4 A = e.csA[a];
-      CSum<float> gx, gy;
-      walk_row(e, a, [&](const uint32_t* ent) {
-        float px = 0.f, py = 0.f;
-#pragma unroll
-        for (int j = 0; j < kBatch; ++j) {
-          const int b0 = ent[j] != kPad ? static_cast<int>(ent[j] >> 5) : a;
-          const bool ok = ent[j] != kPad && b0 < NF;
-          const int b = ok ? b0 : a;
-          const float4 lb = e.lp[b];
-          const float cbv = e.csA[b].x;
-          const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u], cellf);
-          const Radial R = radial(d.x * d.x + d.y * d.y, inv_h);
-          const float gs = sigma * dshape(R.q) * inv_h * R.inv_r;
-          const float w = ok ? (lb.w * vs) * (cbv - A.x) * gs : 0.f;
-          px += w * d.x;
-          py += w * d.y;
-        }
-        gx.add(px);
-        gy.add(py);
+      const double4 pa = ld4(e.pos, a);
+      const double4 A = e.csA[a];
+      double gx = 0.0, gy = 0.0;
+      fluid_row(e, a, [&](int b) {
+        const double4 pb = ld4(e.pos, b);
+        const double dx = pa.x - pb.x, dy = pa.y - pb.y;
+        const KD k = kernel_d(dx, dy, C);
+        const double w = pb.w * C.vol_scale * (e.csA[b].x - A.x) * k.gs;
+        gx += w * dx;
+        gy += w * dy;
       });
       double p, q, r;
-      csf_matrix(e, c, A, e.csB[a].w, p, q, r);
+      const double4 B = e.csB[a];
+      csf_matrix(e, c, A, B.w, p, q, r);
       const double det = p * r - q * q;
-      const double rx = gx.value(), ry = gy.value();
-      const float g0 = static_cast<float>((r * rx - q * ry) / det);
-      const float g1 = static_cast<float>((p * ry - q * rx) / det);
-      mag = sqrtf(g0 * g0 + g1 * g1);
-      const float4 B = e.csB[a];
-      e.csB[a] = make_float4(g0, g1, mag, B.w);
-      e.csN0[a] = mag > 1e-12f ? make_float2(-g0 / mag, -g1 / mag) : make_float2(0.f, 0.f);
+      const double g0 = (r * gx - q * gy) / det, g1 = (p * gy - q * gx) / det;
+      mag = sqrt(g0 * g0 + g1 * g1);
+      e.csB[a] = make_double4(g0, g1, mag, B.w);
+      e.csN0[a] = mag > 1e-12 ? make_double2(-g0 / mag, -g1 / mag) : make_double2(0.0, 0.0);
     } else {
       c = -1;
     }
   }
   // every thread of the block reaches this barrier (the early return above is per block)
   const bool all = __syncthreads_and(c >= 0 || a >= e.nf);
-  case_max_float(e, c, cb, uniform && all, mag, &CaseCtl::csf_gmax, red);
+  case_max_double(e, c, cb, uniform && all, mag, &CaseCtl::csf_gmax, red);
 }
 
 // Q4 / Q5: one Shepard pass of the normal field; the second pass also
 // renormalises on the interface (|grad c| > 1e-12, csf_consistent.py:320-330).
 template <bool kFinal>
 __global__ void __launch_bounds__(kMaxBlock) k_csf_smooth(const __grid_constant__ Dev e) {
-  __shared__ float4 tab[27];
-  fill_units(tab);
-  const int NF = e.NF;
-  const float2* __restrict__ src = kFinal ? e.csN1 : e.csN0;
+  const double2* __restrict__ src = kFinal ? e.csN1 : e.csN0;
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
     const CaseDev& C = e.cases[e.cid[a]];
     if (!C.csf) continue;
-    const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, vs = C.vol_scale;
-    const float4 la = e.lp[a];
-    CSum<float> nx, ny, den;
-    den.add((la.w * vs) * sigma);
-    walk_row(e, a, [&](const uint32_t* ent) {
-      float px = 0.f, py = 0.f, pd = 0.f;
-#pragma unroll
-      for (int j = 0; j < kBatch; ++j) {
-        const int b0 = ent[j] != kPad ? static_cast<int>(ent[j] >> 5) : a;
-        const bool ok = ent[j] != kPad && b0 < NF;
-        const int b = ok ? b0 : a;
-        const float4 lb = e.lp[b];
-        const float2 nb = src[b];
-        const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u], cellf);
-        const float w = ok ? (lb.w * vs) * (sigma * shape(radial(d.x * d.x + d.y * d.y, inv_h).q)) : 0.f;
-        px += w * nb.x;
-        py += w * nb.y;
-        pd += w;
-      }
-      nx.add(px);
-      ny.add(py);
-      den.add(pd);
+    const double4 pa = ld4(e.pos, a);
+    double nx = 0.0, ny = 0.0, den = pa.w * C.vol_scale * C.sigma2d_d;
+    fluid_row(e, a, [&](int b) {
+      const double4 pb = ld4(e.pos, b);
+      const double w = pb.w * C.vol_scale * kernel_d(pa.x - pb.x, pa.y - pb.y, C).w;
+      const double2 nb = src[b];
+      nx += w * nb.x;
+      ny += w * nb.y;
+      den += w;
     });
-    float dd = den.value();
-    dd = dd > 1e-30f ? dd : 1e-30f;
-    const float sx = nx.value() / dd, sy = ny.value() / dd;
+    den = fmax(den, 1e-30);
+    const double sx = nx / den, sy = ny / den;
     if (!kFinal) {
-      e.csN1[a] = make_float2(sx, sy);
+      e.csN1[a] = make_double2(sx, sy);
     } else {
-      const float mag = e.csB[a].z;
-      float2 out = e.csN0[a];
-      if (mag > 1e-12f) {
-        float nrm = sqrtf(sx * sx + sy * sy);
-        nrm = nrm > 1e-12f ? nrm : 1e-12f;
-        out = make_float2(sx / nrm, sy / nrm);
+      double2 out = e.csN0[a];
+      if (e.csB[a].z > 1e-12) {
+        const double nrm = fmax(sqrt(sx * sx + sy * sy), 1e-12);
+        out = make_double2(sx / nrm, sy / nrm);
       }
       e.csN[a] = out;
     }
@@ -938,48 +909,31 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_smooth(const __grid_constant_
 
 // Q6: kappa_mls = trace(S M'^-1), S = sum V_b (n_b - n_a) (x) grad_a W
 __global__ void __launch_bounds__(kMaxBlock) k_csf_div(const __grid_constant__ Dev e) {
-  __shared__ float4 tab[27];
-  fill_units(tab);
-  const int NF = e.NF;
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
     const int c = e.cid[a];
     const CaseDev& C = e.cases[c];
     if (!C.csf) continue;
-    const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, vs = C.vol_scale;
-    const float4 la = e.lp[a];
-    const float2 na = e.csN[a];
-    CSum<float> s00, s01, s10, s11;
-    walk_row(e, a, [&](const uint32_t* ent) {
-      float q00 = 0.f, q01 = 0.f, q10 = 0.f, q11 = 0.f;
-#pragma unroll
-      for (int j = 0; j < kBatch; ++j) {
-        const int b0 = ent[j] != kPad ? static_cast<int>(ent[j] >> 5) : a;
-        const bool ok = ent[j] != kPad && b0 < NF;
-        const int b = ok ? b0 : a;
-        const float4 lb = e.lp[b];
-        const float2 nb = e.csN[b];
-        const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u], cellf);
-        const Radial R = radial(d.x * d.x + d.y * d.y, inv_h);
-        const float gs = ok ? (lb.w * vs) * (sigma * dshape(R.q) * inv_h * R.inv_r) : 0.f;
-        const float g0 = gs * d.x, g1 = gs * d.y;
-        const float dn0 = nb.x - na.x, dn1 = nb.y - na.y;
-        q00 += dn0 * g0;
-        q01 += dn0 * g1;
-        q10 += dn1 * g0;
-        q11 += dn1 * g1;
-      }
-      s00.add(q00);
-      s01.add(q01);
-      s10.add(q10);
-      s11.add(q11);
+    const double4 pa = ld4(e.pos, a);
+    const double2 na = e.csN[a];
+    double s00 = 0.0, s01 = 0.0, s10 = 0.0, s11 = 0.0;
+    fluid_row(e, a, [&](int b) {
+      const double4 pb = ld4(e.pos, b);
+      const double dx = pa.x - pb.x, dy = pa.y - pb.y;
+      const double gs = pb.w * C.vol_scale * kernel_d(dx, dy, C).gs;
+      const double g0 = gs * dx, g1 = gs * dy;
+      const double2 nb = e.csN[b];
+      const double dn0 = nb.x - na.x, dn1 = nb.y - na.y;
+      s00 += dn0 * g0;
+      s01 += dn0 * g1;
+      s10 += dn1 * g0;
+      s11 += dn1 * g1;
     });
     double p, q, r;
     csf_matrix(e, c, e.csA[a], e.csB[a].w, p, q, r);
     const double det = p * r - q * q;
     // M'^-1 = [r -q; -q p] / det; trace(S M'^-1)
-    const double k = (s00.value() * r - s01.value() * q - s10.value() * q + s11.value() * p) / det;
-    float4 K = e.csK[a];
-    K.x = static_cast<float>(k);
+    double4 K = e.csK[a];
+    K.x = (s00 * r - s01 * q - s10 * q + s11 * p) / det;
     e.csK[a] = K;
   }
 }
@@ -988,6 +942,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_div(const __grid_constant__ D
 // fluid particles within 4h (cells within stencil_cells of the home cell),
 // weights w_b = |grad c|_b / max |grad c| (= delta_s / max delta_s).
 __global__ void __launch_bounds__(kMaxBlock) k_csf_fit(const __grid_constant__ Dev e) {
+  __shared__ double red[kMaxBlock / 32];
   const int a0 = blockIdx.x * blockDim.x;
   if (a0 >= e.nf) return;
   const int a = a0 + threadIdx.x;
@@ -999,16 +954,14 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_fit(const __grid_constant__ D
     c = e.cid[a];
     const CaseDev& C = e.cases[c];
     if (C.csf) {
-      const float gmax = __uint_as_float(e.ctl[c].csf_gmax);
-      const float inv_g = 1.f / (gmax > 1e-30f ? gmax : 1e-30f);
-      const float4 la = e.lp[a];
-      const float2 na = e.csN[a];
-      const float tx = -na.y, ty = na.x;
-      const float cellf = C.cellf, st2 = C.stencil2;
+      const double gmax = fmax(__longlong_as_double(static_cast<long long>(e.ctl[c].csf_gmax)), 1e-30);
+      const double4 pa = ld4(e.pos, a);
+      const double2 na = e.csN[a];
+      const double tx = -na.y, ty = na.x;
       const int key = e.home[a] - C.key_off;
       const int cy = (key / C.ncz) % C.ncy, cx = key / (C.ncz * C.ncy);
       const int sc = C.stencil_cells;
-      double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      double s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0, s6 = 0, s7 = 0;
       for (int dx = -sc; dx <= sc; ++dx) {
         const int x = cx + dx;
         if (x < 0 || x >= C.ncx) continue;
@@ -1019,62 +972,51 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_fit(const __grid_constant__ D
           const int fs = e.fstart[cell];
           if (fs < 0) continue;
           const int fe = e.fend[cell];
-          const float ox = static_cast<float>(dx), oy = static_cast<float>(dy);
           for (int b = fs; b < fe; ++b) {
             if (b == a) continue;
-            const float4 lb = e.lp[b];
-            const float ddx = fmaf(-ox, cellf, la.x - lb.x), ddy = fmaf(-oy, cellf, la.y - lb.y);
-            if (ddx * ddx + ddy * ddy > st2) continue;
-            float w = e.csB[b].z * inv_g;
-            w = w < 0.f ? 0.f : (w > 1.f ? 1.f : w);
-            const double u = static_cast<double>(-(ddx * tx + ddy * ty));
-            const double v = static_cast<double>(-(ddx * na.x + ddy * na.y));
+            const double4 pb = ld4(e.pos, b);
+            const double ddx = pa.x - pb.x, ddy = pa.y - pb.y;
+            if (ddx * ddx + ddy * ddy > C.stencil2) continue;
+            double w = e.csB[b].z / gmax;
+            w = w < 0.0 ? 0.0 : (w > 1.0 ? 1.0 : w);
+            const double u = -(ddx * tx + ddy * ty), v = -(ddx * na.x + ddy * na.y);
             const double uu = u * u;
-            s[0] += w;
-            s[1] += w * u;
-            s[2] += w * v;
-            s[3] += w * uu;
-            s[4] += w * u * v;
-            s[5] += w * uu * u;
-            s[6] += w * uu * v;
-            s[7] += w * uu * uu;
+            s0 += w;
+            s1 += w * u;
+            s2 += w * v;
+            s3 += w * uu;
+            s4 += w * (u * v);
+            s5 += w * (uu * u);
+            s6 += w * (uu * v);
+            s7 += w * (uu * uu);
           }
         }
       }
-      float wa = e.csB[a].z * inv_g;
-      wa = wa < 0.f ? 0.f : (wa > 1.f ? 1.f : wa);
-      s[0] += wa;
-      // [s0 s1 s3; s1 s3 s5; s3 s5 s7] (c, b, a) = (s2, s4, s6)
-      const double m00 = s[0], m01 = s[1], m02 = s[3], m11 = s[3], m12 = s[5], m22 = s[7];
-      const double c0 = m11 * m22 - m12 * m12, c1 = m01 * m22 - m12 * m02, c2 = m01 * m12 - m11 * m02;
-      const double det = m00 * c0 - m01 * c1 + m02 * c2;
-      const double r0 = s[2], r1 = s[4], r2 = s[6];
-      // Cramer's rule for the second and third unknowns
-      const double detb = m00 * (r1 * m22 - m12 * r2) - r0 * (m01 * m22 - m12 * m02) + m02 * (m01 * r2 - r1 * m02);
-      const double deta = m00 * (m11 * r2 - r1 * m12) - m01 * (m01 * r2 - r1 * m02) + r0 * (m01 * m12 - m11 * m02);
+      double wa = e.csB[a].z / gmax;
+      wa = wa < 0.0 ? 0.0 : (wa > 1.0 ? 1.0 : wa);
+      s0 += wa;
+      // [s0 s1 s3; s1 s3 s5; s3 s5 s7] (c, b, a) = (s2, s4, s6); Cramer's rule
+      const double c0 = s3 * s7 - s5 * s5, c1 = s1 * s7 - s5 * s3, c2 = s1 * s5 - s3 * s3;
+      const double det = s0 * c0 - s1 * c1 + s3 * c2;
+      const double detb = s0 * (s4 * s7 - s5 * s6) - s2 * c1 + s3 * (s1 * s6 - s4 * s3);
+      const double deta = s0 * (s3 * s6 - s4 * s5) - s1 * (s1 * s6 - s4 * s3) + s2 * c2;
       detabs = fabs(det);
-      float kfit = 0.f;
+      double kfit = 0.0;
       if (det != 0.0) {
         const double bb = detb / det, aa = deta / det;
-        kfit = static_cast<float>(-2.0 * aa / pow(1.0 + bb * bb, 1.5));
+        kfit = -2.0 * aa / pow(1.0 + bb * bb, 1.5);
       }
-      float4 K = e.csK[a];
+      double4 K = e.csK[a];
       K.y = kfit;
       K.z = wa;
-      K.w = static_cast<float>(detabs);
+      K.w = detabs;
       e.csK[a] = K;
     } else {
       c = -1;
     }
   }
-  __shared__ double red[kMaxBlock / 32];
   const bool all = __syncthreads_and(c >= 0 || a >= e.nf);
-  if (uniform && all) {
-    const double m = block_reduce<true>(detabs, red);
-    if (threadIdx.x == 0) atomic_max_nonneg(&e.ctl[cb].csf_fmax, m);
-  } else if (c >= 0) {
-    atomic_max_nonneg(&e.ctl[c].csf_fmax, detabs);
-  }
+  case_max_double(e, c, cb, uniform && all, detabs, &CaseCtl::csf_fmax, red);
 }
 
 // Q8: kappa (fit where active and regular, else kappa_mls), delta_s = 2|grad c|
@@ -1085,16 +1027,16 @@ __global__ void k_csf_final(const __grid_constant__ Dev e) {
     const CaseDev& C = e.cases[c];
     if (!C.csf) continue;
     const CaseCtl& t = e.ctl[c];
-    const float4 K = e.csK[a];
-    const double det_max = ::fmax(__longlong_as_double(static_cast<long long>(t.csf_fmax)), 1e-30);
-    const bool ok = K.z > 0.05f && static_cast<double>(K.w) > 1e-6 * det_max;
-    const float kappa = ok ? K.y : K.x;
-    const float mag = e.csB[a].z;
-    const float gmax = __uint_as_float(t.csf_gmax);
-    const float ds = mag <= 1e-3f * gmax ? 0.f : 2.f * mag;
-    const float2 n = e.csN[a];
-    const float f = -C.sigma_st * kappa * ds / e.rho[a];
-    e.st[a] = make_float2(f * n.x, f * n.y);
+    const double4 K = e.csK[a];
+    const double det_max = fmax(__longlong_as_double(static_cast<long long>(t.csf_fmax)), 1e-30);
+    const bool ok = K.z > 0.05 && K.w > 1e-6 * det_max;
+    const double kappa = ok ? K.y : K.x;
+    const double mag = e.csB[a].z;
+    const double gmax = __longlong_as_double(static_cast<long long>(t.csf_gmax));
+    const double ds = mag <= 1e-3 * gmax ? 0.0 : 2.0 * mag;
+    const double2 n = e.csN[a];
+    const double f = -C.sigma_st * kappa * ds / static_cast<double>(e.rho[a]);
+    e.st[a] = make_float2(static_cast<float>(f * n.x), static_cast<float>(f * n.y));
   }
 }
 
@@ -1554,12 +1496,12 @@ size_t carve(const tsph_engine_params& p, Dev* d, char* base, CaseDev** cases, c
   t.acc = static_cast<float4*>(take(NF * sizeof(float4)));
   t.conc = static_cast<float*>(take(NF * sizeof(float)));
   t.gradc = static_cast<float4*>(take(NF * sizeof(float4)));
-  t.csA = static_cast<float4*>(take(NF * sizeof(float4)));
-  t.csB = static_cast<float4*>(take(NF * sizeof(float4)));
-  t.csN0 = static_cast<float2*>(take(NF * sizeof(float2)));
-  t.csN1 = static_cast<float2*>(take(NF * sizeof(float2)));
-  t.csN = static_cast<float2*>(take(NF * sizeof(float2)));
-  t.csK = static_cast<float4*>(take(NF * sizeof(float4)));
+  t.csA = static_cast<double4*>(take(NF * sizeof(double4)));
+  t.csB = static_cast<double4*>(take(NF * sizeof(double4)));
+  t.csN0 = static_cast<double2*>(take(NF * sizeof(double2)));
+  t.csN1 = static_cast<double2*>(take(NF * sizeof(double2)));
+  t.csN = static_cast<double2*>(take(NF * sizeof(double2)));
+  t.csK = static_cast<double4*>(take(NF * sizeof(double4)));
   t.st = static_cast<float2*>(take(NF * sizeof(float2)));
   t.csf_hist = static_cast<unsigned int*>(take(static_cast<size_t>(p.max_cases) * 256 * sizeof(unsigned int)));
   t.nbr = static_cast<uint32_t*>(take(static_cast<size_t>(p.max_neighbors) * N * sizeof(uint32_t)));
@@ -1674,7 +1616,7 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr) {
     const unsigned gf = static_cast<unsigned>((d.nf + B - 1) / B);
     k_csf_clear<<<gc, 128, 0, s>>>(d);
     k_csf_colour<<<g, B, 0, s>>>(d);
-    for (int shift = 24; shift >= 0; shift -= 8) {
+    for (int shift = 56; shift >= 0; shift -= 8) {
       k_csf_hist<<<gf, B, 0, s>>>(d, shift);
       k_csf_pick<<<gc, 128, 0, s>>>(d, shift);
     }
@@ -1768,11 +1710,12 @@ CaseDev make_case_dev(const tsph_case_params& p, int64_t* ncells) {
   c.rho_floor = static_cast<float>(0.1 * p.rho0);
   c.wall_mass = static_cast<float>(p.wall_mass);
   c.csf = (p.surface_tension > 0.0 && p.dim == 2) ? 1 : 0;
-  c.sigma_st = static_cast<float>(p.surface_tension);
-  c.h = static_cast<float>(p.h);
-  c.vol_scale = static_cast<float>(1.0 / p.rho0);
+  c.sigma_st = p.surface_tension;
+  c.h_d = p.h;
+  c.sigma2d_d = 10.0 / (7.0 * M_PI * p.h * p.h);
+  c.vol_scale = 1.0 / p.rho0;
   c.stencil_cells = static_cast<int>(std::ceil((4.0 * p.h + p.skin) / cell));
-  c.stencil2 = static_cast<float>(16.0 * p.h * p.h);
+  c.stencil2 = 16.0 * p.h * p.h;
   return c;
 }
 
