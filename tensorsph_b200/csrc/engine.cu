@@ -1628,7 +1628,7 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr) {
     k_csf_final<<<g, B, 0, s>>>(d);
     TSPH_LAUNCH_CHECK();
   }
-  mark();
+  mark();  // walls + surface tension
   (one ? k_force<true> : k_force<false>)<<<g, B, 0, s>>>(d);
   mark();
   if (d.n_ob) k_reaction<<<static_cast<unsigned>((d.n_ob + B - 1) / B), B, 0, s>>>(d);

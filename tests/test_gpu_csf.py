@@ -1,13 +1,13 @@
 """CSF surface tension in the device engine against the FP64 oracle
 (oracle/csf.py, pinned to the reference's own outputs).
 
-The engine evaluates the colour, MLS matrix, gradient, Shepard-smoothed
-normal and divergence with compensated FP32 pair sums on exact local
-separations, and the 2x2 / 3x3 solves and the quadratic-fit moments in FP64.
-The surface-tension acceleration is isolated as the difference of one step
-with and without sigma (both FP32 engines) and compared with the oracle's
-a = -sigma kappa delta_s n / rho: within 1e-3 of max |a| (the reference's own
-FP32 run is 0.4-1 % away from its FP64 run on these drops).
+The engine runs the CSF passes in FP64 on the FP64 positions (the operator
+differentiates the colour twice and divides by |grad c|: the reference's own
+FP32 run is 0.4-1 % away from its FP64 run on these drops).  The
+surface-tension acceleration is isolated as the difference of one step with
+and without sigma and compared with the oracle's a = -sigma kappa delta_s n /
+rho: within 1e-5 of max |a| (the density it divides by comes from the FP32
+pair pass).
 """
 import numpy as np
 import pytest
@@ -51,7 +51,7 @@ def test_engine_csf_matches_oracle(gpu):
     scale = np.abs(a_ref).max()
     err = np.abs(a_dev - a_ref).max(axis=1) / scale
     assert scale > 0.1
-    assert err.max() < 1e-3, (err.max(), int(err.argmax()), int((err > 1e-4).sum()))
+    assert err.max() < 1e-5, (err.max(), int(err.argmax()), int((err > 1e-6).sum()))
 
 
 def test_csf_batch_equals_alone(gpu):
