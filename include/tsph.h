@@ -261,6 +261,41 @@ int tsph_kick_drift(void* pos, void* vel, const void* acc, int64_t n, int64_t di
                     double dt, int64_t drift, const double* box, tsph_stream stream);
 
 /* ------------------------------------------------------------------------ */
+/* 2-D delta-plus step: delta_plus.py:105-229 (delta_plus_step), h = 2 dx,    */
+/* Wendland C2, linear EOS, ghost walls with unit normals, psi diffusion,     */
+/* interface band, regularised shift and wall tangent.  Synchronises once to  */
+/* report TSPH_ERR_STATE (status bit 0: nonpositive wall density, bit 1:       */
+/* nonpositive or non-finite density).                                        */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  int64_t dtype, n_fluid, n_wall;
+  double dx, sound_speed, reference_speed, dt, rho0, gravity, viscosity, diffusion, alpha;
+} tsph_delta_plus_params;
+
+typedef struct {
+  const void* pos;            /* (n, 2)                                   */
+  const void* vel;            /* (n, 2)                                   */
+  const void* density;        /* (n)                                      */
+  const void* mass;           /* (n)                                      */
+  const void* wall;           /* (nw, 2) or NULL                          */
+  const void* wall_vel;       /* (nw, 2) or NULL                          */
+  const void* wall_normal;    /* (nw, 2) or NULL, any nonzero length      */
+  const int64_t* rowptr;      /* symmetric rows over n + nw particles     */
+  const uint32_t* entries;
+  void* out_pos;              /* (n, 2)                                   */
+  void* out_vel;              /* (n, 2)                                   */
+  void* out_density;          /* (n)                                      */
+  void* acc;                  /* (n, 2)                                   */
+  void* reaction;             /* (nw, 2) integrated wall forces           */
+  void* shift;                /* (n, 2)                                   */
+  int* status_out;            /* host, nullable                           */
+} tsph_delta_plus_io;
+
+int64_t tsph_delta_plus_workspace_bytes(const tsph_delta_plus_params* prm);
+int tsph_delta_plus_step(const tsph_delta_plus_params* prm, const tsph_delta_plus_io* io, void* ws,
+                         int64_t ws_bytes, tsph_stream stream);
+
+/* ------------------------------------------------------------------------ */
 /* Conservation meters: threed/conservation.py:41-121 (diagnostics) as one   */
 /* FP64 device reduction, deterministic (fixed-order block partials).        */
 /* ------------------------------------------------------------------------ */

@@ -79,6 +79,18 @@ class ClampParams(ctypes.Structure):
                 ("ob_eps", c_double)]
 
 
+class DeltaPlusParams(ctypes.Structure):
+    _fields_ = [(k, c_int64) for k in ("dtype", "n_fluid", "n_wall")] + \
+               [(k, c_double) for k in ("dx", "sound_speed", "reference_speed", "dt", "rho0",
+                                        "gravity", "viscosity", "diffusion", "alpha")]
+
+
+class DeltaPlusIO(ctypes.Structure):
+    _fields_ = [(k, c_void_p) for k in ("pos", "vel", "density", "mass", "wall", "wall_vel",
+                                        "wall_normal", "rowptr", "entries", "out_pos", "out_vel",
+                                        "out_density", "acc", "reaction", "shift", "status_out")]
+
+
 class MeterParams(ctypes.Structure):
     _fields_ = [(k, c_int64) for k in ("dim", "dtype", "n", "periodic")] + \
                [(k, c_double) for k in ("rho0", "sound_speed", "gamma")] + \
@@ -144,6 +156,9 @@ _SIGNATURES = {
                               c_void_p]),
     "tsph_euler_clamp": (c_int, [POINTER(ClampParams), c_void_p, c_void_p, c_void_p, c_double,
                                  c_void_p, c_void_p]),
+    "tsph_delta_plus_workspace_bytes": (c_int64, [POINTER(DeltaPlusParams)]),
+    "tsph_delta_plus_step": (c_int, [POINTER(DeltaPlusParams), POINTER(DeltaPlusIO), c_void_p,
+                                     c_int64, c_void_p]),
     "tsph_meters_workspace_bytes": (c_int64, []),
     "tsph_meters": (c_int, [POINTER(MeterParams), POINTER(MeterIO), c_void_p, c_int64, c_void_p]),
     "tsph_mode_amplitude": (c_int, [c_void_p, c_void_p, c_int64, c_int64, c_double, c_int64,

@@ -1,0 +1,122 @@
+"""2-D delta-plus SPH step on the GPU (``tensorsph.delta_plus``).
+
+``delta_plus_step`` keeps the reference signature, checks, exceptions and
+``DeltaPlusStep`` result (delta_plus.py:19-229): Wendland C2 at h = 2 dx,
+linear EOS, fixed-ghost wall pressure with gravity, pressure + Monaghan radial
+viscosity + slip-wall forces, continuity with the wall flux, psi-form density
+diffusion through the eigen-floored first-moment inverse, the Marrone
+empty-cap interface band and the regularised, wall-tangent positional shift
+-- all in ``csrc/delta_plus.cu`` over one symmetric gather list.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+import math
+
+import torch
+
+from . import _lib
+from .droplet_impact import symmetric_rows
+from .neighbor_search import grid_pairs
+
+__all__ = ["DeltaPlusStep", "delta_plus_step"]
+
+
+@dataclass
+class DeltaPlusStep:
+    position: torch.Tensor
+    velocity: torch.Tensor
+    density: torch.Tensor
+    acceleration: torch.Tensor
+    wall_reaction: torch.Tensor
+    shift: torch.Tensor
+
+
+def delta_plus_step(pos, velocity, density, mass, *, dx, sound_speed, reference_speed,
+                    dt, rho0=1000., gravity=9.81, viscosity=1.e-6, diffusion=.1, alpha=.02,
+                    wall=None, wall_velocity=None, wall_normal=None, pairs=None):
+    """Advance an equal-spacing 2-D liquid by one delta-plus step (h = 2 dx)."""
+    if (pos.ndim != 2 or pos.shape[1] != 2 or velocity.shape != pos.shape
+            or density.shape != pos.shape[:1] or mass.shape != density.shape
+            or not len(pos) or pos.dtype not in (torch.float32, torch.float64)):
+        raise ValueError("expected a nonempty 2-D fluid and one density and mass per particle")
+    if not all(math.isfinite(x) for x in (dx, sound_speed, reference_speed, dt,
+                                          rho0, gravity, viscosity, diffusion, alpha)):
+        raise ValueError("solver parameters must be finite")
+    if min(dx, sound_speed, dt, rho0) <= 0 or min(reference_speed, viscosity, diffusion, alpha) < 0:
+        raise ValueError("invalid length, speed, density, step or transport coefficient")
+    h = 2 * dx
+    radial_viscosity = 8 * viscosity + alpha * h * sound_speed
+    if (dt * sound_speed > .3 * h or dt * radial_viscosity / 8 > .125 * h * h
+            or dt * diffusion * sound_speed > .125 * h):
+        raise ValueError("time step exceeds an acoustic, viscous or diffusive limit")
+    if wall is None:
+        wall = pos.new_empty((0, 2))
+    if wall_velocity is None:
+        wall_velocity = torch.zeros_like(wall)
+    if wall.ndim != 2 or wall.shape[1] != 2 or wall_velocity.shape != wall.shape:
+        raise ValueError("expected matching (W, 2) wall positions and velocities")
+    if wall_normal is None and len(wall) == 0:
+        wall_normal = wall
+    if wall_normal is None or wall_normal.shape != wall.shape:
+        raise ValueError("provide a wall_normal per ghost station for free slip")
+    if any(x.dtype != pos.dtype or x.device != pos.device
+           for x in (velocity, density, mass, wall, wall_velocity, wall_normal)):
+        raise ValueError("states must share a floating dtype and device")
+    if not bool(((density > 0) & (mass > 0) & density.isfinite() & mass.isfinite()).all()):
+        raise ValueError("density and mass must be positive and finite")
+    norms = wall_normal.norm(dim=1)
+    if not bool((norms.isfinite() & (norms > 0)).all()):
+        raise ValueError("wall normals must be finite and nonzero")
+    if not all(bool(x.isfinite().all()) for x in (pos, velocity, wall, wall_velocity)):
+        raise ValueError("particle positions and velocities must be finite")
+    n, nw = pos.shape[0], wall.shape[0]
+    out_device = pos.device
+    dev = _lib.cuda_device(pos)
+    dtype = pos.dtype
+    P, V, R, M = (_lib.to_dev(t.detach(), dev, dtype).contiguous() for t in (pos, velocity, density, mass))
+    W, WV, WN = (_lib.to_dev(t.detach(), dev, dtype).contiguous() for t in (wall, wall_velocity, wall_normal))
+    cloud = torch.cat((P, W)) if nw else P
+    if pairs is None:
+        pairs_dev, _, _ = grid_pairs(cloud, 2 * h) if n + nw >= 2 else (
+            torch.zeros((0, 2), dtype=torch.long, device=dev), 0, None)
+    else:
+        if pairs.ndim != 2 or pairs.shape[1] != 2 or pairs.dtype != torch.long:
+            raise ValueError("expected a (P, 2) long pair list")
+        if pairs.device != pos.device:
+            raise ValueError("pair list must share the device of the state")
+        i, j = pairs.unbind(1)
+        if bool(((i < 0) | (i >= j) | (j >= n + nw)).any()):
+            raise ValueError("each pair must have 0 <= i < j < number of particles")
+        pairs_dev = _lib.to_dev(pairs, dev)
+    rowptr, entries = symmetric_rows(pairs_dev, n + nw)
+    prm = _lib.DeltaPlusParams()
+    prm.dtype, prm.n_fluid, prm.n_wall = _lib.dtype_code(dtype), n, nw
+    prm.dx, prm.sound_speed, prm.reference_speed, prm.dt = float(dx), float(sound_speed), \
+        float(reference_speed), float(dt)
+    prm.rho0, prm.gravity, prm.viscosity = float(rho0), float(gravity), float(viscosity)
+    prm.diffusion, prm.alpha = float(diffusion), float(alpha)
+    out_pos = torch.empty_like(P)
+    out_vel = torch.empty_like(P)
+    out_rho = torch.empty_like(R)
+    acc = torch.empty_like(P)
+    reaction = torch.zeros_like(W)
+    shift = torch.empty_like(P)
+    status = ctypes.c_int(0)
+    ptr = lambda t: t.data_ptr() if t.numel() else None  # noqa: E731
+    io = _lib.DeltaPlusIO(P.data_ptr(), V.data_ptr(), R.data_ptr(), M.data_ptr(), ptr(W), ptr(WV),
+                          ptr(WN), rowptr.data_ptr(), entries.data_ptr(), out_pos.data_ptr(),
+                          out_vel.data_ptr(), out_rho.data_ptr(), acc.data_ptr(), ptr(reaction),
+                          shift.data_ptr(), ctypes.cast(ctypes.pointer(status), ctypes.c_void_p))
+    L = _lib.lib()
+    ws = _lib.workspace(L.tsph_delta_plus_workspace_bytes(ctypes.byref(prm)), dev)
+    rc = L.tsph_delta_plus_step(ctypes.byref(prm), ctypes.byref(io), ws.data_ptr(), ws.numel(),
+                                _lib.stream(dev))
+    if rc == _lib.ERR_STATE:
+        if status.value & 1:
+            raise FloatingPointError("nonpositive extrapolated wall density")
+        raise FloatingPointError("δ⁺-SPH density became nonpositive or nonfinite")
+    _lib.check(rc, "tsph_delta_plus_step")
+    to = lambda t: t.to(out_device)  # noqa: E731
+    return DeltaPlusStep(to(out_pos), to(out_vel), to(out_rho), to(acc), to(reaction), to(shift))

@@ -401,6 +401,55 @@ def csf_cases(ca, di):
     return data
 
 
+def delta_plus_cases(dp):
+    """delta_plus_step on a perturbed lattice block in a walled corner (fluid,
+    slip walls with normals, gravity, diffusion) and on a free block."""
+    data = {}
+    k = 0
+    for dtype in (torch.float64, torch.float32):
+        for kind in ("tank", "free"):
+            g = torch.Generator().manual_seed(90 + k)
+            dx = 0.01
+            ax = (torch.arange(12, dtype=torch.float64) + 0.5) * dx
+            pos = torch.cartesian_prod(ax, ax)
+            pos = pos + 0.08 * dx * torch.randn(pos.shape, generator=g, dtype=torch.float64)
+            vel = 0.05 * torch.randn(pos.shape, generator=g, dtype=torch.float64)
+            rho = 1000.0 + 2.0 * torch.randn((pos.shape[0],), generator=g, dtype=torch.float64)
+            mass = torch.full((pos.shape[0],), 1000.0 * dx * dx, dtype=torch.float64)
+            kw = dict(dx=dx, sound_speed=20.0, reference_speed=0.5, dt=1e-4, gravity=9.81,
+                      viscosity=1e-6, diffusion=0.1, alpha=0.02)
+            wall = wall_v = wall_n = None
+            if kind == "tank":
+                # three rows of stations below the floor y = 0 and left of x = 0
+                layers = []
+                normals = []
+                xs = (torch.arange(-3, 16, dtype=torch.float64) + 0.5) * dx
+                for m in range(1, 4):
+                    ys = torch.full_like(xs, (0.5 - m) * dx)
+                    layers.append(torch.stack((xs, ys), 1))
+                    normals.append(torch.tensor([[0.0, 1.0]]).expand(xs.numel(), 2))
+                    yy = (torch.arange(0, 16, dtype=torch.float64) + 0.5) * dx
+                    layers.append(torch.stack((torch.full_like(yy, (0.5 - m) * dx), yy), 1))
+                    normals.append(torch.tensor([[1.0, 0.0]]).expand(yy.numel(), 2))
+                wall = torch.cat(layers).to(dtype)
+                wall_n = torch.cat(normals).to(dtype).contiguous()
+                wall_v = torch.zeros_like(wall)
+            st = dp.delta_plus_step(pos.to(dtype), vel.to(dtype), rho.to(dtype), mass.to(dtype),
+                                    wall=wall, wall_velocity=wall_v, wall_normal=wall_n, **kw)
+            for name, t in dict(pos=pos.to(dtype), vel=vel.to(dtype), rho=rho.to(dtype),
+                                mass=mass.to(dtype), out_position=st.position,
+                                out_velocity=st.velocity, out_density=st.density,
+                                out_acceleration=st.acceleration, out_wall_reaction=st.wall_reaction,
+                                out_shift=st.shift).items():
+                data[f"c{k}_{name}"] = _np(t)
+            if wall is not None:
+                data[f"c{k}_wall"] = _np(wall)
+                data[f"c{k}_wall_normal"] = _np(wall_n)
+            k += 1
+    data["count"] = np.int64(k)
+    return data
+
+
 def main(src, families=None):
     sys.path.insert(0, str(src))
     import tensorsph.neighbor_search as ns
@@ -413,6 +462,7 @@ def main(src, families=None):
     from tensorsph.threed import conservation as cons
     from tensorsph.threed import solver as sv
     import tensorsph.csf_consistent as ca
+    import tensorsph.delta_plus as dp
 
     meta = {"torch_version": np.array(torch.__version__)}
     torch.set_num_threads(1)
@@ -427,6 +477,7 @@ def main(src, families=None):
         "meters": lambda: meters_cases(cons, di),
         "shear": lambda: shear_cases(sv),
         "csf": lambda: csf_cases(ca, di),
+        "delta_plus": lambda: delta_plus_cases(dp),
     }
     for name in families or makers:
         np.savez_compressed(OUT / f"{name}.npz", **makers[name](), **meta)

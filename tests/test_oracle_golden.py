@@ -200,3 +200,22 @@ def test_csf_oracle_matches_reference(golden):
         for name in ("normal", "kappa"):
             r = g[f"c{k}_{name}"][live]
             assert np.abs(st[name][live] - r).max() <= 1e-8 * np.abs(r).max(), (k, name)
+
+
+def test_delta_plus_oracle_matches_reference(golden):
+    """The oracle's delta-plus step against the reference's own output
+    (tests/golden/delta_plus.npz: a walled corner and a free block)."""
+    from oracle import delta_plus as odp
+    g = golden("delta_plus")
+    kw = dict(dx=0.01, sound_speed=20.0, reference_speed=0.5, dt=1e-4, gravity=9.81, viscosity=1e-6,
+              diffusion=0.1, alpha=0.02)
+    for k in range(int(g["count"])):
+        wall = g[f"c{k}_wall"] if f"c{k}_wall" in g else None
+        wn = g[f"c{k}_wall_normal"] if wall is not None else None
+        out = odp.delta_plus_step(g[f"c{k}_pos"], g[f"c{k}_vel"], g[f"c{k}_rho"], g[f"c{k}_mass"],
+                                  wall=wall, wall_normal=wn, **kw)
+        tol = 1e-12 if g[f"c{k}_pos"].dtype == np.float64 else 5e-6
+        for key in ("position", "velocity", "density", "acceleration", "wall_reaction", "shift"):
+            ref = g[f"c{k}_out_{key}"]
+            if ref.size:
+                assert np.abs(out[key] - ref).max() <= tol * np.abs(ref).max(), (k, key)
