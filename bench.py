@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--dx", type=float, default=0.0069)
     ap.add_argument("--shift-every", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=6)
     ap.add_argument("--ensemble-cases", type=int, default=256)
     ap.add_argument("--ensemble-steps", type=int, default=100)
@@ -169,7 +170,8 @@ def ensemble_leg(args, dev):
     tune = en.autotune(draws[:32], steps=20, warmup=5, device=dev)
     best = tune["best"]
     specs = en.ensemble_specs(draws, skin_factor=best["skin_factor"])
-    batched = en.run_batched(specs, args.ensemble_steps, block=best["block"], device=dev)
+    batched = en.run_batched(specs, args.ensemble_steps, block=best["block"], batch=best["batch"],
+                             device=dev)
     plain = en.run_plain(specs, args.plain_steps, block=128, device=dev)
     return {"workload": f"{len(specs)} independent 2-D droplet impacts (R~U[0.02,0.08] m, dx=R/20, "
                         "depth~U[2R,6R], width 8R, U~U[1,5] m/s, seed 0), CSF sigma=0.0728 N/m",
@@ -280,9 +282,20 @@ def main():
 
     cfg, obstacle = obstacle_case(dx=args.dx)
     host = DamBreak3DEngine.build_host_state(cfg, obstacle)
+    tuning = None
+    if not args.no_tune:
+        # untimed: pick the list skin, block size and batch depth on this case
+        from dataclasses import replace
+        from tensorsph_b200.engine import tune_single_case
+        tuning = tune_single_case(cfg, obstacle=obstacle, shift_every=args.shift_every,
+                                  host_state=host, device=dev)
+        cfg = replace(cfg, pair_skin_factor=tuning["best"]["skin_factor"])
     eng = DamBreak3DEngine(cfg, obstacle=obstacle, shift_every=args.shift_every,
                            host_state=host, diag_ring=max(args.steps + args.warmup + 64, 256),
                            device=dev)
+    if tuning is not None:
+        eng.set_block(tuning["best"]["block"])
+        eng.set_batch(tuning["best"]["batch"])
     nf, nw = eng.n_fluid, eng.n_wall
     eng.step(max(args.warmup, 1))
     torch.cuda.synchronize(dev)
@@ -339,6 +352,9 @@ def main():
         e = DamBreak3DEngine(cfg, obstacle=obstacle, shift_every=args.shift_every,
                              host_state=(pinned[0], pinned[1], pinned[2], n_ob),
                              diag_ring=args.steps + 8, device=dev)
+        if tuning is not None:
+            e.set_block(tuning["best"]["block"])
+            e.set_batch(tuning["best"]["batch"])
         for k in range(args.steps):
             e.step(1)
             with torch.cuda.stream(e.stream):
@@ -391,6 +407,8 @@ def main():
                                    "3.2x1.0x1.0 m tank, obstacle 0.16x0.16x0.4 m, dx="
                                    f"{args.dx:g}", "fluid_particles": nf, "wall_particles": nw,
                        "shift_every": args.shift_every, "density_diffusion": 0.1,
+                       "pair_skin_factor": cfg.pair_skin_factor,
+                       "tuning": None if tuning is None else tuning["best"],
                        "pairs": "FP32 pair arithmetic, FP64 positions/velocities/meters",
                        "l2": "working set (state + neighbour rows) > 126 MB L2, no flush",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},

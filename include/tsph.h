@@ -351,6 +351,7 @@ typedef struct {
   int64_t max_cases;                          /* case slots                         */
   int64_t max_neighbors;                      /* neighbour-row capacity             */
   int64_t diag_ring;                          /* meter rows kept per case           */
+  int64_t max_fit_neighbors;                  /* CSF curvature-fit rows (0: no CSF)  */
 } tsph_engine_params;
 
 typedef struct {
@@ -421,6 +422,9 @@ int tsph_engine_status(tsph_engine* engine, int64_t case_id, int64_t* counters,
 /* Threads per block of the pair kernels: 64, 128 (default) or 256.  A tuning
  * knob (results do not depend on it); the step graph is re-captured. */
 int tsph_engine_set_block(tsph_engine* engine, int64_t threads);
+/* Neighbour records in flight per thread in the pair kernels: 4 (default) or
+ * 8.  A tuning knob (results do not depend on it); the graph is re-captured. */
+int tsph_engine_set_batch(tsph_engine* engine, int64_t depth);
 /* Occupancy (fluid rows, wall rows, obstacle rows, cells, cases) (host). */
 int tsph_engine_usage(const tsph_engine* engine, int64_t* usage);
 int tsph_engine_destroy(tsph_engine* engine);

@@ -103,7 +103,8 @@ class MeterIO(ctypes.Structure):
 
 class EngineParams(ctypes.Structure):
     _fields_ = [(k, c_int64) for k in ("max_fluid", "max_wall", "max_obstacle", "max_cells",
-                                       "max_cases", "max_neighbors", "diag_ring")]
+                                       "max_cases", "max_neighbors", "diag_ring",
+                                       "max_fit_neighbors")]
 
 
 class CaseParams(ctypes.Structure):
@@ -184,6 +185,7 @@ _SIGNATURES = {
     "tsph_engine_status": (c_int, [c_void_p, c_int64, c_void_p, c_void_p]),
     "tsph_engine_usage": (c_int, [c_void_p, c_void_p]),
     "tsph_engine_set_block": (c_int, [c_void_p, c_int64]),
+    "tsph_engine_set_batch": (c_int, [c_void_p, c_int64]),
     "tsph_engine_destroy": (c_int, [c_void_p]),
 }
 

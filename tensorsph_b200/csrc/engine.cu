@@ -65,6 +65,7 @@ struct CaseDev {
   int stencil_cells;       // cells each side covering the 4h fit stencil
   double sigma_st, h_d, sigma2d_d, vol_scale;  // CSF: sigma, h, 10/(7 pi h^2), 1/rho0
   double stencil2;         // (4h)^2
+  double fit_rc2;          // (4h + skin)^2, the fit rows' list cutoff
 };
 
 struct CaseCtl {
@@ -114,7 +115,9 @@ struct Dev {
   double4* csK;      // CSF: kappa_mls, kappa_fit, own fit weight, |det fit|
   float2* st;        // CSF: surface-tension acceleration
   unsigned int* csf_hist;  // [n_slots][256] median-select histograms
-  int has_csf;
+  int has_csf, maxfit;
+  uint32_t* nbr4;    // CSF fit rows (fluid neighbours within 4h + skin), k-major over NF
+  int32_t* cnt4;
   uint32_t* nbr;
   int32_t* cnt;
   int32_t* ob_rows;
@@ -225,23 +228,24 @@ __device__ __forceinline__ float tait(float rho, float rho0, float bulk, float g
   return p > 0.f ? p : 0.f;
 }
 
-// Walk row a in batches of kBatch entries (padded with kPad); the loads of a
-// batch are all issued before any use.
-template <class Body>
+// Walk row a in batches of KB entries (padded with kPad); the loads of a
+// batch are all issued before any use.  KB (the batch depth: neighbour
+// records in flight per thread) is a tuning parameter of the hot kernels.
+template <int KB = kBatch, class Body>
 __device__ __forceinline__ void walk_row(const Dev& e, int64_t a, Body&& body) {
   const int n = e.cnt[a];
   const uint32_t* row = e.nbr + a;
   int k = 0;
-  for (; k + kBatch <= n; k += kBatch) {
-    uint32_t ent[kBatch];
+  for (; k + KB <= n; k += KB) {
+    uint32_t ent[KB];
 #pragma unroll
-    for (int j = 0; j < kBatch; ++j) ent[j] = row[static_cast<int64_t>(k + j) * e.rows];
+    for (int j = 0; j < KB; ++j) ent[j] = row[static_cast<int64_t>(k + j) * e.rows];
     body(ent);
   }
   if (k < n) {
-    uint32_t ent[kBatch];
+    uint32_t ent[KB];
 #pragma unroll
-    for (int j = 0; j < kBatch; ++j) ent[j] = (k + j < n) ? row[static_cast<int64_t>(k + j) * e.rows] : kPad;
+    for (int j = 0; j < KB; ++j) ent[j] = (k + j < n) ? row[static_cast<int64_t>(k + j) * e.rows] : kPad;
     body(ent);
   }
 }
@@ -421,6 +425,37 @@ __global__ void k_rows(Dev e) {
     }
     e.cnt[a] = count < e.maxnb ? count : e.maxnb;
     atomicMax(&ctl.row_max, static_cast<unsigned long long>(count));
+    if (fluid_row && C.csf) {
+      // the CSF fit rows: fluid particles within 4h + skin
+      const int sc = C.stencil_cells;
+      int c4 = 0;
+      for (int dx = -sc; dx <= sc; ++dx) {
+        const int x = cx + dx;
+        if (x < 0 || x >= C.ncx) continue;
+        for (int dy = -sc; dy <= sc; ++dy) {
+          const int y = cy + dy;
+          if (y < 0 || y >= C.ncy) continue;
+          const int cell = C.key_off + (x * C.ncy + y) * C.ncz;
+          const int fs = e.fstart[cell];
+          if (fs < 0) continue;
+          const int fe = e.fend[cell];
+          for (int b = fs; b < fe; ++b) {
+            if (b == a) continue;
+            const double4 pb = ld4(e.pos, b);
+            const double ddx = pa.x - pb.x, ddy = pa.y - pb.y;
+            if (ddx * ddx + ddy * ddy <= C.fit_rc2) {
+              if (c4 < e.maxfit) e.nbr4[static_cast<int64_t>(c4) * e.NF + a] = static_cast<uint32_t>(b) << 5;
+              ++c4;
+            }
+          }
+        }
+      }
+      if (c4 > e.maxfit) {
+        atomicOr(e.status, 1);
+        atomicOr(&ctl.status, 1);
+      }
+      e.cnt4[a] = c4 < e.maxfit ? c4 : e.maxfit;
+    }
   }
 }
 
@@ -444,7 +479,7 @@ __global__ void k_step_begin(Dev e) {
 
 // ------------------------------------------------------------- physics ---
 
-template <bool kOne>
+template <bool kOne, int KB>
 __global__ void __launch_bounds__(kMaxBlock) k_density(const __grid_constant__ Dev e) {
   __shared__ float4 tab[27];
   fill_units(tab);
@@ -454,10 +489,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_density(const __grid_constant__ D
     const float4 la = e.lp[a];
     CSum<float> s;
     s.add(la.w * sigma);
-    walk_row(e, a, [&](const uint32_t* ent) {
+    walk_row<KB>(e, a, [&](const uint32_t* ent) {
       float part = 0.f;
 #pragma unroll
-      for (int j = 0; j < kBatch; ++j) {
+      for (int j = 0; j < KB; ++j) {
         const bool ok = ent[j] != kPad;
         const int b = ok ? static_cast<int>(ent[j] >> 5) : a;
         const float4 lb = e.lp[b];
@@ -474,7 +509,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_density(const __grid_constant__ D
   }
 }
 
-template <bool kOne>
+template <bool kOne, int KB>
 __global__ void __launch_bounds__(kMaxBlock) k_diffusion_eos(const __grid_constant__ Dev e) {
   __shared__ float4 tab[27];
   fill_units(tab);
@@ -488,10 +523,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_diffusion_eos(const __grid_consta
       const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf;
       const int NF = e.NF;
       CSum<float> rate;
-      walk_row(e, a, [&](const uint32_t* ent) {
+      walk_row<KB>(e, a, [&](const uint32_t* ent) {
         float part = 0.f;
 #pragma unroll
-        for (int j = 0; j < kBatch; ++j) {
+        for (int j = 0; j < KB; ++j) {
           const int b0 = ent[j] != kPad ? static_cast<int>(ent[j] >> 5) : a;
           const bool ok = ent[j] != kPad && b0 < NF;
           const int b = ok ? b0 : a;
@@ -518,7 +553,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_diffusion_eos(const __grid_consta
   }
 }
 
-template <bool kOne>
+template <bool kOne, int KB>
 __global__ void __launch_bounds__(kMaxBlock) k_walls(const __grid_constant__ Dev e) {
   __shared__ float4 tab[27];
   fill_units(tab);
@@ -529,10 +564,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_walls(const __grid_constant__ Dev
     const int f0 = C.fluid_begin;
     const float4 la = e.lp[a];
     CSum<float> num, den;
-    walk_row(e, a, [&](const uint32_t* ent) {
+    walk_row<KB>(e, a, [&](const uint32_t* ent) {
       float pn = 0.f, pd = 0.f;
 #pragma unroll
-      for (int j = 0; j < kBatch; ++j) {
+      for (int j = 0; j < KB; ++j) {
         const bool ok = ent[j] != kPad;
         const int f = ok ? static_cast<int>(ent[j] >> 5) : f0;
         const float4 lf = e.lp[f];
@@ -559,7 +594,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_walls(const __grid_constant__ Dev
   }
 }
 
-template <bool kOne>
+template <bool kOne, int KB>
 __global__ void __launch_bounds__(kMaxBlock) k_force(const __grid_constant__ Dev e) {
   __shared__ float4 tab[27];
   fill_units(tab);
@@ -572,10 +607,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(const __grid_constant__ Dev
     const float4 va = e.vb[a];
     const float Pa = e.pq[a];
     CSum<float> ax, ay, az;
-    walk_row(e, a, [&](const uint32_t* ent) {
+    walk_row<KB>(e, a, [&](const uint32_t* ent) {
       float px = 0.f, py = 0.f, pz = 0.f;
 #pragma unroll
-      for (int j = 0; j < kBatch; ++j) {
+      for (int j = 0; j < KB; ++j) {
         const bool ok = ent[j] != kPad;
         const int b = ok ? static_cast<int>(ent[j] >> 5) : a;
         const float4 lb = e.lp[b];
@@ -958,39 +993,25 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_fit(const __grid_constant__ D
       const double4 pa = ld4(e.pos, a);
       const double2 na = e.csN[a];
       const double tx = -na.y, ty = na.x;
-      const int key = e.home[a] - C.key_off;
-      const int cy = (key / C.ncz) % C.ncy, cx = key / (C.ncz * C.ncy);
-      const int sc = C.stencil_cells;
       double s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0, s6 = 0, s7 = 0;
-      for (int dx = -sc; dx <= sc; ++dx) {
-        const int x = cx + dx;
-        if (x < 0 || x >= C.ncx) continue;
-        for (int dy = -sc; dy <= sc; ++dy) {
-          const int y = cy + dy;
-          if (y < 0 || y >= C.ncy) continue;
-          const int cell = C.key_off + (x * C.ncy + y) * C.ncz;
-          const int fs = e.fstart[cell];
-          if (fs < 0) continue;
-          const int fe = e.fend[cell];
-          for (int b = fs; b < fe; ++b) {
-            if (b == a) continue;
-            const double4 pb = ld4(e.pos, b);
-            const double ddx = pa.x - pb.x, ddy = pa.y - pb.y;
-            if (ddx * ddx + ddy * ddy > C.stencil2) continue;
-            double w = e.csB[b].z / gmax;
-            w = w < 0.0 ? 0.0 : (w > 1.0 ? 1.0 : w);
-            const double u = -(ddx * tx + ddy * ty), v = -(ddx * na.x + ddy * na.y);
-            const double uu = u * u;
-            s0 += w;
-            s1 += w * u;
-            s2 += w * v;
-            s3 += w * uu;
-            s4 += w * (u * v);
-            s5 += w * (uu * u);
-            s6 += w * (uu * v);
-            s7 += w * (uu * uu);
-          }
-        }
+      const int n4 = e.cnt4[a];
+      for (int k = 0; k < n4; ++k) {
+        const int b = static_cast<int>(e.nbr4[static_cast<int64_t>(k) * e.NF + a] >> 5);
+        const double4 pb = ld4(e.pos, b);
+        const double ddx = pa.x - pb.x, ddy = pa.y - pb.y;
+        if (ddx * ddx + ddy * ddy > C.stencil2) continue;
+        double w = e.csB[b].z / gmax;
+        w = w < 0.0 ? 0.0 : (w > 1.0 ? 1.0 : w);
+        const double u = -(ddx * tx + ddy * ty), v = -(ddx * na.x + ddy * na.y);
+        const double uu = u * u;
+        s0 += w;
+        s1 += w * u;
+        s2 += w * v;
+        s3 += w * uu;
+        s4 += w * (u * v);
+        s5 += w * (uu * u);
+        s6 += w * (uu * v);
+        s7 += w * (uu * uu);
       }
       double wa = e.csB[a].z / gmax;
       wa = wa < 0.0 ? 0.0 : (wa > 1.0 ? 1.0 : wa);
@@ -1415,6 +1436,13 @@ __global__ void k_remap(Dev e, int fluid_from, int wall_from, int df, int dw, in
       const uint32_t nb = b < static_cast<uint32_t>(e.NF) ? b - df : b - dw;
       ent = (nb << 5) | (ent & 31u);
     }
+    if (a < e.NF && e.cases[e.cid[a]].csf) {
+      const int n4 = e.cnt4[a];
+      for (int k = 0; k < n4; ++k) {
+        uint32_t& ent = e.nbr4[static_cast<int64_t>(k) * e.NF + a];
+        ent = ((ent >> 5) - df) << 5;
+      }
+    }
   }
   for (int q = ob_from + blockIdx.x * blockDim.x + threadIdx.x; q < e.n_ob; q += gridDim.x * blockDim.x)
     e.ob_rows[q] -= dw;
@@ -1461,6 +1489,7 @@ struct tsph_engine {
   std::vector<int> free_slots;
   int64_t total_cells = 0;
   int block = tsph::kBlock;
+  int batch = tsph::kBatch;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaStream_t captured_on = nullptr;
@@ -1504,6 +1533,8 @@ size_t carve(const tsph_engine_params& p, Dev* d, char* base, CaseDev** cases, c
   t.csK = static_cast<double4*>(take(NF * sizeof(double4)));
   t.st = static_cast<float2*>(take(NF * sizeof(float2)));
   t.csf_hist = static_cast<unsigned int*>(take(static_cast<size_t>(p.max_cases) * 256 * sizeof(unsigned int)));
+  t.nbr4 = static_cast<uint32_t*>(take(static_cast<size_t>(p.max_fit_neighbors) * NF * sizeof(uint32_t)));
+  t.cnt4 = static_cast<int32_t*>(take(NF * sizeof(int32_t)));
   t.nbr = static_cast<uint32_t*>(take(static_cast<size_t>(p.max_neighbors) * N * sizeof(uint32_t)));
   t.cnt = static_cast<int32_t*>(take(N * sizeof(int32_t)));
   t.ob_rows = static_cast<int32_t*>(take(std::max<int64_t>(p.max_obstacle, 1) * sizeof(int32_t)));
@@ -1607,11 +1638,13 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr) {
   const int B = E->block;
   const unsigned g = grid_for(d.nf, B);
   const bool one = E->order.size() == 1;
-  (one ? k_density<true> : k_density<false>)<<<g, B, 0, s>>>(d);
+  const bool deep = E->batch == 8;
+#define TSPH_PICK(K) (one ? (deep ? K<true, 8> : K<true, 4>) : (deep ? K<false, 8> : K<false, 4>))
+  TSPH_PICK(k_density)<<<g, B, 0, s>>>(d);
   mark();
-  (one ? k_diffusion_eos<true> : k_diffusion_eos<false>)<<<g, B, 0, s>>>(d);
+  TSPH_PICK(k_diffusion_eos)<<<g, B, 0, s>>>(d);
   mark();
-  if (d.nw) (one ? k_walls<true> : k_walls<false>)<<<grid_for(d.nw, B), B, 0, s>>>(d);
+  if (d.nw) TSPH_PICK(k_walls)<<<grid_for(d.nw, B), B, 0, s>>>(d);
   if (d.has_csf) {
     const unsigned gf = static_cast<unsigned>((d.nf + B - 1) / B);
     k_csf_clear<<<gc, 128, 0, s>>>(d);
@@ -1629,7 +1662,8 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr) {
     TSPH_LAUNCH_CHECK();
   }
   mark();  // walls + surface tension
-  (one ? k_force<true> : k_force<false>)<<<g, B, 0, s>>>(d);
+  TSPH_PICK(k_force)<<<g, B, 0, s>>>(d);
+#undef TSPH_PICK
   mark();
   if (d.n_ob) k_reaction<<<static_cast<unsigned>((d.n_ob + B - 1) / B), B, 0, s>>>(d);
   mark();
@@ -1716,6 +1750,7 @@ CaseDev make_case_dev(const tsph_case_params& p, int64_t* ncells) {
   c.vol_scale = 1.0 / p.rho0;
   c.stencil_cells = static_cast<int>(std::ceil((4.0 * p.h + p.skin) / cell));
   c.stencil2 = 16.0 * p.h * p.h;
+  c.fit_rc2 = (4.0 * p.h + p.skin) * (4.0 * p.h + p.skin);
   return c;
 }
 
@@ -1771,7 +1806,7 @@ extern "C" {
 
 int64_t tsph_engine_bytes(const tsph_engine_params* prm) {
   if (!prm || prm->max_fluid <= 0 || prm->max_wall < 0 || prm->max_obstacle < 0 || prm->max_neighbors <= 0 ||
-      prm->max_cases <= 0 || prm->max_cells <= 0 || prm->diag_ring <= 0)
+      prm->max_cases <= 0 || prm->max_cells <= 0 || prm->diag_ring <= 0 || prm->max_fit_neighbors < 0)
     return -1;
   return static_cast<int64_t>(carve(*prm, nullptr, nullptr, nullptr, nullptr));
 }
@@ -1802,6 +1837,7 @@ int tsph_engine_create(const tsph_engine_params* prm, void* arena, int64_t arena
   d.nf = d.nw = d.n_ob = 0;
   d.n_slots = static_cast<int>(prm->max_cases);
   d.maxnb = static_cast<int>(prm->max_neighbors);
+  d.maxfit = static_cast<int>(prm->max_fit_neighbors);
   d.diag_ring = static_cast<int>(prm->diag_ring);
   d.shift_slot = 0;
   d.one_slot = 0;
@@ -1825,6 +1861,7 @@ int tsph_engine_add_case(tsph_engine* E, const tsph_case_params* p, const double
   // shifting needs the whole batch (its reference concentration is a global quantile)
   if (p->shift_every > 0 && !E->order.empty()) return TSPH_ERR_UNSUPPORTED;
   if (shifting(E)) return TSPH_ERR_UNSUPPORTED;
+  if (p->surface_tension > 0.0 && p->dim == 2 && E->prm.max_fit_neighbors <= 0) return TSPH_ERR_CAPACITY;
   if (E->free_slots.empty()) return TSPH_ERR_CAPACITY;
   Dev& d = E->d;
   int64_t ncells = 0;
@@ -1920,6 +1957,13 @@ int tsph_engine_remove_case(tsph_engine* E, int64_t case_id, tsph_stream stream)
     uint32_t* col = d.nbr + static_cast<int64_t>(k) * d.rows;
     if ((rc = move_down(col, sizeof(uint32_t), fb, fe, ftail, stage, stage_bytes, s))) return rc;
     if ((rc = move_down(col, sizeof(uint32_t), W0 + wb, W0 + we, wtail, stage, stage_bytes, s))) return rc;
+  }
+  if (d.has_csf) {
+    if ((rc = move_down(d.cnt4, sizeof(int32_t), fb, fe, ftail, stage, stage_bytes, s))) return rc;
+    for (int k = 0; k < d.maxfit; ++k)
+      if ((rc = move_down(d.nbr4 + static_cast<int64_t>(k) * d.NF, sizeof(uint32_t), fb, fe, ftail, stage,
+                          stage_bytes, s)))
+        return rc;
   }
   if ((rc = move_down(d.ob_rows, sizeof(int32_t), ob, ob + nob, otail, stage, stage_bytes, s))) return rc;
   CaseCtl off{};
@@ -2089,6 +2133,15 @@ int tsph_engine_set_block(tsph_engine* E, int64_t threads) {
   if (!E || (threads != 64 && threads != 128 && threads != 256)) return TSPH_ERR_ARG;
   if (threads != E->block) {
     E->block = static_cast<int>(threads);
+    invalidate_graph(E);
+  }
+  return TSPH_OK;
+}
+
+int tsph_engine_set_batch(tsph_engine* E, int64_t depth) {
+  if (!E || (depth != 4 && depth != 8)) return TSPH_ERR_ARG;
+  if (depth != E->batch) {
+    E->batch = static_cast<int>(depth);
     invalidate_graph(E);
   }
   return TSPH_OK;

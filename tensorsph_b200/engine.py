@@ -32,9 +32,10 @@ from .dam_break_3d import DamBreak3DConfig, make_column_3d, mass_3d, wall_lattic
 
 __all__ = ["BatchEngine", "CaseSpec", "DamBreak3DEngine", "DamBreak3DRun", "dam_break_2d_case",
            "dam_break_3d_case", "droplet_impact_case", "engine_bytes", "obstacle_case", "obstacle_lattice_3d",
-           "run_case", "run_dam_break_2d", "DIAG_FIELDS"]
+           "run_case", "run_dam_break_2d", "tune_single_case", "DIAG_FIELDS"]
 
 MAX_ROWS = (1 << 27) - 1   # fluid + wall rows of one engine (27-bit row index)
+FIT_NEIGHBORS = 128        # CSF curvature-fit row capacity (2-D, 4h + skin)
 
 DIAG_FIELDS = ("rho_max", "speed_max", "front", "force_x", "force_y", "force_z", "kinetic",
                "potential", "escapes", "clamps", "rebuilds", "row_max", "step", "status",
@@ -276,19 +277,20 @@ def droplet_impact_case(cfg, *, drop_speed: float = 0.0, label: str = "") -> Cas
 # ------------------------------------------------------------------ engine --
 
 def _engine_params(max_fluid, max_wall, max_obstacle, max_cells, max_cases, max_neighbors,
-                   diag_ring) -> _lib.EngineParams:
+                   diag_ring, max_fit_neighbors=0) -> _lib.EngineParams:
     prm = _lib.EngineParams()
     prm.max_fluid, prm.max_wall, prm.max_obstacle = int(max_fluid), int(max_wall), int(max_obstacle)
     prm.max_cells, prm.max_cases = int(max_cells), int(max_cases)
     prm.max_neighbors, prm.diag_ring = int(max_neighbors), int(diag_ring)
+    prm.max_fit_neighbors = int(max_fit_neighbors)
     return prm
 
 
 def engine_bytes(*, max_fluid, max_wall, max_obstacle=0, max_cells, max_cases=1,
-                 max_neighbors=160, diag_ring=1024) -> int:
+                 max_neighbors=160, diag_ring=1024, max_fit_neighbors=0) -> int:
     """Device bytes of an engine with these capacities (its HBM footprint)."""
     prm = _engine_params(max_fluid, max_wall, max_obstacle, max_cells, max_cases, max_neighbors,
-                         diag_ring)
+                         diag_ring, max_fit_neighbors)
     n = _lib.lib().tsph_engine_bytes(ctypes.byref(prm))
     if n <= 0:
         raise ValueError("invalid engine capacities")
@@ -300,16 +302,16 @@ class BatchEngine:
 
     def __init__(self, *, max_fluid: int, max_wall: int, max_obstacle: int = 0, max_cells: int,
                  max_cases: int = 1, max_neighbors: int = 160, diag_ring: int = 1024,
-                 device: torch.device | None = None):
+                 max_fit_neighbors: int = 0, device: torch.device | None = None):
         dev = device or _lib.cuda_device()
         self.device = dev
         self.stream = torch.cuda.Stream(device=dev)
         self.capacity = dict(max_fluid=int(max_fluid), max_wall=int(max_wall),
                              max_obstacle=int(max_obstacle), max_cells=int(max_cells),
                              max_cases=int(max_cases), max_neighbors=int(max_neighbors),
-                             diag_ring=int(diag_ring))
+                             diag_ring=int(diag_ring), max_fit_neighbors=int(max_fit_neighbors))
         self.params = _engine_params(max_fluid, max_wall, max_obstacle, max_cells, max_cases,
-                                     max_neighbors, diag_ring)
+                                     max_neighbors, diag_ring, max_fit_neighbors)
         L = _lib.lib()
         nbytes = L.tsph_engine_bytes(ctypes.byref(self.params))
         if nbytes <= 0:
@@ -372,6 +374,11 @@ class BatchEngine:
         """Threads per block of the pair kernels (64, 128 or 256): a tuning knob."""
         _lib.check(_lib.lib().tsph_engine_set_block(self._handle, int(threads)),
                    "tsph_engine_set_block")
+
+    def set_batch(self, depth: int) -> None:
+        """Neighbour records in flight per thread (4 or 8): a tuning knob."""
+        _lib.check(_lib.lib().tsph_engine_set_batch(self._handle, int(depth)),
+                   "tsph_engine_set_batch")
 
     def step(self, steps: int = 1, graph: bool = True) -> None:
         """Advance every case ``steps`` steps on the engine's stream (no host
@@ -466,11 +473,13 @@ class BatchEngine:
 def capacity_for(specs, *, max_neighbors: int = 160, diag_ring: int = 1024, cases: int | None = None):
     """Capacities that hold every case of ``specs`` at once."""
     specs = list(specs)
+    csf = any(s.dim == 2 and s.params.surface_tension > 0.0 for s in specs)
     return dict(max_fluid=sum(s.n_fluid for s in specs), max_wall=max(1, sum(s.n_wall for s in specs)),
                 max_obstacle=sum(s.n_obstacle for s in specs),
                 max_cells=sum(s.cells() for s in specs),
                 max_cases=cases if cases is not None else len(specs),
-                max_neighbors=max_neighbors, diag_ring=diag_ring)
+                max_neighbors=max_neighbors, diag_ring=diag_ring,
+                max_fit_neighbors=FIT_NEIGHBORS if csf else 0)
 
 
 # ------------------------------------------------------- single-case engine --
@@ -538,6 +547,39 @@ class DamBreak3DEngine(BatchEngine):
 
     def status(self) -> dict:  # type: ignore[override]
         return super().status(self.case_id)
+
+
+def tune_single_case(cfg: DamBreak3DConfig, *, obstacle=None, shift_every: int = 0, host_state=None,
+                     skins=(0.1, 0.15, 0.25), blocks=(128, 256), batches=(4, 8), steps: int = 60,
+                     device=None) -> dict:
+    """Autotune one 3-D case by timing: the Verlet skin (which sets the cell edge
+    2h + skin and how often lists are rebuilt), the pair kernels' block size and
+    their batch depth.  Each trial runs ``steps`` graph steps on the device
+    (rebuilds included); the results do not depend on the choice beyond the
+    summation order of the skin pairs.  Returns the fastest and every trial."""
+    from dataclasses import replace
+    trials = []
+    for skin in skins:
+        c = replace(cfg, pair_skin_factor=float(skin))
+        eng = DamBreak3DEngine(c, obstacle=obstacle, shift_every=shift_every, host_state=host_state,
+                               diag_ring=8, device=device)
+        eng.step(3)
+        for block in blocks:
+            for batch in batches:
+                eng.set_block(block)
+                eng.set_batch(batch)
+                eng.step(2)
+                start = torch.cuda.Event(enable_timing=True)
+                stop = torch.cuda.Event(enable_timing=True)
+                start.record(eng.stream)
+                eng.step(steps)
+                stop.record(eng.stream)
+                stop.synchronize()
+                trials.append({"skin_factor": float(skin), "block": block, "batch": batch,
+                               "ms_per_step": start.elapsed_time(stop) / steps})
+        eng.close()
+    best = min(trials, key=lambda t: t["ms_per_step"])
+    return {"best": best, "trials": trials}
 
 
 def run_case(cfg: DamBreak3DConfig, pair_skin_factor: float | None = None, snapshot_times=None,

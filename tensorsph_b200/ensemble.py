@@ -76,11 +76,12 @@ def _timed_steps(eng: BatchEngine, steps: int) -> float:
     return start.elapsed_time(stop) / 1e3
 
 
-def run_batched(specs, steps: int, *, warmup: int = 3, block: int = 128, max_neighbors: int = 64,
-                device=None) -> dict:
+def run_batched(specs, steps: int, *, warmup: int = 3, block: int = 128, batch: int = 4,
+                max_neighbors: int = 64, device=None) -> dict:
     """All cases in one engine; device time of ``steps`` steps after ``warmup``."""
     eng = BatchEngine(**capacity_for(specs, max_neighbors=max_neighbors, diag_ring=8), device=device)
     eng.set_block(block)
+    eng.set_batch(batch)
     ids = [eng.add(s) for s in specs]
     eng.step(warmup)
     t = _timed_steps(eng, steps)
@@ -109,9 +110,10 @@ def run_plain(specs, steps: int, *, warmup: int = 3, block: int = 128, max_neigh
             "seconds": total_t, "updates_per_s": total_u / total_t}
 
 
-def autotune(draws, *, blocks=(64, 128, 256), skins=(0.15, 0.25, 0.4), steps: int = 30,
-             warmup: int = 10, device=None) -> dict:
-    """Time each (block, skin) on the sample ``draws`` and return the fastest.
+def autotune(draws, *, blocks=(64, 128, 256), batches=(4, 8), skins=(0.15, 0.25, 0.4),
+             steps: int = 30, warmup: int = 10, device=None) -> dict:
+    """Time each (block, batch depth, skin) on the sample ``draws`` and return
+    the fastest.
 
     The skin sets both the cell edge (2h + skin) and how often lists are
     rebuilt, so it is timed over enough steps to include rebuilds."""
@@ -119,7 +121,9 @@ def autotune(draws, *, blocks=(64, 128, 256), skins=(0.15, 0.25, 0.4), steps: in
     for skin in skins:
         specs = ensemble_specs(draws, skin_factor=skin)
         for block in blocks:
-            r = run_batched(specs, steps, warmup=warmup, block=block, device=device)
-            trials.append({"block": block, "skin_factor": skin, "updates_per_s": r["updates_per_s"]})
+            for batch in batches:
+                r = run_batched(specs, steps, warmup=warmup, block=block, batch=batch, device=device)
+                trials.append({"block": block, "batch": batch, "skin_factor": skin,
+                               "updates_per_s": r["updates_per_s"]})
     best = max(trials, key=lambda t: t["updates_per_s"])
     return {"best": best, "trials": trials}
