@@ -63,7 +63,7 @@ struct CaseDev {
   float grav, nu2, nu2f, dscale, dtf, visc_eps, rho_floor, wall_mass;
   int csf;                 // CSF surface tension on (2-D)
   int stencil_cells;       // cells each side covering the 4h fit stencil
-  double sigma_st, h_d, sigma2d_d, vol_scale;  // CSF: sigma, h, 10/(7 pi h^2), 1/rho0
+  double sigma_st, h_d, inv_h_d, sigma2d_d, vol_scale;  // CSF: sigma, h, 1/h, 10/(7 pi h^2), 1/rho0
   double stencil2;         // (4h)^2
   double fit_rc2;          // (4h + skin)^2, the fit rows' list cutoff
 };
@@ -171,6 +171,14 @@ __device__ __forceinline__ double4 ld4(const double4* p, int64_t i) {
   const double2* q = reinterpret_cast<const double2*>(p + i);
   double2 a = q[0], b = q[1];
   return make_double4(a.x, a.y, b.x, b.y);
+}
+
+// x, y of a double4 record (one 16-byte load) and its fourth component
+__device__ __forceinline__ double2 ld_xy(const double4* p, int64_t i) {
+  return *reinterpret_cast<const double2*>(p + i);
+}
+__device__ __forceinline__ double ld_w(const double4* p, int64_t i) {
+  return reinterpret_cast<const double*>(p + i)[3];
 }
 
 __device__ __forceinline__ void st4(double4* p, int64_t i, double4 v) {
@@ -390,13 +398,19 @@ __global__ void k_rows(Dev e) {
           const int fs = e.fstart[cell];
           if (fs >= 0) {
             const int fe = e.fend[cell];
-            for (int b = fs; b < fe; ++b) {
-              if (b == a) continue;
-              const double4 pb = ld4(e.pos, b);
-              const double ddx = pa.x - pb.x, ddy = pa.y - pb.y, ddz = pa.z - pb.z;
-              if (ddx * ddx + ddy * ddy + ddz * ddz <= rc2) {
-                if (count < e.maxnb) e.nbr[static_cast<int64_t>(count) * e.rows + a] = (static_cast<uint32_t>(b) << 5) | code;
-                ++count;
+            for (int b0 = fs; b0 < fe; b0 += 4) {
+              double4 pb[4];
+#pragma unroll
+              for (int j = 0; j < 4; ++j) pb[j] = ld4(e.pos, b0 + j < fe ? b0 + j : b0);
+#pragma unroll
+              for (int j = 0; j < 4; ++j) {
+                const int b = b0 + j;
+                const double ddx = pa.x - pb[j].x, ddy = pa.y - pb[j].y, ddz = pa.z - pb[j].z;
+                if (b < fe && b != a && ddx * ddx + ddy * ddy + ddz * ddz <= rc2) {
+                  if (count < e.maxnb)
+                    e.nbr[static_cast<int64_t>(count) * e.rows + a] = (static_cast<uint32_t>(b) << 5) | code;
+                  ++count;
+                }
               }
             }
           }
@@ -404,14 +418,19 @@ __global__ void k_rows(Dev e) {
             const int ws = e.wstart[cell];
             if (ws >= 0) {
               const int we = e.wend[cell];
-              for (int w = ws; w < we; ++w) {
-                const int64_t b = e.NF + w;
-                const double4 pb = ld4(e.pos, b);
-                const double ddx = pa.x - pb.x, ddy = pa.y - pb.y, ddz = pa.z - pb.z;
-                if (ddx * ddx + ddy * ddy + ddz * ddz <= rc2) {
-                  if (count < e.maxnb)
-                    e.nbr[static_cast<int64_t>(count) * e.rows + a] = (static_cast<uint32_t>(b) << 5) | code;
-                  ++count;
+              for (int w0 = ws; w0 < we; w0 += 4) {
+                double4 pb[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) pb[j] = ld4(e.pos, e.NF + (w0 + j < we ? w0 + j : w0));
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                  const int64_t b = e.NF + w0 + j;
+                  const double ddx = pa.x - pb[j].x, ddy = pa.y - pb[j].y, ddz = pa.z - pb[j].z;
+                  if (w0 + j < we && ddx * ddx + ddy * ddy + ddz * ddz <= rc2) {
+                    if (count < e.maxnb)
+                      e.nbr[static_cast<int64_t>(count) * e.rows + a] = (static_cast<uint32_t>(b) << 5) | code;
+                    ++count;
+                  }
                 }
               }
             }
@@ -439,13 +458,18 @@ __global__ void k_rows(Dev e) {
           const int fs = e.fstart[cell];
           if (fs < 0) continue;
           const int fe = e.fend[cell];
-          for (int b = fs; b < fe; ++b) {
-            if (b == a) continue;
-            const double4 pb = ld4(e.pos, b);
-            const double ddx = pa.x - pb.x, ddy = pa.y - pb.y;
-            if (ddx * ddx + ddy * ddy <= C.fit_rc2) {
-              if (c4 < e.maxfit) e.nbr4[static_cast<int64_t>(c4) * e.NF + a] = static_cast<uint32_t>(b) << 5;
-              ++c4;
+          for (int b0 = fs; b0 < fe; b0 += 4) {
+            double2 pb[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) pb[j] = ld_xy(e.pos, b0 + j < fe ? b0 + j : b0);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              const int b = b0 + j;
+              const double ddx = pa.x - pb[j].x, ddy = pa.y - pb[j].y;
+              if (b < fe && b != a && ddx * ddx + ddy * ddy <= C.fit_rc2) {
+                if (c4 < e.maxfit) e.nbr4[static_cast<int64_t>(c4) * e.NF + a] = static_cast<uint32_t>(b) << 5;
+                ++c4;
+              }
             }
           }
         }
@@ -746,21 +770,31 @@ struct KD {
 };
 __device__ __forceinline__ KD kernel_d(double dx, double dy, const CaseDev& C) {
   const double r = sqrt(dx * dx + dy * dy);
-  const double q = r / C.h_d;
+  const double q = r * C.inv_h_d;
   KD k;
   k.w = C.sigma2d_d * shape_d(q);
-  k.gs = C.sigma2d_d * dshape_d(q) / (C.h_d * fmax(r, 1e-12));
+  k.gs = C.sigma2d_d * dshape_d(q) * C.inv_h_d / fmax(r, 1e-12);
   return k;
 }
 
-// Loop the fluid neighbours b of fluid row a (2h rows; walls skipped).
+// Loop the fluid neighbours of fluid row a (2h rows; walls skipped) in
+// batches of four: body(b[4], ok[4]) gets the entries of a batch at once so
+// that their record loads are all in flight together; padded and wall
+// entries come with ok = false and b = a.
 template <class Body>
 __device__ __forceinline__ void fluid_row(const Dev& e, int a, Body&& body) {
   const int n = e.cnt[a];
   const uint32_t* row = e.nbr + a;
-  for (int k = 0; k < n; ++k) {
-    const uint32_t b = row[static_cast<int64_t>(k) * e.rows] >> 5;
-    if (b < static_cast<uint32_t>(e.NF)) body(static_cast<int>(b));
+  for (int k = 0; k < n; k += 4) {
+    int b[4];
+    bool ok[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const uint32_t v = (k + j < n) ? (row[static_cast<int64_t>(k + j) * e.rows] >> 5) : 0xffffffffu;
+      ok[j] = v < static_cast<uint32_t>(e.NF);
+      b[j] = ok[j] ? static_cast<int>(v) : a;
+    }
+    body(b, ok);
   }
 }
 
@@ -781,16 +815,26 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_colour(const __grid_constant_
     if (!C.csf) continue;
     const double4 pa = ld4(e.pos, a);
     double c = pa.w * C.vol_scale * C.sigma2d_d, m00 = 0.0, m01 = 0.0, m11 = 0.0;
-    fluid_row(e, a, [&](int b) {
-      const double4 pb = ld4(e.pos, b);
-      const double dx = pa.x - pb.x, dy = pa.y - pb.y;
-      const KD k = kernel_d(dx, dy, C);
-      const double vb = pb.w * C.vol_scale;
-      c += vb * k.w;
-      const double g = -vb * k.gs;  // M += V_b (-d) (x) (d gs)
-      m00 += g * (dx * dx);
-      m01 += g * (dx * dy);
-      m11 += g * (dy * dy);
+    fluid_row(e, a, [&](const int* b, const bool* ok) {
+      double2 pb[4];
+      double mb[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        pb[j] = ld_xy(e.pos, b[j]);
+        mb[j] = ld_w(e.pos, b[j]);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (!ok[j]) continue;
+        const double dx = pa.x - pb[j].x, dy = pa.y - pb[j].y;
+        const KD k = kernel_d(dx, dy, C);
+        const double vb = mb[j] * C.vol_scale;
+        c += vb * k.w;
+        const double g = -vb * k.gs;  // M += V_b (-d) (x) (d gs)
+        m00 += g * (dx * dx);
+        m01 += g * (dx * dy);
+        m11 += g * (dy * dy);
+      }
     });
     c = c < 0.0 ? 0.0 : (c > 1.0 ? 1.0 : c);
     e.csA[a] = make_double4(c, m00, m01, m11);
@@ -830,27 +874,49 @@ __global__ void k_csf_hist(const __grid_constant__ Dev e, int shift) {
       if (h[i]) atomicAdd(&e.csf_hist[cb * 256 + i], h[i]);
 }
 
+// One warp per case: lane l owns bins [8l, 8l + 8); the digit holding the
+// rank is found with a warp prefix sum instead of a serial walk of 256 bins.
 __global__ void k_csf_pick(const __grid_constant__ Dev e, int shift) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
   if (c >= e.n_slots) return;
   CaseCtl& t = e.ctl[c];
   const CaseDev& C = e.cases[c];
-  unsigned int* h = e.csf_hist + c * 256;
   if (!t.active || !C.csf) return;
-  if (shift == 56) {
-    t.csf_prefix = 0;
-    t.csf_rank = (C.n_fluid - 1) / 2;
+  unsigned int* h = e.csf_hist + c * 256;
+  const long long rank = shift == 56 ? static_cast<long long>((C.n_fluid - 1) / 2) : t.csf_rank;
+  const unsigned long long prefix = shift == 56 ? 0ull : t.csf_prefix;
+  unsigned int mine[8];
+  long long local = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    mine[i] = h[lane * 8 + i];
+    local += mine[i];
   }
-  long long k = t.csf_rank;
-  int d = 0;
-  for (; d < 255; ++d) {
-    if (k < static_cast<long long>(h[d])) break;
-    k -= h[d];
+  long long incl = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const long long nb = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += nb;
   }
-  t.csf_prefix |= static_cast<unsigned long long>(d) << shift;
-  t.csf_rank = k;
-  for (int i = 0; i < 256; ++i) h[i] = 0;
-  if (shift == 0) t.csf_med = __longlong_as_double(static_cast<long long>(t.csf_prefix));
+  const long long excl = incl - local;
+  // the lane whose range holds the rank (the last lane if counts fall short)
+  const bool holds = rank >= excl && rank < incl;
+  const unsigned int ballot = __ballot_sync(0xffffffffu, holds);
+  const int owner = ballot ? __ffs(ballot) - 1 : 31;
+  if (lane == owner) {
+    long long k = rank - excl;
+    int d = lane * 8;
+    for (int i = 0; i < 8; ++i, ++d) {
+      if (k < static_cast<long long>(mine[i]) || i == 7) break;
+      k -= mine[i];
+    }
+    t.csf_prefix = prefix | (static_cast<unsigned long long>(d) << shift);
+    t.csf_rank = k;
+    if (shift == 0) t.csf_med = __longlong_as_double(static_cast<long long>(t.csf_prefix));
+  }
+#pragma unroll
+  for (int i = 0; i < 8; ++i) h[lane * 8 + i] = 0;
 }
 
 // M' = M, or the identity where |det M| <= 1e-4 median |det M| (csf_consistent.py:106-113)
@@ -884,13 +950,24 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_grad(const __grid_constant__ 
       const double4 pa = ld4(e.pos, a);
       const double4 A = e.csA[a];
       double gx = 0.0, gy = 0.0;
-      fluid_row(e, a, [&](int b) {
-        const double4 pb = ld4(e.pos, b);
-        const double dx = pa.x - pb.x, dy = pa.y - pb.y;
-        const KD k = kernel_d(dx, dy, C);
-        const double w = pb.w * C.vol_scale * (e.csA[b].x - A.x) * k.gs;
-        gx += w * dx;
-        gy += w * dy;
+      fluid_row(e, a, [&](const int* b, const bool* ok) {
+        double2 pb[4];
+        double mb[4], cb[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          pb[j] = ld_xy(e.pos, b[j]);
+          mb[j] = ld_w(e.pos, b[j]);
+          cb[j] = e.csA[b[j]].x;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          if (!ok[j]) continue;
+          const double dx = pa.x - pb[j].x, dy = pa.y - pb[j].y;
+          const KD k = kernel_d(dx, dy, C);
+          const double w = mb[j] * C.vol_scale * (cb[j] - A.x) * k.gs;
+          gx += w * dx;
+          gy += w * dy;
+        }
       });
       double p, q, r;
       const double4 B = e.csB[a];
@@ -919,13 +996,23 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_smooth(const __grid_constant_
     if (!C.csf) continue;
     const double4 pa = ld4(e.pos, a);
     double nx = 0.0, ny = 0.0, den = pa.w * C.vol_scale * C.sigma2d_d;
-    fluid_row(e, a, [&](int b) {
-      const double4 pb = ld4(e.pos, b);
-      const double w = pb.w * C.vol_scale * kernel_d(pa.x - pb.x, pa.y - pb.y, C).w;
-      const double2 nb = src[b];
-      nx += w * nb.x;
-      ny += w * nb.y;
-      den += w;
+    fluid_row(e, a, [&](const int* b, const bool* ok) {
+      double2 pb[4], nb[4];
+      double mb[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        pb[j] = ld_xy(e.pos, b[j]);
+        mb[j] = ld_w(e.pos, b[j]);
+        nb[j] = src[b[j]];
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (!ok[j]) continue;
+        const double w = mb[j] * C.vol_scale * kernel_d(pa.x - pb[j].x, pa.y - pb[j].y, C).w;
+        nx += w * nb[j].x;
+        ny += w * nb[j].y;
+        den += w;
+      }
     });
     den = fmax(den, 1e-30);
     const double sx = nx / den, sy = ny / den;
@@ -951,17 +1038,27 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_div(const __grid_constant__ D
     const double4 pa = ld4(e.pos, a);
     const double2 na = e.csN[a];
     double s00 = 0.0, s01 = 0.0, s10 = 0.0, s11 = 0.0;
-    fluid_row(e, a, [&](int b) {
-      const double4 pb = ld4(e.pos, b);
-      const double dx = pa.x - pb.x, dy = pa.y - pb.y;
-      const double gs = pb.w * C.vol_scale * kernel_d(dx, dy, C).gs;
-      const double g0 = gs * dx, g1 = gs * dy;
-      const double2 nb = e.csN[b];
-      const double dn0 = nb.x - na.x, dn1 = nb.y - na.y;
-      s00 += dn0 * g0;
-      s01 += dn0 * g1;
-      s10 += dn1 * g0;
-      s11 += dn1 * g1;
+    fluid_row(e, a, [&](const int* b, const bool* ok) {
+      double2 pb[4], nb[4];
+      double mb[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        pb[j] = ld_xy(e.pos, b[j]);
+        mb[j] = ld_w(e.pos, b[j]);
+        nb[j] = e.csN[b[j]];
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (!ok[j]) continue;
+        const double dx = pa.x - pb[j].x, dy = pa.y - pb[j].y;
+        const double gs = mb[j] * C.vol_scale * kernel_d(dx, dy, C).gs;
+        const double g0 = gs * dx, g1 = gs * dy;
+        const double dn0 = nb[j].x - na.x, dn1 = nb[j].y - na.y;
+        s00 += dn0 * g0;
+        s01 += dn0 * g1;
+        s10 += dn1 * g0;
+        s11 += dn1 * g1;
+      }
     });
     double p, q, r;
     csf_matrix(e, c, e.csA[a], e.csB[a].w, p, q, r);
@@ -990,30 +1087,45 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_fit(const __grid_constant__ D
     const CaseDev& C = e.cases[c];
     if (C.csf) {
       const double gmax = fmax(__longlong_as_double(static_cast<long long>(e.ctl[c].csf_gmax)), 1e-30);
+      const double inv_g = 1.0 / gmax;
+      const double st2 = C.stencil2;
       const double4 pa = ld4(e.pos, a);
       const double2 na = e.csN[a];
       const double tx = -na.y, ty = na.x;
       double s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0, s6 = 0, s7 = 0;
       const int n4 = e.cnt4[a];
-      for (int k = 0; k < n4; ++k) {
-        const int b = static_cast<int>(e.nbr4[static_cast<int64_t>(k) * e.NF + a] >> 5);
-        const double4 pb = ld4(e.pos, b);
-        const double ddx = pa.x - pb.x, ddy = pa.y - pb.y;
-        if (ddx * ddx + ddy * ddy > C.stencil2) continue;
-        double w = e.csB[b].z / gmax;
-        w = w < 0.0 ? 0.0 : (w > 1.0 ? 1.0 : w);
-        const double u = -(ddx * tx + ddy * ty), v = -(ddx * na.x + ddy * na.y);
-        const double uu = u * u;
-        s0 += w;
-        s1 += w * u;
-        s2 += w * v;
-        s3 += w * uu;
-        s4 += w * (u * v);
-        s5 += w * (uu * u);
-        s6 += w * (uu * v);
-        s7 += w * (uu * uu);
+      for (int k = 0; k < n4; k += 4) {
+        int b[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          b[j] = k + j < n4 ? static_cast<int>(e.nbr4[static_cast<int64_t>(k + j) * e.NF + a] >> 5) : a;
+        double2 pb[4];
+        double mg[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          pb[j] = ld_xy(e.pos, b[j]);
+          mg[j] = e.csB[b[j]].z;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const double ddx = pa.x - pb[j].x, ddy = pa.y - pb[j].y;
+          // padding (b == a) and points beyond the 4h stencil get no weight
+          double w = mg[j] * inv_g;
+          w = w < 0.0 ? 0.0 : (w > 1.0 ? 1.0 : w);
+          w = (k + j < n4 && ddx * ddx + ddy * ddy <= st2) ? w : 0.0;
+          const double u = -(ddx * tx + ddy * ty), v = -(ddx * na.x + ddy * na.y);
+          const double uu = u * u;
+          s0 += w;
+          s1 += w * u;
+          s2 += w * v;
+          s3 += w * uu;
+          s4 += w * (u * v);
+          s5 += w * (uu * u);
+          s6 += w * (uu * v);
+          s7 += w * (uu * uu);
+        }
       }
-      double wa = e.csB[a].z / gmax;
+      double wa = e.csB[a].z * inv_g;
       wa = wa < 0.0 ? 0.0 : (wa > 1.0 ? 1.0 : wa);
       s0 += wa;
       // [s0 s1 s3; s1 s3 s5; s3 s5 s7] (c, b, a) = (s2, s4, s6); Cramer's rule
@@ -1649,9 +1761,11 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr) {
     const unsigned gf = static_cast<unsigned>((d.nf + B - 1) / B);
     k_csf_clear<<<gc, 128, 0, s>>>(d);
     k_csf_colour<<<g, B, 0, s>>>(d);
+    const unsigned gh = static_cast<unsigned>((d.nf + 255) / 256);
+    const unsigned gp = static_cast<unsigned>((d.n_slots + 3) / 4);
     for (int shift = 56; shift >= 0; shift -= 8) {
-      k_csf_hist<<<gf, B, 0, s>>>(d, shift);
-      k_csf_pick<<<gc, 128, 0, s>>>(d, shift);
+      k_csf_hist<<<gh, 256, 0, s>>>(d, shift);
+      k_csf_pick<<<gp, 128, 0, s>>>(d, shift);
     }
     k_csf_grad<<<gf, B, 0, s>>>(d);
     k_csf_smooth<false><<<g, B, 0, s>>>(d);
@@ -1746,6 +1860,7 @@ CaseDev make_case_dev(const tsph_case_params& p, int64_t* ncells) {
   c.csf = (p.surface_tension > 0.0 && p.dim == 2) ? 1 : 0;
   c.sigma_st = p.surface_tension;
   c.h_d = p.h;
+  c.inv_h_d = 1.0 / p.h;
   c.sigma2d_d = 10.0 / (7.0 * M_PI * p.h * p.h);
   c.vol_scale = 1.0 / p.rho0;
   c.stencil_cells = static_cast<int>(std::ceil((4.0 * p.h + p.skin) / cell));
