@@ -127,3 +127,40 @@ def autotune(draws, *, blocks=(64, 128, 256), batches=(4, 8), skins=(0.15, 0.25,
                                "updates_per_s": r["updates_per_s"]})
     best = max(trials, key=lambda t: t["updates_per_s"])
     return {"best": best, "trials": trials}
+
+
+def main(argv=None) -> None:
+    """``python -m tensorsph_b200.ensemble --cases N --steps K``: run one
+    batched droplet ensemble and print its device throughput."""
+    import argparse
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--cases", type=int, default=256)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--skin", type=float, default=0.15)
+    ap.add_argument("--block", type=int, default=64)
+    ap.add_argument("--batch", type=int, default=4)
+    ap.add_argument("--sigma", type=float, default=0.0728)
+    ap.add_argument("--eager", action="store_true", help="launch kernel by kernel (no graph)")
+    args = ap.parse_args(argv)
+    specs = ensemble_specs(draw_ensemble(args.cases, seed=args.seed), skin_factor=args.skin,
+                           surface_tension=args.sigma)
+    eng = BatchEngine(**capacity_for(specs, max_neighbors=64, diag_ring=8))
+    eng.set_block(args.block)
+    eng.set_batch(args.batch)
+    for s in specs:
+        eng.add(s)
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    start.record(eng.stream)
+    eng.step(args.steps, graph=not args.eager)
+    stop.record(eng.stream)
+    stop.synchronize()
+    ms = start.elapsed_time(stop) / max(args.steps, 1)
+    nf = sum(s.n_fluid for s in specs)
+    print(f"cases {len(specs)} fluid {nf} ms/step {ms:.3f} updates/s {nf / ms * 1e3:.3e}")
+    eng.close()
+
+
+if __name__ == "__main__":
+    main()
