@@ -62,6 +62,21 @@ def parse():
     return ap.parse_args()
 
 
+def max_over_ranks(value: float, dist=None, device=None) -> float:
+    """The largest value over all ranks (every rank calls it, in the same order)."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t)
+
+
+def whole_job_rate(units_per_rank: int, steps: int, world: int, seconds: float) -> float:
+    """Units processed by all ranks divided by the (max-over-ranks) time."""
+    return units_per_rank * steps * world / seconds
+
+
 def peaks():
     path = ROOT / "MEASURED_PEAKS.json"
     if path.exists():
@@ -317,14 +332,10 @@ def main():
     torch.cuda.synchronize(dev)
     barrier()
     clocks = sampler.stop()
-    ms = start.elapsed_time(stop)
-    if dist is not None:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t)
+    ms = max_over_ranks(start.elapsed_time(stop), dist, dev)
     status = eng.status()
     ms_step = ms / args.steps
-    value = nf * args.steps * world / (ms / 1e3)
+    value = whole_job_rate(nf, args.steps, world, ms / 1e3)
     kernels_per_step = eng.graph_kernels()
 
     stage = {}
@@ -365,13 +376,10 @@ def main():
         torch.cuda.synchronize(dev)
         t_e2e = time.perf_counter() - t0
         barrier()
-        if dist is not None:
-            t = torch.tensor([t_e2e], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            t_e2e = float(t)
+        t_e2e = max_over_ranks(t_e2e, dist, dev)
         e.close()
         state_bytes = (x.numel() + m.numel() + w.numel()) * 8
-        e2e = {"value": nf * args.steps * world / t_e2e, "unit": "fluid particle-updates/s",
+        e2e = {"value": whole_job_rate(nf, args.steps, world, t_e2e), "unit": "fluid particle-updates/s",
                "h2d_bytes_per_step": state_bytes / args.steps,
                "d2h_bytes_per_step": 16 * 8 + nf * 3 * 8 / args.steps,
                "scope": "engine creation from pinned host lattices + K steps with a per-step "
