@@ -450,6 +450,26 @@ def delta_plus_cases(dp):
     return data
 
 
+def config1_run_case(db):
+    """The reference's own 2-D dam-break loop (dam_break.run_case) on the
+    5,000-particle configuration for 150 steps in FP64: sampled front and
+    energies and the final positions."""
+    c0 = 10.0 * math.sqrt(2.0 * 9.81 * 2.0)
+    torch.set_default_dtype(torch.float64)
+    try:
+        cfg = db.DamBreakConfig(dx=0.02, column_width=1.0, column_height=2.0, pool_width=4.0,
+                                tank_height=3.0, sound_speed=c0, viscosity=1e-6, max_courant=0.25,
+                                dt=0.25 * 1.3 * 0.02 / c0, steps=150, output_every=50,
+                                wall_layers=3, device="cpu")
+        run = db.run_case(cfg)
+    finally:
+        torch.set_default_dtype(torch.float32)
+    return {"times": np.asarray(run.times), "front": np.asarray(run.front),
+            "kinetic": np.asarray(run.kinetic_energy), "potential": np.asarray(run.potential_energy),
+            "final_positions": _np(run.final_positions), "rebuilds": np.int64(run.rebuilds),
+            "escaped": np.int64(run.escaped), "steps": np.int64(run.steps_taken)}
+
+
 def main(src, families=None):
     sys.path.insert(0, str(src))
     import tensorsph.neighbor_search as ns
@@ -478,6 +498,7 @@ def main(src, families=None):
         "shear": lambda: shear_cases(sv),
         "csf": lambda: csf_cases(ca, di),
         "delta_plus": lambda: delta_plus_cases(dp),
+        "config1_run": lambda: config1_run_case(db),
     }
     for name in families or makers:
         np.savez_compressed(OUT / f"{name}.npz", **makers[name](), **meta)

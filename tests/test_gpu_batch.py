@@ -210,3 +210,31 @@ def test_droplet_ensemble_batched_equals_plain(gpu):
         for u, w in zip(g, ref):
             assert torch.equal(u, w)
         assert float(g[1][:, 1].min()) < -0.9   # the drop keeps its impact speed
+
+
+def test_config1_run_follows_reference_run(golden, gpu):
+    """The 5,000-particle 2-D dam break (dx = 0.02, c0 = 62.6, 150 steps) on the
+    device against the reference's own FP64 ``dam_break.run_case``: the sampled
+    front and energies and the final positions (the engine's pair sums are
+    FP32 on FP64 state)."""
+    from tensorsph_b200.dam_break import DamBreakConfig
+    from tensorsph_b200.engine import run_dam_break_2d
+    g = golden("config1_run")
+    c0 = 10.0 * math.sqrt(2.0 * 9.81 * 2.0)
+    cfg = DamBreakConfig(dx=0.02, column_width=1.0, column_height=2.0, pool_width=4.0,
+                         tank_height=3.0, sound_speed=c0, viscosity=1e-6, max_courant=0.25,
+                         dt=0.25 * 1.3 * 0.02 / c0, steps=150, output_every=50, wall_layers=3)
+    saved = torch.get_default_dtype()
+    torch.set_default_dtype(torch.float64)
+    try:
+        run = run_dam_break_2d(cfg)
+    finally:
+        torch.set_default_dtype(saved)
+    assert run.steps_taken == int(g["steps"]) and run.escaped == int(g["escaped"])
+    assert np.allclose(run.times, g["times"], rtol=0, atol=1e-15)
+    assert np.abs(np.asarray(run.front) - g["front"]).max() < 1e-6
+    assert np.abs(np.asarray(run.potential_energy) - g["potential"]).max() < 1e-9 * g["potential"][0]
+    ke = np.asarray(run.kinetic_energy)
+    assert np.abs(ke - g["kinetic"]).max() < 1e-4 * g["kinetic"].max(), (ke, g["kinetic"])
+    dx = np.abs(run.final_positions.numpy() - g["final_positions"]).max()
+    assert dx < 1e-6, dx
