@@ -599,26 +599,30 @@ def run_case(cfg: DamBreak3DConfig, pair_skin_factor: float | None = None, snaps
         from dataclasses import replace
         cfg = replace(cfg, pair_skin_factor=pair_skin_factor)
     eng = DamBreak3DEngine(cfg, obstacle=obstacle, shift_every=shift_every, seed=seed,
-                           max_neighbors=max_neighbors, diag_ring=max(cfg.steps + 1, 1))
+                           max_neighbors=max_neighbors, diag_ring=max(cfg.steps + 2, 2))
     eng.step(cfg.steps)
     with torch.cuda.stream(eng.stream):
-        diag = eng.diagnostics(0, cfg.steps).cpu()
         x, v, rho, p = eng.state()
+        xs, vs = x.cpu(), v.cpu()
     st = eng.status()
-    sample = [k for k in range(cfg.steps) if k % cfg.output_every == 0]
+    # the reference evaluates the right-hand side once more at step == steps
+    # to record the final meters, without integrating it
+    eng.step(1)
+    with torch.cuda.stream(eng.stream):
+        diag = eng.diagnostics(0, cfg.steps + 1).cpu()
+    sample = [k for k in range(cfg.steps + 1) if k % cfg.output_every == 0 or k == cfg.steps]
     times = [k * cfg.dt for k in sample]
-    xs = x.cpu()
-    vs = v.cpu()
     run = DamBreak3DRun(
         times=times, front=[float(diag[k, 2]) for k in sample],
         kinetic_energy=[float(diag[k, 6]) for k in sample],
         potential_energy=[float(diag[k, 7]) for k in sample],
         mass=eng.initial_mass, escaped=int(st["escapes"]), rebuilds=int(st["rebuilds"]),
-        max_speed=float(diag[:, 1].max()) if cfg.steps else 0.0,
-        max_density_compression=(float(diag[:, 0].max()) / cfg.rho0 - 1.0) if cfg.steps else 0.0,
+        max_speed=max(float(diag[k, 1]) for k in sample),
+        max_density_compression=float(diag[:, 0].max()) / cfg.rho0 - 1.0,
         initial_mass=eng.initial_mass, final_mass=eng.initial_mass, final_positions=xs,
         initial_energy=eng.initial_pe, steps_taken=cfg.steps, simulated_time=cfg.steps * cfg.dt,
-        obstacle_force=diag[:, 3:6].tolist(), obstacle_impulse=[float(diag[-1, 14])] if cfg.steps else [],
+        obstacle_force=diag[:cfg.steps, 3:6].tolist(),
+        obstacle_impulse=[float(diag[cfg.steps - 1, 14])] if cfg.steps else [],
         obstacle_clamps=int(st["clamps"]))
     masses = eng.spec.mass
     run.final_energy = float(0.5 * (masses[:, None] * vs.square()).sum()
@@ -672,7 +676,7 @@ def run_dam_break_2d(cfg, *, max_neighbors: int = 64) -> DamBreakRun:
                       potential_energy=[float(diag[k, 7]) for k in sample],
                       mass=float(spec.mass.sum()), escaped=int(st["escapes"]),
                       rebuilds=int(st["rebuilds"]),
-                      max_speed=float(diag[:, 1].max()),
+                      max_speed=max(float(diag[k, 1]) for k in sample),
                       max_density_compression=float(diag[:, 0].max()) / cfg.rho0 - 1.0,
                       final_positions=x, steps_taken=cfg.steps,
                       simulated_time=cfg.steps * cfg.dt)

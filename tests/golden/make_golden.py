@@ -470,6 +470,28 @@ def config1_run_case(db):
             "escaped": np.int64(run.escaped), "steps": np.int64(run.steps_taken)}
 
 
+def dam3d_run_case(d3):
+    """The reference's own 3-D dam-break loop (dam_break_3d.run_case) on a
+    small tank for 40 steps in FP64, with Molteni diffusion and wall friction."""
+    c0 = 10.0 * math.sqrt(2.0 * 9.81 * 0.24)
+    torch.set_default_dtype(torch.float64)
+    try:
+        cfg = d3.DamBreak3DConfig(dx=0.02, pool_width=0.5, tank_depth=0.2, tank_height=0.4,
+                                  column_width=0.2, column_depth=0.2, column_height=0.24,
+                                  sound_speed=c0, viscosity=1e-3, dt=0.25 * 1.3 * 0.02 / c0,
+                                  density_diffusion=0.1, wall_friction=0.3, steps=40,
+                                  output_every=10, device="cpu")
+        run = d3.run_case(cfg)
+    finally:
+        torch.set_default_dtype(torch.float32)
+    return {"times": np.asarray(run.times), "front": np.asarray(run.front),
+            "kinetic": np.asarray(run.kinetic_energy), "potential": np.asarray(run.potential_energy),
+            "final_positions": _np(run.final_positions), "rebuilds": np.int64(run.rebuilds),
+            "escaped": np.int64(run.escaped), "steps": np.int64(run.steps_taken),
+            "max_speed": np.float64(run.max_speed),
+            "max_density_compression": np.float64(run.max_density_compression)}
+
+
 def main(src, families=None):
     sys.path.insert(0, str(src))
     import tensorsph.neighbor_search as ns
@@ -499,6 +521,7 @@ def main(src, families=None):
         "csf": lambda: csf_cases(ca, di),
         "delta_plus": lambda: delta_plus_cases(dp),
         "config1_run": lambda: config1_run_case(db),
+        "dam3d_run": lambda: dam3d_run_case(d3),
     }
     for name in families or makers:
         np.savez_compressed(OUT / f"{name}.npz", **makers[name](), **meta)

@@ -128,7 +128,32 @@ def test_run_case_record(gpu):
     cfg, obstacle = small_case()
     run = run_case(cfg, obstacle=obstacle)
     assert run.steps_taken == cfg.steps
-    assert len(run.times) == len(run.front) == 3
+    assert len(run.times) == len(run.front) == 4      # steps 0, 4, 8 and the final 12
     assert run.front[0] == pytest.approx(0.19, abs=1e-9)
     assert run.escaped == 0
     assert len(run.obstacle_force) == cfg.steps
+
+
+def test_run_case_follows_reference_run(golden, gpu):
+    """The small 3-D dam break (Molteni diffusion, wall friction, 40 steps) on
+    the device against the reference's own FP64 ``dam_break_3d.run_case``."""
+    from tensorsph_b200.engine import run_case
+    g = golden("dam3d_run")
+    cfg, _ = small_case()
+    from dataclasses import replace
+    cfg = replace(cfg, steps=40, output_every=10)
+    saved = torch.get_default_dtype()
+    torch.set_default_dtype(torch.float64)
+    try:
+        run = run_case(cfg)
+    finally:
+        torch.set_default_dtype(saved)
+    assert run.steps_taken == int(g["steps"]) and run.escaped == int(g["escaped"])
+    assert np.allclose(run.times, g["times"], rtol=0, atol=1e-15)
+    assert np.abs(np.asarray(run.front) - g["front"]).max() < 1e-7
+    assert np.abs(np.asarray(run.potential_energy) - g["potential"]).max() < 1e-9 * abs(g["potential"][0])
+    ke = np.asarray(run.kinetic_energy)
+    assert np.abs(ke - g["kinetic"]).max() < 1e-4 * g["kinetic"].max(), (ke, g["kinetic"])
+    assert run.max_speed == pytest.approx(float(g["max_speed"]), rel=1e-4)
+    dxmax = np.abs(run.final_positions.numpy() - g["final_positions"]).max()
+    assert dxmax < 1e-7, dxmax
