@@ -243,18 +243,16 @@ template <int KB = kBatch, class Body>
 __device__ __forceinline__ void walk_row(const Dev& e, int64_t a, Body&& body) {
   const int n = e.cnt[a];
   const uint32_t* row = e.nbr + a;
-  int k = 0;
-  for (; k + KB <= n; k += KB) {
-    uint32_t ent[KB];
+  // the entries of the next batch are loaded while the current one is used
+  uint32_t cur[KB], nxt[KB];
 #pragma unroll
-    for (int j = 0; j < KB; ++j) ent[j] = row[static_cast<int64_t>(k + j) * e.rows];
-    body(ent);
-  }
-  if (k < n) {
-    uint32_t ent[KB];
+  for (int j = 0; j < KB; ++j) cur[j] = j < n ? row[static_cast<int64_t>(j) * e.rows] : kPad;
+  for (int k = 0; k < n; k += KB) {
 #pragma unroll
-    for (int j = 0; j < KB; ++j) ent[j] = (k + j < n) ? row[static_cast<int64_t>(k + j) * e.rows] : kPad;
-    body(ent);
+    for (int j = 0; j < KB; ++j) nxt[j] = (k + KB + j < n) ? row[static_cast<int64_t>(k + KB + j) * e.rows] : kPad;
+    body(cur);
+#pragma unroll
+    for (int j = 0; j < KB; ++j) cur[j] = nxt[j];
   }
 }
 
@@ -785,14 +783,18 @@ template <class Body>
 __device__ __forceinline__ void fluid_row(const Dev& e, int a, Body&& body) {
   const int n = e.cnt[a];
   const uint32_t* row = e.nbr + a;
+  uint32_t nxt[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) nxt[j] = j < n ? (row[static_cast<int64_t>(j) * e.rows] >> 5) : 0xffffffffu;
   for (int k = 0; k < n; k += 4) {
     int b[4];
     bool ok[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      const uint32_t v = (k + j < n) ? (row[static_cast<int64_t>(k + j) * e.rows] >> 5) : 0xffffffffu;
+      const uint32_t v = nxt[j];
       ok[j] = v < static_cast<uint32_t>(e.NF);
       b[j] = ok[j] ? static_cast<int>(v) : a;
+      nxt[j] = (k + 4 + j < n) ? (row[static_cast<int64_t>(k + 4 + j) * e.rows] >> 5) : 0xffffffffu;
     }
     body(b, ok);
   }
@@ -1094,11 +1096,17 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_fit(const __grid_constant__ D
       const double tx = -na.y, ty = na.x;
       double s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0, s6 = 0, s7 = 0;
       const int n4 = e.cnt4[a];
+      int nb4[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) nb4[j] = j < n4 ? static_cast<int>(e.nbr4[static_cast<int64_t>(j) * e.NF + a] >> 5) : a;
       for (int k = 0; k < n4; k += 4) {
         int b[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-          b[j] = k + j < n4 ? static_cast<int>(e.nbr4[static_cast<int64_t>(k + j) * e.NF + a] >> 5) : a;
+        for (int j = 0; j < 4; ++j) {
+          b[j] = nb4[j];
+          // prefetch the next batch's entries
+          nb4[j] = k + 4 + j < n4 ? static_cast<int>(e.nbr4[static_cast<int64_t>(k + 4 + j) * e.NF + a] >> 5) : a;
+        }
         double2 pb[4];
         double mg[4];
 #pragma unroll
