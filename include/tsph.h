@@ -368,6 +368,9 @@ typedef struct {
   double shift_strength, shift_limit, shift_free_surface, shift_vref_floor;
   double grid_lo[3], grid_hi[3];       /* bounds every particle stays in (cell grid) */
   double surface_tension;              /* CSF coefficient sigma (2-D cases); 0 = off  */
+  double periodic_box;                 /* > 0: triply periodic cube [0, L)^3 (3-D, no */
+                                       /* walls); L is snapped to n cells of an FP32 */
+                                       /* edge (relative change < 1e-7)              */
 } tsph_case_params;
 
 typedef struct tsph_engine tsph_engine; /* opaque host handle */

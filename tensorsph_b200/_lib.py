@@ -117,7 +117,8 @@ class CaseParams(ctypes.Structure):
                 ("ob_hi", c_double * 3), ("ob_eps", c_double), ("shift_strength", c_double),
                 ("shift_limit", c_double), ("shift_free_surface", c_double),
                 ("shift_vref_floor", c_double), ("grid_lo", c_double * 3),
-                ("grid_hi", c_double * 3), ("surface_tension", c_double)]
+                ("grid_hi", c_double * 3), ("surface_tension", c_double),
+                ("periodic_box", c_double)]
 
 
 _SIGNATURES = {

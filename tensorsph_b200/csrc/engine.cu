@@ -62,6 +62,8 @@ struct CaseDev {
   float cellf, inv_h, sigma, sig2d, rho0, bulk, gamma, inv_gamma;
   float grav, nu2, nu2f, dscale, dtf, visc_eps, rho_floor, wall_mass;
   int csf;                 // CSF surface tension on (2-D)
+  int periodic;            // triply periodic cube of edge pbox (3-D, no walls)
+  double pbox;             // the cube edge: n cells x the FP32 cell edge, exactly
   int stencil_cells;       // cells each side covering the 4h fit stencil
   double sigma_st, h_d, inv_h_d, sigma2d_d, vol_scale;  // CSF: sigma, h, 1/h, 10/(7 pi h^2), 1/rho0
   double stencil2;         // (4h)^2
@@ -382,14 +384,19 @@ __global__ void k_rows(Dev e) {
     const bool fluid_row = t < e.nf;
     const double rc2 = C.rc2;
     int count = 0;
+    const bool per = C.periodic != 0;
+    const double L = C.pbox;
     for (int dx = -1; dx <= 1; ++dx) {
-      const int x = cx + dx;
+      int x = cx + dx;
+      if (per) x = x < 0 ? x + C.ncx : (x >= C.ncx ? x - C.ncx : x);
       if (x < 0 || x >= C.ncx) continue;
       for (int dy = -1; dy <= 1; ++dy) {
-        const int y = cy + dy;
+        int y = cy + dy;
+        if (per) y = y < 0 ? y + C.ncy : (y >= C.ncy ? y - C.ncy : y);
         if (y < 0 || y >= C.ncy) continue;
         for (int dz = -1; dz <= 1; ++dz) {
-          const int z = cz + dz;
+          int z = cz + dz;
+          if (per) z = z < 0 ? z + C.ncz : (z >= C.ncz ? z - C.ncz : z);
           if (z < 0 || z >= C.ncz) continue;
           const int cell = C.key_off + (x * C.ncy + y) * C.ncz + z;
           const uint32_t code = static_cast<uint32_t>((dx + 1) * 9 + (dy + 1) * 3 + (dz + 1));
@@ -403,7 +410,12 @@ __global__ void k_rows(Dev e) {
 #pragma unroll
               for (int j = 0; j < 4; ++j) {
                 const int b = b0 + j;
-                const double ddx = pa.x - pb[j].x, ddy = pa.y - pb[j].y, ddz = pa.z - pb[j].z;
+                double ddx = pa.x - pb[j].x, ddy = pa.y - pb[j].y, ddz = pa.z - pb[j].z;
+                if (per) {
+                  ddx -= L * rint(ddx / L);
+                  ddy -= L * rint(ddy / L);
+                  ddz -= L * rint(ddz / L);
+                }
                 if (b < fe && b != a && ddx * ddx + ddy * ddy + ddz * ddz <= rc2) {
                   if (count < e.maxnb)
                     e.nbr[static_cast<int64_t>(count) * e.rows + a] = (static_cast<uint32_t>(b) << 5) | code;
@@ -1217,16 +1229,27 @@ __global__ void __launch_bounds__(kMaxBlock) k_integrate(const __grid_constant__
     double vx = v0.x + dt * static_cast<double>(ac.x), vy = v0.y + dt * static_cast<double>(ac.y),
            vz = v0.z + dt * static_cast<double>(ac.z);
     double px = x0.x + dt * vx, py = x0.y + dt * vy, pz = x0.z + dt * vz;
-    const bool ox = px < -C.tol || px > C.box_hi[0] + C.tol;
-    const bool oy = py < -C.tol || py > C.box_hi[1] + C.tol;
-    const bool oz = pz < -C.tol || pz > C.box_hi[2] + C.tol;
-    px = px < 0.0 ? 0.0 : (px > C.box_hi[0] ? C.box_hi[0] : px);
-    py = py < 0.0 ? 0.0 : (py > C.box_hi[1] ? C.box_hi[1] : py);
-    pz = pz < 0.0 ? 0.0 : (pz > C.box_hi[2] ? C.box_hi[2] : pz);
-    vx = ox ? 0.0 : vx;
-    vy = oy ? 0.0 : vy;
-    vz = oz ? 0.0 : vz;
-    if (ox || oy || oz) atomicAdd(&e.ctl[c].escapes, 1ull);
+    if (C.periodic) {
+      // remainder into [0, L)
+      const double L = C.pbox;
+      px -= L * floor(px / L);
+      py -= L * floor(py / L);
+      pz -= L * floor(pz / L);
+      px = px >= L ? px - L : px;
+      py = py >= L ? py - L : py;
+      pz = pz >= L ? pz - L : pz;
+    } else {
+      const bool ox = px < -C.tol || px > C.box_hi[0] + C.tol;
+      const bool oy = py < -C.tol || py > C.box_hi[1] + C.tol;
+      const bool oz = pz < -C.tol || pz > C.box_hi[2] + C.tol;
+      px = px < 0.0 ? 0.0 : (px > C.box_hi[0] ? C.box_hi[0] : px);
+      py = py < 0.0 ? 0.0 : (py > C.box_hi[1] ? C.box_hi[1] : py);
+      pz = pz < 0.0 ? 0.0 : (pz > C.box_hi[2] ? C.box_hi[2] : pz);
+      vx = ox ? 0.0 : vx;
+      vy = oy ? 0.0 : vy;
+      vz = oz ? 0.0 : vz;
+      if (ox || oy || oz) atomicAdd(&e.ctl[c].escapes, 1ull);
+    }
     if (C.has_ob && px > C.ob_lo[0] && px < C.ob_hi[0] && py > C.ob_lo[1] && py < C.ob_hi[1] &&
         pz > C.ob_lo[2] && pz < C.ob_hi[2]) {
       // exit through the nearest face (first minimum, as argmin)
@@ -1264,7 +1287,13 @@ __global__ void __launch_bounds__(kMaxBlock) k_integrate(const __grid_constant__
     st4(e.vel, a, make_double4(v[0], v[1], v[2], 0.0));
     e.lp[a] = local_of(C, e.home[a] - C.key_off, x[0], x[1], x[2], m);
     const double4 an = ld4(e.anchor, a);
-    const double ex = x[0] - an.x, ey = x[1] - an.y, ez = x[2] - an.z;
+    double ex = x[0] - an.x, ey = x[1] - an.y, ez = x[2] - an.z;
+    if (C.periodic) {
+      const double L = C.pbox;
+      ex -= L * rint(ex / L);
+      ey -= L * rint(ey / L);
+      ez -= L * rint(ez / L);
+    }
     dmax = sqrt(ex * ex + ey * ey + ez * ez);
   }
   if (uniform) {
@@ -1821,19 +1850,34 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr) {
 
 CaseDev make_case_dev(const tsph_case_params& p, int64_t* ncells) {
   CaseDev c{};
-  const double cell = 2.0 * p.h + p.skin;
-  c.cell = cell;
-  c.cellf = static_cast<float>(cell);
-  for (int k = 0; k < 3; ++k) c.origin[k] = p.grid_lo[k];
-  const int64_t nx = static_cast<int64_t>(std::ceil((p.grid_hi[0] - p.grid_lo[0]) / cell)) + 1;
-  const int64_t ny = static_cast<int64_t>(std::ceil((p.grid_hi[1] - p.grid_lo[1]) / cell)) + 1;
-  const int64_t nz = p.dim == 3 ? static_cast<int64_t>(std::ceil((p.grid_hi[2] - p.grid_lo[2]) / cell)) + 1 : 1;
-  if (p.dim == 2) c.origin[2] = -0.5 * cell;
+  double cell = 2.0 * p.h + p.skin;
+  int64_t nx, ny, nz;
+  if (p.periodic_box > 0.0) {
+    // n cells of edge L/n >= the list cutoff per axis; the edge is rounded to
+    // FP32 and the box snapped to n times it, so that a separation across
+    // the wrap, (l_a - l_b) - u * cell, is as exact as any other
+    const int64_t n = std::max<int64_t>(3, static_cast<int64_t>(std::floor(p.periodic_box / (cell * (1.0 + 1e-6)))));
+    c.cellf = static_cast<float>(p.periodic_box / static_cast<double>(n));
+    cell = static_cast<double>(c.cellf);
+    c.periodic = 1;
+    c.pbox = static_cast<double>(n) * cell;
+    for (int k = 0; k < 3; ++k) c.origin[k] = 0.0;
+    nx = ny = nz = n;
+    c.cell = cell;
+  } else {
+    c.cell = cell;
+    c.cellf = static_cast<float>(cell);
+    for (int k = 0; k < 3; ++k) c.origin[k] = p.grid_lo[k];
+    nx = static_cast<int64_t>(std::ceil((p.grid_hi[0] - p.grid_lo[0]) / cell)) + 1;
+    ny = static_cast<int64_t>(std::ceil((p.grid_hi[1] - p.grid_lo[1]) / cell)) + 1;
+    nz = p.dim == 3 ? static_cast<int64_t>(std::ceil((p.grid_hi[2] - p.grid_lo[2]) / cell)) + 1 : 1;
+    if (p.dim == 2) c.origin[2] = -0.5 * cell;
+  }
   *ncells = nx * ny * nz;
   c.ncx = static_cast<int>(nx);
   c.ncy = static_cast<int>(ny);
   c.ncz = static_cast<int>(nz);
-  c.rc2 = cell * cell;
+  c.rc2 = (2.0 * p.h + p.skin) * (2.0 * p.h + p.skin);
   c.skin_half = 0.5 * p.skin;
   c.dt = p.dt;
   c.gravity = p.gravity;
@@ -1887,6 +1931,9 @@ bool case_params_ok(const tsph_case_params* p) {
   for (int k = 0; k < p->dim; ++k)
     if (!(p->grid_hi[k] >= p->grid_lo[k]) || !std::isfinite(p->grid_lo[k]) || !std::isfinite(p->grid_hi[k]))
       return false;
+  if (p->periodic_box < 0.0 || (p->periodic_box > 0.0 && (p->dim != 3 || p->n_wall != 0 || p->shift_every != 0 ||
+                                                          !std::isfinite(p->periodic_box))))
+    return false;
   return true;
 }
 

@@ -31,7 +31,7 @@ from . import _lib
 from .dam_break_3d import DamBreak3DConfig, make_column_3d, mass_3d, wall_lattice_3d
 
 __all__ = ["BatchEngine", "CaseSpec", "DamBreak3DEngine", "DamBreak3DRun", "dam_break_2d_case",
-           "dam_break_3d_case", "droplet_impact_case", "engine_bytes", "obstacle_case", "obstacle_lattice_3d",
+           "dam_break_3d_case", "droplet_impact_case", "engine_bytes", "shear_decay_case", "obstacle_case", "obstacle_lattice_3d",
            "run_case", "run_dam_break_2d", "tune_single_case", "DIAG_FIELDS"]
 
 MAX_ROWS = (1 << 27) - 1   # fluid + wall rows of one engine (27-bit row index)
@@ -272,6 +272,43 @@ def droplet_impact_case(cfg, *, drop_speed: float = 0.0, label: str = "") -> Cas
                      lo=allpos.min(dim=0).values.tolist(), hi=allpos.max(dim=0).values.tolist())
     p.surface_tension = float(cfg.surface_tension_coefficient)
     return CaseSpec(p, x, v, mass.double().contiguous(), wall, label or "droplet_impact")
+
+
+def shear_decay_case(n: int, *, box: float = 1.0, amplitude: float = 1.0e-3, nu: float = 1.0e-2,
+                     sound_speed: float = 1.0, rho0: float = 1000.0, gamma: float = 7.0,
+                     h_factor: float = 1.3, jitter: float = 0.01, seed: int = 0,
+                     skin_factor: float = 0.25, courant: float = 0.25, label: str = "") -> CaseSpec:
+    """A triply periodic shear decay u_x = A sin(2 pi z / L) on an n^3 lattice
+    with a seeded uniform jitter of +-jitter dx, as a ``CaseSpec`` of the batch
+    engine (its WCSPH operators: Tait, Morris viscous Laplacian; no gravity, no
+    walls).  dt is the smaller of acoustic CFL ``courant`` and 0.9 x the
+    viscous limit 0.125 h^2 / nu."""
+    dx = box / n
+    h = h_factor * dx
+    dt = min(courant * h / sound_speed, 0.9 * 0.125 * h * h / nu)
+    g = torch.Generator().manual_seed(seed)
+    ax = torch.arange(n, dtype=torch.float64) * dx
+    gx, gy, gz = torch.meshgrid(ax, ax, ax, indexing="ij")
+    x = torch.stack((gx.reshape(-1), gy.reshape(-1), gz.reshape(-1)), -1)
+    x = (x + jitter * dx * (2.0 * torch.rand(x.shape, generator=g, dtype=torch.float64) - 1.0)
+         ).remainder(box).contiguous()
+    k = 2.0 * math.pi / box
+    v = torch.zeros_like(x)
+    v[:, 0] = amplitude * torch.sin(k * x[:, 2])
+    from .dam_break_3d import mass_3d as _mass3d
+    m = torch.full((x.shape[0],), _mass3d(dx, h_factor, rho0, True), dtype=torch.float64)
+    p = _lib.CaseParams()
+    p.dim, p.n_fluid, p.n_wall, p.n_obstacle = 3, x.shape[0], 0, 0
+    p.h, p.rho0, p.sound_speed, p.gamma = h, rho0, sound_speed, gamma
+    p.gravity, p.viscosity, p.wall_friction, p.diffusion_scale = 0.0, nu, 0.0, 0.0
+    p.dt, p.wall_mass, p.skin = dt, 0.0, skin_factor * h
+    for kk in range(3):
+        p.box_hi[kk] = box
+        p.grid_lo[kk], p.grid_hi[kk] = 0.0, box
+    p.tolerance = 0.25 * dx
+    p.shift_vref_floor = 0.05 * sound_speed
+    p.periodic_box = box
+    return CaseSpec(p, x, v, m, torch.zeros((0, 3), dtype=torch.float64), label or "shear_decay_3d")
 
 
 # ------------------------------------------------------------------ engine --

@@ -17,8 +17,9 @@ stream one request at a time in arrival order with the single-case engine.
 
 Case types: ``dam_break_2d`` (1 : 2 column in a 4 x 1.5 tank, dam_break.py),
 ``column_3d`` (hydrostatic 3-D column filling a square tank,
-dam_break_3d.py), each sized by its particle count, c0 = 10 sqrt(2 g H),
-acoustic CFL 0.25.
+dam_break_3d.py), both with c0 = 10 sqrt(2 g H) and acoustic CFL 0.25, and
+``shear_3d`` (triply periodic shear decay u_x = 1e-3 sin(2 pi z) in a unit
+cube, nu = 1e-2, c0 = 1); each sized by its particle count.
 """
 from __future__ import annotations
 
@@ -33,7 +34,7 @@ from .engine import MAX_ROWS, BatchEngine, CaseSpec, dam_break_2d_case, dam_brea
 __all__ = ["Request", "request_stream", "request_spec", "Server", "capacities_for_budget",
            "run_serial", "percentiles"]
 
-CASE_TYPES = ("dam_break_2d", "column_3d")
+CASE_TYPES = ("dam_break_2d", "column_3d", "shear_3d")
 
 
 @dataclass
@@ -97,6 +98,10 @@ def request_spec(req: Request) -> CaseSpec:
                                sound_speed=c0, viscosity=1e-6, dt=0.25 * h / c0,
                                max_courant=0.25)
         spec = dam_break_3d_case(cfg, label=f"r{req.rid}:{req.kind}")
+    elif req.kind == "shear_3d":
+        from .engine import shear_decay_case
+        n = max(8, int(round(req.particles ** (1.0 / 3.0))))
+        spec = shear_decay_case(n, seed=req.rid, label=f"r{req.rid}:{req.kind}")
     else:
         raise ValueError(f"unknown case type {req.kind!r}")
     req.spec = spec
