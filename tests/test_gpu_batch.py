@@ -274,14 +274,17 @@ def _shear_rate(n, steps_per_block=20, blocks=6, with_other=None):
 
 def test_periodic_shear_case_decays_and_batches(gpu):
     """A triply periodic shear decay in the batch engine: the decay rate
-    approaches nu k^2 as the lattice refines (the Morris Laplacian's error is
-    O((kh)^2): about 6 % at n = 20, kh = 0.41), momentum is conserved, and the
-    case is bitwise the same alone and next to a dam break."""
+    approaches nu k^2 as the lattice refines, momentum is conserved, and the
+    case is bitwise the same alone and next to a dam break.
+
+    On the jittered lattice the rate error falls about linearly in h (6.0 %
+    at n = 20, 3.6 % at n = 32, ratio 0.61 against 20/32 = 0.625), so the
+    test asks for at least first-order convergence with 12 % slack."""
     nuk2 = 1e-2 * (2 * math.pi) ** 2
     spec, rate20, moms, scale, got = _shear_rate(20, with_other=dam_break_2d_case_small())
     _, rate32, _, _, _ = _shear_rate(32, steps_per_block=30)
     err20, err32 = abs(rate20 - nuk2) / nuk2, abs(rate32 - nuk2) / nuk2
-    assert err20 < 0.10 and err32 < 0.6 * err20, (rate20, rate32, nuk2)
+    assert err20 < 0.10 and err32 < 0.7 * err20, (rate20, rate32, nuk2)
     assert np.abs(moms[-1] - moms[0]).max() < 1e-10 * scale
     ref, _ = _alone(spec, 120, max_neighbors=160, diag_ring=8)
     for u, w in zip(got, ref):
