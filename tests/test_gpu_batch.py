@@ -279,14 +279,20 @@ def test_periodic_shear_case_decays_and_batches(gpu):
 
     On the jittered lattice the rate error falls about linearly in h (6.0 %
     at n = 20, 3.6 % at n = 32, ratio 0.61 against 20/32 = 0.625), so the
-    test asks for at least first-order convergence with 12 % slack."""
+    test asks for at least first-order convergence with 12 % slack.
+
+    Momentum: the pressure force is antisymmetric per pair, but the Morris
+    viscous term weights each pair by the neighbour's volume V_b = m_b / rho_b
+    (the reference's form), so with the density varying by ~1e-3 over the
+    jittered lattice the viscous impulse leaks at that fraction (measured
+    4.6e-4 of sum m|v| over 100 steps); the bound is 2e-3."""
     nuk2 = 1e-2 * (2 * math.pi) ** 2
     spec, rate20, moms, scale, got = _shear_rate(20, with_other=dam_break_2d_case_small())
     _, rate32, _, _, _ = _shear_rate(32, steps_per_block=30)
     err20, err32 = abs(rate20 - nuk2) / nuk2, abs(rate32 - nuk2) / nuk2
     assert err20 < 0.10 and err32 < 0.7 * err20, (rate20, rate32, nuk2)
-    assert np.abs(moms[-1] - moms[0]).max() < 1e-10 * scale
-    ref, _ = _alone(spec, 120, max_neighbors=160, diag_ring=8)
+    assert np.abs(moms[-1] - moms[0]).max() < 2e-3 * scale
+    ref, _ = _alone(spec, 120, max_neighbors=160, diag_ring=128)
     for u, w in zip(got, ref):
         assert torch.equal(u, w)
     assert float(got[0].min()) >= 0.0 and float(got[0].max()) < 1.0 + 1e-6
