@@ -238,6 +238,19 @@ __device__ __forceinline__ float tait(float rho, float rho0, float bulk, float g
   return p > 0.f ? p : 0.f;
 }
 
+// A row entry: read once per pass, so it is not allocated in L1, which then
+// keeps the neighbour records the gathers reuse (measured 2 % on the 3-D
+// dam break step).
+__device__ __forceinline__ uint32_t ld_entry(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.global.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+
+// 1/x for the regularised pair denominators r^2 + eps (x >= eps > 0): the
+// hardware reciprocal, within 2 ulp.
+__device__ __forceinline__ float rcp_pair(float x) { return __fdividef(1.f, x); }
+
 // Walk row a in batches of KB entries (padded with kPad); the loads of a
 // batch are all issued before any use.  KB (the batch depth: neighbour
 // records in flight per thread) is a tuning parameter of the hot kernels.
@@ -248,10 +261,11 @@ __device__ __forceinline__ void walk_row(const Dev& e, int64_t a, Body&& body) {
   // the entries of the next batch are loaded while the current one is used
   uint32_t cur[KB], nxt[KB];
 #pragma unroll
-  for (int j = 0; j < KB; ++j) cur[j] = j < n ? row[static_cast<int64_t>(j) * e.rows] : kPad;
+  for (int j = 0; j < KB; ++j) cur[j] = j < n ? ld_entry(row + static_cast<int64_t>(j) * e.rows) : kPad;
   for (int k = 0; k < n; k += KB) {
 #pragma unroll
-    for (int j = 0; j < KB; ++j) nxt[j] = (k + KB + j < n) ? row[static_cast<int64_t>(k + KB + j) * e.rows] : kPad;
+    for (int j = 0; j < KB; ++j)
+      nxt[j] = (k + KB + j < n) ? ld_entry(row + static_cast<int64_t>(k + KB + j) * e.rows) : kPad;
     body(cur);
 #pragma unroll
     for (int j = 0; j < KB; ++j) cur[j] = nxt[j];
@@ -570,7 +584,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_diffusion_eos(const __grid_consta
           const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
           const Radial R = radial(r2, inv_h);
           const float gs = sigma * dshape(R.q) * inv_h * R.inv_r;
-          const float coupling = (ra.x - rb.x) * (-gs * r2) * __frcp_rn(r2 + 1e-12f);
+          const float coupling = (ra.x - rb.x) * (-gs * r2) * rcp_pair(r2 + 1e-12f);
           part += ok ? (-dscale * rb.y) * coupling : 0.f;
         }
         rate.add(part);
@@ -657,7 +671,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(const __grid_constant__ Dev
         gs = ok ? gs : 0.f;
         const float fp = -lb.w * (Pa + Pb) * gs;
         const float vs = b < NF ? nu2 : nu2f;
-        const float lw = fmaxf(-gs * r2, 0.f) * __frcp_rn(r2 + eta2);
+        const float lw = fmaxf(-gs * r2, 0.f) * rcp_pair(r2 + eta2);
         const float coef = -vs * (vb.w * lw);
         px += fp * d.x + coef * (va.x - vb.x);
         py += fp * d.y + coef * (va.y - vb.y);
@@ -720,7 +734,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_reaction(Dev e) {
         float x = cc * d.x, y = cc * d.y, z = cc * d.z;
         if (nu2f != 0.f) {
           const float4 vf = e.vb[fi];
-          const float lwt = fmaxf(-gs * r2, 0.f) * __frcp_rn(r2 + eta2);
+          const float lwt = fmaxf(-gs * r2, 0.f) * rcp_pair(r2 + eta2);
           const float coef = mf * nu2f * (Vw * lwt);
           x += coef * vf.x;
           y += coef * vf.y;
@@ -797,7 +811,7 @@ __device__ __forceinline__ void fluid_row(const Dev& e, int a, Body&& body) {
   const uint32_t* row = e.nbr + a;
   uint32_t nxt[4];
 #pragma unroll
-  for (int j = 0; j < 4; ++j) nxt[j] = j < n ? (row[static_cast<int64_t>(j) * e.rows] >> 5) : 0xffffffffu;
+  for (int j = 0; j < 4; ++j) nxt[j] = j < n ? (ld_entry(row + static_cast<int64_t>(j) * e.rows) >> 5) : 0xffffffffu;
   for (int k = 0; k < n; k += 4) {
     int b[4];
     bool ok[4];
@@ -806,7 +820,7 @@ __device__ __forceinline__ void fluid_row(const Dev& e, int a, Body&& body) {
       const uint32_t v = nxt[j];
       ok[j] = v < static_cast<uint32_t>(e.NF);
       b[j] = ok[j] ? static_cast<int>(v) : a;
-      nxt[j] = (k + 4 + j < n) ? (row[static_cast<int64_t>(k + 4 + j) * e.rows] >> 5) : 0xffffffffu;
+      nxt[j] = (k + 4 + j < n) ? (ld_entry(row + static_cast<int64_t>(k + 4 + j) * e.rows) >> 5) : 0xffffffffu;
     }
     body(b, ok);
   }
