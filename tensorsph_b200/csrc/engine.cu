@@ -20,7 +20,7 @@
 //                 of the two local coordinates
 //   vb   float4   FP32 velocity + volume m/rho;  pr, rho, pq = p/rho^2
 //   nbr  uint32[maxnb][rows] k-major rows (thread a reads nbr[k*rows + a]),
-//        entry = row index << 5 | cell-offset code (dx+1)*9 + (dy+1)*3 + (dz+1)
+//        entry = row index << 6 | cell offset (dx+1) | (dy+1) << 2 | (dz+1) << 4
 // Each case rebuilds its rows only when its own particles leave its own skin
 // and the order of its block depends on its own particles only, so a case
 // evolves bit for bit the same alone or batched with others.  Retiring a case
@@ -49,7 +49,10 @@ constexpr int kMaxBlock = 256;  // largest block the kernels are built for
 constexpr int kDiag = 16;
 constexpr int kBatch = 4;
 constexpr uint32_t kPad = 0xffffffffu;
-constexpr int64_t kMaxRows = (int64_t(1) << 27) - 1;  // row index in 27 bits
+constexpr int kCodeBits = 6;                               // cell-offset code bits of a row entry
+constexpr uint32_t kCodeMask = (1u << kCodeBits) - 1;
+constexpr uint32_t kSelfCode = 0x15u;                      // offset (0, 0, 0): fields (1, 1, 1)
+constexpr int64_t kMaxRows = (int64_t(1) << 26) - 1;      // row index in the other 26 bits
 
 struct CaseDev {
   double origin[3];
@@ -212,19 +215,26 @@ __device__ __forceinline__ float4 local_of(const CaseDev& c, int local_key, doub
                      static_cast<float>(z - (c.origin[2] + cz * cs)), static_cast<float>(m));
 }
 
-// Unit cell offsets (c_b - c_a) per entry code, in shared memory; the
-// separation is (l_a - l_b) - u * cell with u * cell exact, so one FMA per
-// axis gives the same bits as a subtraction of a precomputed offset.
-__device__ __forceinline__ void fill_units(float4* tab) {
-  for (int c = threadIdx.x; c < 27; c += blockDim.x)
-    tab[c] = make_float4(static_cast<float>(c / 9 - 1), static_cast<float>((c / 3) % 3 - 1),
-                         static_cast<float>(c % 3 - 1), 0.f);
-  __syncthreads();
+// Cell offset c_b - c_a of a row entry, 2 bits per axis (dx + 1 at bit 0,
+// dy + 1 at bit 2, dz + 1 at bit 4).  unit<S> places a field f in {0, 1, 2}
+// in the top two mantissa bits (21, 22) of 1.0f, giving 1 + f/4 in
+// {1, 1.25, 1.5}, then 4 v - 5 in {-1, 0, 1}, all exact: no table lookup per
+// neighbour.
+template <int kShift>
+__device__ __forceinline__ float unit(uint32_t ent) {
+  const uint32_t bits = ((ent << (21 - kShift)) & (3u << 21)) | 0x3f800000u;
+  return fmaf(4.f, __uint_as_float(bits), -5.f);
 }
 
-__device__ __forceinline__ float3 sep(const float4& la, const float4& lb, const float4& u, float cellf) {
-  return make_float3(fmaf(-u.x, cellf, la.x - lb.x), fmaf(-u.y, cellf, la.y - lb.y),
-                     fmaf(-u.z, cellf, la.z - lb.z));
+__host__ __device__ constexpr uint32_t entry_code(int dx, int dy, int dz) {
+  return static_cast<uint32_t>((dx + 1) | ((dy + 1) << 2) | ((dz + 1) << 4));
+}
+
+// The separation is (l_a - l_b) - u * cell with u * cell exact, so one FMA per
+// axis gives the same bits as a subtraction of a precomputed offset.
+__device__ __forceinline__ float3 sep(const float4& la, const float4& lb, uint32_t ent, float cellf) {
+  return make_float3(fmaf(-unit<0>(ent), cellf, la.x - lb.x), fmaf(-unit<2>(ent), cellf, la.y - lb.y),
+                     fmaf(-unit<4>(ent), cellf, la.z - lb.z));
 }
 
 __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* p, double v) {
@@ -413,7 +423,7 @@ __global__ void k_rows(Dev e) {
           if (per) z = z < 0 ? z + C.ncz : (z >= C.ncz ? z - C.ncz : z);
           if (z < 0 || z >= C.ncz) continue;
           const int cell = C.key_off + (x * C.ncy + y) * C.ncz + z;
-          const uint32_t code = static_cast<uint32_t>((dx + 1) * 9 + (dy + 1) * 3 + (dz + 1));
+          const uint32_t code = entry_code(dx, dy, dz);
           const int fs = e.fstart[cell];
           if (fs >= 0) {
             const int fe = e.fend[cell];
@@ -432,7 +442,7 @@ __global__ void k_rows(Dev e) {
                 }
                 if (b < fe && b != a && ddx * ddx + ddy * ddy + ddz * ddz <= rc2) {
                   if (count < e.maxnb)
-                    e.nbr[static_cast<int64_t>(count) * e.rows + a] = (static_cast<uint32_t>(b) << 5) | code;
+                    e.nbr[static_cast<int64_t>(count) * e.rows + a] = (static_cast<uint32_t>(b) << kCodeBits) | code;
                   ++count;
                 }
               }
@@ -452,7 +462,7 @@ __global__ void k_rows(Dev e) {
                   const double ddx = pa.x - pb[j].x, ddy = pa.y - pb[j].y, ddz = pa.z - pb[j].z;
                   if (w0 + j < we && ddx * ddx + ddy * ddy + ddz * ddz <= rc2) {
                     if (count < e.maxnb)
-                      e.nbr[static_cast<int64_t>(count) * e.rows + a] = (static_cast<uint32_t>(b) << 5) | code;
+                      e.nbr[static_cast<int64_t>(count) * e.rows + a] = (static_cast<uint32_t>(b) << kCodeBits) | code;
                     ++count;
                   }
                 }
@@ -491,7 +501,7 @@ __global__ void k_rows(Dev e) {
               const int b = b0 + j;
               const double ddx = pa.x - pb[j].x, ddy = pa.y - pb[j].y;
               if (b < fe && b != a && ddx * ddx + ddy * ddy <= C.fit_rc2) {
-                if (c4 < e.maxfit) e.nbr4[static_cast<int64_t>(c4) * e.NF + a] = static_cast<uint32_t>(b) << 5;
+                if (c4 < e.maxfit) e.nbr4[static_cast<int64_t>(c4) * e.NF + a] = static_cast<uint32_t>(b) << kCodeBits;
                 ++c4;
               }
             }
@@ -529,8 +539,6 @@ __global__ void k_step_begin(Dev e) {
 
 template <bool kOne, int KB>
 __global__ void __launch_bounds__(kMaxBlock) k_density(const __grid_constant__ Dev e) {
-  __shared__ float4 tab[27];
-  fill_units(tab);
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
     const CaseDev& C = case_of<kOne>(e, a);
     const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, floor_ = C.rho_floor;
@@ -542,9 +550,9 @@ __global__ void __launch_bounds__(kMaxBlock) k_density(const __grid_constant__ D
 #pragma unroll
       for (int j = 0; j < KB; ++j) {
         const bool ok = ent[j] != kPad;
-        const int b = ok ? static_cast<int>(ent[j] >> 5) : a;
+        const int b = ok ? static_cast<int>(ent[j] >> kCodeBits) : a;
         const float4 lb = e.lp[b];
-        const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u], cellf);
+        const float3 d = sep(la, lb, ok ? ent[j] : kSelfCode, cellf);
         const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
         const float W = sigma * shape(radial(r2, inv_h).q);
         part += ok ? lb.w * W : 0.f;
@@ -559,8 +567,6 @@ __global__ void __launch_bounds__(kMaxBlock) k_density(const __grid_constant__ D
 
 template <bool kOne, int KB>
 __global__ void __launch_bounds__(kMaxBlock) k_diffusion_eos(const __grid_constant__ Dev e) {
-  __shared__ float4 tab[27];
-  fill_units(tab);
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
     const CaseDev& C = case_of<kOne>(e, a);
     const float2 ra = e.rs[a];
@@ -575,12 +581,12 @@ __global__ void __launch_bounds__(kMaxBlock) k_diffusion_eos(const __grid_consta
         float part = 0.f;
 #pragma unroll
         for (int j = 0; j < KB; ++j) {
-          const int b0 = ent[j] != kPad ? static_cast<int>(ent[j] >> 5) : a;
+          const int b0 = ent[j] != kPad ? static_cast<int>(ent[j] >> kCodeBits) : a;
           const bool ok = ent[j] != kPad && b0 < NF;
           const int b = ok ? b0 : a;
           const float4 lb = e.lp[b];
           const float2 rb = e.rs[b];
-          const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u], cellf);
+          const float3 d = sep(la, lb, ok ? ent[j] : kSelfCode, cellf);
           const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
           const Radial R = radial(r2, inv_h);
           const float gs = sigma * dshape(R.q) * inv_h * R.inv_r;
@@ -603,8 +609,6 @@ __global__ void __launch_bounds__(kMaxBlock) k_diffusion_eos(const __grid_consta
 
 template <bool kOne, int KB>
 __global__ void __launch_bounds__(kMaxBlock) k_walls(const __grid_constant__ Dev e) {
-  __shared__ float4 tab[27];
-  fill_units(tab);
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < e.nw; t += gridDim.x * blockDim.x) {
     const int64_t a = e.NF + t;
     const CaseDev& C = case_of<kOne>(e, a);
@@ -617,9 +621,9 @@ __global__ void __launch_bounds__(kMaxBlock) k_walls(const __grid_constant__ Dev
 #pragma unroll
       for (int j = 0; j < KB; ++j) {
         const bool ok = ent[j] != kPad;
-        const int f = ok ? static_cast<int>(ent[j] >> 5) : f0;
+        const int f = ok ? static_cast<int>(ent[j] >> kCodeBits) : f0;
         const float4 lf = e.lp[f];
-        const float3 d = sep(la, lf, tab[ok ? (ent[j] & 31u) : 13u], cellf);  // r_w - r_f
+        const float3 d = sep(la, lf, ok ? ent[j] : kSelfCode, cellf);  // r_w - r_f
         const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
         const float W = ok ? sigma * shape(radial(r2, inv_h).q) : 0.f;
         float src = e.pr[f];
@@ -644,8 +648,6 @@ __global__ void __launch_bounds__(kMaxBlock) k_walls(const __grid_constant__ Dev
 
 template <bool kOne, int KB>
 __global__ void __launch_bounds__(kMaxBlock) k_force(const __grid_constant__ Dev e) {
-  __shared__ float4 tab[27];
-  fill_units(tab);
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
     const CaseDev& C = case_of<kOne>(e, a);
     const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, nu2 = C.nu2, nu2f = C.nu2f,
@@ -660,11 +662,11 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(const __grid_constant__ Dev
 #pragma unroll
       for (int j = 0; j < KB; ++j) {
         const bool ok = ent[j] != kPad;
-        const int b = ok ? static_cast<int>(ent[j] >> 5) : a;
+        const int b = ok ? static_cast<int>(ent[j] >> kCodeBits) : a;
         const float4 lb = e.lp[b];
         const float4 vb = e.vb[b];
         const float Pb = e.pq[b];
-        const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u], cellf);
+        const float3 d = sep(la, lb, ok ? ent[j] : kSelfCode, cellf);
         const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
         const Radial R = radial(r2, inv_h);
         float gs = sigma * dshape(R.q) * inv_h * R.inv_r;
@@ -695,9 +697,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(const __grid_constant__ Dev
 // dam_break_3d.py:412-421), summed per case in FP64.  Obstacle rows are grouped
 // by case, so a block whose rows all belong to one case adds one total.
 __global__ void __launch_bounds__(kMaxBlock) k_reaction(Dev e) {
-  __shared__ float4 tab[27];
   __shared__ double red[kMaxBlock / 32];
-  fill_units(tab);
   const int q0 = blockIdx.x * blockDim.x;
   if (q0 >= e.n_ob) return;
   const int q = q0 + threadIdx.x;
@@ -722,9 +722,9 @@ __global__ void __launch_bounds__(kMaxBlock) k_reaction(Dev e) {
 #pragma unroll
       for (int j = 0; j < kBatch; ++j) {
         const bool ok = ent[j] != kPad;
-        const int fi = ok ? static_cast<int>(ent[j] >> 5) : f0;
+        const int fi = ok ? static_cast<int>(ent[j] >> kCodeBits) : f0;
         const float4 lf = e.lp[fi];
-        const float3 d = sep(lw_, lf, tab[ok ? (ent[j] & 31u) : 13u], cellf);
+        const float3 d = sep(lw_, lf, ok ? ent[j] : kSelfCode, cellf);
         const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
         const Radial R = radial(r2, inv_h);
         float gs = sigma * dshape(R.q) * inv_h * R.inv_r;
@@ -811,7 +811,7 @@ __device__ __forceinline__ void fluid_row(const Dev& e, int a, Body&& body) {
   const uint32_t* row = e.nbr + a;
   uint32_t nxt[4];
 #pragma unroll
-  for (int j = 0; j < 4; ++j) nxt[j] = j < n ? (ld_entry(row + static_cast<int64_t>(j) * e.rows) >> 5) : 0xffffffffu;
+  for (int j = 0; j < 4; ++j) nxt[j] = j < n ? (ld_entry(row + static_cast<int64_t>(j) * e.rows) >> kCodeBits) : 0xffffffffu;
   for (int k = 0; k < n; k += 4) {
     int b[4];
     bool ok[4];
@@ -820,7 +820,7 @@ __device__ __forceinline__ void fluid_row(const Dev& e, int a, Body&& body) {
       const uint32_t v = nxt[j];
       ok[j] = v < static_cast<uint32_t>(e.NF);
       b[j] = ok[j] ? static_cast<int>(v) : a;
-      nxt[j] = (k + 4 + j < n) ? (ld_entry(row + static_cast<int64_t>(k + 4 + j) * e.rows) >> 5) : 0xffffffffu;
+      nxt[j] = (k + 4 + j < n) ? (ld_entry(row + static_cast<int64_t>(k + 4 + j) * e.rows) >> kCodeBits) : 0xffffffffu;
     }
     body(b, ok);
   }
@@ -1124,14 +1124,14 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_fit(const __grid_constant__ D
       const int n4 = e.cnt4[a];
       int nb4[4];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) nb4[j] = j < n4 ? static_cast<int>(e.nbr4[static_cast<int64_t>(j) * e.NF + a] >> 5) : a;
+      for (int j = 0; j < 4; ++j) nb4[j] = j < n4 ? static_cast<int>(e.nbr4[static_cast<int64_t>(j) * e.NF + a] >> kCodeBits) : a;
       for (int k = 0; k < n4; k += 4) {
         int b[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
           b[j] = nb4[j];
           // prefetch the next batch's entries
-          nb4[j] = k + 4 + j < n4 ? static_cast<int>(e.nbr4[static_cast<int64_t>(k + 4 + j) * e.NF + a] >> 5) : a;
+          nb4[j] = k + 4 + j < n4 ? static_cast<int>(e.nbr4[static_cast<int64_t>(k + 4 + j) * e.NF + a] >> kCodeBits) : a;
         }
         double2 pb[4];
         double mg[4];
@@ -1370,8 +1370,6 @@ __global__ void k_finalize(Dev e) {
 
 __global__ void __launch_bounds__(kMaxBlock) k_concentration(Dev e) {
   if (!e.ctl[e.shift_slot].shift_now) return;
-  __shared__ float4 tab[27];
-  fill_units(tab);
   const CaseDev& C = e.cases[e.shift_slot];
   const float sig2d = C.sig2d, inv_h = C.inv_h, cellf = C.cellf;
   const int NF = e.NF;
@@ -1383,12 +1381,12 @@ __global__ void __launch_bounds__(kMaxBlock) k_concentration(Dev e) {
       float part = 0.f;
 #pragma unroll
       for (int j = 0; j < kBatch; ++j) {
-        const int b0 = ent[j] != kPad ? static_cast<int>(ent[j] >> 5) : a;
+        const int b0 = ent[j] != kPad ? static_cast<int>(ent[j] >> kCodeBits) : a;
         const bool ok = ent[j] != kPad && b0 < NF;
         const int b = ok ? b0 : a;
         const float4 lb = e.lp[b];
         const float Vb = e.vb[b].w;
-        const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u], cellf);
+        const float3 d = sep(la, lb, ok ? ent[j] : kSelfCode, cellf);
         const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
         part += ok ? Vb * (sig2d * shape(radial(r2, inv_h).q)) : 0.f;
       }
@@ -1400,8 +1398,6 @@ __global__ void __launch_bounds__(kMaxBlock) k_concentration(Dev e) {
 
 __global__ void __launch_bounds__(kMaxBlock) k_conc_gradient(Dev e) {
   if (!e.ctl[e.shift_slot].shift_now) return;
-  __shared__ float4 tab[27];
-  fill_units(tab);
   const CaseDev& C = e.cases[e.shift_slot];
   const float sig2d = C.sig2d, inv_h = C.inv_h, cellf = C.cellf;
   const int NF = e.NF;
@@ -1413,13 +1409,13 @@ __global__ void __launch_bounds__(kMaxBlock) k_conc_gradient(Dev e) {
       float px = 0.f, py = 0.f, pz = 0.f;
 #pragma unroll
       for (int j = 0; j < kBatch; ++j) {
-        const int b0 = ent[j] != kPad ? static_cast<int>(ent[j] >> 5) : a;
+        const int b0 = ent[j] != kPad ? static_cast<int>(ent[j] >> kCodeBits) : a;
         const bool ok = ent[j] != kPad && b0 < NF;
         const int b = ok ? b0 : a;
         const float4 lb = e.lp[b];
         const float Vb = e.vb[b].w;
         const float cb = e.conc[b];
-        const float3 d = sep(la, lb, tab[ok ? (ent[j] & 31u) : 13u], cellf);
+        const float3 d = sep(la, lb, ok ? ent[j] : kSelfCode, cellf);
         const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
         const Radial R = radial(r2, inv_h);
         const float gs = sig2d * dshape(R.q) * inv_h * R.inv_r;
@@ -1595,15 +1591,15 @@ __global__ void k_remap(Dev e, int fluid_from, int wall_from, int df, int dw, in
     const int n = e.cnt[a];
     for (int k = 0; k < n; ++k) {
       uint32_t& ent = e.nbr[static_cast<int64_t>(k) * e.rows + a];
-      const uint32_t b = ent >> 5;
+      const uint32_t b = ent >> kCodeBits;
       const uint32_t nb = b < static_cast<uint32_t>(e.NF) ? b - df : b - dw;
-      ent = (nb << 5) | (ent & 31u);
+      ent = (nb << kCodeBits) | (ent & kCodeMask);
     }
     if (a < e.NF && e.cases[e.cid[a]].csf) {
       const int n4 = e.cnt4[a];
       for (int k = 0; k < n4; ++k) {
         uint32_t& ent = e.nbr4[static_cast<int64_t>(k) * e.NF + a];
-        ent = ((ent >> 5) - df) << 5;
+        ent = ((ent >> kCodeBits) - df) << kCodeBits;
       }
     }
   }
