@@ -112,6 +112,8 @@ struct Dev {
   float4* acc;
   float* conc;
   float4* gradc;
+  float4* lpv;       // shifting: local position + volume m/rho after the Euler update
+  float* tmp_v;      // the volume carried through a rebuild's permutation
   double4* csA;      // CSF: colour, M00, M01, M11
   double4* csB;      // CSF: grad c x, y, |grad c|, |det M|
   double2* csN0;     // CSF: raw normal
@@ -346,6 +348,7 @@ __global__ void k_permute(Dev e) {
     st4(e.tmp4a, a, ld4(e.pos, s));
     st4(e.tmp4b, a, ld4(e.vel, s));
     e.tmp_id[a] = e.id[s];
+    e.tmp_v[a] = e.vb[s].w;
   }
 }
 
@@ -365,6 +368,8 @@ __global__ void k_permute_back(Dev e) {
     e.id[a] = e.tmp_id[a];
     e.home[a] = key;
     e.lp[a] = local_of(C, key - C.key_off, p.x, p.y, p.z, p.w);
+    // the shifting passes after the Euler update read this step's volumes
+    if (C.shift_every > 0) e.lpv[a] = local_of(C, key - C.key_off, p.x, p.y, p.z, e.tmp_v[a]);
   }
 }
 
@@ -1299,7 +1304,9 @@ __global__ void __launch_bounds__(kMaxBlock) k_integrate(const __grid_constant__
     const double v[3] = {vx, vy, vz};
     st4(e.pos, a, make_double4(x[0], x[1], x[2], m));
     st4(e.vel, a, make_double4(v[0], v[1], v[2], 0.0));
-    e.lp[a] = local_of(C, e.home[a] - C.key_off, x[0], x[1], x[2], m);
+    const float4 la = local_of(C, e.home[a] - C.key_off, x[0], x[1], x[2], m);
+    e.lp[a] = la;
+    if (C.shift_every > 0) e.lpv[a] = make_float4(la.x, la.y, la.z, e.vb[a].w);
     const double4 an = ld4(e.anchor, a);
     double ex = x[0] - an.x, ey = x[1] - an.y, ez = x[2] - an.z;
     if (C.periodic) {
@@ -1374,9 +1381,9 @@ __global__ void __launch_bounds__(kMaxBlock) k_concentration(Dev e) {
   const float sig2d = C.sig2d, inv_h = C.inv_h, cellf = C.cellf;
   const int NF = e.NF;
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
-    const float4 la = e.lp[a];
+    const float4 la = e.lpv[a];  // (x, y, z, V) after the Euler update
     CSum<float> s;
-    s.add(e.vb[a].w * sig2d);
+    s.add(la.w * sig2d);
     walk_row(e, a, [&](const uint32_t* ent) {
       float part = 0.f;
 #pragma unroll
@@ -1384,8 +1391,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_concentration(Dev e) {
         const int b0 = ent[j] != kPad ? static_cast<int>(ent[j] >> kCodeBits) : a;
         const bool ok = ent[j] != kPad && b0 < NF;
         const int b = ok ? b0 : a;
-        const float4 lb = e.lp[b];
-        const float Vb = e.vb[b].w;
+        const float4 lb = e.lpv[b];
+        const float Vb = lb.w;
         const float3 d = sep(la, lb, ok ? ent[j] : kSelfCode, cellf);
         const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
         part += ok ? Vb * (sig2d * shape(radial(r2, inv_h).q)) : 0.f;
@@ -1402,7 +1409,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_conc_gradient(Dev e) {
   const float sig2d = C.sig2d, inv_h = C.inv_h, cellf = C.cellf;
   const int NF = e.NF;
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
-    const float4 la = e.lp[a];
+    const float4 la = e.lpv[a];
     const float ca = e.conc[a];
     CSum<float> gx, gy, gz;
     walk_row(e, a, [&](const uint32_t* ent) {
@@ -1412,8 +1419,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_conc_gradient(Dev e) {
         const int b0 = ent[j] != kPad ? static_cast<int>(ent[j] >> kCodeBits) : a;
         const bool ok = ent[j] != kPad && b0 < NF;
         const int b = ok ? b0 : a;
-        const float4 lb = e.lp[b];
-        const float Vb = e.vb[b].w;
+        const float4 lb = e.lpv[b];
+        const float Vb = lb.w;
         const float cb = e.conc[b];
         const float3 d = sep(la, lb, ok ? ent[j] : kSelfCode, cellf);
         const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
@@ -1684,6 +1691,7 @@ size_t carve(const tsph_engine_params& p, Dev* d, char* base, CaseDev** cases, c
   t.acc = static_cast<float4*>(take(NF * sizeof(float4)));
   t.conc = static_cast<float*>(take(NF * sizeof(float)));
   t.gradc = static_cast<float4*>(take(NF * sizeof(float4)));
+  t.lpv = static_cast<float4*>(take(NF * sizeof(float4)));
   t.csA = static_cast<double4*>(take(NF * sizeof(double4)));
   t.csB = static_cast<double4*>(take(NF * sizeof(double4)));
   t.csN0 = static_cast<double2*>(take(NF * sizeof(double2)));
@@ -1708,6 +1716,7 @@ size_t carve(const tsph_engine_params& p, Dev* d, char* base, CaseDev** cases, c
   t.tmp4a = static_cast<double4*>(take(nsort * sizeof(double4)));
   t.tmp4b = static_cast<double4*>(take(nsort * sizeof(double4)));
   t.tmp_id = static_cast<int32_t*>(take(nsort * sizeof(int32_t)));
+  t.tmp_v = static_cast<float*>(take(nsort * sizeof(float)));
   t.ctl = static_cast<CaseCtl*>(take(p.max_cases * sizeof(CaseCtl)));
   t.diag = static_cast<double*>(take(static_cast<size_t>(p.max_cases) * p.diag_ring * kDiag * sizeof(double)));
   t.any_rebuild = static_cast<int*>(take(sizeof(int)));
