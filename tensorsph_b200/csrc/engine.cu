@@ -1444,49 +1444,109 @@ __device__ __forceinline__ uint32_t fkey(float v) {
   return (b >> 31) ? ~b : (b | 0x80000000u);
 }
 
-// Radix select of the k-th smallest concentration, one 8-bit digit per pass.
-__global__ void k_select_hist(Dev e, int shift) {
+// Radix select of the two order statistics around the 95th percentile of the
+// concentration (ranks lo = floor(q), hi = ceil(q)), both in the same three
+// passes over 11-, 11- and 10-bit digits of the order-preserving key.
+// sel[r] holds rank r's key prefix, sel_k[r] its rank within that prefix and
+// sel[2 + r] the selected value; hist holds one 2048-bin histogram per rank
+// (rank 1 reuses rank 0's while their prefixes agree).
+constexpr int kSelBins = 2048;
+
+__global__ void k_select_hist(Dev e, int shift, int width) {
   if (!e.ctl[e.shift_slot].shift_now) return;
-  __shared__ unsigned int h[256];
-  h[threadIdx.x] = 0;
+  __shared__ unsigned int h[2][kSelBins];
+  for (int i = threadIdx.x; i < 2 * kSelBins; i += blockDim.x) (&h[0][0])[i] = 0;
   __syncthreads();
-  const uint32_t prefix = static_cast<uint32_t>(e.sel[0]);
-  const int hs = shift + 8;
+  const int hs = shift + width;
+  const bool first = hs >= 32;
+  const uint32_t p0 = static_cast<uint32_t>(e.sel[0]), p1 = static_cast<uint32_t>(e.sel[1]);
+  const bool same = first || (p0 >> hs) == (p1 >> hs);
+  const uint32_t mask = (1u << width) - 1u;
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
     const uint32_t k = fkey(e.conc[a]);
-    if (hs >= 32 || (k >> hs) == (prefix >> hs)) atomicAdd(&h[(k >> shift) & 255u], 1u);
+    const uint32_t digit = (k >> shift) & mask;
+    if (first || (k >> hs) == (p0 >> hs)) atomicAdd(&h[0][digit], 1u);
+    if (!same && (k >> hs) == (p1 >> hs)) atomicAdd(&h[1][digit], 1u);
   }
   __syncthreads();
-  if (h[threadIdx.x]) atomicAdd(&e.hist[threadIdx.x], h[threadIdx.x]);
+  for (int i = threadIdx.x; i < (same ? 1 : 2) * kSelBins; i += blockDim.x)
+    if ((&h[0][0])[i]) atomicAdd(&e.hist[i], (&h[0][0])[i]);
 }
 
-__global__ void k_select_pick(Dev e, int shift, long long rank, int which) {
-  if (!e.ctl[e.shift_slot].shift_now || threadIdx.x || blockIdx.x) return;
-  if (shift == 24) {
-    e.sel[0] = 0;
-    *e.sel_k = rank;
+// One block of 1024 threads: per rank, an exclusive scan of the bins (two per
+// thread) finds the digit whose run holds the rank; then the histograms are
+// cleared for the next pass.
+__global__ void __launch_bounds__(1024) k_select_pick(Dev e, int shift, int width, long long rank_lo,
+                                                      long long rank_hi) {
+  if (!e.ctl[e.shift_slot].shift_now) return;
+  __shared__ unsigned int warp_sum[32];
+  __shared__ int found_digit;
+  __shared__ unsigned long long found_below;
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const int hs = shift + width;
+  const bool first = hs >= 32;
+  if (first && t == 0) {
+    e.sel[0] = e.sel[1] = 0;
+    e.sel_k[0] = rank_lo;
+    e.sel_k[1] = rank_hi;
   }
-  long long k = *e.sel_k;
-  int d = 0;
-  for (; d < 255; ++d) {
-    if (k < static_cast<long long>(e.hist[d])) break;
-    k -= e.hist[d];
+  __syncthreads();
+  const uint32_t p0 = static_cast<uint32_t>(e.sel[0]), p1 = static_cast<uint32_t>(e.sel[1]);
+  const bool same = first || (p0 >> hs) == (p1 >> hs);
+  for (int r = 0; r < 2; ++r) {
+    if (t == 0) {
+      found_digit = 0;
+      found_below = 0;
+    }
+    const unsigned int* hr = e.hist + (same ? 0 : r) * kSelBins;
+    const unsigned int c0 = hr[2 * t], c1 = hr[2 * t + 1];
+    // block-wide exclusive scan of c0 + c1
+    unsigned int v = c0 + c1;
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned int n = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += n;
+    }
+    if (lane == 31) warp_sum[w] = v;
+    __syncthreads();
+    if (w == 0) {
+      unsigned int s = warp_sum[lane];
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned int n = __shfl_up_sync(0xffffffffu, s, o);
+        if (lane >= o) s += n;
+      }
+      warp_sum[lane] = s;
+    }
+    __syncthreads();
+    const unsigned long long below = static_cast<unsigned long long>(v - c0 - c1) + (w ? warp_sum[w - 1] : 0u);
+    const unsigned long long k = static_cast<unsigned long long>(e.sel_k[r]);
+    if (k >= below && k < below + c0) {
+      found_digit = 2 * t;
+      found_below = below;
+    } else if (k >= below + c0 && k < below + c0 + c1) {
+      found_digit = 2 * t + 1;
+      found_below = below + c0;
+    }
+    __syncthreads();
+    if (t == 0) {
+      e.sel[r] |= static_cast<unsigned long long>(found_digit) << shift;
+      e.sel_k[r] = static_cast<long long>(k - found_below);
+      if (shift == 0) {
+        const uint32_t key = static_cast<uint32_t>(e.sel[r]);
+        const uint32_t b = (key >> 31) ? (key & 0x7fffffffu) : ~key;
+        e.sel[2 + r] = static_cast<unsigned long long>(
+            __double_as_longlong(static_cast<double>(__uint_as_float(b))));
+      }
+    }
+    __syncthreads();
   }
-  e.sel[0] |= static_cast<unsigned long long>(d) << shift;
-  *e.sel_k = k;
-  for (int i = 0; i < 256; ++i) e.hist[i] = 0;
-  if (shift == 0) {
-    const uint32_t key = static_cast<uint32_t>(e.sel[0]);
-    const uint32_t b = (key >> 31) ? (key & 0x7fffffffu) : ~key;
-    e.sel[1 + which] = static_cast<unsigned long long>(__double_as_longlong(static_cast<double>(__uint_as_float(b))));
-  }
+  for (int i = t; i < 2 * kSelBins; i += blockDim.x) e.hist[i] = 0;
 }
 
 // torch.quantile's linear interpolation, computed as torch.lerp does it
 __global__ void k_select_finish(Dev e, double w) {
   if (!e.ctl[e.shift_slot].shift_now || threadIdx.x || blockIdx.x) return;
-  const double a = __longlong_as_double(static_cast<long long>(e.sel[1]));
-  const double b = __longlong_as_double(static_cast<long long>(e.sel[2]));
+  const double a = __longlong_as_double(static_cast<long long>(e.sel[2]));
+  const double b = __longlong_as_double(static_cast<long long>(e.sel[3]));
   e.ctl[e.shift_slot].cref[0] = w < 0.5 ? a + w * (b - a) : b - (b - a) * (1.0 - w);
   e.ctl[e.shift_slot].disp[1] = 0;
 }
@@ -1721,9 +1781,9 @@ size_t carve(const tsph_engine_params& p, Dev* d, char* base, CaseDev** cases, c
   t.diag = static_cast<double*>(take(static_cast<size_t>(p.max_cases) * p.diag_ring * kDiag * sizeof(double)));
   t.any_rebuild = static_cast<int*>(take(sizeof(int)));
   t.status = static_cast<int*>(take(sizeof(int)));
-  t.hist = static_cast<unsigned int*>(take(256 * sizeof(unsigned int)));
+  t.hist = static_cast<unsigned int*>(take(2 * kSelBins * sizeof(unsigned int)));
   t.sel = static_cast<unsigned long long*>(take(4 * sizeof(unsigned long long)));
-  t.sel_k = static_cast<long long*>(take(sizeof(long long)));
+  t.sel_k = static_cast<long long*>(take(2 * sizeof(long long)));
   CaseDev* cd = static_cast<CaseDev*>(take(p.max_cases * sizeof(CaseDev)));
   char* rs = static_cast<char*>(take(radix_scratch_bytes(nsort)));
   if (cases) *cases = cd;
@@ -1852,11 +1912,10 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr) {
     const double pos = 0.95 * static_cast<double>(d.nf - 1);
     const long long lo = static_cast<long long>(std::floor(pos)), hi = static_cast<long long>(std::ceil(pos));
     const unsigned gs = grid_for(d.nf, 256, 148 * 4);
-    for (int which = 0; which < 2; ++which) {
-      for (int shift = 24; shift >= 0; shift -= 8) {
-        k_select_hist<<<gs, 256, 0, s>>>(d, shift);
-        k_select_pick<<<1, 32, 0, s>>>(d, shift, which == 0 ? lo : hi, which);
-      }
+    const int widths[3] = {11, 11, 10}, shifts[3] = {21, 10, 0};
+    for (int pass = 0; pass < 3; ++pass) {
+      k_select_hist<<<gs, 256, 0, s>>>(d, shifts[pass], widths[pass]);
+      k_select_pick<<<1, 1024, 0, s>>>(d, shifts[pass], widths[pass], lo, hi);
     }
     k_select_finish<<<1, 32, 0, s>>>(d, pos - static_cast<double>(lo));
     mark();
@@ -2034,7 +2093,7 @@ int tsph_engine_create(const tsph_engine_params* prm, void* arena, int64_t arena
   for (int64_t c = prm->max_cases - 1; c >= 0; --c) E->free_slots.push_back(static_cast<int>(c));
   if (cudaMemsetAsync(d.ctl, 0, prm->max_cases * sizeof(CaseCtl), s) != cudaSuccess ||
       cudaMemsetAsync(d.status, 0, sizeof(int), s) != cudaSuccess ||
-      cudaMemsetAsync(d.hist, 0, 256 * sizeof(unsigned int), s) != cudaSuccess ||
+      cudaMemsetAsync(d.hist, 0, 2 * kSelBins * sizeof(unsigned int), s) != cudaSuccess ||
       cudaMemsetAsync(E->cases_dev, 0, prm->max_cases * sizeof(CaseDev), s) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess) {
     delete E;

@@ -120,6 +120,9 @@ def test_engine_shift_matches_fp64_oracle(gpu):
         eng.step(2)
         runs[every] = eng.state()[0].cpu().numpy()
         st = eng.status()
+        if every:
+            eng.step(1)   # the meter row of step 2 reports the c_ref of step 1's shift
+            c_ref = float(eng.diagnostics(2, 1).cpu()[0, 15])
         eng.close()
         assert st["status"] == 0 and st["rebuilds"] >= 2 + every
     xn, mn, wn = x.numpy(), mass.numpy(), wall.numpy()
@@ -130,6 +133,8 @@ def test_engine_shift_matches_fp64_oracle(gpu):
     _, info = op.shift_positions(x2, mn / ref[1][0], h, dt=cfg.dt, v_ref=vref, strength=1.0,
                                  limit=0.25, free_surface=0.95)
     shift = info["shift"]
+    # the device radix select of the 95th percentile against np.quantile
+    assert c_ref == pytest.approx(info["c_reference"], rel=1e-5)
     assert np.abs(shift).max() > 1e-6 * cfg.dx
     assert np.abs(runs[0] - x2).max() < 1e-6 * cfg.dx
     err = np.abs((runs[1] - runs[0]) - shift).max()
