@@ -239,6 +239,54 @@ __device__ __forceinline__ float3 sep(const float4& la, const float4& lb, uint32
                      fmaf(-unit<4>(ent), cellf, la.z - lb.z));
 }
 
+// ------------------------------------------------- packed FP32 pairs ---
+// Two neighbours per instruction with the sm_100 FP32x2 operations
+// (__ffma2_rn, __fadd2_rn, __fmul2_rn round each component as the scalar
+// operations do).
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, f2(-1.f), a); }
+
+// Cell offsets of two entries on one axis (see unit).
+template <int kShift>
+__device__ __forceinline__ float2 unit2(uint32_t e0, uint32_t e1) {
+  const uint32_t b0 = ((e0 << (21 - kShift)) & (3u << 21)) | 0x3f800000u;
+  const uint32_t b1 = ((e1 << (21 - kShift)) & (3u << 21)) | 0x3f800000u;
+  return __ffma2_rn(f2(4.f), make_float2(__uint_as_float(b0), __uint_as_float(b1)), f2(-5.f));
+}
+
+// Separations of two neighbours on one axis, (l_a - l_b) - u * cell: the same
+// bits as sep.  ncell = (-cell, -cell).
+template <int kShift>
+__device__ __forceinline__ float2 sep2(float la, float lb0, float lb1, uint32_t e0, uint32_t e1, float2 ncell) {
+  return __ffma2_rn(unit2<kShift>(e0, e1), ncell, sub2(f2(la), make_float2(lb0, lb1)));
+}
+
+struct Radial2 {
+  float2 q, inv_r;
+};
+__device__ __forceinline__ Radial2 radial2(float2 r2, float2 inv_h) {
+  Radial2 o;
+  o.inv_r = make_float2(r2.x > 1e-24f ? rsqrtf(r2.x) : 0.f, r2.y > 1e-24f ? rsqrtf(r2.y) : 0.f);
+  o.q = __fmul2_rn(__fmul2_rn(r2, o.inv_r), inv_h);
+  return o;
+}
+
+// Cubic spline f(q) of two neighbours.
+__device__ __forceinline__ float2 shape2(float2 q) {
+  const float2 t = __ffma2_rn(q, f2(-1.f), f2(2.f));
+  const float2 far = __fmul2_rn(__fmul2_rn(__fmul2_rn(t, t), t), f2(0.25f));
+  const float2 near = __ffma2_rn(__fmul2_rn(q, q), __ffma2_rn(q, f2(0.75f), f2(-1.5f)), f2(1.f));
+  return make_float2(q.x < 1.f ? near.x : (q.x < 2.f ? far.x : 0.f), q.y < 1.f ? near.y : (q.y < 2.f ? far.y : 0.f));
+}
+
+// Cubic spline f'(q) of two neighbours.
+__device__ __forceinline__ float2 dshape2(float2 q) {
+  const float2 t = __ffma2_rn(q, f2(-1.f), f2(2.f));
+  const float2 far = __fmul2_rn(__fmul2_rn(t, t), f2(-0.75f));
+  const float2 near = __fmul2_rn(q, __ffma2_rn(q, f2(2.25f), f2(-3.f)));
+  return make_float2(q.x < 1.f ? near.x : (q.x < 2.f ? far.x : 0.f), q.y < 1.f ? near.y : (q.y < 2.f ? far.y : 0.f));
+}
+
 __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* p, double v) {
   if (v > 0.0) atomicMax(p, static_cast<unsigned long long>(__double_as_longlong(v)));
 }
@@ -548,21 +596,25 @@ __global__ void __launch_bounds__(kMaxBlock) k_density(const __grid_constant__ D
     const CaseDev& C = case_of<kOne>(e, a);
     const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, floor_ = C.rho_floor;
     const float4 la = e.lp[a];
+    const float2 ncell = f2(-cellf), inv_h2 = f2(inv_h), sigma2 = f2(sigma);
     CSum<float> s;
     s.add(la.w * sigma);
     walk_row<KB>(e, a, [&](const uint32_t* ent) {
-      float part = 0.f;
+      float2 part = f2(0.f);
 #pragma unroll
-      for (int j = 0; j < KB; ++j) {
-        const bool ok = ent[j] != kPad;
-        const int b = ok ? static_cast<int>(ent[j] >> kCodeBits) : a;
-        const float4 lb = e.lp[b];
-        const float3 d = sep(la, lb, ok ? ent[j] : kSelfCode, cellf);
-        const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
-        const float W = sigma * shape(radial(r2, inv_h).q);
-        part += ok ? lb.w * W : 0.f;
+      for (int j = 0; j < KB; j += 2) {
+        const bool ok0 = ent[j] != kPad, ok1 = ent[j + 1] != kPad;
+        const uint32_t e0 = ok0 ? ent[j] : kSelfCode, e1 = ok1 ? ent[j + 1] : kSelfCode;
+        const float4 l0 = e.lp[ok0 ? static_cast<int>(ent[j] >> kCodeBits) : a];
+        const float4 l1 = e.lp[ok1 ? static_cast<int>(ent[j + 1] >> kCodeBits) : a];
+        const float2 dx = sep2<0>(la.x, l0.x, l1.x, e0, e1, ncell);
+        const float2 dy = sep2<2>(la.y, l0.y, l1.y, e0, e1, ncell);
+        const float2 dz = sep2<4>(la.z, l0.z, l1.z, e0, e1, ncell);
+        const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+        const float2 W = __fmul2_rn(sigma2, shape2(radial2(r2, inv_h2).q));
+        part = __ffma2_rn(make_float2(ok0 ? l0.w : 0.f, ok1 ? l1.w : 0.f), W, part);
       }
-      s.add(part);
+      s.add(part.x + part.y);
     });
     float rho = s.value();
     rho = rho > floor_ ? rho : floor_;
@@ -581,24 +633,32 @@ __global__ void __launch_bounds__(kMaxBlock) k_diffusion_eos(const __grid_consta
     if (dscale > 0.f) {
       const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf;
       const int NF = e.NF;
+      const float2 ncell = f2(-cellf), inv_h2 = f2(inv_h), gscale = f2(-sigma * inv_h);
       CSum<float> rate;
       walk_row<KB>(e, a, [&](const uint32_t* ent) {
-        float part = 0.f;
+        float2 part = f2(0.f);
 #pragma unroll
-        for (int j = 0; j < KB; ++j) {
-          const int b0 = ent[j] != kPad ? static_cast<int>(ent[j] >> kCodeBits) : a;
-          const bool ok = ent[j] != kPad && b0 < NF;
-          const int b = ok ? b0 : a;
-          const float4 lb = e.lp[b];
-          const float2 rb = e.rs[b];
-          const float3 d = sep(la, lb, ok ? ent[j] : kSelfCode, cellf);
-          const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
-          const Radial R = radial(r2, inv_h);
-          const float gs = sigma * dshape(R.q) * inv_h * R.inv_r;
-          const float coupling = (ra.x - rb.x) * (-gs * r2) * rcp_pair(r2 + 1e-12f);
-          part += ok ? (-dscale * rb.y) * coupling : 0.f;
+        for (int j = 0; j < KB; j += 2) {
+          const int c0 = ent[j] != kPad ? static_cast<int>(ent[j] >> kCodeBits) : a;
+          const int c1 = ent[j + 1] != kPad ? static_cast<int>(ent[j + 1] >> kCodeBits) : a;
+          const bool ok0 = ent[j] != kPad && c0 < NF, ok1 = ent[j + 1] != kPad && c1 < NF;
+          const int b0 = ok0 ? c0 : a, b1 = ok1 ? c1 : a;
+          const uint32_t e0 = ok0 ? ent[j] : kSelfCode, e1 = ok1 ? ent[j + 1] : kSelfCode;
+          const float4 l0 = e.lp[b0], l1 = e.lp[b1];
+          const float2 r0 = e.rs[b0], r1 = e.rs[b1];
+          const float2 dx = sep2<0>(la.x, l0.x, l1.x, e0, e1, ncell);
+          const float2 dy = sep2<2>(la.y, l0.y, l1.y, e0, e1, ncell);
+          const float2 dz = sep2<4>(la.z, l0.z, l1.z, e0, e1, ncell);
+          const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+          const Radial2 R = radial2(r2, inv_h2);
+          // -grad W . r = -sigma f'(q) r / h
+          const float2 ngr = __fmul2_rn(__fmul2_rn(__fmul2_rn(gscale, dshape2(R.q)), R.inv_r), r2);
+          const float2 coupling = __fmul2_rn(__fmul2_rn(sub2(f2(ra.x), make_float2(r0.x, r1.x)), ngr),
+                                             make_float2(rcp_pair(r2.x + 1e-12f), rcp_pair(r2.y + 1e-12f)));
+          const float2 w = make_float2(ok0 ? -dscale * r0.y : 0.f, ok1 ? -dscale * r1.y : 0.f);
+          part = __ffma2_rn(w, coupling, part);
         }
-        rate.add(part);
+        rate.add(part.x + part.y);
       });
       rho = ra.x + C.dtf * rate.value();
       rho = rho > C.rho_floor ? rho : C.rho_floor;
@@ -661,32 +721,41 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(const __grid_constant__ Dev
     const float4 la = e.lp[a];
     const float4 va = e.vb[a];
     const float Pa = e.pq[a];
+    const float2 ncell = f2(-cellf), inv_h2 = f2(inv_h), gscale = f2(sigma * inv_h);
     CSum<float> ax, ay, az;
     walk_row<KB>(e, a, [&](const uint32_t* ent) {
-      float px = 0.f, py = 0.f, pz = 0.f;
+      float2 px = f2(0.f), py = f2(0.f), pz = f2(0.f);
 #pragma unroll
-      for (int j = 0; j < KB; ++j) {
-        const bool ok = ent[j] != kPad;
-        const int b = ok ? static_cast<int>(ent[j] >> kCodeBits) : a;
-        const float4 lb = e.lp[b];
-        const float4 vb = e.vb[b];
-        const float Pb = e.pq[b];
-        const float3 d = sep(la, lb, ok ? ent[j] : kSelfCode, cellf);
-        const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
-        const Radial R = radial(r2, inv_h);
-        float gs = sigma * dshape(R.q) * inv_h * R.inv_r;
-        gs = ok ? gs : 0.f;
-        const float fp = -lb.w * (Pa + Pb) * gs;
-        const float vs = b < NF ? nu2 : nu2f;
-        const float lw = fmaxf(-gs * r2, 0.f) * rcp_pair(r2 + eta2);
-        const float coef = -vs * (vb.w * lw);
-        px += fp * d.x + coef * (va.x - vb.x);
-        py += fp * d.y + coef * (va.y - vb.y);
-        pz += fp * d.z + coef * (va.z - vb.z);
+      for (int j = 0; j < KB; j += 2) {
+        const bool ok0 = ent[j] != kPad, ok1 = ent[j + 1] != kPad;
+        const uint32_t e0 = ok0 ? ent[j] : kSelfCode, e1 = ok1 ? ent[j + 1] : kSelfCode;
+        const int b0 = ok0 ? static_cast<int>(ent[j] >> kCodeBits) : a;
+        const int b1 = ok1 ? static_cast<int>(ent[j + 1] >> kCodeBits) : a;
+        const float4 l0 = e.lp[b0], l1 = e.lp[b1];
+        const float4 v0 = e.vb[b0], v1 = e.vb[b1];
+        const float2 Pb = make_float2(e.pq[b0], e.pq[b1]);
+        const float2 dx = sep2<0>(la.x, l0.x, l1.x, e0, e1, ncell);
+        const float2 dy = sep2<2>(la.y, l0.y, l1.y, e0, e1, ncell);
+        const float2 dz = sep2<4>(la.z, l0.z, l1.z, e0, e1, ncell);
+        const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+        const Radial2 R = radial2(r2, inv_h2);
+        float2 gs = __fmul2_rn(__fmul2_rn(gscale, dshape2(R.q)), R.inv_r);
+        gs = make_float2(ok0 ? gs.x : 0.f, ok1 ? gs.y : 0.f);
+        // pressure: -m_b (P_a + P_b) grad W
+        const float2 fp = __fmul2_rn(__fmul2_rn(make_float2(-l0.w, -l1.w), __fadd2_rn(f2(Pa), Pb)), gs);
+        // viscosity: -nu2 V_b max(-gs r^2, 0) / (r^2 + eta^2) (v_a - v_b)
+        const float2 ngr = __fmul2_rn(gs, r2);
+        const float2 lw = __fmul2_rn(make_float2(fmaxf(-ngr.x, 0.f), fmaxf(-ngr.y, 0.f)),
+                                     make_float2(rcp_pair(r2.x + eta2), rcp_pair(r2.y + eta2)));
+        const float2 nvs = make_float2(b0 < NF ? -nu2 : -nu2f, b1 < NF ? -nu2 : -nu2f);
+        const float2 coef = __fmul2_rn(nvs, __fmul2_rn(make_float2(v0.w, v1.w), lw));
+        px = __ffma2_rn(fp, dx, __ffma2_rn(coef, sub2(f2(va.x), make_float2(v0.x, v1.x)), px));
+        py = __ffma2_rn(fp, dy, __ffma2_rn(coef, sub2(f2(va.y), make_float2(v0.y, v1.y)), py));
+        pz = __ffma2_rn(fp, dz, __ffma2_rn(coef, sub2(f2(va.z), make_float2(v0.z, v1.z)), pz));
       }
-      ax.add(px);
-      ay.add(py);
-      az.add(pz);
+      ax.add(px.x + px.y);
+      ay.add(py.x + py.y);
+      az.add(pz.x + pz.y);
     });
     float sx = 0.f, sy = 0.f;
     if (C.csf) {
@@ -1382,22 +1451,26 @@ __global__ void __launch_bounds__(kMaxBlock) k_concentration(Dev e) {
   const int NF = e.NF;
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
     const float4 la = e.lpv[a];  // (x, y, z, V) after the Euler update
+    const float2 ncell = f2(-cellf), inv_h2 = f2(inv_h), sig2 = f2(sig2d);
     CSum<float> s;
     s.add(la.w * sig2d);
     walk_row(e, a, [&](const uint32_t* ent) {
-      float part = 0.f;
+      float2 part = f2(0.f);
 #pragma unroll
-      for (int j = 0; j < kBatch; ++j) {
-        const int b0 = ent[j] != kPad ? static_cast<int>(ent[j] >> kCodeBits) : a;
-        const bool ok = ent[j] != kPad && b0 < NF;
-        const int b = ok ? b0 : a;
-        const float4 lb = e.lpv[b];
-        const float Vb = lb.w;
-        const float3 d = sep(la, lb, ok ? ent[j] : kSelfCode, cellf);
-        const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
-        part += ok ? Vb * (sig2d * shape(radial(r2, inv_h).q)) : 0.f;
+      for (int j = 0; j < kBatch; j += 2) {
+        const int c0 = ent[j] != kPad ? static_cast<int>(ent[j] >> kCodeBits) : a;
+        const int c1 = ent[j + 1] != kPad ? static_cast<int>(ent[j + 1] >> kCodeBits) : a;
+        const bool ok0 = ent[j] != kPad && c0 < NF, ok1 = ent[j + 1] != kPad && c1 < NF;
+        const uint32_t e0 = ok0 ? ent[j] : kSelfCode, e1 = ok1 ? ent[j + 1] : kSelfCode;
+        const float4 l0 = e.lpv[ok0 ? c0 : a], l1 = e.lpv[ok1 ? c1 : a];
+        const float2 dx = sep2<0>(la.x, l0.x, l1.x, e0, e1, ncell);
+        const float2 dy = sep2<2>(la.y, l0.y, l1.y, e0, e1, ncell);
+        const float2 dz = sep2<4>(la.z, l0.z, l1.z, e0, e1, ncell);
+        const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+        const float2 W = __fmul2_rn(sig2, shape2(radial2(r2, inv_h2).q));
+        part = __ffma2_rn(make_float2(ok0 ? l0.w : 0.f, ok1 ? l1.w : 0.f), W, part);
       }
-      s.add(part);
+      s.add(part.x + part.y);
     });
     e.conc[a] = s.value();
   }
@@ -1411,29 +1484,34 @@ __global__ void __launch_bounds__(kMaxBlock) k_conc_gradient(Dev e) {
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
     const float4 la = e.lpv[a];
     const float ca = e.conc[a];
+    const float2 ncell = f2(-cellf), inv_h2 = f2(inv_h), gscale = f2(sig2d * inv_h);
     CSum<float> gx, gy, gz;
     walk_row(e, a, [&](const uint32_t* ent) {
-      float px = 0.f, py = 0.f, pz = 0.f;
+      float2 px = f2(0.f), py = f2(0.f), pz = f2(0.f);
 #pragma unroll
-      for (int j = 0; j < kBatch; ++j) {
-        const int b0 = ent[j] != kPad ? static_cast<int>(ent[j] >> kCodeBits) : a;
-        const bool ok = ent[j] != kPad && b0 < NF;
-        const int b = ok ? b0 : a;
-        const float4 lb = e.lpv[b];
-        const float Vb = lb.w;
-        const float cb = e.conc[b];
-        const float3 d = sep(la, lb, ok ? ent[j] : kSelfCode, cellf);
-        const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
-        const Radial R = radial(r2, inv_h);
-        const float gs = sig2d * dshape(R.q) * inv_h * R.inv_r;
-        const float cc = ok ? Vb * (cb - ca) * gs : 0.f;
-        px += cc * d.x;
-        py += cc * d.y;
-        pz += cc * d.z;
+      for (int j = 0; j < kBatch; j += 2) {
+        const int c0 = ent[j] != kPad ? static_cast<int>(ent[j] >> kCodeBits) : a;
+        const int c1 = ent[j + 1] != kPad ? static_cast<int>(ent[j + 1] >> kCodeBits) : a;
+        const bool ok0 = ent[j] != kPad && c0 < NF, ok1 = ent[j + 1] != kPad && c1 < NF;
+        const int b0 = ok0 ? c0 : a, b1 = ok1 ? c1 : a;
+        const uint32_t e0 = ok0 ? ent[j] : kSelfCode, e1 = ok1 ? ent[j + 1] : kSelfCode;
+        const float4 l0 = e.lpv[b0], l1 = e.lpv[b1];
+        const float2 cb = make_float2(e.conc[b0], e.conc[b1]);
+        const float2 dx = sep2<0>(la.x, l0.x, l1.x, e0, e1, ncell);
+        const float2 dy = sep2<2>(la.y, l0.y, l1.y, e0, e1, ncell);
+        const float2 dz = sep2<4>(la.z, l0.z, l1.z, e0, e1, ncell);
+        const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+        const Radial2 R = radial2(r2, inv_h2);
+        const float2 gs = __fmul2_rn(__fmul2_rn(gscale, dshape2(R.q)), R.inv_r);
+        const float2 vb = make_float2(ok0 ? l0.w : 0.f, ok1 ? l1.w : 0.f);
+        const float2 cc = __fmul2_rn(__fmul2_rn(vb, sub2(cb, f2(ca))), gs);
+        px = __ffma2_rn(cc, dx, px);
+        py = __ffma2_rn(cc, dy, py);
+        pz = __ffma2_rn(cc, dz, pz);
       }
-      gx.add(px);
-      gy.add(py);
-      gz.add(pz);
+      gx.add(px.x + px.y);
+      gy.add(py.x + py.y);
+      gz.add(pz.x + pz.y);
     });
     e.gradc[a] = make_float4(gx.value(), gy.value(), gz.value(), 0.f);
   }
