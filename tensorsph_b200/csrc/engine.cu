@@ -48,7 +48,6 @@ constexpr int kBlock = 128;     // default threads per block of the pair kernels
 constexpr int kMaxBlock = 256;  // largest block the kernels are built for
 constexpr int kDiag = 16;
 constexpr int kBatch = 4;
-constexpr uint32_t kPad = 0xffffffffu;
 constexpr int kCodeBits = 6;                               // cell-offset code bits of a row entry
 constexpr uint32_t kCodeMask = (1u << kCodeBits) - 1;
 constexpr uint32_t kSelfCode = 0x15u;                      // offset (0, 0, 0): fields (1, 1, 1)
@@ -91,8 +90,12 @@ struct CaseCtl {
 };
 
 struct Dev {
-  int nf, nw, NF, n_slots, maxnb, diag_ring, n_ob, shift_slot, one_slot, pad_;
+  int nf, nw, NF, n_slots, maxnb, diag_ring, n_ob, shift_slot, one_slot, null_row;
   int64_t rows;  // NF + wall capacity: the row stride of nbr
+  // The null row (index rows) of every gathered array: far from every case,
+  // zero mass, volume, pressure and velocity, so that a pair with it adds
+  // exactly zero.  Rows are padded to whole batches with entries of it.
+  uint32_t pad;
   CaseDev one;   // the case of a batch of one (kernel-parameter copy)
   const CaseDev* cases;
   CaseCtl* ctl;
@@ -311,7 +314,7 @@ __device__ __forceinline__ uint32_t ld_entry(const uint32_t* p) {
 // hardware reciprocal, within 2 ulp.
 __device__ __forceinline__ float rcp_pair(float x) { return __fdividef(1.f, x); }
 
-// Walk row a in batches of KB entries (padded with kPad); the loads of a
+// Walk row a in batches of KB entries (padded with null-row entries); the loads of a
 // batch are all issued before any use.  KB (the batch depth: neighbour
 // records in flight per thread) is a tuning parameter of the hot kernels.
 template <int KB = kBatch, class Body>
@@ -321,11 +324,11 @@ __device__ __forceinline__ void walk_row(const Dev& e, int64_t a, Body&& body) {
   // the entries of the next batch are loaded while the current one is used
   uint32_t cur[KB], nxt[KB];
 #pragma unroll
-  for (int j = 0; j < KB; ++j) cur[j] = j < n ? ld_entry(row + static_cast<int64_t>(j) * e.rows) : kPad;
+  for (int j = 0; j < KB; ++j) cur[j] = j < n ? ld_entry(row + static_cast<int64_t>(j) * e.rows) : e.pad;
   for (int k = 0; k < n; k += KB) {
 #pragma unroll
     for (int j = 0; j < KB; ++j)
-      nxt[j] = (k + KB + j < n) ? ld_entry(row + static_cast<int64_t>(k + KB + j) * e.rows) : kPad;
+      nxt[j] = (k + KB + j < n) ? ld_entry(row + static_cast<int64_t>(k + KB + j) * e.rows) : e.pad;
     body(cur);
 #pragma unroll
     for (int j = 0; j < KB; ++j) cur[j] = nxt[j];
@@ -603,16 +606,14 @@ __global__ void __launch_bounds__(kMaxBlock) k_density(const __grid_constant__ D
       float2 part = f2(0.f);
 #pragma unroll
       for (int j = 0; j < KB; j += 2) {
-        const bool ok0 = ent[j] != kPad, ok1 = ent[j + 1] != kPad;
-        const uint32_t e0 = ok0 ? ent[j] : kSelfCode, e1 = ok1 ? ent[j + 1] : kSelfCode;
-        const float4 l0 = e.lp[ok0 ? static_cast<int>(ent[j] >> kCodeBits) : a];
-        const float4 l1 = e.lp[ok1 ? static_cast<int>(ent[j + 1] >> kCodeBits) : a];
+        const uint32_t e0 = ent[j], e1 = ent[j + 1];
+        const float4 l0 = e.lp[e0 >> kCodeBits], l1 = e.lp[e1 >> kCodeBits];
         const float2 dx = sep2<0>(la.x, l0.x, l1.x, e0, e1, ncell);
         const float2 dy = sep2<2>(la.y, l0.y, l1.y, e0, e1, ncell);
         const float2 dz = sep2<4>(la.z, l0.z, l1.z, e0, e1, ncell);
         const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
         const float2 W = __fmul2_rn(sigma2, shape2(radial2(r2, inv_h2).q));
-        part = __ffma2_rn(make_float2(ok0 ? l0.w : 0.f, ok1 ? l1.w : 0.f), W, part);
+        part = __ffma2_rn(make_float2(l0.w, l1.w), W, part);
       }
       s.add(part.x + part.y);
     });
@@ -639,11 +640,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_diffusion_eos(const __grid_consta
         float2 part = f2(0.f);
 #pragma unroll
         for (int j = 0; j < KB; j += 2) {
-          const int c0 = ent[j] != kPad ? static_cast<int>(ent[j] >> kCodeBits) : a;
-          const int c1 = ent[j + 1] != kPad ? static_cast<int>(ent[j + 1] >> kCodeBits) : a;
-          const bool ok0 = ent[j] != kPad && c0 < NF, ok1 = ent[j + 1] != kPad && c1 < NF;
-          const int b0 = ok0 ? c0 : a, b1 = ok1 ? c1 : a;
-          const uint32_t e0 = ok0 ? ent[j] : kSelfCode, e1 = ok1 ? ent[j + 1] : kSelfCode;
+          // wall neighbours do not diffuse: they read the null row
+          const uint32_t e0 = ent[j], e1 = ent[j + 1];
+          const int c0 = static_cast<int>(e0 >> kCodeBits), c1 = static_cast<int>(e1 >> kCodeBits);
+          const int b0 = c0 < NF ? c0 : e.null_row, b1 = c1 < NF ? c1 : e.null_row;
           const float4 l0 = e.lp[b0], l1 = e.lp[b1];
           const float2 r0 = e.rs[b0], r1 = e.rs[b1];
           const float2 dx = sep2<0>(la.x, l0.x, l1.x, e0, e1, ncell);
@@ -655,7 +655,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_diffusion_eos(const __grid_consta
           const float2 ngr = __fmul2_rn(__fmul2_rn(__fmul2_rn(gscale, dshape2(R.q)), R.inv_r), r2);
           const float2 coupling = __fmul2_rn(__fmul2_rn(sub2(f2(ra.x), make_float2(r0.x, r1.x)), ngr),
                                              make_float2(rcp_pair(r2.x + 1e-12f), rcp_pair(r2.y + 1e-12f)));
-          const float2 w = make_float2(ok0 ? -dscale * r0.y : 0.f, ok1 ? -dscale * r1.y : 0.f);
+          const float2 w = make_float2(-dscale * r0.y, -dscale * r1.y);
           part = __ffma2_rn(w, coupling, part);
         }
         rate.add(part.x + part.y);
@@ -685,7 +685,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_walls(const __grid_constant__ Dev
       float pn = 0.f, pd = 0.f;
 #pragma unroll
       for (int j = 0; j < KB; ++j) {
-        const bool ok = ent[j] != kPad;
+        const bool ok = ent[j] != e.pad;
         const int f = ok ? static_cast<int>(ent[j] >> kCodeBits) : f0;
         const float4 lf = e.lp[f];
         const float3 d = sep(la, lf, ok ? ent[j] : kSelfCode, cellf);  // r_w - r_f
@@ -727,10 +727,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(const __grid_constant__ Dev
       float2 px = f2(0.f), py = f2(0.f), pz = f2(0.f);
 #pragma unroll
       for (int j = 0; j < KB; j += 2) {
-        const bool ok0 = ent[j] != kPad, ok1 = ent[j + 1] != kPad;
-        const uint32_t e0 = ok0 ? ent[j] : kSelfCode, e1 = ok1 ? ent[j + 1] : kSelfCode;
-        const int b0 = ok0 ? static_cast<int>(ent[j] >> kCodeBits) : a;
-        const int b1 = ok1 ? static_cast<int>(ent[j + 1] >> kCodeBits) : a;
+        const uint32_t e0 = ent[j], e1 = ent[j + 1];
+        const int b0 = static_cast<int>(e0 >> kCodeBits), b1 = static_cast<int>(e1 >> kCodeBits);
         const float4 l0 = e.lp[b0], l1 = e.lp[b1];
         const float4 v0 = e.vb[b0], v1 = e.vb[b1];
         const float2 Pb = make_float2(e.pq[b0], e.pq[b1]);
@@ -739,8 +737,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(const __grid_constant__ Dev
         const float2 dz = sep2<4>(la.z, l0.z, l1.z, e0, e1, ncell);
         const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
         const Radial2 R = radial2(r2, inv_h2);
-        float2 gs = __fmul2_rn(__fmul2_rn(gscale, dshape2(R.q)), R.inv_r);
-        gs = make_float2(ok0 ? gs.x : 0.f, ok1 ? gs.y : 0.f);
+        const float2 gs = __fmul2_rn(__fmul2_rn(gscale, dshape2(R.q)), R.inv_r);
         // pressure: -m_b (P_a + P_b) grad W
         const float2 fp = __fmul2_rn(__fmul2_rn(make_float2(-l0.w, -l1.w), __fadd2_rn(f2(Pa), Pb)), gs);
         // viscosity: -nu2 V_b max(-gs r^2, 0) / (r^2 + eta^2) (v_a - v_b)
@@ -795,7 +792,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_reaction(Dev e) {
       float px = 0.f, py = 0.f, pz = 0.f;
 #pragma unroll
       for (int j = 0; j < kBatch; ++j) {
-        const bool ok = ent[j] != kPad;
+        const bool ok = ent[j] != e.pad;
         const int fi = ok ? static_cast<int>(ent[j] >> kCodeBits) : f0;
         const float4 lf = e.lp[fi];
         const float3 d = sep(lw_, lf, ok ? ent[j] : kSelfCode, cellf);
@@ -1458,17 +1455,15 @@ __global__ void __launch_bounds__(kMaxBlock) k_concentration(Dev e) {
       float2 part = f2(0.f);
 #pragma unroll
       for (int j = 0; j < kBatch; j += 2) {
-        const int c0 = ent[j] != kPad ? static_cast<int>(ent[j] >> kCodeBits) : a;
-        const int c1 = ent[j + 1] != kPad ? static_cast<int>(ent[j + 1] >> kCodeBits) : a;
-        const bool ok0 = ent[j] != kPad && c0 < NF, ok1 = ent[j + 1] != kPad && c1 < NF;
-        const uint32_t e0 = ok0 ? ent[j] : kSelfCode, e1 = ok1 ? ent[j + 1] : kSelfCode;
-        const float4 l0 = e.lpv[ok0 ? c0 : a], l1 = e.lpv[ok1 ? c1 : a];
+        const uint32_t e0 = ent[j], e1 = ent[j + 1];
+        const int c0 = static_cast<int>(e0 >> kCodeBits), c1 = static_cast<int>(e1 >> kCodeBits);
+        const float4 l0 = e.lpv[c0 < NF ? c0 : e.null_row], l1 = e.lpv[c1 < NF ? c1 : e.null_row];
         const float2 dx = sep2<0>(la.x, l0.x, l1.x, e0, e1, ncell);
         const float2 dy = sep2<2>(la.y, l0.y, l1.y, e0, e1, ncell);
         const float2 dz = sep2<4>(la.z, l0.z, l1.z, e0, e1, ncell);
         const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
         const float2 W = __fmul2_rn(sig2, shape2(radial2(r2, inv_h2).q));
-        part = __ffma2_rn(make_float2(ok0 ? l0.w : 0.f, ok1 ? l1.w : 0.f), W, part);
+        part = __ffma2_rn(make_float2(l0.w, l1.w), W, part);
       }
       s.add(part.x + part.y);
     });
@@ -1490,11 +1485,9 @@ __global__ void __launch_bounds__(kMaxBlock) k_conc_gradient(Dev e) {
       float2 px = f2(0.f), py = f2(0.f), pz = f2(0.f);
 #pragma unroll
       for (int j = 0; j < kBatch; j += 2) {
-        const int c0 = ent[j] != kPad ? static_cast<int>(ent[j] >> kCodeBits) : a;
-        const int c1 = ent[j + 1] != kPad ? static_cast<int>(ent[j + 1] >> kCodeBits) : a;
-        const bool ok0 = ent[j] != kPad && c0 < NF, ok1 = ent[j + 1] != kPad && c1 < NF;
-        const int b0 = ok0 ? c0 : a, b1 = ok1 ? c1 : a;
-        const uint32_t e0 = ok0 ? ent[j] : kSelfCode, e1 = ok1 ? ent[j + 1] : kSelfCode;
+        const uint32_t e0 = ent[j], e1 = ent[j + 1];
+        const int c0 = static_cast<int>(e0 >> kCodeBits), c1 = static_cast<int>(e1 >> kCodeBits);
+        const int b0 = c0 < NF ? c0 : e.null_row, b1 = c1 < NF ? c1 : e.null_row;
         const float4 l0 = e.lpv[b0], l1 = e.lpv[b1];
         const float2 cb = make_float2(e.conc[b0], e.conc[b1]);
         const float2 dx = sep2<0>(la.x, l0.x, l1.x, e0, e1, ncell);
@@ -1503,7 +1496,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_conc_gradient(Dev e) {
         const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
         const Radial2 R = radial2(r2, inv_h2);
         const float2 gs = __fmul2_rn(__fmul2_rn(gscale, dshape2(R.q)), R.inv_r);
-        const float2 vb = make_float2(ok0 ? l0.w : 0.f, ok1 ? l1.w : 0.f);
+        const float2 vb = make_float2(l0.w, l1.w);
         const float2 cc = __fmul2_rn(__fmul2_rn(vb, sub2(cb, f2(ca))), gs);
         px = __ffma2_rn(cc, dx, px);
         py = __ffma2_rn(cc, dy, py);
@@ -1677,6 +1670,22 @@ __global__ void __launch_bounds__(kMaxBlock) k_shift_apply(Dev e) {
   }
 }
 
+// The null row: positions 1e4 m from every cell origin (pairs with it are
+// far outside the support, and every term is multiplied by its zero mass,
+// volume or weight), finite density.
+__global__ void k_null_row(Dev e) {
+  const int64_t n = e.null_row;
+  const float4 far = make_float4(1e4f, 1e4f, 1e4f, 0.f);
+  e.lp[n] = far;
+  e.lpv[n] = far;
+  e.vb[n] = make_float4(0.f, 0.f, 0.f, 0.f);
+  e.pr[n] = 0.f;
+  e.rho[n] = 1.f;
+  e.pq[n] = 0.f;
+  e.rs[n] = make_float2(1.f, 0.f);
+  e.conc[n] = 0.f;
+}
+
 // ----------------------------------------------------- admission, retire ---
 
 __global__ void k_place_fluid(Dev e, int begin, int n, int slot, int dim, const double* __restrict__ x,
@@ -1814,22 +1823,24 @@ size_t carve(const tsph_engine_params& p, Dev* d, char* base, CaseDev** cases, c
   const int64_t nsort = std::max(NF, NW);
   Dev t{};
   t.rows = N;
+  t.null_row = static_cast<int>(N);
+  t.pad = (static_cast<uint32_t>(N) << kCodeBits) | kSelfCode;
   t.pos = static_cast<double4*>(take(N * sizeof(double4)));
   t.vel = static_cast<double4*>(take(NF * sizeof(double4)));
   t.anchor = static_cast<double4*>(take(NF * sizeof(double4)));
-  t.lp = static_cast<float4*>(take(N * sizeof(float4)));
+  t.lp = static_cast<float4*>(take((N + 1) * sizeof(float4)));
   t.home = static_cast<int32_t*>(take(N * sizeof(int32_t)));
   t.id = static_cast<int32_t*>(take(NF * sizeof(int32_t)));
   t.cid = static_cast<int32_t*>(take(N * sizeof(int32_t)));
-  t.vb = static_cast<float4*>(take(N * sizeof(float4)));
-  t.pr = static_cast<float*>(take(N * sizeof(float)));
-  t.rho = static_cast<float*>(take(N * sizeof(float)));
-  t.pq = static_cast<float*>(take(N * sizeof(float)));
-  t.rs = static_cast<float2*>(take(NF * sizeof(float2)));
+  t.vb = static_cast<float4*>(take((N + 1) * sizeof(float4)));
+  t.pr = static_cast<float*>(take((N + 1) * sizeof(float)));
+  t.rho = static_cast<float*>(take((N + 1) * sizeof(float)));
+  t.pq = static_cast<float*>(take((N + 1) * sizeof(float)));
+  t.rs = static_cast<float2*>(take((N + 1) * sizeof(float2)));
   t.acc = static_cast<float4*>(take(NF * sizeof(float4)));
-  t.conc = static_cast<float*>(take(NF * sizeof(float)));
+  t.conc = static_cast<float*>(take((N + 1) * sizeof(float)));
   t.gradc = static_cast<float4*>(take(NF * sizeof(float4)));
-  t.lpv = static_cast<float4*>(take(NF * sizeof(float4)));
+  t.lpv = static_cast<float4*>(take((N + 1) * sizeof(float4)));
   t.csA = static_cast<double4*>(take(NF * sizeof(double4)));
   t.csB = static_cast<double4*>(take(NF * sizeof(double4)));
   t.csN0 = static_cast<double2*>(take(NF * sizeof(double2)));
@@ -2148,7 +2159,8 @@ int tsph_engine_create(const tsph_engine_params* prm, void* arena, int64_t arena
                        tsph_engine** out) {
   if (!prm || !out || !arena) return TSPH_ERR_ARG;
   const int64_t bytes = tsph_engine_bytes(prm);
-  if (bytes < 0 || prm->max_fluid + std::max<int64_t>(prm->max_wall, 1) > kMaxRows ||
+  // the rows and the null row after them
+  if (bytes < 0 || prm->max_fluid + std::max<int64_t>(prm->max_wall, 1) + 1 > kMaxRows ||
       prm->max_cells >= (int64_t(1) << 31) || prm->max_obstacle > prm->max_wall)
     return TSPH_ERR_ARG;
   if (arena_bytes < bytes) return TSPH_ERR_WORKSPACE;
@@ -2173,6 +2185,7 @@ int tsph_engine_create(const tsph_engine_params* prm, void* arena, int64_t arena
       cudaMemsetAsync(d.status, 0, sizeof(int), s) != cudaSuccess ||
       cudaMemsetAsync(d.hist, 0, 2 * kSelBins * sizeof(unsigned int), s) != cudaSuccess ||
       cudaMemsetAsync(E->cases_dev, 0, prm->max_cases * sizeof(CaseDev), s) != cudaSuccess ||
+      (k_null_row<<<1, 1, 0, s>>>(d), cudaGetLastError()) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess) {
     delete E;
     return TSPH_ERR_CUDA;
