@@ -314,7 +314,7 @@ def main():
     nf, nw = eng.n_fluid, eng.n_wall
     eng.step(max(args.warmup, 1))
     torch.cuda.synchronize(dev)
-    eng.status()
+    rebuilds_before = eng.status()["rebuilds"]
 
     def barrier():
         if dist is not None:
@@ -336,7 +336,11 @@ def main():
     status = eng.status()
     ms_step = ms / args.steps
     value = whole_job_rate(nf, args.steps, world, ms / 1e3)
-    kernels_per_step = eng.graph_kernels()
+    # every step's kernels, plus the conditional rebuild body once per list
+    # pass that rebuilt during the timed steps
+    kernels_per_step, kernels_per_rebuild = eng.graph_kernels()
+    rebuild_passes = status["rebuilds"] - rebuilds_before
+    launches = kernels_per_step * args.steps + kernels_per_rebuild * rebuild_passes
 
     stage = {}
     for _ in range(3):
@@ -429,13 +433,14 @@ def main():
                          "step_hbm_frac": ALGO_BYTES_STEP * nf / (ms_step / 1e3) / 1e9 / peak},
             "stage_ms": stage,
             "clocks": clocks,
-            "gpu_launches": kernels_per_step * args.steps,
+            "gpu_launches": launches,
             "e2e": e2e,
             "cpu_baseline": cpu,
             "engine": {"rebuilds": status["rebuilds"], "escapes": status["escapes"],
                        "obstacle_clamps": status["clamps"], "longest_row": status["row_max"],
                        "last_rho_max": float(diag[0]), "last_speed_max": float(diag[1]),
-                       "kernels_per_step": kernels_per_step},
+                       "kernels_per_step": kernels_per_step, "kernels_per_rebuild_pass": kernels_per_rebuild,
+                       "rebuild_passes_timed": rebuild_passes},
         }
         line.update(extra)
         print(json.dumps(line))

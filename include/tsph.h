@@ -405,7 +405,10 @@ int tsph_engine_step_eager(tsph_engine* engine, int64_t steps, tsph_stream strea
  * gradient, reference select, apply. */
 int tsph_engine_step_timed(tsph_engine* engine, tsph_stream stream, float* stage_ms,
                            int64_t* stages);
-/* Number of kernel nodes in the captured step graph (host; after a step). */
+/* Kernel nodes of the captured step graph (host; after a step): kernels[0]
+ * run every step; kernels[1] run once more for each list pass in which some
+ * case rebuilds (the conditional rebuild body; 0 when the rebuild kernels are
+ * unconditional nodes counted in kernels[0]).  `kernels` holds 2 values. */
 int tsph_engine_graph_kernels(tsph_engine* engine, int64_t* kernels);
 /* Fluid state of one case in its original particle order, (n_fluid, dim)
  * FP64 (device, nullable). */

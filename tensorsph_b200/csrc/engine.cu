@@ -1806,6 +1806,9 @@ struct tsph_engine {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaStream_t captured_on = nullptr;
+  cudaStream_t aux = nullptr;  // captures the bodies of the step graph's conditional nodes
+  bool conditional = true;     // rebuilds in conditional nodes (off if the driver refuses them)
+  int64_t rebuild_kernels = 0; // kernel nodes of one conditional rebuild body
 };
 
 namespace tsph {
@@ -1913,12 +1916,12 @@ void batch_changed(tsph_engine* E) {
   }
 }
 
-int enqueue_rebuild(tsph_engine* E, cudaStream_t s, int pass) {
+// The list rebuild after the skin test: keys, sort, permutation, cell table,
+// rows.  Every kernel also returns at once when no case is due.
+int enqueue_rebuild_body(tsph_engine* E, cudaStream_t s) {
   Dev& d = E->d;
   const unsigned g = grid_for(d.nf, kBlock);
   const unsigned gc = grid_for(d.n_slots, 128);
-  TSPH_CUDA_CHECK(cudaMemsetAsync(d.any_rebuild, 0, sizeof(int), s));
-  k_check<<<gc, 128, 0, s>>>(d, pass);
   k_keys<<<g, kBlock, 0, s>>>(d);
   TSPH_LAUNCH_CHECK();
   int rc = radix_sort_u64_i32(d.keys, d.vals, d.keys_tmp, d.vals_tmp, d.nf, key_bits(E->total_cells),
@@ -1934,12 +1937,66 @@ int enqueue_rebuild(tsph_engine* E, cudaStream_t s, int pass) {
   return TSPH_OK;
 }
 
+__global__ void k_set_rebuild_condition(cudaGraphConditionalHandle h, const int* any_rebuild) {
+  cudaGraphSetConditional(h, *any_rebuild ? 1u : 0u);
+}
+
+// Skin test, then the rebuild.  While a step graph is being captured
+// (`conditional`), the rebuild goes into the body of a conditional node that
+// the skin test's flag switches on, so that steps without a rebuild skip its
+// ~20 launches.
+int enqueue_rebuild(tsph_engine* E, cudaStream_t s, int pass, bool conditional) {
+  Dev& d = E->d;
+  const unsigned gc = grid_for(d.n_slots, 128);
+  TSPH_CUDA_CHECK(cudaMemsetAsync(d.any_rebuild, 0, sizeof(int), s));
+  k_check<<<gc, 128, 0, s>>>(d, pass);
+  TSPH_LAUNCH_CHECK();
+  if (!conditional) return enqueue_rebuild_body(E, s);
+  cudaStreamCaptureStatus status;
+  cudaGraph_t graph = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  TSPH_CUDA_CHECK(cudaStreamGetCaptureInfo(s, &status, nullptr, &graph, &deps, &ndeps));
+  if (status != cudaStreamCaptureStatusActive) return TSPH_ERR_CUDA;
+  cudaGraphConditionalHandle handle;
+  TSPH_CUDA_CHECK(cudaGraphConditionalHandleCreate(&handle, graph, 0, 0));
+  k_set_rebuild_condition<<<1, 1, 0, s>>>(handle, d.any_rebuild);
+  TSPH_LAUNCH_CHECK();
+  TSPH_CUDA_CHECK(cudaStreamGetCaptureInfo(s, &status, nullptr, &graph, &deps, &ndeps));
+  cudaGraphNodeParams params{};
+  params.type = cudaGraphNodeTypeConditional;
+  params.conditional.handle = handle;
+  params.conditional.type = cudaGraphCondTypeIf;
+  params.conditional.size = 1;
+  cudaGraphNode_t node;
+  TSPH_CUDA_CHECK(cudaGraphAddNode(&node, graph, deps, ndeps, &params));
+  TSPH_CUDA_CHECK(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+  TSPH_CUDA_CHECK(cudaStreamBeginCaptureToGraph(E->aux, params.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                cudaStreamCaptureModeThreadLocal));
+  const int rc = enqueue_rebuild_body(E, E->aux);
+  cudaGraph_t body = nullptr;
+  const cudaError_t end = cudaStreamEndCapture(E->aux, &body);
+  if (rc) return rc;
+  if (end != cudaSuccess) return TSPH_ERR_CUDA;
+  size_t count = 0;
+  TSPH_CUDA_CHECK(cudaGraphGetNodes(params.conditional.phGraph_out[0], nullptr, &count));
+  std::vector<cudaGraphNode_t> nodes(count);
+  TSPH_CUDA_CHECK(cudaGraphGetNodes(params.conditional.phGraph_out[0], nodes.data(), &count));
+  int64_t k = 0;
+  for (size_t i = 0; i < count; ++i) {
+    cudaGraphNodeType t;
+    if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++k;
+  }
+  E->rebuild_kernels = k;
+  return TSPH_OK;
+}
+
 // Stage marks: when `marks` is non-null an event is recorded after each stage
 // (rebuild, density, diffusion+EOS, walls, force, reaction, integrate+meters,
 // shift rebuild, concentration, gradient, select, apply).
 constexpr int kStages = 12;
 
-int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr) {
+int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr, bool graph = false) {
   Dev& d = E->d;
   int stage = 0;
   auto mark = [&]() {
@@ -1947,7 +2004,7 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr) {
     ++stage;
   };
   if (d.nf == 0) return TSPH_OK;
-  int rc = enqueue_rebuild(E, s, 0);
+  int rc = enqueue_rebuild(E, s, 0, graph);
   if (rc) return rc;
   const unsigned gc = grid_for(d.n_slots, 128);
   k_step_begin<<<gc, 128, 0, s>>>(d);
@@ -1991,7 +2048,7 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr) {
   TSPH_LAUNCH_CHECK();
   mark();
   if (shifting(E)) {
-    rc = enqueue_rebuild(E, s, 1);
+    rc = enqueue_rebuild(E, s, 1, graph);
     if (rc) return rc;
     mark();
     k_concentration<<<g, B, 0, s>>>(d);
@@ -2167,6 +2224,10 @@ int tsph_engine_create(const tsph_engine_params* prm, void* arena, int64_t arena
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   tsph_engine* E = new (std::nothrow) tsph_engine();
   if (!E) return TSPH_ERR_ARG;
+  if (cudaStreamCreateWithFlags(&E->aux, cudaStreamNonBlocking) != cudaSuccess) {
+    delete E;
+    return TSPH_ERR_CUDA;
+  }
   E->prm = *prm;
   E->arena = static_cast<char*>(arena);
   carve(*prm, &E->d, E->arena, &E->cases_dev, &E->radix_scratch);
@@ -2187,6 +2248,7 @@ int tsph_engine_create(const tsph_engine_params* prm, void* arena, int64_t arena
       cudaMemsetAsync(E->cases_dev, 0, prm->max_cases * sizeof(CaseDev), s) != cudaSuccess ||
       (k_null_row<<<1, 1, 0, s>>>(d), cudaGetLastError()) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess) {
+    cudaStreamDestroy(E->aux);
     delete E;
     return TSPH_ERR_CUDA;
   }
@@ -2346,17 +2408,28 @@ int tsph_engine_step(tsph_engine* E, int64_t steps, tsph_stream stream) {
   if (E->order.empty()) return TSPH_OK;
   if (!E->exec || E->captured_on != s) {
     invalidate_graph(E);
-    TSPH_CUDA_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    int rc = enqueue_step(E, s);
-    cudaGraph_t g = nullptr;
-    cudaError_t ce = cudaStreamEndCapture(s, &g);
-    if (rc) {
+    // with conditional rebuild nodes first; without them if the capture or
+    // the instantiation fails
+    for (int attempt = 0;; ++attempt) {
+      const bool cond = E->conditional;
+      TSPH_CUDA_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      int rc = enqueue_step(E, s, nullptr, cond);
+      cudaGraph_t g = nullptr;
+      cudaError_t ce = cudaStreamEndCapture(s, &g);
+      if (rc == TSPH_OK && ce == cudaSuccess) {
+        ce = cudaGraphInstantiate(&E->exec, g, 0);
+        if (ce == cudaSuccess) {
+          E->graph = g;
+          break;
+        }
+        E->exec = nullptr;
+      }
       if (g) cudaGraphDestroy(g);
-      return rc;
+      if (!cond || attempt > 0) return rc ? rc : TSPH_ERR_CUDA;
+      cudaGetLastError();
+      E->conditional = false;
+      E->rebuild_kernels = 0;
     }
-    if (ce != cudaSuccess) return TSPH_ERR_CUDA;
-    E->graph = g;
-    TSPH_CUDA_CHECK(cudaGraphInstantiate(&E->exec, g, 0));
     E->captured_on = s;
   }
   for (int64_t i = 0; i < steps; ++i) TSPH_CUDA_CHECK(cudaGraphLaunch(E->exec, s));
@@ -2394,7 +2467,8 @@ int tsph_engine_step_timed(tsph_engine* E, tsph_stream stream, float* stage_ms, 
 
 int tsph_engine_graph_kernels(tsph_engine* E, int64_t* kernels) {
   if (!E || !kernels) return TSPH_ERR_ARG;
-  *kernels = 0;
+  kernels[0] = 0;
+  kernels[1] = E->conditional ? E->rebuild_kernels : 0;
   if (!E->graph) return TSPH_ERR_ARG;
   size_t count = 0;
   TSPH_CUDA_CHECK(cudaGraphGetNodes(E->graph, nullptr, &count));
@@ -2403,9 +2477,16 @@ int tsph_engine_graph_kernels(tsph_engine* E, int64_t* kernels) {
   int64_t k = 0;
   for (size_t i = 0; i < count; ++i) {
     cudaGraphNodeType t;
-    if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++k;
+    if (cudaGraphNodeGetType(nodes[i], &t) != cudaSuccess) {
+      // the runtime reports no type for a conditional node (cudaErrorUnknown,
+      // not sticky): it is not a kernel, and the error must not reach the
+      // caller's next CUDA check
+      cudaGetLastError();
+      continue;
+    }
+    if (t == cudaGraphNodeTypeKernel) ++k;
   }
-  *kernels = k;
+  kernels[0] = k;
   return TSPH_OK;
 }
 
@@ -2489,6 +2570,7 @@ int tsph_engine_set_batch(tsph_engine* E, int64_t depth) {
 int tsph_engine_destroy(tsph_engine* E) {
   if (!E) return TSPH_OK;
   invalidate_graph(E);
+  if (E->aux) cudaStreamDestroy(E->aux);
   delete E;
   return TSPH_OK;
 }

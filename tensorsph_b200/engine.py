@@ -450,12 +450,13 @@ class BatchEngine:
             self.steps_of[k] += 1
         return {self.STAGES[i]: float(ms[i]) for i in range(n.value)}
 
-    def graph_kernels(self) -> int:
-        """Kernel launches in one captured step (the step graph's kernel nodes)."""
-        k = ctypes.c_int64(0)
-        _lib.check(_lib.lib().tsph_engine_graph_kernels(self._handle, ctypes.byref(k)),
-                   "tsph_engine_graph_kernels")
-        return int(k.value)
+    def graph_kernels(self) -> tuple[int, int]:
+        """Kernel launches of the captured step graph: ``(every step, per list
+        pass that rebuilds)``; the second runs in a conditional node only when
+        some case's lists are rebuilt in that pass."""
+        k = (ctypes.c_int64 * 2)()
+        _lib.check(_lib.lib().tsph_engine_graph_kernels(self._handle, k), "tsph_engine_graph_kernels")
+        return int(k[0]), int(k[1])
 
     # -------------------------------------------------------------- output --
     def diagnostics(self, case_id: int, first: int, count: int) -> torch.Tensor:

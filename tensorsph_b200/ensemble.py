@@ -85,12 +85,13 @@ def run_batched(specs, steps: int, *, warmup: int = 3, block: int = 128, batch: 
     ids = [eng.add(s) for s in specs]
     eng.step(warmup)
     t = _timed_steps(eng, steps)
-    kernels = eng.graph_kernels()
+    kernels, rebuild_kernels = eng.graph_kernels()
     bad = [i for i in ids if eng.status(i)["status"]]
     nf = sum(s.n_fluid for s in specs)
     eng.close()
     return {"cases": len(specs), "fluid": nf, "steps": steps, "seconds": t,
-            "updates_per_s": nf * steps / t, "kernels_per_step": kernels, "failed_cases": bad}
+            "updates_per_s": nf * steps / t, "kernels_per_step": kernels,
+            "kernels_per_rebuild_pass": rebuild_kernels, "failed_cases": bad}
 
 
 def run_plain(specs, steps: int, *, warmup: int = 3, block: int = 128, max_neighbors: int = 64,

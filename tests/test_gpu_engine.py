@@ -161,13 +161,23 @@ def test_engine_shift_runs_and_moves_particles(gpu):
 
 
 def test_engine_graph_and_eager_agree(gpu):
+    """The step graph (its list rebuild in a conditional node that only runs
+    when a case is due) and kernel-by-kernel launches give the same run, with
+    a zero skin so that both list passes rebuild on every step."""
+    from dataclasses import replace
     from tensorsph_b200.engine import DamBreak3DEngine
     cfg, obstacle = small_case()
-    a = DamBreak3DEngine(cfg, obstacle=obstacle, diag_ring=64)
-    b = DamBreak3DEngine(cfg, obstacle=obstacle, diag_ring=64)
-    a.step(5, graph=True)
-    b.step(5, graph=False)
-    assert torch.equal(a.state()[0], b.state()[0])
+    cfg = replace(cfg, pair_skin_factor=0.0)   # any motion rebuilds: both passes of every step
+    a = DamBreak3DEngine(cfg, obstacle=obstacle, shift_every=1, diag_ring=64)
+    b = DamBreak3DEngine(cfg, obstacle=obstacle, shift_every=1, diag_ring=64)
+    a.step(12, graph=True)
+    b.step(12, graph=False)
+    for u, w in zip(a.state(), b.state()):
+        assert torch.equal(u, w)
+    sa, sb = a.status(), b.status()
+    assert sa["rebuilds"] == sb["rebuilds"] > 4
+    every, per_rebuild = a.graph_kernels()
+    assert every > 10 and per_rebuild > 5
     a.close()
     b.close()
 
