@@ -210,6 +210,46 @@ int tsph_threed_accelerations(const tsph_threed_params* prm, const tsph_threed_i
                               int64_t ws_bytes, tsph_stream stream);
 
 /* ------------------------------------------------------------------------ */
+/* 3-D CSF surface tension: tensorsph.threed.csf3.csf_fields3 ("mls"         */
+/* curvature, threed/csf3.py:98-165) and surface_tension_acceleration3       */
+/* (threed/csf3.py:220-238), over the symmetric rows of a pair list.         */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  int64_t n;         /* particles                                          */
+  int64_t dtype;     /* TSPH_F32 or TSPH_F64: every array below            */
+  int64_t periodic;  /* 1: minimum-image separations in box                */
+  double box[3];
+  double h, rho0;    /* smoothing length; rest density (V = m / rho0)      */
+  double sigma;      /* acceleration only: surface tension coefficient     */
+  double cutoff;     /* acceleration only: active if delta_s > cutoff * max */
+} tsph_csf3_params;
+
+typedef struct {
+  const void* pos;          /* (n, 3)                                       */
+  const void* mass;         /* (n)                                          */
+  const void* volume;       /* (n) or null: overrides m / rho0              */
+  const int64_t* rowptr;    /* (n + 1) symmetric rows (tsph_csr_from_pairs) */
+  const uint32_t* entries;  /* neighbour indices (bit 31 ignored)           */
+  void* color;              /* out (n)                                      */
+  void* grad_c;             /* out (n, 3)                                   */
+  void* normal;             /* out (n, 3): -grad c / max(|grad c|, 1e-30)   */
+  void* kappa;              /* out (n): trace(S M^-1), 0 where not valid    */
+  void* delta_s;            /* out (n): |grad c|                            */
+  uint8_t* valid;           /* out (n): |det M| > 1e-6 median |det M|       */
+} tsph_csf3_io;
+
+int64_t tsph_csf3_workspace_bytes(const tsph_csf3_params* prm);
+/* replaces csf_fields3(pos, mass, h, pairs, rho0=, box=, volume=,
+ * curvature="mls") (threed/csf3.py:115-165) */
+int tsph_csf3_fields(const tsph_csf3_params* prm, const tsph_csf3_io* io, void* ws, int64_t ws_bytes,
+                     tsph_stream stream);
+/* replaces surface_tension_acceleration3(state, rho, sigma, cutoff)
+ * (threed/csf3.py:220-238): acc (n, 3) from the fields of tsph_csf3_fields */
+int tsph_csf3_acceleration(const tsph_csf3_params* prm, const void* normal, const void* kappa,
+                           const void* delta_s, const void* rho, void* acc, void* ws, int64_t ws_bytes,
+                           tsph_stream stream);
+
+/* ------------------------------------------------------------------------ */
 /* Particle shifting: particle_shifting.py:93-224 (concentration,            */
 /* concentration_gradient, estimate_reference_concentration, shift_positions)*/
 /* ------------------------------------------------------------------------ */

@@ -60,6 +60,17 @@ class ThreedIO(ctypes.Structure):
                                         "pressure")]
 
 
+class Csf3Params(ctypes.Structure):
+    _fields_ = [(k, c_int64) for k in ("n", "dtype", "periodic")] + \
+               [("box", c_double * 3)] + \
+               [(k, c_double) for k in ("h", "rho0", "sigma", "cutoff")]
+
+
+class Csf3IO(ctypes.Structure):
+    _fields_ = [(k, c_void_p) for k in ("pos", "mass", "volume", "rowptr", "entries", "color",
+                                        "grad_c", "normal", "kappa", "delta_s", "valid")]
+
+
 class ShiftParams(ctypes.Structure):
     _fields_ = [(k, c_int64) for k in ("dim", "dtype", "n")] + \
                [(k, c_double) for k in ("h", "sigma", "magnitude", "cap", "free_surface",
@@ -150,6 +161,10 @@ _SIGNATURES = {
     "tsph_threed_workspace_bytes": (c_int64, [POINTER(ThreedParams)]),
     "tsph_threed_accelerations": (c_int, [POINTER(ThreedParams), POINTER(ThreedIO), c_void_p,
                                           c_int64, c_void_p]),
+    "tsph_csf3_workspace_bytes": (c_int64, [POINTER(Csf3Params)]),
+    "tsph_csf3_fields": (c_int, [POINTER(Csf3Params), POINTER(Csf3IO), c_void_p, c_int64, c_void_p]),
+    "tsph_csf3_acceleration": (c_int, [POINTER(Csf3Params), c_void_p, c_void_p, c_void_p, c_void_p,
+                                       c_void_p, c_void_p, c_int64, c_void_p]),
     "tsph_shift_workspace_bytes": (c_int64, [POINTER(ShiftParams)]),
     "tsph_shift_positions": (c_int, [POINTER(ShiftParams), POINTER(ShiftIO), c_void_p, c_int64,
                                      c_void_p]),

@@ -401,6 +401,61 @@ def csf_cases(ca, di):
     return data
 
 
+def csf3_cases(c3, lc, ns, n3):
+    """3-D CSF fields and acceleration (threed/csf3.py:113-238, "mls"
+    curvature): a lattice ball, a jittered ball in FP64 and FP32, a jittered
+    ball with a volume override and three stray particles (an isolated one
+    and a close pair: degenerate MLS stencils), and the periodic
+    Rayleigh-Plateau column of liquid_column.build_column in its box."""
+    data = {}
+    k = 0
+    dx = 1.0e-3
+    h = 1.3 * dx
+    for dtype, kind in ((torch.float64, "ball"), (torch.float64, "jitter"), (torch.float32, "jitter"),
+                        (torch.float64, "volume"), (torch.float64, "column")):
+        g = torch.Generator().manual_seed(120 + k)
+        box = None
+        if kind == "column":
+            cfg = lc.ColumnConfig(radius=4e-3, dx=dx, kR=0.6971, epsilon=0.02)
+            pos, mass, box = lc.build_column(cfg)
+            pos, mass = pos.to(dtype), mass.to(dtype)
+            h = cfg.h
+            pairs = n3.periodic_pairs(pos, box, 2.0 * h)
+            box = [float(b) for b in box]
+        else:
+            ax = torch.arange(-7, 8, dtype=torch.float64) * dx
+            gx, gy, gz = torch.meshgrid(ax, ax, ax, indexing="ij")
+            pts = torch.stack((gx.reshape(-1), gy.reshape(-1), gz.reshape(-1)), -1)
+            pts = pts[torch.linalg.vector_norm(pts, dim=1) <= 6.2 * dx]
+            if kind != "ball":
+                pts = pts + 0.08 * dx * torch.randn(pts.shape, generator=g, dtype=torch.float64)
+            if kind == "volume":
+                stray = torch.tensor([[0.03, 0.0, 0.0], [0.0, 0.03, 0.0], [0.0, 0.03 + dx, 0.0]],
+                                     dtype=torch.float64)
+                pts = torch.cat((pts, stray))
+            pos = (pts + 0.02).to(dtype)
+            mass = torch.full((pos.shape[0],), 1000.0 * dx ** 3, dtype=dtype)
+            h = 1.3 * dx
+            pairs = ns.cell_linked_pairs(pos, 2.0 * h)
+        rho = (1000.0 * (1.0 + 0.002 * torch.randn((pos.shape[0],), generator=g,
+                                                    dtype=torch.float64))).to(dtype)
+        volume = (mass / rho) if kind == "volume" else None
+        st = c3.csf_fields3(pos, mass, h, pairs, rho0=1000.0, box=box, volume=volume, curvature="mls")
+        acc = c3.surface_tension_acceleration3(st, rho, 0.0728)
+        fields = dict(pos=pos, mass=mass, rho=rho, pairs=pairs, acc=acc, color=st.color,
+                      grad_c=st.grad_c, normal=st.normal, kappa=st.kappa, delta_s=st.delta_s,
+                      valid=st.valid)
+        if volume is not None:
+            fields["volume"] = volume
+        for name, t in fields.items():
+            data[f"c{k}_{name}"] = _np(t)
+        data[f"c{k}_h"] = np.float64(h)
+        data[f"c{k}_box"] = np.asarray(box if box is not None else [0.0, 0.0, 0.0], dtype=np.float64)
+        k += 1
+    data["count"] = np.int64(k)
+    return data
+
+
 def delta_plus_cases(dp):
     """delta_plus_step on a perturbed lattice block in a walled corner (fluid,
     slip walls with normals, gravity, diffusion) and on a free block."""
@@ -505,6 +560,8 @@ def main(src, families=None):
     from tensorsph.threed import solver as sv
     import tensorsph.csf_consistent as ca
     import tensorsph.delta_plus as dp
+    from tensorsph.threed import csf3 as c3
+    from tensorsph.threed import liquid_column as lc
 
     meta = {"torch_version": np.array(torch.__version__)}
     torch.set_num_threads(1)
@@ -520,6 +577,7 @@ def main(src, families=None):
         "shear": lambda: shear_cases(sv),
         "csf": lambda: csf_cases(ca, di),
         "delta_plus": lambda: delta_plus_cases(dp),
+        "csf3": lambda: csf3_cases(c3, lc, ns, n3),
         "config1_run": lambda: config1_run_case(db),
         "dam3d_run": lambda: dam3d_run_case(d3),
     }
