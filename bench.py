@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
     ap.add_argument("--shear-n", type=int, default=64)
     ap.add_argument("--shear-steps", type=int, default=2000)
+    ap.add_argument("--csf3-radius", type=int, default=40, help="column radius in dx (0: no 3-D CSF leg)")
+    ap.add_argument("--csf3-length", type=int, default=200, help="column period in dx")
     return ap.parse_args()
 
 
@@ -257,6 +259,81 @@ def shear_leg(args, dev):
     return out
 
 
+def _column(radius, length, dx, seed, device):
+    """A liquid column along z, periodic in a box of (2R + 8 dx)^2 x L: the
+    lattice points with r <= R, jittered by 0.05 dx (seeded)."""
+    import torch
+    side = 2 * radius + 8
+    box = [side * dx, side * dx, length * dx]
+    g = torch.Generator().manual_seed(seed)
+    a = (torch.arange(side, dtype=torch.float64) + 0.5) * dx
+    X, Y = torch.meshgrid(a, a, indexing="ij")
+    keep = (X - 0.5 * box[0]) ** 2 + (Y - 0.5 * box[1]) ** 2 <= (radius * dx) ** 2
+    xy = torch.stack((X[keep], Y[keep]), -1)
+    z = (torch.arange(length, dtype=torch.float64) + 0.5) * dx
+    pos = torch.cat((xy.repeat(length, 1), z.repeat_interleave(xy.shape[0])[:, None]), 1)
+    pos = pos + 0.05 * dx * (2.0 * torch.rand(pos.shape, generator=g, dtype=torch.float64) - 1.0)
+    pos = torch.remainder(pos, torch.tensor(box, dtype=torch.float64))
+    return pos.to(device), box
+
+
+def csf3_leg(args, dev):
+    """3-D CSF surface tension (csf_fields3 "mls" + surface_tension_acceleration3)
+    on a periodic liquid column (the Rayleigh-Plateau geometry): device time of
+    the drop-in call -- pair rows, fields and acceleration -- per particle, with
+    the oracle's CPU rate on a small column beside it."""
+    import numpy as np
+    import torch
+    from tensorsph_b200.threed.csf3 import csf_fields3, surface_tension_acceleration3
+    from tensorsph_b200.threed.neighbors3 import periodic_pairs
+    dx, h = 1e-3, 1.3e-3
+    pos, box = _column(args.csf3_radius, args.csf3_length, dx, 7, dev)
+    n = pos.shape[0]
+    mass = torch.full((n,), 1000.0 * dx ** 3, dtype=torch.float64, device=dev)
+    rho = torch.full((n,), 1000.0, dtype=torch.float64, device=dev)
+    pairs = periodic_pairs(pos, box, 2.0 * h)
+
+    def call():
+        st = csf_fields3(pos, mass, h, pairs, rho0=1000.0, box=box)
+        return st, surface_tension_acceleration3(st, rho, 0.0728)
+
+    for _ in range(2):
+        st, acc = call()
+    reps = 5
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    start.record()
+    for _ in range(reps):
+        st, acc = call()
+    stop.record()
+    torch.cuda.synchronize(dev)
+    ms = start.elapsed_time(stop) / reps
+    shell = st.surface_mask(0.3) & st.valid
+    off = pos[shell, :2] - torch.tensor(box[:2], dtype=torch.float64, device=dev) * 0.5
+    radial = off / off.norm(dim=1, keepdim=True)
+    a = acc[shell]
+    cos = float(((a[:, :2] * radial).sum(1) / a.norm(dim=1).clamp_min(1e-30)).mean())
+    # CPU: the oracle on a small column (R = 8 dx, period 24 dx)
+    from oracle import csf3 as oc
+    from oracle.neighbors import periodic_pairs as np_periodic_pairs
+    small, sbox = _column(8, 24, dx, 7, "cpu")
+    sp = small.numpy()
+    smass = np.full(sp.shape[0], 1000.0 * dx ** 3)
+    t0 = time.perf_counter()
+    spairs = np_periodic_pairs(sp, np.asarray(sbox), 2.0 * h)
+    sst = oc.csf_fields3(sp, smass, h, spairs, rho0=1000.0, box=np.asarray(sbox))
+    oc.surface_tension_acceleration3(sst, np.full(sp.shape[0], 1000.0), 0.0728)
+    t_cpu = time.perf_counter() - t0
+    return {"workload": f"periodic liquid column R={args.csf3_radius} dx, period {args.csf3_length} dx, "
+                        "dx=1 mm, h=1.3 dx, jitter 0.05 dx (seed 7), FP64",
+            "particles": n, "pairs": int(pairs.shape[0]), "ms_per_call": ms,
+            "particles_per_s": n / (ms / 1e3), "shell_force_cos_to_axis": cos,
+            "valid_fraction": float(st.valid.double().mean()),
+            "cpu_oracle": {"particles_per_s": sp.shape[0] / t_cpu, "particles": sp.shape[0],
+                           "cores": 1, "seconds": t_cpu,
+                           "sample": "R=8 dx, period 24 dx column: pairs + fields + acceleration"}}
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -400,7 +477,8 @@ def main():
     if rank == 0 and world == 1:
         for name, leg, on in (("ensemble", ensemble_leg, args.ensemble_cases > 0),
                               ("serving", serving_leg, args.serve_requests > 0),
-                              ("shear", shear_leg, args.shear_steps > 0)):
+                              ("shear", shear_leg, args.shear_steps > 0),
+                              ("csf3", csf3_leg, args.csf3_radius > 0)):
             if not on:
                 continue
             try:
