@@ -546,6 +546,7 @@ class DamBreak3DRun:
     obstacle_force: list = field(default_factory=list)
     obstacle_impulse: list = field(default_factory=list)
     obstacle_clamps: int = 0
+    snapshots: list = field(default_factory=list)
 
     @property
     def mass_drift(self) -> float:
@@ -620,6 +621,69 @@ def tune_single_case(cfg: DamBreak3DConfig, *, obstacle=None, shift_every: int =
     return {"best": best, "trials": trials}
 
 
+def _sample_steps(steps: int, output_every: int, dt: float):
+    """``(step, elapsed)`` of the reference loops' sample points: every
+    ``output_every`` steps and the last, with ``elapsed`` accumulated step by
+    step as the loops do (dam_break_3d.py:617-705, dam_break.py:365-461)."""
+    out, elapsed = [], 0.0
+    for k in range(steps + 1):
+        if k % output_every == 0 or k == steps:
+            out.append((k, elapsed))
+        elapsed += dt
+    return out
+
+
+def _snapshot_plan(snapshot_times, samples):
+    """``(step, elapsed)`` of each requested snapshot: a target time is taken at
+    the first sample point whose time reaches it (several targets may share
+    one), as dam_break_3d.py:658-664 does."""
+    targets = sorted(float(t) for t in (snapshot_times or []))
+    plan, nxt = [], 0
+    for k, t in samples:
+        while nxt < len(targets) and t >= targets[nxt] - 1.0e-12:
+            plan.append((k, t))
+            nxt += 1
+    return plan
+
+
+class _Snapshots:
+    """Positions and velocities of one case copied to pinned host memory on a
+    side stream: the engine's stream only runs the read kernel, and the copies
+    overlap the steps that follow."""
+
+    def __init__(self, eng, case_id):
+        self.eng, self.case_id = eng, case_id
+        self.side = torch.cuda.Stream(device=eng.device)
+        self.taken = []
+
+    def take(self, elapsed: float):
+        with torch.cuda.stream(self.side):
+            x, v, _, _ = self.eng.read(self.case_id)
+            hx = torch.empty(x.shape, dtype=x.dtype, pin_memory=True)
+            hv = torch.empty(v.shape, dtype=v.dtype, pin_memory=True)
+            hx.copy_(x, non_blocking=True)
+            hv.copy_(v, non_blocking=True)
+        self.taken.append((elapsed, hx, hv))
+
+    def result(self) -> list:
+        self.side.synchronize()
+        return list(self.taken)
+
+
+def _run_with_snapshots(eng, case_id, steps: int, plan) -> list:
+    """Advance ``steps`` steps, taking the planned snapshots on the way."""
+    snaps = _Snapshots(eng, case_id)
+    done = 0
+    for k, t in plan:
+        if k > done:
+            eng.step(k - done)
+            done = k
+        snaps.take(t)
+    if steps > done:
+        eng.step(steps - done)
+    return snaps.result()
+
+
 def run_case(cfg: DamBreak3DConfig, pair_skin_factor: float | None = None, snapshot_times=None,
              seed: int | None = None, *, obstacle=None, shift_every: int = 0,
              max_neighbors: int = 160) -> DamBreak3DRun:
@@ -628,9 +692,10 @@ def run_case(cfg: DamBreak3DConfig, pair_skin_factor: float | None = None, snaps
     Same loop as dam_break_3d.py:569-734: ``cfg.steps`` steps of ``cfg.dt``,
     meters sampled every ``cfg.output_every`` steps and at the end.  The whole
     loop stays on the device; meters come back once at the end.
+    ``snapshot_times`` fills ``run.snapshots`` with ``(time, positions,
+    velocities)`` at the first sample point reaching each time, copied to the
+    host while the loop goes on.
     """
-    if snapshot_times:
-        raise NotImplementedError("snapshot_times is not supported by the device engine")
     if cfg.adaptive_dt:
         raise NotImplementedError("adaptive_dt is not supported by the device engine")
     if pair_skin_factor is not None:
@@ -638,7 +703,8 @@ def run_case(cfg: DamBreak3DConfig, pair_skin_factor: float | None = None, snaps
         cfg = replace(cfg, pair_skin_factor=pair_skin_factor)
     eng = DamBreak3DEngine(cfg, obstacle=obstacle, shift_every=shift_every, seed=seed,
                            max_neighbors=max_neighbors, diag_ring=max(cfg.steps + 2, 2))
-    eng.step(cfg.steps)
+    samples = _sample_steps(cfg.steps, cfg.output_every, cfg.dt)
+    snapshots = _run_with_snapshots(eng, eng.case_id, cfg.steps, _snapshot_plan(snapshot_times, samples))
     with torch.cuda.stream(eng.stream):
         x, v, rho, p = eng.state()
         xs, vs = x.cpu(), v.cpu()
@@ -648,8 +714,8 @@ def run_case(cfg: DamBreak3DConfig, pair_skin_factor: float | None = None, snaps
     eng.step(1)
     with torch.cuda.stream(eng.stream):
         diag = eng.diagnostics(0, cfg.steps + 1).cpu()
-    sample = [k for k in range(cfg.steps + 1) if k % cfg.output_every == 0 or k == cfg.steps]
-    times = [k * cfg.dt for k in sample]
+    sample = [k for k, _ in samples]
+    times = [t for _, t in samples]
     run = DamBreak3DRun(
         times=times, front=[float(diag[k, 2]) for k in sample],
         kinetic_energy=[float(diag[k, 6]) for k in sample],
@@ -661,7 +727,7 @@ def run_case(cfg: DamBreak3DConfig, pair_skin_factor: float | None = None, snaps
         initial_energy=eng.initial_pe, steps_taken=cfg.steps, simulated_time=cfg.steps * cfg.dt,
         obstacle_force=diag[:cfg.steps, 3:6].tolist(),
         obstacle_impulse=[float(diag[cfg.steps - 1, 14])] if cfg.steps else [],
-        obstacle_clamps=int(st["clamps"]))
+        obstacle_clamps=int(st["clamps"]), snapshots=snapshots)
     masses = eng.spec.mass
     run.final_energy = float(0.5 * (masses[:, None] * vs.square()).sum()
                              + (masses * cfg.gravity * xs[:, 1]).sum())
@@ -686,11 +752,13 @@ class DamBreakRun:
     final_positions: torch.Tensor
     steps_taken: int = 0
     simulated_time: float = 0.0
+    snapshots: list = field(default_factory=list)
 
 
-def run_dam_break_2d(cfg, *, max_neighbors: int = 64) -> DamBreakRun:
+def run_dam_break_2d(cfg, *, snapshot_times=None, max_neighbors: int = 64) -> DamBreakRun:
     """Integrate the 2-D dam break (dam_break.py:319-460 with the pair cache,
-    fixed dt, no shifting) on the GPU and return the measured trajectory."""
+    fixed dt, no shifting) on the GPU and return the measured trajectory;
+    ``snapshot_times`` as in ``run_case``."""
     if cfg.adaptive_dt:
         raise NotImplementedError("adaptive_dt is not supported by the device engine")
     if cfg.tvc_every:
@@ -699,7 +767,8 @@ def run_dam_break_2d(cfg, *, max_neighbors: int = 64) -> DamBreakRun:
     eng = BatchEngine(**capacity_for([spec], max_neighbors=max_neighbors,
                                      diag_ring=max(cfg.steps + 1, 1)))
     cid = eng.add(spec)
-    eng.step(cfg.steps)
+    samples = _sample_steps(cfg.steps, cfg.output_every, cfg.dt)
+    snapshots = _run_with_snapshots(eng, cid, cfg.steps, _snapshot_plan(snapshot_times, samples))
     with torch.cuda.stream(eng.stream):
         x = eng.read(cid)[0].cpu()
     # the reference evaluates the right-hand side once more at step == steps
@@ -708,8 +777,8 @@ def run_dam_break_2d(cfg, *, max_neighbors: int = 64) -> DamBreakRun:
     with torch.cuda.stream(eng.stream):
         diag = eng.diagnostics(cid, 0, cfg.steps + 1).cpu()
     st = eng.status(cid)
-    sample = [k for k in range(cfg.steps + 1) if k % cfg.output_every == 0 or k == cfg.steps]
-    run = DamBreakRun(times=[k * cfg.dt for k in sample], front=[float(diag[k, 2]) for k in sample],
+    sample = [k for k, _ in samples]
+    run = DamBreakRun(times=[t for _, t in samples], front=[float(diag[k, 2]) for k in sample],
                       kinetic_energy=[float(diag[k, 6]) for k in sample],
                       potential_energy=[float(diag[k, 7]) for k in sample],
                       mass=float(spec.mass.sum()), escaped=int(st["escapes"]),
@@ -717,6 +786,6 @@ def run_dam_break_2d(cfg, *, max_neighbors: int = 64) -> DamBreakRun:
                       max_speed=max(float(diag[k, 1]) for k in sample),
                       max_density_compression=float(diag[:, 0].max()) / cfg.rho0 - 1.0,
                       final_positions=x, steps_taken=cfg.steps,
-                      simulated_time=cfg.steps * cfg.dt)
+                      simulated_time=cfg.steps * cfg.dt, snapshots=snapshots)
     eng.close()
     return run

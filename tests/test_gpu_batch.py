@@ -178,6 +178,8 @@ def test_run_dam_break_2d_record(gpu):
     assert run.escaped == 0
     assert run.front[0] == pytest.approx(0.19, abs=1e-6)   # FP32 lattice (default dtype)
     assert np.isfinite(run.final_positions.numpy()).all()
+    snap = run_dam_break_2d(cfg, snapshot_times=[cfg.steps * cfg.dt]).snapshots
+    assert len(snap) == 1 and torch.equal(snap[0][1], run.final_positions)
 
 
 def test_served_results_equal_alone(gpu):

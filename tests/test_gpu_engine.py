@@ -193,6 +193,28 @@ def test_run_case_record(gpu):
     assert len(run.obstacle_force) == cfg.steps
 
 
+def test_run_case_snapshots(gpu):
+    """snapshot_times as the reference loop takes them: each target at the
+    first sample point (every output_every steps and the last) whose time
+    reaches it, several targets may share one, targets past the end are not
+    taken; the copies (made on a side stream while the loop goes on) equal
+    the state of a plain run stopped at that step."""
+    from tensorsph_b200.engine import DamBreak3DEngine, run_case
+    cfg, obstacle = small_case()      # 12 steps, samples at 0, 4, 8, 12
+    dt = cfg.dt
+    run = run_case(cfg, obstacle=obstacle, snapshot_times=[0.0, 0.5 * dt, 4 * dt, 9.5 * dt, 100.0])
+    assert [round(t / dt, 9) for t, _, _ in run.snapshots] == [0, 4, 4, 12]
+    assert torch.equal(run.snapshots[-1][1], run.final_positions)
+    eng = DamBreak3DEngine(cfg, obstacle=obstacle, diag_ring=64)
+    eng.step(4)
+    x, v, _, _ = (t.cpu() for t in eng.state())
+    eng.close()
+    for _, sx, sv in run.snapshots[1:3]:
+        assert torch.equal(sx, x) and torch.equal(sv, v)
+    assert torch.equal(run.snapshots[0][1], run_case(cfg, obstacle=obstacle,
+                                                     snapshot_times=[0.0]).snapshots[0][1])
+
+
 def test_run_case_follows_reference_run(golden, gpu):
     """The small 3-D dam break (Molteni diffusion, wall friction, 40 steps) on
     the device against the reference's own FP64 ``dam_break_3d.run_case``."""
