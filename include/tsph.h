@@ -250,6 +250,48 @@ int tsph_csf3_acceleration(const tsph_csf3_params* prm, const void* normal, cons
                            tsph_stream stream);
 
 /* ------------------------------------------------------------------------ */
+/* Transport-velocity correction: kernel_gradient_integral and              */
+/* transport_velocity_correction (transport_velocity_correction.py:285-513) */
+/* over the symmetric rows of a pair list; fluid particles first.           */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  int64_t n_total, n_fluid;  /* particles (fluid first, walls last)          */
+  int64_t dim;               /* 1, 2 or 3: the spline's normalisation         */
+  int64_t dtype;             /* TSPH_F32 or TSPH_F64                          */
+  int64_t has_ratio;         /* 1: per-fluid-particle h_ratio given           */
+  int64_t limiter;           /* 0 none, 1 TruncatedLinear(slope), 2 given     */
+  int64_t has_scope_tol, has_max_shift;
+  double h;                  /* kernel smoothing length                       */
+  double h_ref;              /* reference length of the displacement          */
+  double h_ratio_scale;      /* h / h_ref: the ratio seen by the kernel       */
+  double wall_factor;        /* weight of a wall neighbour (2 upstream)       */
+  double alpha, slope, scope_tol, max_shift;
+} tsph_tvc_params;
+
+typedef struct {
+  const void* pos;           /* (n_total, dim)                                */
+  const void* volume;        /* (n_total) m / rho                             */
+  const void* h_ratio;       /* (n_fluid) or null                             */
+  const void* correction;    /* (n_total) kernel correction C or null (1)     */
+  const int64_t* rowptr;     /* (n_total + 1) symmetric rows                  */
+  const uint32_t* entries;
+  void* gradient;            /* (n_fluid, dim): out of _gradient, in of _shift */
+  void* squared;             /* (n_fluid) |g|^2: same                          */
+  const void* limiter_in;    /* (n_fluid) factors when limiter == 2           */
+  const uint8_t* active;     /* (n_fluid) scope mask or null                  */
+  void* limiter_out;         /* out (n_fluid)                                 */
+  void* shift;               /* out (n_fluid, dim)                            */
+  void* clipped;             /* out: uint64 count of rows scaled to max_shift */
+} tsph_tvc_io;
+
+/* replaces kernel_gradient_integral (transport_velocity_correction.py:285-410):
+ * gradient and squared */
+int tsph_tvc_gradient(const tsph_tvc_params* prm, const tsph_tvc_io* io, tsph_stream stream);
+/* replaces the displacement of transport_velocity_correction
+ * (transport_velocity_correction.py:413-513): limiter, shift, clipped count */
+int tsph_tvc_shift(const tsph_tvc_params* prm, const tsph_tvc_io* io, tsph_stream stream);
+
+/* ------------------------------------------------------------------------ */
 /* Particle shifting: particle_shifting.py:93-224 (concentration,            */
 /* concentration_gradient, estimate_reference_concentration, shift_positions)*/
 /* ------------------------------------------------------------------------ */

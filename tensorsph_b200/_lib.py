@@ -71,6 +71,19 @@ class Csf3IO(ctypes.Structure):
                                         "grad_c", "normal", "kappa", "delta_s", "valid")]
 
 
+class TvcParams(ctypes.Structure):
+    _fields_ = [(k, c_int64) for k in ("n_total", "n_fluid", "dim", "dtype", "has_ratio", "limiter",
+                                       "has_scope_tol", "has_max_shift")] + \
+               [(k, c_double) for k in ("h", "h_ref", "h_ratio_scale", "wall_factor", "alpha", "slope",
+                                        "scope_tol", "max_shift")]
+
+
+class TvcIO(ctypes.Structure):
+    _fields_ = [(k, c_void_p) for k in ("pos", "volume", "h_ratio", "correction", "rowptr", "entries",
+                                        "gradient", "squared", "limiter_in", "active", "limiter_out",
+                                        "shift", "clipped")]
+
+
 class ShiftParams(ctypes.Structure):
     _fields_ = [(k, c_int64) for k in ("dim", "dtype", "n")] + \
                [(k, c_double) for k in ("h", "sigma", "magnitude", "cap", "free_surface",
@@ -161,6 +174,8 @@ _SIGNATURES = {
     "tsph_threed_workspace_bytes": (c_int64, [POINTER(ThreedParams)]),
     "tsph_threed_accelerations": (c_int, [POINTER(ThreedParams), POINTER(ThreedIO), c_void_p,
                                           c_int64, c_void_p]),
+    "tsph_tvc_gradient": (c_int, [POINTER(TvcParams), POINTER(TvcIO), c_void_p]),
+    "tsph_tvc_shift": (c_int, [POINTER(TvcParams), POINTER(TvcIO), c_void_p]),
     "tsph_csf3_workspace_bytes": (c_int64, [POINTER(Csf3Params)]),
     "tsph_csf3_fields": (c_int, [POINTER(Csf3Params), POINTER(Csf3IO), c_void_p, c_int64, c_void_p]),
     "tsph_csf3_acceleration": (c_int, [POINTER(Csf3Params), c_void_p, c_void_p, c_void_p, c_void_p,

@@ -456,6 +456,81 @@ def csf3_cases(c3, lc, ns, n3):
     return data
 
 
+def tvc_cases(tv, ns):
+    """transport_velocity_correction (transport_velocity_correction.py:285-513)
+    on jittered fluid blocks with wall layers: 2-D and 3-D, FP64 and FP32, no
+    limiter and TruncatedLinear, with max_shift, an active scope, scope_tol and
+    a per-particle h_ratio."""
+    data = {}
+    opts = [
+        ("2d", torch.float64, dict()),
+        ("2d", torch.float32, dict()),
+        ("2d", torch.float64, dict(limiter="tl", max_shift=2e-5, scope_tol=0.5)),
+        ("2d", torch.float64, dict(active=True, alpha=0.2, h_ref=0.0031)),
+        ("2d", torch.float64, dict(h_ratio=True)),
+        ("3d", torch.float64, dict()),
+        ("3d", torch.float64, dict(limiter="tl")),
+    ]
+    for k, (kind, dtype, o) in enumerate(opts):
+        g = torch.Generator().manual_seed(200 + k)
+        dx = 0.002
+        h = 1.3 * dx
+        dim = 2 if kind == "2d" else 3
+        nx = 14 if dim == 2 else 8
+        ax = torch.arange(nx, dtype=torch.float64) * dx + 0.5 * dx
+        grids = torch.meshgrid(*([ax] * dim), indexing="ij")
+        fluid = torch.stack([t.reshape(-1) for t in grids], -1)
+        fluid = fluid + 0.08 * dx * torch.randn(fluid.shape, generator=g, dtype=torch.float64)
+        # three wall layers under the block (y < 0)
+        wl = torch.arange(-3, 0, dtype=torch.float64) * dx + 0.5 * dx
+        wx = torch.arange(-3, nx + 3, dtype=torch.float64) * dx + 0.5 * dx
+        if dim == 2:
+            WX, WY = torch.meshgrid(wx, wl, indexing="ij")
+            wall = torch.stack((WX.reshape(-1), WY.reshape(-1)), -1)
+        else:
+            WX, WY, WZ = torch.meshgrid(wx, wl, wx, indexing="ij")
+            wall = torch.stack((WX.reshape(-1), WY.reshape(-1), WZ.reshape(-1)), -1)
+        pos = torch.cat((fluid, wall)).to(dtype)
+        nf, nw = fluid.shape[0], wall.shape[0]
+        volume = (dx ** dim * (1.0 + 0.01 * torch.randn(pos.shape[0], generator=g,
+                                                       dtype=torch.float64))).to(dtype)
+        kw = dict(wall_count=nw)
+        search_h = h
+        if o.get("h_ratio"):
+            ratio = (1.0 + 0.3 * torch.rand(nf, generator=g, dtype=torch.float64)).to(dtype)
+            ratio[::7] = 0.8
+            kw["h_ratio"] = ratio
+            search_h = h / 0.8
+        pairs = ns.cell_linked_pairs(pos, 2.0 * search_h)
+        if o.get("limiter") == "tl":
+            kw["limiter"] = tv.truncated_linear(100.0)
+        for name in ("max_shift", "scope_tol", "alpha", "h_ref"):
+            if name in o:
+                kw[name] = o[name]
+        if o.get("active"):
+            kw["active"] = torch.arange(nf) % 3 != 0
+        res = tv.transport_velocity_correction(pos, volume, h, pairs=pairs, **kw)
+        data[f"c{k}_pos"] = _np(pos)
+        data[f"c{k}_volume"] = _np(volume)
+        data[f"c{k}_pairs"] = _np(pairs)
+        data[f"c{k}_h"] = np.float64(h)
+        data[f"c{k}_n_wall"] = np.int64(nw)
+        data[f"c{k}_opts"] = np.array(repr(sorted((a, b) for a, b in o.items())))
+        for name in ("max_shift", "scope_tol", "alpha", "h_ref"):
+            if name in o:
+                data[f"c{k}_{name}"] = np.float64(o[name])
+        data[f"c{k}_limiter_tl"] = np.int64(o.get("limiter") == "tl")
+        if o.get("active"):
+            data[f"c{k}_active"] = _np(kw["active"])
+        if o.get("h_ratio"):
+            data[f"c{k}_h_ratio"] = _np(kw["h_ratio"])
+        for name in ("gradient_integral", "shift", "squared_norm", "limiter"):
+            data[f"c{k}_{name}"] = _np(getattr(res, name))
+        data[f"c{k}_clipped"] = np.float64(res.clipped)
+    data["count"] = np.int64(len(opts))
+    return data
+
+
 def delta_plus_cases(dp):
     """delta_plus_step on a perturbed lattice block in a walled corner (fluid,
     slip walls with normals, gravity, diffusion) and on a free block."""
@@ -562,6 +637,7 @@ def main(src, families=None):
     import tensorsph.delta_plus as dp
     from tensorsph.threed import csf3 as c3
     from tensorsph.threed import liquid_column as lc
+    import tensorsph.transport_velocity_correction as tv
 
     meta = {"torch_version": np.array(torch.__version__)}
     torch.set_num_threads(1)
@@ -578,6 +654,7 @@ def main(src, families=None):
         "csf": lambda: csf_cases(ca, di),
         "delta_plus": lambda: delta_plus_cases(dp),
         "csf3": lambda: csf3_cases(c3, lc, ns, n3),
+        "tvc": lambda: tvc_cases(tv, ns),
         "config1_run": lambda: config1_run_case(db),
         "dam3d_run": lambda: dam3d_run_case(d3),
     }

@@ -91,6 +91,8 @@ def test_struct_sizes_match_header():
     assert ctypes.sizeof(_lib.CaseParams) == 8 * (6 + 11 + 3 + 1 + 3 + 3 + 1 + 4 + 3 + 3 + 2)
     assert ctypes.sizeof(_lib.Csf3Params) == 8 * (3 + 3 + 4)
     assert ctypes.sizeof(_lib.Csf3IO) == 8 * 11
+    assert ctypes.sizeof(_lib.TvcParams) == 8 * (8 + 8)
+    assert ctypes.sizeof(_lib.TvcIO) == 8 * 13
 
 
 def test_product_path_fails_loudly_without_gpu():

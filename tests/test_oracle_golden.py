@@ -234,6 +234,37 @@ def test_csf3_oracle_matches_reference(golden):
             assert np.abs(st[name] - r).max() <= tol * max(np.abs(r).max(), 1.0), (k, name)
 
 
+def _tvc_kwargs(g, k):
+    kw = dict(wall_count=int(g[f"c{k}_n_wall"]))
+    for name in ("max_shift", "scope_tol", "alpha", "h_ref"):
+        if f"c{k}_{name}" in g:
+            kw[name] = float(g[f"c{k}_{name}"])
+    if f"c{k}_active" in g:
+        kw["active"] = g[f"c{k}_active"]
+    if f"c{k}_h_ratio" in g:
+        kw["h_ratio"] = g[f"c{k}_h_ratio"]
+    return kw
+
+
+def test_tvc_oracle_matches_reference(golden):
+    """The oracle's transport-velocity correction against the reference's own
+    output (tests/golden/tvc.npz: 2-D and 3-D, FP64 and FP32, limiters,
+    max_shift, active scope, scope_tol, per-particle h_ratio)."""
+    from oracle import tvc
+    g = golden("tvc")
+    for k in range(int(g["count"])):
+        kw = _tvc_kwargs(g, k)
+        if int(g[f"c{k}_limiter_tl"]):
+            kw["slope"] = 100.0
+        pos = g[f"c{k}_pos"]
+        r = tvc.transport_velocity_correction(pos, g[f"c{k}_volume"], float(g[f"c{k}_h"]), g[f"c{k}_pairs"], **kw)
+        tol = 1e-13 if pos.dtype == np.float64 else 2e-6
+        for name in ("gradient_integral", "shift", "squared_norm", "limiter"):
+            ref = g[f"c{k}_{name}"]
+            assert np.abs(r[name] - ref).max() <= tol * np.abs(ref).max(), (k, name)
+        assert r["clipped"] == float(g[f"c{k}_clipped"]), k
+
+
 def test_delta_plus_oracle_matches_reference(golden):
     """The oracle's delta-plus step against the reference's own output
     (tests/golden/delta_plus.npz: a walled corner and a free block)."""
