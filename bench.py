@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--shear-steps", type=int, default=2000)
     ap.add_argument("--csf3-radius", type=int, default=40, help="column radius in dx (0: no 3-D CSF leg)")
     ap.add_argument("--csf3-length", type=int, default=200, help="column period in dx")
+    ap.add_argument("--tvc-n", type=int, default=100, help="fluid block edge in dx (0: no TVC leg)")
     return ap.parse_args()
 
 
@@ -334,6 +335,63 @@ def csf3_leg(args, dev):
                            "sample": "R=8 dx, period 24 dx column: pairs + fields + acceleration"}}
 
 
+def tvc_leg(args, dev):
+    """Transport-velocity correction (transport_velocity_correction, no limiter)
+    on a jittered n^3 fluid block over three wall layers: device time of the
+    drop-in call -- pair rows, gradient integral and displacement -- per fluid
+    particle, with the oracle's CPU rate on a small block beside it."""
+    import numpy as np
+    import torch
+    from tensorsph_b200.neighbor_search import cell_linked_pairs
+    from tensorsph_b200.transport_velocity_correction import transport_velocity_correction
+
+    def block(n, seed, device):
+        dx = 0.002
+        g = torch.Generator().manual_seed(seed)
+        ax = (torch.arange(n, dtype=torch.float64) + 0.5) * dx
+        X, Y, Z = torch.meshgrid(ax, ax, ax, indexing="ij")
+        fluid = torch.stack((X.reshape(-1), Y.reshape(-1), Z.reshape(-1)), 1)
+        fluid = fluid + 0.08 * dx * torch.randn(fluid.shape, generator=g, dtype=torch.float64)
+        wx = (torch.arange(-3, n + 3, dtype=torch.float64) + 0.5) * dx
+        wl = (torch.arange(-3, 0, dtype=torch.float64) + 0.5) * dx
+        WX, WY, WZ = torch.meshgrid(wx, wl, wx, indexing="ij")
+        wall = torch.stack((WX.reshape(-1), WY.reshape(-1), WZ.reshape(-1)), 1)
+        pos = torch.cat((fluid, wall)).to(device)
+        vol = torch.full((pos.shape[0],), dx ** 3, dtype=torch.float64, device=device)
+        return pos, vol, wall.shape[0], 1.3 * dx
+
+    pos, vol, nw, h = block(args.tvc_n, 11, dev)
+    pairs = cell_linked_pairs(pos, 2.0 * h)
+    call = lambda: transport_velocity_correction(pos, vol, h, pairs=pairs, wall_count=nw, max_shift=0.05 * h)
+    for _ in range(2):
+        res = call()
+    reps = 5
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    start.record()
+    for _ in range(reps):
+        res = call()
+    stop.record()
+    torch.cuda.synchronize(dev)
+    ms = start.elapsed_time(stop) / reps
+    nf = pos.shape[0] - nw
+    from oracle import tvc as otv
+    from oracle.neighbors import cell_linked_pairs as np_pairs
+    spos, svol, snw, sh = block(16, 11, "cpu")
+    sp, sv = spos.numpy(), svol.numpy()
+    t0 = time.perf_counter()
+    otv.transport_velocity_correction(sp, sv, sh, np_pairs(sp, 2.0 * sh), wall_count=snw, max_shift=0.05 * sh)
+    t_cpu = time.perf_counter() - t0
+    return {"workload": f"{args.tvc_n}^3 jittered fluid block (0.08 dx, seed 11) over 3 wall layers, dx=2 mm, "
+                        "h=1.3 dx, no limiter, max_shift 0.05 h, FP64",
+            "fluid_particles": nf, "wall_particles": nw, "pairs": int(pairs.shape[0]), "ms_per_call": ms,
+            "fluid_particles_per_s": nf / (ms / 1e3), "clipped_fraction": res.clipped,
+            "max_shift_over_h": res.max_shift / h,
+            "cpu_oracle": {"fluid_particles_per_s": (spos.shape[0] - snw) / t_cpu,
+                           "fluid_particles": spos.shape[0] - snw, "cores": 1, "seconds": t_cpu,
+                           "sample": "16^3 block: pairs + gradient integral + displacement"}}
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -436,7 +494,8 @@ def main():
     if not args.no_e2e:
         x, m, w, n_ob = host
         pinned = tuple(t.pin_memory() for t in (x, m, w))
-        rows = torch.empty((args.steps, 16), dtype=torch.float64).pin_memory()
+        from tensorsph_b200.engine import DIAG_FIELDS
+        rows = torch.empty((args.steps, len(DIAG_FIELDS)), dtype=torch.float64).pin_memory()
         final = torch.empty((nf, 3), dtype=torch.float64).pin_memory()
         barrier()
         torch.cuda.synchronize(dev)
@@ -462,7 +521,7 @@ def main():
         state_bytes = (x.numel() + m.numel() + w.numel()) * 8
         e2e = {"value": whole_job_rate(nf, args.steps, world, t_e2e), "unit": "fluid particle-updates/s",
                "h2d_bytes_per_step": state_bytes / args.steps,
-               "d2h_bytes_per_step": 16 * 8 + nf * 3 * 8 / args.steps,
+               "d2h_bytes_per_step": rows.shape[1] * 8 + nf * 3 * 8 / args.steps,
                "scope": "engine creation from pinned host lattices + K steps with a per-step "
                         "meter-row read + final positions read, wall clock"}
 
@@ -478,7 +537,8 @@ def main():
         for name, leg, on in (("ensemble", ensemble_leg, args.ensemble_cases > 0),
                               ("serving", serving_leg, args.serve_requests > 0),
                               ("shear", shear_leg, args.shear_steps > 0),
-                              ("csf3", csf3_leg, args.csf3_radius > 0)):
+                              ("csf3", csf3_leg, args.csf3_radius > 0),
+                              ("tvc", tvc_leg, args.tvc_n > 0)):
             if not on:
                 continue
             try:

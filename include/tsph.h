@@ -453,6 +453,12 @@ typedef struct {
   double periodic_box;                 /* > 0: triply periodic cube [0, L)^3 (3-D, no */
                                        /* walls); L is snapped to n cells of an FP32 */
                                        /* edge (relative change < 1e-7)              */
+  int64_t tvc_every;                   /* transport-velocity correction every k steps */
+                                       /* after the update (3-D, no obstacle, no     */
+                                       /* shifting); 0 disables                      */
+  double tvc_alpha;                    /* its coefficient (displacement alpha h^2 g)  */
+  double tvc_scope_tol;                /* >= 0: only where |g| h <= tol; < 0: all     */
+  double tvc_max_shift;                /* >= 0: clip |shift| to this length; < 0: off */
 } tsph_case_params;
 
 typedef struct tsph_engine tsph_engine; /* opaque host handle */
@@ -496,10 +502,12 @@ int tsph_engine_graph_kernels(tsph_engine* engine, int64_t* kernels);
  * FP64 (device, nullable). */
 int tsph_engine_read(tsph_engine* engine, int64_t case_id, double* x, double* v, double* rho,
                      double* p, tsph_stream stream);
-/* Copy `count` per-step meter rows of one case (16 doubles each: max rho,
+/* Copy `count` per-step meter rows of one case (20 doubles each: max rho,
  * max |v|, front x, obstacle force xyz, kinetic and potential energy,
  * escapes, clamps, rebuilds, longest row, step, status, obstacle impulse x,
- * c_ref) starting at its step `first` into `out` (device). */
+ * c_ref, and the step's transport-velocity correction: max |shift|,
+ * sum |shift|, kept and clipped counts) starting at its step `first` into
+ * `out` (device). */
 int tsph_engine_diag(tsph_engine* engine, int64_t case_id, double* out, int64_t first,
                      int64_t count, tsph_stream stream);
 /* Counters of one case (escapes, clamps, rebuilds, steps, longest row, -,

@@ -46,7 +46,7 @@ namespace {
 
 constexpr int kBlock = 128;     // default threads per block of the pair kernels
 constexpr int kMaxBlock = 256;  // largest block the kernels are built for
-constexpr int kDiag = 16;
+constexpr int kDiag = 20;
 constexpr int kBatch = 4;
 constexpr int kCodeBits = 6;                               // cell-offset code bits of a row entry
 constexpr uint32_t kCodeMask = (1u << kCodeBits) - 1;
@@ -70,6 +70,11 @@ struct CaseDev {
   double sigma_st, h_d, inv_h_d, sigma2d_d, vol_scale;  // CSF: sigma, h, 1/h, 10/(7 pi h^2), 1/rho0
   double stencil2;         // (4h)^2
   double fit_rc2;          // (4h + skin)^2, the fit rows' list cutoff
+  int tvc_every;           // transport-velocity correction every k steps (0: off)
+  float tvc_coef;          // alpha h^2
+  float tvc_wall_vol;      // wall volume m_w / rho0
+  float tvc_tol;           // scope |g| h <= tol (< 0: every particle)
+  float tvc_max;           // displacement clip (< 0: none)
 };
 
 struct CaseCtl {
@@ -87,6 +92,10 @@ struct CaseCtl {
   long long csf_rank;
   unsigned long long csf_fmax;
   double csf_med;
+  int tvc_now, tvc_pad;
+  unsigned long long tvc_max;       // largest |shift| of this step's correction (double bits)
+  double tvc_sum;                   // sum of |shift|
+  unsigned long long tvc_kept, tvc_clipped;
 };
 
 struct Dev {
@@ -126,6 +135,7 @@ struct Dev {
   float2* st;        // CSF: surface-tension acceleration
   unsigned int* csf_hist;  // [n_slots][256] median-select histograms
   int has_csf, maxfit;
+  int has_tvc, tvc_pad_;
   uint32_t* nbr4;    // CSF fit rows (fluid neighbours within 4h + skin), k-major over NF
   int32_t* cnt4;
   uint32_t* nbr;
@@ -1287,6 +1297,23 @@ __global__ void k_csf_clear(Dev e) {
 
 // Semi-implicit Euler, box and obstacle clamps, per-case meters (of the state
 // before the update, as the reference samples them) and the skin displacement.
+// Keep a particle in the box [0, box_hi] and zero the velocity components
+// that crossed it by more than the tolerance (dam_break_3d.py:429-452); true
+// when it escaped.
+__device__ __forceinline__ bool clamp_box(const CaseDev& C, double& px, double& py, double& pz, double& vx,
+                                          double& vy, double& vz) {
+  const bool ox = px < -C.tol || px > C.box_hi[0] + C.tol;
+  const bool oy = py < -C.tol || py > C.box_hi[1] + C.tol;
+  const bool oz = pz < -C.tol || pz > C.box_hi[2] + C.tol;
+  px = px < 0.0 ? 0.0 : (px > C.box_hi[0] ? C.box_hi[0] : px);
+  py = py < 0.0 ? 0.0 : (py > C.box_hi[1] ? C.box_hi[1] : py);
+  pz = pz < 0.0 ? 0.0 : (pz > C.box_hi[2] ? C.box_hi[2] : pz);
+  vx = ox ? 0.0 : vx;
+  vy = oy ? 0.0 : vy;
+  vz = oz ? 0.0 : vz;
+  return ox || oy || oz;
+}
+
 template <bool kOne>
 __global__ void __launch_bounds__(kMaxBlock) k_integrate(const __grid_constant__ Dev e) {
   __shared__ double red[kMaxBlock / 32];
@@ -1323,17 +1350,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_integrate(const __grid_constant__
       px = px >= L ? px - L : px;
       py = py >= L ? py - L : py;
       pz = pz >= L ? pz - L : pz;
-    } else {
-      const bool ox = px < -C.tol || px > C.box_hi[0] + C.tol;
-      const bool oy = py < -C.tol || py > C.box_hi[1] + C.tol;
-      const bool oz = pz < -C.tol || pz > C.box_hi[2] + C.tol;
-      px = px < 0.0 ? 0.0 : (px > C.box_hi[0] ? C.box_hi[0] : px);
-      py = py < 0.0 ? 0.0 : (py > C.box_hi[1] ? C.box_hi[1] : py);
-      pz = pz < 0.0 ? 0.0 : (pz > C.box_hi[2] ? C.box_hi[2] : pz);
-      vx = ox ? 0.0 : vx;
-      vy = oy ? 0.0 : vy;
-      vz = oz ? 0.0 : vz;
-      if (ox || oy || oz) atomicAdd(&e.ctl[c].escapes, 1ull);
+    } else if (clamp_box(C, px, py, pz, vx, vy, vz)) {
+      atomicAdd(&e.ctl[c].escapes, 1ull);
     }
     if (C.has_ob && px > C.ob_lo[0] && px < C.ob_hi[0] && py > C.ob_lo[1] && py < C.ob_hi[1] &&
         pz > C.ob_lo[2] && pz < C.ob_hi[2]) {
@@ -1436,6 +1454,107 @@ __global__ void k_finalize(Dev e) {
   t.steps = step + 1;
   t.shift_now = C.shift_every > 0 && step > 0 && (step % static_cast<unsigned long long>(C.shift_every)) == 0;
   t.shift_done = 0;
+  t.tvc_now = C.tvc_every > 0 && step > 0 && (step % static_cast<unsigned long long>(C.tvc_every)) == 0;
+  t.tvc_max = 0;
+  t.tvc_sum = 0.0;
+  t.tvc_kept = t.tvc_clipped = 0;
+  row[16] = row[17] = row[18] = row[19] = 0.0;
+}
+
+// -------------------------------------------- transport-velocity correction ---
+// After the update of a step whose case asks for it (dam_break_3d.py:675-704):
+//   g_a = -2 sum_b V_b grad_a W_ab over the step's rows (fluid V = m / rho of
+//   this step, wall V = m_w / rho0), shift = alpha h^2 g, kept where
+//   |g| h <= tol, clipped to tvc_max, added to the position, then the box
+//   clamp; the displacement counts toward the next skin test.
+
+__global__ void __launch_bounds__(kMaxBlock) k_tvc_gradient(Dev e) {
+  const int NF = e.NF;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    const int c = e.cid[a];
+    if (!e.ctl[c].tvc_now) continue;
+    const CaseDev& C = e.cases[c];
+    const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, wvol = C.tvc_wall_vol;
+    const float4 la = e.lp[a];
+    CSum<float> gx, gy, gz;
+    walk_row(e, a, [&](const uint32_t* ent) {
+      float px = 0.f, py = 0.f, pz = 0.f;
+#pragma unroll
+      for (int j = 0; j < kBatch; ++j) {
+        const int b = static_cast<int>(ent[j] >> kCodeBits);
+        const float4 lb = e.lp[b];
+        // fluid: this step's m / rho; wall: m_w / rho0; the null row: 0
+        const float vb = b < NF ? e.vb[b].w : (b < e.null_row ? wvol : 0.f);
+        const float3 d = sep(la, lb, ent[j], cellf);
+        const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+        const Radial R = radial(r2, inv_h);
+        const float w = 2.f * vb * (sigma * dshape(R.q) * inv_h * R.inv_r);
+        px += w * d.x;
+        py += w * d.y;
+        pz += w * d.z;
+      }
+      gx.add(px);
+      gy.add(py);
+      gz.add(pz);
+    });
+    const float x = -gx.value(), y = -gy.value(), z = -gz.value();
+    e.gradc[a] = make_float4(x, y, z, x * x + y * y + z * z);
+  }
+}
+
+__global__ void __launch_bounds__(kMaxBlock) k_tvc_apply(Dev e) {
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    const int c = e.cid[a];
+    CaseCtl& t = e.ctl[c];
+    if (!t.tvc_now) continue;
+    const CaseDev& C = e.cases[c];
+    const float4 g = e.gradc[a];
+    float sx = C.tvc_coef * g.x, sy = C.tvc_coef * g.y, sz = C.tvc_coef * g.z;
+    bool kept = true;
+    if (C.tvc_tol >= 0.f && !(sqrtf(g.w) * static_cast<float>(C.h_d) <= C.tvc_tol)) {
+      kept = false;
+      sx = sy = sz = 0.f;
+    }
+    float n = sqrtf(sx * sx + sy * sy + sz * sz);
+    if (C.tvc_max >= 0.f && n > C.tvc_max) {
+      const float k = C.tvc_max / (n > 1e-30f ? n : 1e-30f);
+      sx *= k;
+      sy *= k;
+      sz *= k;
+      n = sqrtf(sx * sx + sy * sy + sz * sz);
+      atomicAdd(&t.tvc_clipped, 1ull);
+    }
+    if (kept) atomicAdd(&t.tvc_kept, 1ull);
+    double4 x = ld4(e.pos, a);
+    double4 v = ld4(e.vel, a);
+    x.x += sx;
+    x.y += sy;
+    x.z += sz;
+    if (clamp_box(C, x.x, x.y, x.z, v.x, v.y, v.z)) atomicAdd(&t.escapes, 1ull);
+    st4(e.pos, a, x);
+    st4(e.vel, a, v);
+    e.lp[a] = local_of(C, e.home[a] - C.key_off, x.x, x.y, x.z, x.w);
+    const double4 an = ld4(e.anchor, a);
+    const double ex = x.x - an.x, ey = x.y - an.y, ez = x.z - an.z;
+    atomic_max_nonneg(&t.disp[0], sqrt(ex * ex + ey * ey + ez * ez));
+    atomic_max_nonneg(&t.tvc_max, static_cast<double>(n));
+    atomicAdd(&t.tvc_sum, static_cast<double>(n));
+  }
+}
+
+// The correction's log in columns 16-19 of the step's meter row: max |shift|,
+// sum |shift|, kept and clipped counts.
+__global__ void k_tvc_finish(Dev e) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= e.n_slots) return;
+  CaseCtl& t = e.ctl[c];
+  if (!t.active || !t.tvc_now) return;
+  const unsigned long long step = t.steps - 1;
+  double* row = e.diag + (static_cast<int64_t>(c) * e.diag_ring + static_cast<int64_t>(step % e.diag_ring)) * kDiag;
+  row[16] = __longlong_as_double(static_cast<long long>(t.tvc_max));
+  row[17] = t.tvc_sum;
+  row[18] = static_cast<double>(t.tvc_kept);
+  row[19] = static_cast<double>(t.tvc_clipped);
 }
 
 // ------------------------------------------------------------- shifting ---
@@ -1906,7 +2025,11 @@ void batch_changed(tsph_engine* E) {
   Dev& d = E->d;
   d.shift_slot = shifting(E) ? E->order[0].slot : 0;
   d.has_csf = 0;
-  for (const CaseHost& c : E->order) d.has_csf |= c.dev.csf;
+  d.has_tvc = 0;
+  for (const CaseHost& c : E->order) {
+    d.has_csf |= c.dev.csf;
+    d.has_tvc |= c.dev.tvc_every > 0 ? 1 : 0;
+  }
   if (E->order.size() == 1) {
     d.one = E->order[0].dev;
     d.one_slot = E->order[0].slot;
@@ -2045,6 +2168,12 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr, b
   mark();
   (one ? k_integrate<true> : k_integrate<false>)<<<static_cast<unsigned>((d.nf + B - 1) / B), B, 0, s>>>(d);
   k_finalize<<<gc, 128, 0, s>>>(d);
+  if (d.has_tvc) {
+    // the correction reads the rows of this step (the pass-0 lists)
+    k_tvc_gradient<<<g, B, 0, s>>>(d);
+    k_tvc_apply<<<g, B, 0, s>>>(d);
+    k_tvc_finish<<<gc, 128, 0, s>>>(d);
+  }
   TSPH_LAUNCH_CHECK();
   mark();
   if (shifting(E)) {
@@ -2142,6 +2271,11 @@ CaseDev make_case_dev(const tsph_case_params& p, int64_t* ncells) {
   c.stencil_cells = static_cast<int>(std::ceil((4.0 * p.h + p.skin) / cell));
   c.stencil2 = 16.0 * p.h * p.h;
   c.fit_rc2 = (4.0 * p.h + p.skin) * (4.0 * p.h + p.skin);
+  c.tvc_every = static_cast<int>(p.tvc_every);
+  c.tvc_coef = static_cast<float>(p.tvc_alpha * p.h * p.h);
+  c.tvc_wall_vol = static_cast<float>(p.wall_mass / p.rho0);
+  c.tvc_tol = static_cast<float>(p.tvc_scope_tol);
+  c.tvc_max = static_cast<float>(p.tvc_max_shift);
   return c;
 }
 
@@ -2157,6 +2291,11 @@ bool case_params_ok(const tsph_case_params* p) {
       return false;
   if (p->periodic_box < 0.0 || (p->periodic_box > 0.0 && (p->dim != 3 || p->n_wall != 0 || p->shift_every != 0 ||
                                                           !std::isfinite(p->periodic_box))))
+    return false;
+  // the correction of the 3-D dam break: no obstacle, shifting or periodic box
+  if (p->tvc_every < 0 || (p->tvc_every > 0 && (p->dim != 3 || p->has_obstacle || p->shift_every != 0 ||
+                                                p->periodic_box > 0.0 || !std::isfinite(p->tvc_alpha) ||
+                                                !std::isfinite(p->tvc_scope_tol) || !std::isfinite(p->tvc_max_shift))))
     return false;
   return true;
 }

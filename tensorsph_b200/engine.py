@@ -39,7 +39,8 @@ FIT_NEIGHBORS = 128        # CSF curvature-fit row capacity (2-D, 4h + skin)
 
 DIAG_FIELDS = ("rho_max", "speed_max", "front", "force_x", "force_y", "force_z", "kinetic",
                "potential", "escapes", "clamps", "rebuilds", "row_max", "step", "status",
-               "impulse_x", "c_reference")
+               "impulse_x", "c_reference", "tvc_max_shift", "tvc_shift_sum", "tvc_kept",
+               "tvc_clipped")
 
 
 def obstacle_lattice_3d(lo, hi, dx: float) -> torch.Tensor:
@@ -163,6 +164,17 @@ def _case_params(*, dim, n_fluid, n_wall, n_obstacle, cfg, h, wall_mass, box_hi,
         for k in range(3):
             p.ob_lo[k], p.ob_hi[k] = obstacle[0][k], obstacle[1][k]
         p.ob_eps = 0.01 * cfg.dx
+    p.tvc_every = int(getattr(cfg, "tvc_every", 0) or 0) if dim == 3 else 0
+    p.tvc_alpha, p.tvc_scope_tol, p.tvc_max_shift = 0.0, -1.0, -1.0
+    if p.tvc_every and (obstacle is not None or shift_every):
+        raise NotImplementedError("transport-velocity correction runs in the 3-D dam break without "
+                                  "an obstacle or shifting, as in dam_break_3d.run_case")
+    if p.tvc_every:
+        # dam_break_3d.py:675-704: the module default 0.2 / 4 unless set; the
+        # clip is given in units of h
+        p.tvc_alpha = 0.05 if cfg.tvc_alpha is None else float(cfg.tvc_alpha)
+        p.tvc_scope_tol = -1.0 if cfg.tvc_scope_tol is None else float(cfg.tvc_scope_tol)
+        p.tvc_max_shift = -1.0 if cfg.tvc_max_shift is None else float(cfg.tvc_max_shift) * h
     p.shift_strength = getattr(cfg, "shift_strength", 1.0)
     p.shift_limit = getattr(cfg, "shift_limit", 0.25)
     p.shift_free_surface = 0.95
@@ -460,9 +472,9 @@ class BatchEngine:
 
     # -------------------------------------------------------------- output --
     def diagnostics(self, case_id: int, first: int, count: int) -> torch.Tensor:
-        """Per-step meter rows ``(count, 16)`` of one case (``DIAG_FIELDS``)."""
+        """Per-step meter rows ``(count, len(DIAG_FIELDS))`` of one case."""
         with torch.cuda.stream(self.stream):
-            out = torch.empty((count, 16), dtype=torch.float64, device=self.device)
+            out = torch.empty((count, len(DIAG_FIELDS)), dtype=torch.float64, device=self.device)
         _lib.check(_lib.lib().tsph_engine_diag(self._handle, int(case_id), out.data_ptr(),
                                                int(first), int(count), self.stream.cuda_stream),
                    "tsph_engine_diag")
@@ -547,6 +559,7 @@ class DamBreak3DRun:
     obstacle_impulse: list = field(default_factory=list)
     obstacle_clamps: int = 0
     snapshots: list = field(default_factory=list)
+    tvc_log: list = field(default_factory=list)
 
     @property
     def mass_drift(self) -> float:
@@ -684,6 +697,28 @@ def _run_with_snapshots(eng, case_id, steps: int, plan) -> list:
     return snaps.result()
 
 
+def _tvc_log(cfg, diag, n_fluid: int) -> list:
+    """The reference's per-application log of the transport-velocity
+    correction (dam_break_3d.py:697-704) from the meter rows: steps
+    k = tvc_every, 2 tvc_every, ... before the last."""
+    every = int(getattr(cfg, "tvc_every", 0) or 0)
+    if not every:
+        return []
+    h = cfg.h_factor * cfg.dx
+    out, elapsed = [], 0.0
+    for k in range(cfg.steps):
+        if k > 0 and k % every == 0:
+            row = diag[k]
+            out.append({"step": k, "time": elapsed,
+                        "max_shift_over_h": float(row[16]) / h,
+                        "mean_shift_over_h": float(row[17]) / n_fluid / h,
+                        "kept_fraction": (None if cfg.tvc_scope_tol is None
+                                          else float(row[18]) / n_fluid),
+                        "clipped_fraction": float(row[19]) / n_fluid})
+        elapsed += cfg.dt
+    return out
+
+
 def run_case(cfg: DamBreak3DConfig, pair_skin_factor: float | None = None, snapshot_times=None,
              seed: int | None = None, *, obstacle=None, shift_every: int = 0,
              max_neighbors: int = 160) -> DamBreak3DRun:
@@ -727,7 +762,7 @@ def run_case(cfg: DamBreak3DConfig, pair_skin_factor: float | None = None, snaps
         initial_energy=eng.initial_pe, steps_taken=cfg.steps, simulated_time=cfg.steps * cfg.dt,
         obstacle_force=diag[:cfg.steps, 3:6].tolist(),
         obstacle_impulse=[float(diag[cfg.steps - 1, 14])] if cfg.steps else [],
-        obstacle_clamps=int(st["clamps"]), snapshots=snapshots)
+        obstacle_clamps=int(st["clamps"]), snapshots=snapshots, tvc_log=_tvc_log(cfg, diag, eng.n_fluid))
     masses = eng.spec.mass
     run.final_energy = float(0.5 * (masses[:, None] * vs.square()).sum()
                              + (masses * cfg.gravity * xs[:, 1]).sum())

@@ -141,6 +141,60 @@ def test_engine_shift_matches_fp64_oracle(gpu):
     assert err < 1e-5 * np.abs(shift).max(), err / np.abs(shift).max()
 
 
+@pytest.mark.parametrize("opts", [dict(), dict(tvc_alpha=0.2, tvc_scope_tol=0.05, tvc_max_shift=1e-4)])
+def test_engine_tvc_matches_fp64_oracle(opts, gpu):
+    """Transport-velocity correction in the engine (dam_break_3d.py:675-704)
+    against the oracle: two steps (the correction runs after the update of
+    step 1), a zero skin so that the rows are the step's 2h pairs at its
+    start, as the reference's cache hands them over, from a lattice jittered
+    by +-0.1 dx.  The displacement (run with the correction minus run
+    without) matches the oracle's shift to 1e-5 of its largest component
+    (1e-4 with the clip: it scales bulk particles, whose g is a strongly
+    cancelling FP32 sum with ~1e-5 relative error, up to the full clip
+    length), and the logged max / mean shift and clipped fraction match."""
+    from dataclasses import replace
+    from oracle import tvc as otv
+    from tensorsph_b200.dam_break_3d import mass_3d
+    from tensorsph_b200.engine import DamBreak3DEngine, run_case
+    cfg, _ = small_case()
+    cfg = replace(cfg, pair_skin_factor=0.0, steps=2, output_every=1)
+    x, mass, wall, n_ob = DamBreak3DEngine.build_host_state(cfg, None)
+    rng = np.random.default_rng(9)
+    x = (x + torch.from_numpy(rng.uniform(-0.1, 0.1, tuple(x.shape)) * cfg.dx)).clamp(min=0.0)
+    runs = {}
+    for every in (0, 1):
+        c = replace(cfg, tvc_every=every, **opts)
+        eng = DamBreak3DEngine(c, host_state=(x, mass, wall, n_ob), diag_ring=64)
+        eng.step(2)
+        runs[every] = eng.state()[0].cpu().numpy()
+        diag = eng.diagnostics(1, 1).cpu().numpy()[0]
+        assert eng.status()["status"] == 0
+        eng.close()
+    xn, mn, wn = x.numpy(), mass.numpy(), wall.numpy()
+    ref, x2, _ = oracle_steps(cfg, ((9, 9, 9), (9, 9, 9)), xn, mn, wn, 0, 2)
+    _, x1, _ = oracle_steps(cfg, ((9, 9, 9), (9, 9, 9)), xn, mn, wn, 0, 1)
+    h = cfg.h_factor * cfg.dx
+    pairs = cell_linked_pairs(np.concatenate((x1, wn)), 2.0 * h)
+    wvol = mass_3d(cfg.dx, cfg.h_factor, cfg.rho0, cfg.density_calibration) / cfg.rho0
+    vol = np.concatenate((mn / ref[1][0], np.full(wn.shape[0], wvol)))
+    c = replace(cfg, tvc_every=1, **opts)
+    res = otv.transport_velocity_correction(
+        np.concatenate((x2, wn)), vol, h, pairs, wall_count=wn.shape[0],
+        alpha=0.05 if c.tvc_alpha is None else c.tvc_alpha, h_ref=h, scope_tol=c.tvc_scope_tol,
+        max_shift=None if c.tvc_max_shift is None else c.tvc_max_shift * h)
+    shift = res["shift"]
+    assert np.abs(shift).max() > 1e-4 * cfg.dx
+    err = np.abs((runs[1] - runs[0]) - shift).max()
+    tol = 1e-4 if c.tvc_max_shift is not None else 1e-5
+    assert err < tol * np.abs(shift).max(), err / np.abs(shift).max()
+    norm = np.linalg.norm(shift, axis=1)
+    assert diag[16] == pytest.approx(norm.max(), rel=1e-5)
+    assert diag[17] == pytest.approx(norm.sum(), rel=1e-5)
+    assert diag[19] / mn.size == pytest.approx(res["clipped"], abs=1.5 / mn.size)
+    log = run_case(replace(cfg, tvc_every=1, steps=3, **opts)).tvc_log
+    assert [e["step"] for e in log] == [1, 2]
+
+
 def test_engine_shift_runs_and_moves_particles(gpu):
     from tensorsph_b200.engine import DamBreak3DEngine
     cfg, obstacle = small_case()
