@@ -250,6 +250,45 @@ int tsph_csf3_acceleration(const tsph_csf3_params* prm, const void* normal, cons
                            tsph_stream stream);
 
 /* ------------------------------------------------------------------------ */
+/* 2-D CSF surface tension: tensorsph.csf_consistent.csf_fields and         */
+/* surface_tension_acceleration (csf_consistent.py:90-446,                  */
+/* csf_curvature.py:78-166) over the symmetric rows of a pair list.         */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  int64_t n, dtype;            /* particles; TSPH_F32 or TSPH_F64           */
+  int64_t normal_smoothing;    /* Shepard passes on the normal              */
+  int64_t color_smoothing;     /* curvature from a colour smoothed this often */
+  int64_t curvature;           /* 0 "mls" (div n), 1 "fit_quadratic"        */
+  int64_t delta_normalization; /* 0 "legacy" (2|grad c|), 1 "local_range"   */
+  double h, rho0;              /* smoothing length; V = m / rho0            */
+  double stencil;              /* fit stencil in units of h (4)             */
+  double sigma;                /* acceleration only                         */
+} tsph_csf2_params;
+
+typedef struct {
+  const void* pos;            /* (n, 2)                                      */
+  const void* mass;           /* (n)                                         */
+  const int64_t* rowptr;      /* (n + 1) symmetric rows                      */
+  const uint32_t* entries;
+  void* color;                /* out (n)                                     */
+  void* grad_c;               /* out (n, 2)                                  */
+  void* normal;               /* out (n, 2)                                  */
+  void* kappa;                /* out (n)                                     */
+  void* delta_s;              /* out (n)                                     */
+  uint8_t* valid;             /* out (n): the MLS matrix is regular          */
+} tsph_csf2_io;
+
+int64_t tsph_csf2_workspace_bytes(const tsph_csf2_params* prm);
+/* replaces csf_fields (csf_consistent.py:262-381; no contact angle) */
+int tsph_csf2_fields(const tsph_csf2_params* prm, const tsph_csf2_io* io, void* ws, int64_t ws_bytes,
+                     tsph_stream stream);
+/* replaces the force of surface_tension_acceleration (csf_consistent.py:
+ * 430-446): delta_s_out = delta_s with the flat particles zeroed, acc (n, 2) */
+int tsph_csf2_acceleration(const tsph_csf2_params* prm, const void* grad_c, const void* normal,
+                           const void* kappa, const void* delta_s, const void* rho, void* delta_s_out,
+                           void* acc, void* ws, int64_t ws_bytes, tsph_stream stream);
+
+/* ------------------------------------------------------------------------ */
 /* Transport-velocity correction: kernel_gradient_integral and              */
 /* transport_velocity_correction (transport_velocity_correction.py:285-513) */
 /* over the symmetric rows of a pair list; fluid particles first.           */

@@ -21,6 +21,14 @@ numpy restatement of the 2-D surface-tension path the droplet case runs
 * a = -sigma kappa delta_s n / rho with delta_s = 0 where |grad c| <= 1e-3 max
   (csf_consistent.py:384-446).  All pairs are the 4h list, as the reference
   builds it for the fit (:415-421).
+
+The variants of ``csf_fields`` (csf_consistent.py:262-381) are restated as
+well: ``curvature_scheme="mls"`` (no fit), ``delta_normalization=
+"local_range"`` (|grad c| over the local colour range max - min of the pair
+neighbourhood, clipped to [0.2, 1]; :231-259), ``normal_smoothing`` passes
+and ``curvature_color_smoothing`` (the curvature from a Shepard-smoothed,
+clipped colour field while the force keeps the sharp one).  Pinned to
+``tests/golden/csf.npz`` and ``tests/golden/csf2d.npz``.
 """
 from __future__ import annotations
 
@@ -144,31 +152,60 @@ def fit_curvature_quadratic(pos, normal, delta_s, pairs, h, fallback, stencil=4.
     return np.where(ok, kappa, fallback).astype(pos.dtype)
 
 
-def csf_fields(pos, mass, pairs, h, rho0, normal_smoothing=2, stencil=4.0):
+def _normal(pos, field, vol, pairs, h, m, passes):
+    """Outward normal of a colour field with ``passes`` Shepard passes."""
+    T = pos.dtype.type
+    grad = mls_gradient(pos, field, vol, pairs, h, m)
+    mag = np.sqrt((grad * grad).sum(1))
+    tiny = T(1e-12)
+    normal = np.where(mag[:, None] > tiny, -grad / np.maximum(mag, tiny)[:, None], T(0))
+    if passes:
+        sm = shepard_smooth(normal, pos, vol, pairs, h, passes)
+        nrm = np.sqrt((sm * sm).sum(1))
+        normal = np.where(mag[:, None] > tiny, sm / np.maximum(nrm, tiny)[:, None], normal)
+    return grad, mag, normal
+
+
+def colour_range(color, pairs):
+    """max - min of the colour over each particle and its pair partners,
+    clipped to [0.2, 1] (csf_consistent.py:231-259)."""
+    hi, lo = color.copy(), color.copy()
+    i, j = pairs[:, 0], pairs[:, 1]
+    np.maximum.at(hi, i, color[j])
+    np.minimum.at(lo, i, color[j])
+    np.maximum.at(hi, j, color[i])
+    np.minimum.at(lo, j, color[i])
+    return np.clip(hi - lo, color.dtype.type(0.2), color.dtype.type(1.0))
+
+
+def csf_fields(pos, mass, pairs, h, rho0, normal_smoothing=2, stencil=4.0, curvature_scheme="fit_quadratic",
+               curvature_color_smoothing=0, delta_normalization="legacy"):
     T = pos.dtype.type
     vol = (mass / T(rho0)).astype(pos.dtype)
     c = colour(pos, vol, pairs, h)
     m, _ = mls_matrix(pos, vol, pairs, h)
-    grad_c = mls_gradient(pos, c, vol, pairs, h, m)
-    mag = np.sqrt((grad_c * grad_c).sum(1))
-    tiny = T(1e-12)
-    normal = np.where(mag[:, None] > tiny, -grad_c / np.maximum(mag, tiny)[:, None], T(0))
-    if normal_smoothing:
-        sm = shepard_smooth(normal, pos, vol, pairs, h, normal_smoothing)
-        nrm = np.sqrt((sm * sm).sum(1))
-        normal = np.where(mag[:, None] > tiny, sm / np.maximum(nrm, tiny)[:, None], normal)
-    kappa = mls_divergence(pos, normal, vol, pairs, h, m)
-    delta_s = T(2) * mag
-    kappa = fit_curvature_quadratic(pos, normal, delta_s, pairs, h, kappa, stencil=stencil)
+    grad_c, mag, normal = _normal(pos, c, vol, pairs, h, m, normal_smoothing)
+    if curvature_color_smoothing > 0:
+        c_s = np.clip(shepard_smooth(c[:, None], pos, vol, pairs, h, curvature_color_smoothing)[:, 0], T(0), T(1))
+        _, _, normal_s = _normal(pos, c_s, vol, pairs, h, m, normal_smoothing)
+        kappa = mls_divergence(pos, normal_s, vol, pairs, h, m)
+    else:
+        kappa = mls_divergence(pos, normal, vol, pairs, h, m)
+    delta_s = T(2) * mag if delta_normalization == "legacy" else mag / colour_range(c, pairs)
+    if curvature_scheme != "mls":
+        kappa = fit_curvature_quadratic(pos, normal, delta_s, pairs, h, kappa, stencil=stencil)
     return {"color": c, "grad_c": grad_c, "normal": normal, "kappa": kappa, "delta_s": delta_s}
 
 
-def surface_tension_acceleration(pos, density, mass, h, sigma, rho0, stencil=4.0):
-    """CSF acceleration of a 2-D fluid cloud and its fields (the 4h pair list
-    is built here, as the reference does for the curvature fit)."""
+def surface_tension_acceleration(pos, density, mass, h, sigma, rho0, stencil=4.0, pairs=None,
+                                 curvature_scheme="fit_quadratic", delta_normalization="legacy"):
+    """CSF acceleration of a 2-D fluid cloud and its fields (with a fit, the
+    4h pair list is built here, as the reference does)."""
     T = pos.dtype.type
-    pairs = cell_linked_pairs(pos, stencil * h)
-    st = csf_fields(pos, mass, pairs, h, rho0, stencil=stencil)
+    if curvature_scheme != "mls" or pairs is None:
+        pairs = cell_linked_pairs(pos, stencil * h)
+    st = csf_fields(pos, mass, pairs, h, rho0, stencil=stencil, curvature_scheme=curvature_scheme,
+                    delta_normalization=delta_normalization)
     mag = np.sqrt((st["grad_c"] ** 2).sum(1))
     ds = st["delta_s"].copy()
     ds[mag <= T(1e-3) * mag.max()] = T(0)

@@ -71,6 +71,17 @@ class Csf3IO(ctypes.Structure):
                                         "grad_c", "normal", "kappa", "delta_s", "valid")]
 
 
+class Csf2Params(ctypes.Structure):
+    _fields_ = [(k, c_int64) for k in ("n", "dtype", "normal_smoothing", "color_smoothing", "curvature",
+                                       "delta_normalization")] + \
+               [(k, c_double) for k in ("h", "rho0", "stencil", "sigma")]
+
+
+class Csf2IO(ctypes.Structure):
+    _fields_ = [(k, c_void_p) for k in ("pos", "mass", "rowptr", "entries", "color", "grad_c", "normal",
+                                        "kappa", "delta_s", "valid")]
+
+
 class TvcParams(ctypes.Structure):
     _fields_ = [(k, c_int64) for k in ("n_total", "n_fluid", "dim", "dtype", "has_ratio", "limiter",
                                        "has_scope_tol", "has_max_shift")] + \
@@ -175,6 +186,10 @@ _SIGNATURES = {
     "tsph_threed_workspace_bytes": (c_int64, [POINTER(ThreedParams)]),
     "tsph_threed_accelerations": (c_int, [POINTER(ThreedParams), POINTER(ThreedIO), c_void_p,
                                           c_int64, c_void_p]),
+    "tsph_csf2_workspace_bytes": (c_int64, [POINTER(Csf2Params)]),
+    "tsph_csf2_fields": (c_int, [POINTER(Csf2Params), POINTER(Csf2IO), c_void_p, c_int64, c_void_p]),
+    "tsph_csf2_acceleration": (c_int, [POINTER(Csf2Params), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                       c_void_p, c_void_p, c_void_p, c_int64, c_void_p]),
     "tsph_tvc_gradient": (c_int, [POINTER(TvcParams), POINTER(TvcIO), c_void_p]),
     "tsph_tvc_shift": (c_int, [POINTER(TvcParams), POINTER(TvcIO), c_void_p]),
     "tsph_csf3_workspace_bytes": (c_int64, [POINTER(Csf3Params)]),

@@ -1,0 +1,566 @@
+// 2-D CSF surface tension of tensorsph.csf_consistent (csf_fields and
+// surface_tension_acceleration, csf_consistent.py:90-446) over the symmetric
+// rows of the caller's pair list, in the dtype of the positions.
+//
+//   K1 colour + MLS     c = clip(V_i W(0) + sum_j V_j W_ij, 0, 1),
+//                       M_i = sum_j V_j (x_j - x_i) (x) grad_i W_ij (symmetric), det
+//   K2 median           lower median of |det M| (radix select); valid where
+//                       |det M| > 1e-4 max(median, 1e-30), else M = I
+//   K3 gradient         grad f = M^-T sum_j V_j (f_j - f_i) grad_i W_ij, |grad|, the
+//                       normal -grad / |grad| where |grad| > 1e-12 (else 0)
+//   K4 Shepard          x_i <- sum_j V_j W_ij x_j / (V_i W(0) + sum_j V_j W_ij), passes
+//                       times, then the normal renormalised where |grad| > 1e-12
+//   K5 curvature        kappa = trace(S M^-1), S = sum_j V_j (n_j - n_i) (x) grad_i W_ij;
+//                       optionally from the normal of a Shepard-smoothed colour
+//   K6 delta_s          2 |grad c| (legacy) or |grad c| / clip(max c - min c, 0.2, 1)
+//                       over the row (local_range)
+//   K7 quadratic fit    v = c + b u + a u^2 in each particle's (t, n) frame over the
+//                       rows within stencil h, weights clip(delta_s_j / max, 0, 1);
+//                       kappa = -2a / (1 + b^2)^1.5 where the particle's weight
+//                       > 0.05 and |det| > 1e-6 max |det| (csf_curvature.py:78-166)
+//   A  acceleration     delta_s = 0 where |grad c| <= 1e-3 max |grad c|;
+//                       a = -sigma kappa delta_s n / rho
+// One thread per row, sums in a fixed order; the global maxima are exact
+// (atomic max on IEEE bits), so results are deterministic.
+#include <cmath>
+
+#include "common.cuh"
+#include "radix_select.cuh"
+#include "sphkernels.cuh"
+
+namespace tsph {
+namespace {
+
+constexpr uint32_t kIndexMask = 0x7fffffffu;
+
+template <class T>
+struct C2 {
+  int64_t n;
+  T rho0, w0, stencil_r;
+  Cubic<T> k;
+};
+
+template <class T>
+__device__ __forceinline__ unsigned long long bits_of(T v) {
+  return sizeof(T) == 8 ? static_cast<unsigned long long>(__double_as_longlong(static_cast<double>(v)))
+                        : static_cast<unsigned long long>(__float_as_uint(static_cast<float>(v)));
+}
+template <class T>
+__device__ __forceinline__ T from_bits(unsigned long long b) {
+  return sizeof(T) == 8 ? static_cast<T>(__longlong_as_double(static_cast<long long>(b)))
+                        : static_cast<T>(__uint_as_float(static_cast<uint32_t>(b)));
+}
+
+template <class T>
+__global__ void k2_pack(C2<T> p, const T* __restrict__ pos, const T* __restrict__ mass, T* __restrict__ xy,
+                        T* __restrict__ vol) {
+  for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < p.n; a += gridDim.x * blockDim.x) {
+    xy[2 * a] = pos[2 * a];
+    xy[2 * a + 1] = pos[2 * a + 1];
+    vol[a] = mass[a] / p.rho0;
+  }
+}
+
+// K1
+template <class T>
+__global__ void k2_colour(C2<T> p, const T* __restrict__ xy, const T* __restrict__ vol,
+                          const int64_t* __restrict__ rowptr, const uint32_t* __restrict__ ent,
+                          T* __restrict__ color, T* __restrict__ mm, T* __restrict__ det, uint64_t* __restrict__ keys) {
+  for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < p.n; a += gridDim.x * blockDim.x) {
+    const T xa = xy[2 * a], ya = xy[2 * a + 1];
+    CSum<T> c, mxx, mxy, myy;
+    for (int64_t e = rowptr[a]; e < rowptr[a + 1]; ++e) {
+      const int64_t b = ent[e] & kIndexMask;
+      const T dx = xa - xy[2 * b], dy = ya - xy[2 * b + 1];
+      T w, g;
+      p.k.wg(sqrt(dx * dx + dy * dy), w, g);
+      const T vb = vol[b];
+      c.add(vb * w);
+      const T s = -vb * g;  // V_b (x_b - x_a) (x) d g
+      mxx.add(s * dx * dx);
+      mxy.add(s * dx * dy);
+      myy.add(s * dy * dy);
+    }
+    c.add(vol[a] * p.w0);
+    T cv = c.value();
+    color[a] = cv < T(0) ? T(0) : (cv > T(1) ? T(1) : cv);
+    const T m0 = mxx.value(), m1 = mxy.value(), m2 = myy.value();
+    mm[3 * a] = m0;
+    mm[3 * a + 1] = m1;
+    mm[3 * a + 2] = m2;
+    const T d = m0 * m2 - m1 * m1;
+    det[a] = d;
+    keys[a] = bits_of<T>(d < T(0) ? -d : d);
+  }
+}
+
+// K3 (first call also writes M^-1 and the validity)
+template <class T>
+__global__ void k2_gradient(C2<T> p, const T* __restrict__ xy, const T* __restrict__ vol,
+                            const int64_t* __restrict__ rowptr, const uint32_t* __restrict__ ent,
+                            const T* __restrict__ field, const T* __restrict__ mm, const T* __restrict__ det,
+                            const unsigned long long* __restrict__ sel, T* __restrict__ minv,
+                            uint8_t* __restrict__ valid, T* __restrict__ grad, T* __restrict__ mag,
+                            T* __restrict__ normal) {
+  const T med = from_bits<T>(sel[0]);
+  const T scale = med > T(1e-30) ? med : T(1e-30);
+  for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < p.n; a += gridDim.x * blockDim.x) {
+    const T xa = xy[2 * a], ya = xy[2 * a + 1];
+    const T fa = field[a];
+    CSum<T> rx, ry;
+    for (int64_t e = rowptr[a]; e < rowptr[a + 1]; ++e) {
+      const int64_t b = ent[e] & kIndexMask;
+      const T dx = xa - xy[2 * b], dy = ya - xy[2 * b + 1];
+      T w, g;
+      p.k.wg(sqrt(dx * dx + dy * dy), w, g);
+      const T s = vol[b] * (field[b] - fa) * g;
+      rx.add(s * dx);
+      ry.add(s * dy);
+    }
+    const T d = det[a];
+    const bool ok = (d < T(0) ? -d : d) > T(1e-4) * scale;
+    T i0 = T(1), i1 = T(0), i2 = T(1);
+    if (ok) {
+      const T r = T(1) / d;
+      i0 = mm[3 * a + 2] * r;
+      i1 = -mm[3 * a + 1] * r;
+      i2 = mm[3 * a] * r;
+    }
+    if (minv) {
+      minv[3 * a] = i0;
+      minv[3 * a + 1] = i1;
+      minv[3 * a + 2] = i2;
+      valid[a] = ok ? 1 : 0;
+    }
+    const T u = rx.value(), v = ry.value();
+    const T gx = i0 * u + i1 * v, gy = i1 * u + i2 * v;
+    const T m = sqrt(gx * gx + gy * gy);
+    grad[2 * a] = gx;
+    grad[2 * a + 1] = gy;
+    mag[a] = m;
+    const T tiny = T(1e-12);
+    const bool on = m > tiny;
+    const T den = m > tiny ? m : tiny;
+    normal[2 * a] = on ? -gx / den : T(0);
+    normal[2 * a + 1] = on ? -gy / den : T(0);
+  }
+}
+
+// K4: one Shepard pass of a field of `nc` components (1 or 2)
+template <class T>
+__global__ void k2_shepard(C2<T> p, const T* __restrict__ xy, const T* __restrict__ vol,
+                           const int64_t* __restrict__ rowptr, const uint32_t* __restrict__ ent, int nc,
+                           const T* __restrict__ in, T* __restrict__ out) {
+  for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < p.n; a += gridDim.x * blockDim.x) {
+    const T xa = xy[2 * a], ya = xy[2 * a + 1];
+    CSum<T> n0, n1, den;
+    den.add(vol[a] * p.w0);
+    for (int64_t e = rowptr[a]; e < rowptr[a + 1]; ++e) {
+      const int64_t b = ent[e] & kIndexMask;
+      const T dx = xa - xy[2 * b], dy = ya - xy[2 * b + 1];
+      const T vw = vol[b] * p.k.w(sqrt(dx * dx + dy * dy));
+      n0.add(vw * in[nc * b]);
+      if (nc == 2) n1.add(vw * in[2 * b + 1]);
+      den.add(vw);
+    }
+    const T dv = den.value();
+    const T dd = dv > T(1e-30) ? dv : T(1e-30);
+    out[nc * a] = n0.value() / dd;
+    if (nc == 2) out[2 * a + 1] = n1.value() / dd;
+  }
+}
+
+template <class T>
+__global__ void k2_renorm(C2<T> p, const T* __restrict__ mag, const T* __restrict__ sm, T* __restrict__ normal) {
+  for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < p.n; a += gridDim.x * blockDim.x) {
+    const T tiny = T(1e-12);
+    if (!(mag[a] > tiny)) continue;
+    const T x = sm[2 * a], y = sm[2 * a + 1];
+    const T nr = sqrt(x * x + y * y);
+    const T d = nr > tiny ? nr : tiny;
+    normal[2 * a] = x / d;
+    normal[2 * a + 1] = y / d;
+  }
+}
+
+template <class T>
+__global__ void k2_clip(C2<T> p, T* __restrict__ f) {
+  for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < p.n; a += gridDim.x * blockDim.x)
+    f[a] = f[a] < T(0) ? T(0) : (f[a] > T(1) ? T(1) : f[a]);
+}
+
+// K5
+template <class T>
+__global__ void k2_kappa(C2<T> p, const T* __restrict__ xy, const T* __restrict__ vol,
+                         const int64_t* __restrict__ rowptr, const uint32_t* __restrict__ ent,
+                         const T* __restrict__ normal, const T* __restrict__ minv, T* __restrict__ kappa) {
+  for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < p.n; a += gridDim.x * blockDim.x) {
+    const T xa = xy[2 * a], ya = xy[2 * a + 1];
+    const T nxa = normal[2 * a], nya = normal[2 * a + 1];
+    CSum<T> s00, s01, s10, s11;
+    for (int64_t e = rowptr[a]; e < rowptr[a + 1]; ++e) {
+      const int64_t b = ent[e] & kIndexMask;
+      const T dx = xa - xy[2 * b], dy = ya - xy[2 * b + 1];
+      T w, g;
+      p.k.wg(sqrt(dx * dx + dy * dy), w, g);
+      const T v = vol[b] * g;
+      const T ex = normal[2 * b] - nxa, ey = normal[2 * b + 1] - nya;
+      s00.add(ex * (v * dx));
+      s01.add(ex * (v * dy));
+      s10.add(ey * (v * dx));
+      s11.add(ey * (v * dy));
+    }
+    const T i0 = minv[3 * a], i1 = minv[3 * a + 1], i2 = minv[3 * a + 2];
+    kappa[a] = s00.value() * i0 + s01.value() * i1 + s10.value() * i1 + s11.value() * i2;
+  }
+}
+
+// K6 (+ the maxima of delta_s and |grad c|)
+template <class T>
+__global__ void k2_delta(C2<T> p, int local_range, const int64_t* __restrict__ rowptr,
+                         const uint32_t* __restrict__ ent, const T* __restrict__ color, const T* __restrict__ mag,
+                         T* __restrict__ delta_s, unsigned long long* __restrict__ maxima) {
+  unsigned long long md = 0, mg = 0;
+  for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < p.n; a += gridDim.x * blockDim.x) {
+    T ds = T(2) * mag[a];
+    if (local_range) {
+      T hi = color[a], lo = color[a];
+      for (int64_t e = rowptr[a]; e < rowptr[a + 1]; ++e) {
+        const T c = color[ent[e] & kIndexMask];
+        hi = c > hi ? c : hi;
+        lo = c < lo ? c : lo;
+      }
+      T r = hi - lo;
+      r = r < T(0.2) ? T(0.2) : (r > T(1) ? T(1) : r);
+      ds = mag[a] / r;
+    }
+    delta_s[a] = ds;
+    const unsigned long long bd = bits_of<T>(ds), bg = bits_of<T>(mag[a]);
+    md = bd > md ? bd : md;
+    mg = bg > mg ? bg : mg;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long x = __shfl_xor_sync(0xffffffffu, md, o);
+    const unsigned long long y = __shfl_xor_sync(0xffffffffu, mg, o);
+    md = x > md ? x : md;
+    mg = y > mg ? y : mg;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&maxima[0], md);
+    atomicMax(&maxima[1], mg);
+  }
+}
+
+// K7a: fit moments s[0..7] and the 3x3 determinant (+ its maximum)
+template <class T>
+__global__ void k2_fit_moments(C2<T> p, const T* __restrict__ xy, const int64_t* __restrict__ rowptr,
+                               const uint32_t* __restrict__ ent, const T* __restrict__ normal,
+                               const T* __restrict__ delta_s, const unsigned long long* __restrict__ maxima,
+                               T* __restrict__ mom, T* __restrict__ fdet, unsigned long long* __restrict__ fmax) {
+  const T dsm = from_bits<T>(maxima[0]);
+  const T ds_max = dsm > T(1e-30) ? dsm : T(1e-30);
+  unsigned long long mb = 0;
+  for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < p.n; a += gridDim.x * blockDim.x) {
+    const T xa = xy[2 * a], ya = xy[2 * a + 1];
+    const T nx = normal[2 * a], ny = normal[2 * a + 1];
+    const T tx = -ny, ty = nx;
+    CSum<T> s[8];
+    T wa = delta_s[a] / ds_max;
+    wa = wa < T(0) ? T(0) : (wa > T(1) ? T(1) : wa);
+    s[0].add(wa);
+    for (int64_t e = rowptr[a]; e < rowptr[a + 1]; ++e) {
+      const int64_t b = ent[e] & kIndexMask;
+      const T dx = xa - xy[2 * b], dy = ya - xy[2 * b + 1];
+      const T r = sqrt(dx * dx + dy * dy);
+      if (!(r <= p.stencil_r)) continue;
+      T w = delta_s[b] / ds_max;
+      w = w < T(0) ? T(0) : (w > T(1) ? T(1) : w);
+      // the neighbour in the particle's frame: (x_b - x_a) . t, . n
+      const T u = -dx * tx + -dy * ty, v = -dx * nx + -dy * ny;
+      const T uu = u * u;
+      s[0].add(w);
+      s[1].add(u * w);
+      s[2].add(v * w);
+      s[3].add(uu * w);
+      s[4].add(u * v * w);
+      s[5].add(uu * u * w);
+      s[6].add(uu * v * w);
+      s[7].add(uu * uu * w);
+    }
+    T sv[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      sv[k] = s[k].value();
+      mom[8 * a + k] = sv[k];
+    }
+    // [[s0 s1 s3] [s1 s3 s5] [s3 s5 s7]]
+    const T d = sv[0] * (sv[3] * sv[7] - sv[5] * sv[5]) - sv[1] * (sv[1] * sv[7] - sv[5] * sv[3]) +
+                sv[3] * (sv[1] * sv[5] - sv[3] * sv[3]);
+    fdet[a] = d;
+    const unsigned long long b = bits_of<T>(d < T(0) ? -d : d);
+    mb = b > mb ? b : mb;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long x = __shfl_xor_sync(0xffffffffu, mb, o);
+    mb = x > mb ? x : mb;
+  }
+  if ((threadIdx.x & 31) == 0) atomicMax(fmax, mb);
+}
+
+// K7b: solve for (c, b, a) by Cramer's rule; kappa where the fit holds
+template <class T>
+__global__ void k2_fit_solve(C2<T> p, const T* __restrict__ delta_s, const unsigned long long* __restrict__ maxima,
+                             const T* __restrict__ mom, const T* __restrict__ fdet,
+                             const unsigned long long* __restrict__ fmax, T* __restrict__ kappa) {
+  const T dsm = from_bits<T>(maxima[0]);
+  const T ds_max = dsm > T(1e-30) ? dsm : T(1e-30);
+  const T dm = from_bits<T>(*fmax);
+  const T scale = dm > T(1e-30) ? dm : T(1e-30);
+  for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < p.n; a += gridDim.x * blockDim.x) {
+    T wa = delta_s[a] / ds_max;
+    wa = wa < T(0) ? T(0) : (wa > T(1) ? T(1) : wa);
+    const T d = fdet[a];
+    if (!(wa > T(0.05)) || !((d < T(0) ? -d : d) > T(1e-6) * scale)) continue;  // keep the MLS value
+    const T* s = mom + 8 * a;
+    const T r0 = s[2], r1 = s[4], r2 = s[6];
+    // columns 1 (b) and 2 (a) replaced by the right-hand side
+    const T db = s[0] * (r1 * s[7] - s[5] * r2) - r0 * (s[1] * s[7] - s[5] * s[3]) + s[3] * (s[1] * r2 - r1 * s[3]);
+    const T da = s[0] * (s[3] * r2 - r1 * s[5]) - s[1] * (s[1] * r2 - r1 * s[3]) + r0 * (s[1] * s[5] - s[3] * s[3]);
+    const T b = db / d, aa = da / d;
+    const T q = T(1) + b * b;
+    kappa[a] = T(-2) * aa / (q * sqrt(q));
+  }
+}
+
+template <class T>
+__global__ void k2_max_mag(C2<T> p, const T* __restrict__ grad, unsigned long long* __restrict__ out) {
+  unsigned long long m = 0;
+  for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < p.n; a += gridDim.x * blockDim.x) {
+    const T gx = grad[2 * a], gy = grad[2 * a + 1];
+    const unsigned long long b = bits_of<T>(sqrt(gx * gx + gy * gy));
+    m = b > m ? b : m;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long x = __shfl_xor_sync(0xffffffffu, m, o);
+    m = x > m ? x : m;
+  }
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+template <class T>
+__global__ void k2_accel(C2<T> p, T sigma, const T* __restrict__ grad, const T* __restrict__ normal,
+                         const T* __restrict__ kappa, const T* __restrict__ delta_s, const T* __restrict__ rho,
+                         const unsigned long long* __restrict__ maxmag, T* __restrict__ ds_out, T* __restrict__ acc) {
+  const T limit = T(1e-3) * from_bits<T>(*maxmag);
+  for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < p.n; a += gridDim.x * blockDim.x) {
+    const T gx = grad[2 * a], gy = grad[2 * a + 1];
+    const T m = sqrt(gx * gx + gy * gy);
+    const T ds = m <= limit ? T(0) : delta_s[a];
+    ds_out[a] = ds;
+    const T f = -sigma * kappa[a] * ds;
+    acc[2 * a] = f * normal[2 * a] / rho[a];
+    acc[2 * a + 1] = f * normal[2 * a + 1] / rho[a];
+  }
+}
+
+struct L2 {
+  size_t xy, vol, mm, minv, det, keys, hist, sel, mag, n0, sm0, sm1, cs, cs1, grad_s, mag_s, normal_s, mom, fdet,
+      maxima, total;
+};
+
+L2 layout2(int64_t n, int64_t dtype) {
+  const size_t t = dtype == TSPH_F64 ? 8 : 4;
+  L2 L{};
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = off;
+    off += align_up(bytes);
+    return at;
+  };
+  L.xy = take(2 * n * t);
+  L.vol = take(n * t);
+  L.mm = take(3 * n * t);
+  L.minv = take(3 * n * t);
+  L.det = take(n * t);
+  L.keys = take(n * 8);
+  L.hist = take(256 * 4);
+  L.sel = take(2 * 8);
+  L.mag = take(n * t);
+  L.n0 = take(2 * n * t);
+  L.sm0 = take(2 * n * t);
+  L.sm1 = take(2 * n * t);
+  L.cs = take(n * t);
+  L.cs1 = take(n * t);
+  L.grad_s = take(2 * n * t);
+  L.mag_s = take(n * t);
+  L.normal_s = take(2 * n * t);
+  L.mom = take(8 * n * t);
+  L.fdet = take(n * t);
+  L.maxima = take(4 * 8);
+  L.total = off;
+  return L;
+}
+
+template <class T>
+C2<T> make_c2(const tsph_csf2_params& prm) {
+  C2<T> p{};
+  p.n = prm.n;
+  p.rho0 = static_cast<T>(prm.rho0);
+  const double sigma2 = 10.0 / (7.0 * M_PI * prm.h * prm.h);
+  p.w0 = static_cast<T>(sigma2);
+  p.stencil_r = static_cast<T>(prm.stencil * prm.h);
+  p.k.h = static_cast<T>(prm.h);
+  p.k.inv_h = static_cast<T>(1.0 / prm.h);
+  p.k.sigma = static_cast<T>(sigma2);
+  p.k.eps = static_cast<T>(1e-12);
+  return p;
+}
+
+// Smoothed normal of a colour field: K3 then `passes` Shepard passes and the
+// renormalisation.  sm0 / sm1 are ping-pong buffers.
+template <class T>
+void normal_of(const C2<T>& p, unsigned g, cudaStream_t s, const T* xy, const T* vol, const int64_t* rowptr,
+               const uint32_t* ent, const T* field, const T* mm, const T* det, const unsigned long long* sel,
+               T* minv, uint8_t* valid, T* grad, T* mag, T* normal, int passes, T* sm0, T* sm1) {
+  k2_gradient<T><<<g, 128, 0, s>>>(p, xy, vol, rowptr, ent, field, mm, det, sel, minv, valid, grad, mag, normal);
+  if (passes <= 0) return;
+  const T* in = normal;
+  T* out = sm0;
+  for (int k = 0; k < passes; ++k) {
+    k2_shepard<T><<<g, 128, 0, s>>>(p, xy, vol, rowptr, ent, 2, in, out);
+    in = out;
+    out = out == sm0 ? sm1 : sm0;
+  }
+  k2_renorm<T><<<g, 128, 0, s>>>(p, mag, in, normal);
+}
+
+template <class T>
+int run_csf2(const tsph_csf2_params& prm, const tsph_csf2_io& io, char* ws, cudaStream_t s) {
+  const L2 L = layout2(prm.n, prm.dtype);
+  const C2<T> p = make_c2<T>(prm);
+  const int64_t n = prm.n;
+  T* xy = reinterpret_cast<T*>(ws + L.xy);
+  T* vol = reinterpret_cast<T*>(ws + L.vol);
+  T* mm = reinterpret_cast<T*>(ws + L.mm);
+  T* minv = reinterpret_cast<T*>(ws + L.minv);
+  T* det = reinterpret_cast<T*>(ws + L.det);
+  uint64_t* keys = reinterpret_cast<uint64_t*>(ws + L.keys);
+  unsigned int* hist = reinterpret_cast<unsigned int*>(ws + L.hist);
+  unsigned long long* sel = reinterpret_cast<unsigned long long*>(ws + L.sel);
+  T* mag = reinterpret_cast<T*>(ws + L.mag);
+  T* sm0 = reinterpret_cast<T*>(ws + L.sm0);
+  T* sm1 = reinterpret_cast<T*>(ws + L.sm1);
+  unsigned long long* maxima = reinterpret_cast<unsigned long long*>(ws + L.maxima);
+  T* color = static_cast<T*>(io.color);
+  T* grad = static_cast<T*>(io.grad_c);
+  T* normal = static_cast<T*>(io.normal);
+  T* kappa = static_cast<T*>(io.kappa);
+  T* delta_s = static_cast<T*>(io.delta_s);
+  const unsigned g = grid_for(n, 128);
+  k2_pack<T><<<grid_for(n, 256), 256, 0, s>>>(p, static_cast<const T*>(io.pos), static_cast<const T*>(io.mass), xy,
+                                               vol);
+  k2_colour<T><<<g, 128, 0, s>>>(p, xy, vol, io.rowptr, io.entries, color, mm, det, keys);
+  TSPH_LAUNCH_CHECK();
+  TSPH_CUDA_CHECK(cudaMemsetAsync(hist, 0, 256 * sizeof(unsigned int), s));
+  TSPH_CUDA_CHECK(cudaMemsetAsync(maxima, 0, 4 * sizeof(unsigned long long), s));
+  radix_select_u64(keys, n, sizeof(T) == 8 ? 64 : 32, (n - 1) / 2, sel, hist, s, grid_for(n, 256, 148 * 4));
+  const int passes = static_cast<int>(prm.normal_smoothing);
+  normal_of<T>(p, g, s, xy, vol, io.rowptr, io.entries, color, mm, det, sel, minv, io.valid, grad, mag, normal,
+               passes, sm0, sm1);
+  const T* curv_normal = normal;
+  if (prm.color_smoothing > 0) {
+    // curvature from the normal of a Shepard-smoothed, clipped colour field
+    T* cs = reinterpret_cast<T*>(ws + L.cs);
+    T* cs1 = reinterpret_cast<T*>(ws + L.cs1);
+    const T* in = color;
+    T* out = cs;
+    for (int k = 0; k < prm.color_smoothing; ++k) {
+      k2_shepard<T><<<g, 128, 0, s>>>(p, xy, vol, io.rowptr, io.entries, 1, in, out);
+      in = out;
+      out = out == cs ? cs1 : cs;
+    }
+    T* cfield = const_cast<T*>(in);
+    k2_clip<T><<<grid_for(n, 256), 256, 0, s>>>(p, cfield);
+    T* normal_s = reinterpret_cast<T*>(ws + L.normal_s);
+    normal_of<T>(p, g, s, xy, vol, io.rowptr, io.entries, cfield, mm, det, sel, nullptr, nullptr,
+                 reinterpret_cast<T*>(ws + L.grad_s), reinterpret_cast<T*>(ws + L.mag_s), normal_s, passes, sm0,
+                 sm1);
+    curv_normal = normal_s;
+  }
+  k2_kappa<T><<<g, 128, 0, s>>>(p, xy, vol, io.rowptr, io.entries, curv_normal, minv, kappa);
+  k2_delta<T><<<grid_for(n, 128), 128, 0, s>>>(p, static_cast<int>(prm.delta_normalization), io.rowptr, io.entries,
+                                               color, mag, delta_s, maxima);
+  TSPH_LAUNCH_CHECK();
+  if (prm.curvature == 1) {
+    T* mom = reinterpret_cast<T*>(ws + L.mom);
+    T* fdet = reinterpret_cast<T*>(ws + L.fdet);
+    k2_fit_moments<T><<<g, 128, 0, s>>>(p, xy, io.rowptr, io.entries, normal, delta_s, maxima, mom, fdet,
+                                        maxima + 2);
+    k2_fit_solve<T><<<g, 128, 0, s>>>(p, delta_s, maxima, mom, fdet, maxima + 2, kappa);
+    TSPH_LAUNCH_CHECK();
+  }
+  return TSPH_OK;
+}
+
+template <class T>
+int run_accel2(const tsph_csf2_params& prm, const void* grad, const void* normal, const void* kappa,
+               const void* delta_s, const void* rho, void* ds_out, void* acc, char* ws, cudaStream_t s) {
+  const L2 L = layout2(prm.n, prm.dtype);
+  const C2<T> p = make_c2<T>(prm);
+  unsigned long long* maxima = reinterpret_cast<unsigned long long*>(ws + L.maxima);
+  TSPH_CUDA_CHECK(cudaMemsetAsync(maxima + 3, 0, sizeof(unsigned long long), s));
+  k2_max_mag<T><<<grid_for(prm.n, 256, 148 * 4), 256, 0, s>>>(p, static_cast<const T*>(grad), maxima + 3);
+  k2_accel<T><<<grid_for(prm.n, 256), 256, 0, s>>>(p, static_cast<T>(prm.sigma), static_cast<const T*>(grad),
+                                                   static_cast<const T*>(normal), static_cast<const T*>(kappa),
+                                                   static_cast<const T*>(delta_s), static_cast<const T*>(rho),
+                                                   maxima + 3, static_cast<T*>(ds_out), static_cast<T*>(acc));
+  TSPH_LAUNCH_CHECK();
+  return TSPH_OK;
+}
+
+bool params2_ok(const tsph_csf2_params* p) {
+  return p && p->n >= 0 && p->n < (int64_t(1) << 31) && p->h > 0.0 && p->rho0 > 0.0 &&
+         (p->dtype == TSPH_F32 || p->dtype == TSPH_F64) && p->normal_smoothing >= 0 && p->normal_smoothing <= 64 &&
+         p->color_smoothing >= 0 && p->color_smoothing <= 64 && (p->curvature == 0 || p->curvature == 1) &&
+         (p->delta_normalization == 0 || p->delta_normalization == 1) && p->stencil > 0.0;
+}
+
+}  // namespace
+}  // namespace tsph
+
+using namespace tsph;
+
+extern "C" {
+
+int64_t tsph_csf2_workspace_bytes(const tsph_csf2_params* prm) {
+  if (!params2_ok(prm)) return -1;
+  return static_cast<int64_t>(layout2(prm->n, prm->dtype).total);
+}
+
+int tsph_csf2_fields(const tsph_csf2_params* prm, const tsph_csf2_io* io, void* ws, int64_t ws_bytes,
+                     tsph_stream stream) {
+  if (!params2_ok(prm) || !io) return TSPH_ERR_ARG;
+  if (prm->n == 0) return TSPH_OK;
+  if (!io->pos || !io->mass || !io->rowptr || !io->entries || !io->color || !io->grad_c || !io->normal ||
+      !io->kappa || !io->delta_s || !io->valid || !ws)
+    return TSPH_ERR_ARG;
+  if (ws_bytes < tsph_csf2_workspace_bytes(prm)) return TSPH_ERR_WORKSPACE;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (prm->dtype == TSPH_F64) return run_csf2<double>(*prm, *io, static_cast<char*>(ws), s);
+  return run_csf2<float>(*prm, *io, static_cast<char*>(ws), s);
+}
+
+int tsph_csf2_acceleration(const tsph_csf2_params* prm, const void* grad_c, const void* normal, const void* kappa,
+                           const void* delta_s, const void* rho, void* delta_s_out, void* acc, void* ws,
+                           int64_t ws_bytes, tsph_stream stream) {
+  if (!params2_ok(prm)) return TSPH_ERR_ARG;
+  if (prm->n == 0) return TSPH_OK;
+  if (!grad_c || !normal || !kappa || !delta_s || !rho || !delta_s_out || !acc || !ws) return TSPH_ERR_ARG;
+  if (ws_bytes < tsph_csf2_workspace_bytes(prm)) return TSPH_ERR_WORKSPACE;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (prm->dtype == TSPH_F64)
+    return run_accel2<double>(*prm, grad_c, normal, kappa, delta_s, rho, delta_s_out, acc, static_cast<char*>(ws), s);
+  return run_accel2<float>(*prm, grad_c, normal, kappa, delta_s, rho, delta_s_out, acc, static_cast<char*>(ws), s);
+}
+
+}  // extern "C"

@@ -531,6 +531,61 @@ def tvc_cases(tv, ns):
     return data
 
 
+def csf2d_cases(ca, di):
+    """2-D CSF variants (csf_consistent.py:262-446): curvature "mls" and
+    "fit_quadratic", delta_s "legacy" and "local_range", normal smoothing off,
+    curvature from a smoothed colour field, FP64 and FP32, through
+    surface_tension_acceleration (the 4h list for the fit) and through direct
+    csf_fields calls on a 2h list (the smoothing options are csf_fields
+    arguments only)."""
+    data = {}
+    variants = [
+        ("jitter", torch.float64, dict(curvature_scheme="mls")),
+        ("jitter", torch.float64, dict(curvature_scheme="mls", delta_normalization="local_range")),
+        ("pool", torch.float64, dict(curvature_scheme="fit_quadratic", delta_normalization="local_range")),
+        ("jitter", torch.float64, dict(curvature_scheme="mls", curvature_color_smoothing=1, direct=True)),
+        ("jitter", torch.float64, dict(curvature_scheme="mls", normal_smoothing=0, direct=True)),
+        ("jitter", torch.float32, dict(curvature_scheme="fit_quadratic")),
+        ("jitter", torch.float64, dict(curvature_scheme="fit_quadratic", direct=True)),
+    ]
+    for k, (kind, dtype, o) in enumerate(variants):
+        g = torch.Generator().manual_seed(300 + k)
+        dx = 0.002
+        h = 1.3 * dx
+        if kind == "pool":
+            cfg = di.Config(dx=dx, pool_width=0.08, pool_depth=0.02, drop_radius=0.01, drop_center_y=0.035)
+            pos, mass = di.make_particles(cfg, "cpu")
+            pos, mass = pos.to(dtype), mass.to(dtype)
+        else:
+            ax = torch.arange(-12, 13, dtype=torch.float64) * dx
+            gx, gy = torch.meshgrid(ax, ax, indexing="xy")
+            pts = torch.stack((gx.reshape(-1), gy.reshape(-1)), -1)
+            pts = pts[torch.linalg.vector_norm(pts, dim=1) <= 10.5 * dx]
+            pts = pts + 0.05 * dx * torch.randn(pts.shape, generator=g, dtype=torch.float64)
+            pos = (pts + 0.05).to(dtype)
+            mass = torch.full((pos.shape[0],), 1000.0 * dx * dx, dtype=dtype)
+        rho = (1000.0 * (1.0 + 0.002 * torch.randn((pos.shape[0],), generator=g, dtype=torch.float64))).to(dtype)
+        o = dict(o)
+        direct = o.pop("direct", False)
+        pairs = di.cell_linked_pairs(pos, 2.0 * h)
+        if direct:
+            st = ca.csf_fields(pos, mass, pairs, h, 1000.0, **o)
+            acc = None
+        else:
+            acc, st = ca.surface_tension_acceleration(pos, rho, mass, pairs, h, 0.0728, rho0=1000.0, **o)
+        fields = dict(pos=pos, mass=mass, rho=rho, pairs=pairs, color=st.color, grad_c=st.grad_c,
+                      normal=st.normal, kappa=st.kappa, delta_s=st.delta_s)
+        if acc is not None:
+            fields["acc"] = acc
+        for name, t in fields.items():
+            data[f"c{k}_{name}"] = _np(t)
+        data[f"c{k}_h"] = np.float64(h)
+        data[f"c{k}_direct"] = np.int64(direct)
+        data[f"c{k}_opts"] = np.array(repr(sorted(o.items())))
+    data["count"] = np.int64(len(variants))
+    return data
+
+
 def delta_plus_cases(dp):
     """delta_plus_step on a perturbed lattice block in a walled corner (fluid,
     slip walls with normals, gravity, diffusion) and on a free block."""
@@ -655,6 +710,7 @@ def main(src, families=None):
         "delta_plus": lambda: delta_plus_cases(dp),
         "csf3": lambda: csf3_cases(c3, lc, ns, n3),
         "tvc": lambda: tvc_cases(tv, ns),
+        "csf2d": lambda: csf2d_cases(ca, di),
         "config1_run": lambda: config1_run_case(db),
         "dam3d_run": lambda: dam3d_run_case(d3),
     }

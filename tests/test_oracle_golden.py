@@ -246,6 +246,32 @@ def _tvc_kwargs(g, k):
     return kw
 
 
+def test_csf2d_oracle_variants_match_reference(golden):
+    """The oracle's 2-D CSF variants (mls / fit_quadratic curvature, legacy /
+    local_range delta_s, normal smoothing off, smoothed-colour curvature)
+    against the reference's own output (tests/golden/csf2d.npz)."""
+    import ast
+    from oracle import csf
+    g = golden("csf2d")
+    for k in range(int(g["count"])):
+        o = dict(ast.literal_eval(str(g[f"c{k}_opts"])))
+        pos, mass, rho, pairs, h = (g[f"c{k}_pos"], g[f"c{k}_mass"], g[f"c{k}_rho"], g[f"c{k}_pairs"],
+                                    float(g[f"c{k}_h"]))
+        if int(g[f"c{k}_direct"]):
+            st = csf.csf_fields(pos, mass, pairs, h, 1000.0, **o)
+        else:
+            acc, st = csf.surface_tension_acceleration(pos, rho, mass, h, 0.0728, 1000.0, pairs=pairs, **o)
+            ref = g[f"c{k}_acc"]
+            assert np.abs(acc - ref).max() <= (1e-10 if pos.dtype == np.float64 else 1e-4) * np.abs(ref).max()
+        live = g[f"c{k}_delta_s"] > 0
+        tol = 1e-9 if pos.dtype == np.float64 else 1e-4
+        for name in ("color", "grad_c", "delta_s", "normal", "kappa"):
+            r, d = g[f"c{k}_{name}"], st[name]
+            if name in ("normal", "kappa"):
+                r, d = r[live], d[live]
+            assert np.abs(d - r).max() <= tol * max(np.abs(r).max(), 1.0), (k, name)
+
+
 def test_tvc_oracle_matches_reference(golden):
     """The oracle's transport-velocity correction against the reference's own
     output (tests/golden/tvc.npz: 2-D and 3-D, FP64 and FP32, limiters,
