@@ -498,6 +498,8 @@ typedef struct {
   double tvc_alpha;                    /* its coefficient (displacement alpha h^2 g)  */
   double tvc_scope_tol;                /* >= 0: only where |g| h <= tol; < 0: all     */
   double tvc_max_shift;                /* >= 0: clip |shift| to this length; < 0: off */
+  int64_t first_step;                  /* step number of the first step (a run       */
+                                       /* resumed from a checkpoint); 0 for a new run */
 } tsph_case_params;
 
 typedef struct tsph_engine tsph_engine; /* opaque host handle */
@@ -541,12 +543,14 @@ int tsph_engine_graph_kernels(tsph_engine* engine, int64_t* kernels);
  * FP64 (device, nullable). */
 int tsph_engine_read(tsph_engine* engine, int64_t case_id, double* x, double* v, double* rho,
                      double* p, tsph_stream stream);
-/* Copy `count` per-step meter rows of one case (20 doubles each: max rho,
+/* Copy `count` per-step meter rows of one case (25 doubles each: max rho,
  * max |v|, front x, obstacle force xyz, kinetic and potential energy,
  * escapes, clamps, rebuilds, longest row, step, status, obstacle impulse x,
- * c_ref, and the step's transport-velocity correction: max |shift|,
- * sum |shift|, kept and clipped counts) starting at its step `first` into
- * `out` (device). */
+ * c_ref, the step's transport-velocity correction: max |shift|,
+ * sum |shift|, kept and clipped counts, obstacle impulse y and z, and the
+ * obstacle clamp impulse xyz; both impulses through the step's update and
+ * counted from the case's admission) starting at its step `first` into
+ * `out` (device).  Row k of a ring of R rows is step k mod R. */
 int tsph_engine_diag(tsph_engine* engine, int64_t case_id, double* out, int64_t first,
                      int64_t count, tsph_stream stream);
 /* Counters of one case (escapes, clamps, rebuilds, steps, longest row, -,

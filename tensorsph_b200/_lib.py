@@ -154,7 +154,8 @@ class CaseParams(ctypes.Structure):
                 ("shift_vref_floor", c_double), ("grid_lo", c_double * 3),
                 ("grid_hi", c_double * 3), ("surface_tension", c_double),
                 ("periodic_box", c_double), ("tvc_every", c_int64), ("tvc_alpha", c_double),
-                ("tvc_scope_tol", c_double), ("tvc_max_shift", c_double)]
+                ("tvc_scope_tol", c_double), ("tvc_max_shift", c_double),
+                ("first_step", c_int64)]
 
 
 _SIGNATURES = {

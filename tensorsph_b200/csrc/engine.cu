@@ -46,7 +46,7 @@ namespace {
 
 constexpr int kBlock = 128;     // default threads per block of the pair kernels
 constexpr int kMaxBlock = 256;  // largest block the kernels are built for
-constexpr int kDiag = 20;
+constexpr int kDiag = 25;
 constexpr int kBatch = 4;
 constexpr int kCodeBits = 6;                               // cell-offset code bits of a row entry
 constexpr uint32_t kCodeMask = (1u << kCodeBits) - 1;
@@ -84,6 +84,7 @@ struct CaseCtl {
   unsigned long long rho_max, speed_max, front_max, row_max;
   double ke, pe;
   double force[3], impulse[3];
+  double clamp_impulse[3];  // momentum the obstacle clamp took out, sum m (v_before - v_after)
   unsigned long long escapes, clamps, rebuilds, steps;
   double cref[2];  // [0] c_ref of the last shift, [1] max speed of the step
   // CSF per-step reductions: max |grad c| (float bits), max |det| of the fit
@@ -1368,16 +1369,24 @@ __global__ void __launch_bounds__(kMaxBlock) k_integrate(const __grid_constant__
         }
       }
       const double to = (which & 1) ? C.ob_eps : -C.ob_eps;
-      if (which < 2) {
+      const int axis = which >> 1;
+      double taken;
+      if (axis == 0) {
         px = ((which & 1) ? C.ob_hi[0] : C.ob_lo[0]) + to;
+        taken = vx;
         vx = 0.0;
-      } else if (which < 4) {
+      } else if (axis == 1) {
         py = ((which & 1) ? C.ob_hi[1] : C.ob_lo[1]) + to;
+        taken = vy;
         vy = 0.0;
       } else {
         pz = ((which & 1) ? C.ob_hi[2] : C.ob_lo[2]) + to;
+        taken = vz;
         vz = 0.0;
       }
+      // the obstacle's share of the clamp (kleefsman_obstacle_3d.py:259-260);
+      // clamps are rare events, so one atomic each
+      atomicAdd(&e.ctl[c].clamp_impulse[axis], m * taken);
       atomicAdd(&e.ctl[c].clamps, 1ull);
     }
     if (!isfinite(px) || !isfinite(py) || !isfinite(pz) || !isfinite(vx) || !isfinite(vy) || !isfinite(vz)) {
@@ -1423,7 +1432,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_integrate(const __grid_constant__
 
 // Per-case meter row: max rho, max |v|, front x, obstacle force xyz, kinetic
 // and potential energy, escapes, clamps, rebuilds, longest row, step, status,
-// obstacle impulse x, c_ref.
+// obstacle impulse x, c_ref, the correction's log (16-19, written after the
+// update), obstacle impulse y and z, and the clamp impulse xyz.
 __global__ void k_finalize(Dev e) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= e.n_slots) return;
@@ -1459,6 +1469,11 @@ __global__ void k_finalize(Dev e) {
   t.tvc_sum = 0.0;
   t.tvc_kept = t.tvc_clipped = 0;
   row[16] = row[17] = row[18] = row[19] = 0.0;
+  row[20] = t.impulse[1];
+  row[21] = t.impulse[2];
+  // k_integrate ran before this kernel: the clamp impulse through this
+  // step's update, like the obstacle impulse through this step's force
+  for (int k = 0; k < 3; ++k) row[22 + k] = t.clamp_impulse[k];
 }
 
 // -------------------------------------------- transport-velocity correction ---
@@ -1543,7 +1558,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_tvc_apply(Dev e) {
 }
 
 // The correction's log in columns 16-19 of the step's meter row: max |shift|,
-// sum |shift|, kept and clipped counts.
+// sum |shift|, kept and clipped counts; the escape count again, with the
+// correction's own box clamps.
 __global__ void k_tvc_finish(Dev e) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= e.n_slots) return;
@@ -1555,6 +1571,7 @@ __global__ void k_tvc_finish(Dev e) {
   row[17] = t.tvc_sum;
   row[18] = static_cast<double>(t.tvc_kept);
   row[19] = static_cast<double>(t.tvc_clipped);
+  row[8] = static_cast<double>(t.escapes);
 }
 
 // ------------------------------------------------------------- shifting ---
@@ -2281,7 +2298,7 @@ CaseDev make_case_dev(const tsph_case_params& p, int64_t* ncells) {
 
 bool case_params_ok(const tsph_case_params* p) {
   if (!p || (p->dim != 2 && p->dim != 3) || p->n_fluid <= 0 || p->n_wall < 0 || p->n_obstacle < 0 ||
-      p->n_obstacle > p->n_wall || p->shift_every < 0)
+      p->n_obstacle > p->n_wall || p->shift_every < 0 || p->first_step < 0)
     return false;
   if (!(p->h > 0) || !(p->dt > 0) || !(p->skin >= 0) || !(p->rho0 > 0) || !(p->gamma > 0) ||
       !(p->sound_speed > 0))
@@ -2422,6 +2439,7 @@ int tsph_engine_add_case(tsph_engine* E, const tsph_case_params* p, const double
   CaseCtl ctl{};
   ctl.first = 1;
   ctl.active = 1;
+  ctl.steps = static_cast<unsigned long long>(p->first_step);
   TSPH_CUDA_CHECK(cudaMemcpyAsync(d.ctl + slot, &ctl, sizeof(CaseCtl), cudaMemcpyHostToDevice, s));
   TSPH_CUDA_CHECK(cudaMemsetAsync(d.diag + static_cast<int64_t>(slot) * d.diag_ring * kDiag, 0,
                                   static_cast<size_t>(d.diag_ring) * kDiag * sizeof(double), s));

@@ -40,7 +40,8 @@ FIT_NEIGHBORS = 128        # CSF curvature-fit row capacity (2-D, 4h + skin)
 DIAG_FIELDS = ("rho_max", "speed_max", "front", "force_x", "force_y", "force_z", "kinetic",
                "potential", "escapes", "clamps", "rebuilds", "row_max", "step", "status",
                "impulse_x", "c_reference", "tvc_max_shift", "tvc_shift_sum", "tvc_kept",
-               "tvc_clipped")
+               "tvc_clipped", "impulse_y", "impulse_z", "clamp_impulse_x", "clamp_impulse_y",
+               "clamp_impulse_z")
 
 
 def obstacle_lattice_3d(lo, hi, dx: float) -> torch.Tensor:
@@ -143,12 +144,13 @@ class CaseSpec:
 
 
 def _case_params(*, dim, n_fluid, n_wall, n_obstacle, cfg, h, wall_mass, box_hi, lo, hi,
-                 shift_every=0, obstacle=None):
+                 shift_every=0, obstacle=None, first_step=0):
     if cfg.density_diffusion > 0.0 and cfg.density_diffusion_form != "molteni":
         raise NotImplementedError("the device engine implements the 'molteni' diffusion form only")
     p = _lib.CaseParams()
     p.dim, p.n_fluid, p.n_wall, p.n_obstacle = dim, n_fluid, n_wall, n_obstacle
     p.shift_every = int(shift_every)
+    p.first_step = int(first_step)
     p.has_obstacle = 1 if obstacle is not None else 0
     p.h, p.rho0, p.sound_speed, p.gamma = h, cfg.rho0, cfg.sound_speed, cfg.gamma
     p.gravity, p.viscosity, p.wall_friction = cfg.gravity, cfg.viscosity, cfg.wall_friction
@@ -207,9 +209,10 @@ def dam_break_3d_host_state(cfg: DamBreak3DConfig, obstacle=None, seed=None):
 
 
 def dam_break_3d_case(cfg: DamBreak3DConfig, *, obstacle=None, shift_every: int = 0, seed=None,
-                      host_state=None, velocity=None, label: str = "") -> CaseSpec:
+                      host_state=None, velocity=None, first_step: int = 0, label: str = "") -> CaseSpec:
     """The 3-D dam break of ``tensorsph.dam_break_3d`` (optionally with the box
-    obstacle of kleefsman_obstacle_3d.py) as a ``CaseSpec``."""
+    obstacle of kleefsman_obstacle_3d.py) as a ``CaseSpec``; ``first_step``
+    numbers the first step of a resumed run."""
     if host_state is None:
         host_state = dam_break_3d_host_state(cfg, obstacle, seed)
     x, mass, wall, n_ob = host_state
@@ -222,7 +225,7 @@ def dam_break_3d_case(cfg: DamBreak3DConfig, *, obstacle=None, shift_every: int 
                      wall_mass=mass_3d(cfg.dx, cfg.h_factor, cfg.rho0, cfg.density_calibration),
                      box_hi=box, lo=allpos.min(dim=0).values.tolist(),
                      hi=allpos.max(dim=0).values.tolist(), shift_every=shift_every,
-                     obstacle=obstacle)
+                     obstacle=obstacle, first_step=first_step)
     v = torch.zeros_like(x) if velocity is None else velocity.double().contiguous()
     return CaseSpec(p, x, v, mass.double().contiguous(), wall, label or "dam_break_3d")
 
@@ -556,10 +559,12 @@ class DamBreak3DRun:
     steps_taken: int = 0
     simulated_time: float = 0.0
     obstacle_force: list = field(default_factory=list)
-    obstacle_impulse: list = field(default_factory=list)
+    obstacle_impulse: list = field(default_factory=list)   # SPH force impulse [x, y, z], N s
+    clamp_impulse: list = field(default_factory=list)      # obstacle clamp impulse [x, y, z], N s
     obstacle_clamps: int = 0
     snapshots: list = field(default_factory=list)
     tvc_log: list = field(default_factory=list)
+    resumed: bool = False
 
     @property
     def mass_drift(self) -> float:
@@ -571,9 +576,10 @@ class DamBreak3DEngine(BatchEngine):
 
     def __init__(self, cfg: DamBreak3DConfig, *, obstacle=None, shift_every: int = 0,
                  seed: int | None = None, max_neighbors: int = 160, diag_ring: int = 8192,
-                 device: torch.device | None = None, host_state=None):
+                 device: torch.device | None = None, host_state=None, velocity=None,
+                 first_step: int = 0):
         spec = dam_break_3d_case(cfg, obstacle=obstacle, shift_every=shift_every, seed=seed,
-                                 host_state=host_state)
+                                 host_state=host_state, velocity=velocity, first_step=first_step)
         super().__init__(**capacity_for([spec], max_neighbors=max_neighbors, diag_ring=diag_ring),
                          device=device)
         self.cfg = cfg
@@ -697,18 +703,20 @@ def _run_with_snapshots(eng, case_id, steps: int, plan) -> list:
     return snaps.result()
 
 
-def _tvc_log(cfg, diag, n_fluid: int) -> list:
+def _tvc_log(cfg, diag, n_fluid: int, first: int = 0, upto: int | None = None) -> list:
     """The reference's per-application log of the transport-velocity
-    correction (dam_break_3d.py:697-704) from the meter rows: steps
-    k = tvc_every, 2 tvc_every, ... before the last."""
+    correction (dam_break_3d.py:697-704) from the meter rows ``diag`` of
+    steps ``first, first + 1, ...``: steps k = tvc_every, 2 tvc_every, ...
+    below ``upto`` (default ``cfg.steps``) and from ``first`` on."""
     every = int(getattr(cfg, "tvc_every", 0) or 0)
     if not every:
         return []
+    upto = cfg.steps if upto is None else upto
     h = cfg.h_factor * cfg.dx
     out, elapsed = [], 0.0
-    for k in range(cfg.steps):
-        if k > 0 and k % every == 0:
-            row = diag[k]
+    for k in range(upto):
+        if k >= first and k > 0 and k % every == 0:
+            row = diag[k - first]
             out.append({"step": k, "time": elapsed,
                         "max_shift_over_h": float(row[16]) / h,
                         "mean_shift_over_h": float(row[17]) / n_fluid / h,
@@ -719,9 +727,79 @@ def _tvc_log(cfg, diag, n_fluid: int) -> list:
     return out
 
 
+def _elapsed_after(steps: int, dt: float) -> list:
+    """``out[k]``: simulated time at the start of step k, accumulated step by
+    step as the reference loops do."""
+    out, elapsed = [0.0], 0.0
+    for _ in range(steps + 1):
+        elapsed += dt
+        out.append(elapsed)
+    return out
+
+
+class _DeviceRecord:
+    """Series, maxima, counters and impulses of a 3-D device run through a
+    global step, from the meter rows of steps ``first, first + 1, ...`` and,
+    for a resumed run, the checkpoint it resumed from (whose series cover the
+    steps before ``first``)."""
+
+    def __init__(self, cfg, samples, first: int, prev: dict | None, n_fluid: int, initial_energy: float):
+        self.cfg, self.samples, self.first, self.n_fluid = cfg, samples, first, n_fluid
+        self.prev = prev or {}
+        self.dev = self.prev.get("device_run", {})
+        self.initial_energy = float(self.dev.get("initial_energy", initial_energy))
+
+    def collect(self, rows, upto: int) -> dict:
+        """Everything through global step ``upto``: samples and maxima over
+        rows ``first..upto``, forces, counters and impulses through the last
+        integrated step ``min(upto, steps - 1)``."""
+        cfg, first, prev, dev = self.cfg, self.first, self.prev, self.dev
+        rows = torch.as_tensor(rows)
+        new = [(k, t) for k, t in self.samples if first <= k <= upto]
+        last = min(upto, cfg.steps - 1) - first  # row of the last integrated step (< 0: none)
+
+        def series(key, col):
+            return list(prev.get(key, dev.get(key, []))) + [float(rows[k - first, col]) for k, _ in new]
+
+        out = {
+            "times": list(prev.get("times", [])) + [t for _, t in new],
+            "front": series("front", 2),
+            "kinetic_energy": list(dev.get("kinetic_energy", [])) + [float(rows[k - first, 6]) for k, _ in new],
+            "potential_energy": list(dev.get("potential_energy", [])) + [float(rows[k - first, 7]) for k, _ in new],
+            "speed_samples": list(dev.get("speed_samples", [])) + [float(rows[k - first, 1]) for k, _ in new],
+            "obstacle_force": list(dev.get("obstacle_force", [])) + (rows[:last + 1, 3:6].tolist() if last >= 0 else []),
+            "tvc_log": list(dev.get("tvc_log", [])) + _tvc_log(cfg, rows, self.n_fluid, first, min(upto + 1, cfg.steps)),
+        }
+        imp = [float(v) for v in prev.get("sph_impulse", [0.0, 0.0, 0.0])]
+        cimp = [float(v) for v in prev.get("clamp_impulse", [0.0, 0.0, 0.0])]
+        escapes, clamps, rebuilds = int(prev.get("escapes", 0)), int(prev.get("clamps", 0)), int(dev.get("rebuilds", 0))
+        if last >= 0:
+            r = rows[last]
+            imp = [imp[0] + float(r[14]), imp[1] + float(r[20]), imp[2] + float(r[21])]
+            cimp = [cimp[i] + float(r[22 + i]) for i in range(3)]
+            escapes, clamps, rebuilds = escapes + int(r[8]), clamps + int(r[9]), rebuilds + int(r[10])
+        seen = rows[:upto - first + 1]
+        speeds = float(prev.get("speeds", 0.0))
+        compression = float(prev.get("compression", -1.0))
+        if seen.shape[0]:
+            speeds = max(speeds, float(seen[:, 1].max()))
+            compression = max(compression, float(seen[:, 0].max()) / cfg.rho0 - 1.0)
+        out.update(sph_impulse=imp, clamp_impulse=cimp, escapes=escapes, clamps=clamps, rebuilds=rebuilds,
+                   speeds=speeds, compression=compression)
+        return out
+
+    def payload(self, rows, step: int) -> dict:
+        """What the checkpoint after the update of ``step`` stores."""
+        r = self.collect(rows, step)
+        keep = ("kinetic_energy", "potential_energy", "speed_samples", "obstacle_force", "tvc_log", "rebuilds")
+        extra = {"device_run": {**{k: r[k] for k in keep}, "initial_energy": self.initial_energy}}
+        return {**r, "dt": self.cfg.dt, "extra": extra}
+
+
 def run_case(cfg: DamBreak3DConfig, pair_skin_factor: float | None = None, snapshot_times=None,
              seed: int | None = None, *, obstacle=None, shift_every: int = 0,
-             max_neighbors: int = 160) -> DamBreak3DRun:
+             max_neighbors: int = 160, checkpoint_path=None, checkpoint_every: int = 0,
+             resume: bool = True) -> DamBreak3DRun:
     """Integrate the 3-D dam break on the GPU and return the run record.
 
     Same loop as dam_break_3d.py:569-734: ``cfg.steps`` steps of ``cfg.dt``,
@@ -730,43 +808,101 @@ def run_case(cfg: DamBreak3DConfig, pair_skin_factor: float | None = None, snaps
     ``snapshot_times`` fills ``run.snapshots`` with ``(time, positions,
     velocities)`` at the first sample point reaching each time, copied to the
     host while the loop goes on.
+
+    Checkpoints follow kleefsman_obstacle_3d.py:553-706: with
+    ``checkpoint_path`` naming an existing file and ``resume`` the run
+    continues from it (a file of another configuration or particle count is
+    refused); with ``checkpoint_every > 0`` the state after the update of
+    every step k with ``k % checkpoint_every == 0`` is written there in that
+    case's format (by ``CheckpointWriter``, off the step loop); a completed
+    run removes the file.  A resumed run rebuilds its neighbour lists at the
+    resume step, so it agrees with an uninterrupted one to round-off.
     """
+    from pathlib import Path
+    from .checkpoint import CheckpointWriter, load_checkpoint
     if cfg.adaptive_dt:
         raise NotImplementedError("adaptive_dt is not supported by the device engine")
     if pair_skin_factor is not None:
         from dataclasses import replace
         cfg = replace(cfg, pair_skin_factor=pair_skin_factor)
+    host = dam_break_3d_host_state(cfg, obstacle, seed)
+    prev = None
+    if checkpoint_path is not None and resume and Path(checkpoint_path).exists():
+        prev = load_checkpoint(checkpoint_path, cfg, obstacle)
+        if tuple(prev["positions"].shape) != tuple(host[0].shape):
+            raise ValueError(f"checkpoint holds {tuple(prev['positions'].shape)} particles, "
+                             f"this configuration builds {tuple(host[0].shape)}")
+        if "device_run" not in prev:
+            raise ValueError("checkpoint carries no device run record; it was written by another driver")
+        if prev["step"] + 1 > cfg.steps:
+            raise ValueError(f"checkpoint step {prev['step']} is not below the run's {cfg.steps} steps")
+    first = prev["step"] + 1 if prev else 0
+    if prev:
+        host = (prev["positions"].double(), host[1], host[2], host[3])
     eng = DamBreak3DEngine(cfg, obstacle=obstacle, shift_every=shift_every, seed=seed,
-                           max_neighbors=max_neighbors, diag_ring=max(cfg.steps + 2, 2))
+                           max_neighbors=max_neighbors, diag_ring=max(cfg.steps + 2, 2), host_state=host,
+                           velocity=prev["velocity"] if prev else None, first_step=first)
     samples = _sample_steps(cfg.steps, cfg.output_every, cfg.dt)
-    snapshots = _run_with_snapshots(eng, eng.case_id, cfg.steps, _snapshot_plan(snapshot_times, samples))
-    with torch.cuda.stream(eng.stream):
-        x, v, rho, p = eng.state()
-        xs, vs = x.cpu(), v.cpu()
-    st = eng.status()
-    # the reference evaluates the right-hand side once more at step == steps
-    # to record the final meters, without integrating it
-    eng.step(1)
-    with torch.cuda.stream(eng.stream):
-        diag = eng.diagnostics(0, cfg.steps + 1).cpu()
-    sample = [k for k, _ in samples]
-    times = [t for _, t in samples]
+    record = _DeviceRecord(cfg, samples, first, prev, eng.n_fluid, eng.initial_pe)
+    writer = None
+    if checkpoint_path is not None and checkpoint_every > 0:
+        writer = CheckpointWriter(eng, eng.case_id, checkpoint_path, cfg, obstacle=obstacle)
+    # (steps done, kind, arg): a snapshot before the update of its sample
+    # step, a checkpoint after the update of its step
+    events = [(k, 0, t) for k, t in _snapshot_plan(snapshot_times, samples) if k >= first]
+    if writer is not None:
+        events += [(k + 1, 1, k) for k in range(first, cfg.steps) if k % checkpoint_every == 0]
+    events.sort(key=lambda e: (e[0], e[1]))
+    after = _elapsed_after(cfg.steps, cfg.dt)
+    snaps = _Snapshots(eng, eng.case_id)
+    done = first
+    try:
+        for at, kind, arg in events:
+            if at > done:
+                eng.step(at - done)
+                done = at
+            if kind == 0:
+                snaps.take(arg)
+            else:
+                writer.take(arg, after[arg + 1], first, arg - first + 1,
+                            lambda rows, k=arg: record.payload(rows, k))
+        if cfg.steps > done:
+            eng.step(cfg.steps - done)
+        snapshots = snaps.result()
+        with torch.cuda.stream(eng.stream):
+            x, v, rho, p = eng.state()
+            xs, vs = x.cpu(), v.cpu()
+        eng.status()
+        # the reference evaluates the right-hand side once more at step == steps
+        # to record the final meters, without integrating it
+        eng.step(1)
+        with torch.cuda.stream(eng.stream):
+            diag = eng.diagnostics(first, cfg.steps + 1 - first).cpu()
+        if writer is not None:
+            writer.close()
+    finally:
+        if writer is not None and writer.thread is not None:
+            writer.thread.join()
+    rec = record.collect(diag, cfg.steps)
     run = DamBreak3DRun(
-        times=times, front=[float(diag[k, 2]) for k in sample],
-        kinetic_energy=[float(diag[k, 6]) for k in sample],
-        potential_energy=[float(diag[k, 7]) for k in sample],
-        mass=eng.initial_mass, escaped=int(st["escapes"]), rebuilds=int(st["rebuilds"]),
-        max_speed=max(float(diag[k, 1]) for k in sample),
-        max_density_compression=float(diag[:, 0].max()) / cfg.rho0 - 1.0,
-        initial_mass=eng.initial_mass, final_mass=eng.initial_mass, final_positions=xs,
-        initial_energy=eng.initial_pe, steps_taken=cfg.steps, simulated_time=cfg.steps * cfg.dt,
-        obstacle_force=diag[:cfg.steps, 3:6].tolist(),
-        obstacle_impulse=[float(diag[cfg.steps - 1, 14])] if cfg.steps else [],
-        obstacle_clamps=int(st["clamps"]), snapshots=snapshots, tvc_log=_tvc_log(cfg, diag, eng.n_fluid))
+        times=rec["times"], front=rec["front"], kinetic_energy=rec["kinetic_energy"],
+        potential_energy=rec["potential_energy"], mass=eng.initial_mass, escaped=rec["escapes"],
+        rebuilds=rec["rebuilds"], max_speed=max(rec["speed_samples"]),
+        max_density_compression=rec["compression"], initial_mass=eng.initial_mass,
+        final_mass=eng.initial_mass, final_positions=xs, initial_energy=record.initial_energy,
+        steps_taken=cfg.steps, simulated_time=cfg.steps * cfg.dt, obstacle_force=rec["obstacle_force"],
+        obstacle_impulse=rec["sph_impulse"], clamp_impulse=rec["clamp_impulse"],
+        obstacle_clamps=rec["clamps"], snapshots=snapshots, tvc_log=rec["tvc_log"], resumed=prev is not None)
     masses = eng.spec.mass
     run.final_energy = float(0.5 * (masses[:, None] * vs.square()).sum()
                              + (masses * cfg.gravity * xs[:, 1]).sum())
     eng.close()
+    if checkpoint_path is not None:
+        # a completed run must not be resumed by the next attempt
+        try:
+            Path(checkpoint_path).unlink()
+        except FileNotFoundError:
+            pass
     return run
 
 

@@ -677,6 +677,35 @@ def dam3d_run_case(d3):
             "max_density_compression": np.float64(run.max_density_compression)}
 
 
+def checkpoint_case(kl):
+    """A checkpoint file as the obstacle case writes it (save_checkpoint,
+    kleefsman_obstacle_3d.py:499-528): its bytes, the configuration's
+    fingerprint and the inputs, for the format tests."""
+    import json
+    import tempfile
+    cfg = kl.Kleefsman3DConfig(dx=0.05)
+    g = torch.Generator().manual_seed(300)
+    pos = torch.rand((12, 3), generator=g, dtype=torch.float64)
+    vel = torch.randn((12, 3), generator=g, dtype=torch.float64)
+    run = kl.Kleefsman3DRun(cfg=cfg, fluid_particles=12, wall_particles=5)
+    run.times, run.slab, run.local_h2 = [0.0, 0.0065], [0.01, 0.02], [0.011, 0.021]
+    run.height, run.front, run.bypass = [0.012, 0.022], [1.2, 1.3], [0.0, 1.0]
+    run.sph_impulse, run.clamp_impulse = [0.5, -0.25, 0.125], [0.0, 0.03125, 0.0]
+    args = dict(step=25, elapsed=0.0065, dt=2.6e-4, speeds=1.5, compression=0.01, escapes=2, clamps=1)
+    with tempfile.TemporaryDirectory() as d:
+        path = Path(d) / "state.pt"
+        kl.save_checkpoint(path, cfg, positions=pos, velocity=vel, run=run, **args)
+        raw = path.read_bytes()
+    series = {k: getattr(run, k) for k in ("times", "slab", "local_h2", "height", "front", "bypass",
+                                           "sph_impulse", "clamp_impulse")}
+    return {"raw": np.frombuffer(raw, dtype=np.uint8).copy(),
+            "fingerprint": np.array(json.dumps(kl.checkpoint_fingerprint(cfg))),
+            "fields": np.array(json.dumps(list(kl.CHECKPOINT_FINGERPRINT_FIELDS))),
+            "version": np.array(kl.CHECKPOINT_VERSION),
+            "args": np.array(json.dumps(args)), "series": np.array(json.dumps(series)),
+            "pos": _np(pos), "vel": _np(vel)}
+
+
 def main(src, families=None):
     sys.path.insert(0, str(src))
     import tensorsph.neighbor_search as ns
@@ -693,6 +722,7 @@ def main(src, families=None):
     from tensorsph.threed import csf3 as c3
     from tensorsph.threed import liquid_column as lc
     import tensorsph.transport_velocity_correction as tv
+    import tensorsph.kleefsman_obstacle_3d as kl
 
     meta = {"torch_version": np.array(torch.__version__)}
     torch.set_num_threads(1)
@@ -713,6 +743,7 @@ def main(src, families=None):
         "csf2d": lambda: csf2d_cases(ca, di),
         "config1_run": lambda: config1_run_case(db),
         "dam3d_run": lambda: dam3d_run_case(d3),
+        "checkpoint": lambda: checkpoint_case(kl),
     }
     for name in families or makers:
         np.savez_compressed(OUT / f"{name}.npz", **makers[name](), **meta)
