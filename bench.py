@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--csf3-radius", type=int, default=40, help="column radius in dx (0: no 3-D CSF leg)")
     ap.add_argument("--csf3-length", type=int, default=200, help="column period in dx")
     ap.add_argument("--tvc-n", type=int, default=100, help="fluid block edge in dx (0: no TVC leg)")
+    ap.add_argument("--ckpt-steps", type=int, default=200, help="steps of the checkpoint leg (0: no leg)")
+    ap.add_argument("--ckpt-every", type=int, default=100, help="checkpoint interval of the checkpoint leg")
     return ap.parse_args()
 
 
@@ -392,6 +394,71 @@ def tvc_leg(args, dev):
                            "sample": "16^3 block: pairs + gradient integral + displacement"}}
 
 
+def checkpoint_leg(args, dev, cfg, obstacle, host, tuning):
+    """The headline run with crash-safe checkpoints (the obstacle case's
+    format, kleefsman_obstacle_3d.py:477-546) every ``--ckpt-every`` steps,
+    against the same steps without: device time of the step loop on the
+    engine's stream (the state read kernel is on it; the copies to pinned
+    memory are on a side stream and the file write on a thread), the wall
+    time of the loop, and each write's time on its thread."""
+    import shutil
+    import tempfile
+
+    import torch
+    from tensorsph_b200.checkpoint import CheckpointWriter
+    from tensorsph_b200.engine import DamBreak3DEngine, _DeviceRecord, _elapsed_after, _sample_steps
+    steps, every, warm = args.ckpt_steps, max(args.ckpt_every, 1), 3
+    folder = tempfile.mkdtemp(prefix="tsph_ckpt_")
+    path = os.path.join(folder, "state.pt")
+    out = {"steps": steps, "every": every}
+    try:
+        for mode in ("plain", "checkpoint"):
+            eng = DamBreak3DEngine(cfg, obstacle=obstacle, shift_every=args.shift_every, host_state=host,
+                                   diag_ring=steps + warm + 16, device=dev)
+            if tuning is not None:
+                eng.set_block(tuning["best"]["block"])
+                eng.set_batch(tuning["best"]["batch"])
+            eng.step(warm)
+            torch.cuda.synchronize(dev)
+            writer = None
+            if mode == "checkpoint":
+                writer = CheckpointWriter(eng, eng.case_id, path, cfg, obstacle=obstacle)
+                record = _DeviceRecord(cfg, _sample_steps(cfg.steps, cfg.output_every, cfg.dt), 0, None,
+                                       eng.n_fluid, eng.initial_pe)
+                after = _elapsed_after(cfg.steps, cfg.dt)
+            start = torch.cuda.Event(enable_timing=True)
+            stop = torch.cuda.Event(enable_timing=True)
+            t0 = time.perf_counter()
+            start.record(eng.stream)
+            done = warm
+            for _ in range(steps // every):
+                eng.step(every)
+                done += every
+                if writer is not None:
+                    k = done - 1
+                    writer.take(k, after[k + 1], 0, k + 1, lambda rows, k=k: record.payload(rows, k))
+            stop.record(eng.stream)
+            torch.cuda.synchronize(dev)
+            loop_s = time.perf_counter() - t0
+            row = {"device_ms_per_step": start.elapsed_time(stop) / (done - warm),
+                   "wall_ms_per_step": loop_s * 1e3 / (done - warm)}
+            if writer is not None:
+                writer.close()
+                row.update(written=writer.written, write_s=writer.write_seconds,
+                           file_bytes=os.path.getsize(path),
+                           drain_s=time.perf_counter() - t0 - loop_s)
+            out[mode] = row
+            eng.close()
+            del eng
+            torch.cuda.empty_cache()
+        p, c = out["plain"], out["checkpoint"]
+        out["device_overhead"] = c["device_ms_per_step"] / p["device_ms_per_step"] - 1.0
+        out["wall_overhead"] = c["wall_ms_per_step"] / p["wall_ms_per_step"] - 1.0
+    finally:
+        shutil.rmtree(folder, ignore_errors=True)
+    return out
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -533,6 +600,12 @@ def main():
                          f"({n_cpu} fluid), {t_cpu:.1f} s"}
 
     extra = {}
+    if rank == 0 and world == 1 and args.ckpt_steps > 0:
+        try:
+            extra["checkpoint"] = checkpoint_leg(args, dev, cfg, obstacle, host, tuning)
+        except Exception as exc:  # reported, never hides the headline
+            extra["checkpoint"] = {"error": f"{type(exc).__name__}: {exc}"}
+        torch.cuda.empty_cache()
     if rank == 0 and world == 1:
         for name, leg, on in (("ensemble", ensemble_leg, args.ensemble_cases > 0),
                               ("serving", serving_leg, args.serve_requests > 0),

@@ -252,13 +252,14 @@ int tsph_csf3_acceleration(const tsph_csf3_params* prm, const void* normal, cons
 /* ------------------------------------------------------------------------ */
 /* 2-D CSF surface tension: tensorsph.csf_consistent.csf_fields and         */
 /* surface_tension_acceleration (csf_consistent.py:90-446,                  */
-/* csf_curvature.py:78-166) over the symmetric rows of a pair list.         */
+/* csf_curvature.py:78-213) over the symmetric rows of a pair list.         */
 /* ------------------------------------------------------------------------ */
 typedef struct {
   int64_t n, dtype;            /* particles; TSPH_F32 or TSPH_F64           */
   int64_t normal_smoothing;    /* Shepard passes on the normal              */
   int64_t color_smoothing;     /* curvature from a colour smoothed this often */
-  int64_t curvature;           /* 0 "mls" (div n), 1 "fit_quadratic"        */
+  int64_t curvature;           /* 0 "mls" (div n), 1 "fit_quadratic",       */
+                               /* 2 "fit_circle"                            */
   int64_t delta_normalization; /* 0 "legacy" (2|grad c|), 1 "local_range"   */
   double h, rho0;              /* smoothing length; V = m / rho0            */
   double stencil;              /* fit stencil in units of h (4)             */

@@ -17,7 +17,8 @@ numpy restatement of the 2-D surface-tension path the droplet case runs
   of each particle over the 4h stencil, weights w_j = clamp(delta_s_j /
   max delta_s), kappa = -2a / (1 + b^2)^1.5 where the particle is active
   (w > 0.05) and the 3x3 system is regular (|det| > 1e-6 max|det|), else
-  kappa_mls (csf_curvature.py:78-166);
+  kappa_mls (csf_curvature.py:78-166); or the Pratt circle fit with the same
+  weights (``curvature_scheme="fit_circle"``, :179-213);
 * a = -sigma kappa delta_s n / rho with delta_s = 0 where |grad c| <= 1e-3 max
   (csf_consistent.py:384-446).  All pairs are the 4h list, as the reference
   builds it for the fit (:415-421).
@@ -152,6 +153,51 @@ def fit_curvature_quadratic(pos, normal, delta_s, pairs, h, fallback, stencil=4.
     return np.where(ok, kappa, fallback).astype(pos.dtype)
 
 
+def fit_curvature_circle(pos, normal, delta_s, pairs, h, fallback, stencil=4.0, min_weight_fraction=0.05):
+    """Pratt algebraic circle fit x^2 + y^2 + D x + E y + F = 0 in the frame
+    centred on each particle, same weights and activity as the quadratic fit;
+    kappa = -sign(c . n) / r with c = -(D, E) / 2, r = sqrt(|c|^2 - F), where
+    the 3x3 system is regular and c . n != 0 (csf_curvature.py:179-213)."""
+    T = pos.dtype.type
+    n = pos.shape[0]
+    ds_max = max(delta_s.max(), T(1e-30))
+    w_node = np.clip(delta_s / ds_max, T(0), T(1))
+    i, j = pairs[:, 0], pairs[:, 1]
+    delta = pos[i] - pos[j]
+    r = np.sqrt((delta * delta).sum(1))
+    inside = r <= T(stencil * h)
+    w_ij = np.where(inside, w_node[j], T(0))
+    w_ji = np.where(inside, w_node[i], T(0))
+    active = w_node > min_weight_fraction
+
+    def moments(x, y, w, dst):
+        f = x * x + y * y
+        feats = np.stack([np.ones_like(x), x, y, x * x, x * y, y * y, x * f, y * f, f]) * w
+        out = np.zeros((9, n), dtype=pos.dtype)
+        for k in range(9):
+            np.add.at(out[k], dst, feats[k])
+        return out
+
+    z = moments(-delta[:, 0], -delta[:, 1], w_ij, i) + moments(delta[:, 0], delta[:, 1], w_ji, j)
+    z[0] = z[0] + w_node
+    mat = np.zeros((n, 3, 3), dtype=pos.dtype)
+    mat[:, 0] = np.stack([z[3], z[4], z[1]], 1)
+    mat[:, 1] = np.stack([z[4], z[5], z[2]], 1)
+    mat[:, 2] = np.stack([z[1], z[2], z[0]], 1)
+    rhs = -np.stack([z[6], z[7], z[8]], 1)
+    det = np.linalg.det(mat)
+    scale = max(np.abs(det).max(), T(1e-30))
+    ok = active & (np.abs(det) > T(1e-6) * scale)
+    mat[~ok] = np.eye(3, dtype=pos.dtype)
+    sol = np.linalg.solve(mat, rhs[..., None])[..., 0]
+    cx, cy = T(-0.5) * sol[:, 0], T(-0.5) * sol[:, 1]
+    rad = np.sqrt(np.maximum(cx * cx + cy * cy - sol[:, 2], T(1e-30)))
+    sign = np.sign(cx * normal[:, 0] + cy * normal[:, 1])
+    kappa = -sign / np.maximum(rad, T(1e-30))
+    ok = ok & (sign != 0)
+    return np.where(ok, kappa, fallback).astype(pos.dtype)
+
+
 def _normal(pos, field, vol, pairs, h, m, passes):
     """Outward normal of a colour field with ``passes`` Shepard passes."""
     T = pos.dtype.type
@@ -192,8 +238,12 @@ def csf_fields(pos, mass, pairs, h, rho0, normal_smoothing=2, stencil=4.0, curva
     else:
         kappa = mls_divergence(pos, normal, vol, pairs, h, m)
     delta_s = T(2) * mag if delta_normalization == "legacy" else mag / colour_range(c, pairs)
-    if curvature_scheme != "mls":
+    if curvature_scheme == "fit_quadratic":
         kappa = fit_curvature_quadratic(pos, normal, delta_s, pairs, h, kappa, stencil=stencil)
+    elif curvature_scheme == "fit_circle":
+        kappa = fit_curvature_circle(pos, normal, delta_s, pairs, h, kappa, stencil=stencil)
+    elif curvature_scheme != "mls":
+        raise ValueError(f"unknown curvature_scheme {curvature_scheme!r}")
     return {"color": c, "grad_c": grad_c, "normal": normal, "kappa": kappa, "delta_s": delta_s}
 
 

@@ -22,6 +22,7 @@ from __future__ import annotations
 
 import os
 import threading
+import time
 from pathlib import Path
 
 import torch
@@ -161,6 +162,7 @@ class CheckpointWriter:
         self.thread: threading.Thread | None = None
         self.error: BaseException | None = None
         self.written = 0
+        self.write_seconds: list[float] = []  # per file: copies awaited, payload built, written
 
     def take(self, step: int, elapsed: float, first_row: int, rows: int, assemble) -> None:
         """Checkpoint the state after the update of global step ``step``;
@@ -180,6 +182,7 @@ class CheckpointWriter:
             done.record(self.side)
 
         def write():
+            t0 = time.perf_counter()
             try:
                 done.synchronize()
                 info = assemble(hd)
@@ -189,6 +192,7 @@ class CheckpointWriter:
                                 compression=info["compression"], escapes=info["escapes"],
                                 clamps=info["clamps"], obstacle=self.obstacle, extra=info.get("extra"))
                 self.written += 1
+                self.write_seconds.append(time.perf_counter() - t0)
             except BaseException as exc:  # re-raised on the caller's thread
                 self.error = exc
 

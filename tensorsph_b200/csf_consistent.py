@@ -7,10 +7,11 @@ signatures and the ``CSFState`` fields (csf_consistent.py:75-446):
 * MLS gradient ``M^-T sum_j V_j (c_j - c_i) grad_i W`` with the identity
   for ``|det M| <= 1e-4 median |det M|``;
 * normal ``-grad c / |grad c|`` with ``normal_smoothing`` Shepard passes;
-* curvature ``div n`` (``"mls"``) or the weighted quadratic interface fit
-  over ``curvature_stencil * h`` (``"fit_quadratic"``, csf_curvature.py:78-166,
-  the MLS value where the fit is not regular), optionally from the normal of
-  a Shepard-smoothed colour (``curvature_color_smoothing``);
+* curvature ``div n`` (``"mls"``), the weighted quadratic interface fit over
+  ``curvature_stencil * h`` (``"fit_quadratic"``, csf_curvature.py:78-166) or
+  the Pratt circle fit with the same weights (``"fit_circle"``, :179-213),
+  the MLS value where a fit is not regular; ``div n`` optionally from the
+  normal of a Shepard-smoothed colour (``curvature_color_smoothing``);
 * ``delta_s = 2 |grad c|`` (``"legacy"``) or ``|grad c| / clip(max c - min c,
   0.2, 1)`` over the neighbourhood (``"local_range"``);
 * ``a = -sigma kappa delta_s n / rho`` with ``delta_s = 0`` where
@@ -19,8 +20,7 @@ signatures and the ``CSFState`` fields (csf_consistent.py:75-446):
 
 All of it runs in the kernels of ``csrc/csf2.cu`` over symmetric pair rows,
 in the dtype of the positions.  Contact angles (``wall`` + ``contact_angle``)
-and the ``"fit_circle"`` curvature are not built and raise
-``NotImplementedError``.
+are not built and raise ``NotImplementedError``.
 """
 from __future__ import annotations
 
@@ -35,7 +35,7 @@ from .droplet_impact import symmetric_rows
 __all__ = ["CSFState", "csf_fields", "surface_tension_acceleration", "CONTACT_ANGLE_REACH"]
 
 CONTACT_ANGLE_REACH = 2.0
-_CURVATURE = {"mls": 0, "fit_quadratic": 1}
+_CURVATURE = {"mls": 0, "fit_quadratic": 1, "fit_circle": 2}
 _DELTA = {"legacy": 0, "local_range": 1}
 
 
@@ -59,8 +59,6 @@ def _options(curvature_scheme, delta_normalization, wall, contact_angle):
     if delta_normalization not in _DELTA:
         raise ValueError(f"unknown delta_normalization {delta_normalization!r}; "
                          "expected ('legacy', 'local_range')")
-    if curvature_scheme == "fit_circle":
-        raise NotImplementedError("the 'fit_circle' curvature is not built; use 'fit_quadratic' or 'mls'")
     if curvature_scheme not in _CURVATURE:
         raise ValueError(f"unknown curvature_scheme {curvature_scheme!r}")
     if wall is not None and contact_angle is not None:

@@ -18,6 +18,10 @@
 //                       rows within stencil h, weights clip(delta_s_j / max, 0, 1);
 //                       kappa = -2a / (1 + b^2)^1.5 where the particle's weight
 //                       > 0.05 and |det| > 1e-6 max |det| (csf_curvature.py:78-166)
+//      or circle fit    Pratt: x^2 + y^2 + D x + E y + F = 0 in the particle-centred
+//                       frame, same weights; centre c = -(D, E) / 2, radius
+//                       sqrt(|c|^2 - F), kappa = -sign(c . n) / r where the system
+//                       is regular and c . n != 0 (csf_curvature.py:179-213)
 //   A  acceleration     delta_s = 0 where |grad c| <= 1e-3 max |grad c|;
 //                       a = -sigma kappa delta_s n / rho
 // One thread per row, sums in a fixed order; the global maxima are exact
@@ -251,6 +255,95 @@ __global__ void k2_delta(C2<T> p, int local_range, const int64_t* __restrict__ r
   }
 }
 
+// determinant of the row-major 3x3 matrix (a b c; d e f; g h i)
+template <class T>
+__device__ __forceinline__ T det3(T a, T b, T c, T d, T e, T f, T g, T h, T i) {
+  return a * (e * i - f * h) - b * (d * i - f * g) + c * (d * h - e * g);
+}
+
+// K7a (circle): moments z[0..8] of (1, x, y, x^2, xy, y^2, x f, y f, f), f = x^2 + y^2,
+// over the neighbours' offsets x_b - x_a within the stencil; the determinant
+// of [[z3 z4 z1] [z4 z5 z2] [z1 z2 z0]] (+ its maximum)
+template <class T>
+__global__ void k2_circle_moments(C2<T> p, const T* __restrict__ xy, const int64_t* __restrict__ rowptr,
+                                  const uint32_t* __restrict__ ent, const T* __restrict__ delta_s,
+                                  const unsigned long long* __restrict__ maxima, T* __restrict__ mom,
+                                  T* __restrict__ fdet, unsigned long long* __restrict__ fmax) {
+  const T dsm = from_bits<T>(maxima[0]);
+  const T ds_max = dsm > T(1e-30) ? dsm : T(1e-30);
+  unsigned long long mb = 0;
+  for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < p.n; a += gridDim.x * blockDim.x) {
+    const T xa = xy[2 * a], ya = xy[2 * a + 1];
+    CSum<T> z[9];
+    T wa = delta_s[a] / ds_max;
+    wa = wa < T(0) ? T(0) : (wa > T(1) ? T(1) : wa);
+    z[0].add(wa);
+    for (int64_t e = rowptr[a]; e < rowptr[a + 1]; ++e) {
+      const int64_t b = ent[e] & kIndexMask;
+      const T x = xy[2 * b] - xa, y = xy[2 * b + 1] - ya;
+      const T r = sqrt(x * x + y * y);
+      if (!(r <= p.stencil_r)) continue;
+      T w = delta_s[b] / ds_max;
+      w = w < T(0) ? T(0) : (w > T(1) ? T(1) : w);
+      const T f = x * x + y * y;
+      z[0].add(w);
+      z[1].add(x * w);
+      z[2].add(y * w);
+      z[3].add(x * x * w);
+      z[4].add(x * y * w);
+      z[5].add(y * y * w);
+      z[6].add(x * f * w);
+      z[7].add(y * f * w);
+      z[8].add(f * w);
+    }
+    T zv[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      zv[k] = z[k].value();
+      mom[9 * a + k] = zv[k];
+    }
+    const T d = det3(zv[3], zv[4], zv[1], zv[4], zv[5], zv[2], zv[1], zv[2], zv[0]);
+    fdet[a] = d;
+    const unsigned long long bits = bits_of<T>(d < T(0) ? -d : d);
+    mb = bits > mb ? bits : mb;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long x = __shfl_xor_sync(0xffffffffu, mb, o);
+    mb = x > mb ? x : mb;
+  }
+  if ((threadIdx.x & 31) == 0) atomicMax(fmax, mb);
+}
+
+// K7b (circle): (D, E, F) by Cramer's rule, kappa where the fit holds
+template <class T>
+__global__ void k2_circle_solve(C2<T> p, const T* __restrict__ delta_s, const T* __restrict__ normal,
+                                const unsigned long long* __restrict__ maxima, const T* __restrict__ mom,
+                                const T* __restrict__ fdet, const unsigned long long* __restrict__ fmax,
+                                T* __restrict__ kappa) {
+  const T dsm = from_bits<T>(maxima[0]);
+  const T ds_max = dsm > T(1e-30) ? dsm : T(1e-30);
+  const T dm = from_bits<T>(*fmax);
+  const T scale = dm > T(1e-30) ? dm : T(1e-30);
+  for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < p.n; a += gridDim.x * blockDim.x) {
+    T wa = delta_s[a] / ds_max;
+    wa = wa < T(0) ? T(0) : (wa > T(1) ? T(1) : wa);
+    const T d = fdet[a];
+    if (!(wa > T(0.05)) || !((d < T(0) ? -d : d) > T(1e-6) * scale)) continue;  // keep the MLS value
+    const T* z = mom + 9 * a;
+    const T r0 = -z[6], r1 = -z[7], r2 = -z[8];
+    const T dd = det3(r0, z[4], z[1], r1, z[5], z[2], r2, z[2], z[0]) / d;
+    const T de = det3(z[3], r0, z[1], z[4], r1, z[2], z[1], r2, z[0]) / d;
+    const T df = det3(z[3], z[4], r0, z[4], z[5], r1, z[1], z[2], r2) / d;
+    const T cx = T(-0.5) * dd, cy = T(-0.5) * de;
+    const T q = cx * cx + cy * cy - df;
+    const T rad = sqrt(q > T(1e-30) ? q : T(1e-30));
+    const T side = cx * normal[2 * a] + cy * normal[2 * a + 1];
+    if (side == T(0)) continue;
+    const T sign = side > T(0) ? T(1) : T(-1);
+    kappa[a] = -sign / (rad > T(1e-30) ? rad : T(1e-30));
+  }
+}
+
 // K7a: fit moments s[0..7] and the 3x3 determinant (+ its maximum)
 template <class T>
 __global__ void k2_fit_moments(C2<T> p, const T* __restrict__ xy, const int64_t* __restrict__ rowptr,
@@ -394,7 +487,7 @@ L2 layout2(int64_t n, int64_t dtype) {
   L.grad_s = take(2 * n * t);
   L.mag_s = take(n * t);
   L.normal_s = take(2 * n * t);
-  L.mom = take(8 * n * t);
+  L.mom = take(9 * n * t);
   L.fdet = take(n * t);
   L.maxima = take(4 * 8);
   L.total = off;
@@ -498,6 +591,12 @@ int run_csf2(const tsph_csf2_params& prm, const tsph_csf2_io& io, char* ws, cuda
                                         maxima + 2);
     k2_fit_solve<T><<<g, 128, 0, s>>>(p, delta_s, maxima, mom, fdet, maxima + 2, kappa);
     TSPH_LAUNCH_CHECK();
+  } else if (prm.curvature == 2) {
+    T* mom = reinterpret_cast<T*>(ws + L.mom);
+    T* fdet = reinterpret_cast<T*>(ws + L.fdet);
+    k2_circle_moments<T><<<g, 128, 0, s>>>(p, xy, io.rowptr, io.entries, delta_s, maxima, mom, fdet, maxima + 2);
+    k2_circle_solve<T><<<g, 128, 0, s>>>(p, delta_s, normal, maxima, mom, fdet, maxima + 2, kappa);
+    TSPH_LAUNCH_CHECK();
   }
   return TSPH_OK;
 }
@@ -521,7 +620,7 @@ int run_accel2(const tsph_csf2_params& prm, const void* grad, const void* normal
 bool params2_ok(const tsph_csf2_params* p) {
   return p && p->n >= 0 && p->n < (int64_t(1) << 31) && p->h > 0.0 && p->rho0 > 0.0 &&
          (p->dtype == TSPH_F32 || p->dtype == TSPH_F64) && p->normal_smoothing >= 0 && p->normal_smoothing <= 64 &&
-         p->color_smoothing >= 0 && p->color_smoothing <= 64 && (p->curvature == 0 || p->curvature == 1) &&
+         p->color_smoothing >= 0 && p->color_smoothing <= 64 && (p->curvature >= 0 && p->curvature <= 2) &&
          (p->delta_normalization == 0 || p->delta_normalization == 1) && p->stencil > 0.0;
 }
 

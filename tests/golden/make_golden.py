@@ -532,8 +532,8 @@ def tvc_cases(tv, ns):
 
 
 def csf2d_cases(ca, di):
-    """2-D CSF variants (csf_consistent.py:262-446): curvature "mls" and
-    "fit_quadratic", delta_s "legacy" and "local_range", normal smoothing off,
+    """2-D CSF variants (csf_consistent.py:262-446): curvature "mls",
+    "fit_quadratic" and "fit_circle", delta_s "legacy" and "local_range", normal smoothing off,
     curvature from a smoothed colour field, FP64 and FP32, through
     surface_tension_acceleration (the 4h list for the fit) and through direct
     csf_fields calls on a 2h list (the smoothing options are csf_fields
@@ -547,6 +547,10 @@ def csf2d_cases(ca, di):
         ("jitter", torch.float64, dict(curvature_scheme="mls", normal_smoothing=0, direct=True)),
         ("jitter", torch.float32, dict(curvature_scheme="fit_quadratic")),
         ("jitter", torch.float64, dict(curvature_scheme="fit_quadratic", direct=True)),
+        ("pool", torch.float64, dict(curvature_scheme="fit_circle")),
+        ("jitter", torch.float64, dict(curvature_scheme="fit_circle", delta_normalization="local_range")),
+        ("jitter", torch.float32, dict(curvature_scheme="fit_circle")),
+        ("jitter", torch.float64, dict(curvature_scheme="fit_circle", direct=True)),
     ]
     for k, (kind, dtype, o) in enumerate(variants):
         g = torch.Generator().manual_seed(300 + k)

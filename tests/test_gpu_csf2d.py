@@ -1,5 +1,5 @@
 """2-D CSF drop-in (csf_fields / surface_tension_acceleration with the
-"mls" and "fit_quadratic" curvatures, "legacy" and "local_range" delta_s,
+"mls", "fit_quadratic" and "fit_circle" curvatures, "legacy" and "local_range" delta_s,
 normal smoothing off, curvature from a smoothed colour) on the GPU against
 the reference's own outputs (tests/golden/csf2d.npz, csf.npz).
 
@@ -89,8 +89,8 @@ def test_csf2d_options_and_errors(gpu):
     pairs = torch.zeros((0, 2), dtype=torch.int64, device="cuda")
     a, st = cc.surface_tension_acceleration(pos, mass * 1e6, mass, pairs, 0.002, 0.0)
     assert st is None and float(a.abs().max()) == 0.0
-    with pytest.raises(NotImplementedError):
-        cc.csf_fields(pos, mass, pairs, 0.002, 1000.0, curvature_scheme="fit_circle")
+    with pytest.raises(ValueError):
+        cc.csf_fields(pos, mass, pairs, 0.002, 1000.0, curvature_scheme="fit_ellipse")
     with pytest.raises(ValueError):
         cc.csf_fields(pos, mass, pairs, 0.002, 1000.0, delta_normalization="other")
     with pytest.raises(NotImplementedError):
