@@ -198,10 +198,13 @@ def fit_curvature_circle(pos, normal, delta_s, pairs, h, fallback, stencil=4.0, 
     return np.where(ok, kappa, fallback).astype(pos.dtype)
 
 
-def _normal(pos, field, vol, pairs, h, m, passes):
-    """Outward normal of a colour field with ``passes`` Shepard passes."""
+def _normal(pos, field, vol, pairs, h, m, passes, bc=None):
+    """Outward normal of a colour field with ``passes`` Shepard passes
+    (``bc``: the wall boundary applied to the gradient first)."""
     T = pos.dtype.type
     grad = mls_gradient(pos, field, vol, pairs, h, m)
+    if bc is not None:
+        grad = bc(grad)
     mag = np.sqrt((grad * grad).sum(1))
     tiny = T(1e-12)
     normal = np.where(mag[:, None] > tiny, -grad / np.maximum(mag, tiny)[:, None], T(0))
@@ -225,15 +228,25 @@ def colour_range(color, pairs):
 
 
 def csf_fields(pos, mass, pairs, h, rho0, normal_smoothing=2, stencil=4.0, curvature_scheme="fit_quadratic",
-               curvature_color_smoothing=0, delta_normalization="legacy"):
+               curvature_color_smoothing=0, delta_normalization="legacy", wall=None, contact_angle=None,
+               contact_angle_reach=2.0):
+    """The fields of csf_consistent.py:262-381; with ``wall`` and
+    ``contact_angle`` the contact-angle boundary acts on both colour gradients
+    (:309-311, :330-332)."""
     T = pos.dtype.type
     vol = (mass / T(rho0)).astype(pos.dtype)
     c = colour(pos, vol, pairs, h)
     m, _ = mls_matrix(pos, vol, pairs, h)
-    grad_c, mag, normal = _normal(pos, c, vol, pairs, h, m, normal_smoothing)
+    bc = None
+    if wall is not None and contact_angle is not None:
+        from .contact_angle import apply_contact_angle_boundary
+
+        def bc(g):
+            return apply_contact_angle_boundary(g, pos, wall, h, contact_angle, contact_angle_reach)
+    grad_c, mag, normal = _normal(pos, c, vol, pairs, h, m, normal_smoothing, bc)
     if curvature_color_smoothing > 0:
         c_s = np.clip(shepard_smooth(c[:, None], pos, vol, pairs, h, curvature_color_smoothing)[:, 0], T(0), T(1))
-        _, _, normal_s = _normal(pos, c_s, vol, pairs, h, m, normal_smoothing)
+        _, _, normal_s = _normal(pos, c_s, vol, pairs, h, m, normal_smoothing, bc)
         kappa = mls_divergence(pos, normal_s, vol, pairs, h, m)
     else:
         kappa = mls_divergence(pos, normal, vol, pairs, h, m)
@@ -248,17 +261,26 @@ def csf_fields(pos, mass, pairs, h, rho0, normal_smoothing=2, stencil=4.0, curva
 
 
 def surface_tension_acceleration(pos, density, mass, h, sigma, rho0, stencil=4.0, pairs=None,
-                                 curvature_scheme="fit_quadratic", delta_normalization="legacy"):
+                                 curvature_scheme="fit_quadratic", delta_normalization="legacy", wall=None,
+                                 contact_angle=None, contact_angle_reach=2.0, contact_angle_model="rotate"):
     """CSF acceleration of a 2-D fluid cloud and its fields (with a fit, the
-    4h pair list is built here, as the reference does)."""
+    4h pair list is built here, as the reference does); with a wall and a
+    contact angle either the normal boundary ("rotate") or the wall-adhesion
+    traction ("young", "brackbill") of csf_consistent.py:411-443."""
     T = pos.dtype.type
     if curvature_scheme != "mls" or pairs is None:
         pairs = cell_linked_pairs(pos, stencil * h)
+    model = contact_angle_model if contact_angle is not None else None
+    rotate = model in (None, "rotate")
     st = csf_fields(pos, mass, pairs, h, rho0, stencil=stencil, curvature_scheme=curvature_scheme,
-                    delta_normalization=delta_normalization)
+                    delta_normalization=delta_normalization, wall=wall,
+                    contact_angle=contact_angle if rotate else None, contact_angle_reach=contact_angle_reach)
     mag = np.sqrt((st["grad_c"] ** 2).sum(1))
     ds = st["delta_s"].copy()
     ds[mag <= T(1e-3) * mag.max()] = T(0)
     st["delta_s"] = ds
     force = (T(-sigma) * st["kappa"] * ds)[:, None] * st["normal"]
+    if model in ("young", "brackbill") and wall is not None:
+        from .contact_angle import wall_adhesion_force
+        force = force + wall_adhesion_force(pos, wall, st["normal"], contact_angle, sigma, ds, h, model=model)
     return (force / density[:, None]).astype(pos.dtype), st

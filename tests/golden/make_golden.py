@@ -590,6 +590,69 @@ def csf2d_cases(ca, di):
     return data
 
 
+def contact_cases(ca, seed=400):
+    """The contact-angle terms of the 2-D CSF (csf_consistent.py:411-560,
+    contact_angle_isph.py:75-213) on a jittered sessile half-drop (radius
+    10 dx) on a flat three-layer wall lattice: nearest_wall (one particle
+    sitting on a wall particle), apply_contact_angle_boundary at two angles,
+    and csf_fields / surface_tension_acceleration with the "rotate" boundary
+    and the "young" and "brackbill" tractions, FP64 and FP32."""
+    data = {}
+    dx = 0.002
+    h = 1.3 * dx
+    wx = torch.arange(-16, 17, dtype=torch.float64) * dx
+    wall64 = torch.cat([torch.stack((wx, torch.full_like(wx, -0.5 * dx - k * dx)), -1) for k in range(3)])
+    ax = (torch.arange(-11, 11, dtype=torch.float64) + 0.5) * dx
+    gx, gy = torch.meshgrid(ax, (torch.arange(0, 11, dtype=torch.float64) + 0.5) * dx, indexing="xy")
+    pts = torch.stack((gx.reshape(-1), gy.reshape(-1)), -1)
+    pts = pts[torch.linalg.vector_norm(pts, dim=1) <= 10.5 * dx]
+    g = torch.Generator().manual_seed(seed)
+    pts64 = pts + 0.05 * dx * torch.randn(pts.shape, generator=g, dtype=torch.float64)
+    rho64 = 1000.0 * (1.0 + 0.002 * torch.randn((pts.shape[0],), generator=g, dtype=torch.float64))
+    grad64 = torch.randn(pts.shape, generator=g, dtype=torch.float64) * 100.0
+    # standalone nearest_wall with one particle on a wall particle, and the boundary
+    probe = torch.cat((pts64, wall64[40:41]))
+    d, nrm = ca.nearest_wall(probe, wall64)
+    data.update(nw_pos=_np(probe), nw_dist=_np(d), nw_normal=_np(nrm), wall=_np(wall64), h=np.float64(h))
+    for k, theta in enumerate((math.pi / 6, 2 * math.pi / 3)):
+        data[f"bc{k}_theta"] = np.float64(theta)
+        data[f"bc{k}_out"] = _np(ca.apply_contact_angle_boundary(grad64.clone(), pts64, wall64, h, theta))
+    data["bc_grad"] = _np(grad64)
+    variants = [
+        (torch.float64, dict(contact_angle=math.pi / 3, contact_angle_model="rotate", curvature_scheme="mls")),
+        (torch.float64, dict(contact_angle=2 * math.pi / 3, contact_angle_model="rotate",
+                             curvature_scheme="fit_quadratic")),
+        (torch.float64, dict(contact_angle=math.pi / 3, curvature_color_smoothing=1, direct=True)),
+        (torch.float64, dict(contact_angle=math.pi / 3, contact_angle_model="young", curvature_scheme="mls")),
+        (torch.float64, dict(contact_angle=2 * math.pi / 3, contact_angle_model="brackbill",
+                             curvature_scheme="fit_quadratic")),
+        (torch.float32, dict(contact_angle=math.pi / 3, contact_angle_model="rotate", curvature_scheme="mls")),
+        (torch.float32, dict(contact_angle=math.pi / 3, contact_angle_model="young", curvature_scheme="mls")),
+    ]
+    from tensorsph.neighbor_search import cell_linked_pairs
+    for k, (dtype, o) in enumerate(variants):
+        pos, wall, rho = pts64.to(dtype), wall64.to(dtype), rho64.to(dtype)
+        mass = torch.full((pos.shape[0],), 1000.0 * dx * dx, dtype=dtype)
+        pairs = cell_linked_pairs(pos, 2.0 * h)
+        o = dict(o)
+        direct = o.pop("direct", False)
+        if direct:
+            st = ca.csf_fields(pos, mass, pairs, h, 1000.0, wall=wall, **o)
+            acc = None
+        else:
+            acc, st = ca.surface_tension_acceleration(pos, rho, mass, pairs, h, 0.0728, rho0=1000.0, wall=wall, **o)
+        fields = dict(pos=pos, mass=mass, rho=rho, pairs=pairs, color=st.color, grad_c=st.grad_c,
+                      normal=st.normal, kappa=st.kappa, delta_s=st.delta_s)
+        if acc is not None:
+            fields["acc"] = acc
+        for name, t in fields.items():
+            data[f"c{k}_{name}"] = _np(t)
+        data[f"c{k}_direct"] = np.int64(direct)
+        data[f"c{k}_opts"] = np.array(repr(sorted(o.items())))
+    data["count"] = np.int64(len(variants))
+    return data
+
+
 def delta_plus_cases(dp):
     """delta_plus_step on a perturbed lattice block in a walled corner (fluid,
     slip walls with normals, gravity, diffusion) and on a free block."""
@@ -748,6 +811,7 @@ def main(src, families=None):
         "config1_run": lambda: config1_run_case(db),
         "dam3d_run": lambda: dam3d_run_case(d3),
         "checkpoint": lambda: checkpoint_case(kl),
+        "contact": lambda: contact_cases(ca),
     }
     for name in families or makers:
         np.savez_compressed(OUT / f"{name}.npz", **makers[name](), **meta)

@@ -308,3 +308,51 @@ def test_delta_plus_oracle_matches_reference(golden):
             ref = g[f"c{k}_out_{key}"]
             if ref.size:
                 assert np.abs(out[key] - ref).max() <= tol * np.abs(ref).max(), (k, key)
+
+
+def _contact_compare(st, acc, g, k, f64, tol_dir):
+    live = g[f"c{k}_delta_s"] > 0
+    tol = 1e-9 if f64 else 1e-4
+    for name in ("color", "grad_c", "delta_s"):
+        r = g[f"c{k}_{name}"]
+        assert np.abs(st[name] - r).max() <= tol * max(np.abs(r).max(), 1.0), (k, name)
+    for name in ("normal", "kappa"):
+        r = g[f"c{k}_{name}"][live]
+        assert np.abs(st[name][live] - r).max() <= tol_dir * np.abs(r).max(), (k, name)
+    if acc is not None:
+        r = g[f"c{k}_acc"]
+        assert np.abs(acc - r).max() <= tol_dir * np.abs(r).max(), (k, "acc")
+
+
+def test_contact_angle_oracle_matches_reference(golden):
+    """nearest_wall, apply_contact_angle_boundary and the CSF with the
+    "rotate" boundary and the "young" / "brackbill" tractions against the
+    reference's own outputs (tests/golden/contact.npz)."""
+    import ast
+    from oracle import contact_angle as oc
+    from oracle import csf
+    g = golden("contact")
+    wall, h = g["wall"], float(g["h"])
+    d, nrm = oc.nearest_wall(g["nw_pos"], wall)
+    assert np.abs(d - g["nw_dist"]).max() <= 1e-12
+    assert np.abs(nrm - g["nw_normal"]).max() <= 1e-12
+    pos = g["nw_pos"][:-1]
+    for k in range(2):
+        out = oc.apply_contact_angle_boundary(g["bc_grad"], pos, wall, h, float(g[f"bc{k}_theta"]))
+        assert np.abs(out - g[f"bc{k}_out"]).max() <= 1e-12 * np.abs(g[f"bc{k}_out"]).max()
+    for k in range(int(g["count"])):
+        o = dict(ast.literal_eval(str(g[f"c{k}_opts"])))
+        p, mass, rho, pairs = g[f"c{k}_pos"], g[f"c{k}_mass"], g[f"c{k}_rho"], g[f"c{k}_pairs"]
+        w = wall.astype(p.dtype)
+        f64 = p.dtype == np.float64
+        if int(g[f"c{k}_direct"]):
+            st = csf.csf_fields(p, mass, pairs, h, 1000.0, stencil=4.0, curvature_scheme="mls", wall=w,
+                                contact_angle=o["contact_angle"],
+                                curvature_color_smoothing=o.get("curvature_color_smoothing", 0))
+            acc = None
+        else:
+            acc, st = csf.surface_tension_acceleration(p, rho, mass, h, 0.0728, 1000.0, pairs=pairs, wall=w,
+                                                       curvature_scheme=o["curvature_scheme"],
+                                                       contact_angle=o["contact_angle"],
+                                                       contact_angle_model=o["contact_angle_model"])
+        _contact_compare(st, acc, g, k, f64, 1e-8 if f64 else 1e-3)
