@@ -261,9 +261,16 @@ typedef struct {
   int64_t curvature;           /* 0 "mls" (div n), 1 "fit_quadratic",       */
                                /* 2 "fit_circle"                            */
   int64_t delta_normalization; /* 0 "legacy" (2|grad c|), 1 "local_range"   */
+  int64_t n_wall;              /* wall particles at io.wall; 0: no wall     */
+  int64_t contact_model;       /* with walls: 0 none, 1 "rotate" (normal    */
+                               /* boundary in the fields), 2 "young", 3     */
+                               /* "brackbill" (traction in the acceleration) */
   double h, rho0;              /* smoothing length; V = m / rho0            */
   double stencil;              /* fit stencil in units of h (4)             */
   double sigma;                /* acceleration only                         */
+  double contact_angle;        /* radians, measured inside the liquid       */
+  double contact_reach;        /* boundary thickness in units of h (2)      */
+  double traction_calibration; /* C of the young / brackbill traction       */
 } tsph_csf2_params;
 
 typedef struct {
@@ -277,17 +284,31 @@ typedef struct {
   void* kappa;                /* out (n)                                     */
   void* delta_s;              /* out (n)                                     */
   uint8_t* valid;             /* out (n): the MLS matrix is regular          */
+  const void* wall;           /* (n_wall, 2) wall particles, or NULL         */
 } tsph_csf2_io;
 
 int64_t tsph_csf2_workspace_bytes(const tsph_csf2_params* prm);
-/* replaces csf_fields (csf_consistent.py:262-381; no contact angle) */
+/* replaces csf_fields (csf_consistent.py:262-381), with the contact-angle
+ * boundary of :483-560 on both colour gradients when contact_model is 1 */
 int tsph_csf2_fields(const tsph_csf2_params* prm, const tsph_csf2_io* io, void* ws, int64_t ws_bytes,
                      tsph_stream stream);
 /* replaces the force of surface_tension_acceleration (csf_consistent.py:
- * 430-446): delta_s_out = delta_s with the flat particles zeroed, acc (n, 2) */
-int tsph_csf2_acceleration(const tsph_csf2_params* prm, const void* grad_c, const void* normal,
-                           const void* kappa, const void* delta_s, const void* rho, void* delta_s_out,
-                           void* acc, void* ws, int64_t ws_bytes, tsph_stream stream);
+ * 430-446) from the fields in io (grad_c, normal, kappa, delta_s; pos and
+ * wall for the young / brackbill traction of contact_angle_isph.py:148-213):
+ * delta_s_out = delta_s with the flat particles zeroed, acc (n, 2) */
+int tsph_csf2_acceleration(const tsph_csf2_params* prm, const tsph_csf2_io* io, const void* rho,
+                           void* delta_s_out, void* acc, void* ws, int64_t ws_bytes, tsph_stream stream);
+/* replaces nearest_wall (csf_consistent.py:449-480): distance to the nearest
+ * wall particle (the first of equals) and the unit direction from it to the
+ * particle, dist (n) and normal (n, 2) */
+int tsph_csf2_nearest_wall(const tsph_csf2_params* prm, const void* pos, const void* wall, void* dist,
+                           void* normal, void* ws, int64_t ws_bytes, tsph_stream stream);
+/* replaces apply_contact_angle_boundary (csf_consistent.py:483-560) on a
+ * given gradient: grad_out (may be grad_in) = grad_in with the near-wall
+ * normals turned toward prm->contact_angle */
+int tsph_csf2_contact_boundary(const tsph_csf2_params* prm, const void* pos, const void* wall,
+                               const void* grad_in, void* grad_out, void* ws, int64_t ws_bytes,
+                               tsph_stream stream);
 
 /* ------------------------------------------------------------------------ */
 /* Transport-velocity correction: kernel_gradient_integral and              */

@@ -73,13 +73,14 @@ class Csf3IO(ctypes.Structure):
 
 class Csf2Params(ctypes.Structure):
     _fields_ = [(k, c_int64) for k in ("n", "dtype", "normal_smoothing", "color_smoothing", "curvature",
-                                       "delta_normalization")] + \
-               [(k, c_double) for k in ("h", "rho0", "stencil", "sigma")]
+                                       "delta_normalization", "n_wall", "contact_model")] + \
+               [(k, c_double) for k in ("h", "rho0", "stencil", "sigma", "contact_angle", "contact_reach",
+                                        "traction_calibration")]
 
 
 class Csf2IO(ctypes.Structure):
     _fields_ = [(k, c_void_p) for k in ("pos", "mass", "rowptr", "entries", "color", "grad_c", "normal",
-                                        "kappa", "delta_s", "valid")]
+                                        "kappa", "delta_s", "valid", "wall")]
 
 
 class TvcParams(ctypes.Structure):
@@ -189,8 +190,12 @@ _SIGNATURES = {
                                           c_int64, c_void_p]),
     "tsph_csf2_workspace_bytes": (c_int64, [POINTER(Csf2Params)]),
     "tsph_csf2_fields": (c_int, [POINTER(Csf2Params), POINTER(Csf2IO), c_void_p, c_int64, c_void_p]),
-    "tsph_csf2_acceleration": (c_int, [POINTER(Csf2Params), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
-                                       c_void_p, c_void_p, c_void_p, c_int64, c_void_p]),
+    "tsph_csf2_acceleration": (c_int, [POINTER(Csf2Params), POINTER(Csf2IO), c_void_p, c_void_p, c_void_p,
+                                       c_void_p, c_int64, c_void_p]),
+    "tsph_csf2_nearest_wall": (c_int, [POINTER(Csf2Params), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                       c_int64, c_void_p]),
+    "tsph_csf2_contact_boundary": (c_int, [POINTER(Csf2Params), c_void_p, c_void_p, c_void_p, c_void_p,
+                                           c_void_p, c_int64, c_void_p]),
     "tsph_tvc_gradient": (c_int, [POINTER(TvcParams), POINTER(TvcIO), c_void_p]),
     "tsph_tvc_shift": (c_int, [POINTER(TvcParams), POINTER(TvcIO), c_void_p]),
     "tsph_csf3_workspace_bytes": (c_int64, [POINTER(Csf3Params)]),

@@ -92,8 +92,8 @@ def test_struct_sizes_match_header():
     assert ctypes.sizeof(_lib.Csf3Params) == 8 * (3 + 3 + 4)
     assert ctypes.sizeof(_lib.Csf3IO) == 8 * 11
     assert ctypes.sizeof(_lib.TvcParams) == 8 * (8 + 8)
-    assert ctypes.sizeof(_lib.Csf2Params) == 8 * (6 + 4)
-    assert ctypes.sizeof(_lib.Csf2IO) == 8 * 10
+    assert ctypes.sizeof(_lib.Csf2Params) == 8 * (8 + 7)
+    assert ctypes.sizeof(_lib.Csf2IO) == 8 * 11
     assert ctypes.sizeof(_lib.TvcIO) == 8 * 13
 
 
