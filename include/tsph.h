@@ -515,13 +515,17 @@ typedef struct {
                                        /* walls); L is snapped to n cells of an FP32 */
                                        /* edge (relative change < 1e-7)              */
   int64_t tvc_every;                   /* transport-velocity correction every k steps */
-                                       /* after the update (3-D, no obstacle, no     */
-                                       /* shifting); 0 disables                      */
+                                       /* after the update (2-D or 3-D, no obstacle, */
+                                       /* no shifting); 0 disables                   */
   double tvc_alpha;                    /* its coefficient (displacement alpha h^2 g)  */
   double tvc_scope_tol;                /* >= 0: only where |g| h <= tol; < 0: all     */
   double tvc_max_shift;                /* >= 0: clip |shift| to this length; < 0: off */
   int64_t first_step;                  /* step number of the first step (a run       */
                                        /* resumed from a checkpoint); 0 for a new run */
+  double tvc_slope;                    /* > 0: the truncated_linear limiter          */
+                                       /* min(slope h^2 |g|^2, 1); <= 0: none         */
+  double tvc_wall_volume;              /* wall particle volume in the correction;    */
+                                       /* <= 0: wall_mass / rho0                     */
 } tsph_case_params;
 
 typedef struct tsph_engine tsph_engine; /* opaque host handle */

@@ -75,6 +75,7 @@ struct CaseDev {
   float tvc_wall_vol;      // wall volume m_w / rho0
   float tvc_tol;           // scope |g| h <= tol (< 0: every particle)
   float tvc_max;           // displacement clip (< 0: none)
+  float tvc_slope_hh;      // truncated_linear limiter slope h^2 (< 0: none)
 };
 
 struct CaseCtl {
@@ -1524,7 +1525,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_tvc_apply(Dev e) {
     if (!t.tvc_now) continue;
     const CaseDev& C = e.cases[c];
     const float4 g = e.gradc[a];
-    float sx = C.tvc_coef * g.x, sy = C.tvc_coef * g.y, sz = C.tvc_coef * g.z;
+    // the limiter min(slope h^2 |g|^2, 1) (transport_velocity_correction.py:180-223)
+    float coef = C.tvc_coef;
+    if (C.tvc_slope_hh > 0.f) coef *= fminf(C.tvc_slope_hh * g.w, 1.f);
+    float sx = coef * g.x, sy = coef * g.y, sz = coef * g.z;
     bool kept = true;
     if (C.tvc_tol >= 0.f && !(sqrtf(g.w) * static_cast<float>(C.h_d) <= C.tvc_tol)) {
       kept = false;
@@ -2290,9 +2294,10 @@ CaseDev make_case_dev(const tsph_case_params& p, int64_t* ncells) {
   c.fit_rc2 = (4.0 * p.h + p.skin) * (4.0 * p.h + p.skin);
   c.tvc_every = static_cast<int>(p.tvc_every);
   c.tvc_coef = static_cast<float>(p.tvc_alpha * p.h * p.h);
-  c.tvc_wall_vol = static_cast<float>(p.wall_mass / p.rho0);
+  c.tvc_wall_vol = static_cast<float>(p.tvc_wall_volume > 0.0 ? p.tvc_wall_volume : p.wall_mass / p.rho0);
   c.tvc_tol = static_cast<float>(p.tvc_scope_tol);
   c.tvc_max = static_cast<float>(p.tvc_max_shift);
+  c.tvc_slope_hh = p.tvc_slope > 0.0 ? static_cast<float>(p.tvc_slope * p.h * p.h) : -1.f;
   return c;
 }
 
@@ -2309,10 +2314,11 @@ bool case_params_ok(const tsph_case_params* p) {
   if (p->periodic_box < 0.0 || (p->periodic_box > 0.0 && (p->dim != 3 || p->n_wall != 0 || p->shift_every != 0 ||
                                                           !std::isfinite(p->periodic_box))))
     return false;
-  // the correction of the 3-D dam break: no obstacle, shifting or periodic box
-  if (p->tvc_every < 0 || (p->tvc_every > 0 && (p->dim != 3 || p->has_obstacle || p->shift_every != 0 ||
-                                                p->periodic_box > 0.0 || !std::isfinite(p->tvc_alpha) ||
-                                                !std::isfinite(p->tvc_scope_tol) || !std::isfinite(p->tvc_max_shift))))
+  // the correction of the dam breaks: no obstacle, shifting or periodic box
+  if (p->tvc_every < 0 || (p->tvc_every > 0 && (p->has_obstacle || p->shift_every != 0 || p->periodic_box > 0.0 ||
+                                                !std::isfinite(p->tvc_alpha) || !std::isfinite(p->tvc_scope_tol) ||
+                                                !std::isfinite(p->tvc_max_shift) || !std::isfinite(p->tvc_slope) ||
+                                                !std::isfinite(p->tvc_wall_volume))))
     return false;
   return true;
 }

@@ -166,17 +166,35 @@ def _case_params(*, dim, n_fluid, n_wall, n_obstacle, cfg, h, wall_mass, box_hi,
         for k in range(3):
             p.ob_lo[k], p.ob_hi[k] = obstacle[0][k], obstacle[1][k]
         p.ob_eps = 0.01 * cfg.dx
-    p.tvc_every = int(getattr(cfg, "tvc_every", 0) or 0) if dim == 3 else 0
+    p.tvc_every = int(getattr(cfg, "tvc_every", 0) or 0)
     p.tvc_alpha, p.tvc_scope_tol, p.tvc_max_shift = 0.0, -1.0, -1.0
+    p.tvc_slope, p.tvc_wall_volume = -1.0, -1.0
     if p.tvc_every and (obstacle is not None or shift_every):
-        raise NotImplementedError("transport-velocity correction runs in the 3-D dam break without "
-                                  "an obstacle or shifting, as in dam_break_3d.run_case")
+        raise NotImplementedError("the device engine runs the transport-velocity correction in the "
+                                  "dam breaks without an obstacle or shifting")
     if p.tvc_every:
-        # dam_break_3d.py:675-704: the module default 0.2 / 4 unless set; the
-        # clip is given in units of h
+        # the module default 0.2 / 4 unless set; the clip is given in units of h
         p.tvc_alpha = 0.05 if cfg.tvc_alpha is None else float(cfg.tvc_alpha)
-        p.tvc_scope_tol = -1.0 if cfg.tvc_scope_tol is None else float(cfg.tvc_scope_tol)
         p.tvc_max_shift = -1.0 if cfg.tvc_max_shift is None else float(cfg.tvc_max_shift) * h
+        if dim == 3:
+            # dam_break_3d.py:675-704: scope by |g| h, walls at m_w / rho0
+            p.tvc_scope_tol = -1.0 if cfg.tvc_scope_tol is None else float(cfg.tvc_scope_tol)
+        else:
+            # dam_break.py:434-459: scope "all" or "bulk_g" (|g| h <= tvc_bulk_g),
+            # the named limiter, walls at dx^2
+            scope = getattr(cfg, "tvc_scope", "all")
+            if scope == "bulk":
+                raise NotImplementedError("tvc_scope='bulk' (the concentration mask) is not part of the "
+                                          "device engine; use 'all' or 'bulk_g'")
+            if scope not in ("all", "bulk_g"):
+                raise ValueError(f"unknown tvc_scope {scope!r}")
+            p.tvc_scope_tol = float(cfg.tvc_bulk_g) if scope == "bulk_g" else -1.0
+            limiter = getattr(cfg, "tvc_limiter", None)
+            if limiter == "truncated_linear":
+                p.tvc_slope = float(cfg.tvc_limiter_slope)
+            elif limiter not in (None, "none"):
+                raise ValueError(f"unknown tvc_limiter {limiter!r}")
+            p.tvc_wall_volume = float(cfg.dx) ** 2
     p.shift_strength = getattr(cfg, "shift_strength", 1.0)
     p.shift_limit = getattr(cfg, "shift_limit", 0.25)
     p.shift_free_surface = 0.95
@@ -924,16 +942,18 @@ class DamBreakRun:
     steps_taken: int = 0
     simulated_time: float = 0.0
     snapshots: list = field(default_factory=list)
+    max_tvc_shift: float = 0.0       # largest |shift| of one correction, m
+    max_tvc_clipped: float = 0.0     # largest fraction of fluid one correction clipped
 
 
 def run_dam_break_2d(cfg, *, snapshot_times=None, max_neighbors: int = 64) -> DamBreakRun:
     """Integrate the 2-D dam break (dam_break.py:319-460 with the pair cache,
-    fixed dt, no shifting) on the GPU and return the measured trajectory;
-    ``snapshot_times`` as in ``run_case``."""
+    fixed dt) on the GPU and return the measured trajectory;
+    ``snapshot_times`` as in ``run_case``.  Shifting and the transport-velocity
+    correction (``tvc_every``, scopes "all" and "bulk_g", the
+    ``truncated_linear`` limiter, the clip) each run, not both together."""
     if cfg.adaptive_dt:
         raise NotImplementedError("adaptive_dt is not supported by the device engine")
-    if cfg.tvc_every:
-        raise NotImplementedError("transport-velocity correction is not part of the device engine")
     spec = dam_break_2d_case(cfg, shift_every=cfg.shift_every)
     eng = BatchEngine(**capacity_for([spec], max_neighbors=max_neighbors,
                                      diag_ring=max(cfg.steps + 1, 1)))
@@ -958,5 +978,10 @@ def run_dam_break_2d(cfg, *, snapshot_times=None, max_neighbors: int = 64) -> Da
                       max_density_compression=float(diag[:, 0].max()) / cfg.rho0 - 1.0,
                       final_positions=x, steps_taken=cfg.steps,
                       simulated_time=cfg.steps * cfg.dt, snapshots=snapshots)
+    every = int(cfg.tvc_every or 0)
+    applied = [k for k in range(1, cfg.steps) if every and k % every == 0]
+    if applied:
+        run.max_tvc_shift = max(float(diag[k, 16]) for k in applied)
+        run.max_tvc_clipped = max(float(diag[k, 19]) for k in applied) / spec.n_fluid
     eng.close()
     return run

@@ -303,3 +303,73 @@ def test_periodic_shear_case_decays_and_batches(gpu):
 def dam_break_2d_case_small():
     from tensorsph_b200.engine import dam_break_2d_case
     return dam_break_2d_case(small_2d())
+
+
+@pytest.mark.parametrize("opts", [dict(), dict(tvc_alpha=0.2, tvc_scope="bulk_g", tvc_limiter="truncated_linear",
+                                               tvc_limiter_slope=10.0, tvc_max_shift=2e-3)])
+def test_2d_tvc_matches_fp64_oracle(opts, gpu):
+    """The 2-D dam break's transport-velocity correction in the engine
+    (dam_break.py:434-459: after the update, volumes m / rho of the step,
+    walls at dx^2, scope "all" or "bulk_g", the truncated_linear limiter, the
+    clip) against the oracle: two steps (the correction runs after the update
+    of step 1) with a zero skin, from a lattice jittered by +-0.1 dx.  The
+    displacement (run with the correction minus run without) matches the
+    oracle's shift to 1e-4 of its largest component, and run_dam_break_2d
+    reports the largest shift and clipped fraction."""
+    from dataclasses import replace
+
+    from oracle import tvc as otv
+    from tensorsph_b200.engine import dam_break_2d_case, run_dam_break_2d
+    cfg = replace(small_2d(), pair_skin_factor=0.0, steps=2, output_every=1)
+    base = dam_break_2d_case(cfg)
+    rng = np.random.default_rng(13)
+    x = (base.x + torch.from_numpy(rng.uniform(-0.1, 0.1, tuple(base.x.shape)) * cfg.dx)).clamp(min=0.0)
+    runs, diags = {}, {}
+    for every in (0, 1):
+        spec = dam_break_2d_case(replace(cfg, tvc_every=every, **opts))
+        spec.x = x.clone()
+        eng = engine_for([spec], max_neighbors=64, diag_ring=16)
+        cid = eng.add(spec)
+        eng.step(2)
+        runs[every] = eng.read(cid)[0].cpu().numpy()
+        diags[every] = eng.diagnostics(cid, 1, 1).cpu().numpy()[0]
+        assert eng.status(cid)["status"] == 0
+        eng.close()
+    xn, mn, wn = x.numpy(), base.mass.numpy(), base.wall.numpy()
+    ref, x2, _ = oracle_2d_steps(cfg, xn, mn, wn, 2)
+    _, x1, _ = oracle_2d_steps(cfg, xn, mn, wn, 1)
+    h = cfg.h_factor * cfg.dx
+    pairs = cell_linked_pairs(np.concatenate((x1, wn)), 2.0 * h)
+    vol = np.concatenate((mn / ref[1][0], np.full(wn.shape[0], cfg.dx ** 2)))
+    c = replace(cfg, tvc_every=1, **opts)
+    res = otv.transport_velocity_correction(
+        np.concatenate((x2, wn)), vol, h, pairs, wall_count=wn.shape[0],
+        alpha=0.05 if c.tvc_alpha is None else c.tvc_alpha, h_ref=h,
+        slope=c.tvc_limiter_slope if c.tvc_limiter == "truncated_linear" else None,
+        scope_tol=c.tvc_bulk_g if c.tvc_scope == "bulk_g" else None,
+        max_shift=None if c.tvc_max_shift is None else c.tvc_max_shift * h)
+    shift = res["shift"]
+    assert np.abs(shift).max() > 1e-5 * cfg.dx
+    err = np.abs((runs[1] - runs[0]) - shift).max()
+    assert err < 1e-4 * np.abs(shift).max(), err / np.abs(shift).max()
+    norm = np.linalg.norm(shift, axis=1)
+    assert diags[1][16] == pytest.approx(norm.max(), rel=1e-4)
+    assert diags[1][19] / mn.size == pytest.approx(res["clipped"], abs=1.5 / mn.size)
+    run = run_dam_break_2d(replace(c, steps=3))
+    assert run.max_tvc_shift >= 0.0 and 0.0 <= run.max_tvc_clipped <= 1.0
+    if not opts:
+        assert run.max_tvc_shift > 0.0      # scope "all": the free surface moves
+    if c.tvc_max_shift is not None:
+        assert run.max_tvc_shift <= c.tvc_max_shift * h * (1 + 1e-6)
+
+
+def test_2d_tvc_refuses_bulk_scope_and_shifting():
+    from dataclasses import replace
+
+    from tensorsph_b200.engine import dam_break_2d_case
+    with pytest.raises(NotImplementedError):
+        dam_break_2d_case(replace(small_2d(), tvc_every=1, tvc_scope="bulk"))
+    with pytest.raises(NotImplementedError):
+        dam_break_2d_case(replace(small_2d(), tvc_every=1), shift_every=1)
+    with pytest.raises(ValueError):
+        dam_break_2d_case(replace(small_2d(), tvc_every=1, tvc_limiter="cubic"))
