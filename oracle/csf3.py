@@ -7,11 +7,16 @@ Restates, with the reference's pair-list scatter structure (``np.add.at`` for
 
 * ``_mls_matrix``                     src/tensorsph/threed/csf3.py:98-112
 * ``csf_fields3`` ("mls" curvature)   src/tensorsph/threed/csf3.py:115-165
+* ``curvature_axisymmetric``          src/tensorsph/threed/csf3.py:168-220: the
+  2-D quadratic interface fit (``oracle.csf.fit_curvature_quadratic``, 4h
+  stencil, zero fallback) on the meridional projection (r, z) of the particles
+  and of their normals, plus n_r / max(r, h / 4)
 * ``surface_tension_acceleration3``   src/tensorsph/threed/csf3.py:220-238
 * pair geometry (minimum image)       src/tensorsph/threed/operators3.py:51-67
 * 3-D cubic spline and its gradient   src/tensorsph/threed/kernel3.py:90-105
 
-Pinned to ``tests/golden/csf3.npz`` (written by running the reference).
+Pinned to ``tests/golden/csf3.npz`` and ``tests/golden/csf3axi.npz`` (written
+by running the reference).
 """
 from __future__ import annotations
 
@@ -20,7 +25,7 @@ import numpy as np
 from .neighbors import minimum_image
 from .pairpass import cubic_kernel, cubic_pair_kernels
 
-__all__ = ["csf_fields3", "surface_tension_acceleration3"]
+__all__ = ["csf_fields3", "curvature_axisymmetric", "surface_tension_acceleration3"]
 
 
 def _lower_median(x):
@@ -29,7 +34,21 @@ def _lower_median(x):
     return s[(s.size - 1) // 2]
 
 
-def csf_fields3(pos, mass, h, pairs, *, rho0, box=None, volume=None):
+def curvature_axisymmetric(pos, normal, delta_s, pairs, h):
+    """Curvature of a surface of revolution about z: meridional fit + n_r / r."""
+    from .csf import fit_curvature_quadratic
+    dt = pos.dtype.type
+    r = np.sqrt(pos[:, 0] * pos[:, 0] + pos[:, 1] * pos[:, 1])
+    mer = np.stack((r, pos[:, 2]), axis=1)
+    radial = pos[:, :2] / np.maximum(r, dt(1e-30))[:, None]
+    n_r = (normal[:, :2] * radial).sum(axis=1)
+    m = np.stack((n_r, normal[:, 2]), axis=1)
+    m_normal = m / np.maximum(np.sqrt((m * m).sum(axis=1)), dt(1e-30))[:, None]
+    k_mer = fit_curvature_quadratic(mer, m_normal, delta_s, pairs, h, np.zeros_like(r))
+    return (k_mer + n_r / np.maximum(r, dt(0.25 * h))).astype(pos.dtype)
+
+
+def csf_fields3(pos, mass, h, pairs, *, rho0, box=None, volume=None, curvature="mls"):
     """``dict(color, grad_c, normal, kappa, delta_s, valid)`` of a 3-D cloud."""
     dt = pos.dtype.type
     n, dim = pos.shape
@@ -73,6 +92,10 @@ def csf_fields3(pos, mass, h, pairs, *, rho0, box=None, volume=None):
     inv = np.linalg.inv(big_m)
     kappa = (s_mat * np.transpose(inv, (0, 2, 1))).sum(axis=(1, 2))
     kappa = np.where(valid, kappa, dt(0))
+    if curvature == "axisym":
+        kappa = curvature_axisymmetric(pos, normal, delta_s, pairs, h)
+    elif curvature != "mls":
+        raise ValueError(f"unknown curvature {curvature!r}")
     return dict(color=color, grad_c=grad_c, normal=normal, kappa=kappa, delta_s=delta_s, valid=valid)
 
 

@@ -456,6 +456,50 @@ def csf3_cases(c3, lc, ns, n3):
     return data
 
 
+def csf3axi_cases(c3, lc, ns, n3):
+    """The 3-D CSF with the "axisym" curvature (threed/csf3.py:159-220,
+    meridional quadratic fit + n_r / r) on 4h pair lists: a jittered ball
+    (FP64, FP32) and the periodic Rayleigh-Plateau column of
+    liquid_column.build_column in its box (FP64)."""
+    data = {}
+    k = 0
+    dx = 1.0e-3
+    for dtype, kind in ((torch.float64, "ball"), (torch.float32, "ball"), (torch.float64, "column")):
+        g = torch.Generator().manual_seed(500 + k)
+        box = None
+        if kind == "column":
+            cfg = lc.ColumnConfig(radius=4e-3, dx=dx, kR=0.6971, epsilon=0.02)
+            pos, mass, box = lc.build_column(cfg)
+            pos, mass = pos.to(dtype), mass.to(dtype)
+            h = cfg.h
+            pairs = n3.periodic_pairs(pos, box, 4.0 * h)
+            box = [float(b) for b in box]
+        else:
+            ax = torch.arange(-7, 8, dtype=torch.float64) * dx
+            gx, gy, gz = torch.meshgrid(ax, ax, ax, indexing="ij")
+            pts = torch.stack((gx.reshape(-1), gy.reshape(-1), gz.reshape(-1)), -1)
+            pts = pts[torch.linalg.vector_norm(pts, dim=1) <= 6.2 * dx]
+            pts = pts + 0.08 * dx * torch.randn(pts.shape, generator=g, dtype=torch.float64)
+            pos = pts.to(dtype)
+            mass = torch.full((pos.shape[0],), 1000.0 * dx ** 3, dtype=dtype)
+            h = 1.3 * dx
+            pairs = ns.cell_linked_pairs(pos, 4.0 * h)
+        rho = (1000.0 * (1.0 + 0.002 * torch.randn((pos.shape[0],), generator=g,
+                                                    dtype=torch.float64))).to(dtype)
+        st = c3.csf_fields3(pos, mass, h, pairs, rho0=1000.0, box=box, curvature="axisym")
+        acc = c3.surface_tension_acceleration3(st, rho, 0.0728)
+        fields = dict(pos=pos, mass=mass, rho=rho, pairs=pairs, acc=acc, color=st.color,
+                      grad_c=st.grad_c, normal=st.normal, kappa=st.kappa, delta_s=st.delta_s,
+                      valid=st.valid)
+        for name, t in fields.items():
+            data[f"c{k}_{name}"] = _np(t)
+        data[f"c{k}_h"] = np.float64(h)
+        data[f"c{k}_box"] = np.asarray(box if box is not None else [0.0, 0.0, 0.0], dtype=np.float64)
+        k += 1
+    data["count"] = np.int64(k)
+    return data
+
+
 def tvc_cases(tv, ns):
     """transport_velocity_correction (transport_velocity_correction.py:285-513)
     on jittered fluid blocks with wall layers: 2-D and 3-D, FP64 and FP32, no
@@ -812,6 +856,7 @@ def main(src, families=None):
         "dam3d_run": lambda: dam3d_run_case(d3),
         "checkpoint": lambda: checkpoint_case(kl),
         "contact": lambda: contact_cases(ca),
+        "csf3axi": lambda: csf3axi_cases(c3, lc, ns, n3),
     }
     for name in families or makers:
         np.savez_compressed(OUT / f"{name}.npz", **makers[name](), **meta)

@@ -356,3 +356,24 @@ def test_contact_angle_oracle_matches_reference(golden):
                                                        contact_angle=o["contact_angle"],
                                                        contact_angle_model=o["contact_angle_model"])
         _contact_compare(st, acc, g, k, f64, 1e-8 if f64 else 1e-3)
+
+
+def test_csf3_axisym_oracle_matches_reference(golden):
+    """The oracle's 3-D CSF with the "axisym" curvature (meridional quadratic
+    fit + n_r / r) against the reference's own output
+    (tests/golden/csf3axi.npz): FP64 within 1e-9 of the largest curvature,
+    FP32 within 1e-3."""
+    from oracle import csf3
+    g = golden("csf3axi")
+    for k in range(int(g["count"])):
+        pos = g[f"c{k}_pos"]
+        box = g[f"c{k}_box"]
+        st = csf3.csf_fields3(pos, g[f"c{k}_mass"], float(g[f"c{k}_h"]), g[f"c{k}_pairs"], rho0=1000.0,
+                              box=None if not box.any() else box, curvature="axisym")
+        tol = 1e-9 if pos.dtype == np.float64 else 1e-3
+        live = g[f"c{k}_delta_s"] > 1e-3 * g[f"c{k}_delta_s"].max()
+        r = g[f"c{k}_kappa"][live]
+        assert np.abs(st["kappa"][live] - r).max() <= tol * np.abs(r).max(), k
+        acc = csf3.surface_tension_acceleration3(st, g[f"c{k}_rho"], 0.0728)
+        ra = g[f"c{k}_acc"]
+        assert np.abs(acc - ra).max() <= tol * np.abs(ra).max(), k
