@@ -210,9 +210,10 @@ int tsph_threed_accelerations(const tsph_threed_params* prm, const tsph_threed_i
                               int64_t ws_bytes, tsph_stream stream);
 
 /* ------------------------------------------------------------------------ */
-/* 3-D CSF surface tension: tensorsph.threed.csf3.csf_fields3 ("mls"         */
-/* curvature, threed/csf3.py:98-165) and surface_tension_acceleration3       */
-/* (threed/csf3.py:220-238), over the symmetric rows of a pair list.         */
+/* 3-D CSF surface tension: tensorsph.threed.csf3.csf_fields3 ("mls" and     */
+/* "axisym" curvature, threed/csf3.py:98-220) and                           */
+/* surface_tension_acceleration3 (threed/csf3.py:220-238), over the         */
+/* symmetric rows of a pair list.                                           */
 /* ------------------------------------------------------------------------ */
 typedef struct {
   int64_t n;         /* particles                                          */
@@ -222,6 +223,9 @@ typedef struct {
   double h, rho0;    /* smoothing length; rest density (V = m / rho0)      */
   double sigma;      /* acceleration only: surface tension coefficient     */
   double cutoff;     /* acceleration only: active if delta_s > cutoff * max */
+  int64_t curvature; /* 0 "mls": trace(S M^-1); 1 "axisym": the quadratic   */
+                     /* fit of the meridional projection (r, z) within 4 h  */
+                     /* plus n_r / max(r, h / 4) (rows must reach 4 h)      */
 } tsph_csf3_params;
 
 typedef struct {
@@ -240,7 +244,7 @@ typedef struct {
 
 int64_t tsph_csf3_workspace_bytes(const tsph_csf3_params* prm);
 /* replaces csf_fields3(pos, mass, h, pairs, rho0=, box=, volume=,
- * curvature="mls") (threed/csf3.py:115-165) */
+ * curvature=) (threed/csf3.py:115-220) */
 int tsph_csf3_fields(const tsph_csf3_params* prm, const tsph_csf3_io* io, void* ws, int64_t ws_bytes,
                      tsph_stream stream);
 /* replaces surface_tension_acceleration3(state, rho, sigma, cutoff)

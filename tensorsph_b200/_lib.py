@@ -63,7 +63,8 @@ class ThreedIO(ctypes.Structure):
 class Csf3Params(ctypes.Structure):
     _fields_ = [(k, c_int64) for k in ("n", "dtype", "periodic")] + \
                [("box", c_double * 3)] + \
-               [(k, c_double) for k in ("h", "rho0", "sigma", "cutoff")]
+               [(k, c_double) for k in ("h", "rho0", "sigma", "cutoff")] + \
+               [("curvature", c_int64)]
 
 
 class Csf3IO(ctypes.Structure):

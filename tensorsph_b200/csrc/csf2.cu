@@ -42,6 +42,7 @@
 #include <cmath>
 
 #include "common.cuh"
+#include "quadfit.cuh"
 #include "radix_select.cuh"
 #include "sphkernels.cuh"
 
@@ -56,17 +57,6 @@ struct C2 {
   T rho0, w0, stencil_r;
   Cubic<T> k;
 };
-
-template <class T>
-__device__ __forceinline__ unsigned long long bits_of(T v) {
-  return sizeof(T) == 8 ? static_cast<unsigned long long>(__double_as_longlong(static_cast<double>(v)))
-                        : static_cast<unsigned long long>(__float_as_uint(static_cast<float>(v)));
-}
-template <class T>
-__device__ __forceinline__ T from_bits(unsigned long long b) {
-  return sizeof(T) == 8 ? static_cast<T>(__longlong_as_double(static_cast<long long>(b)))
-                        : static_cast<T>(__uint_as_float(static_cast<uint32_t>(b)));
-}
 
 template <class T>
 __global__ void k2_pack(C2<T> p, const T* __restrict__ pos, const T* __restrict__ mass, T* __restrict__ xy,
@@ -357,86 +347,6 @@ __global__ void k2_circle_solve(C2<T> p, const T* __restrict__ delta_s, const T*
   }
 }
 
-// K7a: fit moments s[0..7] and the 3x3 determinant (+ its maximum)
-template <class T>
-__global__ void k2_fit_moments(C2<T> p, const T* __restrict__ xy, const int64_t* __restrict__ rowptr,
-                               const uint32_t* __restrict__ ent, const T* __restrict__ normal,
-                               const T* __restrict__ delta_s, const unsigned long long* __restrict__ maxima,
-                               T* __restrict__ mom, T* __restrict__ fdet, unsigned long long* __restrict__ fmax) {
-  const T dsm = from_bits<T>(maxima[0]);
-  const T ds_max = dsm > T(1e-30) ? dsm : T(1e-30);
-  unsigned long long mb = 0;
-  for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < p.n; a += gridDim.x * blockDim.x) {
-    const T xa = xy[2 * a], ya = xy[2 * a + 1];
-    const T nx = normal[2 * a], ny = normal[2 * a + 1];
-    const T tx = -ny, ty = nx;
-    CSum<T> s[8];
-    T wa = delta_s[a] / ds_max;
-    wa = wa < T(0) ? T(0) : (wa > T(1) ? T(1) : wa);
-    s[0].add(wa);
-    for (int64_t e = rowptr[a]; e < rowptr[a + 1]; ++e) {
-      const int64_t b = ent[e] & kIndexMask;
-      const T dx = xa - xy[2 * b], dy = ya - xy[2 * b + 1];
-      const T r = sqrt(dx * dx + dy * dy);
-      if (!(r <= p.stencil_r)) continue;
-      T w = delta_s[b] / ds_max;
-      w = w < T(0) ? T(0) : (w > T(1) ? T(1) : w);
-      // the neighbour in the particle's frame: (x_b - x_a) . t, . n
-      const T u = -dx * tx + -dy * ty, v = -dx * nx + -dy * ny;
-      const T uu = u * u;
-      s[0].add(w);
-      s[1].add(u * w);
-      s[2].add(v * w);
-      s[3].add(uu * w);
-      s[4].add(u * v * w);
-      s[5].add(uu * u * w);
-      s[6].add(uu * v * w);
-      s[7].add(uu * uu * w);
-    }
-    T sv[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      sv[k] = s[k].value();
-      mom[8 * a + k] = sv[k];
-    }
-    // [[s0 s1 s3] [s1 s3 s5] [s3 s5 s7]]
-    const T d = sv[0] * (sv[3] * sv[7] - sv[5] * sv[5]) - sv[1] * (sv[1] * sv[7] - sv[5] * sv[3]) +
-                sv[3] * (sv[1] * sv[5] - sv[3] * sv[3]);
-    fdet[a] = d;
-    const unsigned long long b = bits_of<T>(d < T(0) ? -d : d);
-    mb = b > mb ? b : mb;
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    const unsigned long long x = __shfl_xor_sync(0xffffffffu, mb, o);
-    mb = x > mb ? x : mb;
-  }
-  if ((threadIdx.x & 31) == 0) atomicMax(fmax, mb);
-}
-
-// K7b: solve for (c, b, a) by Cramer's rule; kappa where the fit holds
-template <class T>
-__global__ void k2_fit_solve(C2<T> p, const T* __restrict__ delta_s, const unsigned long long* __restrict__ maxima,
-                             const T* __restrict__ mom, const T* __restrict__ fdet,
-                             const unsigned long long* __restrict__ fmax, T* __restrict__ kappa) {
-  const T dsm = from_bits<T>(maxima[0]);
-  const T ds_max = dsm > T(1e-30) ? dsm : T(1e-30);
-  const T dm = from_bits<T>(*fmax);
-  const T scale = dm > T(1e-30) ? dm : T(1e-30);
-  for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < p.n; a += gridDim.x * blockDim.x) {
-    T wa = delta_s[a] / ds_max;
-    wa = wa < T(0) ? T(0) : (wa > T(1) ? T(1) : wa);
-    const T d = fdet[a];
-    if (!(wa > T(0.05)) || !((d < T(0) ? -d : d) > T(1e-6) * scale)) continue;  // keep the MLS value
-    const T* s = mom + 8 * a;
-    const T r0 = s[2], r1 = s[4], r2 = s[6];
-    // columns 1 (b) and 2 (a) replaced by the right-hand side
-    const T db = s[0] * (r1 * s[7] - s[5] * r2) - r0 * (s[1] * s[7] - s[5] * s[3]) + s[3] * (s[1] * r2 - r1 * s[3]);
-    const T da = s[0] * (s[3] * r2 - r1 * s[5]) - s[1] * (s[1] * r2 - r1 * s[3]) + r0 * (s[1] * s[5] - s[3] * s[3]);
-    const T b = db / d, aa = da / d;
-    const T q = T(1) + b * b;
-    kappa[a] = T(-2) * aa / (q * sqrt(q));
-  }
-}
 
 constexpr int kTile = 256;  // block size of the wall kernels (shared-memory tiles)
 
@@ -886,9 +796,9 @@ int run_csf2(const tsph_csf2_params& prm, const tsph_csf2_io& io, char* ws, cuda
   if (prm.curvature == 1) {
     T* mom = reinterpret_cast<T*>(ws + L.mom);
     T* fdet = reinterpret_cast<T*>(ws + L.fdet);
-    k2_fit_moments<T><<<g, 128, 0, s>>>(p, xy, io.rowptr, io.entries, normal, delta_s, maxima, mom, fdet,
-                                        maxima + 2);
-    k2_fit_solve<T><<<g, 128, 0, s>>>(p, delta_s, maxima, mom, fdet, maxima + 2, kappa);
+    qf_moments<T><<<g, 128, 0, s>>>(p.n, p.stencil_r, xy, io.rowptr, io.entries, normal, delta_s, maxima, mom,
+                                    fdet, maxima + 2);
+    qf_solve<T><<<g, 128, 0, s>>>(p.n, delta_s, maxima, mom, fdet, maxima + 2, kappa);
     TSPH_LAUNCH_CHECK();
   } else if (prm.curvature == 2) {
     T* mom = reinterpret_cast<T*>(ws + L.mom);

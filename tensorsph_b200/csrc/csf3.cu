@@ -11,6 +11,11 @@
 //                           grad_a W_ab; delta_s = |grad c|; n = -grad c / |grad c|
 //   C4 curvature            kappa_a = trace(S_a M_a^-1),
 //                           S_a = sum_b V_b (n_b - n_a) (x) grad_a W_ab (0 if !valid)
+//   C5 axisym (optional)    kappa_a = k_fit(a) + n_r / max(r, h / 4): the quadratic
+//                           interface fit of quadfit.cuh on the meridional
+//                           projection (r, z) of the positions (not wrapped) and
+//                           of the normals (n_r, n_z) / |(n_r, n_z)|, stencil 4 h,
+//                           0 where the fit does not hold (csf3.py:168-220)
 //   A  acceleration         a = -sigma kappa delta_s [delta_s > cutoff max delta_s] n / rho
 // Separations use the minimum image in a periodic box (operators3.py:51-67).
 // Every row is summed by its own thread in a fixed order: no floating-point
@@ -21,6 +26,7 @@
 #include "common.cuh"
 #include "fpmath.cuh"
 #include "sphkernels.cuh"
+#include "quadfit.cuh"
 #include "radix_select.cuh"
 
 namespace tsph {
@@ -257,11 +263,50 @@ __global__ void c_accel(CP<T> p, const T* __restrict__ normal, const T* __restri
   }
 }
 
+// C5: meridional coordinates and normals, the azimuthal term, the fit's
+// fallback (0) and the largest delta_s (IEEE bits)
+template <class T>
+__global__ void c_axis(int64_t n, T quarter_h, const T* __restrict__ pos, const T* __restrict__ normal,
+                       const T* __restrict__ delta_s, T* __restrict__ mer, T* __restrict__ mnormal,
+                       T* __restrict__ azimuthal, T* __restrict__ kfit, unsigned long long* __restrict__ dsmax) {
+  unsigned long long mb = 0;
+  for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
+    const T x = pos[3 * a], y = pos[3 * a + 1], z = pos[3 * a + 2];
+    const T r = sqrt(x * x + y * y);
+    const T rd = r > T(1e-30) ? r : T(1e-30);
+    const T nr = normal[3 * a] * (x / rd) + normal[3 * a + 1] * (y / rd);
+    const T nz = normal[3 * a + 2];
+    const T m = sqrt(nr * nr + nz * nz);
+    const T md = m > T(1e-30) ? m : T(1e-30);
+    mer[2 * a] = r;
+    mer[2 * a + 1] = z;
+    mnormal[2 * a] = nr / md;
+    mnormal[2 * a + 1] = nz / md;
+    azimuthal[a] = nr / (r > quarter_h ? r : quarter_h);
+    kfit[a] = T(0);
+    const T ds = delta_s[a];
+    const unsigned long long b = bits_of<T>(ds);
+    mb = b > mb ? b : mb;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long v = __shfl_xor_sync(0xffffffffu, mb, o);
+    mb = v > mb ? v : mb;
+  }
+  if ((threadIdx.x & 31) == 0) atomicMax(dsmax, mb);
+}
+
+template <class T>
+__global__ void c_axis_sum(int64_t n, const T* __restrict__ kfit, const T* __restrict__ azimuthal,
+                           T* __restrict__ kappa) {
+  for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x)
+    kappa[a] = kfit[a] + azimuthal[a];
+}
+
 struct CLayout {
-  size_t pv, nq, color_ws, mm, minv, det, keys, hist, sel, maxbits, total;
+  size_t pv, nq, color_ws, mm, minv, det, keys, hist, sel, maxbits, mer, mnormal, az, kfit, mom, fdet, fitmax, total;
 };
 
-CLayout c_layout(int64_t n, int64_t dtype) {
+CLayout c_layout(int64_t n, int64_t dtype, int64_t curvature) {
   const size_t t = dtype == TSPH_F64 ? 8 : 4;
   CLayout L{};
   size_t off = 0;
@@ -279,6 +324,14 @@ CLayout c_layout(int64_t n, int64_t dtype) {
   L.hist = take(256 * 4);
   L.sel = take(2 * 8);
   L.maxbits = take(8);
+  const bool axi = curvature == 1;
+  L.mer = take(axi ? 2 * n * t : 0);
+  L.mnormal = take(axi ? 2 * n * t : 0);
+  L.az = take(axi ? n * t : 0);
+  L.kfit = take(axi ? n * t : 0);
+  L.mom = take(axi ? 8 * n * t : 0);
+  L.fdet = take(axi ? n * t : 0);
+  L.fitmax = take(axi ? 2 * 8 : 0);
   L.total = off;
   return L;
 }
@@ -303,7 +356,7 @@ CP<T> make_cp(const tsph_csf3_params& prm) {
 
 template <class T>
 int run_fields(const tsph_csf3_params& prm, const tsph_csf3_io& io, char* ws, cudaStream_t s) {
-  const CLayout L = c_layout(prm.n, prm.dtype);
+  const CLayout L = c_layout(prm.n, prm.dtype, prm.curvature);
   CP<T> p = make_cp<T>(prm);
   p.has_volume = io.volume != nullptr;
   const int64_t n = prm.n;
@@ -333,13 +386,32 @@ int run_fields(const tsph_csf3_params& prm, const tsph_csf3_io& io, char* ws, cu
                                   static_cast<T*>(io.delta_s), io.valid);
   c_kappa<T><<<g, 128, 0, s>>>(p, pv, io.rowptr, io.entries, nq, minv, io.valid, static_cast<T*>(io.kappa));
   TSPH_LAUNCH_CHECK();
+  if (prm.curvature == 1) {
+    T* mer = reinterpret_cast<T*>(ws + L.mer);
+    T* mnormal = reinterpret_cast<T*>(ws + L.mnormal);
+    T* az = reinterpret_cast<T*>(ws + L.az);
+    T* kfit = reinterpret_cast<T*>(ws + L.kfit);
+    unsigned long long* fitmax = reinterpret_cast<unsigned long long*>(ws + L.fitmax);
+    const T* delta_s = static_cast<const T*>(io.delta_s);
+    TSPH_CUDA_CHECK(cudaMemsetAsync(fitmax, 0, 2 * sizeof(unsigned long long), s));
+    c_axis<T><<<grid_for(n, 256, 148 * 4), 256, 0, s>>>(n, static_cast<T>(0.25 * prm.h), static_cast<const T*>(io.pos),
+                                                        static_cast<const T*>(io.normal), delta_s, mer, mnormal, az,
+                                                        kfit, fitmax);
+    T* mom = reinterpret_cast<T*>(ws + L.mom);
+    T* fdet = reinterpret_cast<T*>(ws + L.fdet);
+    qf_moments<T><<<g, 128, 0, s>>>(n, static_cast<T>(4.0 * prm.h), mer, io.rowptr, io.entries, mnormal, delta_s,
+                                    fitmax, mom, fdet, fitmax + 1);
+    qf_solve<T><<<g, 128, 0, s>>>(n, delta_s, fitmax, mom, fdet, fitmax + 1, kfit);
+    c_axis_sum<T><<<grid_for(n, 256), 256, 0, s>>>(n, kfit, az, static_cast<T*>(io.kappa));
+    TSPH_LAUNCH_CHECK();
+  }
   return TSPH_OK;
 }
 
 template <class T>
 int run_accel(const tsph_csf3_params& prm, const void* normal, const void* kappa, const void* delta_s,
               const void* rho, void* acc, char* ws, cudaStream_t s) {
-  const CLayout L = c_layout(prm.n, prm.dtype);
+  const CLayout L = c_layout(prm.n, prm.dtype, prm.curvature);
   const CP<T> p = make_cp<T>(prm);
   unsigned long long* maxbits = reinterpret_cast<unsigned long long*>(ws + L.maxbits);
   TSPH_CUDA_CHECK(cudaMemsetAsync(maxbits, 0, sizeof(unsigned long long), s));
@@ -353,7 +425,8 @@ int run_accel(const tsph_csf3_params& prm, const void* normal, const void* kappa
 
 bool params_ok(const tsph_csf3_params* prm) {
   return prm && prm->n >= 0 && prm->n < (int64_t(1) << 31) && prm->h > 0.0 && prm->rho0 > 0.0 &&
-         (prm->dtype == TSPH_F32 || prm->dtype == TSPH_F64) && (prm->periodic == 0 || prm->periodic == 1);
+         (prm->dtype == TSPH_F32 || prm->dtype == TSPH_F64) && (prm->periodic == 0 || prm->periodic == 1) &&
+         (prm->curvature == 0 || prm->curvature == 1);
 }
 
 }  // namespace
@@ -365,7 +438,7 @@ extern "C" {
 
 int64_t tsph_csf3_workspace_bytes(const tsph_csf3_params* prm) {
   if (!params_ok(prm)) return -1;
-  return static_cast<int64_t>(c_layout(prm->n, prm->dtype).total);
+  return static_cast<int64_t>(c_layout(prm->n, prm->dtype, prm->curvature).total);
 }
 
 int tsph_csf3_fields(const tsph_csf3_params* prm, const tsph_csf3_io* io, void* ws, int64_t ws_bytes,

@@ -15,9 +15,11 @@ signatures (threed/csf3.py:115-165, 220-238) and its ``CSFState3`` fields:
 
 The pair list becomes symmetric gather rows, and the passes run as the
 kernels of ``csrc/csf3.cu``, in the dtype of the positions.  Separations use
-the minimum image when ``box`` is given.  The ``"axisym"`` curvature (a
-meridional fit that the reference documents as biased on a cylinder) is not
-built and raises ``NotImplementedError``.
+the minimum image when ``box`` is given.  ``curvature="axisym"``
+(csf3.py:168-220) replaces the curvature by the quadratic interface fit of
+the meridional projection (r, z) within 4 h plus the azimuthal n_r / r; its
+pair list must reach 4 h.  The reference documents that estimator as biased
+on a cylinder and keeps it as a comparison arm; it is reproduced as it is.
 """
 from __future__ import annotations
 
@@ -31,7 +33,7 @@ from .neighbors3 import _box_list
 
 __all__ = ["csf_fields3", "surface_tension_acceleration3", "CSFState3", "CURVATURE_SCHEMES"]
 
-#: The curvature schemes of the reference; only ``"mls"`` runs here.
+#: The curvature schemes of the reference.
 CURVATURE_SCHEMES = ("mls", "axisym")
 
 
@@ -57,8 +59,9 @@ class CSFState3:
                 "kappa": self.kappa, "delta_s": self.delta_s, "valid": self.valid}
 
 
-def _params(n, dtype, h, rho0, box, sigma=0.0, cutoff=1.0e-3):
+def _params(n, dtype, h, rho0, box, sigma=0.0, cutoff=1.0e-3, curvature="mls"):
     prm = _lib.Csf3Params()
+    prm.curvature = CURVATURE_SCHEMES.index(curvature)
     prm.n, prm.dtype = int(n), _lib.dtype_code(dtype)
     if box is not None:
         prm.periodic = 1
@@ -75,8 +78,6 @@ def csf_fields3(pos: torch.Tensor, mass: torch.Tensor, h: float, pairs: torch.Te
     """Colour, normal, curvature and delta function of a 3-D particle cloud."""
     if curvature not in CURVATURE_SCHEMES:
         raise ValueError(f"unknown curvature {curvature!r}; expected {CURVATURE_SCHEMES}")
-    if curvature != "mls":
-        raise NotImplementedError("csf_fields3 implements the 'mls' curvature only")
     if pos.dim() != 2 or pos.shape[1] != 3:
         raise ValueError("csf_fields3 implements 3-D clouds")
     n = pos.shape[0]
@@ -92,7 +93,7 @@ def csf_fields3(pos: torch.Tensor, mass: torch.Tensor, h: float, pairs: torch.Te
     kappa = torch.empty(n, dtype=dtype, device=dev)
     delta_s = torch.empty(n, dtype=dtype, device=dev)
     valid = torch.empty(n, dtype=torch.uint8, device=dev)
-    prm = _params(n, dtype, h, rho0, box)
+    prm = _params(n, dtype, h, rho0, box, curvature=curvature)
     io = _lib.Csf3IO(P.data_ptr(), M.data_ptr(), 0 if Vol is None else Vol.data_ptr(),
                      rowptr.data_ptr(), entries.data_ptr(), color.data_ptr(), grad_c.data_ptr(),
                      normal.data_ptr(), kappa.data_ptr(), delta_s.data_ptr(), valid.data_ptr())

@@ -108,3 +108,27 @@ def test_csf3_matches_oracle_on_a_larger_jittered_ball(gpu):
         d = np.abs(getattr(st, name).cpu().numpy() - r).max() / max(np.abs(r).max(), 1.0)
         assert d <= 1e-11, (name, d)
     assert np.abs(acc.cpu().numpy() - ref_acc).max() <= 1e-11 * np.abs(ref_acc).max()
+
+
+def test_csf3_axisym_matches_reference(golden, gpu):
+    """csf_fields3(curvature="axisym") on 4h lists (a jittered ball in FP64
+    and FP32, the periodic liquid column in FP64) against the reference's own
+    output (tests/golden/csf3axi.npz): the curvature of the surface particles
+    (delta_s > 1e-3 max) within 1e-9 (FP64) / 1e-3 (FP32) of its largest
+    value, and the acceleration the same."""
+    from tensorsph_b200.threed.csf3 import csf_fields3, surface_tension_acceleration3
+    g = golden("csf3axi")
+    for k in range(int(g["count"])):
+        pos = g[f"c{k}_pos"]
+        box = g[f"c{k}_box"]
+        dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+        st = csf_fields3(dev(pos), dev(g[f"c{k}_mass"]), float(g[f"c{k}_h"]), dev(g[f"c{k}_pairs"]),
+                         rho0=1000.0, box=None if not box.any() else box.tolist(), curvature="axisym")
+        tol = 1e-9 if pos.dtype == np.float64 else 1e-3
+        live = g[f"c{k}_delta_s"] > 1e-3 * g[f"c{k}_delta_s"].max()
+        r = g[f"c{k}_kappa"][live]
+        got = st.kappa.cpu().numpy()[live]
+        assert np.abs(got - r).max() <= tol * np.abs(r).max(), k
+        acc = surface_tension_acceleration3(st, dev(g[f"c{k}_rho"]), 0.0728).cpu().numpy()
+        ra = g[f"c{k}_acc"]
+        assert np.abs(acc - ra).max() <= tol * np.abs(ra).max(), k
