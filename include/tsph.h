@@ -530,6 +530,10 @@ typedef struct {
                                        /* min(slope h^2 |g|^2, 1); <= 0: none         */
   double tvc_wall_volume;              /* wall particle volume in the correction;    */
                                        /* <= 0: wall_mass / rho0                     */
+  double tvc_bulk_c;                   /* > 0: the correction moves only particles   */
+                                       /* whose concentration after the update is    */
+                                       /* >= tvc_bulk_c times its 95th percentile    */
+                                       /* (a batch of one, as shifting); 0: off      */
 } tsph_case_params;
 
 typedef struct tsph_engine tsph_engine; /* opaque host handle */

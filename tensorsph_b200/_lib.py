@@ -157,7 +157,8 @@ class CaseParams(ctypes.Structure):
                 ("grid_hi", c_double * 3), ("surface_tension", c_double),
                 ("periodic_box", c_double), ("tvc_every", c_int64), ("tvc_alpha", c_double),
                 ("tvc_scope_tol", c_double), ("tvc_max_shift", c_double),
-                ("first_step", c_int64), ("tvc_slope", c_double), ("tvc_wall_volume", c_double)]
+                ("first_step", c_int64), ("tvc_slope", c_double), ("tvc_wall_volume", c_double),
+                ("tvc_bulk_c", c_double)]
 
 
 _SIGNATURES = {

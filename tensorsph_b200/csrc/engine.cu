@@ -76,6 +76,8 @@ struct CaseDev {
   float tvc_tol;           // scope |g| h <= tol (< 0: every particle)
   float tvc_max;           // displacement clip (< 0: none)
   float tvc_slope_hh;      // truncated_linear limiter slope h^2 (< 0: none)
+  int tvc_bulk;            // the correction only where C >= tvc_bulk_c c_ref (after the second list pass)
+  double tvc_bulk_c;
 };
 
 struct CaseCtl {
@@ -94,7 +96,7 @@ struct CaseCtl {
   long long csf_rank;
   unsigned long long csf_fmax;
   double csf_med;
-  int tvc_now, tvc_pad;
+  int tvc_now, conc_now;  // conc_now: the concentration and its percentile this step
   unsigned long long tvc_max;       // largest |shift| of this step's correction (double bits)
   double tvc_sum;                   // sum of |shift|
   unsigned long long tvc_kept, tvc_clipped;
@@ -137,7 +139,7 @@ struct Dev {
   float2* st;        // CSF: surface-tension acceleration
   unsigned int* csf_hist;  // [n_slots][256] median-select histograms
   int has_csf, maxfit;
-  int has_tvc, tvc_pad_;
+  int has_tvc, tvc_late;  // tvc_late: the correction runs after the second list pass
   uint32_t* nbr4;    // CSF fit rows (fluid neighbours within 4h + skin), k-major over NF
   int32_t* cnt4;
   uint32_t* nbr;
@@ -432,7 +434,7 @@ __global__ void k_permute_back(Dev e) {
     e.home[a] = key;
     e.lp[a] = local_of(C, key - C.key_off, p.x, p.y, p.z, p.w);
     // the shifting passes after the Euler update read this step's volumes
-    if (C.shift_every > 0) e.lpv[a] = local_of(C, key - C.key_off, p.x, p.y, p.z, e.tmp_v[a]);
+    if (C.shift_every > 0 || C.tvc_bulk) e.lpv[a] = local_of(C, key - C.key_off, p.x, p.y, p.z, e.tmp_v[a]);
   }
 }
 
@@ -1400,7 +1402,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_integrate(const __grid_constant__
     st4(e.vel, a, make_double4(v[0], v[1], v[2], 0.0));
     const float4 la = local_of(C, e.home[a] - C.key_off, x[0], x[1], x[2], m);
     e.lp[a] = la;
-    if (C.shift_every > 0) e.lpv[a] = make_float4(la.x, la.y, la.z, e.vb[a].w);
+    if (C.shift_every > 0 || C.tvc_bulk) e.lpv[a] = make_float4(la.x, la.y, la.z, e.vb[a].w);
     const double4 an = ld4(e.anchor, a);
     double ex = x[0] - an.x, ey = x[1] - an.y, ez = x[2] - an.z;
     if (C.periodic) {
@@ -1466,6 +1468,7 @@ __global__ void k_finalize(Dev e) {
   t.shift_now = C.shift_every > 0 && step > 0 && (step % static_cast<unsigned long long>(C.shift_every)) == 0;
   t.shift_done = 0;
   t.tvc_now = C.tvc_every > 0 && step > 0 && (step % static_cast<unsigned long long>(C.tvc_every)) == 0;
+  t.conc_now = t.shift_now || (t.tvc_now && C.tvc_bulk);
   t.tvc_max = 0;
   t.tvc_sum = 0.0;
   t.tvc_kept = t.tvc_clipped = 0;
@@ -1484,6 +1487,9 @@ __global__ void k_finalize(Dev e) {
 //   |g| h <= tol, clipped to tvc_max, added to the position, then the box
 //   clamp; the displacement counts toward the next skin test.
 
+// kLate: after the second list pass, whose rebuild may have permuted the
+// fluid rows; the volumes then come from lpv, which travels with them
+template <bool kLate>
 __global__ void __launch_bounds__(kMaxBlock) k_tvc_gradient(Dev e) {
   const int NF = e.NF;
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
@@ -1500,7 +1506,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_tvc_gradient(Dev e) {
         const int b = static_cast<int>(ent[j] >> kCodeBits);
         const float4 lb = e.lp[b];
         // fluid: this step's m / rho; wall: m_w / rho0; the null row: 0
-        const float vb = b < NF ? e.vb[b].w : (b < e.null_row ? wvol : 0.f);
+        const float vb = b < NF ? (kLate ? e.lpv[b].w : e.vb[b].w) : (b < e.null_row ? wvol : 0.f);
         const float3 d = sep(la, lb, ent[j], cellf);
         const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
         const Radial R = radial(r2, inv_h);
@@ -1531,6 +1537,11 @@ __global__ void __launch_bounds__(kMaxBlock) k_tvc_apply(Dev e) {
     float sx = coef * g.x, sy = coef * g.y, sz = coef * g.z;
     bool kept = true;
     if (C.tvc_tol >= 0.f && !(sqrtf(g.w) * static_cast<float>(C.h_d) <= C.tvc_tol)) {
+      kept = false;
+      sx = sy = sz = 0.f;
+    }
+    // the bulk scope: C_a >= tvc_bulk_c c_ref (dam_break.py:441-444)
+    if (C.tvc_bulk && !(static_cast<double>(e.conc[a]) >= C.tvc_bulk_c * t.cref[0])) {
       kept = false;
       sx = sy = sz = 0.f;
     }
@@ -1582,7 +1593,7 @@ __global__ void k_tvc_finish(Dev e) {
 // One case (slot e.shift_slot) owns every fluid row when shifting runs.
 
 __global__ void __launch_bounds__(kMaxBlock) k_concentration(Dev e) {
-  if (!e.ctl[e.shift_slot].shift_now) return;
+  if (!e.ctl[e.shift_slot].conc_now) return;
   const CaseDev& C = e.cases[e.shift_slot];
   const float sig2d = C.sig2d, inv_h = C.inv_h, cellf = C.cellf;
   const int NF = e.NF;
@@ -1664,7 +1675,7 @@ __device__ __forceinline__ uint32_t fkey(float v) {
 constexpr int kSelBins = 2048;
 
 __global__ void k_select_hist(Dev e, int shift, int width) {
-  if (!e.ctl[e.shift_slot].shift_now) return;
+  if (!e.ctl[e.shift_slot].conc_now) return;
   __shared__ unsigned int h[2][kSelBins];
   for (int i = threadIdx.x; i < 2 * kSelBins; i += blockDim.x) (&h[0][0])[i] = 0;
   __syncthreads();
@@ -1689,7 +1700,7 @@ __global__ void k_select_hist(Dev e, int shift, int width) {
 // cleared for the next pass.
 __global__ void __launch_bounds__(1024) k_select_pick(Dev e, int shift, int width, long long rank_lo,
                                                       long long rank_hi) {
-  if (!e.ctl[e.shift_slot].shift_now) return;
+  if (!e.ctl[e.shift_slot].conc_now) return;
   __shared__ unsigned int warp_sum[32];
   __shared__ int found_digit;
   __shared__ unsigned long long found_below;
@@ -1755,7 +1766,7 @@ __global__ void __launch_bounds__(1024) k_select_pick(Dev e, int shift, int widt
 
 // torch.quantile's linear interpolation, computed as torch.lerp does it
 __global__ void k_select_finish(Dev e, double w) {
-  if (!e.ctl[e.shift_slot].shift_now || threadIdx.x || blockIdx.x) return;
+  if (!e.ctl[e.shift_slot].conc_now || threadIdx.x || blockIdx.x) return;
   const double a = __longlong_as_double(static_cast<long long>(e.sel[2]));
   const double b = __longlong_as_double(static_cast<long long>(e.sel[3]));
   e.ctl[e.shift_slot].cref[0] = w < 0.5 ? a + w * (b - a) : b - (b - a) * (1.0 - w);
@@ -2040,13 +2051,22 @@ void invalidate_graph(tsph_engine* E) {
 
 bool shifting(const tsph_engine* E) { return E->order.size() == 1 && E->order[0].prm.shift_every > 0; }
 
+// A case that needs the whole batch: shifting, or the correction's bulk
+// scope (both take a percentile of the concentration over the batch).
+bool whole_batch(const tsph_case_params& p) { return p.shift_every > 0 || (p.tvc_every > 0 && p.tvc_bulk_c > 0.0); }
+
+// The step has a second list pass (after the update): shifting or a bulk-
+// scope correction, in a batch of one.
+bool second_pass(const tsph_engine* E) { return E->order.size() == 1 && whole_batch(E->order[0].prm); }
+
 // Per-batch fields of the kernel parameters: the shifting slot and, for a
 // batch of one, the case itself.
 void batch_changed(tsph_engine* E) {
   Dev& d = E->d;
-  d.shift_slot = shifting(E) ? E->order[0].slot : 0;
+  d.shift_slot = second_pass(E) ? E->order[0].slot : 0;
   d.has_csf = 0;
   d.has_tvc = 0;
+  d.tvc_late = second_pass(E) && E->order[0].dev.tvc_bulk ? 1 : 0;
   for (const CaseHost& c : E->order) {
     d.has_csf |= c.dev.csf;
     d.has_tvc |= c.dev.tvc_every > 0 ? 1 : 0;
@@ -2189,21 +2209,21 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr, b
   mark();
   (one ? k_integrate<true> : k_integrate<false>)<<<static_cast<unsigned>((d.nf + B - 1) / B), B, 0, s>>>(d);
   k_finalize<<<gc, 128, 0, s>>>(d);
-  if (d.has_tvc) {
+  if (d.has_tvc && !d.tvc_late) {
     // the correction reads the rows of this step (the pass-0 lists)
-    k_tvc_gradient<<<g, B, 0, s>>>(d);
+    k_tvc_gradient<false><<<g, B, 0, s>>>(d);
     k_tvc_apply<<<g, B, 0, s>>>(d);
     k_tvc_finish<<<gc, 128, 0, s>>>(d);
   }
   TSPH_LAUNCH_CHECK();
   mark();
-  if (shifting(E)) {
+  if (second_pass(E)) {
     rc = enqueue_rebuild(E, s, 1, graph);
     if (rc) return rc;
     mark();
     k_concentration<<<g, B, 0, s>>>(d);
     mark();
-    k_conc_gradient<<<g, B, 0, s>>>(d);
+    if (shifting(E)) k_conc_gradient<<<g, B, 0, s>>>(d);
     mark();
     const double pos = 0.95 * static_cast<double>(d.nf - 1);
     const long long lo = static_cast<long long>(std::floor(pos)), hi = static_cast<long long>(std::ceil(pos));
@@ -2215,7 +2235,13 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr, b
     }
     k_select_finish<<<1, 32, 0, s>>>(d, pos - static_cast<double>(lo));
     mark();
-    k_shift_apply<<<g, B, 0, s>>>(d);
+    if (shifting(E)) k_shift_apply<<<g, B, 0, s>>>(d);
+    if (d.tvc_late) {
+      // the bulk scope: the rows of the second pass, the mask of its percentile
+      k_tvc_gradient<true><<<g, B, 0, s>>>(d);
+      k_tvc_apply<<<g, B, 0, s>>>(d);
+      k_tvc_finish<<<gc, 128, 0, s>>>(d);
+    }
     TSPH_LAUNCH_CHECK();
     mark();
   }
@@ -2298,6 +2324,8 @@ CaseDev make_case_dev(const tsph_case_params& p, int64_t* ncells) {
   c.tvc_tol = static_cast<float>(p.tvc_scope_tol);
   c.tvc_max = static_cast<float>(p.tvc_max_shift);
   c.tvc_slope_hh = p.tvc_slope > 0.0 ? static_cast<float>(p.tvc_slope * p.h * p.h) : -1.f;
+  c.tvc_bulk = p.tvc_every > 0 && p.tvc_bulk_c > 0.0 ? 1 : 0;
+  c.tvc_bulk_c = p.tvc_bulk_c;
   return c;
 }
 
@@ -2318,7 +2346,8 @@ bool case_params_ok(const tsph_case_params* p) {
   if (p->tvc_every < 0 || (p->tvc_every > 0 && (p->has_obstacle || p->shift_every != 0 || p->periodic_box > 0.0 ||
                                                 !std::isfinite(p->tvc_alpha) || !std::isfinite(p->tvc_scope_tol) ||
                                                 !std::isfinite(p->tvc_max_shift) || !std::isfinite(p->tvc_slope) ||
-                                                !std::isfinite(p->tvc_wall_volume))))
+                                                !std::isfinite(p->tvc_wall_volume) || !std::isfinite(p->tvc_bulk_c) ||
+                                                p->tvc_bulk_c < 0.0)))
     return false;
   return true;
 }
@@ -2422,8 +2451,8 @@ int tsph_engine_add_case(tsph_engine* E, const tsph_case_params* p, const double
                          const double* mass, const double* wall, tsph_stream stream, int64_t* case_id) {
   if (!E || !x || !v || !mass || !case_id || !case_params_ok(p) || (p->n_wall > 0 && !wall)) return TSPH_ERR_ARG;
   // shifting needs the whole batch (its reference concentration is a global quantile)
-  if (p->shift_every > 0 && !E->order.empty()) return TSPH_ERR_UNSUPPORTED;
-  if (shifting(E)) return TSPH_ERR_UNSUPPORTED;
+  if (whole_batch(*p) && !E->order.empty()) return TSPH_ERR_UNSUPPORTED;
+  if (second_pass(E)) return TSPH_ERR_UNSUPPORTED;
   if (p->surface_tension > 0.0 && p->dim == 2 && E->prm.max_fit_neighbors <= 0) return TSPH_ERR_CAPACITY;
   if (E->free_slots.empty()) return TSPH_ERR_CAPACITY;
   Dev& d = E->d;
@@ -2617,7 +2646,7 @@ int tsph_engine_step_timed(tsph_engine* E, tsph_stream stream, float* stage_ms, 
   for (int i = 0; i <= kStages; ++i) TSPH_CUDA_CHECK(cudaEventCreate(&ev[i]));
   TSPH_CUDA_CHECK(cudaEventRecord(ev[0], s));
   int rc = enqueue_step(E, s, ev + 1);
-  const int n = shifting(E) ? kStages : 7;
+  const int n = second_pass(E) ? kStages : 7;
   if (rc == TSPH_OK) {
     if (cudaEventSynchronize(ev[n]) != cudaSuccess) rc = TSPH_ERR_CUDA;
     for (int i = 0; i < n && rc == TSPH_OK; ++i)

@@ -168,7 +168,7 @@ def _case_params(*, dim, n_fluid, n_wall, n_obstacle, cfg, h, wall_mass, box_hi,
         p.ob_eps = 0.01 * cfg.dx
     p.tvc_every = int(getattr(cfg, "tvc_every", 0) or 0)
     p.tvc_alpha, p.tvc_scope_tol, p.tvc_max_shift = 0.0, -1.0, -1.0
-    p.tvc_slope, p.tvc_wall_volume = -1.0, -1.0
+    p.tvc_slope, p.tvc_wall_volume, p.tvc_bulk_c = -1.0, -1.0, 0.0
     if p.tvc_every and (obstacle is not None or shift_every):
         raise NotImplementedError("the device engine runs the transport-velocity correction in the "
                                   "dam breaks without an obstacle or shifting")
@@ -180,15 +180,17 @@ def _case_params(*, dim, n_fluid, n_wall, n_obstacle, cfg, h, wall_mass, box_hi,
             # dam_break_3d.py:675-704: scope by |g| h, walls at m_w / rho0
             p.tvc_scope_tol = -1.0 if cfg.tvc_scope_tol is None else float(cfg.tvc_scope_tol)
         else:
-            # dam_break.py:434-459: scope "all" or "bulk_g" (|g| h <= tvc_bulk_g),
-            # the named limiter, walls at dx^2
+            # dam_break.py:434-459: scope "all", "bulk_g" (|g| h <= tvc_bulk_g)
+            # or "bulk" (C >= tvc_bulk_c c_ref after the update), the named
+            # limiter, walls at dx^2
             scope = getattr(cfg, "tvc_scope", "all")
-            if scope == "bulk":
-                raise NotImplementedError("tvc_scope='bulk' (the concentration mask) is not part of the "
-                                          "device engine; use 'all' or 'bulk_g'")
-            if scope not in ("all", "bulk_g"):
+            if scope not in ("all", "bulk_g", "bulk"):
                 raise ValueError(f"unknown tvc_scope {scope!r}")
             p.tvc_scope_tol = float(cfg.tvc_bulk_g) if scope == "bulk_g" else -1.0
+            if scope == "bulk":
+                if not cfg.tvc_bulk_c > 0.0:
+                    raise ValueError("tvc_scope='bulk' needs tvc_bulk_c > 0")
+                p.tvc_bulk_c = float(cfg.tvc_bulk_c)
             limiter = getattr(cfg, "tvc_limiter", None)
             if limiter == "truncated_linear":
                 p.tvc_slope = float(cfg.tvc_limiter_slope)
@@ -950,7 +952,7 @@ def run_dam_break_2d(cfg, *, snapshot_times=None, max_neighbors: int = 64) -> Da
     """Integrate the 2-D dam break (dam_break.py:319-460 with the pair cache,
     fixed dt) on the GPU and return the measured trajectory;
     ``snapshot_times`` as in ``run_case``.  Shifting and the transport-velocity
-    correction (``tvc_every``, scopes "all" and "bulk_g", the
+    correction (``tvc_every``, scopes "all", "bulk_g" and "bulk", the
     ``truncated_linear`` limiter, the clip) each run, not both together."""
     if cfg.adaptive_dt:
         raise NotImplementedError("adaptive_dt is not supported by the device engine")

@@ -306,7 +306,8 @@ def dam_break_2d_case_small():
 
 
 @pytest.mark.parametrize("opts", [dict(), dict(tvc_alpha=0.2, tvc_scope="bulk_g", tvc_limiter="truncated_linear",
-                                               tvc_limiter_slope=10.0, tvc_max_shift=2e-3)])
+                                               tvc_limiter_slope=10.0, tvc_max_shift=2e-3),
+                                  dict(tvc_scope="bulk", tvc_bulk_c=0.95)])
 def test_2d_tvc_matches_fp64_oracle(opts, gpu):
     """The 2-D dam break's transport-velocity correction in the engine
     (dam_break.py:434-459: after the update, volumes m / rho of the step,
@@ -315,7 +316,11 @@ def test_2d_tvc_matches_fp64_oracle(opts, gpu):
     of step 1) with a zero skin, from a lattice jittered by +-0.1 dx.  The
     displacement (run with the correction minus run without) matches the
     oracle's shift to 1e-4 of its largest component, and run_dam_break_2d
-    reports the largest shift and clipped fraction."""
+    reports the largest shift and clipped fraction.  The "bulk" scope masks
+    by the concentration after the update against its 95th percentile (the
+    oracle's shifting concentration); particles within 1e-5 of that
+    threshold, where FP32 rounding may decide, are left out of the
+    comparison."""
     from dataclasses import replace
 
     from oracle import tvc as otv
@@ -342,18 +347,26 @@ def test_2d_tvc_matches_fp64_oracle(opts, gpu):
     pairs = cell_linked_pairs(np.concatenate((x1, wn)), 2.0 * h)
     vol = np.concatenate((mn / ref[1][0], np.full(wn.shape[0], cfg.dx ** 2)))
     c = replace(cfg, tvc_every=1, **opts)
+    active, keep = None, np.ones(mn.size, dtype=bool)
+    if c.tvc_scope == "bulk":
+        _, info = op.shift_positions(x2, mn / ref[1][0], h, dt=cfg.dt, v_ref=1.0)
+        thr = c.tvc_bulk_c * info["c_reference"]
+        active = info["concentration"] >= thr
+        keep = np.abs(info["concentration"] - thr) > 1e-5 * thr
+        assert 0 < active.sum() < mn.size
     res = otv.transport_velocity_correction(
         np.concatenate((x2, wn)), vol, h, pairs, wall_count=wn.shape[0],
         alpha=0.05 if c.tvc_alpha is None else c.tvc_alpha, h_ref=h,
         slope=c.tvc_limiter_slope if c.tvc_limiter == "truncated_linear" else None,
-        scope_tol=c.tvc_bulk_g if c.tvc_scope == "bulk_g" else None,
+        scope_tol=c.tvc_bulk_g if c.tvc_scope == "bulk_g" else None, active=active,
         max_shift=None if c.tvc_max_shift is None else c.tvc_max_shift * h)
     shift = res["shift"]
     assert np.abs(shift).max() > 1e-5 * cfg.dx
-    err = np.abs((runs[1] - runs[0]) - shift).max()
+    err = np.abs((runs[1] - runs[0])[keep] - shift[keep]).max()
     assert err < 1e-4 * np.abs(shift).max(), err / np.abs(shift).max()
     norm = np.linalg.norm(shift, axis=1)
-    assert diags[1][16] == pytest.approx(norm.max(), rel=1e-4)
+    if keep.all():
+        assert diags[1][16] == pytest.approx(norm.max(), rel=1e-4)
     assert diags[1][19] / mn.size == pytest.approx(res["clipped"], abs=1.5 / mn.size)
     run = run_dam_break_2d(replace(c, steps=3))
     assert run.max_tvc_shift >= 0.0 and 0.0 <= run.max_tvc_clipped <= 1.0
@@ -363,12 +376,12 @@ def test_2d_tvc_matches_fp64_oracle(opts, gpu):
         assert run.max_tvc_shift <= c.tvc_max_shift * h * (1 + 1e-6)
 
 
-def test_2d_tvc_refuses_bulk_scope_and_shifting():
+def test_2d_tvc_refuses_shifting_and_unknown_options():
     from dataclasses import replace
 
     from tensorsph_b200.engine import dam_break_2d_case
-    with pytest.raises(NotImplementedError):
-        dam_break_2d_case(replace(small_2d(), tvc_every=1, tvc_scope="bulk"))
+    with pytest.raises(ValueError):
+        dam_break_2d_case(replace(small_2d(), tvc_every=1, tvc_scope="surface"))
     with pytest.raises(NotImplementedError):
         dam_break_2d_case(replace(small_2d(), tvc_every=1), shift_every=1)
     with pytest.raises(ValueError):
