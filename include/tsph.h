@@ -534,6 +534,9 @@ typedef struct {
                                        /* whose concentration after the update is    */
                                        /* >= tvc_bulk_c times its 95th percentile    */
                                        /* (a batch of one, as shifting); 0: off      */
+  int64_t csf_curvature;               /* with surface_tension: 0 "fit_quadratic",   */
+                                       /* 1 "mls" (div n), 2 "fit_circle"            */
+  int64_t csf_delta_normalization;     /* 0 "legacy" (2 |grad c|), 1 "local_range"   */
 } tsph_case_params;
 
 typedef struct tsph_engine tsph_engine; /* opaque host handle */

@@ -64,6 +64,8 @@ struct CaseDev {
   float cellf, inv_h, sigma, sig2d, rho0, bulk, gamma, inv_gamma;
   float grav, nu2, nu2f, dscale, dtf, visc_eps, rho_floor, wall_mass;
   int csf;                 // CSF surface tension on (2-D)
+  int csf_fit;             // curvature fit: 0 none ("mls"), 1 quadratic, 2 circle
+  int csf_range;           // delta_s = |grad c| / local colour range ("local_range")
   int periodic;            // triply periodic cube of edge pbox (3-D, no walls)
   double pbox;             // the cube edge: n cells x the FP32 cell edge, exactly
   int stencil_cells;       // cells each side covering the 4h fit stencil
@@ -95,6 +97,7 @@ struct CaseCtl {
   unsigned long long csf_gmax, csf_prefix;
   long long csf_rank;
   unsigned long long csf_fmax;
+  unsigned long long csf_dmax;  // largest local_range delta_s (double bits)
   double csf_med;
   int tvc_now, conc_now;  // conc_now: the concentration and its percentile this step
   unsigned long long tvc_max;       // largest |shift| of this step's correction (double bits)
@@ -136,6 +139,7 @@ struct Dev {
   double2* csN1;     // CSF: normal after one Shepard pass
   double2* csN;      // CSF: final normal
   double4* csK;      // CSF: kappa_mls, kappa_fit, own fit weight, |det fit|
+  double* csD;       // CSF: delta_s = |grad c| / local colour range ("local_range")
   float2* st;        // CSF: surface-tension acceleration
   unsigned int* csf_hist;  // [n_slots][256] median-select histograms
   int has_csf, maxfit;
@@ -1099,6 +1103,61 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_grad(const __grid_constant__ 
   case_max_double(e, c, cb, uniform && all, mag, &CaseCtl::csf_gmax, red);
 }
 
+// Q3b ("local_range"): the colour range max c - min c over the particle and
+// its partners, clipped to [0.2, 1] (csf_consistent.py:231-259); delta_s =
+// |grad c| / range and its per-case maximum.  The partners are the list rows
+// with "mls" (the list the droplet step hands over) and the fit rows within
+// 4 h with a fit (the 4h list the reference builds for it).
+__global__ void __launch_bounds__(kMaxBlock) k_csf_range(const __grid_constant__ Dev e) {
+  __shared__ double red[kMaxBlock / 32];
+  const int a0 = blockIdx.x * blockDim.x;
+  if (a0 >= e.nf) return;
+  const int a = a0 + threadIdx.x;
+  const int cb = e.cid[a0];
+  const bool uniform = cb == e.cid[min(a0 + static_cast<int>(blockDim.x), e.nf) - 1];
+  int c = -1;
+  double ds = 0.0;
+  if (a < e.nf) {
+    c = e.cid[a];
+    const CaseDev& C = e.cases[c];
+    if (C.csf && C.csf_range) {
+      const double ca = e.csA[a].x;
+      double hi = ca, lo = ca;
+      if (C.csf_fit) {
+        const double4 pa = ld4(e.pos, a);
+        const int n4 = e.cnt4[a];
+        for (int k = 0; k < n4; ++k) {
+          const int b = static_cast<int>(e.nbr4[static_cast<int64_t>(k) * e.NF + a] >> kCodeBits);
+          const double2 pb = ld_xy(e.pos, b);
+          const double dx = pa.x - pb.x, dy = pa.y - pb.y;
+          if (!(dx * dx + dy * dy <= C.stencil2)) continue;
+          const double cv = e.csA[b].x;
+          hi = cv > hi ? cv : hi;
+          lo = cv < lo ? cv : lo;
+        }
+      } else {
+        fluid_row(e, a, [&](const int* b, const bool* ok) {
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            if (!ok[j]) continue;
+            const double cv = e.csA[b[j]].x;
+            hi = cv > hi ? cv : hi;
+            lo = cv < lo ? cv : lo;
+          }
+        });
+      }
+      double r = hi - lo;
+      r = r < 0.2 ? 0.2 : (r > 1.0 ? 1.0 : r);
+      ds = e.csB[a].z / r;
+      e.csD[a] = ds;
+    } else {
+      c = -1;
+    }
+  }
+  const bool all = __syncthreads_and(c >= 0 || a >= e.nf);
+  case_max_double(e, c, cb, uniform && all, ds, &CaseCtl::csf_dmax, red);
+}
+
 // Q4 / Q5: one Shepard pass of the normal field; the second pass also
 // renormalises on the interface (|grad c| > 1e-12, csf_consistent.py:320-330).
 template <bool kFinal>
@@ -1198,14 +1257,19 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_fit(const __grid_constant__ D
   if (a < e.nf) {
     c = e.cid[a];
     const CaseDev& C = e.cases[c];
-    if (C.csf) {
-      const double gmax = fmax(__longlong_as_double(static_cast<long long>(e.ctl[c].csf_gmax)), 1e-30);
+    if (C.csf && C.csf_fit == 0) {
+      detabs = 0.0;  // "mls": no fit
+    } else if (C.csf) {
+      // the fit weights: delta_s_b / max delta_s (legacy: |grad c| / max |grad c|)
+      const bool rng = C.csf_range != 0;
+      const double gmax = fmax(__longlong_as_double(static_cast<long long>(rng ? e.ctl[c].csf_dmax : e.ctl[c].csf_gmax)),
+                               1e-30);
       const double inv_g = 1.0 / gmax;
       const double st2 = C.stencil2;
       const double4 pa = ld4(e.pos, a);
       const double2 na = e.csN[a];
       const double tx = -na.y, ty = na.x;
-      double s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0, s6 = 0, s7 = 0;
+      double s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0, s6 = 0, s7 = 0, s8 = 0;
       const int n4 = e.cnt4[a];
       int nb4[4];
 #pragma unroll
@@ -1223,7 +1287,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_fit(const __grid_constant__ D
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
           pb[j] = ld_xy(e.pos, b[j]);
-          mg[j] = e.csB[b[j]].z;
+          mg[j] = rng ? e.csD[b[j]] : e.csB[b[j]].z;
         }
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
@@ -1232,6 +1296,20 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_fit(const __grid_constant__ D
           double w = mg[j] * inv_g;
           w = w < 0.0 ? 0.0 : (w > 1.0 ? 1.0 : w);
           w = (k + j < n4 && ddx * ddx + ddy * ddy <= st2) ? w : 0.0;
+          if (C.csf_fit == 2) {
+            // circle moments of the offset (x, y) = x_b - x_a, f = x^2 + y^2
+            const double x = -ddx, y = -ddy, f = x * x + y * y;
+            s0 += w;
+            s1 += w * x;
+            s2 += w * y;
+            s3 += w * (x * x);
+            s4 += w * (x * y);
+            s5 += w * (y * y);
+            s6 += w * (x * f);
+            s7 += w * (y * f);
+            s8 += w * f;
+            continue;
+          }
           const double u = -(ddx * tx + ddy * ty), v = -(ddx * na.x + ddy * na.y);
           const double uu = u * u;
           s0 += w;
@@ -1244,9 +1322,32 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_fit(const __grid_constant__ D
           s7 += w * (uu * uu);
         }
       }
-      double wa = e.csB[a].z * inv_g;
+      double wa = (rng ? e.csD[a] : e.csB[a].z) * inv_g;
       wa = wa < 0.0 ? 0.0 : (wa > 1.0 ? 1.0 : wa);
       s0 += wa;
+      if (C.csf_fit == 2) {
+        // Pratt: x^2 + y^2 + D x + E y + F = 0, [[s3 s4 s1] [s4 s5 s2] [s1 s2 s0]]
+        // (D, E, F) = -(s6, s7, s8) by Cramer's rule (csf_curvature.py:179-213)
+        const double det = s3 * (s5 * s0 - s2 * s2) - s4 * (s4 * s0 - s2 * s1) + s1 * (s4 * s2 - s5 * s1);
+        const double r0 = -s6, r1 = -s7, r2 = -s8;
+        double4 K = e.csK[a];
+        double kfit = K.x;  // kept where the centre's side is undefined
+        if (det != 0.0) {
+          const double dd = (r0 * (s5 * s0 - s2 * s2) - s4 * (r1 * s0 - s2 * r2) + s1 * (r1 * s2 - s5 * r2)) / det;
+          const double de = (s3 * (r1 * s0 - s2 * r2) - r0 * (s4 * s0 - s2 * s1) + s1 * (s4 * r2 - r1 * s1)) / det;
+          const double df = (s3 * (s5 * r2 - r1 * s2) - s4 * (s4 * r2 - r1 * s1) + r0 * (s4 * s2 - s5 * s1)) / det;
+          const double cx = -0.5 * dd, cy = -0.5 * de;
+          const double q = cx * cx + cy * cy - df;
+          const double rad = sqrt(q > 1e-30 ? q : 1e-30);
+          const double side = cx * na.x + cy * na.y;
+          if (side != 0.0) kfit = -(side > 0.0 ? 1.0 : -1.0) / (rad > 1e-30 ? rad : 1e-30);
+        }
+        detabs = fabs(det);
+        K.y = kfit;
+        K.z = wa;
+        K.w = detabs;
+        e.csK[a] = K;
+      } else {
       // [s0 s1 s3; s1 s3 s5; s3 s5 s7] (c, b, a) = (s2, s4, s6); Cramer's rule
       const double c0 = s3 * s7 - s5 * s5, c1 = s1 * s7 - s5 * s3, c2 = s1 * s5 - s3 * s3;
       const double det = s0 * c0 - s1 * c1 + s3 * c2;
@@ -1263,6 +1364,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_fit(const __grid_constant__ D
       K.z = wa;
       K.w = detabs;
       e.csK[a] = K;
+      }
     } else {
       c = -1;
     }
@@ -1272,7 +1374,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_fit(const __grid_constant__ D
 }
 
 // Q8: kappa (fit where active and regular, else kappa_mls), delta_s = 2|grad c|
-// with the flat mask, a = -sigma kappa delta_s n / rho
+// or the local_range value, with the flat mask, a = -sigma kappa delta_s n / rho
 __global__ void k_csf_final(const __grid_constant__ Dev e) {
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
     const int c = e.cid[a];
@@ -1281,11 +1383,11 @@ __global__ void k_csf_final(const __grid_constant__ Dev e) {
     const CaseCtl& t = e.ctl[c];
     const double4 K = e.csK[a];
     const double det_max = fmax(__longlong_as_double(static_cast<long long>(t.csf_fmax)), 1e-30);
-    const bool ok = K.z > 0.05 && K.w > 1e-6 * det_max;
+    const bool ok = C.csf_fit != 0 && K.z > 0.05 && K.w > 1e-6 * det_max;
     const double kappa = ok ? K.y : K.x;
     const double mag = e.csB[a].z;
     const double gmax = __longlong_as_double(static_cast<long long>(t.csf_gmax));
-    const double ds = mag <= 1e-3 * gmax ? 0.0 : 2.0 * mag;
+    const double ds = mag <= 1e-3 * gmax ? 0.0 : (C.csf_range ? e.csD[a] : 2.0 * mag);
     const double2 n = e.csN[a];
     const double f = -C.sigma_st * kappa * ds / static_cast<double>(e.rho[a]);
     e.st[a] = make_float2(static_cast<float>(f * n.x), static_cast<float>(f * n.y));
@@ -1297,6 +1399,7 @@ __global__ void k_csf_clear(Dev e) {
   if (c >= e.n_slots) return;
   e.ctl[c].csf_gmax = 0;
   e.ctl[c].csf_fmax = 0;
+  e.ctl[c].csf_dmax = 0;
 }
 
 // Semi-implicit Euler, box and obstacle clamps, per-case meters (of the state
@@ -2001,6 +2104,7 @@ size_t carve(const tsph_engine_params& p, Dev* d, char* base, CaseDev** cases, c
   t.csN1 = static_cast<double2*>(take(NF * sizeof(double2)));
   t.csN = static_cast<double2*>(take(NF * sizeof(double2)));
   t.csK = static_cast<double4*>(take(NF * sizeof(double4)));
+  t.csD = static_cast<double*>(take(NF * sizeof(double)));
   t.st = static_cast<float2*>(take(NF * sizeof(float2)));
   t.csf_hist = static_cast<unsigned int*>(take(static_cast<size_t>(p.max_cases) * 256 * sizeof(unsigned int)));
   t.nbr4 = static_cast<uint32_t*>(take(static_cast<size_t>(p.max_fit_neighbors) * NF * sizeof(uint32_t)));
@@ -2194,6 +2298,7 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr, b
       k_csf_pick<<<gp, 128, 0, s>>>(d, shift);
     }
     k_csf_grad<<<gf, B, 0, s>>>(d);
+    k_csf_range<<<gf, B, 0, s>>>(d);
     k_csf_smooth<false><<<g, B, 0, s>>>(d);
     k_csf_smooth<true><<<g, B, 0, s>>>(d);
     k_csf_div<<<g, B, 0, s>>>(d);
@@ -2310,6 +2415,8 @@ CaseDev make_case_dev(const tsph_case_params& p, int64_t* ncells) {
   c.rho_floor = static_cast<float>(0.1 * p.rho0);
   c.wall_mass = static_cast<float>(p.wall_mass);
   c.csf = (p.surface_tension > 0.0 && p.dim == 2) ? 1 : 0;
+  c.csf_fit = p.csf_curvature == 1 ? 0 : (p.csf_curvature == 2 ? 2 : 1);
+  c.csf_range = p.csf_delta_normalization == 1 ? 1 : 0;
   c.sigma_st = p.surface_tension;
   c.h_d = p.h;
   c.inv_h_d = 1.0 / p.h;
@@ -2332,6 +2439,9 @@ CaseDev make_case_dev(const tsph_case_params& p, int64_t* ncells) {
 bool case_params_ok(const tsph_case_params* p) {
   if (!p || (p->dim != 2 && p->dim != 3) || p->n_fluid <= 0 || p->n_wall < 0 || p->n_obstacle < 0 ||
       p->n_obstacle > p->n_wall || p->shift_every < 0 || p->first_step < 0)
+    return false;
+  if (p->csf_curvature < 0 || p->csf_curvature > 2 || p->csf_delta_normalization < 0 ||
+      p->csf_delta_normalization > 1)
     return false;
   if (!(p->h > 0) || !(p->dt > 0) || !(p->skin >= 0) || !(p->rho0 > 0) || !(p->gamma > 0) ||
       !(p->sound_speed > 0))

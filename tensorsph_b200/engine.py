@@ -280,15 +280,20 @@ def droplet_impact_case(cfg, *, drop_speed: float = 0.0, label: str = "") -> Cas
     ``domain_top``, droplet_impact.py:666-760) as a ``CaseSpec``; the drop
     starts with the downward speed ``drop_speed`` (the reference drops it from
     rest).  ``surface_tension_coefficient > 0`` turns on the consistent CSF
-    force with the quadratic curvature fit (csf_consistent.py:384-446)."""
+    force (csf_consistent.py:384-446) with the configuration's curvature
+    ("fit_quadratic", "mls" or "fit_circle") and delta_s normalisation
+    ("legacy" or "local_range")."""
     from .droplet_impact import domain_top, lattice_mass_unit, make_particles, validate_config, wall_lattice
     validate_config(cfg)
+    curvature = {"fit_quadratic": 0, "mls": 1, "fit_circle": 2}
+    normalization = {"legacy": 0, "local_range": 1}
     if cfg.surface_tension_coefficient > 0.0:
-        if (cfg.csf_scheme != "consistent" or cfg.csf_curvature != "fit_quadratic"
-                or cfg.csf_delta_normalization != "legacy" or cfg.contact_angle is not None):
+        if cfg.csf_scheme != "consistent" or cfg.contact_angle is not None:
             raise NotImplementedError("the device engine implements the consistent CSF scheme "
-                                      "with the fit_quadratic curvature, legacy delta_s and no "
-                                      "contact angle")
+                                      "without a contact angle")
+        if cfg.csf_curvature not in curvature or cfg.csf_delta_normalization not in normalization:
+            raise ValueError(f"unknown csf_curvature {cfg.csf_curvature!r} or csf_delta_normalization "
+                             f"{cfg.csf_delta_normalization!r}")
     if cfg.density_renormalization or cfg.boundary_consistent_density:
         raise NotImplementedError("density_renormalization and boundary_consistent_density are "
                                   "not part of the device engine")
@@ -306,6 +311,9 @@ def droplet_impact_case(cfg, *, drop_speed: float = 0.0, label: str = "") -> Cas
                      wall_mass=lattice_mass_unit(cfg), box_hi=(cfg.pool_width, top, 0.0),
                      lo=allpos.min(dim=0).values.tolist(), hi=allpos.max(dim=0).values.tolist())
     p.surface_tension = float(cfg.surface_tension_coefficient)
+    if p.surface_tension > 0.0:
+        p.csf_curvature = curvature[cfg.csf_curvature]
+        p.csf_delta_normalization = normalization[cfg.csf_delta_normalization]
     return CaseSpec(p, x, v, mass.double().contiguous(), wall, label or "droplet_impact")
 
 

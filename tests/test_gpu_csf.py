@@ -30,23 +30,34 @@ def drop_config(sigma):
                   surface_tension_coefficient=sigma)
 
 
-def test_engine_csf_matches_oracle(gpu):
+@pytest.mark.parametrize("curvature,normalization", [("fit_quadratic", "legacy"), ("mls", "legacy"),
+                                                     ("mls", "local_range"), ("fit_quadratic", "local_range"),
+                                                     ("fit_circle", "legacy")])
+def test_engine_csf_matches_oracle(curvature, normalization, gpu):
+    """The droplet case's CSF options (csf_curvature, csf_delta_normalization).
+    With "mls" the reference hands the CSF the step's cached fluid list, so the
+    oracle gets the fluid pairs within 2h + skin of the first build (what
+    "local_range" reads); the fits use the 4h list the reference builds."""
+    from dataclasses import replace
+
     from tensorsph_b200.engine import BatchEngine, capacity_for, droplet_impact_case
     got = {}
     for sigma in (0.0728, 0.0):
-        cfg = drop_config(sigma)
+        cfg = replace(drop_config(sigma), csf_curvature=curvature, csf_delta_normalization=normalization)
         spec = droplet_impact_case(cfg)
         eng = BatchEngine(**capacity_for([spec], max_neighbors=64, diag_ring=8))
         cid = eng.add(spec)
         eng.step(1)
         got[sigma] = eng.read(cid)[1].cpu().numpy()
         eng.close()
-    cfg = drop_config(0.0728)
+    cfg = replace(drop_config(0.0728), csf_curvature=curvature, csf_delta_normalization=normalization)
     x, m, w = spec.x.numpy(), spec.mass.numpy(), spec.wall.numpy()
     h = cfg.h_factor * cfg.dx
     pairs = cell_linked_pairs(np.concatenate((x, w)), 2.0 * h)
     rho, _, _ = op.rhs(x, np.zeros_like(x), m, cfg, pairs=pairs, wall=w, dt=cfg.dt)
-    a_ref, st = csf.surface_tension_acceleration(x, rho, m, h, 0.0728, cfg.rho0)
+    listed = cell_linked_pairs(x, (2.0 + cfg.pair_skin_factor) * h) if curvature == "mls" else None
+    a_ref, st = csf.surface_tension_acceleration(x, rho, m, h, 0.0728, cfg.rho0, pairs=listed,
+                                                 curvature_scheme=curvature, delta_normalization=normalization)
     a_dev = (got[0.0728] - got[0.0]) / cfg.dt
     scale = np.abs(a_ref).max()
     err = np.abs(a_dev - a_ref).max(axis=1) / scale
