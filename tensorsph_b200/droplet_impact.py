@@ -406,8 +406,9 @@ def rhs(pos, vel, mass, cfg: Config, pairs=None, wall=None, dt=None, wall_vel=No
                                   "B200 particle pass")
     if cfg.surface_pressure_closure:
         raise NotImplementedError("surface_pressure_closure is not part of the B200 particle pass")
-    if cfg.surface_tension_coefficient > 0.0:
-        raise NotImplementedError("CSF surface tension is not part of the B200 particle pass")
+    if cfg.surface_tension_coefficient > 0.0 and cfg.csf_scheme != "consistent":
+        raise NotImplementedError("the neighbour-count CSF scheme (csf_scheme='legacy') is not part of "
+                                  "the B200 particle pass")
     if cfg.density_diffusion > 0.0 and cfg.density_diffusion_form not in ("molteni", "antuono"):
         raise ValueError(f"unknown density_diffusion_form {cfg.density_diffusion_form!r}; "
                          "expected one of ('molteni', 'antuono')")
@@ -509,6 +510,18 @@ def rhs(pos, vel, mass, cfg: Config, pairs=None, wall=None, dt=None, wall_vel=No
     ws = _lib.workspace(L.tsph_wcsph_workspace_bytes(ctypes.byref(prm)), dev)
     _lib.check(L.tsph_wcsph_rhs(ctypes.byref(prm), ctypes.byref(io), ws.data_ptr(), ws.numel(),
                                 _lib.stream(dev)), "tsph_wcsph_rhs")
+    if cfg.surface_tension_coefficient > 0.0 and not empty:
+        # droplet_impact.py:1210-1222: the consistent CSF over the fluid pairs
+        # of the step's list, with the configuration's options and the walls
+        fluid_pairs = pairs_dev[(pairs_dev[:, 0] < n) & (pairs_dev[:, 1] < n)]
+        if fluid_pairs.shape[0]:
+            from .csf_consistent import surface_tension_acceleration
+            a_st, _ = surface_tension_acceleration(
+                P, rho, M, fluid_pairs, h, float(cfg.surface_tension_coefficient), rho0=cfg.rho0, wall=Wp,
+                contact_angle=cfg.contact_angle, contact_angle_reach=cfg.contact_angle_reach,
+                curvature_scheme=cfg.csf_curvature, delta_normalization=cfg.csf_delta_normalization,
+                contact_angle_model=cfg.contact_angle_model)
+            acc = acc + a_st
     result = (rho.to(out_device), pressure.to(out_device), acc.to(out_device))
     if split and not empty:
         return (*result, {"reaction": reaction.to(out_device),

@@ -697,6 +697,46 @@ def contact_cases(ca, seed=400):
     return data
 
 
+def rhs_csf_cases(di):
+    """droplet_impact.rhs with CSF surface tension (droplet_impact.py:1210-1222:
+    the fluid pairs of the step's list through compute_surface_tension_force)
+    on a jittered drop above a walled pool, FP64 (default dtype float64, so
+    the wall masses are not rounded to FP32): the default options, "mls" with
+    "local_range", and contact angles with "rotate" and "young"."""
+    saved = torch.get_default_dtype()
+    torch.set_default_dtype(torch.float64)
+    try:
+        return _rhs_csf_cases(di)
+    finally:
+        torch.set_default_dtype(saved)
+
+
+def _rhs_csf_cases(di):
+    data = {}
+    dx = 0.002
+    variants = [dict(), dict(csf_curvature="mls", csf_delta_normalization="local_range"),
+                dict(contact_angle=math.pi / 3),
+                dict(contact_angle=2 * math.pi / 3, contact_angle_model="young")]
+    for k, o in enumerate(variants):
+        cfg = di.Config(dx=dx, pool_width=0.08, pool_depth=0.02, drop_radius=0.01, drop_center_y=0.035,
+                        surface_tension_coefficient=0.0728, density_diffusion=0.1, **o)
+        pos, mass = di.make_particles(cfg, "cpu")
+        wall = di.wall_lattice(cfg, "cpu").double()
+        g = torch.Generator().manual_seed(600 + k)
+        pos = pos.double() + 0.02 * dx * torch.randn(pos.shape, generator=g, dtype=torch.float64)
+        mass = mass.double()
+        vel = 0.01 * torch.randn(pos.shape, generator=g, dtype=torch.float64)
+        h = cfg.h_factor * cfg.dx
+        pairs = di.cell_linked_pairs(torch.cat((pos, wall)), 2.0 * h)
+        rho, p, acc = di.rhs(pos, vel, mass, cfg, pairs=pairs, wall=wall, dt=cfg.dt)
+        for name, t in dict(pos=pos, vel=vel, mass=mass, wall=wall, pairs=pairs, rho=rho, p=p,
+                            acc=acc).items():
+            data[f"c{k}_{name}"] = _np(t)
+        data[f"c{k}_opts"] = np.array(repr(sorted(o.items())))
+    data["count"] = np.int64(len(variants))
+    return data
+
+
 def delta_plus_cases(dp):
     """delta_plus_step on a perturbed lattice block in a walled corner (fluid,
     slip walls with normals, gravity, diffusion) and on a free block."""
@@ -857,6 +897,7 @@ def main(src, families=None):
         "checkpoint": lambda: checkpoint_case(kl),
         "contact": lambda: contact_cases(ca),
         "csf3axi": lambda: csf3axi_cases(c3, lc, ns, n3),
+        "rhs_csf": lambda: rhs_csf_cases(di),
     }
     for name in families or makers:
         np.savez_compressed(OUT / f"{name}.npz", **makers[name](), **meta)

@@ -157,7 +157,7 @@ def test_rhs_pairs_none_and_empty(gpu, default_dtype):
     assert torch.equal(acc[:, 0].cpu(), torch.zeros(2, dtype=torch.float64))
     assert torch.allclose(acc[:, 1].cpu(), torch.full((2,), -9.81, dtype=torch.float64))
     with pytest.raises(NotImplementedError):
-        rhs(pos, vel, mass, _cfg(surface_tension_coefficient=0.07))
+        rhs(pos, vel, mass, _cfg(surface_tension_coefficient=0.07, csf_scheme="legacy"))
 
 
 def test_rhs3d_matches_reference(gpu, golden):
@@ -176,3 +176,41 @@ def test_rhs3d_matches_reference(gpu, golden):
             tol = tr if name in ("rho", "p") else tf
             scale = bulk(cfg) if name == "p" else None
             assert rel_err(got.cpu(), g[f"c{k}_{name}"], scale) < tol, (k, name)
+
+
+def test_rhs_with_csf_matches_reference(golden, gpu):
+    """droplet_impact.rhs with CSF surface tension (the fluid pairs of the
+    step's list through the 2-D CSF drop-in, droplet_impact.py:1210-1222)
+    against the reference's own rhs (tests/golden/rhs_csf.npz, default dtype
+    float64): density within 1e-12 of rho0 and the acceleration within 1e-8 of
+    the largest surface-tension term, for the default options, "mls" +
+    "local_range", and contact angles "rotate" and "young"."""
+    import ast
+    from dataclasses import replace
+
+    from oracle import csf
+    from tensorsph_b200.droplet_impact import Config, rhs
+    g = golden("rhs_csf")
+    saved = torch.get_default_dtype()
+    torch.set_default_dtype(torch.float64)
+    try:
+        for k in range(int(g["count"])):
+            o = dict(ast.literal_eval(str(g[f"c{k}_opts"])))
+            cfg = replace(Config(dx=0.002, pool_width=0.08, pool_depth=0.02, drop_radius=0.01,
+                                 drop_center_y=0.035, surface_tension_coefficient=0.0728,
+                                 density_diffusion=0.1), **o)
+            pos, vel, mass, wall, pairs = (g[f"c{k}_{n}"] for n in ("pos", "vel", "mass", "wall", "pairs"))
+            dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+            rho, _, acc = rhs(dev(pos), dev(vel), dev(mass), cfg, pairs=dev(pairs), wall=dev(wall), dt=cfg.dt)
+            assert np.abs(rho.cpu().numpy() - g[f"c{k}_rho"]).max() <= 1e-12 * cfg.rho0, k
+            n = pos.shape[0]
+            fluid = pairs[(pairs[:, 0] < n) & (pairs[:, 1] < n)]
+            h = cfg.h_factor * cfg.dx
+            a_st, _ = csf.surface_tension_acceleration(
+                pos, g[f"c{k}_rho"], mass, h, 0.0728, cfg.rho0, pairs=fluid, curvature_scheme=cfg.csf_curvature,
+                delta_normalization=cfg.csf_delta_normalization, wall=wall, contact_angle=cfg.contact_angle,
+                contact_angle_model=cfg.contact_angle_model)
+            err = np.abs(acc.cpu().numpy() - g[f"c{k}_acc"]).max()
+            assert err <= 1e-8 * np.abs(a_st).max(), (k, err / np.abs(a_st).max())
+    finally:
+        torch.set_default_dtype(saved)

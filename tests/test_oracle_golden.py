@@ -377,3 +377,33 @@ def test_csf3_axisym_oracle_matches_reference(golden):
         acc = csf3.surface_tension_acceleration3(st, g[f"c{k}_rho"], 0.0728)
         ra = g[f"c{k}_acc"]
         assert np.abs(acc - ra).max() <= tol * np.abs(ra).max(), k
+
+
+def test_rhs_with_csf_oracle_matches_reference(golden):
+    """The droplet rhs with CSF surface tension (droplet_impact.py:1210-1222)
+    as the oracle's rhs plus its CSF over the fluid pairs, against the
+    reference's own rhs (tests/golden/rhs_csf.npz): default options, "mls" +
+    "local_range", contact angles "rotate" and "young"."""
+    import ast
+    from dataclasses import replace
+    from oracle import csf
+    from oracle import pairpass as op
+    from tensorsph_b200.droplet_impact import Config
+    g = golden("rhs_csf")
+    for k in range(int(g["count"])):
+        o = dict(ast.literal_eval(str(g[f"c{k}_opts"])))
+        cfg = replace(Config(dx=0.002, pool_width=0.08, pool_depth=0.02, drop_radius=0.01, drop_center_y=0.035,
+                             surface_tension_coefficient=0.0728, density_diffusion=0.1), **o)
+        pos, vel, mass, wall, pairs = (g[f"c{k}_{n}"] for n in ("pos", "vel", "mass", "wall", "pairs"))
+        h = cfg.h_factor * cfg.dx
+        plain = replace(cfg, surface_tension_coefficient=0.0)
+        rho, p, acc = op.rhs(pos, vel, mass, plain, pairs=pairs, wall=wall, dt=cfg.dt)
+        n = pos.shape[0]
+        fluid = pairs[(pairs[:, 0] < n) & (pairs[:, 1] < n)]
+        a_st, _ = csf.surface_tension_acceleration(
+            pos, rho, mass, h, cfg.surface_tension_coefficient, cfg.rho0, pairs=fluid,
+            curvature_scheme=cfg.csf_curvature, delta_normalization=cfg.csf_delta_normalization, wall=wall,
+            contact_angle=cfg.contact_angle, contact_angle_model=cfg.contact_angle_model)
+        assert np.abs(rho - g[f"c{k}_rho"]).max() <= 1e-12 * cfg.rho0
+        ref = g[f"c{k}_acc"]
+        assert np.abs(acc + a_st - ref).max() <= 1e-9 * np.abs(a_st).max(), k
