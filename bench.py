@@ -90,15 +90,20 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic_per_fluid_particle():
-    """DRAM bytes per fluid particle of one force launch, from the committed ncu summary."""
+def _force_profile_figure(key: str):
+    """A figure of the committed ncu summary of the force pass (``key: value`` line)."""
     path = ROOT / "profiles" / "engine_force_dam_break_3d.md"
     if not path.exists():
         return None
     for line in path.read_text().splitlines():
-        if line.startswith("traffic_bytes_per_fluid_particle:"):
+        if line.startswith(key + ":"):
             return float(line.split(":", 1)[1].strip())
     return None
+
+
+def ncu_traffic_per_fluid_particle():
+    """DRAM bytes per fluid particle of one force launch, from the committed ncu summary."""
+    return _force_profile_figure("traffic_bytes_per_fluid_particle")
 
 
 class ClockSampler:
@@ -641,7 +646,10 @@ def main():
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                          "algorithmic_bytes_per_launch": ALGO_BYTES_FORCE * nf,
                          "launch_ms": stage["force"],
-                         "step_hbm_frac": ALGO_BYTES_STEP * nf / (ms_step / 1e3) / 1e9 / peak},
+                         "step_hbm_frac": ALGO_BYTES_STEP * nf / (ms_step / 1e3) / 1e9 / peak,
+                         # what bounds the pass: the L1 data pipe and issue, not HBM
+                         # (ncu, l1tex throughput of the same kernel on the 2x coarser rung)
+                         "l1tex_throughput_frac_ncu": _force_profile_figure("l1tex_throughput_frac")},
             "stage_ms": stage,
             "clocks": clocks,
             "gpu_launches": launches,
