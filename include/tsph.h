@@ -537,6 +537,13 @@ typedef struct {
   int64_t csf_curvature;               /* with surface_tension: 0 "fit_quadratic",   */
                                        /* 1 "mls" (div n), 2 "fit_circle"            */
   int64_t csf_delta_normalization;     /* 0 "legacy" (2 |grad c|), 1 "local_range"   */
+  int64_t csf_contact_model;           /* contact angle at the walls: 0 none,        */
+                                       /* 1 "rotate", 2 "young", 3 "brackbill"       */
+  double csf_contact_angle;            /* radians, measured inside the liquid        */
+  double csf_contact_reach;            /* rotate: boundary thickness in h, <= 2      */
+  double csf_wall_area;                /* young / brackbill: the wall area A of the  */
+                                       /* wall delta (squared median wall spacing)   */
+  double csf_traction_calibration;     /* young / brackbill: the traction's C        */
 } tsph_case_params;
 
 typedef struct tsph_engine tsph_engine; /* opaque host handle */

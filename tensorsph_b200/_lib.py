@@ -158,7 +158,9 @@ class CaseParams(ctypes.Structure):
                 ("periodic_box", c_double), ("tvc_every", c_int64), ("tvc_alpha", c_double),
                 ("tvc_scope_tol", c_double), ("tvc_max_shift", c_double),
                 ("first_step", c_int64), ("tvc_slope", c_double), ("tvc_wall_volume", c_double),
-                ("tvc_bulk_c", c_double), ("csf_curvature", c_int64), ("csf_delta_normalization", c_int64)]
+                ("tvc_bulk_c", c_double), ("csf_curvature", c_int64), ("csf_delta_normalization", c_int64),
+                ("csf_contact_model", c_int64), ("csf_contact_angle", c_double), ("csf_contact_reach", c_double),
+                ("csf_wall_area", c_double), ("csf_traction_calibration", c_double)]
 
 
 _SIGNATURES = {

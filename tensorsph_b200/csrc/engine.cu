@@ -66,6 +66,11 @@ struct CaseDev {
   int csf;                 // CSF surface tension on (2-D)
   int csf_fit;             // curvature fit: 0 none ("mls"), 1 quadratic, 2 circle
   int csf_range;           // delta_s = |grad c| / local colour range ("local_range")
+  int csf_contact;         // contact angle: 0 none, 1 rotate, 2 young, 3 brackbill
+  double ca_cos, ca_sin;   // of the angle (the rotate boundary's target direction)
+  double ca_reach_h;       // rotate: the boundary thickness reach h
+  double ca_area_factor;   // traction: the wall delta's A / (1/2)
+  double ca_c_sigma;       // traction: C sigma
   int periodic;            // triply periodic cube of edge pbox (3-D, no walls)
   double pbox;             // the cube edge: n cells x the FP32 cell edge, exactly
   int stencil_cells;       // cells each side covering the 4h fit stencil
@@ -881,6 +886,30 @@ __device__ __forceinline__ double dshape_d(double q) {
 struct KD {
   double w, gs;
 };
+
+// The nearest wall particle of fluid row a among its list entries (every wall
+// particle within 2h + skin, which holds the nearest one whenever it is
+// within 2h): squared distance and the direction from it to a; false when the
+// row holds no wall particle.  Equal distances keep the first in row order.
+__device__ __forceinline__ bool row_nearest_wall(const Dev& e, int a, double ax, double ay, double& d2, double& nx,
+                                                 double& ny) {
+  const int n = e.cnt[a];
+  const uint32_t* row = e.nbr + a;
+  bool any = false;
+  for (int k = 0; k < n; ++k) {
+    const uint32_t b = ld_entry(row + static_cast<int64_t>(k) * e.rows) >> kCodeBits;
+    if (b < static_cast<uint32_t>(e.NF) || b >= static_cast<uint32_t>(e.null_row)) continue;
+    const double2 pw = ld_xy(e.pos, static_cast<int>(b));
+    const double dx = ax - pw.x, dy = ay - pw.y, r2 = dx * dx + dy * dy;
+    if (!any || r2 < d2) {
+      d2 = r2;
+      nx = dx;
+      ny = dy;
+      any = true;
+    }
+  }
+  return any;
+}
 __device__ __forceinline__ KD kernel_d(double dx, double dy, const CaseDev& C) {
   const double r = sqrt(dx * dx + dy * dy);
   const double q = r * C.inv_h_d;
@@ -1090,8 +1119,34 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_grad(const __grid_constant__ 
       const double4 B = e.csB[a];
       csf_matrix(e, c, A, B.w, p, q, r);
       const double det = p * r - q * q;
-      const double g0 = (r * gx - q * gy) / det, g1 = (p * gy - q * gx) / det;
+      double g0 = (r * gx - q * gy) / det, g1 = (p * gy - q * gx) / det;
       mag = sqrt(g0 * g0 + g1 * g1);
+      if (C.csf_contact == 1 && mag > 0.0) {
+        // the contact-angle boundary (csf_consistent.py:483-560): within reach h
+        // of the nearest wall particle the normal turns toward cos(theta) n_w +
+        // sin(theta) t, t the wall tangent on the interface's side; |grad c| kept
+        double d2, wx, wy;
+        if (row_nearest_wall(e, a, pa.x, pa.y, d2, wx, wy)) {
+          const double d = sqrt(d2);
+          const double wm = sqrt(wx * wx + wy * wy);
+          if (d < C.ca_reach_h && wm >= 1e-12) {
+            wx /= wm;
+            wy /= wm;
+            const double nx = -g0 / mag, ny = -g1 / mag;
+            const double dot = nx * wx + ny * wy;
+            const double tx = nx - dot * wx, ty = ny - dot * wy;
+            const double sgn = (tx * -wy + ty * wx) < 0.0 ? -1.0 : 1.0;
+            const double qx = C.ca_cos * wx + C.ca_sin * (-wy * sgn), qy = C.ca_cos * wy + C.ca_sin * (wx * sgn);
+            double blend = 1.0 - d / C.ca_reach_h;
+            blend = blend < 0.0 ? 0.0 : (blend > 1.0 ? 1.0 : blend);
+            double mx = (1.0 - blend) * nx + blend * qx, my = (1.0 - blend) * ny + blend * qy;
+            const double mr = fmax(sqrt(mx * mx + my * my), 1e-30);
+            g0 = -mag * (mx / mr);
+            g1 = -mag * (my / mr);
+            mag = sqrt(g0 * g0 + g1 * g1);
+          }
+        }
+      }
       e.csB[a] = make_double4(g0, g1, mag, B.w);
       e.csN0[a] = mag > 1e-12 ? make_double2(-g0 / mag, -g1 / mag) : make_double2(0.0, 0.0);
     } else {
@@ -1389,8 +1444,55 @@ __global__ void k_csf_final(const __grid_constant__ Dev e) {
     const double gmax = __longlong_as_double(static_cast<long long>(t.csf_gmax));
     const double ds = mag <= 1e-3 * gmax ? 0.0 : (C.csf_range ? e.csD[a] : 2.0 * mag);
     const double2 n = e.csN[a];
-    const double f = -C.sigma_st * kappa * ds / static_cast<double>(e.rho[a]);
-    e.st[a] = make_float2(static_cast<float>(f * n.x), static_cast<float>(f * n.y));
+    const double f = -C.sigma_st * kappa * ds;
+    double fx = f * n.x, fy = f * n.y;
+    if (C.csf_contact >= 2 && ds != 0.0) {
+      // the wall-adhesion traction C sigma delta_s w d (contact_angle_isph.py:148-213)
+      const double4 pa = ld4(e.pos, a);
+      double d2, wx, wy;
+      if (row_nearest_wall(e, a, pa.x, pa.y, d2, wx, wy)) {
+        double sw = 0.0;  // sum of W over the wall particles (all within 2h are in the row)
+        const int cnt = e.cnt[a];
+        for (int k = 0; k < cnt; ++k) {
+          const uint32_t b = ld_entry(e.nbr + a + static_cast<int64_t>(k) * e.rows) >> kCodeBits;
+          if (b < static_cast<uint32_t>(e.NF) || b >= static_cast<uint32_t>(e.null_row)) continue;
+          const double2 pw = ld_xy(e.pos, static_cast<int>(b));
+          sw += kernel_d(pa.x - pw.x, pa.y - pw.y, C).w;
+        }
+        double w = sw * C.ca_area_factor / 0.4734;
+        w = w < 0.0 ? 0.0 : (w > 1.0 ? 1.0 : w);
+        const double wm = sqrt(wx * wx + wy * wy);
+        if (w > 0.0 && wm >= 1e-12) {
+          wx /= wm;
+          wy /= wm;
+          double dx, dy;
+          if (C.csf_contact == 2) {
+            const double dot = n.x * wx + n.y * wy;
+            const double tx = n.x - dot * wx, ty = n.y - dot * wy;
+            const double tm = sqrt(tx * tx + ty * ty);
+            if (tm < 1e-9) {
+              const double ux = 1.0 - wx * wx, uy = -wx * wy;
+              const double um = fmax(sqrt(ux * ux + uy * uy), 1e-30);
+              dx = ux / um;
+              dy = uy / um;
+            } else {
+              dx = tx / tm;
+              dy = ty / tm;
+            }
+            dx *= C.ca_cos;
+            dy *= C.ca_cos;
+          } else {
+            dx = wx - C.ca_cos * n.x;
+            dy = wy - C.ca_cos * n.y;
+          }
+          const double coef = C.ca_c_sigma * ds * w;
+          fx += coef * dx;
+          fy += coef * dy;
+        }
+      }
+    }
+    const double rho = static_cast<double>(e.rho[a]);
+    e.st[a] = make_float2(static_cast<float>(fx / rho), static_cast<float>(fy / rho));
   }
 }
 
@@ -2417,6 +2519,12 @@ CaseDev make_case_dev(const tsph_case_params& p, int64_t* ncells) {
   c.csf = (p.surface_tension > 0.0 && p.dim == 2) ? 1 : 0;
   c.csf_fit = p.csf_curvature == 1 ? 0 : (p.csf_curvature == 2 ? 2 : 1);
   c.csf_range = p.csf_delta_normalization == 1 ? 1 : 0;
+  c.csf_contact = c.csf ? static_cast<int>(p.csf_contact_model) : 0;
+  c.ca_cos = std::cos(p.csf_contact_angle);
+  c.ca_sin = std::sin(p.csf_contact_angle);
+  c.ca_reach_h = p.csf_contact_reach * p.h;
+  c.ca_area_factor = p.csf_wall_area / 0.5;
+  c.ca_c_sigma = p.csf_traction_calibration * p.surface_tension;
   c.sigma_st = p.surface_tension;
   c.h_d = p.h;
   c.inv_h_d = 1.0 / p.h;
@@ -2441,7 +2549,10 @@ bool case_params_ok(const tsph_case_params* p) {
       p->n_obstacle > p->n_wall || p->shift_every < 0 || p->first_step < 0)
     return false;
   if (p->csf_curvature < 0 || p->csf_curvature > 2 || p->csf_delta_normalization < 0 ||
-      p->csf_delta_normalization > 1)
+      p->csf_delta_normalization > 1 || p->csf_contact_model < 0 || p->csf_contact_model > 3 ||
+      !std::isfinite(p->csf_contact_angle) ||
+      (p->csf_contact_model == 1 && !(p->csf_contact_reach > 0.0 && p->csf_contact_reach <= 2.0)) ||
+      (p->csf_contact_model >= 2 && !(p->csf_wall_area > 0.0 && std::isfinite(p->csf_traction_calibration))))
     return false;
   if (!(p->h > 0) || !(p->dt > 0) || !(p->skin >= 0) || !(p->rho0 > 0) || !(p->gamma > 0) ||
       !(p->sound_speed > 0))

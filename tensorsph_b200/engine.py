@@ -274,6 +274,18 @@ def dam_break_2d_case(cfg, *, shift_every: int = 0, velocity=None, label: str = 
     return CaseSpec(p, x, v, mass.double().contiguous(), wall, label or "dam_break_2d")
 
 
+def _wall_spacing(wall: torch.Tensor) -> float:
+    """Lower median of the wall particles' nearest-neighbour distances (host,
+    once per case)."""
+    if wall.shape[0] < 2:
+        return 1.0
+    from scipy.spatial import cKDTree
+    w = wall.double().numpy()
+    d, _ = cKDTree(w).query(w, k=2)
+    nn = sorted(d[:, 1].tolist())
+    return float(nn[(len(nn) - 1) // 2])
+
+
 def droplet_impact_case(cfg, *, drop_speed: float = 0.0, label: str = "") -> CaseSpec:
     """The 2-D droplet impact of ``tensorsph.droplet_impact`` (pool plus
     circular drop from ``make_particles``, walls from ``wall_lattice`` up to
@@ -287,13 +299,19 @@ def droplet_impact_case(cfg, *, drop_speed: float = 0.0, label: str = "") -> Cas
     validate_config(cfg)
     curvature = {"fit_quadratic": 0, "mls": 1, "fit_circle": 2}
     normalization = {"legacy": 0, "local_range": 1}
+    contact = {"rotate": 1, "young": 2, "brackbill": 3}
     if cfg.surface_tension_coefficient > 0.0:
-        if cfg.csf_scheme != "consistent" or cfg.contact_angle is not None:
-            raise NotImplementedError("the device engine implements the consistent CSF scheme "
-                                      "without a contact angle")
+        if cfg.csf_scheme != "consistent":
+            raise NotImplementedError("the device engine implements the consistent CSF scheme")
         if cfg.csf_curvature not in curvature or cfg.csf_delta_normalization not in normalization:
             raise ValueError(f"unknown csf_curvature {cfg.csf_curvature!r} or csf_delta_normalization "
                              f"{cfg.csf_delta_normalization!r}")
+        if cfg.contact_angle is not None:
+            if cfg.contact_angle_model not in contact:
+                raise ValueError(f"unknown contact_angle_model {cfg.contact_angle_model!r}")
+            if cfg.contact_angle_model == "rotate" and not 0.0 < cfg.contact_angle_reach <= 2.0:
+                raise NotImplementedError("the device engine's contact-angle boundary reaches at most 2 h "
+                                          "(the wall particles of the list rows)")
     if cfg.density_renormalization or cfg.boundary_consistent_density:
         raise NotImplementedError("density_renormalization and boundary_consistent_density are "
                                   "not part of the device engine")
@@ -314,6 +332,15 @@ def droplet_impact_case(cfg, *, drop_speed: float = 0.0, label: str = "") -> Cas
     if p.surface_tension > 0.0:
         p.csf_curvature = curvature[cfg.csf_curvature]
         p.csf_delta_normalization = normalization[cfg.csf_delta_normalization]
+        if cfg.contact_angle is not None and wall.shape[0]:
+            p.csf_contact_model = contact[cfg.contact_angle_model]
+            p.csf_contact_angle = float(cfg.contact_angle)
+            p.csf_contact_reach = float(cfg.contact_angle_reach)
+            if cfg.contact_angle_model != "rotate":
+                # contact_angle_isph.py:75-81 and :104-107: A = (median nearest-
+                # neighbour wall spacing)^2, the traction calibration 0.9611
+                p.csf_wall_area = _wall_spacing(wall) ** 2
+                p.csf_traction_calibration = 0.9611
     return CaseSpec(p, x, v, mass.double().contiguous(), wall, label or "droplet_impact")
 
 

@@ -84,3 +84,57 @@ def test_csf_batch_equals_alone(gpu):
         e2.close()
         for u, v in zip(got[i], ref):
             assert torch.equal(u, v)
+
+
+@pytest.mark.parametrize("model,theta", [("rotate", np.pi / 3), ("young", 2 * np.pi / 3), ("brackbill", np.pi / 3)])
+def test_engine_csf_contact_angle_matches_oracle(model, theta, gpu):
+    """Contact angles in the engine's CSF (the droplet case's contact_angle,
+    contact_angle_model) against the oracle on a drop above a walled pool
+    (positions jittered by 0.02 dx so that no fluid particle is equidistant
+    from two wall particles): the surface-tension acceleration within 1e-5 of
+    max |a|, and for the tractions the traction alone (with the contact angle
+    minus without) within four FP32 steps of the total acceleration the
+    engine records (plus 1e-5 of the traction's largest value)."""
+    from dataclasses import replace
+
+    from tensorsph_b200.engine import BatchEngine, capacity_for, droplet_impact_case
+    rng = np.random.default_rng(21)
+    base = droplet_impact_case(drop_config(0.0728))
+    x = base.x + torch.from_numpy(rng.uniform(-0.02, 0.02, tuple(base.x.shape)) * 0.002)
+
+    def run(cfg):
+        spec = droplet_impact_case(cfg)
+        spec.x = x.clone()
+        eng = BatchEngine(**capacity_for([spec], max_neighbors=64, diag_ring=8))
+        cid = eng.add(spec)
+        eng.step(1)
+        v = eng.read(cid)[1].cpu().numpy()
+        eng.close()
+        return v
+
+    with_ca = replace(drop_config(0.0728), contact_angle=float(theta), contact_angle_model=model)
+    got = run(with_ca)
+    bare = run(drop_config(0.0728))
+    zero = run(drop_config(0.0))
+    cfg = with_ca
+    xn, m, w = x.numpy(), base.mass.numpy(), base.wall.numpy()
+    h = cfg.h_factor * cfg.dx
+    pairs = cell_linked_pairs(np.concatenate((xn, w)), 2.0 * h)
+    rho, _, _ = op.rhs(xn, np.zeros_like(xn), m, cfg, pairs=pairs, wall=w, dt=cfg.dt)
+    a_ref, _ = csf.surface_tension_acceleration(xn, rho, m, h, 0.0728, cfg.rho0, wall=w, contact_angle=float(theta),
+                                                contact_angle_model=model)
+    a_bare, _ = csf.surface_tension_acceleration(xn, rho, m, h, 0.0728, cfg.rho0)
+    a_dev = (got - zero) / cfg.dt
+    scale = np.abs(a_ref).max()
+    assert np.abs(a_ref - a_bare).max() > 1e-4 * scale          # the contact angle acts
+    err = np.abs(a_dev - a_ref).max() / scale
+    assert err < 1e-5, err
+    if model != "rotate":
+        # the engine stores the step's total acceleration in FP32 (~10 m/s^2
+        # of gravity and pressure); the traction (~1e-3 of the CSF term) is
+        # resolved to a few FP32 steps of that total
+        t_ref = a_ref - a_bare
+        t_dev = (got - bare) / cfg.dt
+        ulp = float(np.spacing(np.float32(np.abs(got / cfg.dt).max())))
+        terr = np.abs(t_dev - t_ref).max()
+        assert terr <= 4 * ulp + 1e-5 * np.abs(t_ref).max(), (terr, ulp, np.abs(t_ref).max())
