@@ -149,6 +149,9 @@ struct Dev {
   unsigned int* csf_hist;  // [n_slots][256] median-select histograms
   int has_csf, maxfit;
   int has_tvc, tvc_late;  // tvc_late: the correction runs after the second list pass
+  int csf_kinds;          // CSF options present in the batch: fits 1 quadratic, 2 circle,
+                          // 16 quadratic + local_range, 32 circle + local_range; 4 local_range,
+                          // 8 wall traction (only those passes are launched)
   uint32_t* nbr4;    // CSF fit rows (fluid neighbours within 4h + skin), k-major over NF
   int32_t* cnt4;
   uint32_t* nbr;
@@ -1300,6 +1303,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_div(const __grid_constant__ D
 // Q7: weighted fit v = c + b u + a u^2 in the frame (t, n) of row a over the
 // fluid particles within 4h (cells within stencil_cells of the home cell),
 // weights w_b = |grad c|_b / max |grad c| (= delta_s / max delta_s).
+// kFit: 1 the quadratic fit, 2 the circle fit; kRange: local_range weights.
+// Each instance serves the cases of its kind (separate instances keep the
+// default one's registers).
+template <int kFit, bool kRange>
 __global__ void __launch_bounds__(kMaxBlock) k_csf_fit(const __grid_constant__ Dev e) {
   __shared__ double red[kMaxBlock / 32];
   const int a0 = blockIdx.x * blockDim.x;
@@ -1312,11 +1319,9 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_fit(const __grid_constant__ D
   if (a < e.nf) {
     c = e.cid[a];
     const CaseDev& C = e.cases[c];
-    if (C.csf && C.csf_fit == 0) {
-      detabs = 0.0;  // "mls": no fit
-    } else if (C.csf) {
+    if (C.csf && C.csf_fit == kFit && (C.csf_range != 0) == kRange) {
       // the fit weights: delta_s_b / max delta_s (legacy: |grad c| / max |grad c|)
-      const bool rng = C.csf_range != 0;
+      constexpr bool rng = kRange;
       const double gmax = fmax(__longlong_as_double(static_cast<long long>(rng ? e.ctl[c].csf_dmax : e.ctl[c].csf_gmax)),
                                1e-30);
       const double inv_g = 1.0 / gmax;
@@ -1351,7 +1356,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_fit(const __grid_constant__ D
           double w = mg[j] * inv_g;
           w = w < 0.0 ? 0.0 : (w > 1.0 ? 1.0 : w);
           w = (k + j < n4 && ddx * ddx + ddy * ddy <= st2) ? w : 0.0;
-          if (C.csf_fit == 2) {
+          if (kFit == 2) {
             // circle moments of the offset (x, y) = x_b - x_a, f = x^2 + y^2
             const double x = -ddx, y = -ddy, f = x * x + y * y;
             s0 += w;
@@ -1380,7 +1385,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_fit(const __grid_constant__ D
       double wa = (rng ? e.csD[a] : e.csB[a].z) * inv_g;
       wa = wa < 0.0 ? 0.0 : (wa > 1.0 ? 1.0 : wa);
       s0 += wa;
-      if (C.csf_fit == 2) {
+      if (kFit == 2) {
         // Pratt: x^2 + y^2 + D x + E y + F = 0, [[s3 s4 s1] [s4 s5 s2] [s1 s2 s0]]
         // (D, E, F) = -(s6, s7, s8) by Cramer's rule (csf_curvature.py:179-213)
         const double det = s3 * (s5 * s0 - s2 * s2) - s4 * (s4 * s0 - s2 * s1) + s1 * (s4 * s2 - s5 * s1);
@@ -1430,6 +1435,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_fit(const __grid_constant__ D
 
 // Q8: kappa (fit where active and regular, else kappa_mls), delta_s = 2|grad c|
 // or the local_range value, with the flat mask, a = -sigma kappa delta_s n / rho
+template <bool kTraction>
 __global__ void k_csf_final(const __grid_constant__ Dev e) {
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
     const int c = e.cid[a];
@@ -1446,7 +1452,7 @@ __global__ void k_csf_final(const __grid_constant__ Dev e) {
     const double2 n = e.csN[a];
     const double f = -C.sigma_st * kappa * ds;
     double fx = f * n.x, fy = f * n.y;
-    if (C.csf_contact >= 2 && ds != 0.0) {
+    if (kTraction && C.csf_contact >= 2 && ds != 0.0) {
       // the wall-adhesion traction C sigma delta_s w d (contact_angle_isph.py:148-213)
       const double4 pa = ld4(e.pos, a);
       double d2, wx, wy;
@@ -2272,9 +2278,13 @@ void batch_changed(tsph_engine* E) {
   d.shift_slot = second_pass(E) ? E->order[0].slot : 0;
   d.has_csf = 0;
   d.has_tvc = 0;
+  d.csf_kinds = 0;
   d.tvc_late = second_pass(E) && E->order[0].dev.tvc_bulk ? 1 : 0;
   for (const CaseHost& c : E->order) {
     d.has_csf |= c.dev.csf;
+    if (c.dev.csf)
+      d.csf_kinds |= (c.dev.csf_fit ? (c.dev.csf_fit == 1 ? 1 : 2) << (c.dev.csf_range ? 4 : 0) : 0) |
+                     (c.dev.csf_range ? 4 : 0) | (c.dev.csf_contact >= 2 ? 8 : 0);
     d.has_tvc |= c.dev.tvc_every > 0 ? 1 : 0;
   }
   if (E->order.size() == 1) {
@@ -2400,12 +2410,18 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr, b
       k_csf_pick<<<gp, 128, 0, s>>>(d, shift);
     }
     k_csf_grad<<<gf, B, 0, s>>>(d);
-    k_csf_range<<<gf, B, 0, s>>>(d);
+    if (d.csf_kinds & 4) k_csf_range<<<gf, B, 0, s>>>(d);
     k_csf_smooth<false><<<g, B, 0, s>>>(d);
     k_csf_smooth<true><<<g, B, 0, s>>>(d);
     k_csf_div<<<g, B, 0, s>>>(d);
-    k_csf_fit<<<gf, B, 0, s>>>(d);
-    k_csf_final<<<g, B, 0, s>>>(d);
+    if (d.csf_kinds & 1) k_csf_fit<1, false><<<gf, B, 0, s>>>(d);
+    if (d.csf_kinds & 16) k_csf_fit<1, true><<<gf, B, 0, s>>>(d);
+    if (d.csf_kinds & 2) k_csf_fit<2, false><<<gf, B, 0, s>>>(d);
+    if (d.csf_kinds & 32) k_csf_fit<2, true><<<gf, B, 0, s>>>(d);
+    if (d.csf_kinds & 8)
+      k_csf_final<true><<<g, B, 0, s>>>(d);
+    else
+      k_csf_final<false><<<g, B, 0, s>>>(d);
     TSPH_LAUNCH_CHECK();
   }
   mark();  // walls + surface tension
