@@ -1,0 +1,89 @@
+"""Host side of the engine's case builders (no GPU): how the droplet case's
+CSF options, contact angles and the dam breaks' transport-velocity
+correction options become case parameters, and what they refuse."""
+import math
+from dataclasses import replace
+
+import numpy as np
+import pytest
+import torch
+
+
+def _drop(**kw):
+    from tensorsph_b200.droplet_impact import Config
+    dx = 0.002
+    h = 1.3 * dx
+    return replace(Config(dx=dx, pool_width=0.08, pool_depth=0.02, drop_radius=0.01, drop_center_y=0.035,
+                          sound_speed=20.0, viscosity=1e-6, dt=0.25 * h / 20.0, max_courant=0.25,
+                          surface_tension_coefficient=0.0728), **kw)
+
+
+def test_wall_spacing_matches_oracle():
+    from oracle.contact_angle import wall_spacing
+    from tensorsph_b200.engine import _wall_spacing
+    rng = np.random.default_rng(4)
+    for n in (2, 3, 57, 400):
+        w = rng.random((n, 2))
+        assert _wall_spacing(torch.from_numpy(w)) == wall_spacing(w)
+    assert _wall_spacing(torch.zeros((1, 2), dtype=torch.float64)) == 1.0
+
+
+def test_droplet_csf_options_become_case_parameters():
+    from tensorsph_b200.engine import _wall_spacing, droplet_impact_case
+    p = droplet_impact_case(_drop()).params
+    assert (p.csf_curvature, p.csf_delta_normalization, p.csf_contact_model) == (0, 0, 0)
+    p = droplet_impact_case(_drop(csf_curvature="mls", csf_delta_normalization="local_range")).params
+    assert (p.csf_curvature, p.csf_delta_normalization) == (1, 1)
+    assert droplet_impact_case(_drop(csf_curvature="fit_circle")).params.csf_curvature == 2
+    spec = droplet_impact_case(_drop(contact_angle=1.0, contact_angle_reach=1.5))
+    assert (spec.params.csf_contact_model, spec.params.csf_contact_angle, spec.params.csf_contact_reach) == (1, 1.0, 1.5)
+    assert spec.params.csf_wall_area == 0.0
+    spec = droplet_impact_case(_drop(contact_angle=2.0, contact_angle_model="young"))
+    assert spec.params.csf_contact_model == 2
+    assert spec.params.csf_wall_area == pytest.approx(_wall_spacing(spec.wall) ** 2, rel=0, abs=0)
+    assert spec.params.csf_traction_calibration == 0.9611
+    assert droplet_impact_case(_drop(contact_angle=2.0, contact_angle_model="brackbill")).params.csf_contact_model == 3
+    # without surface tension the options are not carried
+    p = droplet_impact_case(_drop(surface_tension_coefficient=0.0, contact_angle=1.0)).params
+    assert (p.csf_contact_model, p.surface_tension) == (0, 0.0)
+
+
+def test_droplet_csf_refusals():
+    from tensorsph_b200.engine import droplet_impact_case
+    with pytest.raises(NotImplementedError):
+        droplet_impact_case(_drop(csf_scheme="legacy"))
+    with pytest.raises(NotImplementedError):
+        droplet_impact_case(_drop(contact_angle=1.0, contact_angle_reach=2.5))
+    with pytest.raises(ValueError):
+        droplet_impact_case(_drop(contact_angle=1.0, contact_angle_model="hoffman"))
+    with pytest.raises(ValueError):
+        droplet_impact_case(_drop(csf_curvature="fit_ellipse"))
+
+
+def _dam2d(**kw):
+    from tensorsph_b200.dam_break import DamBreakConfig
+    dx = 0.02
+    c0 = 10.0 * math.sqrt(2.0 * 9.81 * 0.4)
+    return replace(DamBreakConfig(dx=dx, column_width=0.2, column_height=0.4, pool_width=0.6, tank_height=0.6,
+                                  sound_speed=c0, dt=0.25 * 1.3 * dx / c0, max_courant=0.25, steps=10), **kw)
+
+
+def test_dam_break_2d_tvc_options_become_case_parameters():
+    from tensorsph_b200.engine import dam_break_2d_case
+    h = 1.3 * 0.02
+    p = dam_break_2d_case(_dam2d(tvc_every=2)).params
+    assert (p.tvc_every, p.tvc_alpha, p.tvc_scope_tol, p.tvc_max_shift, p.tvc_slope, p.tvc_bulk_c) == \
+        (2, 0.05, -1.0, -1.0, -1.0, 0.0)
+    assert p.tvc_wall_volume == pytest.approx(0.02 ** 2)
+    p = dam_break_2d_case(_dam2d(tvc_every=1, tvc_scope="bulk_g", tvc_bulk_g=0.03, tvc_limiter="truncated_linear",
+                                 tvc_limiter_slope=7.0, tvc_max_shift=0.1, tvc_alpha=0.2)).params
+    assert (p.tvc_scope_tol, p.tvc_slope, p.tvc_alpha) == (0.03, 7.0, 0.2)
+    assert p.tvc_max_shift == pytest.approx(0.1 * h)
+    p = dam_break_2d_case(_dam2d(tvc_every=1, tvc_scope="bulk", tvc_bulk_c=0.9)).params
+    assert (p.tvc_bulk_c, p.tvc_scope_tol) == (0.9, -1.0)
+    with pytest.raises(ValueError):
+        dam_break_2d_case(_dam2d(tvc_every=1, tvc_scope="bulk", tvc_bulk_c=0.0))
+    with pytest.raises(ValueError):
+        dam_break_2d_case(_dam2d(tvc_every=1, tvc_limiter="cubic"))
+    with pytest.raises(NotImplementedError):
+        dam_break_2d_case(_dam2d(tvc_every=1), shift_every=1)
