@@ -32,7 +32,8 @@ __all__ = [
     "calibrated_particle_mass", "lattice_mass_unit", "cell_centres", "pool_lattice",
     "make_particles", "wall_lattice", "wall_mass", "drop_wall_wall_pairs", "rhs",
     "symmetric_rows", "boundary_box", "apply_boundary", "domain_top",
-    "PairListCache", "cell_linked_pairs", "density_from_neighbor_pairs",
+    "PairListCache", "cell_linked_pairs", "density_from_neighbor_pairs", "rhs_all_pairs",
+    "acoustic_dt_limit", "capillary_dt_limit", "stable_dt", "next_dt",
 ]
 
 VISCOUS_LAPLACIAN_FACTOR = 2.0
@@ -171,6 +172,38 @@ def viscous_dt_limit(cfg: Config, safety: float = 0.125) -> float:
         return float("inf")
     h = cfg.h_factor * cfg.dx
     return safety * h * h / cfg.viscosity
+
+
+def acoustic_dt_limit(cfg: Config, max_speed: float = 0.0) -> float:
+    """Largest step with dt (c0 + |v|) / h <= max_courant (droplet_impact.py:510-519)."""
+    return (cfg.max_courant * cfg.h_factor * cfg.dx
+            / (cfg.sound_speed + max(0.0, max_speed)))
+
+
+def capillary_dt_limit(cfg: Config, safety: float = 0.25) -> float:
+    """Capillary-wave step limit safety / sqrt(sigma k^3 / rho0) with k = 1/h
+    (surface_tension.py:294-318, surface_tension_dispersion.py:755-778);
+    infinite without surface tension."""
+    if cfg.surface_tension_coefficient <= 0.0:
+        return float("inf")
+    h = cfg.h_factor * cfg.dx
+    k = 1.0 / h
+    return safety / math.sqrt(cfg.surface_tension_coefficient * k ** 3 / cfg.rho0)
+
+
+def stable_dt(cfg: Config, max_speed: float = 0.0) -> float:
+    """The smallest of the acoustic (for |v|), viscous, gravity, diffusion and
+    capillary limits (droplet_impact.py:522-534)."""
+    return min(acoustic_dt_limit(cfg, max_speed), viscous_dt_limit(cfg), gravity_dt_limit(cfg),
+               diffusion_dt_limit(cfg), capillary_dt_limit(cfg))
+
+
+def next_dt(cfg: Config, dt: float, max_speed: float = 0.0) -> float:
+    """The next adaptive step: dt_safety times the stable step, grown by at
+    most dt_growth, never above the configured dt (droplet_impact.py:537-556)."""
+    target = cfg.dt_safety * stable_dt(cfg, max_speed)
+    grown = dt * cfg.dt_growth if cfg.dt_growth >= 1.0 else target
+    return min(target, grown, cfg.dt)
 
 
 def diffusion_dt_limit(cfg: Config, safety: float = 0.125) -> float:
@@ -527,6 +560,27 @@ def rhs(pos, vel, mass, cfg: Config, pairs=None, wall=None, dt=None, wall_vel=No
         return (*result, {"reaction": reaction.to(out_device),
                           "face_pressure": face.to(out_device)})
     return result
+
+
+def rhs_all_pairs(pos, vel, mass, cfg: Config, dt=None):
+    """The reference's dense formulation (droplet_impact.py:1232-1281): every
+    fluid particle against every other, no walls; ``(rho, pressure, acc)`` on
+    ``pos``'s device.
+
+    The kernel vanishes beyond 2h, so this is the pair pass over every pair
+    within 2h (the device all-pairs search) with the dense formulation's
+    choices: the Molteni diffusion term whatever form is configured, and no
+    density renormalisation, boundary-consistent density, density
+    regularisation or surface tension."""
+    from dataclasses import replace
+    from .neighbor_search import brute_force_pairs
+    if cfg.surface_pressure_closure:
+        raise NotImplementedError("surface_pressure_closure is not part of the B200 particle pass")
+    dense = replace(cfg, density_diffusion_form="molteni", density_renormalization=False,
+                    boundary_consistent_density=False, density_regularization="none",
+                    surface_tension_coefficient=0.0)
+    pairs = brute_force_pairs(pos, 2.0 * cfg.h_factor * cfg.dx)
+    return rhs(pos, vel, mass, dense, pairs=pairs.to(pos.device), dt=dt)
 
 
 # -------------------------------------------------------------- boundary ---

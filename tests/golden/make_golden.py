@@ -737,6 +737,47 @@ def _rhs_csf_cases(di):
     return data
 
 
+def dt_cases(di):
+    """The step-limit helpers (droplet_impact.py:495-556, surface_tension.py:
+    294-318) on a few configurations and speeds."""
+    rows = []
+    for o in (dict(), dict(viscosity=1e-3), dict(density_diffusion=0.1, surface_tension_coefficient=0.0728),
+              dict(dt_growth=0.9, surface_tension_coefficient=0.5, dx=0.001)):
+        cfg = di.Config(**o)
+        from tensorsph.surface_tension import capillary_dt_limit
+        for speed in (0.0, 1.5, 30.0):
+            for dt in (cfg.dt, 0.5 * cfg.dt):
+                rows.append([di.acoustic_dt_limit(cfg, speed), capillary_dt_limit(cfg), di.stable_dt(cfg, speed),
+                             di.next_dt(cfg, dt, speed)])
+    return {"values": np.asarray(rows, dtype=np.float64)}
+
+
+def dense_cases(di):
+    """rhs_all_pairs (droplet_impact.py:1232-1281), the dense O(N^2)
+    formulation without walls, on seeded jittered blocks in FP64: plain, with
+    Molteni diffusion, with the "antuono" form selected (the dense
+    formulation keeps the Molteni term) and with viscosity."""
+    data = {}
+    variants = [dict(), dict(density_diffusion=0.1), dict(density_diffusion=0.1, density_diffusion_form="antuono"),
+                dict(viscosity=1e-3, density_diffusion=0.05)]
+    for k, o in enumerate(variants):
+        g = torch.Generator().manual_seed(700 + k)
+        dx = 0.02
+        cfg = di.Config(dx=dx, pool_width=0.4, pool_depth=0.15, drop_radius=0.05, drop_center_y=0.25, **o)
+        ax = (torch.arange(0, 14, dtype=torch.float64) + 0.5) * dx
+        gx, gy = torch.meshgrid(ax, ax, indexing="xy")
+        pos = torch.stack((gx.reshape(-1), gy.reshape(-1)), -1)
+        pos = pos + 0.1 * dx * torch.randn(pos.shape, generator=g, dtype=torch.float64)
+        vel = 0.05 * torch.randn(pos.shape, generator=g, dtype=torch.float64)
+        mass = torch.full((pos.shape[0],), 1000.0 * dx * dx, dtype=torch.float64)
+        rho, p, acc = di.rhs_all_pairs(pos, vel, mass, cfg)
+        for name, t in dict(pos=pos, vel=vel, mass=mass, rho=rho, p=p, acc=acc).items():
+            data[f"c{k}_{name}"] = _np(t)
+        data[f"c{k}_opts"] = np.array(repr(sorted(o.items())))
+    data["count"] = np.int64(len(variants))
+    return data
+
+
 def delta_plus_cases(dp):
     """delta_plus_step on a perturbed lattice block in a walled corner (fluid,
     slip walls with normals, gravity, diffusion) and on a free block."""
@@ -898,6 +939,8 @@ def main(src, families=None):
         "contact": lambda: contact_cases(ca),
         "csf3axi": lambda: csf3axi_cases(c3, lc, ns, n3),
         "rhs_csf": lambda: rhs_csf_cases(di),
+        "dense": lambda: dense_cases(di),
+        "dt": lambda: dt_cases(di),
     }
     for name in families or makers:
         np.savez_compressed(OUT / f"{name}.npz", **makers[name](), **meta)

@@ -87,3 +87,19 @@ def test_dam_break_2d_tvc_options_become_case_parameters():
         dam_break_2d_case(_dam2d(tvc_every=1, tvc_limiter="cubic"))
     with pytest.raises(NotImplementedError):
         dam_break_2d_case(_dam2d(tvc_every=1), shift_every=1)
+
+
+def test_step_limits_match_reference(golden):
+    """acoustic_dt_limit, capillary_dt_limit, stable_dt and next_dt against
+    values the reference wrote (tests/golden/dt.npz): bit for bit."""
+    from tensorsph_b200 import droplet_impact as di
+    g = golden("dt")["values"]
+    rows = []
+    for o in (dict(), dict(viscosity=1e-3), dict(density_diffusion=0.1, surface_tension_coefficient=0.0728),
+              dict(dt_growth=0.9, surface_tension_coefficient=0.5, dx=0.001)):
+        cfg = di.Config(**o)
+        for speed in (0.0, 1.5, 30.0):
+            for dt in (cfg.dt, 0.5 * cfg.dt):
+                rows.append([di.acoustic_dt_limit(cfg, speed), di.capillary_dt_limit(cfg), di.stable_dt(cfg, speed),
+                             di.next_dt(cfg, dt, speed)])
+    assert np.array_equal(np.asarray(rows), g)
