@@ -544,6 +544,13 @@ typedef struct {
   double csf_wall_area;                /* young / brackbill: the wall area A of the  */
                                        /* wall delta (squared median wall spacing)   */
   double csf_traction_calibration;     /* young / brackbill: the traction's C        */
+  int64_t adaptive_dt;                 /* 1: next_dt after every step (a new run);   */
+                                       /* dt above is the first and largest step     */
+  double courant_h;                    /* max_courant * h_factor * dx                 */
+  double dt_limit;                     /* min(viscous, gravity, diffusion, capillary) */
+                                       /* step limits (may be +inf)                  */
+  double dt_growth, dt_safety;         /* next_dt's growth cap and safety factor     */
+  double target_time;                  /* steps * dt: the run ends at this time      */
 } tsph_case_params;
 
 typedef struct tsph_engine tsph_engine; /* opaque host handle */
@@ -587,18 +594,20 @@ int tsph_engine_graph_kernels(tsph_engine* engine, int64_t* kernels);
  * FP64 (device, nullable). */
 int tsph_engine_read(tsph_engine* engine, int64_t case_id, double* x, double* v, double* rho,
                      double* p, tsph_stream stream);
-/* Copy `count` per-step meter rows of one case (25 doubles each: max rho,
+/* Copy `count` per-step meter rows of one case (28 doubles each: max rho,
  * max |v|, front x, obstacle force xyz, kinetic and potential energy,
  * escapes, clamps, rebuilds, longest row, step, status, obstacle impulse x,
  * c_ref, the step's transport-velocity correction: max |shift|,
  * sum |shift|, kept and clipped counts, obstacle impulse y and z, and the
  * obstacle clamp impulse xyz; both impulses through the step's update and
- * counted from the case's admission) starting at its step `first` into
- * `out` (device).  Row k of a ring of R rows is step k mod R. */
+ * counted from the case's admission; the time at the step's start, the step
+ * taken and the step before its clamp to the target time) starting at its
+ * step `first` into `out` (device).  Row k of a ring of R rows is step k mod R. */
 int tsph_engine_diag(tsph_engine* engine, int64_t case_id, double* out, int64_t first,
                      int64_t count, tsph_stream stream);
-/* Counters of one case (escapes, clamps, rebuilds, steps, longest row, -,
- * status, -) to the host; synchronises.  Returns TSPH_ERR_STATE on a
+/* Counters of one case (escapes, clamps, rebuilds, steps, longest row,
+ * adaptive run finished, status, the step of its final meters) to the host;
+ * synchronises.  Returns TSPH_ERR_STATE on a
  * non-finite state and TSPH_ERR_CAPACITY when a neighbour row overflowed. */
 int tsph_engine_status(tsph_engine* engine, int64_t case_id, int64_t* counters,
                        tsph_stream stream);

@@ -160,7 +160,9 @@ class CaseParams(ctypes.Structure):
                 ("first_step", c_int64), ("tvc_slope", c_double), ("tvc_wall_volume", c_double),
                 ("tvc_bulk_c", c_double), ("csf_curvature", c_int64), ("csf_delta_normalization", c_int64),
                 ("csf_contact_model", c_int64), ("csf_contact_angle", c_double), ("csf_contact_reach", c_double),
-                ("csf_wall_area", c_double), ("csf_traction_calibration", c_double)]
+                ("csf_wall_area", c_double), ("csf_traction_calibration", c_double),
+                ("adaptive_dt", c_int64), ("courant_h", c_double), ("dt_limit", c_double),
+                ("dt_growth", c_double), ("dt_safety", c_double), ("target_time", c_double)]
 
 
 _SIGNATURES = {

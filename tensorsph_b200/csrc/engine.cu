@@ -46,7 +46,7 @@ namespace {
 
 constexpr int kBlock = 128;     // default threads per block of the pair kernels
 constexpr int kMaxBlock = 256;  // largest block the kernels are built for
-constexpr int kDiag = 25;
+constexpr int kDiag = 28;
 constexpr int kBatch = 4;
 constexpr int kCodeBits = 6;                               // cell-offset code bits of a row entry
 constexpr uint32_t kCodeMask = (1u << kCodeBits) - 1;
@@ -85,6 +85,13 @@ struct CaseDev {
   float tvc_slope_hh;      // truncated_linear limiter slope h^2 (< 0: none)
   int tvc_bulk;            // the correction only where C >= tvc_bulk_c c_ref (after the second list pass)
   double tvc_bulk_c;
+  int adaptive;            // adaptive time step (next_dt after every step)
+  double courant_h;        // max_courant h_factor dx: the acoustic limit's numerator
+  double c0_d;             // sound speed
+  double dt_limit;         // min of the viscous, gravity, diffusion and capillary limits
+  double dt_growth, dt_safety;
+  double target_time, time_tol;
+  double shift_strength_h; // shifting's strength h (times dt and v_ref)
 };
 
 struct CaseCtl {
@@ -108,6 +115,12 @@ struct CaseCtl {
   unsigned long long tvc_max;       // largest |shift| of this step's correction (double bits)
   double tvc_sum;                   // sum of |shift|
   unsigned long long tvc_kept, tvc_clipped;
+  double elapsed;       // simulated time at the start of the step
+  double dt_now;        // the (adaptive) step before its clamp to the target time
+  double dt_step;       // this step's dt: the diffusion, shifting and meters
+  double dt_int;        // this step's integration dt (0 on the final and after it)
+  int finished;         // adaptive: the target time is reached (later steps are frozen)
+  int final_step;       // adaptive: the step that recorded the final meters
 };
 
 struct Dev {
@@ -615,6 +628,22 @@ __global__ void k_step_begin(Dev e) {
   t.ke = t.pe = 0;
   t.force[0] = t.force[1] = t.force[2] = 0;
   t.disp[0] = 0;
+  if (!t.active) return;
+  const CaseDev& C = e.cases[c];
+  if (C.adaptive) {
+    // dam_break.py:379-408: step_dt = min(dt, target - elapsed); the step at
+    // which elapsed reaches the target records the final meters and is not
+    // integrated; after it the case stays frozen
+    const bool final_now = !t.finished && t.elapsed >= C.target_time - C.time_tol;
+    t.dt_step = t.finished ? 0.0 : fmin(t.dt_now, C.target_time - t.elapsed);
+    t.dt_int = (t.finished || final_now) ? 0.0 : t.dt_step;
+    if (final_now) {
+      t.finished = 1;
+      t.final_step = static_cast<int>(t.steps);
+    }
+  } else {
+    t.dt_step = t.dt_int = C.dt;
+  }
 }
 
 // ------------------------------------------------------------- physics ---
@@ -686,7 +715,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_diffusion_eos(const __grid_consta
         }
         rate.add(part.x + part.y);
       });
-      rho = ra.x + C.dtf * rate.value();
+      const float dtf = C.adaptive ? static_cast<float>(e.ctl[kOne ? e.one_slot : e.cid[a]].dt_step) : C.dtf;
+      rho = ra.x + dtf * rate.value();
       rho = rho > C.rho_floor ? rho : C.rho_floor;
     }
     const float p = tait(rho, C.rho0, C.bulk, C.gamma);
@@ -1546,7 +1576,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_integrate(const __grid_constant__
     const double4 v0 = ld4(e.vel, a);
     const float4 ac = e.acc[a];
     const double m = x0.w;
-    const double dt = C.dt;
+    const double dt = C.adaptive ? e.ctl[c].dt_int : C.dt;
     const double v2 = v0.x * v0.x + v0.y * v0.y + v0.z * v0.z;
     ke = 0.5 * m * v2;
     pe = m * C.gravity * x0.y;
@@ -1662,7 +1692,7 @@ __global__ void k_finalize(Dev e) {
   row[2] = __longlong_as_double(static_cast<long long>(t.front_max));
   for (int k = 0; k < 3; ++k) {
     row[3 + k] = t.force[k];
-    t.impulse[k] += t.force[k] * C.dt;
+    t.impulse[k] += t.force[k] * (C.adaptive ? t.dt_int : C.dt);
   }
   row[6] = t.ke;
   row[7] = t.pe;
@@ -1676,9 +1706,11 @@ __global__ void k_finalize(Dev e) {
   row[15] = t.cref[0];
   t.cref[1] = vmax;  // the shift's reference speed
   t.steps = step + 1;
-  t.shift_now = C.shift_every > 0 && step > 0 && (step % static_cast<unsigned long long>(C.shift_every)) == 0;
+  // an adaptive case's final step records its meters and moves nothing
+  const bool moves = !C.adaptive || t.dt_int > 0.0;
+  t.shift_now = moves && C.shift_every > 0 && step > 0 && (step % static_cast<unsigned long long>(C.shift_every)) == 0;
   t.shift_done = 0;
-  t.tvc_now = C.tvc_every > 0 && step > 0 && (step % static_cast<unsigned long long>(C.tvc_every)) == 0;
+  t.tvc_now = moves && C.tvc_every > 0 && step > 0 && (step % static_cast<unsigned long long>(C.tvc_every)) == 0;
   t.conc_now = t.shift_now || (t.tvc_now && C.tvc_bulk);
   t.tvc_max = 0;
   t.tvc_sum = 0.0;
@@ -1689,6 +1721,18 @@ __global__ void k_finalize(Dev e) {
   // k_integrate ran before this kernel: the clamp impulse through this
   // step's update, like the obstacle impulse through this step's force
   for (int k = 0; k < 3; ++k) row[22 + k] = t.clamp_impulse[k];
+  // time at the step's start, the step taken, the step before its clamp
+  row[25] = t.elapsed;
+  row[26] = t.dt_step;
+  row[27] = C.adaptive ? t.dt_now : C.dt;
+  t.elapsed += t.dt_int;
+  if (C.adaptive && t.dt_int > 0.0) {
+    // next_dt (droplet_impact.py:522-556) with the speed at the step's start
+    const double stable = fmin(C.courant_h / (C.c0_d + fmax(0.0, vmax)), C.dt_limit);
+    const double target = C.dt_safety * stable;
+    const double grown = C.dt_growth >= 1.0 ? t.dt_now * C.dt_growth : target;
+    t.dt_now = fmin(fmin(target, grown), C.dt);
+  }
 }
 
 // -------------------------------------------- transport-velocity correction ---
@@ -1992,7 +2036,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_shift_apply(Dev e) {
   const double cref = t.cref[0];
   const float thresh = static_cast<float>(C.shift_fs * cref);
   const double vref = fmax(t.cref[1], C.vref_floor);
-  const float mag = static_cast<float>(C.shift_strength_h_dt * vref);
+  const float mag = static_cast<float>(C.adaptive ? C.shift_strength_h * t.dt_step * vref
+                                                  : C.shift_strength_h_dt * vref);
   const float cap = static_cast<float>(C.shift_cap);
   double dmax = 0;
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
@@ -2557,12 +2602,24 @@ CaseDev make_case_dev(const tsph_case_params& p, int64_t* ncells) {
   c.tvc_slope_hh = p.tvc_slope > 0.0 ? static_cast<float>(p.tvc_slope * p.h * p.h) : -1.f;
   c.tvc_bulk = p.tvc_every > 0 && p.tvc_bulk_c > 0.0 ? 1 : 0;
   c.tvc_bulk_c = p.tvc_bulk_c;
+  c.adaptive = p.adaptive_dt ? 1 : 0;
+  c.courant_h = p.courant_h;
+  c.c0_d = p.sound_speed;
+  c.dt_limit = p.dt_limit;
+  c.dt_growth = p.dt_growth;
+  c.dt_safety = p.dt_safety;
+  c.target_time = p.target_time;
+  c.time_tol = 1.0e-12 * std::max(1.0, p.target_time);
+  c.shift_strength_h = p.shift_strength * p.h;
   return c;
 }
 
 bool case_params_ok(const tsph_case_params* p) {
   if (!p || (p->dim != 2 && p->dim != 3) || p->n_fluid <= 0 || p->n_wall < 0 || p->n_obstacle < 0 ||
       p->n_obstacle > p->n_wall || p->shift_every < 0 || p->first_step < 0)
+    return false;
+  if (p->adaptive_dt && (p->first_step != 0 || !(p->courant_h > 0.0) || !(p->dt_limit > 0.0) ||
+                        !(p->dt_safety > 0.0) || !(p->target_time > 0.0) || !std::isfinite(p->dt_growth)))
     return false;
   if (p->csf_curvature < 0 || p->csf_curvature > 2 || p->csf_delta_normalization < 0 ||
       p->csf_delta_normalization > 1 || p->csf_contact_model < 0 || p->csf_contact_model > 3 ||
@@ -2712,6 +2769,8 @@ int tsph_engine_add_case(tsph_engine* E, const tsph_case_params* p, const double
   ctl.first = 1;
   ctl.active = 1;
   ctl.steps = static_cast<unsigned long long>(p->first_step);
+  ctl.dt_now = p->dt;
+  ctl.dt_step = ctl.dt_int = p->dt;
   TSPH_CUDA_CHECK(cudaMemcpyAsync(d.ctl + slot, &ctl, sizeof(CaseCtl), cudaMemcpyHostToDevice, s));
   TSPH_CUDA_CHECK(cudaMemsetAsync(d.diag + static_cast<int64_t>(slot) * d.diag_ring * kDiag, 0,
                                   static_cast<size_t>(d.diag_ring) * kDiag * sizeof(double), s));
@@ -2960,9 +3019,9 @@ int tsph_engine_status(tsph_engine* E, int64_t case_id, int64_t* counters, tsph_
   counters[2] = static_cast<int64_t>(t.rebuilds);
   counters[3] = static_cast<int64_t>(t.steps);
   counters[4] = static_cast<int64_t>(t.row_max);
-  counters[5] = 0;
+  counters[5] = t.finished;
   counters[6] = t.status;
-  counters[7] = 0;
+  counters[7] = t.final_step;
   if (t.status & 2) return TSPH_ERR_STATE;
   if (t.status & 1) return TSPH_ERR_CAPACITY;
   return TSPH_OK;

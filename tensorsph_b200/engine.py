@@ -41,7 +41,7 @@ DIAG_FIELDS = ("rho_max", "speed_max", "front", "force_x", "force_y", "force_z",
                "potential", "escapes", "clamps", "rebuilds", "row_max", "step", "status",
                "impulse_x", "c_reference", "tvc_max_shift", "tvc_shift_sum", "tvc_kept",
                "tvc_clipped", "impulse_y", "impulse_z", "clamp_impulse_x", "clamp_impulse_y",
-               "clamp_impulse_z")
+               "clamp_impulse_z", "time", "dt", "dt_unclamped")
 
 
 def obstacle_lattice_3d(lo, hi, dx: float) -> torch.Tensor:
@@ -144,7 +144,7 @@ class CaseSpec:
 
 
 def _case_params(*, dim, n_fluid, n_wall, n_obstacle, cfg, h, wall_mass, box_hi, lo, hi,
-                 shift_every=0, obstacle=None, first_step=0):
+                 shift_every=0, obstacle=None, first_step=0, adaptive=False):
     if cfg.density_diffusion > 0.0 and cfg.density_diffusion_form != "molteni":
         raise NotImplementedError("the device engine implements the 'molteni' diffusion form only")
     p = _lib.CaseParams()
@@ -197,6 +197,16 @@ def _case_params(*, dim, n_fluid, n_wall, n_obstacle, cfg, h, wall_mass, box_hi,
             elif limiter not in (None, "none"):
                 raise ValueError(f"unknown tvc_limiter {limiter!r}")
             p.tvc_wall_volume = float(cfg.dx) ** 2
+    if adaptive:
+        # next_dt (droplet_impact.py:522-556) on the device: the acoustic limit
+        # there, the others are constants of the case
+        from .droplet_impact import capillary_dt_limit, diffusion_dt_limit, gravity_dt_limit, viscous_dt_limit
+        p.adaptive_dt = 1
+        p.courant_h = cfg.max_courant * cfg.h_factor * cfg.dx
+        p.dt_limit = min(viscous_dt_limit(cfg), gravity_dt_limit(cfg), diffusion_dt_limit(cfg),
+                         capillary_dt_limit(cfg))
+        p.dt_growth, p.dt_safety = float(cfg.dt_growth), float(cfg.dt_safety)
+        p.target_time = cfg.steps * cfg.dt
     p.shift_strength = getattr(cfg, "shift_strength", 1.0)
     p.shift_limit = getattr(cfg, "shift_limit", 0.25)
     p.shift_free_surface = 0.95
@@ -245,7 +255,7 @@ def dam_break_3d_case(cfg: DamBreak3DConfig, *, obstacle=None, shift_every: int 
                      wall_mass=mass_3d(cfg.dx, cfg.h_factor, cfg.rho0, cfg.density_calibration),
                      box_hi=box, lo=allpos.min(dim=0).values.tolist(),
                      hi=allpos.max(dim=0).values.tolist(), shift_every=shift_every,
-                     obstacle=obstacle, first_step=first_step)
+                     obstacle=obstacle, first_step=first_step, adaptive=cfg.adaptive_dt)
     v = torch.zeros_like(x) if velocity is None else velocity.double().contiguous()
     return CaseSpec(p, x, v, mass.double().contiguous(), wall, label or "dam_break_3d")
 
@@ -269,7 +279,7 @@ def dam_break_2d_case(cfg, *, shift_every: int = 0, velocity=None, label: str = 
     p = _case_params(dim=2, n_fluid=x.shape[0], n_wall=wall.shape[0], n_obstacle=0, cfg=cfg, h=h,
                      wall_mass=lattice_mass_unit(cfg), box_hi=box,
                      lo=allpos.min(dim=0).values.tolist(), hi=allpos.max(dim=0).values.tolist(),
-                     shift_every=shift_every)
+                     shift_every=shift_every, adaptive=cfg.adaptive_dt)
     v = torch.zeros_like(x) if velocity is None else velocity.double().contiguous()
     return CaseSpec(p, x, v, mass.double().contiguous(), wall, label or "dam_break_2d")
 
@@ -558,7 +568,7 @@ class BatchEngine:
         buf = (ctypes.c_int64 * 8)()
         rc = _lib.lib().tsph_engine_status(self._handle, int(case_id), buf, self.stream.cuda_stream)
         out = dict(escapes=buf[0], clamps=buf[1], rebuilds=buf[2], steps=buf[3], row_max=buf[4],
-                   status=buf[6])
+                   finished=bool(buf[5]), status=buf[6], final_step=buf[7])
         if rc == _lib.ERR_CAPACITY:
             raise RuntimeError(f"neighbour row capacity exceeded (longest row {buf[4]}); "
                                "raise max_neighbors")
@@ -620,6 +630,9 @@ class DamBreak3DRun:
     snapshots: list = field(default_factory=list)
     tvc_log: list = field(default_factory=list)
     resumed: bool = False
+    dt_min: float = 0.0              # smallest and largest step of the run
+    dt_max: float = 0.0
+    max_acoustic_courant: float = 0.0
 
     @property
     def mass_drift(self) -> float:
@@ -767,12 +780,13 @@ def _tvc_log(cfg, diag, n_fluid: int, first: int = 0, upto: int | None = None) -
     if not every:
         return []
     upto = cfg.steps if upto is None else upto
+    adaptive = bool(getattr(cfg, "adaptive_dt", False))   # times from the rows
     h = cfg.h_factor * cfg.dx
     out, elapsed = [], 0.0
     for k in range(upto):
         if k >= first and k > 0 and k % every == 0:
             row = diag[k - first]
-            out.append({"step": k, "time": elapsed,
+            out.append({"step": k, "time": float(row[25]) if adaptive else elapsed,
                         "max_shift_over_h": float(row[16]) / h,
                         "mean_shift_over_h": float(row[17]) / n_fluid / h,
                         "kept_fraction": (None if cfg.tvc_scope_tol is None
@@ -875,11 +889,14 @@ def run_case(cfg: DamBreak3DConfig, pair_skin_factor: float | None = None, snaps
     """
     from pathlib import Path
     from .checkpoint import CheckpointWriter, load_checkpoint
-    if cfg.adaptive_dt:
-        raise NotImplementedError("adaptive_dt is not supported by the device engine")
     if pair_skin_factor is not None:
         from dataclasses import replace
         cfg = replace(cfg, pair_skin_factor=pair_skin_factor)
+    if cfg.adaptive_dt:
+        if snapshot_times or checkpoint_path is not None:
+            raise NotImplementedError("snapshots and checkpoints with adaptive_dt are not supported "
+                                      "by the device engine")
+        return _run_3d_adaptive(cfg, obstacle, shift_every, seed, max_neighbors)
     host = dam_break_3d_host_state(cfg, obstacle, seed)
     prev = None
     if checkpoint_path is not None and resume and Path(checkpoint_path).exists():
@@ -942,12 +959,14 @@ def run_case(cfg: DamBreak3DConfig, pair_skin_factor: float | None = None, snaps
     run = DamBreak3DRun(
         times=rec["times"], front=rec["front"], kinetic_energy=rec["kinetic_energy"],
         potential_energy=rec["potential_energy"], mass=eng.initial_mass, escaped=rec["escapes"],
-        rebuilds=rec["rebuilds"], max_speed=max(rec["speed_samples"]),
+        rebuilds=rec["rebuilds"], max_speed=rec["speeds"],
         max_density_compression=rec["compression"], initial_mass=eng.initial_mass,
         final_mass=eng.initial_mass, final_positions=xs, initial_energy=record.initial_energy,
         steps_taken=cfg.steps, simulated_time=cfg.steps * cfg.dt, obstacle_force=rec["obstacle_force"],
         obstacle_impulse=rec["sph_impulse"], clamp_impulse=rec["clamp_impulse"],
-        obstacle_clamps=rec["clamps"], snapshots=snapshots, tvc_log=rec["tvc_log"], resumed=prev is not None)
+        obstacle_clamps=rec["clamps"], snapshots=snapshots, tvc_log=rec["tvc_log"], resumed=prev is not None,
+        dt_min=cfg.dt, dt_max=cfg.dt,
+        max_acoustic_courant=cfg.dt * (cfg.sound_speed + rec["speeds"]) / (cfg.h_factor * cfg.dx))
     masses = eng.spec.mass
     run.final_energy = float(0.5 * (masses[:, None] * vs.square()).sum()
                              + (masses * cfg.gravity * xs[:, 1]).sum())
@@ -958,6 +977,38 @@ def run_case(cfg: DamBreak3DConfig, pair_skin_factor: float | None = None, snaps
             Path(checkpoint_path).unlink()
         except FileNotFoundError:
             pass
+    return run
+
+
+def _run_3d_adaptive(cfg, obstacle, shift_every: int, seed, max_neighbors: int) -> DamBreak3DRun:
+    """The 3-D loop with adaptive_dt (dam_break_3d.py:617-711): meters at
+    every output_every-th step and at the final one, times from the device."""
+    from dataclasses import replace
+    eng = DamBreak3DEngine(cfg, obstacle=obstacle, shift_every=shift_every, seed=seed,
+                           max_neighbors=max_neighbors, diag_ring=4 * cfg.steps + 1100,
+                           host_state=dam_break_3d_host_state(cfg, obstacle, seed))
+    final = _advance_adaptive(eng, eng.case_id, cfg)
+    with torch.cuda.stream(eng.stream):
+        x, v, _, _ = eng.state()
+        xs, vs = x.cpu(), v.cpu()
+        diag = eng.diagnostics(0, final + 1).cpu()
+    samples = [(k, float(diag[k, 25])) for k in range(final + 1) if k % cfg.output_every == 0 or k == final]
+    # the record of a fixed-step run of ``final`` steps, with these samples
+    rec = _DeviceRecord(replace(cfg, steps=final), samples, 0, None, eng.n_fluid, eng.initial_pe).collect(diag, final)
+    dts = diag[:, 27]
+    run = DamBreak3DRun(
+        times=rec["times"], front=rec["front"], kinetic_energy=rec["kinetic_energy"],
+        potential_energy=rec["potential_energy"], mass=eng.initial_mass, escaped=rec["escapes"],
+        rebuilds=int(diag[final, 10]), max_speed=rec["speeds"], max_density_compression=rec["compression"],
+        initial_mass=eng.initial_mass, final_mass=eng.initial_mass, final_positions=xs,
+        initial_energy=eng.initial_pe, steps_taken=final, simulated_time=float(diag[final, 25]),
+        obstacle_force=rec["obstacle_force"], obstacle_impulse=rec["sph_impulse"],
+        clamp_impulse=rec["clamp_impulse"], obstacle_clamps=rec["clamps"], tvc_log=rec["tvc_log"],
+        dt_min=float(dts.min()), dt_max=float(dts.max()), max_acoustic_courant=_max_courant(cfg, diag))
+    masses = eng.spec.mass
+    run.final_energy = float(0.5 * (masses[:, None] * vs.square()).sum()
+                             + (masses * cfg.gravity * xs[:, 1]).sum())
+    eng.close()
     return run
 
 
@@ -981,6 +1032,60 @@ class DamBreakRun:
     snapshots: list = field(default_factory=list)
     max_tvc_shift: float = 0.0       # largest |shift| of one correction, m
     max_tvc_clipped: float = 0.0     # largest fraction of fluid one correction clipped
+    dt_min: float = 0.0              # smallest and largest step of the run
+    dt_max: float = 0.0
+    max_acoustic_courant: float = 0.0
+
+
+def _max_courant(cfg, diag) -> float:
+    """max over the steps of dt (c0 + |v|max) / h (dam_break.py:394-397)."""
+    h = cfg.h_factor * cfg.dx
+    return max(float(diag[k, 26]) * (cfg.sound_speed + float(diag[k, 1])) / h for k in range(diag.shape[0]))
+
+
+def _advance_adaptive(eng, cid, cfg, chunk: int = 64) -> int:
+    """Step an adaptive case until it records its final meters (the step at
+    which the simulated time reaches steps * dt); returns that step.  Steps
+    after it leave the case as it is."""
+    max_steps = 4 * cfg.steps + 1000
+    done = 0
+    while done <= max_steps:
+        n = min(chunk, max_steps + 1 - done)
+        eng.step(n)
+        done += n
+        st = BatchEngine.status(eng, cid)
+        if st["finished"]:
+            return int(st["final_step"])
+    raise RuntimeError(f"the adaptive run did not reach {cfg.steps * cfg.dt} s in {max_steps} steps")
+
+
+def _run_2d_adaptive(cfg, max_neighbors: int) -> "DamBreakRun":
+    """The 2-D loop with adaptive_dt (dam_break.py:367-465): meters at every
+    output_every-th step and at the final one, times from the device."""
+    spec = dam_break_2d_case(cfg, shift_every=cfg.shift_every)
+    eng = BatchEngine(**capacity_for([spec], max_neighbors=max_neighbors, diag_ring=4 * cfg.steps + 1100))
+    cid = eng.add(spec)
+    final = _advance_adaptive(eng, cid, cfg)
+    with torch.cuda.stream(eng.stream):
+        x = eng.read(cid)[0].cpu()
+        diag = eng.diagnostics(cid, 0, final + 1).cpu()
+    sample = [k for k in range(final + 1) if k % cfg.output_every == 0 or k == final]
+    dts = diag[:, 27]
+    run = DamBreakRun(times=[float(diag[k, 25]) for k in sample], front=[float(diag[k, 2]) for k in sample],
+                      kinetic_energy=[float(diag[k, 6]) for k in sample],
+                      potential_energy=[float(diag[k, 7]) for k in sample],
+                      mass=float(spec.mass.sum()), escaped=int(diag[final - 1, 8]) if final else 0,
+                      rebuilds=int(diag[final, 10]), max_speed=float(diag[:, 1].max()),
+                      max_density_compression=float(diag[:, 0].max()) / cfg.rho0 - 1.0,
+                      final_positions=x, steps_taken=final, simulated_time=float(diag[final, 25]),
+                      dt_min=float(dts.min()), dt_max=float(dts.max()), max_acoustic_courant=_max_courant(cfg, diag))
+    every = int(cfg.tvc_every or 0)
+    applied = [k for k in range(1, final) if every and k % every == 0]
+    if applied:
+        run.max_tvc_shift = max(float(diag[k, 16]) for k in applied)
+        run.max_tvc_clipped = max(float(diag[k, 19]) for k in applied) / spec.n_fluid
+    eng.close()
+    return run
 
 
 def run_dam_break_2d(cfg, *, snapshot_times=None, max_neighbors: int = 64) -> DamBreakRun:
@@ -990,7 +1095,9 @@ def run_dam_break_2d(cfg, *, snapshot_times=None, max_neighbors: int = 64) -> Da
     correction (``tvc_every``, scopes "all", "bulk_g" and "bulk", the
     ``truncated_linear`` limiter, the clip) each run, not both together."""
     if cfg.adaptive_dt:
-        raise NotImplementedError("adaptive_dt is not supported by the device engine")
+        if snapshot_times:
+            raise NotImplementedError("snapshot_times with adaptive_dt are not supported by the device engine")
+        return _run_2d_adaptive(cfg, max_neighbors)
     spec = dam_break_2d_case(cfg, shift_every=cfg.shift_every)
     eng = BatchEngine(**capacity_for([spec], max_neighbors=max_neighbors,
                                      diag_ring=max(cfg.steps + 1, 1)))
@@ -1011,10 +1118,12 @@ def run_dam_break_2d(cfg, *, snapshot_times=None, max_neighbors: int = 64) -> Da
                       potential_energy=[float(diag[k, 7]) for k in sample],
                       mass=float(spec.mass.sum()), escaped=int(st["escapes"]),
                       rebuilds=int(st["rebuilds"]),
-                      max_speed=max(float(diag[k, 1]) for k in sample),
+                      max_speed=float(diag[:, 1].max()),
                       max_density_compression=float(diag[:, 0].max()) / cfg.rho0 - 1.0,
                       final_positions=x, steps_taken=cfg.steps,
-                      simulated_time=cfg.steps * cfg.dt, snapshots=snapshots)
+                      simulated_time=cfg.steps * cfg.dt, snapshots=snapshots,
+                      dt_min=cfg.dt, dt_max=cfg.dt,
+                      max_acoustic_courant=_max_courant(cfg, diag))
     every = int(cfg.tvc_every or 0)
     applied = [k for k in range(1, cfg.steps) if every and k % every == 0]
     if applied:

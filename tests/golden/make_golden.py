@@ -869,6 +869,31 @@ def dam3d_run_case(d3):
             "max_density_compression": np.float64(run.max_density_compression)}
 
 
+def adaptive_run_case(db):
+    """The reference's own 2-D dam-break loop with adaptive_dt (dam_break.py:
+    362-465) in FP64 on the tank of its Courant-limit test (dx = 0.04,
+    c0 = 25, 0.25 s): the step-size range, the Courant peak, the sampled
+    meters and the final positions."""
+    torch.set_default_dtype(torch.float64)
+    try:
+        cfg = db.DamBreakConfig(dx=0.04, pool_width=2.0, column_width=0.2, column_height=0.4,
+                                sound_speed=25.0, adaptive_dt=True, device="cpu")
+        cfg.dt = cfg.dt_from_courant()
+        cfg.steps = int(round(0.25 / cfg.dt))
+        cfg.output_every = max(1, int(round(0.05 / cfg.dt)))
+        run = db.run_case(cfg)
+    finally:
+        torch.set_default_dtype(torch.float32)
+    return {"times": np.asarray(run.times), "front": np.asarray(run.front),
+            "kinetic": np.asarray(run.kinetic_energy), "potential": np.asarray(run.potential_energy),
+            "final_positions": _np(run.final_positions), "rebuilds": np.int64(run.rebuilds),
+            "escaped": np.int64(run.escaped), "steps": np.int64(run.steps_taken),
+            "simulated_time": np.float64(run.simulated_time), "dt_min": np.float64(run.dt_min),
+            "dt_max": np.float64(run.dt_max), "max_acoustic_courant": np.float64(run.max_acoustic_courant),
+            "max_speed": np.float64(run.max_speed), "dt": np.float64(cfg.dt),
+            "cfg_steps": np.int64(cfg.steps), "output_every": np.int64(cfg.output_every)}
+
+
 def checkpoint_case(kl):
     """A checkpoint file as the obstacle case writes it (save_checkpoint,
     kleefsman_obstacle_3d.py:499-528): its bytes, the configuration's
@@ -941,6 +966,7 @@ def main(src, families=None):
         "rhs_csf": lambda: rhs_csf_cases(di),
         "dense": lambda: dense_cases(di),
         "dt": lambda: dt_cases(di),
+        "adaptive_run": lambda: adaptive_run_case(db),
     }
     for name in families or makers:
         np.savez_compressed(OUT / f"{name}.npz", **makers[name](), **meta)

@@ -386,3 +386,81 @@ def test_2d_tvc_refuses_shifting_and_unknown_options():
         dam_break_2d_case(replace(small_2d(), tvc_every=1), shift_every=1)
     with pytest.raises(ValueError):
         dam_break_2d_case(replace(small_2d(), tvc_every=1, tvc_limiter="cubic"))
+
+
+def _adaptive_tank():
+    from tensorsph_b200.dam_break import DamBreakConfig
+    cfg = DamBreakConfig(dx=0.04, pool_width=2.0, column_width=0.2, column_height=0.4, sound_speed=25.0,
+                         adaptive_dt=True)
+    cfg.dt = cfg.dt_from_courant()
+    cfg.steps = int(round(0.25 / cfg.dt))
+    cfg.output_every = max(1, int(round(0.05 / cfg.dt)))
+    return cfg
+
+
+def assert_adaptive_rows(cfg, diag, final):
+    """The device's step sizes against the host next_dt (droplet_impact.py:
+    537-552) fed the step's own starting speed, bit for bit: row k holds the
+    time at step k's start (col 25), the step taken (col 26, clipped to the
+    target time) and the step before the clip (col 27)."""
+    from tensorsph_b200.droplet_impact import next_dt
+    d = diag.numpy()
+    target = cfg.steps * cfg.dt
+    assert d[0, 25] == 0.0 and d[0, 27] == cfg.dt
+    for k in range(final):
+        assert d[k, 26] == min(d[k, 27], target - d[k, 25]), k
+        assert d[k + 1, 25] == d[k, 25] + d[k, 26], k
+        assert d[k + 1, 27] == next_dt(cfg, float(d[k, 27]), float(d[k, 1])), k
+        assert d[k, 25] < target - 1e-12 * max(1.0, target), k
+    assert d[final, 25] >= target - 1e-12 * max(1.0, target)
+
+
+def test_adaptive_dam_break_follows_reference_run(golden, gpu):
+    """adaptive_dt (dam_break.py:362-465) on the device against the
+    reference's own FP64 run of its Courant-limit tank (dx = 0.04, c0 = 25,
+    0.25 s, 474 steps): steps taken, step-size range, Courant peak, sampled
+    meters and final positions; then each step's size against next_dt."""
+    from tensorsph_b200.engine import (BatchEngine, _advance_adaptive, capacity_for, dam_break_2d_case,
+                                       run_dam_break_2d)
+    g = golden("adaptive_run")
+    cfg = _adaptive_tank()
+    assert (cfg.dt, cfg.steps, cfg.output_every) == (float(g["dt"]), int(g["cfg_steps"]), int(g["output_every"]))
+    saved = torch.get_default_dtype()
+    torch.set_default_dtype(torch.float64)
+    try:
+        run = run_dam_break_2d(cfg)
+        spec = dam_break_2d_case(cfg)
+    finally:
+        torch.set_default_dtype(saved)
+    assert run.steps_taken == int(g["steps"]) and run.escaped == int(g["escaped"])
+    assert run.simulated_time == pytest.approx(float(g["simulated_time"]), rel=1e-12)
+    assert len(run.times) == len(g["times"])
+    assert np.allclose(run.times, g["times"], rtol=1e-5, atol=0)
+    assert run.dt_max == float(g["dt_max"]) == cfg.dt
+    assert run.dt_min == pytest.approx(float(g["dt_min"]), rel=1e-5)
+    assert run.max_acoustic_courant == pytest.approx(float(g["max_acoustic_courant"]), rel=1e-9)
+    assert run.max_speed == pytest.approx(float(g["max_speed"]), rel=1e-4)
+    # the reference's own claims for this case (tests/test_adaptive_dt.py:114-140)
+    assert run.max_acoustic_courant <= cfg.max_courant * 1.02 and run.dt_min < run.dt_max
+    front = float(np.abs(np.asarray(run.front) - g["front"]).max())
+    pe, ke = np.asarray(run.potential_energy), np.asarray(run.kinetic_energy)
+    dpe = g["potential"] - g["potential"][0]
+    assert front < 2e-5, front
+    assert np.abs((pe - pe[0]) - dpe).max() < 5e-4 * np.abs(dpe).max()
+    assert np.abs(ke - g["kinetic"]).max() < 5e-4 * g["kinetic"].max()
+    x0 = _config1_start(cfg)
+    moved = np.abs(g["final_positions"] - x0).max()
+    assert np.abs(run.final_positions.numpy() - g["final_positions"]).max() < 1e-3 * moved
+    # the step sequence itself, from a case run through the batch engine
+    eng = BatchEngine(**capacity_for([spec], max_neighbors=64, diag_ring=4 * cfg.steps + 1100))
+    cid = eng.add(spec)
+    final = _advance_adaptive(eng, cid, cfg)
+    with torch.cuda.stream(eng.stream):
+        diag = eng.diagnostics(cid, 0, final + 1).cpu()
+        x_end = eng.read(cid)[0].cpu()
+    eng.step(8)   # a finished case stays where it is
+    with torch.cuda.stream(eng.stream):
+        assert torch.equal(eng.read(cid)[0].cpu(), x_end)
+    eng.close()
+    assert final == run.steps_taken
+    assert_adaptive_rows(cfg, diag, final)

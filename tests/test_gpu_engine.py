@@ -291,3 +291,49 @@ def test_run_case_follows_reference_run(golden, gpu):
     moved = np.abs(g["final_positions"] - x0).max()
     dxmax = np.abs(run.final_positions.numpy() - g["final_positions"]).max()
     assert dxmax < 1e-4 * moved, (dxmax, moved)
+
+
+def test_adaptive_3d_run_with_obstacle(gpu):
+    """adaptive_dt in the 3-D loop (dam_break_3d.py:617-711) with the
+    obstacle: at max_courant 0.25 the step shrinks to dt_safety of the
+    acoustic limit at once, so the run takes more steps than the fixed one
+    to reach steps * dt; each step against next_dt, the obstacle impulse as
+    the sum of force times step, and the fixed-step record unchanged when the
+    limit never binds."""
+    from dataclasses import replace
+    from tensorsph_b200.engine import DamBreak3DEngine, _advance_adaptive, run_case
+    from tests.test_gpu_batch import assert_adaptive_rows
+    cfg, obstacle = small_case()
+    cfg = replace(cfg, steps=30, output_every=10, max_courant=0.25, adaptive_dt=True)
+    saved = torch.get_default_dtype()
+    torch.set_default_dtype(torch.float64)
+    try:
+        run = run_case(cfg, obstacle=obstacle)
+        eng = DamBreak3DEngine(cfg, obstacle=obstacle, max_neighbors=160, diag_ring=4 * cfg.steps + 1100)
+        final = _advance_adaptive(eng, eng.case_id, cfg)
+        with torch.cuda.stream(eng.stream):
+            diag = eng.diagnostics(0, final + 1).cpu()
+        eng.close()
+        # max_courant 0.6: the target step stays above dt, so only the last
+        # step could be clipped and the record is the fixed-step one
+        loose = replace(cfg, max_courant=0.6)
+        a, f = run_case(loose, obstacle=obstacle), run_case(replace(loose, adaptive_dt=False), obstacle=obstacle)
+    finally:
+        torch.set_default_dtype(saved)
+    assert final == run.steps_taken > cfg.steps
+    assert_adaptive_rows(cfg, diag, final)
+    d = diag.numpy()
+    assert run.dt_max == cfg.dt and run.dt_min == pytest.approx(0.9 * cfg.dt, rel=0.05)
+    assert run.simulated_time == pytest.approx(cfg.steps * cfg.dt, rel=1e-12)
+    assert run.times == [float(d[k, 25]) for k in range(final + 1) if k % 10 == 0 or k == final]
+    impulse = sum(float(d[k, 3]) * float(d[k, 26]) for k in range(final))
+    assert run.obstacle_impulse[0] == pytest.approx(impulse, rel=1e-12, abs=1e-15)
+    assert len(run.obstacle_force) == final
+    assert a.steps_taken == f.steps_taken == cfg.steps and a.dt_min == a.dt_max == cfg.dt
+    assert np.allclose(a.times, f.times, rtol=1e-12, atol=0)
+    for key in ("front", "kinetic_energy", "potential_energy"):
+        assert np.allclose(getattr(a, key), getattr(f, key), rtol=1e-9, atol=1e-12), key
+    # the final step's size is clipped to the target time (about 0), so its
+    # speed, counted in the fixed run's Courant peak, adds nothing here
+    assert a.max_speed == pytest.approx(f.max_speed, rel=1e-9)
+    assert a.max_acoustic_courant <= f.max_acoustic_courant
