@@ -133,7 +133,11 @@ enum {
   TSPH_RHS_BOUNDARY_DENSITY = 2, /* Config.boundary_consistent_density       */
   TSPH_RHS_SPLIT = 4,            /* rhs(split=True) / rhs_3d(return_wall_force) */
   TSPH_RHS_WALL_SELF = 8,        /* walls carry the W(0) self term (3-D)      */
-  TSPH_RHS_WRAP_X = 16           /* periodic x with period wrap_width          */
+  TSPH_RHS_WRAP_X = 16,          /* periodic x with period wrap_width          */
+  TSPH_RHS_COMPRESSION = 32,     /* Config.density_regularization="compression" */
+                                 /* (droplet_impact.py:982-1028; 2-D)           */
+  TSPH_RHS_SURFACE_CLOSURE = 64  /* Config.surface_pressure_closure             */
+                                 /* (droplet_impact.py:429-492, 1030-1037; 2-D) */
 };
 
 typedef struct {
@@ -142,6 +146,17 @@ typedef struct {
   double h, sigma, rho0, sound_speed, gamma, gravity, viscosity, wall_friction;
   double diffusion_scale; /* 2 delta c0 h; 0 disables the diffusive term      */
   double eigen_floor, dt, wall_mass, wrap_width, lattice_sum;
+  /* COMPRESSION: rule 0 "internal", 1 "free_surface"; kref = the inverse
+   * reference compression this call uses (1 for normalization "none").
+   * Needs no diffusion, renormalisation, boundary-consistent density or
+   * density offset (the reference raises for each).                        */
+  int64_t compression_rule;
+  double compression_kref;
+  /* SURFACE_CLOSURE: particles with rho < surface_threshold rho0 receive;
+   * donors 0 "interior" (surface_layers passes), 1 "all", 2 "all" plus the
+   * receiver itself (the dense formulation, rhs_all_pairs).                */
+  int64_t surface_donors, surface_layers;
+  double surface_threshold;
 } tsph_wcsph_params;
 
 typedef struct {
@@ -160,6 +175,9 @@ typedef struct {
   void* acc;                  /* out (n, D)                     */
   void* reaction;             /* out (nw, D) when SPLIT         */
   void* face_pressure;        /* out (nw) when SPLIT            */
+  double* compression_out;    /* out (2, device) when COMPRESSION: the
+                                 inverse reference compression for the next
+                                 call, the particles counted (S > 1)      */
 } tsph_wcsph_io;
 
 int64_t tsph_wcsph_workspace_bytes(const tsph_wcsph_params* prm);

@@ -182,12 +182,69 @@ def antuono_rate(rho, mass, delta, radial, dist2, i, j, scale, grad_rho):
 
 # ------------------------------------------------------------------ 2-D rhs ---
 
+def compression_sums(all_mass, rho0, w_self, i, j, wij, n, inverse_reference):
+    """S_a = W(0) Vref_a + Kref sum_b W_ab Vref_b over the fluid rows, Vref =
+    m / rho0, Kref on the neighbour term only (compression_regularization.py:
+    96-139)."""
+    vol = all_mass / all_mass.dtype.type(rho0)
+    sums = all_mass.dtype.type(w_self) * vol[:n]
+    weighted = all_mass.dtype.type(inverse_reference) * wij
+    np.add.at(sums, i, weighted * vol[j])
+    back = j < n
+    np.add.at(sums, j[back], weighted[back] * vol[i[back]])
+    return sums
+
+
+def average_inverse_reference(sums):
+    """(1 / mean{S : S > 1}, count), 1 for an empty set
+    (compression_regularization.py:142-161)."""
+    mask = sums > 1.0
+    counted = int(mask.sum())
+    if counted == 0:
+        return 1.0, 0
+    total = float(sums[mask].sum())
+    if total <= 0.0:
+        return 1.0, 0
+    return counted / total, counted
+
+
+def free_surface_pressure(rho, pressure, delta, wij, i, j, cfg):
+    """Adami's extrapolation onto particles with rho < threshold rho0 over the
+    fluid pairs (droplet_impact.py:429-492): "interior" donors in
+    surface_pressure_layers Jacobi passes, "all" in one."""
+    T = pressure.dtype.type
+    n = pressure.shape[0]
+    known = ~(rho < T(cfg.surface_pressure_threshold * cfg.rho0))
+    p = pressure.copy()
+    grav = T(cfg.gravity) * delta[:, 1]
+    literal = cfg.surface_pressure_donors == "all"
+    for _ in range(1 if literal else max(1, cfg.surface_pressure_layers)):
+        receive = ~known
+        if not receive.any():
+            break
+        w_i = wij if literal else wij * known[j].astype(wij.dtype)
+        w_j = wij if literal else wij * known[i].astype(wij.dtype)
+        num = np.zeros(n, dtype=p.dtype)
+        den = np.zeros(n, dtype=p.dtype)
+        np.add.at(num, i, w_i * (p[j] - grav * rho[j]))
+        np.add.at(den, i, w_i)
+        np.add.at(num, j, w_j * (p[i] + grav * rho[i]))
+        np.add.at(den, j, w_j)
+        filled = receive & (den > T(1.0e-30))
+        p = np.where(filled, np.maximum(num / np.maximum(den, T(1.0e-30)), T(0)), p)
+        known = known | filled
+    return p
+
+
 def rhs(pos, vel, mass, cfg, pairs=None, wall=None, dt=None, wall_vel=None,
         wall_accel=None, split=False, wrap_width=None, nu_field=None,
-        density_offset=None):
+        density_offset=None, state=None):
     """2-D WCSPH right-hand side (droplet_impact.py:810-1228).
 
-    ``cfg`` is any object with the reference ``Config`` attributes.
+    ``cfg`` is any object with the reference ``Config`` attributes.  With
+    ``density_regularization="compression"`` the inverse reference
+    compression is read from and written to ``state["inverse_reference"]``
+    (1 when absent), the count to ``state["counted"]``.
     """
     T = pos.dtype.type
     h = cfg.h_factor * cfg.dx
@@ -245,7 +302,19 @@ def rhs(pos, vel, mass, cfg, pairs=None, wall=None, dt=None, wall_vel=None,
             rate = antuono_rate(rho, mass, delta[ff], radial, distance[ff] ** 2,
                                 i[ff], j[ff], scale, grad_rho)
         rho = np.maximum(rho + T(step_dt) * rate, T(0.1 * cfg.rho0))
+    if getattr(cfg, "density_regularization", "none") == "compression":
+        state = {} if state is None else state
+        used = (state.get("inverse_reference", 1.0)
+                if cfg.compression_normalization == "reference_mean" else 1.0)
+        sums = compression_sums(all_mass, cfg.rho0, w0, i, j, wij, n, used)
+        state["inverse_reference"], state["counted"] = average_inverse_reference(sums)
+        if cfg.compression_regularization_rule == "free_surface":
+            sums = np.maximum(sums, T(1))
+        rho = np.maximum(sums * T(cfg.rho0), T(0.1 * cfg.rho0))
     pressure = tait(rho, cfg.rho0, cfg.sound_speed, cfg.gamma)
+    if getattr(cfg, "surface_pressure_closure", False):
+        ff = (i < n) & (j < n)
+        pressure = free_surface_pressure(rho, pressure, delta[ff], wij[ff], i[ff], j[ff], cfg)
     wall_pressure = np.zeros(nw, dtype=pos.dtype)
     if nw:
         i_fluid = i < n

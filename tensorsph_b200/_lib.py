@@ -22,6 +22,7 @@ ERR_ARG, ERR_NONFINITE, ERR_CUDA, ERR_WORKSPACE, ERR_CAPACITY = 1, 2, 3, 4, 5
 ERR_UNSUPPORTED, ERR_INDEX, ERR_GRID, ERR_STATE, ERR_TIMEOUT = 6, 7, 8, 9, 10
 
 RHS_RENORMALIZE, RHS_BOUNDARY_DENSITY, RHS_SPLIT, RHS_WALL_SELF, RHS_WRAP_X = 1, 2, 4, 8, 16
+RHS_COMPRESSION, RHS_SURFACE_CLOSURE = 32, 64
 
 
 class Grid(ctypes.Structure):
@@ -37,13 +38,17 @@ class WcsphParams(ctypes.Structure):
                [(k, c_double) for k in ("h", "sigma", "rho0", "sound_speed", "gamma", "gravity",
                                         "viscosity", "wall_friction", "diffusion_scale",
                                         "eigen_floor", "dt", "wall_mass", "wrap_width",
-                                        "lattice_sum")]
+                                        "lattice_sum")] + \
+               [("compression_rule", c_int64), ("compression_kref", c_double),
+                ("surface_donors", c_int64), ("surface_layers", c_int64),
+                ("surface_threshold", c_double)]
 
 
 class WcsphIO(ctypes.Structure):
     _fields_ = [(k, c_void_p) for k in ("pos", "vel", "mass", "wall", "wall_vel", "wall_accel",
                                         "nu_field", "density_offset", "rowptr", "entries", "rho",
-                                        "pressure", "acc", "reaction", "face_pressure")]
+                                        "pressure", "acc", "reaction", "face_pressure",
+                                        "compression_out")]
 
 
 class ThreedParams(ctypes.Structure):

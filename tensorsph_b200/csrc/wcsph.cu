@@ -13,6 +13,12 @@
 //   K5 force      a_a = -sum m_b (p_a/rho_a^2 + p_b/rho_b^2) grad W
 //                       - sum 2 nu blend (v_a - v_b) (m_b / rho_b) L_ab + g   fluid rows
 //   K6 reaction   force of the fluid on each wall particle (split / 3-D)    wall rows
+//
+// Two options of the 2-D rhs run between K3 and K4:
+//   compression   rho_a = rule(W(0) Vref_a + Kref sum_b W_ab Vref_b) rho0, Vref = m / rho0,
+//                 then 1 / mean{S > 1} for the next call (one block)      fluid rows
+//   closure       p_a = max(0, sum_b (p_b - g (y_a - y_b) rho_b) W_ab / sum_b W_ab) over
+//                 fluid donors, on rho_a < threshold rho0 (Jacobi passes)  fluid rows
 #include <cmath>
 #include <mutex>
 
@@ -126,6 +132,127 @@ __global__ void density_kernel(WP<T> p, const Q4<T>* __restrict__ pm, const int6
     if (!p.diffusion) {
       rho_all[a] = rho;
       p_all[a] = tait(rho, p);
+    }
+  }
+}
+
+// ------------------------------------------- compression regularisation ---
+// droplet_impact.py:982-1028 with compression_regularization.py:96-187: the
+// summation density is replaced by rule(S) rho0; S goes to csum for the
+// average that the next call uses.
+
+template <class T, int D>
+__global__ void compression_kernel(WP<T> p, const Q4<T>* __restrict__ pm, const int64_t* __restrict__ rowptr,
+                                   const uint32_t* __restrict__ ent, T kref, int free_surface,
+                                   T* __restrict__ csum, T* __restrict__ rho_s, T* __restrict__ rho_all,
+                                   T* __restrict__ p_all) {
+  for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < p.n; a += gridDim.x * blockDim.x) {
+    const Q4<T> pa = pm[a];
+    CSum<T> s;
+    const int64_t beg = rowptr[a], end = rowptr[a + 1];
+    for (int64_t e = beg; e < end; ++e) {
+      const Q4<T> pb = pm[ent[e] & kIndexMask];
+      T d[3];
+      separation<T, D>(pa, pb, p, d);
+      s.add(p.k.w(sqrt(norm2<T, D>(d))) * (pb.w / p.rho0));
+    }
+    const T S = p.w0 * (pa.w / p.rho0) + kref * s.value();
+    csum[a] = S;
+    const T K = free_surface ? (S > T(1) ? S : T(1)) : S;
+    T rho = K * p.rho0;
+    rho = rho > p.rho_floor ? rho : p.rho_floor;
+    rho_s[a] = rho;
+    rho_all[a] = rho;
+    p_all[a] = tait(rho, p);
+  }
+}
+
+// AverageCompression: out[0] = count / sum over S > 1 (1 for an empty set),
+// out[1] = count.  One block, fixed order: the result does not depend on timing.
+template <class T>
+__global__ void __launch_bounds__(1024) compression_average(const T* __restrict__ csum, int64_t n,
+                                                           double* __restrict__ out) {
+  __shared__ double part[32];
+  __shared__ unsigned long long cnt[32];
+  double sum = 0.0;
+  unsigned long long c = 0;
+  for (int64_t a = threadIdx.x; a < n; a += blockDim.x) {
+    const double v = static_cast<double>(csum[a]);
+    if (v > 1.0) {
+      sum += v;
+      ++c;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    sum += __shfl_down_sync(0xffffffffu, sum, o);
+    c += __shfl_down_sync(0xffffffffu, c, o);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    part[warp] = sum;
+    cnt[warp] = c;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double total = 0.0;
+    unsigned long long count = 0;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) {
+      total += part[w];
+      count += cnt[w];
+    }
+    const bool ok = count > 0 && total > 0.0;
+    out[0] = ok ? static_cast<double>(count) / total : 1.0;
+    out[1] = ok ? static_cast<double>(count) : 0.0;
+  }
+}
+
+// ------------------------------------------------ free-surface closure ---
+// droplet_impact.py:429-492 over the fluid neighbours.  donors: 0 the known
+// ones ("interior"), 1 all ("all"), 2 all plus the particle itself (the dense
+// formulation's pair set includes i == j).
+
+template <class T>
+__global__ void closure_init(WP<T> p, const T* __restrict__ rho_all, T threshold, uint8_t* __restrict__ known) {
+  for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < p.n; a += gridDim.x * blockDim.x)
+    known[a] = rho_all[a] < threshold ? 0 : 1;
+}
+
+template <class T, int D>
+__global__ void closure_pass(WP<T> p, const Q4<T>* __restrict__ pm, const int64_t* __restrict__ rowptr,
+                             const uint32_t* __restrict__ ent, const T* __restrict__ rho_all, int donors,
+                             const T* __restrict__ p_in, const uint8_t* __restrict__ known_in,
+                             T* __restrict__ p_out, uint8_t* __restrict__ known_out) {
+  for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < p.n; a += gridDim.x * blockDim.x) {
+    if (known_in[a]) {
+      p_out[a] = p_in[a];
+      known_out[a] = 1;
+      continue;
+    }
+    const Q4<T> pa = pm[a];
+    CSum<T> num, den;
+    if (donors == 2) {
+      num.add(p.w0 * p_in[a]);
+      den.add(p.w0);
+    }
+    const int64_t beg = rowptr[a], end = rowptr[a + 1];
+    for (int64_t e = beg; e < end; ++e) {
+      const uint32_t b = ent[e] & kIndexMask;
+      if (b >= p.n || (donors == 0 && !known_in[b])) continue;
+      const Q4<T> pb = pm[b];
+      T d[3];
+      separation<T, D>(pa, pb, p, d);
+      const T W = p.k.w(sqrt(norm2<T, D>(d)));
+      num.add(W * (p_in[b] - p.grav * d[1] * rho_all[b]));
+      den.add(W);
+    }
+    const T dn = den.value();
+    if (dn > T(1.0e-30)) {
+      const T v = num.value() / dn;
+      p_out[a] = v > T(0) ? v : T(0);
+      known_out[a] = 1;
+    } else {
+      p_out[a] = p_in[a];
+      known_out[a] = 0;
     }
   }
 }
@@ -403,7 +530,7 @@ __global__ void copy_out(const T* __restrict__ src, T* __restrict__ dst, int64_t
 }
 
 struct RhsLayout {
-  size_t pm, vv, rho_all, p_all, rho_s, grad, total;
+  size_t pm, vv, rho_all, p_all, rho_s, grad, csum, p_tmp, known, total;
 };
 
 RhsLayout rhs_layout(const tsph_wcsph_params& prm) {
@@ -417,6 +544,10 @@ RhsLayout rhs_layout(const tsph_wcsph_params& prm) {
   L.p_all = off; off += align_up(all * ts);
   L.rho_s = off; off += align_up(prm.n_fluid * ts);
   L.grad = off; off += align_up(prm.n_fluid * prm.dim * ts);
+  const bool comp = prm.flags & TSPH_RHS_COMPRESSION, closure = prm.flags & TSPH_RHS_SURFACE_CLOSURE;
+  L.csum = off; off += comp ? align_up(prm.n_fluid * ts) : 0;
+  L.p_tmp = off; off += closure ? align_up(prm.n_fluid * ts) : 0;
+  L.known = off; off += closure ? align_up(2 * prm.n_fluid) : 0;
   L.total = off + 256;
   return L;
 }
@@ -482,6 +613,35 @@ int run_rhs(const tsph_wcsph_params& prm, const tsph_wcsph_io& io, char* ws, cud
                                                         rho_all, p_all);
     TSPH_LAUNCH_CHECK();
   }
+  if (prm.flags & TSPH_RHS_COMPRESSION) {
+    T* csum = reinterpret_cast<T*>(ws + L.csum);
+    compression_kernel<T, D><<<grid_for(n, B), B, 0, s>>>(p, pm, io.rowptr, io.entries,
+                                                          static_cast<T>(prm.compression_kref),
+                                                          prm.compression_rule == 1 ? 1 : 0, csum, rho_s,
+                                                          rho_all, p_all);
+    TSPH_LAUNCH_CHECK();
+    compression_average<T><<<1, 1024, 0, s>>>(csum, n, io.compression_out);
+    TSPH_LAUNCH_CHECK();
+  }
+  if (prm.flags & TSPH_RHS_SURFACE_CLOSURE) {
+    T* p_tmp = reinterpret_cast<T*>(ws + L.p_tmp);
+    uint8_t* known[2] = {reinterpret_cast<uint8_t*>(ws + L.known), reinterpret_cast<uint8_t*>(ws + L.known) + n};
+    T* pres[2] = {p_all, p_tmp};
+    closure_init<T><<<grid_for(n, 256), 256, 0, s>>>(p, rho_all, static_cast<T>(prm.surface_threshold * prm.rho0),
+                                                     known[0]);
+    TSPH_LAUNCH_CHECK();
+    const int donors = static_cast<int>(prm.surface_donors);
+    const int64_t passes = donors == 0 ? (prm.surface_layers > 1 ? prm.surface_layers : 1) : 1;
+    for (int64_t k = 0; k < passes; ++k) {
+      closure_pass<T, D><<<grid_for(n, B), B, 0, s>>>(p, pm, io.rowptr, io.entries, rho_all, donors,
+                                                      pres[k & 1], known[k & 1], pres[(k + 1) & 1],
+                                                      known[(k + 1) & 1]);
+      TSPH_LAUNCH_CHECK();
+    }
+    if (passes & 1) {
+      TSPH_CUDA_CHECK(cudaMemcpyAsync(p_all, p_tmp, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    }
+  }
   T* face = (prm.flags & TSPH_RHS_SPLIT) ? static_cast<T*>(io.face_pressure) : nullptr;
   if (nw) {
     wall_kernel<T, D><<<grid_for(nw, B), B, 0, s>>>(p, pm, io.rowptr, io.entries,
@@ -534,6 +694,14 @@ int tsph_wcsph_rhs(const tsph_wcsph_params* prm, const tsph_wcsph_io* io, void* 
   if (ws_bytes < tsph_wcsph_workspace_bytes(prm)) return TSPH_ERR_WORKSPACE;
   if (prm->n_wall > 0 && !io->wall) return TSPH_ERR_ARG;
   if ((prm->flags & TSPH_RHS_SPLIT) && prm->n_wall > 0 && (!io->reaction || !io->face_pressure))
+    return TSPH_ERR_ARG;
+  if ((prm->flags & TSPH_RHS_COMPRESSION) &&
+      (prm->dim != 2 || !io->compression_out || !(prm->compression_kref > 0.0) ||
+       (prm->compression_rule != 0 && prm->compression_rule != 1) || prm->diffusion_scale > 0.0 ||
+       (prm->flags & (TSPH_RHS_RENORMALIZE | TSPH_RHS_BOUNDARY_DENSITY)) || io->density_offset))
+    return TSPH_ERR_ARG;
+  if ((prm->flags & TSPH_RHS_SURFACE_CLOSURE) &&
+      (prm->dim != 2 || prm->surface_donors < 0 || prm->surface_donors > 2 || prm->surface_layers > 1024))
     return TSPH_ERR_ARG;
   if (prm->n_fluid == 0) return TSPH_OK;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);

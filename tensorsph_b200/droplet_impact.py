@@ -7,9 +7,9 @@ return contract.  ``rhs`` runs entirely in CUDA (``csrc/wcsph.cu``): the pair
 list is turned into per-particle gather rows once, then four fused kernels
 produce density (+ diffusion), the Adami wall state, and the acceleration.
 
-Options of the reference ``rhs`` that belong to other subsystems -- the
-compression density regularisation, the free-surface pressure closure and CSF
-surface tension -- raise ``NotImplementedError`` instead of being ignored.
+The compression density regularisation and the free-surface pressure
+closure run as two more kernels between the density and the wall pass; CSF
+surface tension runs through the 2-D CSF drop-in over the fluid pairs.
 """
 from __future__ import annotations
 
@@ -423,22 +423,24 @@ def _wall_mass_value(cfg: Config) -> float:
 
 def rhs(pos, vel, mass, cfg: Config, pairs=None, wall=None, dt=None, wall_vel=None,
         wall_accel=None, state=None, split: bool = False, wrap_width: float | None = None,
-        nu_field: torch.Tensor | None = None, density_offset: torch.Tensor | None = None):
+        nu_field: torch.Tensor | None = None, density_offset: torch.Tensor | None = None,
+        *, _self_donor: bool = False):
     """2-D WCSPH right-hand side on the GPU; returns ``(rho, pressure, acc)``
     (plus ``{"reaction", "face_pressure"}`` when ``split``), on ``pos``'s device.
 
-    Contract and arithmetic of droplet_impact.py:810-1228.
+    Contract and arithmetic of droplet_impact.py:810-1228.  With
+    ``density_regularization="compression"`` the call reads the inverse
+    reference compression from ``state["compression"]`` (a fresh
+    ``CompressionRegularization`` when absent) and writes the new one there,
+    the particle count to ``state["compression_counted"]``.
+    ``_self_donor``: the free-surface closure's "all" donors include the
+    receiver itself, as in the dense formulation (``rhs_all_pairs``).
     """
     h = cfg.h_factor * cfg.dx
     n = pos.shape[0]
     step_dt = cfg.dt if dt is None else float(dt)
     if pos.shape[1] != 2:
         raise ValueError(f"rhs implements 2-D smoothing only, got {pos.shape[1]} dimensions")
-    if cfg.density_regularization != "none":
-        raise NotImplementedError("density_regularization='compression' is not part of the "
-                                  "B200 particle pass")
-    if cfg.surface_pressure_closure:
-        raise NotImplementedError("surface_pressure_closure is not part of the B200 particle pass")
     if cfg.surface_tension_coefficient > 0.0 and cfg.csf_scheme != "consistent":
         raise NotImplementedError("the neighbour-count CSF scheme (csf_scheme='legacy') is not part of "
                                   "the B200 particle pass")
@@ -499,6 +501,32 @@ def rhs(pos, vel, mass, cfg: Config, pairs=None, wall=None, dt=None, wall_vel=No
             raise ValueError("density_offset must have the fluid dtype")
         if cfg.density_regularization != "none" or cfg.density_renormalization:
             raise ValueError("density_offset requires unnormalised summation density")
+    compression = cfg.density_regularization != "none" and not empty
+    if compression:
+        # droplet_impact.py:982-1006
+        from .compression_regularization import NORMALIZATIONS, RULES, CompressionRegularization
+        if cfg.density_regularization != "compression":
+            raise ValueError(f"unknown density_regularization {cfg.density_regularization!r};"
+                             " expected 'none' or 'compression'")
+        if cfg.density_renormalization:
+            raise ValueError("density_regularization='compression' replaces the summation density; "
+                             "combining it with density_renormalization would normalise an "
+                             "already-normalised field")
+        if cfg.compression_regularization_rule not in RULES:
+            raise ValueError(f"unknown compression_regularization_rule "
+                             f"{cfg.compression_regularization_rule!r}; expected one of {RULES}")
+        if cfg.compression_normalization not in NORMALIZATIONS:
+            raise ValueError(f"unknown compression_normalization {cfg.compression_normalization!r}; "
+                             f"expected one of {NORMALIZATIONS}")
+        if cfg.density_diffusion > 0.0:
+            raise ValueError("density_regularization='compression' and density_diffusion are two "
+                             "different ways of obtaining the density; pick one")
+        if cfg.compression_regularization_rule == "free_stream":
+            raise ValueError("rule 'free_stream' needs an indicator array")
+        regularizer = None if state is None else state.get("compression")
+        if regularizer is None:
+            regularizer = CompressionRegularization(rule=cfg.compression_regularization_rule,
+                                                    normalization=cfg.compression_normalization)
 
     rowptr, entries = symmetric_rows(pairs_dev, n + nw)
     prm = _lib.WcsphParams()
@@ -513,7 +541,21 @@ def rhs(pos, vel, mass, cfg: Config, pairs=None, wall=None, dt=None, wall_vel=No
             flags |= _lib.RHS_SPLIT
         if wrap_width is not None:
             flags |= _lib.RHS_WRAP_X
+        if compression:
+            flags |= _lib.RHS_COMPRESSION
+        if cfg.surface_pressure_closure:
+            flags |= _lib.RHS_SURFACE_CLOSURE
     prm.flags = flags
+    comp_out = None
+    if compression:
+        prm.compression_rule = 1 if cfg.compression_regularization_rule == "free_surface" else 0
+        prm.compression_kref = (float(regularizer.inverse_reference_compression)
+                                if cfg.compression_normalization == "reference_mean" else 1.0)
+        comp_out = torch.empty(2, dtype=torch.float64, device=dev)
+    literal = cfg.surface_pressure_donors == "all"
+    prm.surface_donors = (2 if _self_donor else 1) if literal else 0
+    prm.surface_layers = max(1, int(cfg.surface_pressure_layers))
+    prm.surface_threshold = float(cfg.surface_pressure_threshold)
     prm.diffusion_form = 1 if cfg.density_diffusion_form == "antuono" else 0
     prm.h = h
     prm.sigma = 10.0 / (7.0 * math.pi * h * h)
@@ -538,11 +580,18 @@ def rhs(pos, vel, mass, cfg: Config, pairs=None, wall=None, dt=None, wall_vel=No
     io = _lib.WcsphIO(P.data_ptr(), V.data_ptr(), M.data_ptr(), _lib.ptr(Wp), _lib.ptr(keep[0]),
                       _lib.ptr(keep[1]), _lib.ptr(keep[2]), _lib.ptr(keep[3]), rowptr.data_ptr(),
                       entries.data_ptr(), rho.data_ptr(), pressure.data_ptr(), acc.data_ptr(),
-                      _lib.ptr(reaction), _lib.ptr(face))
+                      _lib.ptr(reaction), _lib.ptr(face), _lib.ptr(comp_out))
     L = _lib.lib()
     ws = _lib.workspace(L.tsph_wcsph_workspace_bytes(ctypes.byref(prm)), dev)
     _lib.check(L.tsph_wcsph_rhs(ctypes.byref(prm), ctypes.byref(io), ws.data_ptr(), ws.numel(),
                                 _lib.stream(dev)), "tsph_wcsph_rhs")
+    if compression:
+        # the reduce writes the scalar after this call consumed it
+        written, counted = comp_out.tolist()
+        regularizer.inverse_reference_compression = written
+        if state is not None:
+            state["compression"] = regularizer
+            state["compression_counted"] = int(counted)
     if cfg.surface_tension_coefficient > 0.0 and not empty:
         # droplet_impact.py:1210-1222: the consistent CSF over the fluid pairs
         # of the step's list, with the configuration's options and the walls
@@ -569,18 +618,17 @@ def rhs_all_pairs(pos, vel, mass, cfg: Config, dt=None):
 
     The kernel vanishes beyond 2h, so this is the pair pass over every pair
     within 2h (the device all-pairs search) with the dense formulation's
-    choices: the Molteni diffusion term whatever form is configured, and no
+    choices: the Molteni diffusion term whatever form is configured, no
     density renormalisation, boundary-consistent density, density
-    regularisation or surface tension."""
+    regularisation or surface tension, and a free-surface closure whose pair
+    set includes each particle with itself (droplet_impact.py:1255-1259)."""
     from dataclasses import replace
     from .neighbor_search import brute_force_pairs
-    if cfg.surface_pressure_closure:
-        raise NotImplementedError("surface_pressure_closure is not part of the B200 particle pass")
     dense = replace(cfg, density_diffusion_form="molteni", density_renormalization=False,
                     boundary_consistent_density=False, density_regularization="none",
                     surface_tension_coefficient=0.0)
     pairs = brute_force_pairs(pos, 2.0 * cfg.h_factor * cfg.dx)
-    return rhs(pos, vel, mass, dense, pairs=pairs.to(pos.device), dt=dt)
+    return rhs(pos, vel, mass, dense, pairs=pairs.to(pos.device), dt=dt, _self_donor=True)
 
 
 # -------------------------------------------------------------- boundary ---

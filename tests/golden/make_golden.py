@@ -756,10 +756,14 @@ def dense_cases(di):
     """rhs_all_pairs (droplet_impact.py:1232-1281), the dense O(N^2)
     formulation without walls, on seeded jittered blocks in FP64: plain, with
     Molteni diffusion, with the "antuono" form selected (the dense
-    formulation keeps the Molteni term) and with viscosity."""
+    formulation keeps the Molteni term), with viscosity, and with the
+    free-surface pressure closure ("interior" and "all" donors, whose dense
+    pair set holds each particle with itself)."""
     data = {}
     variants = [dict(), dict(density_diffusion=0.1), dict(density_diffusion=0.1, density_diffusion_form="antuono"),
-                dict(viscosity=1e-3, density_diffusion=0.05)]
+                dict(viscosity=1e-3, density_diffusion=0.05),
+                dict(surface_pressure_closure=True, density_diffusion=0.05),
+                dict(surface_pressure_closure=True, surface_pressure_donors="all")]
     for k, o in enumerate(variants):
         g = torch.Generator().manual_seed(700 + k)
         dx = 0.02
@@ -869,6 +873,57 @@ def dam3d_run_case(d3):
             "max_density_compression": np.float64(run.max_density_compression)}
 
 
+REGULARIZED_OPTION_SETS = [
+    dict(density_regularization="compression"),
+    dict(density_regularization="compression", compression_regularization_rule="internal",
+         compression_normalization="none", wall_friction=0.5),
+    dict(surface_pressure_closure=True, density_diffusion=0.1),
+    dict(surface_pressure_closure=True, surface_pressure_donors="all"),
+    dict(surface_pressure_closure=True, surface_pressure_layers=3, boundary_consistent_density=True),
+]
+
+
+def regularized_cases(di, db):
+    """2-D ``rhs`` with the compression density regularisation
+    (droplet_impact.py:982-1028, two calls sharing one ``state``: the second
+    uses the inverse reference compression the first wrote) and the
+    free-surface pressure closure (:1030-1037, 429-492) on jittered resting
+    columns with walls, FP32 and FP64."""
+    data = {}
+    k = 0
+    for dtype in (torch.float32, torch.float64):
+        torch.set_default_dtype(dtype)
+        try:
+            for oi, opts in enumerate(REGULARIZED_OPTION_SETS):
+                cfg = db.DamBreakConfig(dx=0.05, column_width=0.5, column_height=0.6,
+                                        pool_width=1.2, tank_height=0.9, sound_speed=20.0,
+                                        viscosity=1e-3, dt=2e-4, **opts)
+                pos, mass = db.make_column(cfg, torch.device("cpu"))
+                wall = di.wall_lattice(cfg, torch.device("cpu"), top=cfg.tank_top())
+                g = torch.Generator().manual_seed(61 + oi)
+                pos = pos + 0.1 * cfg.dx * torch.randn(pos.shape, generator=g).to(dtype)
+                vel = 0.3 * torch.randn(pos.shape, generator=g).to(dtype)
+                h = cfg.h_factor * cfg.dx
+                cache = di.PairListCache(2.0 * h, 0.25 * h, fluid_count=pos.shape[0])
+                pairs, _ = cache.get(torch.cat((pos, wall)))
+                state = {}
+                for call in (0, 1):
+                    out = di.rhs(pos, vel, mass, cfg, pairs=pairs, wall=wall, dt=cfg.dt, state=state)
+                    data[f"c{k}_rho{call}"], data[f"c{k}_p{call}"], data[f"c{k}_acc{call}"] = map(_np, out[:3])
+                    if "compression" in state:
+                        data[f"c{k}_kref{call}"] = np.float64(state["compression"].inverse_reference_compression)
+                        data[f"c{k}_counted{call}"] = np.int64(state["compression_counted"])
+                data[f"c{k}_pos"], data[f"c{k}_vel"] = _np(pos), _np(vel)
+                data[f"c{k}_mass"], data[f"c{k}_wall"] = _np(mass), _np(wall)
+                data[f"c{k}_pairs"] = _np(pairs)
+                data[f"c{k}_opts"] = np.int64(oi)
+                k += 1
+        finally:
+            torch.set_default_dtype(torch.float32)
+    data["count"] = np.int64(k)
+    return data
+
+
 def adaptive_run_case(db):
     """The reference's own 2-D dam-break loop with adaptive_dt (dam_break.py:
     362-465) in FP64 on the tank of its Courant-limit test (dx = 0.04,
@@ -967,6 +1022,7 @@ def main(src, families=None):
         "dense": lambda: dense_cases(di),
         "dt": lambda: dt_cases(di),
         "adaptive_run": lambda: adaptive_run_case(db),
+        "regularized": lambda: regularized_cases(di, db),
     }
     for name in families or makers:
         np.savez_compressed(OUT / f"{name}.npz", **makers[name](), **meta)

@@ -82,8 +82,8 @@ def test_struct_sizes_match_header():
     """ctypes mirrors of the parameter structs have the C layout (all 8-byte fields)."""
     from tensorsph_b200 import _lib
     assert ctypes.sizeof(_lib.Grid) == 8 * (4 + 1 + 3 + 3 + 3 + 3 + 4)
-    assert ctypes.sizeof(_lib.WcsphParams) == 8 * (6 + 14)
-    assert ctypes.sizeof(_lib.WcsphIO) == 8 * 15
+    assert ctypes.sizeof(_lib.WcsphParams) == 8 * (6 + 14 + 5)
+    assert ctypes.sizeof(_lib.WcsphIO) == 8 * 16
     assert ctypes.sizeof(_lib.ThreedParams) == 8 * (9 + 8 + 6)
     assert ctypes.sizeof(_lib.ShiftParams) == 8 * 9
     assert ctypes.sizeof(_lib.ClampParams) == 8 * (3 + 3 + 3 + 1 + 1 + 3 + 3 + 1)

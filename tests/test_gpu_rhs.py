@@ -235,3 +235,46 @@ def test_rhs_all_pairs_matches_reference(golden, gpu):
         for name, t in (("p", p), ("acc", acc)):
             ref = g[f"c{k}_{name}"]
             assert np.abs(t.cpu().numpy() - ref).max() <= 1e-12 * max(np.abs(ref).max(), 1.0), (k, name)
+
+
+def test_regularized_rhs_matches_reference(gpu, golden, default_dtype):
+    """The compression density regularisation (rules "free_surface" and
+    "internal", normalisations "reference_mean" and "none") and the
+    free-surface pressure closure ("interior" with 2 and 3 passes, "all",
+    with diffusion, with the boundary-consistent density) against the
+    reference's rhs (tests/golden/regularized.npz), FP32 and FP64: two calls
+    sharing one state, so the second uses the inverse reference compression
+    the first wrote; that scalar and the count are checked too."""
+    from tensorsph_b200.droplet_impact import rhs
+    from tests.golden.make_golden import REGULARIZED_OPTION_SETS
+    g = golden("regularized")
+    for k in range(int(g["count"])):
+        default_dtype(torch.from_numpy(g[f"c{k}_pos"][:1]).dtype)
+        cfg = _cfg(dx=0.05, sound_speed=20.0, viscosity=1e-3, dt=2e-4,
+                   **REGULARIZED_OPTION_SETS[int(g[f"c{k}_opts"])])
+        t = {name: torch.from_numpy(g[f"c{k}_{name}"]).to(gpu) for name in ("pos", "vel", "mass", "wall", "pairs")}
+        tr, tf = TOL[g[f"c{k}_pos"].dtype]
+        state = {}
+        for call in (0, 1):
+            out = rhs(t["pos"], t["vel"], t["mass"], cfg, pairs=t["pairs"], wall=t["wall"], dt=cfg.dt, state=state)
+            assert rel_err(out[0].cpu(), g[f"c{k}_rho{call}"]) < tr, (k, call, "rho")
+            assert rel_err(out[1].cpu(), g[f"c{k}_p{call}"], bulk(cfg)) < tr, (k, call, "p")
+            assert rel_err(out[2].cpu(), g[f"c{k}_acc{call}"]) < tf, (k, call, "acc")
+            if f"c{k}_kref{call}" in g:
+                kref = state["compression"].inverse_reference_compression
+                assert kref == pytest.approx(float(g[f"c{k}_kref{call}"]), rel=tr), (k, call)
+                assert state["compression_counted"] == int(g[f"c{k}_counted{call}"]), (k, call)
+
+
+def test_regularized_rhs_refusals(gpu):
+    """The reference's ValueErrors for the compression regularisation."""
+    from tensorsph_b200.droplet_impact import rhs
+    pos = torch.tensor([[0.0, 0.0], [0.04, 0.0]], dtype=torch.float64, device=gpu)
+    for bad in (dict(density_regularization="shepard"),
+                dict(density_regularization="compression", density_renormalization=True),
+                dict(density_regularization="compression", density_diffusion=0.1),
+                dict(density_regularization="compression", compression_regularization_rule="free_stream"),
+                dict(density_regularization="compression", compression_normalization="median")):
+        with pytest.raises(ValueError):
+            rhs(pos, torch.zeros_like(pos), torch.full((2,), 2.5, dtype=torch.float64, device=gpu),
+                _cfg(dx=0.05, **bad))

@@ -407,3 +407,31 @@ def test_rhs_with_csf_oracle_matches_reference(golden):
         assert np.abs(rho - g[f"c{k}_rho"]).max() <= 1e-12 * cfg.rho0
         ref = g[f"c{k}_acc"]
         assert np.abs(acc + a_st - ref).max() <= 1e-9 * np.abs(a_st).max(), k
+
+
+REGULARIZED_DEFAULTS = dict(density_regularization="none", compression_regularization_rule="free_surface",
+                            compression_normalization="reference_mean", surface_pressure_closure=False,
+                            surface_pressure_threshold=0.99, surface_pressure_donors="interior",
+                            surface_pressure_layers=2)
+
+
+def test_regularized_rhs_matches_reference(golden):
+    """The oracle's compression regularisation and free-surface closure
+    against the reference's rhs (tests/golden/regularized.npz): two calls
+    sharing one state, the written inverse reference compression and count."""
+    from tests.golden.make_golden import REGULARIZED_OPTION_SETS
+    g = golden("regularized")
+    for k in range(int(g["count"])):
+        opts = {**REGULARIZED_DEFAULTS, **REGULARIZED_OPTION_SETS[int(g[f"c{k}_opts"])]}
+        cfg = _cfg2d(opts)
+        tol = 1e-12 if g[f"c{k}_pos"].dtype == np.float64 else 2e-5
+        state = {}
+        for call in (0, 1):
+            out = op.rhs(g[f"c{k}_pos"], g[f"c{k}_vel"], g[f"c{k}_mass"], cfg, pairs=g[f"c{k}_pairs"],
+                         wall=g[f"c{k}_wall"], dt=cfg.dt, state=state)
+            assert rel_err(out[0], g[f"c{k}_rho{call}"]) < tol, (k, call)
+            assert rel_err(out[1], g[f"c{k}_p{call}"]) < max(tol, 1e-11) * 50, (k, call)
+            assert rel_err(out[2], g[f"c{k}_acc{call}"]) < max(tol, 1e-11) * 50, (k, call)
+            if f"c{k}_kref{call}" in g:
+                assert state["inverse_reference"] == pytest.approx(float(g[f"c{k}_kref{call}"]), rel=tol)
+                assert state["counted"] == int(g[f"c{k}_counted{call}"])
