@@ -137,7 +137,8 @@ enum {
   TSPH_RHS_COMPRESSION = 32,     /* Config.density_regularization="compression" */
                                  /* (droplet_impact.py:982-1028; 2-D)           */
   TSPH_RHS_SURFACE_CLOSURE = 64  /* Config.surface_pressure_closure             */
-                                 /* (droplet_impact.py:429-492, 1030-1037; 2-D) */
+                                 /* (droplet_impact.py:429-492, 1030-1037;      */
+                                 /* dam_break_3d.py:339-342)                    */
 };
 
 typedef struct {

@@ -469,6 +469,10 @@ def rhs_3d(pos, vel, mass, cfg, pairs=None, wall=None, dt=None, return_wall_forc
         rate = molteni_rate(rho, mass, radial, distance[ff] ** 2, i[ff], j[ff], scale)
         rho = np.maximum(rho + T(step_dt) * rate, T(0.1 * cfg.rho0))
     pressure = tait(rho, cfg.rho0, cfg.sound_speed, cfg.gamma)
+    if getattr(cfg, "surface_pressure_closure", False):
+        # dam_break_3d.py:339-342
+        ff = (i < n) & (j < n)
+        pressure = free_surface_pressure(rho, pressure, delta[ff], wij[ff], i[ff], j[ff], cfg)
     if nw:
         i_fluid = i < n
         crossing = i_fluid != (j < n)

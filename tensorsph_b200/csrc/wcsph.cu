@@ -701,7 +701,7 @@ int tsph_wcsph_rhs(const tsph_wcsph_params* prm, const tsph_wcsph_io* io, void* 
        (prm->flags & (TSPH_RHS_RENORMALIZE | TSPH_RHS_BOUNDARY_DENSITY)) || io->density_offset))
     return TSPH_ERR_ARG;
   if ((prm->flags & TSPH_RHS_SURFACE_CLOSURE) &&
-      (prm->dim != 2 || prm->surface_donors < 0 || prm->surface_donors > 2 || prm->surface_layers > 1024))
+      (prm->surface_donors < 0 || prm->surface_donors > 2 || prm->surface_layers > 1024))
     return TSPH_ERR_ARG;
   if (prm->n_fluid == 0) return TSPH_OK;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);

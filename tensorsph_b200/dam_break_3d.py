@@ -144,8 +144,9 @@ def wall_lattice_3d(cfg: DamBreak3DConfig, device, top: float | None = None) -> 
 
 def rhs_3d(pos, vel, mass, cfg: DamBreak3DConfig, pairs=None, wall=None, dt=None, *,
            return_wall_force=False):
-    """3-D density, pressure and acceleration on the GPU (dam_break_3d.py:290-422);
-    returns ``(rho, p, acc[, reaction])`` on ``pos``'s device."""
+    """3-D density, pressure and acceleration on the GPU (dam_break_3d.py:290-422),
+    with the free-surface pressure closure when configured; returns
+    ``(rho, p, acc[, reaction])`` on ``pos``'s device."""
     n = pos.shape[0]
     nw = wall.shape[0] if wall is not None else 0
     h = cfg.h_factor * cfg.dx
@@ -153,8 +154,6 @@ def rhs_3d(pos, vel, mass, cfg: DamBreak3DConfig, pairs=None, wall=None, dt=None
     if cfg.density_diffusion > 0.0 and cfg.density_diffusion_form != "molteni":
         raise ValueError("density_diffusion_rate implements the 'molteni' form only; the "
                          f"configured form is {cfg.density_diffusion_form!r}")
-    if cfg.surface_pressure_closure:
-        raise NotImplementedError("surface_pressure_closure is not part of the B200 particle pass")
     out_device = pos.device
     dev = _lib.cuda_device(pos)
     dtype = pos.dtype
@@ -172,6 +171,12 @@ def rhs_3d(pos, vel, mass, cfg: DamBreak3DConfig, pairs=None, wall=None, dt=None
     prm = _lib.WcsphParams()
     prm.dim, prm.dtype, prm.n_fluid, prm.n_wall = 3, code, n, nw
     prm.flags = _lib.RHS_WALL_SELF | (_lib.RHS_SPLIT if return_wall_force else 0)
+    if cfg.surface_pressure_closure:
+        # dam_break_3d.py:339-342: the 2-D closure over the fluid pairs
+        prm.flags |= _lib.RHS_SURFACE_CLOSURE
+        prm.surface_donors = 1 if cfg.surface_pressure_donors == "all" else 0
+        prm.surface_layers = max(1, int(cfg.surface_pressure_layers))
+        prm.surface_threshold = float(cfg.surface_pressure_threshold)
     prm.diffusion_form = 0
     prm.h, prm.sigma = h, 1.0 / (math.pi * h ** 3)
     prm.rho0, prm.sound_speed, prm.gamma = cfg.rho0, cfg.sound_speed, cfg.gamma

@@ -147,6 +147,9 @@ def _case_params(*, dim, n_fluid, n_wall, n_obstacle, cfg, h, wall_mass, box_hi,
                  shift_every=0, obstacle=None, first_step=0, adaptive=False):
     if cfg.density_diffusion > 0.0 and cfg.density_diffusion_form != "molteni":
         raise NotImplementedError("the device engine implements the 'molteni' diffusion form only")
+    if getattr(cfg, "density_regularization", "none") != "none" or getattr(cfg, "surface_pressure_closure", False):
+        raise NotImplementedError("density_regularization and surface_pressure_closure are options of the "
+                                  "rhs drop-ins, not of the device engine")
     p = _lib.CaseParams()
     p.dim, p.n_fluid, p.n_wall, p.n_obstacle = dim, n_fluid, n_wall, n_obstacle
     p.shift_every = int(shift_every)
@@ -893,10 +896,9 @@ def run_case(cfg: DamBreak3DConfig, pair_skin_factor: float | None = None, snaps
         from dataclasses import replace
         cfg = replace(cfg, pair_skin_factor=pair_skin_factor)
     if cfg.adaptive_dt:
-        if snapshot_times or checkpoint_path is not None:
-            raise NotImplementedError("snapshots and checkpoints with adaptive_dt are not supported "
-                                      "by the device engine")
-        return _run_3d_adaptive(cfg, obstacle, shift_every, seed, max_neighbors)
+        if checkpoint_path is not None:
+            raise NotImplementedError("checkpoints with adaptive_dt are not supported by the device engine")
+        return _run_3d_adaptive(cfg, obstacle, shift_every, seed, max_neighbors, snapshot_times)
     host = dam_break_3d_host_state(cfg, obstacle, seed)
     prev = None
     if checkpoint_path is not None and resume and Path(checkpoint_path).exists():
@@ -980,14 +982,14 @@ def run_case(cfg: DamBreak3DConfig, pair_skin_factor: float | None = None, snaps
     return run
 
 
-def _run_3d_adaptive(cfg, obstacle, shift_every: int, seed, max_neighbors: int) -> DamBreak3DRun:
+def _run_3d_adaptive(cfg, obstacle, shift_every: int, seed, max_neighbors: int, snapshot_times=None) -> DamBreak3DRun:
     """The 3-D loop with adaptive_dt (dam_break_3d.py:617-711): meters at
     every output_every-th step and at the final one, times from the device."""
     from dataclasses import replace
     eng = DamBreak3DEngine(cfg, obstacle=obstacle, shift_every=shift_every, seed=seed,
                            max_neighbors=max_neighbors, diag_ring=4 * cfg.steps + 1100,
                            host_state=dam_break_3d_host_state(cfg, obstacle, seed))
-    final = _advance_adaptive(eng, eng.case_id, cfg)
+    final, snapshots = _advance_adaptive(eng, eng.case_id, cfg, snapshot_times=snapshot_times or [])
     with torch.cuda.stream(eng.stream):
         x, v, _, _ = eng.state()
         xs, vs = x.cpu(), v.cpu()
@@ -1004,7 +1006,8 @@ def _run_3d_adaptive(cfg, obstacle, shift_every: int, seed, max_neighbors: int) 
         initial_energy=eng.initial_pe, steps_taken=final, simulated_time=float(diag[final, 25]),
         obstacle_force=rec["obstacle_force"], obstacle_impulse=rec["sph_impulse"],
         clamp_impulse=rec["clamp_impulse"], obstacle_clamps=rec["clamps"], tvc_log=rec["tvc_log"],
-        dt_min=float(dts.min()), dt_max=float(dts.max()), max_acoustic_courant=_max_courant(cfg, diag))
+        snapshots=snapshots, dt_min=float(dts.min()), dt_max=float(dts.max()),
+        max_acoustic_courant=_max_courant(cfg, diag))
     masses = eng.spec.mass
     run.final_energy = float(0.5 * (masses[:, None] * vs.square()).sum()
                              + (masses * cfg.gravity * xs[:, 1]).sum())
@@ -1043,29 +1046,56 @@ def _max_courant(cfg, diag) -> float:
     return max(float(diag[k, 26]) * (cfg.sound_speed + float(diag[k, 1])) / h for k in range(diag.shape[0]))
 
 
-def _advance_adaptive(eng, cid, cfg, chunk: int = 64) -> int:
+def _advance_adaptive(eng, cid, cfg, chunk: int = 64, snapshot_times=None):
     """Step an adaptive case until it records its final meters (the step at
-    which the simulated time reaches steps * dt); returns that step.  Steps
-    after it leave the case as it is."""
+    which the simulated time reaches steps * dt); returns that step, and with
+    ``snapshot_times`` also the snapshots.  Steps after the final one leave
+    the case as it is.
+
+    A snapshot target is taken at the first sample step (every
+    ``output_every``-th and the final one) whose starting time reaches it, as
+    dam_break.py:409-414 does: the chunks then end on the sample steps, and
+    the time at the start of step k is read from the meter row of step k-1."""
     max_steps = 4 * cfg.steps + 1000
+    targets = sorted(float(t) for t in (snapshot_times or []))
+    snaps, nxt = [], 0
+
+    def take(t):
+        nonlocal nxt
+        while nxt < len(targets) and t >= targets[nxt] - 1.0e-12:
+            with torch.cuda.stream(eng.stream):
+                x, v = eng.read(cid)[:2]
+                snaps.append((t, x.cpu(), v.cpu()))
+            nxt += 1
+
+    every = max(1, int(cfg.output_every)) if targets else chunk
+    take(0.0)
     done = 0
     while done <= max_steps:
-        n = min(chunk, max_steps + 1 - done)
+        n = min(every - done % every, max_steps + 1 - done)
         eng.step(n)
         done += n
         st = BatchEngine.status(eng, cid)
         if st["finished"]:
-            return int(st["final_step"])
+            final = int(st["final_step"])
+            if targets:
+                with torch.cuda.stream(eng.stream):
+                    take(float(BatchEngine.diagnostics(eng, cid, final, 1).cpu()[0, 25]))
+            return (final, snaps) if snapshot_times is not None else final
+        if nxt < len(targets):
+            with torch.cuda.stream(eng.stream):
+                row = BatchEngine.diagnostics(eng, cid, done - 1, 1).cpu()[0]
+            take(float(row[25]) + float(row[26]))
     raise RuntimeError(f"the adaptive run did not reach {cfg.steps * cfg.dt} s in {max_steps} steps")
 
 
-def _run_2d_adaptive(cfg, max_neighbors: int) -> "DamBreakRun":
+def _run_2d_adaptive(cfg, max_neighbors: int, snapshot_times=None) -> "DamBreakRun":
     """The 2-D loop with adaptive_dt (dam_break.py:367-465): meters at every
     output_every-th step and at the final one, times from the device."""
     spec = dam_break_2d_case(cfg, shift_every=cfg.shift_every)
     eng = BatchEngine(**capacity_for([spec], max_neighbors=max_neighbors, diag_ring=4 * cfg.steps + 1100))
     cid = eng.add(spec)
-    final = _advance_adaptive(eng, cid, cfg)
+    final, snapshots = _advance_adaptive(eng, cid, cfg, snapshot_times=snapshot_times or [])
     with torch.cuda.stream(eng.stream):
         x = eng.read(cid)[0].cpu()
         diag = eng.diagnostics(cid, 0, final + 1).cpu()
@@ -1078,7 +1108,8 @@ def _run_2d_adaptive(cfg, max_neighbors: int) -> "DamBreakRun":
                       rebuilds=int(diag[final, 10]), max_speed=float(diag[:, 1].max()),
                       max_density_compression=float(diag[:, 0].max()) / cfg.rho0 - 1.0,
                       final_positions=x, steps_taken=final, simulated_time=float(diag[final, 25]),
-                      dt_min=float(dts.min()), dt_max=float(dts.max()), max_acoustic_courant=_max_courant(cfg, diag))
+                      snapshots=snapshots, dt_min=float(dts.min()), dt_max=float(dts.max()),
+                      max_acoustic_courant=_max_courant(cfg, diag))
     every = int(cfg.tvc_every or 0)
     applied = [k for k in range(1, final) if every and k % every == 0]
     if applied:
@@ -1095,9 +1126,7 @@ def run_dam_break_2d(cfg, *, snapshot_times=None, max_neighbors: int = 64) -> Da
     correction (``tvc_every``, scopes "all", "bulk_g" and "bulk", the
     ``truncated_linear`` limiter, the clip) each run, not both together."""
     if cfg.adaptive_dt:
-        if snapshot_times:
-            raise NotImplementedError("snapshot_times with adaptive_dt are not supported by the device engine")
-        return _run_2d_adaptive(cfg, max_neighbors)
+        return _run_2d_adaptive(cfg, max_neighbors, snapshot_times)
     spec = dam_break_2d_case(cfg, shift_every=cfg.shift_every)
     eng = BatchEngine(**capacity_for([spec], max_neighbors=max_neighbors,
                                      diag_ring=max(cfg.steps + 1, 1)))

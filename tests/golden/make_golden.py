@@ -226,6 +226,42 @@ def rhs3d_cases(d3, di):
     return data
 
 
+def rhs3d_closure_cases(d3, di):
+    """rhs_3d with the free-surface pressure closure (dam_break_3d.py:
+    339-342) on jittered 3-D columns with walls, FP32 and FP64: "interior"
+    donors with diffusion and friction, "all" donors."""
+    data = {}
+    k = 0
+    for dtype in (torch.float32, torch.float64):
+        for opts in (dict(surface_pressure_closure=True, density_diffusion=0.1, wall_friction=0.3),
+                     dict(surface_pressure_closure=True, surface_pressure_donors="all")):
+            torch.set_default_dtype(dtype)
+            try:
+                cfg = d3.DamBreak3DConfig(dx=0.04, tank_height=0.4, tank_depth=0.2,
+                                          column_width=0.2, column_depth=0.2,
+                                          column_height=0.24, pool_width=0.5,
+                                          sound_speed=15.0, viscosity=1e-3, dt=1e-4, **opts)
+                pos, mass = d3.make_column_3d(cfg, torch.device("cpu"), seed=5)
+                wall = d3.wall_lattice_3d(cfg, torch.device("cpu"))
+                g = torch.Generator().manual_seed(90 + k)
+                pos = pos + 0.1 * cfg.dx * torch.randn(pos.shape, generator=g).to(dtype)
+                vel = 0.2 * torch.randn(pos.shape, generator=g).to(dtype)
+                h = cfg.h_factor * cfg.dx
+                cache = di.PairListCache(2.0 * h, 0.25 * h, fluid_count=pos.shape[0])
+                pairs, _ = cache.get(torch.cat((pos, wall)))
+                rho, p, acc, reaction = d3.rhs_3d(pos, vel, mass, cfg, pairs=pairs, wall=wall,
+                                                  dt=cfg.dt, return_wall_force=True)
+                for name, t in dict(pos=pos, vel=vel, mass=mass, wall=wall, pairs=pairs,
+                                    rho=rho, p=p, acc=acc, reaction=reaction).items():
+                    data[f"c{k}_{name}"] = _np(t)
+                data[f"c{k}_opts"] = np.array(repr(sorted(opts.items())))
+                k += 1
+            finally:
+                torch.set_default_dtype(torch.float32)
+    data["count"] = np.int64(k)
+    return data
+
+
 def threed_cases(t3):
     data = {}
     k = 0
@@ -1023,6 +1059,7 @@ def main(src, families=None):
         "dt": lambda: dt_cases(di),
         "adaptive_run": lambda: adaptive_run_case(db),
         "regularized": lambda: regularized_cases(di, db),
+        "rhs3d_closure": lambda: rhs3d_closure_cases(d3, di),
     }
     for name in families or makers:
         np.savez_compressed(OUT / f"{name}.npz", **makers[name](), **meta)

@@ -103,3 +103,16 @@ def test_step_limits_match_reference(golden):
                 rows.append([di.acoustic_dt_limit(cfg, speed), di.capillary_dt_limit(cfg), di.stable_dt(cfg, speed),
                              di.next_dt(cfg, dt, speed)])
     assert np.array_equal(np.asarray(rows), g)
+
+
+def test_engine_refuses_rhs_only_options():
+    """The compression regularisation and the free-surface closure are
+    options of the rhs drop-ins: a device case built with either is refused,
+    not run without it."""
+    from tensorsph_b200.engine import dam_break_2d_case, droplet_impact_case
+    with pytest.raises(NotImplementedError):
+        dam_break_2d_case(_dam2d(surface_pressure_closure=True))
+    with pytest.raises(NotImplementedError):
+        dam_break_2d_case(_dam2d(density_regularization="compression"))
+    with pytest.raises(NotImplementedError):
+        droplet_impact_case(_drop(surface_pressure_closure=True))

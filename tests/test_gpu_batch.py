@@ -464,3 +464,26 @@ def test_adaptive_dam_break_follows_reference_run(golden, gpu):
     eng.close()
     assert final == run.steps_taken
     assert_adaptive_rows(cfg, diag, final)
+
+
+def test_adaptive_snapshots(gpu):
+    """snapshot_times in an adaptive run (dam_break.py:409-414): each target
+    is taken at the first sample step whose starting time reaches it, the
+    last at the final step; the copies are the states there, so the final
+    one equals the run's final positions and a target past the end is
+    dropped."""
+    from tensorsph_b200.engine import run_dam_break_2d
+    cfg = _adaptive_tank()
+    targets = [0.0, 0.06, 0.1, 0.25, 1.0]
+    saved = torch.get_default_dtype()
+    torch.set_default_dtype(torch.float64)
+    try:
+        run = run_dam_break_2d(cfg, snapshot_times=targets)
+    finally:
+        torch.set_default_dtype(saved)
+    times = [t for t, _, _ in run.snapshots]
+    assert len(times) == 4
+    expect = [next(t for t in run.times if t >= want - 1e-12) for want in targets[:4]]
+    assert times == expect and times[-1] == run.times[-1] == run.simulated_time
+    assert torch.equal(run.snapshots[-1][1], run.final_positions)
+    assert torch.equal(run.snapshots[0][1], torch.as_tensor(_config1_start(cfg)))

@@ -435,3 +435,21 @@ def test_regularized_rhs_matches_reference(golden):
             if f"c{k}_kref{call}" in g:
                 assert state["inverse_reference"] == pytest.approx(float(g[f"c{k}_kref{call}"]), rel=tol)
                 assert state["counted"] == int(g[f"c{k}_counted{call}"])
+
+
+def test_rhs3d_closure_matches_reference(golden):
+    """The oracle's rhs_3d with the free-surface closure against the
+    reference's (tests/golden/rhs3d_closure.npz)."""
+    import ast
+    g = golden("rhs3d_closure")
+    for k in range(int(g["count"])):
+        opts = {**REGULARIZED_DEFAULTS, "wall_friction": 0.0, "density_diffusion": 0.0,
+                **dict(ast.literal_eval(str(g[f"c{k}_opts"])))}
+        cfg = SimpleNamespace(dx=0.04, h_factor=1.3, rho0=1000.0, sound_speed=15.0, gamma=7.0, gravity=9.81,
+                              viscosity=1e-3, dt=1e-4, density_diffusion_form="molteni", density_calibration=True,
+                              **opts)
+        out = op.rhs_3d(g[f"c{k}_pos"], g[f"c{k}_vel"], g[f"c{k}_mass"], cfg, pairs=g[f"c{k}_pairs"],
+                        wall=g[f"c{k}_wall"], dt=cfg.dt, return_wall_force=True)
+        tol = 1e-12 if g[f"c{k}_pos"].dtype == np.float64 else 2e-5
+        for got, name in zip(out, ("rho", "p", "acc", "reaction")):
+            assert rel_err(got, g[f"c{k}_{name}"]) < tol * (1 if name == "rho" else 50), (k, name)
