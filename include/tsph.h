@@ -570,6 +570,11 @@ typedef struct {
                                        /* step limits (may be +inf)                  */
   double dt_growth, dt_safety;         /* next_dt's growth cap and safety factor     */
   double target_time;                  /* steps * dt: the run ends at this time      */
+  /* DamBreakConfig.shift_v_ref (dam_break.py:425-427): with shift_vref_given
+   * the shift's reference speed is shift_vref, else max(|v|max,
+   * shift_vref_floor)                                                       */
+  int64_t shift_vref_given;
+  double shift_vref;
 } tsph_case_params;
 
 typedef struct tsph_engine tsph_engine; /* opaque host handle */

@@ -167,7 +167,8 @@ class CaseParams(ctypes.Structure):
                 ("csf_contact_model", c_int64), ("csf_contact_angle", c_double), ("csf_contact_reach", c_double),
                 ("csf_wall_area", c_double), ("csf_traction_calibration", c_double),
                 ("adaptive_dt", c_int64), ("courant_h", c_double), ("dt_limit", c_double),
-                ("dt_growth", c_double), ("dt_safety", c_double), ("target_time", c_double)]
+                ("dt_growth", c_double), ("dt_safety", c_double), ("target_time", c_double),
+                ("shift_vref_given", c_int64), ("shift_vref", c_double)]
 
 
 _SIGNATURES = {

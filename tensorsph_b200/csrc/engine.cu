@@ -58,6 +58,8 @@ struct CaseDev {
   double cell, rc2, skin_half;
   double dt, gravity, box_hi[3], tol, ob_lo[3], ob_hi[3], ob_eps;
   double shift_strength_h_dt, shift_cap, shift_fs, vref_floor;
+  int vref_given;          // a fixed shift reference speed (vref_fixed)
+  double vref_fixed;
   int ncx, ncy, ncz, key_off;
   int fluid_begin, n_fluid, wall_begin, n_wall;
   int ob_begin, n_ob, has_ob, shift_every;
@@ -2035,7 +2037,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_shift_apply(Dev e) {
   const CaseDev& C = e.cases[e.shift_slot];
   const double cref = t.cref[0];
   const float thresh = static_cast<float>(C.shift_fs * cref);
-  const double vref = fmax(t.cref[1], C.vref_floor);
+  const double vref = C.vref_given ? C.vref_fixed : fmax(t.cref[1], C.vref_floor);
   const float mag = static_cast<float>(C.adaptive ? C.shift_strength_h * t.dt_step * vref
                                                   : C.shift_strength_h_dt * vref);
   const float cap = static_cast<float>(C.shift_cap);
@@ -2562,6 +2564,8 @@ CaseDev make_case_dev(const tsph_case_params& p, int64_t* ncells) {
   c.shift_cap = p.shift_limit * p.h;
   c.shift_fs = p.shift_free_surface;
   c.vref_floor = p.shift_vref_floor;
+  c.vref_given = p.shift_vref_given ? 1 : 0;
+  c.vref_fixed = p.shift_vref;
   c.inv_h = static_cast<float>(1.0 / p.h);
   c.sigma = static_cast<float>(p.dim == 3 ? 1.0 / (M_PI * p.h * p.h * p.h) : 10.0 / (7.0 * M_PI * p.h * p.h));
   c.sig2d = static_cast<float>(10.0 / (7.0 * M_PI * p.h * p.h));

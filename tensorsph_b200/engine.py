@@ -214,6 +214,8 @@ def _case_params(*, dim, n_fluid, n_wall, n_obstacle, cfg, h, wall_mass, box_hi,
     p.shift_limit = getattr(cfg, "shift_limit", 0.25)
     p.shift_free_surface = 0.95
     p.shift_vref_floor = 0.05 * cfg.sound_speed
+    if getattr(cfg, "shift_v_ref", None) is not None:
+        p.shift_vref_given, p.shift_vref = 1, float(cfg.shift_v_ref)
     margin = 2.0 * cfg.dx
     for k in range(3):
         if k < dim:
@@ -269,6 +271,8 @@ def dam_break_2d_case(cfg, *, shift_every: int = 0, velocity=None, label: str = 
     from .dam_break import make_column, validate_case
     from .droplet_impact import lattice_mass_unit, wall_lattice
     validate_case(cfg)
+    if cfg.surface_tension_coefficient > 0.0:
+        raise NotImplementedError("surface tension in the dam-break case is not part of the device engine")
     if cfg.density_renormalization or cfg.boundary_consistent_density:
         raise NotImplementedError("density_renormalization and boundary_consistent_density are "
                                   "not part of the device engine")

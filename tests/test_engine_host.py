@@ -116,3 +116,15 @@ def test_engine_refuses_rhs_only_options():
         dam_break_2d_case(_dam2d(density_regularization="compression"))
     with pytest.raises(NotImplementedError):
         droplet_impact_case(_drop(surface_pressure_closure=True))
+
+
+def test_dam_break_2d_shift_reference_speed_and_refusals():
+    """shift_v_ref (dam_break.py:425-427) becomes the case's fixed shift
+    reference speed; surface tension in the dam break is refused."""
+    from tensorsph_b200.engine import dam_break_2d_case
+    p = dam_break_2d_case(_dam2d(), shift_every=1).params
+    assert (p.shift_vref_given, p.shift_vref_floor) == (0, 0.05 * _dam2d().sound_speed)
+    p = dam_break_2d_case(_dam2d(shift_v_ref=0.7), shift_every=1).params
+    assert (p.shift_vref_given, p.shift_vref) == (1, 0.7)
+    with pytest.raises(NotImplementedError):
+        dam_break_2d_case(_dam2d(surface_tension_coefficient=0.07))

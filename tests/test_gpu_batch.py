@@ -487,3 +487,29 @@ def test_adaptive_snapshots(gpu):
     assert times == expect and times[-1] == run.times[-1] == run.simulated_time
     assert torch.equal(run.snapshots[-1][1], run.final_positions)
     assert torch.equal(run.snapshots[0][1], torch.as_tensor(_config1_start(cfg)))
+
+
+def test_2d_shift_reference_speed(gpu):
+    """With shift_v_ref the 2-D shift's reference speed is that constant
+    (dam_break.py:425-427): the shift is linear in it, so the displacement
+    of two steps with shifting (the first shift is after the update of step
+    1) at v_ref = 2 is twice the one at v_ref = 1, to FP32 rounding, and
+    neither equals the default max(|v|max, 0.05 c0)."""
+    from dataclasses import replace
+    from tensorsph_b200.engine import BatchEngine, capacity_for, dam_break_2d_case
+    base = replace(small_2d(), pair_skin_factor=0.0)
+    got = {}
+    for key, cfg, every in (("none", base, 0), ("auto", base, 1), ("one", replace(base, shift_v_ref=1.0), 1),
+                            ("two", replace(base, shift_v_ref=2.0), 1)):
+        spec = dam_break_2d_case(cfg, shift_every=every)
+        eng = BatchEngine(**capacity_for([spec], max_neighbors=64, diag_ring=8))
+        cid = eng.add(spec)
+        eng.step(2)
+        with torch.cuda.stream(eng.stream):
+            got[key] = eng.read(cid)[0].cpu().numpy()
+        eng.close()
+    d1, d2, da = (got[k] - got["none"] for k in ("one", "two", "auto"))
+    scale = np.abs(d2).max()
+    assert scale > 0.0
+    assert np.abs(d2 - 2.0 * d1).max() < 1e-4 * scale
+    assert np.abs(da - d1).max() > 1e-3 * scale
