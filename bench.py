@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--csf3-radius", type=int, default=40, help="column radius in dx (0: no 3-D CSF leg)")
     ap.add_argument("--csf3-length", type=int, default=200, help="column period in dx")
     ap.add_argument("--tvc-n", type=int, default=100, help="fluid block edge in dx (0: no TVC leg)")
+    ap.add_argument("--rhs2d-dx", type=float, default=0.0014,
+                    help="lattice spacing of the 2-D rhs leg's 1 x 2 m column (0: no rhs leg)")
     ap.add_argument("--ckpt-steps", type=int, default=200, help="steps of the checkpoint leg (0: no leg)")
     ap.add_argument("--ckpt-every", type=int, default=100, help="checkpoint interval of the checkpoint leg")
     return ap.parse_args()
@@ -431,6 +433,74 @@ def tvc_leg(args, dev):
                            "sample": "16^3 block: pairs + gradient integral + displacement"}}
 
 
+def rhs2d_leg(args, dev):
+    """The 2-D rhs drop-in (droplet_impact.rhs, droplet_impact.py:810-1228) on
+    a jittered resting dam-break column with three wall layers, FP32 as the
+    reference runs it: device time of one call with the step's pair list
+    given -- gather rows, density, Molteni diffusion, Tait, Adami walls,
+    pressure and viscous force -- per fluid particle, with the oracle's CPU
+    rate on a small column beside it."""
+    import numpy as np
+    import torch
+    from oracle import pairpass as op
+    from oracle.neighbors import cell_linked_pairs as np_pairs
+    from tensorsph_b200.dam_break import DamBreakConfig, make_column
+    from tensorsph_b200.droplet_impact import rhs, wall_lattice
+    from tensorsph_b200.neighbor_search import cell_linked_pairs
+
+    def state(dx, device):
+        c0 = 62.6
+        cfg = DamBreakConfig(dx=dx, column_width=1.0, column_height=2.0, pool_width=4.0, tank_height=3.0,
+                             sound_speed=c0, viscosity=1e-6, density_diffusion=0.1, max_courant=0.25,
+                             dt=0.25 * 1.3 * dx / c0, wall_layers=3)
+        pos, mass = make_column(cfg, "cpu")
+        wall = wall_lattice(cfg, "cpu", top=cfg.tank_top())
+        g = torch.Generator().manual_seed(5)
+        pos = pos + (0.05 * dx * torch.randn(pos.shape, generator=g, dtype=torch.float64)).to(pos.dtype)
+        return cfg, pos.to(device), mass.to(device), wall.to(device)
+
+    saved = torch.get_default_dtype()
+    torch.set_default_dtype(torch.float32)
+    try:
+        cfg, pos, mass, wall = state(args.rhs2d_dx, dev)
+        h = cfg.h_factor * cfg.dx
+        allpos = torch.cat((pos, wall))
+        pairs = cell_linked_pairs(allpos, 2.0 * h)
+        pairs = pairs[(pairs[:, 0] < pos.shape[0]) | (pairs[:, 1] < pos.shape[0])]
+        vel = torch.zeros_like(pos)
+        call = lambda: rhs(pos, vel, mass, cfg, pairs=pairs, wall=wall, dt=cfg.dt)  # noqa: E731
+        for _ in range(2):
+            rho, p, acc = call()
+        reps = 5
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        start.record()
+        for _ in range(reps):
+            rho, p, acc = call()
+        stop.record()
+        torch.cuda.synchronize(dev)
+        ms = start.elapsed_time(stop) / reps
+        scfg, spos, smass, swall = state(0.02, "cpu")
+        sp, sw = spos.numpy(), swall.numpy()
+        sall = np.concatenate((sp, sw))
+        t0 = time.perf_counter()
+        spairs = np_pairs(sall, 2.0 * scfg.h_factor * scfg.dx)
+        spairs = spairs[(spairs[:, 0] < sp.shape[0]) | (spairs[:, 1] < sp.shape[0])]
+        op.rhs(sp, np.zeros_like(sp), smass.numpy(), scfg, pairs=spairs, wall=sw, dt=scfg.dt)
+        t_cpu = time.perf_counter() - t0
+    finally:
+        torch.set_default_dtype(saved)
+    n = pos.shape[0]
+    return {"workload": f"resting 1.0 x 2.0 m column, dx={args.rhs2d_dx} m, jitter 0.05 dx (seed 5), 3 wall layers, "
+                        "c0=62.6, Molteni delta=0.1, FP32, pair list given",
+            "fluid_particles": n, "wall_particles": int(wall.shape[0]), "pairs": int(pairs.shape[0]),
+            "ms_per_call": ms, "fluid_particles_per_s": n / (ms / 1e3),
+            "rho_max_over_rho0": float(rho.max()) / cfg.rho0,
+            "cpu_oracle": {"fluid_particles_per_s": sp.shape[0] / t_cpu, "fluid_particles": sp.shape[0],
+                           "cores": 1, "seconds": t_cpu,
+                           "sample": "dx=0.02 column: pairs + density, diffusion, walls, force"}}
+
+
 def checkpoint_leg(args, dev, cfg, obstacle, host, tuning):
     """The headline run with crash-safe checkpoints (the obstacle case's
     format, kleefsman_obstacle_3d.py:477-546) every ``--ckpt-every`` steps,
@@ -650,7 +720,8 @@ def main():
                               ("serving", serving_leg, args.serve_requests > 0),
                               ("shear", shear_leg, args.shear_steps > 0),
                               ("csf3", csf3_leg, args.csf3_radius > 0),
-                              ("tvc", tvc_leg, args.tvc_n > 0)):
+                              ("tvc", tvc_leg, args.tvc_n > 0),
+                              ("rhs2d", rhs2d_leg, args.rhs2d_dx > 0)):
             if not on:
                 continue
             try:
