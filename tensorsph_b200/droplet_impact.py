@@ -521,8 +521,6 @@ def rhs(pos, vel, mass, cfg: Config, pairs=None, wall=None, dt=None, wall_vel=No
         if cfg.density_diffusion > 0.0:
             raise ValueError("density_regularization='compression' and density_diffusion are two "
                              "different ways of obtaining the density; pick one")
-        if cfg.compression_regularization_rule == "free_stream":
-            raise ValueError("rule 'free_stream' needs an indicator array")
         regularizer = None if state is None else state.get("compression")
         if regularizer is None:
             regularizer = CompressionRegularization(rule=cfg.compression_regularization_rule,
@@ -589,6 +587,10 @@ def rhs(pos, vel, mass, cfg: Config, pairs=None, wall=None, dt=None, wall_vel=No
         # the reduce writes the scalar after this call consumed it
         written, counted = comp_out.tolist()
         regularizer.inverse_reference_compression = written
+        if cfg.compression_regularization_rule == "free_stream":
+            # compression_regularization.py:164-184: rhs passes no indicator;
+            # the scalar is already written, the state entry is not
+            raise ValueError("rule 'free_stream' needs an indicator array")
         if state is not None:
             state["compression"] = regularizer
             state["compression_counted"] = int(counted)

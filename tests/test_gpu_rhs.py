@@ -298,3 +298,19 @@ def test_rhs3d_closure_matches_reference(gpu, golden):
             tol = tr if name in ("rho", "p") else tf
             scale = bulk(cfg) if name == "p" else None
             assert rel_err(got.cpu(), g[f"c{k}_{name}"], scale) < tol, (k, name)
+
+
+def test_free_stream_rule_raises_after_writing_the_scalar(gpu):
+    """rhs passes no indicator, so the rule "free_stream" raises -- after the
+    call wrote the new inverse reference compression into the regulariser it
+    carries, and without storing the count (compression_regularization.py:
+    164-184, droplet_impact.py:1013-1028)."""
+    from tensorsph_b200.compression_regularization import CompressionRegularization
+    from tensorsph_b200.droplet_impact import rhs
+    pos = torch.tensor([[0.0, 0.0], [0.04, 0.0]], dtype=torch.float64, device=gpu)
+    reg = CompressionRegularization(rule="free_stream")
+    state = {"compression": reg}
+    cfg = _cfg(dx=0.05, density_regularization="compression", compression_regularization_rule="free_stream")
+    with pytest.raises(ValueError):
+        rhs(pos, torch.zeros_like(pos), torch.full((2,), 25.0, dtype=torch.float64, device=gpu), cfg, state=state)
+    assert reg.inverse_reference_compression != 1.0 and "compression_counted" not in state
