@@ -178,7 +178,9 @@ typedef struct {
   void* face_pressure;        /* out (nw) when SPLIT            */
   double* compression_out;    /* out (2, device) when COMPRESSION: the
                                  inverse reference compression for the next
-                                 call, the particles counted (S > 1)      */
+                                 call, the particles counted (S > 1); a
+                                 call without fluid particles writes
+                                 (1, 0), no compressed particle           */
 } tsph_wcsph_io;
 
 int64_t tsph_wcsph_workspace_bytes(const tsph_wcsph_params* prm);
@@ -199,6 +201,10 @@ int tsph_wcsph_rhs(const tsph_wcsph_params* prm, const tsph_wcsph_io* io, void* 
  * wall) in FP32, 150,000 in FP64.  The first call on a device looks up the
  * array's device address (with that device current), so make that first call
  * before any stream capture; the stream must belong to the current device.
+ * The address is kept per device together with the id of the context it was
+ * taken in: after cudaDeviceReset (or a context destroyed and created again)
+ * the next call takes it again, and that call too should come before any
+ * stream capture.
  * Every call shares the one array and leaves its contents behind: calls that
  * overlap on the GPU (other streams, other threads, the same device) race on
  * it, so serialise them.  No part of the array has to start at zero. */
@@ -641,9 +647,30 @@ int tsph_engine_set_block(tsph_engine* engine, int64_t threads);
 /* Neighbour records in flight per thread in the pair kernels: 4 (default) or
  * 8.  A tuning knob (results do not depend on it); the graph is re-captured. */
 int tsph_engine_set_batch(tsph_engine* engine, int64_t depth);
+/* Entries of the current neighbour rows: out[0] over the fluid rows, out[1]
+ * over the wall rows (synchronises the stream).  The pair passes' work per
+ * step is proportional to these counts. */
+int tsph_engine_row_entries(tsph_engine* engine, int64_t* out, tsph_stream stream);
 /* Occupancy (fluid rows, wall rows, obstacle rows, cells, cases) (host). */
 int tsph_engine_usage(const tsph_engine* engine, int64_t* usage);
 int tsph_engine_destroy(tsph_engine* engine);
+
+/* ------------------------------------------------------------------------ */
+/* Roofline probes (no counterpart in the reference, which runs on torch     */
+/* alone): the FP32 FMA rate and the device copy bandwidth of this GPU, the  */
+/* denominators the pair passes are measured against.                       */
+/* ------------------------------------------------------------------------ */
+
+/* blocks x threads threads (threads <= 256, a multiple of 32) each run 8
+ * independent chains of `iters` FMAs, scalar (packed = 0) or packed FP32x2
+ * (packed = 1), and write one float to out[blocks * threads]. */
+int tsph_probe_fma(float* out, int64_t blocks, int64_t threads, int64_t iters, int64_t packed,
+                   tsph_stream stream);
+/* FLOPs of one tsph_probe_fma launch (an FMA counts 2). */
+int64_t tsph_probe_fma_flops(int64_t blocks, int64_t threads, int64_t iters, int64_t packed);
+/* Copy `bytes` (a multiple of 16; both pointers 16-byte aligned) with a
+ * grid-stride 16-byte loop over `blocks` blocks of 256 threads. */
+int tsph_probe_copy(const void* src, void* dst, int64_t bytes, int64_t blocks, tsph_stream stream);
 
 #ifdef __cplusplus
 }

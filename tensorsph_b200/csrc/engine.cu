@@ -188,6 +188,7 @@ struct Dev {
   unsigned int* hist;
   unsigned long long* sel;
   long long* sel_k;
+  unsigned long long* entries;  // [2]: list entries of the fluid rows, of the wall rows
 };
 
 // ------------------------------------------------------------- helpers ---
@@ -335,10 +336,15 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* p, double 
   if (v > 0.0) atomicMax(p, static_cast<unsigned long long>(__double_as_longlong(v)));
 }
 
-__device__ __forceinline__ float tait(float rho, float rho0, float bulk, float gamma) {
-  float ratio = rho / rho0;
-  ratio = ratio > 0.01f ? ratio : 0.01f;
-  float p = bulk * (powf(ratio, gamma) - 1.f);
+// Tait pressure B ((rho / rho0)^gamma - 1) (tait_pressure, droplet_impact.py:415-427;
+// ratio clamped to >= 0.01, p >= 0) from the density deviation d = rho - rho0:
+// B expm1(gamma log1p(d / rho0)).  No ratio near 1 is rounded before 1 is
+// subtracted, so the FP32 pressure keeps the relative precision of d instead of
+// losing the leading digits of rho / rho0 (about gamma x 6e-8 of B).
+__device__ __forceinline__ float tait_dev(float d, float rho0, float bulk, float gamma) {
+  float x = d / rho0;
+  x = x > -0.99f ? x : -0.99f;
+  const float p = bulk * expm1f(gamma * log1pf(x));
   return p > 0.f ? p : 0.f;
 }
 
@@ -614,6 +620,24 @@ __global__ void k_rows(Dev e) {
   }
 }
 
+// Entries of the current rows: fluid rows into entries[0], wall rows into
+// entries[1] (entries cleared by the caller).
+__global__ void k_count_entries(Dev e) {
+  unsigned long long f = 0, w = 0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < e.nf + e.nw; t += gridDim.x * blockDim.x) {
+    if (t < e.nf)
+      f += static_cast<unsigned long long>(e.cnt[t]);
+    else
+      w += static_cast<unsigned long long>(e.cnt[e.NF + (t - e.nf)]);
+  }
+  f = warp_reduce_sum(f);
+  w = warp_reduce_sum(w);
+  if ((threadIdx.x & 31) == 0) {
+    if (f) atomicAdd(&e.entries[0], f);
+    if (w) atomicAdd(&e.entries[1], w);
+  }
+}
+
 __global__ void k_rebuilt(Dev e) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= e.n_slots || !e.ctl[c].rebuild) return;
@@ -657,7 +681,9 @@ __global__ void __launch_bounds__(kMaxBlock) k_density(const __grid_constant__ D
     const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, floor_ = C.rho_floor;
     const float4 la = e.lp[a];
     const float2 ncell = f2(-cellf), inv_h2 = f2(inv_h), sigma2 = f2(sigma);
+    // the deviation rho - rho0, summed with compensation from -rho0
     CSum<float> s;
+    s.add(-C.rho0);
     s.add(la.w * sigma);
     walk_row<KB>(e, a, [&](const uint32_t* ent) {
       float2 part = f2(0.f);
@@ -674,9 +700,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_density(const __grid_constant__ D
       }
       s.add(part.x + part.y);
     });
-    float rho = s.value();
-    rho = rho > floor_ ? rho : floor_;
-    e.rs[a] = make_float2(rho, la.w / rho);
+    const float dfloor = floor_ - C.rho0;
+    float d = s.value();
+    d = d > dfloor ? d : dfloor;
+    e.rs[a] = make_float2(d, la.w / (C.rho0 + d));
   }
 }
 
@@ -684,9 +711,9 @@ template <bool kOne, int KB>
 __global__ void __launch_bounds__(kMaxBlock) k_diffusion_eos(const __grid_constant__ Dev e) {
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
     const CaseDev& C = case_of<kOne>(e, a);
-    const float2 ra = e.rs[a];
+    const float2 ra = e.rs[a];  // (rho - rho0, m / rho)
     const float4 la = e.lp[a];
-    float rho = ra.x;
+    float d = ra.x;
     const float dscale = C.dscale;
     if (dscale > 0.f) {
       const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf;
@@ -718,10 +745,12 @@ __global__ void __launch_bounds__(kMaxBlock) k_diffusion_eos(const __grid_consta
         rate.add(part.x + part.y);
       });
       const float dtf = C.adaptive ? static_cast<float>(e.ctl[kOne ? e.one_slot : e.cid[a]].dt_step) : C.dtf;
-      rho = ra.x + dtf * rate.value();
-      rho = rho > C.rho_floor ? rho : C.rho_floor;
+      const float dfloor = C.rho_floor - C.rho0;
+      d = ra.x + dtf * rate.value();
+      d = d > dfloor ? d : dfloor;
     }
-    const float p = tait(rho, C.rho0, C.bulk, C.gamma);
+    const float rho = C.rho0 + d;
+    const float p = tait_dev(d, C.rho0, C.bulk, C.gamma);
     const double4 v = ld4(e.vel, a);
     e.vb[a] = make_float4(static_cast<float>(v.x), static_cast<float>(v.y), static_cast<float>(v.z), la.w / rho);
     e.rho[a] = rho;
@@ -2091,7 +2120,7 @@ __global__ void k_null_row(Dev e) {
   e.pr[n] = 0.f;
   e.rho[n] = 1.f;
   e.pq[n] = 0.f;
-  e.rs[n] = make_float2(1.f, 0.f);
+  e.rs[n] = make_float2(0.f, 0.f);
   e.conc[n] = 0.f;
 }
 
@@ -2286,6 +2315,7 @@ size_t carve(const tsph_engine_params& p, Dev* d, char* base, CaseDev** cases, c
   t.hist = static_cast<unsigned int*>(take(2 * kSelBins * sizeof(unsigned int)));
   t.sel = static_cast<unsigned long long*>(take(4 * sizeof(unsigned long long)));
   t.sel_k = static_cast<long long*>(take(2 * sizeof(long long)));
+  t.entries = static_cast<unsigned long long*>(take(2 * sizeof(unsigned long long)));
   CaseDev* cd = static_cast<CaseDev*>(take(p.max_cases * sizeof(CaseDev)));
   char* rs = static_cast<char*>(take(radix_scratch_bytes(nsort)));
   if (cases) *cases = cd;
@@ -3028,6 +3058,20 @@ int tsph_engine_status(tsph_engine* E, int64_t case_id, int64_t* counters, tsph_
   counters[7] = t.final_step;
   if (t.status & 2) return TSPH_ERR_STATE;
   if (t.status & 1) return TSPH_ERR_CAPACITY;
+  return TSPH_OK;
+}
+
+int tsph_engine_row_entries(tsph_engine* E, int64_t* out, tsph_stream stream) {
+  if (!E || !out) return TSPH_ERR_ARG;
+  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  unsigned long long host[2] = {0, 0};
+  TSPH_CUDA_CHECK(cudaMemsetAsync(E->d.entries, 0, 2 * sizeof(unsigned long long), s));
+  if (E->d.nf + E->d.nw > 0) k_count_entries<<<grid_for(E->d.nf + E->d.nw, 256), 256, 0, s>>>(E->d);
+  TSPH_CUDA_CHECK(cudaGetLastError());
+  TSPH_CUDA_CHECK(cudaMemcpyAsync(host, E->d.entries, sizeof(host), cudaMemcpyDeviceToHost, s));
+  TSPH_CUDA_CHECK(cudaStreamSynchronize(s));
+  out[0] = static_cast<int64_t>(host[0]);
+  out[1] = static_cast<int64_t>(host[1]);
   return TSPH_OK;
 }
 

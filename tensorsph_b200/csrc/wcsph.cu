@@ -206,6 +206,13 @@ __global__ void __launch_bounds__(1024) compression_average(const T* __restrict_
   }
 }
 
+// The regulariser's result of a call without fluid particles: no particle is
+// compressed, so the reference keeps 1 / mean{S > 1} at 1 with a count of 0.
+__global__ void compression_identity(double* __restrict__ out) {
+  out[0] = 1.0;
+  out[1] = 0.0;
+}
+
 // ------------------------------------------------ free-surface closure ---
 // droplet_impact.py:429-492 over the fluid neighbours.  donors: 0 the known
 // ones ("interior"), 1 all ("all"), 2 all plus the particle itself (the dense
@@ -703,8 +710,14 @@ int tsph_wcsph_rhs(const tsph_wcsph_params* prm, const tsph_wcsph_io* io, void* 
   if ((prm->flags & TSPH_RHS_SURFACE_CLOSURE) &&
       (prm->surface_donors < 0 || prm->surface_donors > 2 || prm->surface_layers > 1024))
     return TSPH_ERR_ARG;
-  if (prm->n_fluid == 0) return TSPH_OK;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (prm->n_fluid == 0) {
+    if (prm->flags & TSPH_RHS_COMPRESSION) {
+      compression_identity<<<1, 1, 0, s>>>(io->compression_out);
+      if (cudaGetLastError() != cudaSuccess) return TSPH_ERR_CUDA;
+    }
+    return TSPH_OK;
+  }
   char* w = static_cast<char*>(ws);
   if (prm->dtype == TSPH_F32) {
     return prm->dim == 2 ? run_rhs<float, 2>(*prm, *io, w, s) : run_rhs<float, 3>(*prm, *io, w, s);
@@ -731,7 +744,40 @@ static __device__ __align__(256) unsigned char g_rhs_noalloc_scratch[kNoAllocScr
 namespace {
 constexpr int kMaxDevices = 128;
 std::mutex g_noalloc_mutex;
+// Per device: the array's address and the id of the context it was taken in.
+// A module is loaded per context, so when the context changes (after
+// cudaDeviceReset, or a driver-API context destroyed and created again) the
+// array may live elsewhere and the address is taken again.
 void* g_noalloc_ptr[kMaxDevices] = {};
+unsigned long long g_noalloc_ctx[kMaxDevices] = {};
+
+typedef int (*CtxGetCurrentFn)(void**);
+typedef int (*CtxGetIdFn)(void*, unsigned long long*);
+
+// Id of the current context (cuCtxGetCurrent + cuCtxGetId through the
+// runtime's driver entry points, so the library does not link libcuda); 0
+// when it cannot be read.
+unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static bool looked = false;
+  if (!looked) {
+    looked = true;
+    cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = q1;
+    void* f1 = nullptr;
+    void* f2 = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f1, 12000, cudaEnableDefault, &q1) == cudaSuccess &&
+        cudaGetDriverEntryPointByVersion("cuCtxGetId", &f2, 12000, cudaEnableDefault, &q2) == cudaSuccess &&
+        q1 == cudaDriverEntryPointSuccess && q2 == cudaDriverEntryPointSuccess) {
+      get_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+      get_id = reinterpret_cast<CtxGetIdFn>(f2);
+    }
+  }
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
 }  // namespace
 
 extern "C" int tsph_wcsph_rhs_noalloc(const tsph_wcsph_params* prm, const tsph_wcsph_io* io,
@@ -744,12 +790,19 @@ extern "C" int tsph_wcsph_rhs_noalloc(const tsph_wcsph_params* prm, const tsph_w
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return TSPH_ERR_CUDA;
   void* scratch = nullptr;
   {
+    // the first call on a device (and the first after its context changed)
+    // takes the array's device address; that call should come before any
+    // stream capture (when the context id cannot be read, the address is
+    // taken on every call)
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    const unsigned long long ctx = current_context_id();
     scratch = g_noalloc_ptr[dev];
-    if (!scratch) {
+    if (!scratch || ctx == 0 || ctx != g_noalloc_ctx[dev]) {
+      scratch = nullptr;
       if (cudaGetSymbolAddress(&scratch, g_rhs_noalloc_scratch) != cudaSuccess || !scratch)
         return TSPH_ERR_CUDA;
       g_noalloc_ptr[dev] = scratch;
+      g_noalloc_ctx[dev] = current_context_id();
     }
   }
   // Nothing in the scratch needs to start at zero: every byte the rhs kernels

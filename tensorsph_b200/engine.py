@@ -457,6 +457,14 @@ class BatchEngine:
         _lib.check(_lib.lib().tsph_engine_usage(self._handle, u), "tsph_engine_usage")
         return dict(fluid=u[0], wall=u[1], obstacle=u[2], cells=u[3], cases=u[4])
 
+    def row_entries(self) -> tuple[int, int]:
+        """Entries of the current neighbour rows ``(fluid rows, wall rows)``
+        (synchronises the engine stream)."""
+        out = (ctypes.c_int64 * 2)()
+        _lib.check(_lib.lib().tsph_engine_row_entries(self._handle, out, self.stream.cuda_stream),
+                   "tsph_engine_row_entries")
+        return int(out[0]), int(out[1])
+
     def fits(self, spec: CaseSpec) -> bool:
         """Whether ``spec`` fits in the free capacity right now."""
         u = self.usage()

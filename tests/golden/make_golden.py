@@ -1074,5 +1074,8 @@ RHS2D_OPTION_SETS = [
 ]
 
 if __name__ == "__main__":
-    # make_golden.py [SRC] [FAMILY ...]: regenerate the named families (default all)
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"), sys.argv[2:] or None)
+    # make_golden.py SRC [FAMILY ...]: regenerate the named families (default all)
+    # from the reference source tree SRC (the directory that holds `tensorsph/`)
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_golden.py SRC [FAMILY ...]  (SRC: the reference's src/ directory)")
+    main(Path(sys.argv[1]), sys.argv[2:] or None)

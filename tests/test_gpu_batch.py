@@ -3,7 +3,7 @@ bit for bit the same alone and batched with others admitted and retired
 around it (continuous batching).
 
 Tolerances of the FP32 pair pass against the FP64 oracle are those of the 3-D
-engine test: density |d rho| / rho0 < 2e-6, pressure |d p| / B < 2e-5,
+engine test: density |d rho| / rho0 < 1e-5, pressure |d p| / B < 1e-5,
 velocity after one step |d v| / max|v| < 2e-4.  Alone against batched, the
 state (positions, velocities, density, pressure) must be bitwise equal; the
 energy meters are FP64 sums accumulated with atomics, equal to 1e-12.
@@ -80,8 +80,8 @@ def test_2d_case_matches_fp64_oracle(gpu):
     ex, ev, erho, ep = [t.cpu().numpy() for t in eng.read(cid)]
     bulk = cfg.rho0 * cfg.sound_speed ** 2 / cfg.gamma
     rho0, p0, acc0 = ref[0]
-    assert np.abs(erho - rho0).max() / cfg.rho0 < 2e-6
-    assert np.abs(ep - p0).max() / bulk < 2e-5
+    assert np.abs(erho - rho0).max() / cfg.rho0 < 1e-5
+    assert np.abs(ep - p0).max() / bulk < 1e-5
     v1 = cfg.dt * acc0
     assert np.abs(ev - v1).max() / np.abs(v1).max() < 2e-4
     eng.step(steps - 1)
@@ -437,7 +437,10 @@ def test_adaptive_dam_break_follows_reference_run(golden, gpu):
     assert len(run.times) == len(g["times"])
     assert np.allclose(run.times, g["times"], rtol=1e-5, atol=0)
     assert run.dt_max == float(g["dt_max"]) == cfg.dt
-    assert run.dt_min == pytest.approx(float(g["dt_min"]), rel=1e-5)
+    # dt = 0.9 courant h / (c0 + max |v|): the FP32-pair trajectory's speed,
+    # held to 1e-4 below, moves dt by 1e-4 max|v| / (c0 + max|v|) at most
+    vmax = float(g["max_speed"])
+    assert run.dt_min == pytest.approx(float(g["dt_min"]), rel=1e-4 * vmax / (cfg.sound_speed + vmax))
     assert run.max_acoustic_courant == pytest.approx(float(g["max_acoustic_courant"]), rel=1e-9)
     assert run.max_speed == pytest.approx(float(g["max_speed"]), rel=1e-4)
     # the reference's own claims for this case (tests/test_adaptive_dt.py:114-140)
