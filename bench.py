@@ -8,16 +8,22 @@ dx = 0.0069 m (1,968,048 fluid particles) in a 3.2 x 1.0 x 1.0 m tank with
 three wall layers and a 0.16 x 0.16 x 0.4 m obstacle (776k wall particles),
 h = 1.3 dx, Tait rho0 = 1000, gamma = 7, c0 = 10 sqrt(2 g 0.55), Molteni
 diffusion delta = 0.1, Lind shifting every step, CFL 0.25; FP32 pair
-arithmetic with FP64 positions, velocities and meters.  A step is one
-graph-captured engine step (skin test and device-side rebuild, density,
-diffusion + EOS, Adami walls, force, obstacle force, Euler + clamps, shift).
+arithmetic with FP64 positions, velocities and meters.
+
+A bench step is ``--chunk`` solver steps (default: enough that the K timed
+bench steps cover at least 200 solver steps, so that the timed region holds
+the neighbour-list rebuilds at their natural rate, about one per list pass
+every 20-40 steps).  A solver step is one graph-launched engine step: per-case
+skin test and device-side rebuild (conditional), density, diffusion + EOS,
+Adami walls, force, obstacle force, Euler + clamps, shifting.
 
 One JSON line on rank 0.  ``value`` is device-timed (CUDA events on the
 engine stream, max over ranks); ``e2e`` is the same metric through the public
 API from pinned host memory: engine creation from the host lattice (H2D), the
-K steps with one device->host read of the step's meter row per step, and the
-final state back to the host.  ``--impl reference`` times the CPU oracle port
-of the same algorithm (numpy, one core) on a 4x coarser rung of the same case.
+K bench steps with one device->host read of a meter row per bench step, and
+the final state back to the host.  ``--impl reference`` times the reference's
+own CPU code (``baseline/_ref``, torch on every host core) on a 4x coarser
+rung of the same case.
 """
 from __future__ import annotations
 
@@ -36,8 +42,19 @@ sys.path.insert(0, str(ROOT))
 
 ALGO_BYTES_FORCE = 52      # per fluid particle: pos+mass 16, vel+rho 16, p/rho^2 4 in; acc 16 out
 ALGO_BYTES_STEP = 244      # per fluid update, compulsory bytes of the whole step (3-D plain path)
-FLOPS_PER_PAIR_FORCE = 60  # kernel + pressure + viscosity per in-support pair
-CANDIDATE_FLOPS = 10       # separation + radius test per listed neighbour
+ALGO_BYTES_WALL = 48       # per wall particle and step
+# FP32 operations per listed neighbour of each pair pass, counted from the
+# kernel source (an FMA counts 2, every other arithmetic instruction 1,
+# including rsqrt and reciprocals and the cell-offset decode; a packed FP32x2
+# instruction counts once per neighbour it serves).
+PAIR_FLOPS = {"density": 39, "diffusion": 62, "walls": 41, "force": 77, "concentration": 39,
+              "gradient": 63}
+# DRAM bytes of one force launch per fluid particle: ncu capture of the force
+# pass on the dx = 0.0138 rung (241,560 fluid), dram__bytes_read.sum +
+# dram__bytes_write.sum divided by the fluid rows (profiles/engine_force_dam_break_3d.md).
+FORCE_TRAFFIC_PER_FLUID = 428.0
+FORCE_TRAFFIC_RUNG = "dx=0.0138 (241,560 fluid), ncu capture scaled by fluid rows"
+MIN_TIMED_SOLVER_STEPS = 200
 
 
 def parse():
@@ -45,6 +62,13 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--chunk", type=int, default=0,
+                    help="solver steps per bench step (0: the least that makes K bench steps "
+                         f"cover {MIN_TIMED_SOLVER_STEPS} solver steps)")
+    ap.add_argument("--ref-dx", type=float, default=0.0276,
+                    help="lattice spacing of the CPU reference rung")
+    ap.add_argument("--ref-sample-steps", type=int, default=3,
+                    help="solver steps of the reference's CPU code timed for cpu_baseline")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--dx", type=float, default=0.0069)
     ap.add_argument("--shift-every", type=int, default=1)
@@ -84,28 +108,55 @@ def whole_job_rate(units_per_rank: int, steps: int, world: int, seconds: float) 
     return units_per_rank * steps * world / seconds
 
 
-def peaks():
+def driver_peaks():
+    """HBM GB/s and bf16 TF/s measured on this pool (MEASURED_PEAKS.json), if present."""
     path = ROOT / "MEASURED_PEAKS.json"
     if path.exists():
-        data = json.loads(path.read_text())
-        return float(data["hbm_gbs"]), "measured"
-    return 6650.0, "fallback"
-
-
-def _force_profile_figure(key: str):
-    """A figure of the committed ncu summary of the force pass (``key: value`` line)."""
-    path = ROOT / "profiles" / "engine_force_dam_break_3d.md"
-    if not path.exists():
-        return None
-    for line in path.read_text().splitlines():
-        if line.startswith(key + ":"):
-            return float(line.split(":", 1)[1].strip())
+        return json.loads(path.read_text())
     return None
 
 
-def ncu_traffic_per_fluid_particle():
-    """DRAM bytes per fluid particle of one force launch, from the committed ncu summary."""
-    return _force_profile_figure("traffic_bytes_per_fluid_particle")
+def probe_peaks(dev):
+    """The FP32 FMA rate (scalar and packed FP32x2 chains, the larger) and the
+    device copy bandwidth of this GPU, each the best of 3 CUDA-event-timed
+    launches of the library's probe kernels after a warm-up launch."""
+    import torch
+    from tensorsph_b200 import _lib
+    L = _lib.lib()
+    s = torch.cuda.current_stream(dev)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    blocks, threads, iters = sms * 8, 256, 4096
+    out = torch.empty(blocks * threads, dtype=torch.float32, device=dev)
+
+    def best_ms(launch):
+        best = None
+        for rep in range(4):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(s)
+            launch()
+            b.record(s)
+            b.synchronize()
+            if rep:
+                ms = a.elapsed_time(b)
+                best = ms if best is None else min(best, ms)
+        return best
+
+    fma = {}
+    for packed in (0, 1):
+        ms = best_ms(lambda: _lib.check(L.tsph_probe_fma(out.data_ptr(), blocks, threads, iters, packed,
+                                                         s.cuda_stream), "tsph_probe_fma"))
+        fma["packed" if packed else "scalar"] = (L.tsph_probe_fma_flops(blocks, threads, iters, packed)
+                                                 / (ms / 1e3) / 1e12)
+    nbytes = 2 << 30
+    src = torch.ones(nbytes, dtype=torch.uint8, device=dev)
+    dst = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    ms = best_ms(lambda: _lib.check(L.tsph_probe_copy(src.data_ptr(), dst.data_ptr(), nbytes, sms * 16,
+                                                      s.cuda_stream), "tsph_probe_copy"))
+    del src, dst
+    torch.cuda.empty_cache()
+    return {"fp32_tflops": max(fma.values()), "fp32_scalar_tflops": fma["scalar"],
+            "fp32_packed_tflops": fma["packed"], "copy_gbs": 2 * nbytes / (ms / 1e3) / 1e9,
+            "probe": f"FMA: {blocks}x{threads} threads x 8 chains x {iters}; copy: 2 GiB read + 2 GiB write"}
 
 
 class ClockSampler:
@@ -151,74 +202,173 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def cpu_baseline(dx, steps, shift_every):
-    """Oracle port (numpy, 1 core): rhs_3d + Euler + clamps, skin-cached pairs."""
+REF_PATH = ROOT / "baseline" / "_ref"
+
+
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def reference_available() -> bool:
+    return (REF_PATH / "tensorsph" / "dam_break_3d.py").exists()
+
+
+def reference_loop(dx, steps, warmup, shift_every, threads=None):
+    """The reference's own CPU code on one rung of the headline case: the
+    obstacle loop of kleefsman_obstacle_3d.py:644-706 (PairListCache.get,
+    rhs_3d with the wall force, Euler, apply_boundary_3d, clamp_out_of_obstacle)
+    with the shifting hook of dam_break.py:424-433 (shift_positions every
+    ``shift_every`` steps from the second step on), in the reference's default
+    dtype (FP32), torch on ``threads`` host threads (all usable cores).  The
+    tank and obstacle are this case's geometry, built with the reference's own
+    lattice builders; validate_case is skipped because the geometry is not
+    Kleefsman's (kleefsman_obstacle_3d.py:129-147).  Returns fluid
+    particle-updates/s over ``steps`` timed steps after ``warmup`` steps."""
+    if str(REF_PATH) not in sys.path:
+        sys.path.insert(0, str(REF_PATH))
+    import torch
+    from tensorsph.dam_break_3d import DamBreak3DConfig, apply_boundary_3d, make_column_3d, rhs_3d, wall_lattice_3d
+    from tensorsph.kleefsman_obstacle_3d import clamp_out_of_obstacle, obstacle_lattice_3d
+    from tensorsph.neighbor_search import PairListCache
+    from tensorsph.particle_shifting import shift_positions
+    threads = threads or max(1, len(os.sched_getaffinity(0)))
+    torch.set_num_threads(threads)
+    c0 = 10.0 * math.sqrt(2.0 * 9.81 * 0.55)
+    h = 1.3 * dx
+    cfg = DamBreak3DConfig(dx=dx, pool_width=3.2, tank_depth=1.0, tank_height=1.0, column_width=1.2,
+                           column_depth=1.0, column_height=0.55, wall_layers=3, density_diffusion=0.1,
+                           sound_speed=c0, viscosity=1.0e-6, dt=0.25 * h / c0, max_courant=0.25, steps=5000)
+
+    class ObstacleBox:
+        """The obstacle fields clamp_out_of_obstacle and obstacle_lattice_3d read."""
+        obstacle_x, obstacle_height, obstacle_z = 3.2 - 0.744 - 0.08, 0.16, 0.3
+
+        def __init__(self):
+            self.dx = dx
+
+        def obstacle_x1(self):
+            return self.obstacle_x + 0.16
+
+        def obstacle_z1(self):
+            return 0.7
+
+    box = ObstacleBox()
+    dev = torch.device("cpu")
+    pos, mass = make_column_3d(cfg, dev)
+    wall = torch.cat((wall_lattice_3d(cfg, dev, top=cfg.tank_top()),
+                      obstacle_lattice_3d(box, dev).to(pos.dtype)))
+    vel = torch.zeros_like(pos)
+    n = pos.shape[0]
+    cache = PairListCache(2.0 * h, cfg.pair_skin_factor * h, fluid_count=n)
+    all_pos = torch.cat((pos, wall))
+    t0 = None
+    for step in range(warmup + steps):
+        if step == warmup:
+            t0 = time.perf_counter()
+        all_pos[:n] = pos
+        pairs, _ = cache.get(all_pos)
+        rho, _, acc, _ = rhs_3d(pos, vel, mass, cfg, pairs=pairs, wall=wall, dt=cfg.dt, return_wall_force=True)
+        speed = float(torch.linalg.vector_norm(vel, dim=-1).max())
+        vel = vel + cfg.dt * acc
+        pos = pos + cfg.dt * vel
+        apply_boundary_3d(pos, vel, cfg, top=cfg.tank_top())
+        clamp_out_of_obstacle(pos, vel, box)
+        if shift_every and step > 0 and step % shift_every == 0:
+            pos = shift_positions(pos, mass / rho, h, dt=cfg.dt, v_ref=max(speed, 0.05 * c0))
+    elapsed = time.perf_counter() - t0
+    return {"value": n * steps / elapsed, "fluid": n, "seconds": elapsed, "cores": threads,
+            "rebuilds": cache.rebuilds, "torch": torch.__version__, "cpu": cpu_model(),
+            "dtype": str(pos.dtype).replace("torch.", "")}
+
+
+def oracle_port_and_errors(dx, dev, shift_every, tuning, max_lead=8000):
+    """The oracle port (numpy FP64, one core) on one rung of the headline
+    case, timed, and the engine's FP32-pair run of the same rung against it,
+    field by field (the FP64 run each reported field carries its error
+    against).  Two phases: from rest (3 steps), and the impact on the obstacle
+    (the engine runs from rest until the surge loads the obstacle, at most
+    ``max_lead`` steps; from its state both take 2 steps).  Errors: density /
+    rho0, pressure / B, acceleration / its largest value, obstacle force / its
+    largest value, front / dx."""
     import numpy as np
-    from oracle import neighbors as on
-    from oracle import pairpass as op
+    from dataclasses import replace
+    from oracle import dam3d
     from tensorsph_b200.engine import DamBreak3DEngine, obstacle_case
     cfg, ob = obstacle_case(dx=dx)
-    x, m, w, _ = DamBreak3DEngine.build_host_state(cfg, ob)
-    x, m, w = x.numpy(), m.numpy(), w.numpy()
-    n = x.shape[0]
-    v = np.zeros_like(x)
-    h = cfg.h_factor * cfg.dx
-    skin = cfg.pair_skin_factor * h
-    box = np.array([cfg.pool_width, cfg.tank_height, cfg.tank_depth])
-    anchor, pairs = None, None
+    if tuning is not None:
+        cfg = replace(cfg, pair_skin_factor=tuning["best"]["skin_factor"])
+    x, m, w, n_ob = DamBreak3DEngine.build_host_state(cfg, ob)
+    bulk = cfg.rho0 * cfg.sound_speed ** 2 / cfg.gamma
+    out = {"rung": f"dx={dx:g} ({x.shape[0]} fluid + {w.shape[0]} wall)"}
+    port_steps, port_time = 0, 0.0
+
+    def fields(eng, recs, first, count, k_state):
+        diag = eng.diagnostics(first, count).cpu().numpy()
+        _, _, erho, ep = (t.cpu().numpy() for t in eng.state())
+        r = recs[k_state]
+        e = {"density": float(np.abs(erho - r["rho"]).max()) / cfg.rho0,
+             "pressure": float(np.abs(ep - r["p"]).max()) / bulk,
+             "rho_max": max(abs(diag[k, 0] - recs[k]["rho"].max()) for k in range(count)) / cfg.rho0,
+             "front": max(abs(diag[k, 2] - recs[k]["front"]) for k in range(count)) / cfg.dx}
+        fmax = max(float(np.abs(rr["force"]).max()) for rr in recs)
+        if fmax > 0:
+            e["obstacle_force"] = max(float(np.abs(diag[k, 3:6] - recs[k]["force"]).max())
+                                      for k in range(count)) / fmax
+            e["obstacle_force_N"] = fmax
+        return e
+
+    # from rest
     t0 = time.perf_counter()
-    for _ in range(steps):
-        allp = np.concatenate((x, w))
-        if anchor is None or np.sqrt(((x - anchor) ** 2).sum(1)).max() > 0.5 * skin:
-            pairs = on.cell_linked_pairs_batched(allp, 2.0 * h + skin)
-            pairs = pairs[pairs[:, 0] < n]
-            anchor = x.copy()
-        rho, p, acc, react = op.rhs_3d(x, v, m, cfg, pairs=pairs, wall=w, dt=cfg.dt,
-                                       return_wall_force=True)
-        v = v + cfg.dt * acc
-        x = x + cfg.dt * v
-        out = (x < -0.25 * cfg.dx) | (x > box + 0.25 * cfg.dx)
-        x = np.clip(x, 0.0, box)
-        v[out] = 0.0
-        if shift_every:
-            vol = m / rho
-            x, _ = op.shift_positions(x, vol, h, dt=cfg.dt,
-                                      v_ref=max(float(np.sqrt((v * v).sum(1)).max()),
-                                                0.05 * cfg.sound_speed))
-    elapsed = time.perf_counter() - t0
-    return n * steps / elapsed, n, elapsed
-
-
-def _baseline_worker(dx, steps, shift_every, barrier, out):
-    """One core's copy of the CPU sample: build, wait for the others, run."""
-    import os as _os
-    for var in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
-        _os.environ[var] = "1"
-    barrier.wait()
-    out.put(cpu_baseline(dx, steps, shift_every))
-
-
-def cpu_baseline_all_cores(dx, steps, shift_every):
-    """The CPU sample on every core this process may use: one independent copy
-    per core (spawned processes, started together at a barrier), each timing
-    its own loop; the rate is the sum of the copies' rates."""
-    import multiprocessing as mp
-    workers = max(1, len(os.sched_getaffinity(0)))
-    if workers == 1:
-        rate, n, elapsed = cpu_baseline(dx, steps, shift_every)
-        return rate, n, elapsed, 1
-    ctx = mp.get_context("spawn")
-    barrier = ctx.Barrier(workers)
-    out = ctx.Queue()
-    procs = [ctx.Process(target=_baseline_worker, args=(dx, steps, shift_every, barrier, out))
-             for _ in range(workers)]
-    for p in procs:
-        p.start()
-    results = [out.get() for _ in procs]
-    for p in procs:
-        p.join()
-    rate = sum(r[0] for r in results)
-    return rate, results[0][1], max(r[2] for r in results), workers
+    recs, _, _ = dam3d.run(cfg, ob, x.numpy(), m.numpy(), w.numpy(), n_ob, 3, shift_every=shift_every)
+    port_time += time.perf_counter() - t0
+    port_steps += 3
+    eng = DamBreak3DEngine(cfg, obstacle=ob, shift_every=shift_every, host_state=(x, m, w, n_ob),
+                           diag_ring=64, device=dev)
+    eng.step(1)
+    _, ev, erho, ep = (t.cpu().numpy() for t in eng.state())
+    v1 = cfg.dt * recs[0]["acc"]
+    rest = {"density": float(np.abs(erho - recs[0]["rho"]).max()) / cfg.rho0,
+            "pressure": float(np.abs(ep - recs[0]["p"]).max()) / bulk,
+            "acceleration": float(np.abs(ev - v1).max()) / float(np.abs(v1).max()),
+            "acceleration_yardstick": "max |a| of the step (hydrostatic cancellation)"}
+    eng.step(2)
+    rest.update({f"{k}_step3": v for k, v in fields(eng, recs, 0, 3, 2).items()})
+    eng.close()
+    out["from_rest"] = rest
+    # impact on the obstacle
+    eng = DamBreak3DEngine(cfg, obstacle=ob, shift_every=shift_every, host_state=(x, m, w, n_ob),
+                           diag_ring=max_lead + 64, device=dev)
+    lead, f_lead = 0, np.zeros(3)
+    while np.abs(f_lead).max() < 1.0 and lead < max_lead:
+        eng.step(250)
+        lead += 250
+        f_lead = eng.diagnostics(lead - 1, 1).cpu().numpy()[0, 3:6]
+    eng.step(50)
+    lead += 50
+    xs, vs, _, _ = (t.cpu() for t in eng.state())
+    eng.close()
+    t0 = time.perf_counter()
+    recs, _, _ = dam3d.run(cfg, ob, xs.numpy(), m.numpy(), w.numpy(), n_ob, 2, shift_every=shift_every,
+                           v0=vs.numpy(), first_step=lead)
+    port_time += time.perf_counter() - t0
+    port_steps += 2
+    eng = DamBreak3DEngine(cfg, obstacle=ob, shift_every=shift_every, host_state=(xs, m, w, n_ob),
+                           velocity=vs, first_step=lead, diag_ring=64, device=dev)
+    eng.step(2)
+    impact = fields(eng, recs, lead, 2, 1)
+    impact["after_steps"] = lead
+    eng.close()
+    out["impact"] = impact
+    out["port"] = {"value": x.shape[0] * port_steps / port_time, "unit": "fluid particle-updates/s",
+                   "cores": 1, "kind": "port", "seconds": port_time,
+                   "sample": f"{port_steps} FP64 steps of the oracle loop on the {out['rung']} rung"}
+    return out
 
 
 def ensemble_leg(args, dev):
@@ -571,26 +721,42 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    coarse = args.dx * 4.0
+    chunk = args.chunk if args.chunk > 0 else max(1, math.ceil(MIN_TIMED_SOLVER_STEPS / max(args.steps, 1)))
 
     if args.impl == "reference":
         if rank != 0:
             return
-        for _ in range(max(args.warmup, 0) and 1):
-            cpu_baseline(coarse, 1, args.shift_every)
-        sample_steps = max(args.steps // 20, 2)
-        value, n, elapsed, cores = cpu_baseline_all_cores(coarse, sample_steps, args.shift_every)
+        workload = (f"3-D dam break with obstacle (headline geometry), the reference's own CPU step "
+                    f"loop on the dx={args.ref_dx:g} rung")
+        if reference_available():
+            r = reference_loop(args.ref_dx, args.steps, max(args.warmup, 1), args.shift_every)
+            kind = "reference"
+            sample = (f"{args.steps} solver steps after {max(args.warmup, 1)} warm-up steps of the "
+                      f"dx={args.ref_dx:g} rung ({r['fluid']} fluid), tensorsph from baseline/_ref, "
+                      f"torch {r['torch']} {r['dtype']} on {r['cores']} threads ({r['cpu']}), "
+                      f"{r['seconds']:.1f} s, {r['rebuilds']} list builds")
+            value, cores, dtype = r["value"], r["cores"], r["dtype"]
+        else:
+            # the reference is not installed: its algorithm, restated as the
+            # oracle port (numpy FP64, one core)
+            from tensorsph_b200.engine import DamBreak3DEngine, obstacle_case
+            from oracle import dam3d
+            cfg, ob = obstacle_case(dx=args.ref_dx)
+            x, m, w, n_ob = DamBreak3DEngine.build_host_state(cfg, ob)
+            k = max(args.steps // 10, 2)
+            t0 = time.perf_counter()
+            dam3d.run(cfg, ob, x.numpy(), m.numpy(), w.numpy(), n_ob, k, shift_every=args.shift_every,
+                      record=False)
+            el = time.perf_counter() - t0
+            value, cores, dtype, kind = x.shape[0] * k / el, 1, "f64", "port"
+            sample = f"{k} steps of the oracle port on the dx={args.ref_dx:g} rung, {el:.1f} s"
         line = {"metric": "particle-updates/s", "value": value, "unit": "fluid particle-updates/s",
                 "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
                 "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded lattice)",
-                "config": {"workload": f"3-D dam break with obstacle, CPU oracle port on the "
-                           f"dx={coarse:g} rung ({n} fluid)"},
+                "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded lattice)",
+                "config": {"workload": workload},
                 "cpu_baseline": {"value": value, "unit": "fluid particle-updates/s", "cores": cores,
-                                 "kind": "port",
-                                 "sample": f"{sample_steps} steps of the dx={coarse:g} rung ({n} fluid) "
-                                           f"on each of {cores} cores (one independent copy per core, "
-                                           f"summed rates), {elapsed:.1f} s"},
+                                 "kind": kind, "sample": sample},
                 "e2e": {"value": value, "unit": "fluid particle-updates/s",
                         "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -616,14 +782,15 @@ def main():
         tuning = tune_single_case(cfg, obstacle=obstacle, shift_every=args.shift_every,
                                   host_state=host, device=dev)
         cfg = replace(cfg, pair_skin_factor=tuning["best"]["skin_factor"])
-    eng = DamBreak3DEngine(cfg, obstacle=obstacle, shift_every=args.shift_every,
-                           host_state=host, diag_ring=max(args.steps + args.warmup + 64, 256),
+    solver_steps = args.steps * chunk
+    eng = DamBreak3DEngine(cfg, obstacle=obstacle, shift_every=args.shift_every, host_state=host,
+                           diag_ring=max(solver_steps + (max(args.warmup, 3) + 4) * chunk + 64, 256),
                            device=dev)
     if tuning is not None:
         eng.set_block(tuning["best"]["block"])
         eng.set_batch(tuning["best"]["batch"])
     nf, nw = eng.n_fluid, eng.n_wall
-    eng.step(max(args.warmup, 1))
+    eng.step(max(args.warmup, 3) * chunk)
     torch.cuda.synchronize(dev)
     rebuilds_before = eng.status()["rebuilds"]
 
@@ -638,7 +805,8 @@ def main():
     start = torch.cuda.Event(enable_timing=True)
     stop = torch.cuda.Event(enable_timing=True)
     start.record(eng.stream)
-    eng.step(args.steps)
+    for _ in range(args.steps):
+        eng.step(chunk)
     stop.record(eng.stream)
     torch.cuda.synchronize(dev)
     barrier()
@@ -646,25 +814,52 @@ def main():
     ms = max_over_ranks(start.elapsed_time(stop), dist, dev)
     status = eng.status()
     ms_step = ms / args.steps
-    value = whole_job_rate(nf, args.steps, world, ms / 1e3)
-    # every step's kernels, plus the conditional rebuild body once per list
-    # pass that rebuilt during the timed steps
+    ms_solver = ms / solver_steps
+    value = whole_job_rate(nf, solver_steps, world, ms / 1e3)
+    # every solver step's kernels, plus the conditional rebuild body once per
+    # list pass that rebuilt during the timed steps
     kernels_per_step, kernels_per_rebuild = eng.graph_kernels()
     rebuild_passes = status["rebuilds"] - rebuilds_before
-    launches = kernels_per_step * args.steps + kernels_per_rebuild * rebuild_passes
+    launches = kernels_per_step * solver_steps + kernels_per_rebuild * rebuild_passes
+    entries_f, entries_w = eng.row_entries()
 
     stage = {}
     for _ in range(3):
         for k, v in eng.step_timed().items():
             stage.setdefault(k, []).append(v)
     stage = {k: statistics.median(v) for k, v in stage.items()}
-    t_force = stage["force"] / 1e3
-    peak, peak_kind = peaks()
-    achieved = ALGO_BYTES_FORCE * nf / t_force / 1e9
-    traffic_pp = ncu_traffic_per_fluid_particle()
     diag = eng.diagnostics(eng.steps_done - 1, 1).cpu()[0]
     eng.close()
     del eng
+    torch.cuda.empty_cache()
+
+    # roofline: the force pass against HBM, and the step against the binding
+    # one of HBM and the FP32 pipe (both peaks measured here by the library's
+    # probes unless the driver's HBM figure is present)
+    probes = probe_peaks(dev)
+    dp = driver_peaks()
+    hbm_peak = float(dp["hbm_gbs"]) if dp and "hbm_gbs" in dp else probes["copy_gbs"]
+    hbm_src = ("measured (MEASURED_PEAKS.json hbm_gbs)" if dp and "hbm_gbs" in dp
+               else "measured in this run (tsph_probe_copy)")
+    fp32_peak = probes["fp32_tflops"]
+    t_force = stage["force"] / 1e3
+    achieved = ALGO_BYTES_FORCE * nf / t_force / 1e9
+    shift_passes = 1 if args.shift_every else 0
+    flops_step = (entries_f * (PAIR_FLOPS["density"] + PAIR_FLOPS["diffusion"] + PAIR_FLOPS["force"]
+                               + shift_passes * (PAIR_FLOPS["concentration"] + PAIR_FLOPS["gradient"]))
+                  + entries_w * PAIR_FLOPS["walls"])
+    bytes_step = ALGO_BYTES_STEP * nf + ALGO_BYTES_WALL * nw
+    t_hbm = bytes_step / (hbm_peak * 1e9)
+    t_fp32 = flops_step / (fp32_peak * 1e12)
+    binding = {"bound": "fp32" if t_fp32 > t_hbm else "hbm",
+               "frac": max(t_hbm, t_fp32) / (ms_solver / 1e3),
+               "hbm_frac": t_hbm / (ms_solver / 1e3), "fp32_frac": t_fp32 / (ms_solver / 1e3),
+               "bytes_per_step": bytes_step, "flops_per_step": flops_step,
+               "fp32_tflops_achieved": flops_step / (ms_solver / 1e3) / 1e12,
+               "row_entries": {"fluid": entries_f, "wall": entries_w},
+               "flops_per_entry": PAIR_FLOPS,
+               "note": "solver-step time against max(bytes / HBM peak, FLOPs / FP32 peak); FLOPs "
+                       "counted from the kernel source per listed neighbour"}
 
     e2e = None
     if not args.no_e2e:
@@ -678,14 +873,14 @@ def main():
         t0 = time.perf_counter()
         e = DamBreak3DEngine(cfg, obstacle=obstacle, shift_every=args.shift_every,
                              host_state=(pinned[0], pinned[1], pinned[2], n_ob),
-                             diag_ring=args.steps + 8, device=dev)
+                             diag_ring=solver_steps + 8, device=dev)
         if tuning is not None:
             e.set_block(tuning["best"]["block"])
             e.set_batch(tuning["best"]["batch"])
         for k in range(args.steps):
-            e.step(1)
+            e.step(chunk)
             with torch.cuda.stream(e.stream):
-                rows[k].copy_(e.diagnostics(k, 1)[0], non_blocking=True)
+                rows[k].copy_(e.diagnostics((k + 1) * chunk - 1, 1)[0], non_blocking=True)
         xs = e.state()[0]
         with torch.cuda.stream(e.stream):
             final.copy_(xs, non_blocking=True)
@@ -695,18 +890,35 @@ def main():
         t_e2e = max_over_ranks(t_e2e, dist, dev)
         e.close()
         state_bytes = (x.numel() + m.numel() + w.numel()) * 8
-        e2e = {"value": whole_job_rate(nf, args.steps, world, t_e2e), "unit": "fluid particle-updates/s",
+        e2e = {"value": whole_job_rate(nf, solver_steps, world, t_e2e), "unit": "fluid particle-updates/s",
                "h2d_bytes_per_step": state_bytes / args.steps,
                "d2h_bytes_per_step": rows.shape[1] * 8 + nf * 3 * 8 / args.steps,
-               "scope": "engine creation from pinned host lattices + K steps with a per-step "
-                        "meter-row read + final positions read, wall clock"}
+               "scope": "engine creation from pinned host lattices + K bench steps with a meter-row "
+                        "read each + final positions read, wall clock"}
+        torch.cuda.empty_cache()
 
     cpu = None
+    accuracy = None
     if rank == 0 and world == 1 and args.cpu_sample_steps > 0:
-        v_cpu, n_cpu, t_cpu = cpu_baseline(4.0 * args.dx, args.cpu_sample_steps, args.shift_every)
-        cpu = {"value": v_cpu, "unit": "fluid particle-updates/s", "cores": 1, "kind": "port",
-               "sample": f"{args.cpu_sample_steps} steps of the dx={4.0 * args.dx:g} rung "
-                         f"({n_cpu} fluid), {t_cpu:.1f} s"}
+        # the reference's own CPU code, and the FP64 oracle port with the
+        # engine's field errors against it, on the 4x coarser rung
+        port = None
+        try:
+            accuracy = oracle_port_and_errors(args.ref_dx, dev, args.shift_every, tuning)
+            port = accuracy.pop("port")
+        except Exception as exc:  # reported, never hides the headline
+            accuracy = {"error": f"{type(exc).__name__}: {exc}"}
+        if reference_available():
+            r = reference_loop(args.ref_dx, args.ref_sample_steps, 1, args.shift_every)
+            cpu = {"value": r["value"], "unit": "fluid particle-updates/s", "cores": r["cores"],
+                   "kind": "reference",
+                   "sample": f"{args.ref_sample_steps} solver steps after 1 warm-up step of the "
+                             f"dx={args.ref_dx:g} rung ({r['fluid']} fluid): tensorsph from baseline/_ref, "
+                             f"torch {r['torch']} {r['dtype']} on {r['cores']} threads ({r['cpu']}), "
+                             f"{r['seconds']:.1f} s", "port": port}
+        elif port is not None:
+            cpu = dict(port)
+        torch.cuda.empty_cache()
 
     extra = {}
     if rank == 0 and world == 1 and args.ckpt_steps > 0:
@@ -739,27 +951,30 @@ def main():
             "config": {"workload": "3-D dam break with box obstacle: 1.2x1.0x0.55 m fluid in a "
                                    "3.2x1.0x1.0 m tank, obstacle 0.16x0.16x0.4 m, dx="
                                    f"{args.dx:g}", "fluid_particles": nf, "wall_particles": nw,
+                       "solver_steps_per_step": chunk, "ms_per_solver_step": ms_solver,
                        "shift_every": args.shift_every, "density_diffusion": 0.1,
                        "pair_skin_factor": cfg.pair_skin_factor,
                        "tuning": None if tuning is None else tuning["best"],
                        "pairs": "FP32 pair arithmetic, FP64 positions/velocities/meters",
                        "l2": "working set (state + neighbour rows) > 126 MB L2, no flush",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-            "roofline": {"bound": "hbm", "kernel": "k_force", "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None if traffic_pp is None else traffic_pp * nf,
-                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+            "roofline": {"bound": binding["bound"], "kernel": "k_force", "achieved": achieved,
+                         "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                         "traffic": FORCE_TRAFFIC_PER_FLUID * nf,
+                         "traffic_source": f"from_profile: {FORCE_TRAFFIC_RUNG}",
+                         "peak_source": hbm_src,
                          "algorithmic_bytes_per_launch": ALGO_BYTES_FORCE * nf,
                          "launch_ms": stage["force"],
-                         "step_hbm_frac": ALGO_BYTES_STEP * nf / (ms_step / 1e3) / 1e9 / peak,
-                         # what bounds the pass: the L1 data pipe and issue, not HBM
-                         # (ncu, l1tex throughput of the same kernel on the 2x coarser rung)
-                         "l1tex_throughput_frac_ncu": _force_profile_figure("l1tex_throughput_frac")},
+                         "step_hbm_frac": bytes_step / (ms_solver / 1e3) / 1e9 / hbm_peak,
+                         "step_binding": binding},
+            "peaks": {**probes, "hbm_gbs_used": hbm_peak,
+                      "driver": dp if dp else "MEASURED_PEAKS.json absent"},
             "stage_ms": stage,
             "clocks": clocks,
             "gpu_launches": launches,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "errors_vs_fp64": accuracy,
             "engine": {"rebuilds": status["rebuilds"], "escapes": status["escapes"],
                        "obstacle_clamps": status["clamps"], "longest_row": status["row_max"],
                        "last_rho_max": float(diag[0]), "last_speed_max": float(diag[1]),
