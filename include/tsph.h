@@ -433,33 +433,39 @@ int tsph_kick_drift(void* pos, void* vel, const void* acc, int64_t n, int64_t di
                     double dt, int64_t drift, const double* box, tsph_stream stream);
 
 /* ------------------------------------------------------------------------ */
-/* 2-D delta-plus step: delta_plus.py:105-229 (delta_plus_step), h = 2 dx,    */
+/* delta-plus step: delta_plus.py:105-229 (delta_plus_step), h = 2 dx,        */
 /* Wendland C2, linear EOS, ghost walls with unit normals, psi diffusion,     */
-/* interface band, regularised shift and wall tangent.  Synchronises once to  */
-/* report TSPH_ERR_STATE (status bit 0: nonpositive wall density, bit 1:       */
+/* interface band, regularised shift and wall tangent.  dim 2 (or 0) is the   */
+/* reference's 2-D step; dim 3 the same statements in 3-D (the 3-D Wendland   */
+/* constant, radial viscosity 2 (D + 2) nu, wall stations of volume dx^3, the */
+/* 3 x 3 first moment, |ray x n| in the empty-cap test, and a conflicting     */
+/* wall tangent reduced to the line n_wall x n_surface), which the reference  */
+/* does not have (its dimension check: delta_plus.py:119).  Synchronises once */
+/* to report TSPH_ERR_STATE (status bit 0: nonpositive wall density, bit 1:   */
 /* nonpositive or non-finite density).                                        */
 /* ------------------------------------------------------------------------ */
 typedef struct {
   int64_t dtype, n_fluid, n_wall;
   double dx, sound_speed, reference_speed, dt, rho0, gravity, viscosity, diffusion, alpha;
+  int64_t dim;                /* 2 (0 reads as 2) or 3                    */
 } tsph_delta_plus_params;
 
 typedef struct {
-  const void* pos;            /* (n, 2)                                   */
-  const void* vel;            /* (n, 2)                                   */
+  const void* pos;            /* (n, D)                                   */
+  const void* vel;            /* (n, D)                                   */
   const void* density;        /* (n)                                      */
   const void* mass;           /* (n)                                      */
-  const void* wall;           /* (nw, 2) or NULL                          */
-  const void* wall_vel;       /* (nw, 2) or NULL                          */
-  const void* wall_normal;    /* (nw, 2) or NULL, any nonzero length      */
+  const void* wall;           /* (nw, D) or NULL                          */
+  const void* wall_vel;       /* (nw, D) or NULL                          */
+  const void* wall_normal;    /* (nw, D) or NULL, any nonzero length      */
   const int64_t* rowptr;      /* symmetric rows over n + nw particles     */
   const uint32_t* entries;
-  void* out_pos;              /* (n, 2)                                   */
-  void* out_vel;              /* (n, 2)                                   */
+  void* out_pos;              /* (n, D)                                   */
+  void* out_vel;              /* (n, D)                                   */
   void* out_density;          /* (n)                                      */
-  void* acc;                  /* (n, 2)                                   */
-  void* reaction;             /* (nw, 2) integrated wall forces           */
-  void* shift;                /* (n, 2)                                   */
+  void* acc;                  /* (n, D)                                   */
+  void* reaction;             /* (nw, D) integrated wall forces           */
+  void* shift;                /* (n, D)                                   */
   int* status_out;            /* host, nullable                           */
 } tsph_delta_plus_io;
 

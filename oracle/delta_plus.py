@@ -1,4 +1,4 @@
-"""Oracle (test infrastructure only): the 2-D delta-plus step.
+"""Oracle (test infrastructure only): the delta-plus step, 2-D and 3-D.
 
 numpy restatement of delta_plus.py:105-229 (``delta_plus_step``) with its
 helpers: the fluid geometry of :36-50 (first moment M, eigenvalues, eigen-
@@ -6,6 +6,24 @@ floored inverse and the renormalised gradient), the boundary band of :53-69,
 the regularisation of :72-76 and the wall tangent of :79-102, plus the
 psi-form diffusion of density_diffusion.py:145-172.  h = 2 dx, Wendland C2.
 Pairs: unique i < j within 2h (strict), fluid first, wall-wall pairs dropped.
+
+The reference step is 2-D only (delta_plus.py:119).  The same statements are
+written here for D = 2 or 3 (read from the positions' shape); for D = 2 every
+operation is the reference's.  What D = 3 changes, each a generalisation of a
+2-D statement with no 3-D reference to pin it:
+
+* the 3-D Wendland C2 constant 21 / (16 pi h^3) (threed/kernel3.py:139-164);
+* Monaghan's radial viscous stress coefficient 2 (D + 2) nu (8 nu in 2-D,
+  as the comment at delta_plus.py:185 derives it);
+* wall stations of volume dx^D (dx^2 per unit span in 2-D); gravity along -y;
+* the D x D first moment and its eigen-decomposition;
+* the empty-cap test's tangential distance |ray x n| (the 2-D cross product
+  is its z component);
+* the wall tangent: a particle whose wall-tangent shift conflicts with the
+  interface normal keeps the part of that shift along the line both tangent
+  planes share (n_wall x n_surface); in 2-D the two tangent lines share only
+  the origin, which is the reference's zero.  Stations at the same distance
+  with conflicting normals pin the particle, as in 2-D.
 """
 from __future__ import annotations
 
@@ -16,20 +34,27 @@ import numpy as np
 from .neighbors import cell_linked_pairs
 
 
-def wendland(r, h):
+def wendland_sigma(h, dim=2):
+    """Wendland C2 normalisation: 7 / (4 pi h^2) in 2-D (droplet_impact.py:320-346),
+    21 / (16 pi h^3) in 3-D (threed/kernel3.py:139-164)."""
+    return 7.0 / (4.0 * math.pi * h * h) if dim == 2 else 21.0 / (16.0 * math.pi * h * h * h)
+
+
+def wendland(r, h, dim=2):
     T = r.dtype.type
     q = r / T(h)
     t = np.maximum(T(1) - T(0.5) * q, T(0))
-    return T(7.0 / (4.0 * math.pi * h * h)) * t ** 4 * (T(2) * q + T(1))
+    return T(wendland_sigma(h, dim)) * t ** 4 * (T(2) * q + T(1))
 
 
 def wendland_grad(delta, h, eps=1.0e-12):
     T = delta.dtype.type
+    dim = delta.shape[1]
     r = np.sqrt((delta * delta).sum(1))
     q = r / T(h)
     t = np.maximum(T(1) - T(0.5) * q, T(0))
     ds = T(-5.0) * q * t ** 3
-    scale = T(7.0 / (4.0 * math.pi * h * h)) * ds / (T(h) * np.maximum(r, T(eps)))
+    scale = T(wendland_sigma(h, dim)) * ds / (T(h) * np.maximum(r, T(eps)))
     return delta * scale[:, None]
 
 
@@ -51,11 +76,12 @@ def delta_plus_step(pos, velocity, density, mass, *, dx, sound_speed, reference_
                     wall=None, wall_velocity=None, wall_normal=None, pairs=None):
     T = pos.dtype.type
     dt_ = pos.dtype
-    n = pos.shape[0]
+    n, D = pos.shape
     h = 2 * dx
-    nu_r = 8 * viscosity + alpha * h * sound_speed
+    nu_r = 2 * (D + 2) * viscosity + alpha * h * sound_speed
+    vol_w = dx ** D   # wall station volume
     if wall is None:
-        wall = np.zeros((0, 2), dtype=dt_)
+        wall = np.zeros((0, D), dtype=dt_)
     if wall_velocity is None:
         wall_velocity = np.zeros_like(wall)
     if wall_normal is None:
@@ -69,7 +95,7 @@ def delta_plus_step(pos, velocity, density, mass, *, dx, sound_speed, reference_
     i, j = i[keep], j[keep]
     sep = cloud[i] - cloud[j]
     radius = np.sqrt((sep * sep).sum(1))
-    weight = wendland(radius, h)
+    weight = wendland(radius, h, D)
     grad = wendland_grad(sep, h)
     ff = j < n
     a, b, d, g = i[ff], j[ff], sep[ff], grad[ff]
@@ -95,31 +121,33 @@ def delta_plus_step(pos, velocity, density, mass, *, dx, sound_speed, reference_
     closing = ((velocity[f] - wall_velocity[w]) * toward).sum(1)
     normal_grad = (gw * toward).sum(1)[:, None] * toward
     twice = p[f] + wall_p[w] + T(2) * density[f] * T(sound_speed) * closing
-    wall_force = -(volume[f] * T(dx ** 2) * twice)[:, None] * normal_grad
-    net = _both((n, 2), dt_, a, b, force, -force)
+    wall_force = -(volume[f] * T(vol_w) * twice)[:, None] * normal_grad
+    net = _both((n, D), dt_, a, b, force, -force)
     np.add.at(net, f, wall_force)
-    reaction = np.zeros((nw, 2), dtype=dt_)
+    reaction = np.zeros((nw, D), dtype=dt_)
     np.add.at(reaction, w, -wall_force)
-    acc = net / mass[:, None] + np.array([0.0, -gravity], dtype=dt_)
+    gvec = np.zeros(D, dtype=dt_)
+    gvec[1] = -gravity
+    acc = net / mass[:, None] + gvec
     new_v = velocity + T(dt) * acc
 
     # fluid geometry (delta_plus.py:36-50)
     outer = -d[:, :, None] * g[:, None, :]
-    moment = _both((n, 2, 2), dt_, a, b, volume[b, None, None] * outer, volume[a, None, None] * outer)
+    moment = _both((n, D, D), dt_, a, b, volume[b, None, None] * outer, volume[a, None, None] * outer)
     eig, axes = _eigh2(moment)
     floor = np.maximum(T(0.1) * eig.mean(1, keepdims=True), T(1.0e-12))
     inverse = (axes / np.maximum(eig, floor)[:, None, :]) @ np.transpose(axes, (0, 2, 1))
 
     def gradient(values):
         pg = (values[b] - values[a])[:, None] * g
-        s = _both((n, 2), dt_, a, b, volume[b, None] * pg, volume[a, None] * pg)
+        s = _both((n, D), dt_, a, b, volume[b, None] * pg, volume[a, None] * pg)
         return (inverse @ s[:, :, None])[:, :, 0]
 
     lam = eig[:, 0]
     div_pair = ((new_v[b] - new_v[a]) * g).sum(1)
     div = _both((n,), dt_, a, b, volume[b] * div_pair, volume[a] * div_pair)
     normal_speed = ((wall_velocity[w] - new_v[f]) * n_wall).sum(1)
-    np.add.at(div, f, T(2 * dx ** 2) * normal_speed * (n_wall * gw).sum(1))
+    np.add.at(div, f, T(2 * vol_w) * normal_speed * (n_wall * gw).sum(1))
     rate = -density * div
     if diffusion:
         grad_rho = gradient(density)
@@ -142,7 +170,10 @@ def delta_plus_step(pos, velocity, density, mass, *, dx, sound_speed, reference_
 
     def occupied(ray, direction):
         axial = (ray * direction).sum(1)
-        tang = np.abs(ray[:, 0] * direction[:, 1] - ray[:, 1] * direction[:, 0])
+        if D == 2:
+            tang = np.abs(ray[:, 0] * direction[:, 1] - ray[:, 1] * direction[:, 0])
+        else:
+            tang = np.sqrt((np.cross(ray, direction) ** 2).sum(1))
         off = ray - T(h) * direction
         return np.where((ray * ray).sum(1) >= T(2 * h * h), (off * off).sum(1) < T(h * h),
                         np.abs(axial - T(h)) + tang < T(h))
@@ -154,11 +185,11 @@ def delta_plus_step(pos, velocity, density, mass, *, dx, sound_speed, reference_
     strength = mag * T(h)
 
     # positional shift (delta_plus.py:205-226)
-    w_ref = wendland(np.array([dx], dtype=dt_), h)[0]
+    w_ref = wendland(np.array([dx], dtype=dt_), h, D)[0]
     repulsion = (T(1) + T(0.2) * (weight / w_ref) ** 4)[:, None] * grad
     q = repulsion[ff] / (density[a] + density[b])[:, None]
-    raw = _both((n, 2), dt_, a, b, mass[b, None] * q, -mass[a, None] * q)
-    wall_ratio = wall_rho[w] * T(dx ** 2) / (density[f] + wall_rho[w])
+    raw = _both((n, D), dt_, a, b, mass[b, None] * q, -mass[a, None] * q)
+    wall_ratio = wall_rho[w] * T(vol_w) / (density[f] + wall_rho[w])
     np.add.at(raw, f, wall_ratio[:, None] * repulsion[~ff])
     raw = raw * T(-(dt * sound_speed / h) * (reference_speed / sound_speed) * (2 * h) ** 2)
     tangent = raw - (raw * normal).sum(1)[:, None] * normal
@@ -179,7 +210,18 @@ def delta_plus_step(pos, velocity, density, mass, *, dx, sound_speed, reference_
         tol = T(1.0e-6) * np.sqrt((shift * shift).sum(1))
         conflict = band & (np.abs((tan * normal).sum(1)) > tol)
         other = np.abs((tan[part] * normals).sum(1)) > tol[part]
-        np.maximum.at(conflict, part, other)
-        shift = np.where(np.isfinite(nearest)[:, None], np.where(conflict[:, None], T(0), tan), shift)
+        pinned = np.zeros(n, dtype=bool)
+        np.maximum.at(pinned, part, other)
+        if D == 2:
+            keep = tan * T(0)
+        else:
+            # the line both tangent planes share: n_wall x n_surface
+            line = np.cross(direction, normal)
+            ln = np.sqrt((line * line).sum(1))
+            line = np.where((ln > T(1.0e-12))[:, None], line / np.maximum(ln, T(1.0e-30))[:, None], T(0))
+            keep = (tan * line).sum(1)[:, None] * line
+        constrained = np.where(conflict[:, None], keep, tan)
+        constrained = np.where(pinned[:, None], T(0), constrained)
+        shift = np.where(np.isfinite(nearest)[:, None], constrained, shift)
     return {"position": pos + T(dt) * new_v + shift, "velocity": new_v, "density": new_rho,
             "acceleration": acc, "wall_reaction": reaction, "shift": shift}

@@ -124,7 +124,8 @@ class ClampParams(ctypes.Structure):
 class DeltaPlusParams(ctypes.Structure):
     _fields_ = [(k, c_int64) for k in ("dtype", "n_fluid", "n_wall")] + \
                [(k, c_double) for k in ("dx", "sound_speed", "reference_speed", "dt", "rho0",
-                                        "gravity", "viscosity", "diffusion", "alpha")]
+                                        "gravity", "viscosity", "diffusion", "alpha")] + \
+               [("dim", c_int64)]
 
 
 class DeltaPlusIO(ctypes.Structure):

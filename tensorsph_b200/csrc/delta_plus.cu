@@ -1,4 +1,5 @@
-// One 2-D delta-plus step (delta_plus.py:105-229) over symmetric gather rows.
+// One delta-plus step (delta_plus.py:105-229) over symmetric gather rows, in
+// 2-D (the reference's step) or 3-D (the same statements for D = 3).
 //
 //   P0 fluid    V = m / rho, p = c0^2 (rho - rho0)
 //   P1 walls    ghost pressure p_w = sum W (p_f + rho_f g (y_f - y_w)) / sum W,
@@ -6,7 +7,7 @@
 //               reaction (minus the wall force it exerts on its fluid pairs)
 //   P2 fluid    pressure + Monaghan radial viscosity + slip-wall force ->
 //               acc, v' = v + dt acc; first moment M, its eigenvalues (lambda =
-//               the smaller) and the eigen-floored inverse (delta_plus.py:36-45)
+//               the smallest) and the eigen-floored inverse (delta_plus.py:36-45)
 //   P3 fluid    continuity div v' with the wall flux, renormalised grad rho
 //               and grad lambda, interface normal and strength
 //   P4 fluid    psi-form diffusion (density_diffusion.py:145-172), rho',
@@ -16,7 +17,15 @@
 // Pairs are kept when |x_i - x_j|^2 < (2h)^2 (strictly), h = 2 dx; each row
 // sums its own contributions in the input dtype (compensated in FP32), so
 // the result does not depend on the order of the pair list.
+//
+// 3-D (no reference step; each item generalises a 2-D statement): Wendland C2
+// with 21 / (16 pi h^3); radial viscosity 2 (D + 2) nu + alpha h c0; wall
+// stations of volume dx^3; gravity along -y; the 3 x 3 first moment; the
+// empty-cap tangential distance |ray x n|; and a wall-tangent shift that
+// conflicts with the interface normal keeps its part along n_wall x n_surface
+// (in 2-D the two tangent lines share only the origin: the reference's zero).
 #include <cmath>
+#include <limits>
 
 #include "common.cuh"
 #include "sphkernels.cuh"
@@ -27,10 +36,19 @@ namespace {
 
 constexpr uint32_t kIdx = 0x7fffffffu;
 
+// packed symmetric D x D: 2-D (00, 01, 11), 3-D (00, 01, 02, 11, 12, 22)
+template <int D>
+struct Sym {
+  static constexpr int N = D * (D + 1) / 2;
+  __host__ __device__ static constexpr int at(int i, int j) {
+    return D == 2 ? (i + j) : (i <= j ? (i == 0 ? j : (i == 1 ? 2 + j : 5)) : at(j, i));
+  }
+};
+
 template <class T>
 struct DPP {
   int64_t n, nw;
-  T dx, h, c0, c2, rho0, g, rho0_nu, dt, dscale, shift_scale, w_ref, support2, dx2, tiny;
+  T dx, h, c0, c2, rho0, g, rho0_nu, dt, dscale, shift_scale, w_ref, support2, dxd, tiny;
   Wendland<T> k;
 };
 
@@ -55,27 +73,51 @@ struct DPW {
   T* vol;
   T* p;
   T* lam;
-  T* inv;    // 3 per fluid row: inv00, inv01, inv11
-  T* grho;   // 2 per fluid row
-  T* nrm;    // 2 per fluid row: interface normal
+  T* inv;    // D (D + 1) / 2 per fluid row (Sym<D>)
+  T* grho;   // D per fluid row
+  T* nrm;    // D per fluid row: interface normal
   T* str;    // interface strength |grad lambda| h
   T* rate;   // -rho div v'
   int* surf;
   T* wp;     // wall pressure
   T* wrho;   // wall density
-  T* wn;     // unit wall normals
+  T* wn;     // unit wall normals, D per station
   int* status;  // bit 0: nonpositive wall density, bit 1: nonpositive/non-finite density
 };
 
+template <class T, int D>
+__device__ __forceinline__ void point(const DPP<T>& p, const DPW<T>& w, int64_t r, T x[D]) {
+  const T* src = r < p.n ? w.pos + D * r : w.wall + D * (r - p.n);
+#pragma unroll
+  for (int k = 0; k < D; ++k) x[k] = src[k];
+}
+
+template <class T, int D>
+__device__ __forceinline__ T dot(const T a[D], const T b[D]) {
+  T s = a[0] * b[0];
+#pragma unroll
+  for (int k = 1; k < D; ++k) s = s + a[k] * b[k];
+  return s;
+}
+
 template <class T>
-__device__ __forceinline__ void xy(const DPP<T>& p, const DPW<T>& w, int64_t r, T& x, T& y) {
-  if (r < p.n) {
-    x = w.pos[2 * r];
-    y = w.pos[2 * r + 1];
-  } else {
-    x = w.wall[2 * (r - p.n)];
-    y = w.wall[2 * (r - p.n) + 1];
-  }
+__device__ __forceinline__ T sgn(T v) {
+  return v > T(0) ? T(1) : (v < T(0) ? T(-1) : T(0));
+}
+
+template <class T>
+__device__ __forceinline__ T absv(T v) {
+  return v < T(0) ? -v : v;
+}
+
+// |a x b|: the 2-D cross product's magnitude, or the 3-D cross product's norm
+template <class T, int D>
+__device__ __forceinline__ T cross_norm(const T a[D], const T b[D]) {
+  if (D == 2) return absv(a[0] * b[1] - a[1] * b[0]);
+  const T cx = a[1] * b[D - 1] - a[D - 1] * b[1];
+  const T cy = a[D - 1] * b[0] - a[0] * b[D - 1];
+  const T cz = a[0] * b[1] - a[1] * b[0];
+  return sqrt(cx * cx + cy * cy + cz * cz);
 }
 
 template <class T>
@@ -86,178 +128,261 @@ __global__ void p0_state(DPP<T> p, DPW<T> w) {
   }
 }
 
-template <class T>
+template <class T, int D>
 __global__ void p1_walls(DPP<T> p, DPW<T> w) {
   for (int64_t s = blockIdx.x * blockDim.x + threadIdx.x; s < p.nw; s += gridDim.x * blockDim.x) {
     const int64_t r = p.n + s;
-    const T xw = w.wall[2 * s], yw = w.wall[2 * s + 1];
-    T nx = w.wall_normal[2 * s], ny = w.wall_normal[2 * s + 1];
-    const T nn = sqrt(nx * nx + ny * ny);
-    nx = nx / nn;
-    ny = ny / nn;
-    w.wn[2 * s] = nx;
-    w.wn[2 * s + 1] = ny;
+    T xw[D], nv[D];
+    point<T, D>(p, w, r, xw);
+#pragma unroll
+    for (int k = 0; k < D; ++k) nv[k] = w.wall_normal[D * s + k];
+    const T nn = sqrt(dot<T, D>(nv, nv));
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      nv[k] = nv[k] / nn;
+      w.wn[D * s + k] = nv[k];
+    }
     CSum<T> num, den;
     int pairs = 0;
     for (int64_t e = w.rowptr[r]; e < w.rowptr[r + 1]; ++e) {
       const int64_t f = w.ent[e] & kIdx;
       if (f >= p.n) continue;
-      const T dxf = w.pos[2 * f] - xw, dyf = w.pos[2 * f + 1] - yw;  // x_f - x_w
-      const T r2 = dxf * dxf + dyf * dyf;
+      T d[D];  // x_f - x_w
+#pragma unroll
+      for (int k = 0; k < D; ++k) d[k] = w.pos[D * f + k] - xw[k];
+      const T r2 = dot<T, D>(d, d);
       if (!(r2 < p.support2)) continue;
       const T W = p.k.w(sqrt(r2));
-      num.add(W * (w.p[f] + w.rho[f] * p.g * dyf));
+      num.add(W * (w.p[f] + w.rho[f] * p.g * d[1]));
       den.add(W);
       ++pairs;
     }
-    const T d = den.value();
-    const T wp = num.value() / (d > p.tiny ? d : p.tiny);
+    const T dd = den.value();
+    const T wp = num.value() / (dd > p.tiny ? dd : p.tiny);
     const T wr = p.rho0 + wp / p.c2;
     w.wp[s] = wp;
     w.wrho[s] = wr;
     if (pairs > 0 && !(wr > T(0))) atomicOr(w.status, 1);
     // reaction: minus the force this station exerts on each fluid pair
-    CSum<T> rx, ry;
+    CSum<T> rc[D];
     for (int64_t e = w.rowptr[r]; e < w.rowptr[r + 1]; ++e) {
       const int64_t f = w.ent[e] & kIdx;
       if (f >= p.n) continue;
-      const T dxf = w.pos[2 * f] - xw, dyf = w.pos[2 * f + 1] - yw;
-      const T r2 = dxf * dxf + dyf * dyf;
+      T d[D];
+#pragma unroll
+      for (int k = 0; k < D; ++k) d[k] = w.pos[D * f + k] - xw[k];
+      const T r2 = dot<T, D>(d, d);
       if (!(r2 < p.support2)) continue;
       T W, gs;
       p.k.wg(sqrt(r2), W, gs);
-      const T gx = dxf * gs, gy = dyf * gs;  // grad_f W
-      const T gn = gx * nx + gy * ny;
-      const T sg = gn > T(0) ? T(1) : (gn < T(0) ? T(-1) : T(0));
-      const T tx = nx * sg, ty = ny * sg;
-      const T closing = (w.vel[2 * f] - w.wall_vel[2 * s]) * tx + (w.vel[2 * f + 1] - w.wall_vel[2 * s + 1]) * ty;
-      const T ng = gx * tx + gy * ty;
+      T gv[D], tv[D], rel[D];
+#pragma unroll
+      for (int k = 0; k < D; ++k) gv[k] = d[k] * gs;  // grad_f W
+      const T sg = sgn(dot<T, D>(gv, nv));
+#pragma unroll
+      for (int k = 0; k < D; ++k) {
+        tv[k] = nv[k] * sg;
+        rel[k] = w.vel[D * f + k] - w.wall_vel[D * s + k];
+      }
+      const T closing = dot<T, D>(rel, tv);
+      const T ng = dot<T, D>(gv, tv);
       const T twice = w.p[f] + wp + T(2) * w.rho[f] * p.c0 * closing;
-      const T c = -(w.vol[f] * p.dx2 * twice) * ng;
-      rx.add(-(c * tx));
-      ry.add(-(c * ty));
+      const T c = -(w.vol[f] * p.dxd * twice) * ng;
+#pragma unroll
+      for (int k = 0; k < D; ++k) rc[k].add(-(c * tv[k]));
     }
-    w.reaction[2 * s] = rx.value();
-    w.reaction[2 * s + 1] = ry.value();
+#pragma unroll
+    for (int k = 0; k < D; ++k) w.reaction[D * s + k] = rc[k].value();
   }
 }
 
-template <class T>
+template <class T, int D>
 __global__ void p2_force(DPP<T> p, DPW<T> w) {
+  using S = Sym<D>;
   for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < p.n; a += gridDim.x * blockDim.x) {
-    const T xa = w.pos[2 * a], ya = w.pos[2 * a + 1];
-    const T vxa = w.vel[2 * a], vya = w.vel[2 * a + 1];
+    T xa[D], va[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      xa[k] = w.pos[D * a + k];
+      va[k] = w.vel[D * a + k];
+    }
     const T Va = w.vol[a], pa = w.p[a], ra = w.rho[a];
-    CSum<T> fx, fy, m00, m01, m11;
+    CSum<T> fc[D], mom[S::N];
     for (int64_t e = w.rowptr[a]; e < w.rowptr[a + 1]; ++e) {
       const int64_t b = w.ent[e] & kIdx;
-      T xb, yb;
-      xy(p, w, b, xb, yb);
-      const T dx = xa - xb, dy = ya - yb;
-      const T r2 = dx * dx + dy * dy;
+      T xb[D], d[D];
+      point<T, D>(p, w, b, xb);
+#pragma unroll
+      for (int k = 0; k < D; ++k) d[k] = xa[k] - xb[k];
+      const T r2 = dot<T, D>(d, d);
       if (!(r2 < p.support2)) continue;
       T W, gs;
       p.k.wg(sqrt(r2), W, gs);
-      const T gx = dx * gs, gy = dy * gs;
+      T gv[D];
+#pragma unroll
+      for (int k = 0; k < D; ++k) gv[k] = d[k] * gs;
       if (b < p.n) {
         const T Vb = w.vol[b];
         T c = -(Va * Vb * (pa + w.p[b]));
         if (p.rho0_nu != T(0)) {
-          const T approach = (vxa - w.vel[2 * b]) * dx + (vya - w.vel[2 * b + 1]) * dy;
+          T dv[D];
+#pragma unroll
+          for (int k = 0; k < D; ++k) dv[k] = va[k] - w.vel[D * b + k];
+          const T approach = dot<T, D>(dv, d);
           const T floor2 = T(1e-12) * p.h * p.h;
           const T pi = approach / (r2 > floor2 ? r2 : floor2);
           c = c + p.rho0_nu * Va * Vb * pi;
         }
-        fx.add(c * gx);
-        fy.add(c * gy);
+#pragma unroll
+        for (int k = 0; k < D; ++k) fc[k].add(c * gv[k]);
         // M += V_b (-d) (x) grad W
-        m00.add(Vb * -(dx * gx));
-        m01.add(Vb * -(dx * gy));
-        m11.add(Vb * -(dy * gy));
+#pragma unroll
+        for (int i = 0; i < D; ++i)
+#pragma unroll
+          for (int j = i; j < D; ++j) mom[S::at(i, j)].add(Vb * -(d[i] * gv[j]));
       } else {
         const int64_t s = b - p.n;
-        const T nx = w.wn[2 * s], ny = w.wn[2 * s + 1];
-        const T gn = gx * nx + gy * ny;
-        const T sg = gn > T(0) ? T(1) : (gn < T(0) ? T(-1) : T(0));
-        const T tx = nx * sg, ty = ny * sg;
-        const T closing = (vxa - w.wall_vel[2 * s]) * tx + (vya - w.wall_vel[2 * s + 1]) * ty;
-        const T ng = gx * tx + gy * ty;
+        T nv[D], tv[D], rel[D];
+#pragma unroll
+        for (int k = 0; k < D; ++k) nv[k] = w.wn[D * s + k];
+        const T sg = sgn(dot<T, D>(gv, nv));
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+          tv[k] = nv[k] * sg;
+          rel[k] = va[k] - w.wall_vel[D * s + k];
+        }
+        const T closing = dot<T, D>(rel, tv);
+        const T ng = dot<T, D>(gv, tv);
         const T twice = pa + w.wp[s] + T(2) * ra * p.c0 * closing;
-        const T c = -(Va * p.dx2 * twice) * ng;
-        fx.add(c * tx);
-        fy.add(c * ty);
+        const T c = -(Va * p.dxd * twice) * ng;
+#pragma unroll
+        for (int k = 0; k < D; ++k) fc[k].add(c * tv[k]);
       }
     }
     const T m = w.mass[a];
-    const T ax = fx.value() / m, ay = fy.value() / m - p.g;
-    w.acc[2 * a] = ax;
-    w.acc[2 * a + 1] = ay;
-    w.out_vel[2 * a] = vxa + p.dt * ax;
-    w.out_vel[2 * a + 1] = vya + p.dt * ay;
-    // eigenvalues and the eigen-floored inverse of M (delta_plus.py:39-42)
-    double mm[3][3] = {{static_cast<double>(m00.value()), 0, 0}, {static_cast<double>(m01.value()), 0, 0}, {0, 0, 0}};
-    mm[1][1] = static_cast<double>(m11.value());
-    mm[0][1] = mm[1][0];
-    double lam[2], vec[2][2];
-    eig2(mm, lam, vec);
-    double fl = 0.1 * 0.5 * (lam[0] + lam[1]);
-    fl = fl > 1e-12 ? fl : 1e-12;
-    double inv[3] = {0, 0, 0};
-    for (int k = 0; k < 2; ++k) {
-      const double l = lam[k] > fl ? lam[k] : fl;
-      inv[0] += vec[k][0] * vec[k][0] / l;
-      inv[1] += vec[k][0] * vec[k][1] / l;
-      inv[2] += vec[k][1] * vec[k][1] / l;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      const T ak = fc[k].value() / m - (k == 1 ? p.g : T(0));
+      w.acc[D * a + k] = ak;
+      w.out_vel[D * a + k] = va[k] + p.dt * ak;
     }
-    w.lam[a] = static_cast<T>(lam[0]);
-    w.inv[3 * a] = static_cast<T>(inv[0]);
-    w.inv[3 * a + 1] = static_cast<T>(inv[1]);
-    w.inv[3 * a + 2] = static_cast<T>(inv[2]);
+    // eigenvalues and the eigen-floored inverse of M (delta_plus.py:39-42)
+    double mm[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+      for (int j = 0; j < D; ++j) mm[i][j] = static_cast<double>(mom[S::at(i, j)].value());
+    double lam[3] = {0, 0, 0}, vec[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    if (D == 2) {
+      double v2[2][2];
+      eig2(mm, lam, v2);
+      for (int k = 0; k < 2; ++k)
+        for (int i = 0; i < 2; ++i) vec[k][i] = v2[k][i];
+    } else {
+      eig3(mm, lam, vec);
+    }
+    double lmin = lam[0], sum = lam[0];
+#pragma unroll
+    for (int k = 1; k < D; ++k) {
+      lmin = lam[k] < lmin ? lam[k] : lmin;
+      sum += lam[k];
+    }
+    double fl = 0.1 * (sum / D);
+    fl = fl > 1e-12 ? fl : 1e-12;
+    double inv[S::N];
+#pragma unroll
+    for (int q = 0; q < S::N; ++q) inv[q] = 0.0;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      const double l = lam[k] > fl ? lam[k] : fl;
+#pragma unroll
+      for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int j = i; j < D; ++j) inv[S::at(i, j)] += vec[k][i] * vec[k][j] / l;
+    }
+    w.lam[a] = static_cast<T>(lmin);
+#pragma unroll
+    for (int q = 0; q < S::N; ++q) w.inv[S::N * a + q] = static_cast<T>(inv[q]);
   }
 }
 
-template <class T>
+template <class T, int D>
+__device__ __forceinline__ void apply_inverse(const T* inv, const T s[D], T out[D]) {
+  using S = Sym<D>;
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    T acc = inv[S::at(i, 0)] * s[0];
+#pragma unroll
+    for (int j = 1; j < D; ++j) acc = acc + inv[S::at(i, j)] * s[j];
+    out[i] = acc;
+  }
+}
+
+template <class T, int D>
 __global__ void p3_geometry(DPP<T> p, DPW<T> w) {
+  using S = Sym<D>;
   for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < p.n; a += gridDim.x * blockDim.x) {
-    const T xa = w.pos[2 * a], ya = w.pos[2 * a + 1];
-    const T ux = w.out_vel[2 * a], uy = w.out_vel[2 * a + 1];
+    T xa[D], ua[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      xa[k] = w.pos[D * a + k];
+      ua[k] = w.out_vel[D * a + k];
+    }
     const T ra = w.rho[a], la = w.lam[a];
-    CSum<T> div, grx, gry, glx, gly;
+    CSum<T> div, gr[D], gl[D];
     for (int64_t e = w.rowptr[a]; e < w.rowptr[a + 1]; ++e) {
       const int64_t b = w.ent[e] & kIdx;
-      T xb, yb;
-      xy(p, w, b, xb, yb);
-      const T dx = xa - xb, dy = ya - yb;
-      const T r2 = dx * dx + dy * dy;
+      T xb[D], d[D];
+      point<T, D>(p, w, b, xb);
+#pragma unroll
+      for (int k = 0; k < D; ++k) d[k] = xa[k] - xb[k];
+      const T r2 = dot<T, D>(d, d);
       if (!(r2 < p.support2)) continue;
       T W, gs;
       p.k.wg(sqrt(r2), W, gs);
-      const T gx = dx * gs, gy = dy * gs;
+      T gv[D];
+#pragma unroll
+      for (int k = 0; k < D; ++k) gv[k] = d[k] * gs;
       if (b < p.n) {
         const T Vb = w.vol[b];
-        div.add(Vb * ((w.out_vel[2 * b] - ux) * gx + (w.out_vel[2 * b + 1] - uy) * gy));
+        T du[D];
+#pragma unroll
+        for (int k = 0; k < D; ++k) du[k] = w.out_vel[D * b + k] - ua[k];
+        div.add(Vb * dot<T, D>(du, gv));
         const T dr = Vb * (w.rho[b] - ra), dl = Vb * (w.lam[b] - la);
-        grx.add(dr * gx);
-        gry.add(dr * gy);
-        glx.add(dl * gx);
-        gly.add(dl * gy);
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+          gr[k].add(dr * gv[k]);
+          gl[k].add(dl * gv[k]);
+        }
       } else {
         const int64_t s = b - p.n;
-        const T nx = w.wn[2 * s], ny = w.wn[2 * s + 1];
-        const T ns = (w.wall_vel[2 * s] - ux) * nx + (w.wall_vel[2 * s + 1] - uy) * ny;
-        div.add(T(2) * p.dx2 * ns * (nx * gx + ny * gy));
+        T nv[D], rel[D];
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+          nv[k] = w.wn[D * s + k];
+          rel[k] = w.wall_vel[D * s + k] - ua[k];
+        }
+        const T ns = dot<T, D>(rel, nv);
+        div.add(T(2) * p.dxd * ns * dot<T, D>(nv, gv));
       }
     }
-    const T i0 = w.inv[3 * a], i1 = w.inv[3 * a + 1], i2 = w.inv[3 * a + 2];
-    const T sx = grx.value(), sy = gry.value();
-    w.grho[2 * a] = i0 * sx + i1 * sy;
-    w.grho[2 * a + 1] = i1 * sx + i2 * sy;
-    const T lx = glx.value(), ly = gly.value();
-    const T gx = i0 * lx + i1 * ly, gy = i1 * lx + i2 * ly;
-    const T mag = sqrt(gx * gx + gy * gy);
+    const T* inv = w.inv + S::N * a;
+    T sr[D], sl[D], outr[D], outl[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      sr[k] = gr[k].value();
+      sl[k] = gl[k].value();
+    }
+    apply_inverse<T, D>(inv, sr, outr);
+    apply_inverse<T, D>(inv, sl, outl);
+    const T mag = sqrt(dot<T, D>(outl, outl));
     const T den = mag > T(1e-12) ? mag : T(1e-12);
-    w.nrm[2 * a] = -gx / den;
-    w.nrm[2 * a + 1] = -gy / den;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      w.grho[D * a + k] = outr[k];
+      w.nrm[D * a + k] = -outl[k] / den;
+    }
     w.str[a] = mag * p.h;
     w.rate[a] = -ra * div.value();
   }
@@ -265,39 +390,53 @@ __global__ void p3_geometry(DPP<T> p, DPW<T> w) {
 
 // Marrone-style empty cap: is the neighbour at `ray` (from the particle)
 // inside the cap of radius h centred h along `dir` (delta_plus.py:58-65)
-template <class T>
-__device__ __forceinline__ bool occupied(T rx, T ry, T dx, T dy, T h) {
-  const T axial = rx * dx + ry * dy;
-  T tang = rx * dy - ry * dx;
-  tang = tang < T(0) ? -tang : tang;
-  const T ox = rx - h * dx, oy = ry - h * dy;
-  if (rx * rx + ry * ry >= T(2) * h * h) return ox * ox + oy * oy < h * h;
-  T ad = axial - h;
-  ad = ad < T(0) ? -ad : ad;
-  return ad + tang < h;
+template <class T, int D>
+__device__ __forceinline__ bool occupied(const T ray[D], const T dir[D], T h) {
+  const T axial = dot<T, D>(ray, dir);
+  const T tang = cross_norm<T, D>(ray, dir);
+  T off[D];
+#pragma unroll
+  for (int k = 0; k < D; ++k) off[k] = ray[k] - h * dir[k];
+  if (dot<T, D>(ray, ray) >= T(2) * h * h) return dot<T, D>(off, off) < h * h;
+  return absv(axial - h) + tang < h;
 }
 
-template <class T>
+template <class T, int D>
 __global__ void p4_density(DPP<T> p, DPW<T> w) {
   for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < p.n; a += gridDim.x * blockDim.x) {
-    const T xa = w.pos[2 * a], ya = w.pos[2 * a + 1];
+    T xa[D], ga[D], na[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      xa[k] = w.pos[D * a + k];
+      ga[k] = w.grho[D * a + k];
+      na[k] = w.nrm[D * a + k];
+    }
     const T ra = w.rho[a];
-    const T gax = w.grho[2 * a], gay = w.grho[2 * a + 1];
-    const T nx = w.nrm[2 * a], ny = w.nrm[2 * a + 1];
     CSum<T> diff;
     int covered = 0;
     for (int64_t e = w.rowptr[a]; e < w.rowptr[a + 1]; ++e) {
       const int64_t b = w.ent[e] & kIdx;
       if (b >= p.n) continue;
-      const T dx = xa - w.pos[2 * b], dy = ya - w.pos[2 * b + 1];
-      const T r2 = dx * dx + dy * dy;
+      T d[D], ray[D];
+#pragma unroll
+      for (int k = 0; k < D; ++k) {
+        d[k] = xa[k] - w.pos[D * b + k];
+        ray[k] = -d[k];
+      }
+      const T r2 = dot<T, D>(d, d);
       if (!(r2 < p.support2)) continue;
-      covered += occupied(-dx, -dy, nx, ny, p.h);
+      covered += occupied<T, D>(ray, na, p.h);
       if (p.dscale != T(0)) {
         T W, gs;
         p.k.wg(sqrt(r2), W, gs);
-        const T radial = -(dx * (dx * gs) + dy * (dy * gs));
-        const T proj = T(0.5) * ((gax + w.grho[2 * b]) * dx + (gay + w.grho[2 * b + 1]) * dy);
+        T gdd[D], sg[D];
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+          gdd[k] = d[k] * gs;
+          sg[k] = ga[k] + w.grho[D * b + k];
+        }
+        const T radial = -dot<T, D>(d, gdd);
+        const T proj = T(0.5) * dot<T, D>(sg, d);
         const T contrast = (ra - w.rho[b]) - proj;
         const T coupling = contrast * radial / (r2 + T(1e-12));
         diff.add(-p.dscale * w.vol[b] * coupling);
@@ -311,22 +450,25 @@ __global__ void p4_density(DPP<T> p, DPW<T> w) {
   }
 }
 
-template <class T>
+template <class T, int D>
 __global__ void p5_shift(DPP<T> p, DPW<T> w) {
   for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < p.n; a += gridDim.x * blockDim.x) {
-    const T xa = w.pos[2 * a], ya = w.pos[2 * a + 1];
+    T xa[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) xa[k] = w.pos[D * a + k];
     const T ra = w.rho[a];
     bool band = w.surf[a] != 0;
-    CSum<T> sx, sy;
+    CSum<T> sc[D];
     T nearest = T(0);
     bool has_wall = false;
     int64_t first_wall = -1;
     for (int64_t e = w.rowptr[a]; e < w.rowptr[a + 1]; ++e) {
       const int64_t b = w.ent[e] & kIdx;
-      T xb, yb;
-      xy(p, w, b, xb, yb);
-      const T dx = xa - xb, dy = ya - yb;
-      const T r2 = dx * dx + dy * dy;
+      T xb[D], d[D];
+      point<T, D>(p, w, b, xb);
+#pragma unroll
+      for (int k = 0; k < D; ++k) d[k] = xa[k] - xb[k];
+      const T r2 = dot<T, D>(d, d);
       if (!(r2 < p.support2)) continue;
       T W, gs;
       p.k.wg(sqrt(r2), W, gs);
@@ -336,14 +478,14 @@ __global__ void p5_shift(DPP<T> p, DPW<T> w) {
       if (b < p.n) {
         band = band || (w.surf[b] != 0);
         const T c = w.mass[b] * rep / (ra + w.rho[b]);
-        sx.add(c * dx);
-        sy.add(c * dy);
+#pragma unroll
+        for (int k = 0; k < D; ++k) sc[k].add(c * d[k]);
       } else {
         const int64_t s = b - p.n;
         const T wr = w.wrho[s];
-        const T c = (wr * p.dx2 / (ra + wr)) * rep;
-        sx.add(c * dx);
-        sy.add(c * dy);
+        const T c = (wr * p.dxd / (ra + wr)) * rep;
+#pragma unroll
+        for (int k = 0; k < D; ++k) sc[k].add(c * d[k]);
         if (!has_wall || r2 < nearest) {
           nearest = r2;
           first_wall = s;
@@ -351,43 +493,76 @@ __global__ void p5_shift(DPP<T> p, DPW<T> w) {
         has_wall = true;
       }
     }
-    T rx = sx.value() * p.shift_scale, ry = sy.value() * p.shift_scale;
-    const T nx = w.nrm[2 * a], ny = w.nrm[2 * a + 1];
-    T shx = rx, shy = ry;
+    T raw[D], na[D], sh[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      raw[k] = sc[k].value() * p.shift_scale;
+      na[k] = w.nrm[D * a + k];
+      sh[k] = raw[k];
+    }
     if (band) {
       const bool resolved = w.lam[a] >= T(0.55) && w.str[a] > T(1e-6);
-      const T dot = rx * nx + ry * ny;
-      shx = resolved ? rx - dot * nx : T(0);
-      shy = resolved ? ry - dot * ny : T(0);
+      const T dn = dot<T, D>(raw, na);
+#pragma unroll
+      for (int k = 0; k < D; ++k) sh[k] = resolved ? raw[k] - dn * na[k] : T(0);
     }
     if (has_wall) {
       // nearest station (first in row order among exact ties) sets the tangent
-      const T dnx = w.wn[2 * first_wall], dny = w.wn[2 * first_wall + 1];
-      const T dot = shx * dnx + shy * dny;
-      const T tx = shx - dot * dnx, ty = shy - dot * dny;
-      const T tol = T(1e-6) * sqrt(shx * shx + shy * shy);
-      T tn = tx * nx + ty * ny;
-      tn = tn < T(0) ? -tn : tn;
-      bool conflict = band && tn > tol;
-      for (int64_t e = w.rowptr[a]; e < w.rowptr[a + 1] && !conflict; ++e) {
+      T dn[D], tv[D];
+#pragma unroll
+      for (int k = 0; k < D; ++k) dn[k] = w.wn[D * first_wall + k];
+      const T dd = dot<T, D>(sh, dn);
+#pragma unroll
+      for (int k = 0; k < D; ++k) tv[k] = sh[k] - dd * dn[k];
+      const T tol = T(1e-6) * sqrt(dot<T, D>(sh, sh));
+      const bool conflict = band && absv(dot<T, D>(tv, na)) > tol;
+      bool pinned = false;
+      for (int64_t e = w.rowptr[a]; e < w.rowptr[a + 1] && !pinned; ++e) {
         const int64_t b = w.ent[e] & kIdx;
         if (b < p.n) continue;
         const int64_t s = b - p.n;
-        const T dx = xa - w.wall[2 * s], dy = ya - w.wall[2 * s + 1];
-        if (dx * dx + dy * dy != nearest) continue;
-        T o = tx * w.wn[2 * s] + ty * w.wn[2 * s + 1];
-        o = o < T(0) ? -o : o;
-        conflict = o > tol;
+        T d[D], ns[D];
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+          d[k] = xa[k] - w.wall[D * s + k];
+          ns[k] = w.wn[D * s + k];
+        }
+        if (dot<T, D>(d, d) != nearest) continue;
+        pinned = absv(dot<T, D>(tv, ns)) > tol;
       }
-      shx = conflict ? T(0) : tx;
-      shy = conflict ? T(0) : ty;
+      if (pinned) {
+#pragma unroll
+        for (int k = 0; k < D; ++k) sh[k] = T(0);
+      } else if (conflict) {
+        if (D == 2) {
+#pragma unroll
+          for (int k = 0; k < D; ++k) sh[k] = T(0);
+        } else {
+          // keep the part along the line both tangent planes share
+          T ln[3] = {dn[1] * na[D - 1] - dn[D - 1] * na[1], dn[D - 1] * na[0] - dn[0] * na[D - 1],
+                     dn[0] * na[1] - dn[1] * na[0]};
+          const T lnn = sqrt(ln[0] * ln[0] + ln[1] * ln[1] + ln[2] * ln[2]);
+          const T inv = lnn > T(1e-12) ? T(1) / lnn : T(0);
+#pragma unroll
+          for (int k = 0; k < 3; ++k) ln[k] = ln[k] * inv;
+          const T along = tv[0] * ln[0] + tv[1] * ln[1] + tv[D - 1] * ln[2];
+#pragma unroll
+          for (int k = 0; k < D; ++k) sh[k] = along * ln[k];
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < D; ++k) sh[k] = tv[k];
+      }
     }
-    w.shift[2 * a] = shx;
-    w.shift[2 * a + 1] = shy;
-    w.out_pos[2 * a] = xa + p.dt * w.out_vel[2 * a] + shx;
-    w.out_pos[2 * a + 1] = ya + p.dt * w.out_vel[2 * a + 1] + shy;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      w.shift[D * a + k] = sh[k];
+      w.out_pos[D * a + k] = xa[k] + p.dt * w.out_vel[D * a + k] + sh[k];
+    }
   }
 }
+
+int dp_dim(const tsph_delta_plus_params& p) { return p.dim == 3 ? 3 : 2; }
 
 struct Layout {
   size_t total;
@@ -396,9 +571,10 @@ struct Layout {
 
 Layout dp_layout(const tsph_delta_plus_params& p) {
   const size_t ts = p.dtype == TSPH_F64 ? 8 : 4;
+  const size_t D = static_cast<size_t>(dp_dim(p));
   const size_t n = static_cast<size_t>(p.n_fluid), nw = static_cast<size_t>(p.n_wall);
-  const size_t sizes[14] = {n * ts, n * ts, n * ts, 3 * n * ts, 2 * n * ts, 2 * n * ts, n * ts, n * ts,
-                            n * sizeof(int), nw * ts, nw * ts, 2 * nw * ts, sizeof(int), 0};
+  const size_t sizes[14] = {n * ts, n * ts, n * ts, D * (D + 1) / 2 * n * ts, D * n * ts, D * n * ts, n * ts,
+                            n * ts, n * sizeof(int), nw * ts, nw * ts, D * nw * ts, sizeof(int), 0};
   Layout L{};
   size_t used = 0;
   for (int k = 0; k < 14; ++k) {
@@ -409,7 +585,7 @@ Layout dp_layout(const tsph_delta_plus_params& p) {
   return L;
 }
 
-template <class T>
+template <class T, int D>
 int run_dp(const tsph_delta_plus_params& prm, const tsph_delta_plus_io& io, char* ws, cudaStream_t s) {
   DPP<T> p{};
   p.n = prm.n_fluid;
@@ -421,17 +597,18 @@ int run_dp(const tsph_delta_plus_params& prm, const tsph_delta_plus_io& io, char
   p.c2 = static_cast<T>(prm.sound_speed * prm.sound_speed);
   p.rho0 = static_cast<T>(prm.rho0);
   p.g = static_cast<T>(prm.gravity);
-  const double nu_r = 8.0 * prm.viscosity + prm.alpha * h * prm.sound_speed;
+  // Monaghan's radial viscous stress, 2 (D + 2) nu (delta_plus.py:184-186)
+  const double nu_r = 2.0 * (D + 2) * prm.viscosity + prm.alpha * h * prm.sound_speed;
   p.rho0_nu = static_cast<T>(prm.rho0 * nu_r);
   p.dt = static_cast<T>(prm.dt);
   p.dscale = static_cast<T>(2.0 * prm.diffusion * h * prm.sound_speed);
   p.shift_scale = static_cast<T>(-(prm.dt * prm.sound_speed / h) * (prm.reference_speed / prm.sound_speed) *
                                  (2.0 * h) * (2.0 * h));
   p.support2 = static_cast<T>((2.0 * h) * (2.0 * h));
-  p.dx2 = static_cast<T>(prm.dx * prm.dx);
-  p.tiny = prm.dtype == TSPH_F64 ? static_cast<T>(2.2250738585072014e-308) : static_cast<T>(1.1754943508222875e-38);
+  p.dxd = static_cast<T>(D == 2 ? prm.dx * prm.dx : prm.dx * prm.dx * prm.dx);
+  p.tiny = std::numeric_limits<T>::min();  // torch.finfo(dtype).tiny
   p.k.h = static_cast<T>(h);
-  p.k.sigma = static_cast<T>(7.0 / (4.0 * M_PI * h * h));
+  p.k.sigma = static_cast<T>(D == 2 ? 7.0 / (4.0 * M_PI * h * h) : 21.0 / (16.0 * M_PI * h * h * h));
   p.k.eps = static_cast<T>(1e-12);
   {
     // W(dx) in the dtype, as wendland_c2_kernel(tensor(dx), h)
@@ -473,11 +650,11 @@ int run_dp(const tsph_delta_plus_params& prm, const tsph_delta_plus_io& io, char
   TSPH_CUDA_CHECK(cudaMemsetAsync(w.status, 0, sizeof(int), s));
   const unsigned g = grid_for(p.n, 128);
   p0_state<T><<<grid_for(p.n, 256), 256, 0, s>>>(p, w);
-  if (p.nw) p1_walls<T><<<grid_for(p.nw, 128), 128, 0, s>>>(p, w);
-  p2_force<T><<<g, 128, 0, s>>>(p, w);
-  p3_geometry<T><<<g, 128, 0, s>>>(p, w);
-  p4_density<T><<<g, 128, 0, s>>>(p, w);
-  p5_shift<T><<<g, 128, 0, s>>>(p, w);
+  if (p.nw) p1_walls<T, D><<<grid_for(p.nw, 128), 128, 0, s>>>(p, w);
+  p2_force<T, D><<<g, 128, 0, s>>>(p, w);
+  p3_geometry<T, D><<<g, 128, 0, s>>>(p, w);
+  p4_density<T, D><<<g, 128, 0, s>>>(p, w);
+  p5_shift<T, D><<<g, 128, 0, s>>>(p, w);
   TSPH_LAUNCH_CHECK();
   int st = 0;
   TSPH_CUDA_CHECK(cudaMemcpyAsync(&st, w.status, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -502,6 +679,7 @@ int tsph_delta_plus_step(const tsph_delta_plus_params* prm, const tsph_delta_plu
                          int64_t ws_bytes, tsph_stream stream) {
   if (!prm || !io || prm->n_fluid < 1 || prm->n_wall < 0 || prm->n_fluid + prm->n_wall >= (int64_t(1) << 31))
     return TSPH_ERR_ARG;
+  if (prm->dim != 0 && prm->dim != 2 && prm->dim != 3) return TSPH_ERR_ARG;
   if (!io->pos || !io->vel || !io->density || !io->mass || !io->rowptr || !io->out_pos || !io->out_vel ||
       !io->out_density || !io->acc || !io->shift)
     return TSPH_ERR_ARG;
@@ -510,8 +688,9 @@ int tsph_delta_plus_step(const tsph_delta_plus_params* prm, const tsph_delta_plu
   if (ws_bytes < tsph_delta_plus_workspace_bytes(prm)) return TSPH_ERR_WORKSPACE;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   char* w = static_cast<char*>(ws);
-  if (prm->dtype == TSPH_F32) return run_dp<float>(*prm, *io, w, s);
-  if (prm->dtype == TSPH_F64) return run_dp<double>(*prm, *io, w, s);
+  const bool three = dp_dim(*prm) == 3;
+  if (prm->dtype == TSPH_F32) return three ? run_dp<float, 3>(*prm, *io, w, s) : run_dp<float, 2>(*prm, *io, w, s);
+  if (prm->dtype == TSPH_F64) return three ? run_dp<double, 3>(*prm, *io, w, s) : run_dp<double, 2>(*prm, *io, w, s);
   return TSPH_ERR_ARG;
 }
 

@@ -20,7 +20,7 @@ from . import _lib
 from .droplet_impact import symmetric_rows
 from .neighbor_search import grid_pairs
 
-__all__ = ["DeltaPlusStep", "delta_plus_step"]
+__all__ = ["DeltaPlusStep", "delta_plus_step", "delta_plus_step3"]
 
 
 @dataclass
@@ -37,26 +37,56 @@ def delta_plus_step(pos, velocity, density, mass, *, dx, sound_speed, reference_
                     dt, rho0=1000., gravity=9.81, viscosity=1.e-6, diffusion=.1, alpha=.02,
                     wall=None, wall_velocity=None, wall_normal=None, pairs=None):
     """Advance an equal-spacing 2-D liquid by one delta-plus step (h = 2 dx)."""
-    if (pos.ndim != 2 or pos.shape[1] != 2 or velocity.shape != pos.shape
+    return _delta_plus(2, pos, velocity, density, mass, dx=dx, sound_speed=sound_speed,
+                       reference_speed=reference_speed, dt=dt, rho0=rho0, gravity=gravity,
+                       viscosity=viscosity, diffusion=diffusion, alpha=alpha, wall=wall,
+                       wall_velocity=wall_velocity, wall_normal=wall_normal, pairs=pairs)
+
+
+def delta_plus_step3(pos, velocity, density, mass, *, dx, sound_speed, reference_speed,
+                     dt, rho0=1000., gravity=9.81, viscosity=1.e-6, diffusion=.1, alpha=.02,
+                     wall=None, wall_velocity=None, wall_normal=None, pairs=None):
+    """The delta-plus step of ``delta_plus_step`` for a 3-D liquid (y up).
+
+    The reference's step is 2-D only (delta_plus.py:119); this is the same
+    sequence of statements in 3-D: the 3-D Wendland C2 constant
+    21 / (16 pi h^3) (threed/kernel3.py:139-164), the radial viscous stress
+    coefficient 2 (D + 2) nu = 10 nu (and its time-step limit dt nu_r / 10 <=
+    h^2 / 8), wall stations of volume dx^3, the 3 x 3 first moment, the
+    empty-cap test's tangential distance |ray x n|, and a wall-tangent shift
+    that conflicts with the interface normal reduced to its part along
+    n_wall x n_surface instead of to zero.  Arguments, checks, exceptions and
+    the ``DeltaPlusStep`` result are the 2-D step's with (N, 3) arrays."""
+    return _delta_plus(3, pos, velocity, density, mass, dx=dx, sound_speed=sound_speed,
+                       reference_speed=reference_speed, dt=dt, rho0=rho0, gravity=gravity,
+                       viscosity=viscosity, diffusion=diffusion, alpha=alpha, wall=wall,
+                       wall_velocity=wall_velocity, wall_normal=wall_normal, pairs=pairs)
+
+
+def _delta_plus(dim, pos, velocity, density, mass, *, dx, sound_speed, reference_speed,
+                dt, rho0, gravity, viscosity, diffusion, alpha, wall, wall_velocity, wall_normal,
+                pairs):
+    if (pos.ndim != 2 or pos.shape[1] != dim or velocity.shape != pos.shape
             or density.shape != pos.shape[:1] or mass.shape != density.shape
             or not len(pos) or pos.dtype not in (torch.float32, torch.float64)):
-        raise ValueError("expected a nonempty 2-D fluid and one density and mass per particle")
+        raise ValueError(f"expected a nonempty {dim}-D fluid and one density and mass per particle")
     if not all(math.isfinite(x) for x in (dx, sound_speed, reference_speed, dt,
                                           rho0, gravity, viscosity, diffusion, alpha)):
         raise ValueError("solver parameters must be finite")
     if min(dx, sound_speed, dt, rho0) <= 0 or min(reference_speed, viscosity, diffusion, alpha) < 0:
         raise ValueError("invalid length, speed, density, step or transport coefficient")
     h = 2 * dx
-    radial_viscosity = 8 * viscosity + alpha * h * sound_speed
-    if (dt * sound_speed > .3 * h or dt * radial_viscosity / 8 > .125 * h * h
+    coef = 2 * (dim + 2)   # Monaghan's radial viscous stress, 8 in 2-D
+    radial_viscosity = coef * viscosity + alpha * h * sound_speed
+    if (dt * sound_speed > .3 * h or dt * radial_viscosity / coef > .125 * h * h
             or dt * diffusion * sound_speed > .125 * h):
         raise ValueError("time step exceeds an acoustic, viscous or diffusive limit")
     if wall is None:
-        wall = pos.new_empty((0, 2))
+        wall = pos.new_empty((0, dim))
     if wall_velocity is None:
         wall_velocity = torch.zeros_like(wall)
-    if wall.ndim != 2 or wall.shape[1] != 2 or wall_velocity.shape != wall.shape:
-        raise ValueError("expected matching (W, 2) wall positions and velocities")
+    if wall.ndim != 2 or wall.shape[1] != dim or wall_velocity.shape != wall.shape:
+        raise ValueError(f"expected matching (W, {dim}) wall positions and velocities")
     if wall_normal is None and len(wall) == 0:
         wall_normal = wall
     if wall_normal is None or wall_normal.shape != wall.shape:
@@ -97,6 +127,7 @@ def delta_plus_step(pos, velocity, density, mass, *, dx, sound_speed, reference_
         float(reference_speed), float(dt)
     prm.rho0, prm.gravity, prm.viscosity = float(rho0), float(gravity), float(viscosity)
     prm.diffusion, prm.alpha = float(diffusion), float(alpha)
+    prm.dim = dim
     out_pos = torch.empty_like(P)
     out_vel = torch.empty_like(P)
     out_rho = torch.empty_like(R)
