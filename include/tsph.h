@@ -587,6 +587,20 @@ typedef struct {
    * shift_vref_floor)                                                       */
   int64_t shift_vref_given;
   double shift_vref;
+  /* density diffusion form: 0 Molteni (density_diffusion.py:78-92), 1 the
+   * psi form with the renormalised density gradient (density_diffusion.py:
+   * 95-172, eigenvalue floor diffusion_eigen_floor * trace / D), both over
+   * fluid neighbours with scale diffusion_scale                            */
+  int64_t diffusion_form;
+  double diffusion_eigen_floor;
+  /* 2-D rhs options (droplet_impact.py:954-964, 1090-1112):
+   * density_renormalization: the summation density times
+   * lattice_kernel_sum / sum_b W_ab (Shepard); boundary_consistent_density:
+   * the fluid density corrected by the extrapolated wall densities, the EOS
+   * and the wall extrapolation taken again                                 */
+  int64_t density_renormalization;
+  double lattice_kernel_sum;
+  int64_t boundary_consistent_density;
 } tsph_case_params;
 
 typedef struct tsph_engine tsph_engine; /* opaque host handle */

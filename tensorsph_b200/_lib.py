@@ -169,7 +169,10 @@ class CaseParams(ctypes.Structure):
                 ("csf_wall_area", c_double), ("csf_traction_calibration", c_double),
                 ("adaptive_dt", c_int64), ("courant_h", c_double), ("dt_limit", c_double),
                 ("dt_growth", c_double), ("dt_safety", c_double), ("target_time", c_double),
-                ("shift_vref_given", c_int64), ("shift_vref", c_double)]
+                ("shift_vref_given", c_int64), ("shift_vref", c_double),
+                ("diffusion_form", c_int64), ("diffusion_eigen_floor", c_double),
+                ("density_renormalization", c_int64), ("lattice_kernel_sum", c_double),
+                ("boundary_consistent_density", c_int64)]
 
 
 _SIGNATURES = {

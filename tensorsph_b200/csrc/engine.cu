@@ -40,6 +40,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "symeig.cuh"
 
 namespace tsph {
 namespace {
@@ -94,6 +95,12 @@ struct CaseDev {
   double dt_growth, dt_safety;
   double target_time, time_tol;
   double shift_strength_h; // shifting's strength h (times dt and v_ref)
+  int dim;                 // 2 or 3 (a 2-D case has z = 0 and one cell layer)
+  int psi;                 // psi-form diffusion with the renormalised density gradient
+  double eig_floor;        // its eigenvalue floor fraction of trace / dim
+  int renorm;              // Shepard renormalisation of the summation density
+  float lattice_sum;       // its full-support kernel sum
+  int bcd;                 // boundary-consistent density (a second wall pass)
 };
 
 struct CaseCtl {
@@ -148,6 +155,8 @@ struct Dev {
   float* rho;
   float* pq;
   float2* rs;
+  float4* gg;    // psi diffusion: the renormalised density gradient <grad rho>
+  float* dlt;    // the fluid density deviation rho - rho0 after diffusion
   float4* acc;
   float* conc;
   float4* gradc;
@@ -163,6 +172,8 @@ struct Dev {
   float2* st;        // CSF: surface-tension acceleration
   unsigned int* csf_hist;  // [n_slots][256] median-select histograms
   int has_csf, maxfit;
+  int has_psi;            // some case uses the psi diffusion form (one more gather)
+  int has_bcd;            // some case uses the boundary-consistent density
   int has_tvc, tvc_late;  // tvc_late: the correction runs after the second list pass
   int csf_kinds;          // CSF options present in the batch: fits 1 quadratic, 2 circle,
                           // 16 quadratic + local_range, 32 circle + local_range; 4 local_range,
@@ -682,11 +693,12 @@ __global__ void __launch_bounds__(kMaxBlock) k_density(const __grid_constant__ D
     const float4 la = e.lp[a];
     const float2 ncell = f2(-cellf), inv_h2 = f2(inv_h), sigma2 = f2(sigma);
     // the deviation rho - rho0, summed with compensation from -rho0
-    CSum<float> s;
+    CSum<float> s, kt;
     s.add(-C.rho0);
     s.add(la.w * sigma);
+    const bool renorm = C.renorm != 0;
     walk_row<KB>(e, a, [&](const uint32_t* ent) {
-      float2 part = f2(0.f);
+      float2 part = f2(0.f), wsum = f2(0.f);
 #pragma unroll
       for (int j = 0; j < KB; j += 2) {
         const uint32_t e0 = ent[j], e1 = ent[j + 1];
@@ -697,13 +709,89 @@ __global__ void __launch_bounds__(kMaxBlock) k_density(const __grid_constant__ D
         const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
         const float2 W = __fmul2_rn(sigma2, shape2(radial2(r2, inv_h2).q));
         part = __ffma2_rn(make_float2(l0.w, l1.w), W, part);
+        if (renorm) wsum = __fadd2_rn(wsum, W);
       }
       s.add(part.x + part.y);
+      if (renorm) kt.add(wsum.x + wsum.y);
     });
     const float dfloor = floor_ - C.rho0;
     float d = s.value();
     d = d > dfloor ? d : dfloor;
+    if (renorm) {
+      // rho S / T - rho0 = d S / T + rho0 (S - T) / T, T = W(0) + sum_b W_ab
+      // (droplet_impact.py:954-964)
+      kt.add(sigma);
+      float total = kt.value();
+      total = total > 1e-12f ? total : 1e-12f;
+      CSum<float> diff;
+      diff.add(C.lattice_sum);
+      diff.add(-kt.s);
+      diff.add(-kt.c);
+      d = d * (C.lattice_sum / total) + C.rho0 * (diff.value() / total);
+      d = d > dfloor ? d : dfloor;
+    }
     e.rs[a] = make_float2(d, la.w / (C.rho0 + d));
+  }
+}
+
+// E1b (cases with the psi diffusion form): the renormalised density gradient
+// <grad rho>_a = M_a^-1 sum_b V_b (rho_b - rho_a) grad_a W_ab with the first
+// moment M_a = sum_b V_b (-d_ab) (x) grad_a W_ab over the fluid neighbours,
+// the inverse floored at eig_floor x trace / D (density_diffusion.py:95-142).
+template <bool kOne, int KB>
+__global__ void __launch_bounds__(kMaxBlock) k_density_gradient(const __grid_constant__ Dev e) {
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    const CaseDev& C = case_of<kOne>(e, a);
+    if (!C.psi) continue;
+    const float4 la = e.lp[a];
+    const float2 ra = e.rs[a];
+    const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf;
+    const int NF = e.NF;
+    const float2 ncell = f2(-cellf), inv_h2 = f2(inv_h), gscale = f2(sigma * inv_h);
+    CSum<float> gx, gy, gz, mxx, mxy, mxz, myy, myz, mzz;
+    walk_row<KB>(e, a, [&](const uint32_t* ent) {
+#pragma unroll
+      for (int j = 0; j < KB; j += 2) {
+        const uint32_t e0 = ent[j], e1 = ent[j + 1];
+        const int c0 = static_cast<int>(e0 >> kCodeBits), c1 = static_cast<int>(e1 >> kCodeBits);
+        const int b0 = c0 < NF ? c0 : e.null_row, b1 = c1 < NF ? c1 : e.null_row;
+        const float4 l0 = e.lp[b0], l1 = e.lp[b1];
+        const float2 r0 = e.rs[b0], r1 = e.rs[b1];
+        const float2 dx = sep2<0>(la.x, l0.x, l1.x, e0, e1, ncell);
+        const float2 dy = sep2<2>(la.y, l0.y, l1.y, e0, e1, ncell);
+        const float2 dz = sep2<4>(la.z, l0.z, l1.z, e0, e1, ncell);
+        const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+        const Radial2 R = radial2(r2, inv_h2);
+        const float2 gs = __fmul2_rn(__fmul2_rn(gscale, dshape2(R.q)), R.inv_r);
+        const float2 vb = make_float2(r0.y, r1.y);
+        // V_b (rho_b - rho_a) grad_a W and V_b (-grad_a W) (x) d, grad_a W = gs d
+        const float2 cg = __fmul2_rn(__fmul2_rn(vb, sub2(make_float2(r0.x, r1.x), f2(ra.x))), gs);
+        const float2 cm = __fmul2_rn(vb, make_float2(-gs.x, -gs.y));
+        const float2 mx = __fmul2_rn(cm, dx), my = __fmul2_rn(cm, dy), mz = __fmul2_rn(cm, dz);
+        const float2 ex = __fmul2_rn(cg, dx), ey = __fmul2_rn(cg, dy), ez = __fmul2_rn(cg, dz);
+        gx.add(ex.x + ex.y);
+        gy.add(ey.x + ey.y);
+        gz.add(ez.x + ez.y);
+        const float2 xx = __fmul2_rn(mx, dx), xy = __fmul2_rn(mx, dy), xz = __fmul2_rn(mx, dz);
+        const float2 yy = __fmul2_rn(my, dy), yz = __fmul2_rn(my, dz), zz = __fmul2_rn(mz, dz);
+        mxx.add(xx.x + xx.y);
+        mxy.add(xy.x + xy.y);
+        mxz.add(xz.x + xz.y);
+        myy.add(yy.x + yy.y);
+        myz.add(yz.x + yz.y);
+        mzz.add(zz.x + zz.y);
+      }
+    });
+    const double m[3][3] = {{mxx.value(), mxy.value(), mxz.value()},
+                            {mxy.value(), myy.value(), myz.value()},
+                            {mxz.value(), myz.value(), mzz.value()}};
+    const double g[3] = {gx.value(), gy.value(), gz.value()};
+    double out[3] = {0.0, 0.0, 0.0};
+    if (C.dim == 2)
+      floored_solve<2>(m, g, C.eig_floor, out);
+    else
+      floored_solve<3>(m, g, C.eig_floor, out);
+    e.gg[a] = make_float4(static_cast<float>(out[0]), static_cast<float>(out[1]), static_cast<float>(out[2]), 0.f);
   }
 }
 
@@ -715,7 +803,47 @@ __global__ void __launch_bounds__(kMaxBlock) k_diffusion_eos(const __grid_consta
     const float4 la = e.lp[a];
     float d = ra.x;
     const float dscale = C.dscale;
-    if (dscale > 0.f) {
+    if (dscale > 0.f && C.psi) {
+      // psi form (density_diffusion.py:145-172): the contrast
+      // (rho_a - rho_b) - (<grad rho>_a + <grad rho>_b) . d / 2
+      const float4 ga = e.gg[a];
+      const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf;
+      const int NF = e.NF;
+      const float2 ncell = f2(-cellf), inv_h2 = f2(inv_h), gscale = f2(-sigma * inv_h);
+      CSum<float> rate;
+      walk_row<KB>(e, a, [&](const uint32_t* ent) {
+        float2 part = f2(0.f);
+#pragma unroll
+        for (int j = 0; j < KB; j += 2) {
+          const uint32_t e0 = ent[j], e1 = ent[j + 1];
+          const int c0 = static_cast<int>(e0 >> kCodeBits), c1 = static_cast<int>(e1 >> kCodeBits);
+          const int b0 = c0 < NF ? c0 : e.null_row, b1 = c1 < NF ? c1 : e.null_row;
+          const float4 l0 = e.lp[b0], l1 = e.lp[b1];
+          const float2 r0 = e.rs[b0], r1 = e.rs[b1];
+          const float4 g0 = e.gg[b0], g1 = e.gg[b1];
+          const float2 dx = sep2<0>(la.x, l0.x, l1.x, e0, e1, ncell);
+          const float2 dy = sep2<2>(la.y, l0.y, l1.y, e0, e1, ncell);
+          const float2 dz = sep2<4>(la.z, l0.z, l1.z, e0, e1, ncell);
+          const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+          const Radial2 R = radial2(r2, inv_h2);
+          const float2 ngr = __fmul2_rn(__fmul2_rn(__fmul2_rn(gscale, dshape2(R.q)), R.inv_r), r2);
+          const float2 sx = __fadd2_rn(f2(ga.x), make_float2(g0.x, g1.x));
+          const float2 sy = __fadd2_rn(f2(ga.y), make_float2(g0.y, g1.y));
+          const float2 sz = __fadd2_rn(f2(ga.z), make_float2(g0.z, g1.z));
+          const float2 proj = __fmul2_rn(f2(0.5f), __ffma2_rn(sz, dz, __ffma2_rn(sy, dy, __fmul2_rn(sx, dx))));
+          const float2 contrast = sub2(sub2(f2(ra.x), make_float2(r0.x, r1.x)), proj);
+          const float2 coupling = __fmul2_rn(__fmul2_rn(contrast, ngr),
+                                             make_float2(rcp_pair(r2.x + 1e-12f), rcp_pair(r2.y + 1e-12f)));
+          const float2 w = make_float2(-dscale * r0.y, -dscale * r1.y);
+          part = __ffma2_rn(w, coupling, part);
+        }
+        rate.add(part.x + part.y);
+      });
+      const float dfloor = C.rho_floor - C.rho0;
+      const float dtf = C.adaptive ? static_cast<float>(e.ctl[kOne ? e.one_slot : e.cid[a]].dt_step) : C.dtf;
+      d = ra.x + dtf * rate.value();
+      d = d > dfloor ? d : dfloor;
+    } else if (dscale > 0.f) {
       const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf;
       const int NF = e.NF;
       const float2 ncell = f2(-cellf), inv_h2 = f2(inv_h), gscale = f2(-sigma * inv_h);
@@ -749,10 +877,59 @@ __global__ void __launch_bounds__(kMaxBlock) k_diffusion_eos(const __grid_consta
       d = ra.x + dtf * rate.value();
       d = d > dfloor ? d : dfloor;
     }
+    e.dlt[a] = d;
     const float rho = C.rho0 + d;
     const float p = tait_dev(d, C.rho0, C.bulk, C.gamma);
     const double4 v = ld4(e.vel, a);
     e.vb[a] = make_float4(static_cast<float>(v.x), static_cast<float>(v.y), static_cast<float>(v.z), la.w / rho);
+    e.rho[a] = rho;
+    e.pr[a] = p;
+    e.pq[a] = p / (rho * rho);
+  }
+}
+
+// E3b (cases with boundary_consistent_density, droplet_impact.py:1090-1112):
+// the fluid density corrected by sum_w m_w (rho_w / rho0 - 1) W_aw over the
+// wall neighbours with the wall densities just extrapolated, then the EOS
+// again; the walls are extrapolated once more after it.
+template <bool kOne, int KB>
+__global__ void __launch_bounds__(kMaxBlock) k_bcd(const __grid_constant__ Dev e) {
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    const CaseDev& C = case_of<kOne>(e, a);
+    if (!C.bcd) continue;
+    const float4 la = e.lp[a];
+    const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, inv_rho0 = 1.f / C.rho0;
+    const int NF = e.NF;
+    const float2 ncell = f2(-cellf), inv_h2 = f2(inv_h), sigma2 = f2(sigma);
+    CSum<float> corr;
+    walk_row<KB>(e, a, [&](const uint32_t* ent) {
+      float2 part = f2(0.f);
+#pragma unroll
+      for (int j = 0; j < KB; j += 2) {
+        // fluid neighbours read the null row (zero mass)
+        const uint32_t e0 = ent[j], e1 = ent[j + 1];
+        const int c0 = static_cast<int>(e0 >> kCodeBits), c1 = static_cast<int>(e1 >> kCodeBits);
+        const int b0 = c0 >= NF ? c0 : e.null_row, b1 = c1 >= NF ? c1 : e.null_row;
+        const float4 l0 = e.lp[b0], l1 = e.lp[b1];
+        const float2 dx = sep2<0>(la.x, l0.x, l1.x, e0, e1, ncell);
+        const float2 dy = sep2<2>(la.y, l0.y, l1.y, e0, e1, ncell);
+        const float2 dz = sep2<4>(la.z, l0.z, l1.z, e0, e1, ncell);
+        const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+        const float2 W = __fmul2_rn(sigma2, shape2(radial2(r2, inv_h2).q));
+        const float2 dm = make_float2(l0.w * ((e.rho[b0] - C.rho0) * inv_rho0),
+                                      l1.w * ((e.rho[b1] - C.rho0) * inv_rho0));
+        part = __ffma2_rn(dm, W, part);
+      }
+      corr.add(part.x + part.y);
+    });
+    const float dfloor = C.rho_floor - C.rho0;
+    float d = e.dlt[a] + corr.value();
+    d = d > dfloor ? d : dfloor;
+    e.dlt[a] = d;
+    const float rho = C.rho0 + d;
+    const float p = tait_dev(d, C.rho0, C.bulk, C.gamma);
+    const float4 v = e.vb[a];
+    e.vb[a] = make_float4(v.x, v.y, v.z, la.w / rho);
     e.rho[a] = rho;
     e.pr[a] = p;
     e.pq[a] = p / (rho * rho);
@@ -2121,6 +2298,7 @@ __global__ void k_null_row(Dev e) {
   e.rho[n] = 1.f;
   e.pq[n] = 0.f;
   e.rs[n] = make_float2(0.f, 0.f);
+  e.gg[n] = make_float4(0.f, 0.f, 0.f, 0.f);
   e.conc[n] = 0.f;
 }
 
@@ -2278,6 +2456,8 @@ size_t carve(const tsph_engine_params& p, Dev* d, char* base, CaseDev** cases, c
   t.rho = static_cast<float*>(take((N + 1) * sizeof(float)));
   t.pq = static_cast<float*>(take((N + 1) * sizeof(float)));
   t.rs = static_cast<float2*>(take((N + 1) * sizeof(float2)));
+  t.gg = static_cast<float4*>(take((N + 1) * sizeof(float4)));
+  t.dlt = static_cast<float*>(take(NF * sizeof(float)));
   t.acc = static_cast<float4*>(take(NF * sizeof(float4)));
   t.conc = static_cast<float*>(take((N + 1) * sizeof(float)));
   t.gradc = static_cast<float4*>(take(NF * sizeof(float4)));
@@ -2355,10 +2535,14 @@ void batch_changed(tsph_engine* E) {
   d.shift_slot = second_pass(E) ? E->order[0].slot : 0;
   d.has_csf = 0;
   d.has_tvc = 0;
+  d.has_psi = 0;
+  d.has_bcd = 0;
   d.csf_kinds = 0;
   d.tvc_late = second_pass(E) && E->order[0].dev.tvc_bulk ? 1 : 0;
   for (const CaseHost& c : E->order) {
     d.has_csf |= c.dev.csf;
+    d.has_psi |= c.dev.psi;
+    d.has_bcd |= c.dev.bcd;
     if (c.dev.csf)
       d.csf_kinds |= (c.dev.csf_fit ? (c.dev.csf_fit == 1 ? 1 : 2) << (c.dev.csf_range ? 4 : 0) : 0) |
                      (c.dev.csf_range ? 4 : 0) | (c.dev.csf_contact >= 2 ? 8 : 0);
@@ -2472,10 +2656,15 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr, b
   const bool deep = E->batch == 8;
 #define TSPH_PICK(K) (one ? (deep ? K<true, 8> : K<true, 4>) : (deep ? K<false, 8> : K<false, 4>))
   TSPH_PICK(k_density)<<<g, B, 0, s>>>(d);
+  if (d.has_psi) TSPH_PICK(k_density_gradient)<<<g, B, 0, s>>>(d);
   mark();
   TSPH_PICK(k_diffusion_eos)<<<g, B, 0, s>>>(d);
   mark();
   if (d.nw) TSPH_PICK(k_walls)<<<grid_for(d.nw, B), B, 0, s>>>(d);
+  if (d.has_bcd && d.nw) {
+    TSPH_PICK(k_bcd)<<<g, B, 0, s>>>(d);
+    TSPH_PICK(k_walls)<<<grid_for(d.nw, B), B, 0, s>>>(d);
+  }
   if (d.has_csf) {
     const unsigned gf = static_cast<unsigned>((d.nf + B - 1) / B);
     k_csf_clear<<<gc, 128, 0, s>>>(d);
@@ -2607,6 +2796,12 @@ CaseDev make_case_dev(const tsph_case_params& p, int64_t* ncells) {
   c.nu2 = static_cast<float>(2.0 * p.viscosity);
   c.nu2f = static_cast<float>(2.0 * p.viscosity * p.wall_friction);
   c.dscale = static_cast<float>(p.diffusion_scale);
+  c.dim = static_cast<int>(p.dim);
+  c.psi = p.diffusion_form == 1 && p.diffusion_scale > 0.0 ? 1 : 0;
+  c.eig_floor = p.diffusion_eigen_floor;
+  c.renorm = p.density_renormalization ? 1 : 0;
+  c.lattice_sum = static_cast<float>(p.lattice_kernel_sum);
+  c.bcd = p.boundary_consistent_density && p.n_wall > 0 ? 1 : 0;
   c.dtf = static_cast<float>(p.dt);
   c.visc_eps = static_cast<float>(0.01 * p.h * p.h);
   c.rho_floor = static_cast<float>(0.1 * p.rho0);

@@ -145,8 +145,14 @@ class CaseSpec:
 
 def _case_params(*, dim, n_fluid, n_wall, n_obstacle, cfg, h, wall_mass, box_hi, lo, hi,
                  shift_every=0, obstacle=None, first_step=0, adaptive=False):
-    if cfg.density_diffusion > 0.0 and cfg.density_diffusion_form != "molteni":
-        raise NotImplementedError("the device engine implements the 'molteni' diffusion form only")
+    psi = cfg.density_diffusion > 0.0 and cfg.density_diffusion_form == "antuono"
+    if psi and dim == 3:
+        # rhs_3d's contract (dam_break_3d.py:330-336)
+        raise ValueError("density_diffusion_rate implements the 'molteni' form only; the "
+                         f"configured form is {cfg.density_diffusion_form!r}")
+    if dim == 3 and (cfg.density_renormalization or cfg.boundary_consistent_density):
+        raise NotImplementedError("density_renormalization and boundary_consistent_density are "
+                                  "options of the 2-D rhs")
     if getattr(cfg, "density_regularization", "none") != "none" or getattr(cfg, "surface_pressure_closure", False):
         raise NotImplementedError("density_regularization and surface_pressure_closure are options of the "
                                   "rhs drop-ins, not of the device engine")
@@ -162,6 +168,15 @@ def _case_params(*, dim, n_fluid, n_wall, n_obstacle, cfg, h, wall_mass, box_hi,
     p.dt = cfg.dt
     p.wall_mass = wall_mass
     p.skin = cfg.pair_skin_factor * h
+    # the psi diffusion form (density_diffusion.py:95-172) and the 2-D rhs's
+    # density options (droplet_impact.py:954-964, 1090-1112)
+    p.diffusion_form = 1 if psi else 0
+    p.diffusion_eigen_floor = float(cfg.density_diffusion_eigenvalue_floor)
+    if cfg.density_renormalization:
+        from .droplet_impact import lattice_kernel_sum
+        p.density_renormalization = 1
+        p.lattice_kernel_sum = float(lattice_kernel_sum(h, cfg.dx))
+    p.boundary_consistent_density = 1 if cfg.boundary_consistent_density else 0
     for k in range(3):
         p.box_hi[k] = box_hi[k]
     p.tolerance = 0.25 * cfg.dx
@@ -273,9 +288,6 @@ def dam_break_2d_case(cfg, *, shift_every: int = 0, velocity=None, label: str = 
     validate_case(cfg)
     if cfg.surface_tension_coefficient > 0.0:
         raise NotImplementedError("surface tension in the dam-break case is not part of the device engine")
-    if cfg.density_renormalization or cfg.boundary_consistent_density:
-        raise NotImplementedError("density_renormalization and boundary_consistent_density are "
-                                  "not part of the device engine")
     x, mass = make_column(cfg, "cpu")
     wall = wall_lattice(cfg, "cpu", top=cfg.tank_top())
     x = x.double().contiguous()
@@ -329,9 +341,6 @@ def droplet_impact_case(cfg, *, drop_speed: float = 0.0, label: str = "") -> Cas
             if cfg.contact_angle_model == "rotate" and not 0.0 < cfg.contact_angle_reach <= 2.0:
                 raise NotImplementedError("the device engine's contact-angle boundary reaches at most 2 h "
                                           "(the wall particles of the list rows)")
-    if cfg.density_renormalization or cfg.boundary_consistent_density:
-        raise NotImplementedError("density_renormalization and boundary_consistent_density are "
-                                  "not part of the device engine")
     x, mass = make_particles(cfg, "cpu")
     wall = wall_lattice(cfg, "cpu")
     x = x.double().contiguous()

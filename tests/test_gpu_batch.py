@@ -67,9 +67,21 @@ def engine_for(specs, **kw):
     return BatchEngine(**capacity_for(specs, **kw))
 
 
-def test_2d_case_matches_fp64_oracle(gpu):
+OPTION_SETS = [dict(), dict(density_diffusion_form="antuono"), dict(density_renormalization=True),
+               dict(boundary_consistent_density=True),
+               dict(density_diffusion_form="antuono", boundary_consistent_density=True,
+                    density_diffusion_eigenvalue_floor=0.2)]
+
+
+@pytest.mark.parametrize("opts", OPTION_SETS)
+def test_2d_case_matches_fp64_oracle(opts, gpu):
+    """The 2-D dam break in the engine against the FP64 oracle's rhs + Euler
+    + clamps, for the rhs options the engine runs: Molteni diffusion, the
+    psi form with the renormalised density gradient, the Shepard density
+    renormalisation and the boundary-consistent density."""
+    from dataclasses import replace
     from tensorsph_b200.engine import dam_break_2d_case
-    cfg = small_2d()
+    cfg = replace(small_2d(), **opts)
     spec = dam_break_2d_case(cfg)
     eng = engine_for([spec], max_neighbors=64, diag_ring=32)
     cid = eng.add(spec)
