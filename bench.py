@@ -395,25 +395,39 @@ def ensemble_leg(args, dev):
 
 
 def serving_leg(args, dev):
-    """Continuous-batching server vs serial single-case runs of one seeded stream."""
+    """Continuous-batching server vs serial single-case runs of one seeded
+    stream, at the configured budget and, with ``--serve-tight-gb``, again
+    under a budget small enough that admissions wait for retirements
+    (admission by HBM footprint)."""
+    import torch
     from tensorsph_b200 import serving as sv
-    reqs = sv.request_stream(args.serve_requests, rate=20.0, seed=0,
-                             time_scale=args.serve_time_scale)
-    srv = sv.Server(budget_bytes=args.serve_budget_gb * 1e9, device=dev)
-    served = srv.serve(reqs)
-    engine_gb = srv.engine_bytes / 1e9
-    srv.close()
-    serial = sv.run_serial(sv.request_stream(args.serve_requests, rate=20.0, seed=0,
-                                             time_scale=args.serve_time_scale), device=dev)
-    return {"workload": f"{args.serve_requests} requests, Poisson 20/s (seed 0), types "
-                        f"{list(sv.CASE_TYPES)}, fluid log-uniform [1e3, 2e6], simulated time "
-                        f"U[0.1, 1.0] s x {args.serve_time_scale:g}",
-            "budget_gb": args.serve_budget_gb, "engine_gb": engine_gb,
-            "batched": {"updates_per_s": served["updates_per_s"], "wall_s": served["wall_s"],
-                        "latency_s": served["latency_s"]},
-            "serial": {"updates_per_s": serial["updates_per_s"], "wall_s": serial["wall_s"],
-                       "latency_s": serial["latency_s"]},
-            "throughput_vs_serial": served["updates_per_s"] / serial["updates_per_s"]}
+
+    def stream():
+        return sv.request_stream(args.serve_requests, rate=20.0, seed=0, time_scale=args.serve_time_scale)
+
+    out = {"workload": f"{args.serve_requests} requests, Poisson 20/s (seed 0), types "
+                       f"{list(sv.CASE_TYPES)}, fluid log-uniform [1e3, 2e6], simulated time "
+                       f"U[0.1, 1.0] s x {args.serve_time_scale:g}",
+           "time_scale": args.serve_time_scale}
+    serial = sv.run_serial(stream(), device=dev)
+    out["serial"] = {"updates_per_s": serial["updates_per_s"], "wall_s": serial["wall_s"],
+                     "latency_s": serial["latency_s"]}
+    for name, budget in (("batched", args.serve_budget_gb), ("batched_tight", args.serve_tight_gb)):
+        if budget <= 0:
+            continue
+        srv = sv.Server(budget_bytes=budget * 1e9, device=dev)
+        served = srv.serve(stream())
+        engine_gb = srv.engine_bytes / 1e9
+        srv.close()
+        torch.cuda.empty_cache()
+        out[name] = {"budget_gb": budget, "engine_gb": engine_gb,
+                     "updates_per_s": served["updates_per_s"], "wall_s": served["wall_s"],
+                     "latency_s": served["latency_s"], "admissions_blocked": served["admissions_blocked"],
+                     "graph_instantiations": served["graph_instantiations"],
+                     "graph_updates": served["graph_updates"], "engine_steps": served["engine_steps"],
+                     "throughput_vs_serial": served["updates_per_s"] / serial["updates_per_s"]}
+    out["throughput_vs_serial"] = out["batched"]["throughput_vs_serial"]
+    return out
 
 
 def shear_leg(args, dev):

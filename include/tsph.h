@@ -616,11 +616,16 @@ int tsph_engine_create(const tsph_engine_params* prm, void* arena, int64_t arena
  * FP64 and wall (n_wall, dim) FP64; *case_id receives its slot.  Returns
  * TSPH_ERR_CAPACITY when a capacity would be exceeded (nothing changes) and
  * TSPH_ERR_UNSUPPORTED for a shifting case in a non-empty batch.
- * Synchronises; the step graph is re-captured at the next step. */
+ * Stream-ordered, no host synchronisation: the arrays are read on `stream`,
+ * so they must stay valid until the stream has passed this call.  The next
+ * step captures the changed batch and updates the instantiated step graph
+ * in place (cudaGraphExecUpdate; a new instantiation when the kernels
+ * change). */
 int tsph_engine_add_case(tsph_engine* engine, const tsph_case_params* prm, const double* x,
                          const double* v, const double* mass, const double* wall,
                          tsph_stream stream, int64_t* case_id);
-/* Retire a case and compact the others (synchronises). */
+/* Retire a case and compact the others (stream-ordered, no host
+ * synchronisation; the step graph is updated at the next step). */
 int tsph_engine_remove_case(tsph_engine* engine, int64_t case_id, tsph_stream stream);
 /* Advance every case `steps` steps: the first call after a change of the
  * batch captures one step as a CUDA graph on `stream` (which must not be the
@@ -671,6 +676,9 @@ int tsph_engine_set_batch(tsph_engine* engine, int64_t depth);
  * over the wall rows (synchronises the stream).  The pair passes' work per
  * step is proportional to these counts. */
 int tsph_engine_row_entries(tsph_engine* engine, int64_t* out, tsph_stream stream);
+/* Step graphs instantiated and batch changes absorbed by an in-place graph
+ * update since the engine was created: stats[0], stats[1] (host). */
+int tsph_engine_graph_stats(const tsph_engine* engine, int64_t* stats);
 /* Occupancy (fluid rows, wall rows, obstacle rows, cells, cases) (host). */
 int tsph_engine_usage(const tsph_engine* engine, int64_t* usage);
 int tsph_engine_destroy(tsph_engine* engine);

@@ -254,6 +254,7 @@ _SIGNATURES = {
     "tsph_engine_status": (c_int, [c_void_p, c_int64, c_void_p, c_void_p]),
     "tsph_engine_usage": (c_int, [c_void_p, c_void_p]),
     "tsph_engine_row_entries": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "tsph_engine_graph_stats": (c_int, [c_void_p, c_void_p]),
     "tsph_engine_set_block": (c_int, [c_void_p, c_int64]),
     "tsph_engine_set_batch": (c_int, [c_void_p, c_int64]),
     "tsph_engine_destroy": (c_int, [c_void_p]),

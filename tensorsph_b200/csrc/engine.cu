@@ -2425,6 +2425,9 @@ struct tsph_engine {
   cudaStream_t aux = nullptr;  // captures the bodies of the step graph's conditional nodes
   bool conditional = true;     // rebuilds in conditional nodes (off if the driver refuses them)
   int64_t rebuild_kernels = 0; // kernel nodes of one conditional rebuild body
+  bool stale = false;          // the batch changed: the next step re-captures and updates exec
+  int64_t instantiations = 0;  // step graphs instantiated
+  int64_t updates = 0;         // batch changes absorbed by cudaGraphExecUpdate
 };
 
 namespace tsph {
@@ -3031,9 +3034,8 @@ int tsph_engine_add_case(tsph_engine* E, const tsph_case_params* p, const double
   batch_changed(E);
   int rc = refresh_wall_table(E, s);
   if (rc) return rc;
-  invalidate_graph(E);
-  // the caller's buffers may be released as soon as this returns
-  TSPH_CUDA_CHECK(cudaStreamSynchronize(s));
+  // the next step captures the changed batch and updates the instantiated graph
+  E->stale = true;
   *case_id = slot;
   return TSPH_OK;
 }
@@ -3114,8 +3116,7 @@ int tsph_engine_remove_case(tsph_engine* E, int64_t case_id, tsph_stream stream)
     k_clear_table<<<grid_for(E->total_cells, 256), 256, 0, s>>>(d.fstart, d.fend, E->total_cells, nullptr);
   if (d.nf) k_fill_table<<<grid_for(d.nf, 256), 256, 0, s>>>(d.home, nullptr, d.nf, d.fstart, d.fend, nullptr);
   TSPH_LAUNCH_CHECK();
-  invalidate_graph(E);
-  TSPH_CUDA_CHECK(cudaStreamSynchronize(s));
+  E->stale = true;
   return TSPH_OK;
 }
 
@@ -3123,8 +3124,36 @@ int tsph_engine_step(tsph_engine* E, int64_t steps, tsph_stream stream) {
   if (!E || steps < 0) return TSPH_ERR_ARG;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   if (E->order.empty()) return TSPH_OK;
-  if (!E->exec || E->captured_on != s) {
+  if (E->exec && E->stale && E->captured_on == s) {
+    // a batch change: capture the new step and update the instantiated graph
+    // in place (same kernels and topology, new parameters and grids); a
+    // change of topology falls through to a new instantiation
+    E->stale = false;
+    TSPH_CUDA_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_step(E, s, nullptr, E->conditional);
+    cudaGraph_t g = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(s, &g);
+    if (rc == TSPH_OK && ce == cudaSuccess) {
+      cudaGraphExecUpdateResultInfo info{};
+      if (cudaGraphExecUpdate(E->exec, g, &info) == cudaSuccess) {
+        if (E->graph) cudaGraphDestroy(E->graph);
+        E->graph = g;
+        ++E->updates;
+      } else {
+        cudaGetLastError();
+        cudaGraphDestroy(g);
+        invalidate_graph(E);
+      }
+    } else {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      invalidate_graph(E);
+      if (rc) return rc;
+    }
+  }
+  if (!E->exec || E->captured_on != s || E->stale) {
     invalidate_graph(E);
+    E->stale = false;
     // with conditional rebuild nodes first; without them if the capture or
     // the instantiation fails
     for (int attempt = 0;; ++attempt) {
@@ -3137,6 +3166,7 @@ int tsph_engine_step(tsph_engine* E, int64_t steps, tsph_stream stream) {
         ce = cudaGraphInstantiate(&E->exec, g, 0);
         if (ce == cudaSuccess) {
           E->graph = g;
+          ++E->instantiations;
           break;
         }
         E->exec = nullptr;
@@ -3267,6 +3297,13 @@ int tsph_engine_row_entries(tsph_engine* E, int64_t* out, tsph_stream stream) {
   TSPH_CUDA_CHECK(cudaStreamSynchronize(s));
   out[0] = static_cast<int64_t>(host[0]);
   out[1] = static_cast<int64_t>(host[1]);
+  return TSPH_OK;
+}
+
+int tsph_engine_graph_stats(const tsph_engine* E, int64_t* stats) {
+  if (!E || !stats) return TSPH_ERR_ARG;
+  stats[0] = E->instantiations;
+  stats[1] = E->updates;
   return TSPH_OK;
 }
 

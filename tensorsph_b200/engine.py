@@ -466,6 +466,13 @@ class BatchEngine:
         _lib.check(_lib.lib().tsph_engine_usage(self._handle, u), "tsph_engine_usage")
         return dict(fluid=u[0], wall=u[1], obstacle=u[2], cells=u[3], cases=u[4])
 
+    def graph_stats(self) -> dict:
+        """Step graphs instantiated and batch changes absorbed by in-place
+        graph updates since the engine was created."""
+        out = (ctypes.c_int64 * 2)()
+        _lib.check(_lib.lib().tsph_engine_graph_stats(self._handle, out), "tsph_engine_graph_stats")
+        return {"instantiations": int(out[0]), "updates": int(out[1])}
+
     def row_entries(self) -> tuple[int, int]:
         """Entries of the current neighbour rows ``(fluid rows, wall rows)``
         (synchronises the engine stream)."""

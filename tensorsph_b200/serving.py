@@ -11,9 +11,13 @@ moment they reach their own step count, which frees room for the next ones.
 
 The engine advances in chunks of at most ``max_chunk`` steps that never pass
 the next completion, so a case runs exactly its own number of steps and each
-result equals the same request run alone (bitwise: see the engine).  Latency
-is wall clock from arrival to completion; ``run_serial`` serves the same
-stream one request at a time in arrival order with the single-case engine.
+result equals the same request run alone (bitwise: see the engine).  The host
+enqueues chunks, retirements and admissions on the engine stream without
+waiting in between (one chunk in flight ahead of the one being prepared), and
+the engine absorbs a change of the batch by updating its instantiated step
+graph in place.  Latency is from arrival to the device time at which the
+request's last step completed; ``run_serial`` serves the same stream one
+request at a time in arrival order with the single-case engine.
 
 Case types: ``dam_break_2d`` (1 : 2 column in a 4 x 1.5 tank, dam_break.py),
 ``column_3d`` (hydrostatic 3-D column filling a square tank,
@@ -150,7 +154,16 @@ class Server:
 
     def serve(self, requests, *, max_chunk: int = 64, keep_results: bool = False) -> dict:
         """Serve the stream in real time; returns per-request latencies and
-        aggregate throughput."""
+        aggregate throughput.
+
+        The host never waits for the device between chunks: a chunk's steps,
+        the retirement of the cases it completes and the admission of the
+        requests that have arrived are all enqueued on the engine stream, and
+        the host only waits for the chunk before the one in flight, so the
+        device always has the next chunk queued.  A request's completion time
+        is the device time (CUDA events on the engine stream, from an event
+        recorded when serving starts) of the end of its last chunk."""
+        import torch
         eng = self.engine
         pending = sorted(requests, key=lambda r: r.arrival)
         for r in pending:
@@ -161,9 +174,26 @@ class Server:
         results = {}
         updates = 0
         steps_run = 0
+        blocked = set()      # requests that arrived and had to wait for room
+        stats0 = eng.graph_stats()
+        inflight: list = []  # (event, [(request, last meter row, state or None)])
         t0 = time.perf_counter()
+        start = torch.cuda.Event(enable_timing=True)
+        start.record(eng.stream)
+
+        def retire(entry):
+            ev, done = entry
+            ev.synchronize()
+            at = start.elapsed_time(ev) / 1e3
+            for r, row, state in done:
+                if float(row[0, 13]) != 0.0:
+                    raise FloatingPointError(f"request {r.rid} went non-finite")
+                r.finished = at
+                if state is not None:
+                    results[r.rid] = [t.cpu() for t in state]
+
         i = 0
-        while i < len(pending) or waiting or active:
+        while i < len(pending) or waiting or active or inflight:
             now = time.perf_counter() - t0
             while i < len(pending) and pending[i].arrival <= now:
                 waiting.append(pending[i])
@@ -174,7 +204,11 @@ class Server:
                     r.admitted = time.perf_counter() - t0
                     active[cid] = (r, r.steps)
                     waiting.remove(r)
+                else:
+                    blocked.add(r.rid)
             if not active:
+                while inflight:
+                    retire(inflight.pop(0))
                 if waiting and i >= len(pending):
                     raise RuntimeError(f"request {waiting[0].rid} can never fit the budget")
                 if i < len(pending):
@@ -182,29 +216,39 @@ class Server:
                 continue
             chunk = min(max_chunk, min(left for _, left in active.values()))
             eng.step(chunk)
-            eng.stream.synchronize()
             steps_run += chunk
             updates += chunk * sum(r.spec.n_fluid for r, _ in active.values())
-            done_at = time.perf_counter() - t0
+            done = []
             for cid in list(active):
                 r, left = active[cid]
                 left -= chunk
                 if left == 0:
-                    if keep_results:
-                        results[r.rid] = [t.cpu() for t in eng.read(cid)]
-                    st = eng.status(cid)
-                    if st["status"]:
-                        raise FloatingPointError(f"request {r.rid} went non-finite")
+                    row = eng.diagnostics(cid, eng.steps_of[cid] - 1, 1)
+                    state = eng.read(cid) if keep_results else None
                     eng.remove(cid)
-                    r.finished = done_at
+                    done.append((r, row, state))
                     del active[cid]
                 else:
                     active[cid] = (r, left)
-        wall = time.perf_counter() - t0
+            ev = torch.cuda.Event(enable_timing=True)
+            ev.record(eng.stream)
+            inflight.append((ev, done))
+            while len(inflight) > 1:
+                retire(inflight.pop(0))
+        while inflight:
+            retire(inflight.pop(0))
+        end = torch.cuda.Event(enable_timing=True)
+        end.record(eng.stream)
+        end.synchronize()
+        wall = max(time.perf_counter() - t0, start.elapsed_time(end) / 1e3)
         lat = [r.latency for r in pending]
+        stats = eng.graph_stats()
         return {"requests": len(pending), "wall_s": wall, "updates": updates,
                 "updates_per_s": updates / wall, "engine_steps": steps_run,
-                "latency_s": percentiles(lat), "results": results}
+                "latency_s": percentiles(lat), "results": results,
+                "admissions_blocked": len(blocked),
+                "graph_instantiations": stats["instantiations"] - stats0["instantiations"],
+                "graph_updates": stats["updates"] - stats0["updates"]}
 
 
 def run_serial(requests, *, max_neighbors: int = 160, device=None, keep_results: bool = False) -> dict:

@@ -210,6 +210,35 @@ def test_served_results_equal_alone(gpu):
             assert torch.equal(u, w), rid
 
 
+def test_served_large_cases_equal_alone(gpu):
+    """A 3-D column of 60k particles and a periodic shear decay of 54,872 next
+    to small 2-D and 3-D requests, under a budget that holds only part of
+    them at a time (admissions wait for retirements): each result is bitwise
+    the one of the same request run alone, and the batch changes are absorbed
+    by graph updates or new instantiations counted by the engine."""
+    from tensorsph_b200 import serving as sv
+
+    def stream():
+        return [sv.Request(0, 0.0, "column_3d", 60000, 0.005, height=1.0),
+                sv.Request(1, 0.0, "shear_3d", 54872, 0.3),
+                sv.Request(2, 0.001, "dam_break_2d", 3000, 0.004, height=0.8),
+                sv.Request(3, 0.002, "column_3d", 8000, 0.003, height=0.6),
+                sv.Request(4, 0.003, "dam_break_2d", 1500, 0.002, height=0.5)]
+
+    reqs = stream()
+    srv = sv.Server(budget_bytes=0.17e9, max_cases=8, max_neighbors=160)
+    out = srv.serve(reqs, max_chunk=9, keep_results=True)
+    srv.close()
+    assert out["requests"] == 5 and all(r.finished > r.arrival for r in reqs)
+    assert out["admissions_blocked"] >= 1
+    assert out["graph_instantiations"] + out["graph_updates"] >= 2
+    assert reqs[0].spec.n_fluid >= 50000 and reqs[1].spec.n_fluid >= 50000
+    alone = sv.run_serial(stream(), keep_results=True)
+    for rid, got in out["results"].items():
+        for u, w in zip(got, alone["results"][rid]):
+            assert torch.equal(u, w), rid
+
+
 def test_droplet_ensemble_batched_equals_plain(gpu):
     from tensorsph_b200 import ensemble as en
     from tensorsph_b200.engine import BatchEngine, capacity_for
