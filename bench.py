@@ -81,6 +81,9 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=48)
     ap.add_argument("--serve-time-scale", type=float, default=0.05)
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
+    ap.add_argument("--dplus-dx", type=float, default=0.0138,
+                    help="lattice spacing of the 3-D delta-plus leg (0: no leg)")
+    ap.add_argument("--dplus-steps", type=int, default=20)
     ap.add_argument("--shear-n", type=int, default=64)
     ap.add_argument("--shear-steps", type=int, default=2000)
     ap.add_argument("--csf3-radius", type=int, default=40, help="column radius in dx (0: no 3-D CSF leg)")
@@ -428,6 +431,27 @@ def serving_leg(args, dev):
                      "throughput_vs_serial": served["updates_per_s"] / serial["updates_per_s"]}
     out["throughput_vs_serial"] = out["batched"]["throughput_vs_serial"]
     return out
+
+
+def delta_plus_leg(args, dev):
+    """The 3-D dam break with the obstacle advanced by delta-plus steps
+    (delta_plus_step3 through threed/delta_plus3.py, FP32): device time per
+    step, pair cache included, with the density deviation and the front."""
+    import torch
+    from tensorsph_b200.engine import obstacle_case
+    from tensorsph_b200.threed.delta_plus3 import delta_plus_case_3d, run_delta_plus_3d
+    cfg, ob = obstacle_case(dx=args.dplus_dx)
+    host = delta_plus_case_3d(cfg, ob, torch.float32)
+    run_delta_plus_3d(cfg, 2, obstacle=ob, dtype=torch.float32, host_state=host, device=dev)
+    run = run_delta_plus_3d(cfg, args.dplus_steps, obstacle=ob, dtype=torch.float32, host_state=host, device=dev)
+    return {"workload": f"3-D dam break with the box obstacle, delta-plus (h = 2 dx, Wendland C2, psi "
+                        f"diffusion 0.1, alpha 0.02, 4 station layers), dx={args.dplus_dx:g}, FP32, "
+                        f"{args.dplus_steps} steps from the hydrostatic start",
+            "fluid_particles": run.n_fluid, "wall_stations": run.n_wall,
+            "ms_per_step": 1e3 * run.seconds / run.steps,
+            "fluid_particles_per_s": run.n_fluid * run.steps / run.seconds,
+            "pair_rebuilds": run.rebuilds, "max_density_deviation": max(run.density_deviation),
+            "max_shift_over_dx": run.max_shift_over_dx, "front": [run.front[0], run.front[-1]]}
 
 
 def shear_leg(args, dev):
@@ -944,6 +968,7 @@ def main():
     if rank == 0 and world == 1:
         for name, leg, on in (("ensemble", ensemble_leg, args.ensemble_cases > 0),
                               ("serving", serving_leg, args.serve_requests > 0),
+                              ("delta_plus_3d", delta_plus_leg, args.dplus_dx > 0),
                               ("shear", shear_leg, args.shear_steps > 0),
                               ("csf3", csf3_leg, args.csf3_radius > 0),
                               ("tvc", tvc_leg, args.tvc_n > 0),
