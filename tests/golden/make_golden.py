@@ -1014,6 +1014,39 @@ def checkpoint_case(kl):
             "pos": _np(pos), "vel": _np(vel)}
 
 
+HYDROSTATIC_CASES = [
+    dict(nx=6, ny=5, nz=7, steps=30, sample_every=5, settle_fraction=0.5),
+    dict(nx=5, ny=5, nz=6, steps=24, sample_every=4, settle_fraction=0.5, lid=False,
+         density_diffusion=0.1, wall_model="adami"),
+]
+
+
+def hydrostatic_cases(sv):
+    """Short runs of the reference's wall-bounded column (threed/solver.py:353-484):
+    the sampled bottom pressure and centre of mass, and the profile's rows,
+    lattice rows and scalar accuracy numbers."""
+    data = {}
+    for k, kw in enumerate(HYDROSTATIC_CASES):
+        r = sv.run_hydrostatic(dtype=torch.float64, **kw)
+        prof = r.profile
+        data[f"c{k}_times"] = np.asarray(r.times, dtype=np.float64)
+        data[f"c{k}_bottom"] = np.asarray(r.bottom_pressure, dtype=np.float64)
+        data[f"c{k}_com"] = np.asarray(r.centre_of_mass_z, dtype=np.float64)
+        data[f"c{k}_counts"] = np.asarray([r.steps, r.fluid_particles, r.wall_particles], dtype=np.int64)
+        data[f"c{k}_rows_p"] = np.asarray([row["p_measured"] for row in prof["rows"]], dtype=np.float64)
+        data[f"c{k}_rows_rho"] = np.asarray([row["rho_measured"] for row in prof["rows"]], dtype=np.float64)
+        data[f"c{k}_lat_p"] = np.asarray([row["p_measured"] for row in prof["rows_by_lattice"]], dtype=np.float64)
+        data[f"c{k}_lat_z"] = np.asarray([row["z"] for row in prof["rows_by_lattice"]], dtype=np.float64)
+        for key in ("integral_p_measured", "odd_even_amplitude_over_scale", "max_rel_error_core_lattice",
+                    "wall_displacement"):
+            data[f"c{k}_{key}"] = np.float64(prof[key] if prof[key] is not None else np.nan)
+        data[f"c{k}_binning"] = np.asarray([prof["binning"][key] for key in
+                                            ("mean_offset_over_dx", "rms_offset_over_dx", "misplaced_fraction")])
+        data[f"c{k}_kinetic"] = np.float64(r.diagnostics[0]["kinetic_energy"])
+    data["count"] = np.int64(len(HYDROSTATIC_CASES))
+    return data
+
+
 def main(src, families=None):
     sys.path.insert(0, str(src))
     import tensorsph.neighbor_search as ns
@@ -1060,6 +1093,7 @@ def main(src, families=None):
         "adaptive_run": lambda: adaptive_run_case(db),
         "regularized": lambda: regularized_cases(di, db),
         "rhs3d_closure": lambda: rhs3d_closure_cases(d3, di),
+        "hydrostatic": lambda: hydrostatic_cases(sv),
     }
     for name in families or makers:
         np.savez_compressed(OUT / f"{name}.npz", **makers[name](), **meta)
