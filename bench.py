@@ -77,7 +77,7 @@ def parse():
     ap.add_argument("--cpu-sample-steps", type=int, default=6)
     ap.add_argument("--ensemble-cases", type=int, default=256)
     ap.add_argument("--ensemble-steps", type=int, default=100)
-    ap.add_argument("--plain-steps", type=int, default=20)
+    ap.add_argument("--plain-steps", type=int, default=100)
     ap.add_argument("--serve-requests", type=int, default=48)
     ap.add_argument("--serve-time-scale", type=float, default=0.05)
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
@@ -384,7 +384,11 @@ def ensemble_leg(args, dev):
     specs = en.ensemble_specs(draws, skin_factor=best["skin_factor"])
     batched = en.run_batched(specs, args.ensemble_steps, block=best["block"], batch=best["batch"],
                              device=dev)
-    plain = en.run_plain(specs, args.plain_steps, block=128, device=dev)
+    # the one-at-a-time arm tuned the same way, on one case alone
+    tune_plain = en.autotune(draws[:1], steps=20, warmup=5, device=dev)
+    bp = tune_plain["best"]
+    plain = en.run_plain(en.ensemble_specs(draws, skin_factor=bp["skin_factor"]), args.plain_steps,
+                         block=bp["block"], batch=bp["batch"], device=dev)
     return {"workload": f"{len(specs)} independent 2-D droplet impacts (R~U[0.02,0.08] m, dx=R/20, "
                         "depth~U[2R,6R], width 8R, U~U[1,5] m/s, seed 0), CSF sigma=0.0728 N/m",
             "fluid_particles": batched["fluid"],
@@ -393,7 +397,8 @@ def ensemble_leg(args, dev):
             "plain_updates_per_s": plain["updates_per_s"],
             "speedup_vs_plain": batched["updates_per_s"] / plain["updates_per_s"],
             "kernels_per_step": batched["kernels_per_step"], "failed_cases": batched["failed_cases"],
-            "autotune": {"best": best, "trials": len(tune["trials"])},
+            "autotune": {"best": best, "trials": len(tune["trials"]), "cached": tune.get("cached"),
+                         "plain_best": bp},
             "steps": {"batched": batched["steps"], "plain_per_case": plain["steps"]}}
 
 

@@ -711,13 +711,27 @@ class DamBreak3DEngine(BatchEngine):
 
 def tune_single_case(cfg: DamBreak3DConfig, *, obstacle=None, shift_every: int = 0, host_state=None,
                      skins=(0.1, 0.15, 0.25), blocks=(128, 256), batches=(4, 8), steps: int = 60,
-                     device=None) -> dict:
+                     device=None, cache: bool = True) -> dict:
     """Autotune one 3-D case by timing: the Verlet skin (which sets the cell edge
     2h + skin and how often lists are rebuilt), the pair kernels' block size and
     their batch depth.  Each trial runs ``steps`` graph steps on the device
     (rebuilds included); the results do not depend on the choice beyond the
-    summation order of the skin pairs.  Returns the fastest and every trial."""
+    summation order of the skin pairs.  Returns the fastest and every trial;
+    with ``cache`` a previous result for the same workload and GPU
+    (``tensorsph_b200.tuning``) is returned without timing, and a new one kept."""
     from dataclasses import replace
+    from . import tuning
+    key = None
+    if cache:
+        n = host_state[0].shape[0] if host_state is not None else dam_break_3d_host_state(cfg, obstacle)[0].shape[0]
+        dev = device or torch.device("cuda", torch.cuda.current_device())
+        key = tuning.tuning_key("dam_break_3d" + ("+obstacle" if obstacle is not None else "")
+                                + f"+shift{shift_every}", dim=3, particles=n, h_over_dx=cfg.h_factor,
+                                candidates={"skins": skins, "blocks": blocks, "batches": batches},
+                                gpu=torch.cuda.get_device_name(dev))
+        hit = tuning.lookup(key)
+        if hit is not None:
+            return {"best": hit, "trials": [], "cached": True}
     trials = []
     for skin in skins:
         c = replace(cfg, pair_skin_factor=float(skin))
@@ -739,7 +753,9 @@ def tune_single_case(cfg: DamBreak3DConfig, *, obstacle=None, shift_every: int =
                                "ms_per_step": start.elapsed_time(stop) / steps})
         eng.close()
     best = min(trials, key=lambda t: t["ms_per_step"])
-    return {"best": best, "trials": trials}
+    if key is not None:
+        tuning.store(key, best)
+    return {"best": best, "trials": trials, "cached": False}
 
 
 def _sample_steps(steps: int, output_every: int, dt: float):

@@ -94,14 +94,15 @@ def run_batched(specs, steps: int, *, warmup: int = 3, block: int = 128, batch: 
             "kernels_per_rebuild_pass": rebuild_kernels, "failed_cases": bad}
 
 
-def run_plain(specs, steps: int, *, warmup: int = 3, block: int = 128, max_neighbors: int = 64,
-              device=None) -> dict:
+def run_plain(specs, steps: int, *, warmup: int = 3, block: int = 128, batch: int = 4,
+              max_neighbors: int = 64, device=None) -> dict:
     """The same cases one at a time, each in its own single-case engine (the
     plain drop-in loop); device time summed over the cases."""
     total_t, total_u = 0.0, 0
     for s in specs:
         eng = BatchEngine(**capacity_for([s], max_neighbors=max_neighbors, diag_ring=8), device=device)
         eng.set_block(block)
+        eng.set_batch(batch)
         eng.add(s)
         eng.step(warmup)
         total_t += _timed_steps(eng, steps)
@@ -112,12 +113,25 @@ def run_plain(specs, steps: int, *, warmup: int = 3, block: int = 128, max_neigh
 
 
 def autotune(draws, *, blocks=(64, 128, 256), batches=(4, 8), skins=(0.15, 0.25, 0.4),
-             steps: int = 30, warmup: int = 10, device=None) -> dict:
+             steps: int = 30, warmup: int = 10, device=None, cache: bool = True) -> dict:
     """Time each (block, batch depth, skin) on the sample ``draws`` and return
     the fastest.
 
     The skin sets both the cell edge (2h + skin) and how often lists are
-    rebuilt, so it is timed over enough steps to include rebuilds."""
+    rebuilt, so it is timed over enough steps to include rebuilds.  With
+    ``cache`` a previous result for the same sample size and GPU
+    (``tensorsph_b200.tuning``) is returned without timing, and a new one kept."""
+    from . import tuning
+    key = None
+    if cache:
+        dev = device or torch.device("cuda", torch.cuda.current_device())
+        n = sum(s.n_fluid for s in ensemble_specs(draws, skin_factor=skins[0]))
+        key = tuning.tuning_key(f"droplet_ensemble{len(draws)}", dim=2, particles=n, h_over_dx=1.3,
+                                candidates={"skins": skins, "blocks": blocks, "batches": batches},
+                                gpu=torch.cuda.get_device_name(dev))
+        hit = tuning.lookup(key)
+        if hit is not None:
+            return {"best": hit, "trials": [], "cached": True}
     trials = []
     for skin in skins:
         specs = ensemble_specs(draws, skin_factor=skin)
@@ -127,7 +141,9 @@ def autotune(draws, *, blocks=(64, 128, 256), batches=(4, 8), skins=(0.15, 0.25,
                 trials.append({"block": block, "batch": batch, "skin_factor": skin,
                                "updates_per_s": r["updates_per_s"]})
     best = max(trials, key=lambda t: t["updates_per_s"])
-    return {"best": best, "trials": trials}
+    if key is not None:
+        tuning.store(key, best)
+    return {"best": best, "trials": trials, "cached": False}
 
 
 def main(argv=None) -> None:

@@ -128,3 +128,21 @@ def test_dam_break_2d_shift_reference_speed_and_refusals():
     assert (p.shift_vref_given, p.shift_vref) == (1, 0.7)
     with pytest.raises(NotImplementedError):
         dam_break_2d_case(_dam2d(surface_tension_coefficient=0.07))
+
+
+def test_tuning_cache_roundtrip(tmp_path, monkeypatch):
+    """The autotuning cache: a stored best comes back under the same key
+    only (workload, particle count to 3 significant digits, candidates, GPU)."""
+    from tensorsph_b200 import tuning
+    monkeypatch.setenv("TSPH_TUNING_CACHE", str(tmp_path / "t.json"))
+    k1 = tuning.tuning_key("dam_break_3d", dim=3, particles=1968048, h_over_dx=1.3,
+                           candidates={"skins": (0.1, 0.15)}, gpu="NVIDIA B200")
+    k2 = tuning.tuning_key("dam_break_3d", dim=3, particles=1968400, h_over_dx=1.3,
+                           candidates={"skins": (0.1, 0.15)}, gpu="NVIDIA B200")
+    k3 = tuning.tuning_key("dam_break_3d", dim=3, particles=1968048, h_over_dx=1.3,
+                           candidates={"skins": (0.1, 0.15)}, gpu="NVIDIA H100")
+    assert k1 == k2 and k1 != k3
+    assert tuning.lookup(k1) is None
+    tuning.store(k1, {"skin_factor": 0.15, "block": 128, "batch": 8})
+    assert tuning.lookup(k2) == {"skin_factor": 0.15, "block": 128, "batch": 8}
+    assert tuning.lookup(k3) is None
