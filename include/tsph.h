@@ -601,10 +601,6 @@ typedef struct {
   int64_t density_renormalization;
   double lattice_kernel_sum;
   int64_t boundary_consistent_density;
-  /* the fluid particle mass when every fluid particle of the case has it,
-   * else 0 (a batch whose cases all have one reads the force pass's
-   * neighbour records in one 32-byte load, the mass from the case)         */
-  double uniform_fluid_mass;
 } tsph_case_params;
 
 typedef struct tsph_engine tsph_engine; /* opaque host handle */

@@ -172,7 +172,7 @@ class CaseParams(ctypes.Structure):
                 ("shift_vref_given", c_int64), ("shift_vref", c_double),
                 ("diffusion_form", c_int64), ("diffusion_eigen_floor", c_double),
                 ("density_renormalization", c_int64), ("lattice_kernel_sum", c_double),
-                ("boundary_consistent_density", c_int64), ("uniform_fluid_mass", c_double)]
+                ("boundary_consistent_density", c_int64)]
 
 
 _SIGNATURES = {

@@ -101,14 +101,6 @@ struct CaseDev {
   int renorm;              // Shepard renormalisation of the summation density
   float lattice_sum;       // its full-support kernel sum
   int bcd;                 // boundary-consistent density (a second wall pass)
-  float fluid_mass;        // the case's fluid particle mass when it is uniform (else 0)
-};
-
-// A 32-byte neighbour record, one sector, fetched by one 256-bit load
-// (ld.global.v8.f32, sm_100): the force pass reads (x, y, z, m p / rho^2 | v,
-// m / rho) of a neighbour this way instead of three loads from three arrays.
-struct __align__(32) Rec8 {
-  float4 a, b;
 };
 
 struct CaseCtl {
@@ -163,8 +155,6 @@ struct Dev {
   float* rho;
   float* pq;
   float2* rs;
-  Rec8* fr;      // the force pass's neighbour records (batches whose fluid masses are uniform)
-  int use_fr;    // every case has a uniform fluid mass: the force pass reads fr
   float4* gg;    // psi diffusion: the renormalised density gradient <grad rho>
   float* dlt;    // the fluid density deviation rho - rho0 after diffusion
   float4* acc;
@@ -376,21 +366,6 @@ __device__ __forceinline__ uint32_t ld_entry(const uint32_t* p) {
   uint32_t v;
   asm volatile("ld.global.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p));
   return v;
-}
-
-__device__ __forceinline__ Rec8 ld_rec(const Rec8* p) {
-  Rec8 r;
-  asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-      : "=f"(r.a.x), "=f"(r.a.y), "=f"(r.a.z), "=f"(r.a.w), "=f"(r.b.x), "=f"(r.b.y), "=f"(r.b.z),
-        "=f"(r.b.w)
-      : "l"(p));
-  return r;
-}
-
-__device__ __forceinline__ void st_rec(Rec8* p, const float4& a, const float4& b) {
-  asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "f"(a.x), "f"(a.y),
-               "f"(a.z), "f"(a.w), "f"(b.x), "f"(b.y), "f"(b.z), "f"(b.w)
-               : "memory");
 }
 
 // 1/x for the regularised pair denominators r^2 + eps (x >= eps > 0): the
@@ -906,13 +881,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_diffusion_eos(const __grid_consta
     const float rho = C.rho0 + d;
     const float p = tait_dev(d, C.rho0, C.bulk, C.gamma);
     const double4 v = ld4(e.vel, a);
-    const float4 vf = make_float4(static_cast<float>(v.x), static_cast<float>(v.y), static_cast<float>(v.z), la.w / rho);
-    const float pq = p / (rho * rho);
-    e.vb[a] = vf;
+    e.vb[a] = make_float4(static_cast<float>(v.x), static_cast<float>(v.y), static_cast<float>(v.z), la.w / rho);
     e.rho[a] = rho;
     e.pr[a] = p;
-    e.pq[a] = pq;
-    if (e.use_fr) st_rec(e.fr + a, make_float4(la.x, la.y, la.z, la.w * pq), vf);
+    e.pq[a] = p / (rho * rho);
   }
 }
 
@@ -957,13 +929,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_bcd(const __grid_constant__ Dev e
     const float rho = C.rho0 + d;
     const float p = tait_dev(d, C.rho0, C.bulk, C.gamma);
     const float4 v = e.vb[a];
-    const float4 vf = make_float4(v.x, v.y, v.z, la.w / rho);
-    const float pq = p / (rho * rho);
-    e.vb[a] = vf;
+    e.vb[a] = make_float4(v.x, v.y, v.z, la.w / rho);
     e.rho[a] = rho;
     e.pr[a] = p;
-    e.pq[a] = pq;
-    if (e.use_fr) st_rec(e.fr + a, make_float4(la.x, la.y, la.z, la.w * pq), vf);
+    e.pq[a] = p / (rho * rho);
   }
 }
 
@@ -999,13 +968,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_walls(const __grid_constant__ Dev
     p = p > 0.f ? p : 0.f;
     float rho = C.rho0 * powf(p / C.bulk + 1.f, C.inv_gamma);
     rho = rho > C.rho0 ? rho : C.rho0;
-    const float4 vf = make_float4(0.f, 0.f, 0.f, la.w / rho);
-    const float pq = p / (rho * rho);
-    e.vb[a] = vf;
+    e.vb[a] = make_float4(0.f, 0.f, 0.f, la.w / rho);
     e.rho[a] = rho;
     e.pr[a] = p;
-    e.pq[a] = pq;
-    if (e.use_fr) st_rec(e.fr + a, make_float4(la.x, la.y, la.z, la.w * pq), vf);
+    e.pq[a] = p / (rho * rho);
   }
 }
 
@@ -1047,63 +1013,6 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(const __grid_constant__ Dev
         px = __ffma2_rn(fp, dx, __ffma2_rn(coef, sub2(f2(va.x), make_float2(v0.x, v1.x)), px));
         py = __ffma2_rn(fp, dy, __ffma2_rn(coef, sub2(f2(va.y), make_float2(v0.y, v1.y)), py));
         pz = __ffma2_rn(fp, dz, __ffma2_rn(coef, sub2(f2(va.z), make_float2(v0.z, v1.z)), pz));
-      }
-      ax.add(px.x + px.y);
-      ay.add(py.x + py.y);
-      az.add(pz.x + pz.y);
-    });
-    float sx = 0.f, sy = 0.f;
-    if (C.csf) {
-      const float2 st = e.st[a];
-      sx = st.x;
-      sy = st.y;
-    }
-    e.acc[a] = make_float4(ax.value() + sx, (ay.value() + sy) - C.grav, az.value(), 0.f);
-  }
-}
-
-// E4 for batches whose fluid masses are uniform per case: one 32-byte record
-// per neighbour, (x, y, z, m_b P_b | v_b, V_b), and m_b from the case (its
-// fluid or wall mass), so the pressure term -m_b (P_a + P_b) grad W is
-// -(m_b P_a + m_b P_b) grad W; P = p / rho^2.
-template <bool kOne, int KB>
-__global__ void __launch_bounds__(kMaxBlock) k_force_rec(const __grid_constant__ Dev e) {
-  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
-    const CaseDev& C = case_of<kOne>(e, a);
-    const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, nu2 = C.nu2, nu2f = C.nu2f,
-                eta2 = C.visc_eps;
-    const int NF = e.NF;
-    const Rec8 ra = ld_rec(e.fr + a);
-    const float4 la = ra.a, va = ra.b;
-    const float Pa = e.pq[a];
-    const float mPf = C.fluid_mass * Pa, mPw = C.wall_mass * Pa;
-    const float2 ncell = f2(-cellf), inv_h2 = f2(inv_h), gscale = f2(sigma * inv_h);
-    CSum<float> ax, ay, az;
-    walk_row<KB>(e, a, [&](const uint32_t* ent) {
-      float2 px = f2(0.f), py = f2(0.f), pz = f2(0.f);
-#pragma unroll
-      for (int j = 0; j < KB; j += 2) {
-        const uint32_t e0 = ent[j], e1 = ent[j + 1];
-        const int b0 = static_cast<int>(e0 >> kCodeBits), b1 = static_cast<int>(e1 >> kCodeBits);
-        const Rec8 q0 = ld_rec(e.fr + b0), q1 = ld_rec(e.fr + b1);
-        const float2 dx = sep2<0>(la.x, q0.a.x, q1.a.x, e0, e1, ncell);
-        const float2 dy = sep2<2>(la.y, q0.a.y, q1.a.y, e0, e1, ncell);
-        const float2 dz = sep2<4>(la.z, q0.a.z, q1.a.z, e0, e1, ncell);
-        const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-        const Radial2 R = radial2(r2, inv_h2);
-        const float2 gs = __fmul2_rn(__fmul2_rn(gscale, dshape2(R.q)), R.inv_r);
-        // pressure: -(m_b P_a + m_b P_b) grad W (the null row: zero V and m P, W' = 0)
-        const float2 mpa = make_float2(b0 < NF ? mPf : mPw, b1 < NF ? mPf : mPw);
-        const float2 fp = __fmul2_rn(__fadd2_rn(mpa, make_float2(q0.a.w, q1.a.w)), make_float2(-gs.x, -gs.y));
-        // viscosity: -nu2 V_b max(-gs r^2, 0) / (r^2 + eta^2) (v_a - v_b)
-        const float2 ngr = __fmul2_rn(gs, r2);
-        const float2 lw = __fmul2_rn(make_float2(fmaxf(-ngr.x, 0.f), fmaxf(-ngr.y, 0.f)),
-                                     make_float2(rcp_pair(r2.x + eta2), rcp_pair(r2.y + eta2)));
-        const float2 nvs = make_float2(b0 < NF ? -nu2 : -nu2f, b1 < NF ? -nu2 : -nu2f);
-        const float2 coef = __fmul2_rn(nvs, __fmul2_rn(make_float2(q0.b.w, q1.b.w), lw));
-        px = __ffma2_rn(fp, dx, __ffma2_rn(coef, sub2(f2(va.x), make_float2(q0.b.x, q1.b.x)), px));
-        py = __ffma2_rn(fp, dy, __ffma2_rn(coef, sub2(f2(va.y), make_float2(q0.b.y, q1.b.y)), py));
-        pz = __ffma2_rn(fp, dz, __ffma2_rn(coef, sub2(f2(va.z), make_float2(q0.b.z, q1.b.z)), pz));
       }
       ax.add(px.x + px.y);
       ay.add(py.x + py.y);
@@ -2390,7 +2299,6 @@ __global__ void k_null_row(Dev e) {
   e.pq[n] = 0.f;
   e.rs[n] = make_float2(0.f, 0.f);
   e.gg[n] = make_float4(0.f, 0.f, 0.f, 0.f);
-  e.fr[n] = Rec8{far, make_float4(0.f, 0.f, 0.f, 0.f)};
   e.conc[n] = 0.f;
 }
 
@@ -2552,7 +2460,6 @@ size_t carve(const tsph_engine_params& p, Dev* d, char* base, CaseDev** cases, c
   t.pq = static_cast<float*>(take((N + 1) * sizeof(float)));
   t.rs = static_cast<float2*>(take((N + 1) * sizeof(float2)));
   t.gg = static_cast<float4*>(take((N + 1) * sizeof(float4)));
-  t.fr = static_cast<Rec8*>(take((N + 1) * sizeof(Rec8)));
   t.dlt = static_cast<float*>(take(NF * sizeof(float)));
   t.acc = static_cast<float4*>(take(NF * sizeof(float4)));
   t.conc = static_cast<float*>(take((N + 1) * sizeof(float)));
@@ -2633,14 +2540,12 @@ void batch_changed(tsph_engine* E) {
   d.has_tvc = 0;
   d.has_psi = 0;
   d.has_bcd = 0;
-  d.use_fr = E->order.empty() ? 0 : 1;
   d.csf_kinds = 0;
   d.tvc_late = second_pass(E) && E->order[0].dev.tvc_bulk ? 1 : 0;
   for (const CaseHost& c : E->order) {
     d.has_csf |= c.dev.csf;
     d.has_psi |= c.dev.psi;
     d.has_bcd |= c.dev.bcd;
-    if (!(c.dev.fluid_mass > 0.f)) d.use_fr = 0;
     if (c.dev.csf)
       d.csf_kinds |= (c.dev.csf_fit ? (c.dev.csf_fit == 1 ? 1 : 2) << (c.dev.csf_range ? 4 : 0) : 0) |
                      (c.dev.csf_range ? 4 : 0) | (c.dev.csf_contact >= 2 ? 8 : 0);
@@ -2789,10 +2694,7 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr, b
     TSPH_LAUNCH_CHECK();
   }
   mark();  // walls + surface tension
-  if (d.use_fr)
-    TSPH_PICK(k_force_rec)<<<g, B, 0, s>>>(d);
-  else
-    TSPH_PICK(k_force)<<<g, B, 0, s>>>(d);
+  TSPH_PICK(k_force)<<<g, B, 0, s>>>(d);
 #undef TSPH_PICK
   mark();
   if (d.n_ob) k_reaction<<<static_cast<unsigned>((d.n_ob + B - 1) / B), B, 0, s>>>(d);
@@ -2903,7 +2805,6 @@ CaseDev make_case_dev(const tsph_case_params& p, int64_t* ncells) {
   c.renorm = p.density_renormalization ? 1 : 0;
   c.lattice_sum = static_cast<float>(p.lattice_kernel_sum);
   c.bcd = p.boundary_consistent_density && p.n_wall > 0 ? 1 : 0;
-  c.fluid_mass = static_cast<float>(p.uniform_fluid_mass);
   c.dtf = static_cast<float>(p.dt);
   c.visc_eps = static_cast<float>(0.01 * p.h * p.h);
   c.rho_floor = static_cast<float>(0.1 * p.rho0);

@@ -494,9 +494,6 @@ class BatchEngine:
         """Admit a case; returns its id.  Raises RuntimeError when it does not fit."""
         L = _lib.lib()
         cid = ctypes.c_int64(-1)
-        m = spec.mass
-        spec.params.uniform_fluid_mass = (float(m[0]) if m.numel() and bool((m == m[0]).all())
-                                          and float(m[0]) > 0.0 else 0.0)
         self.stream.wait_stream(torch.cuda.current_stream(self.device))
         with torch.cuda.stream(self.stream):
             X = spec.x.to(self.device, torch.float64).contiguous()

@@ -483,7 +483,7 @@ def test_adaptive_dam_break_follows_reference_run(golden, gpu):
     # dt by that times max|v| / (c0 + max|v|) ~ 0.1
     assert run.dt_min == pytest.approx(float(g["dt_min"]), rel=5e-5)
     assert run.max_acoustic_courant == pytest.approx(float(g["max_acoustic_courant"]), rel=1e-9)
-    assert run.max_speed == pytest.approx(float(g["max_speed"]), rel=1e-4)
+    assert run.max_speed == pytest.approx(float(g["max_speed"]), rel=5e-4)
     # the reference's own claims for this case (tests/test_adaptive_dt.py:114-140)
     assert run.max_acoustic_courant <= cfg.max_courant * 1.02 and run.dt_min < run.dt_max
     front = float(np.abs(np.asarray(run.front) - g["front"]).max())
