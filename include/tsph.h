@@ -199,12 +199,10 @@ int tsph_wcsph_rhs(const tsph_wcsph_params* prm, const tsph_wcsph_io* io, void* 
  * whose tsph_wcsph_workspace_bytes exceeds 16 MiB are rejected with
  * TSPH_ERR_CAPACITY before any GPU work: about 300,000 particles (fluid +
  * wall) in FP32, 150,000 in FP64.  The first call on a device looks up the
- * array's device address (with that device current), so make that first call
- * before any stream capture; the stream must belong to the current device.
- * The address is kept per device together with the id of the context it was
- * taken in: after cudaDeviceReset (or a context destroyed and created again)
- * the next call takes it again, and that call too should come before any
- * stream capture.
+ * array's device address (with that device current); the stream must belong
+ * to the current device.  The address is kept per device together with the
+ * id of the context it was taken in: after cudaDeviceReset (or a context
+ * destroyed and created again) the next call takes it again.
  * Every call shares the one array and leaves its contents behind: calls that
  * overlap on the GPU (other streams, other threads, the same device) race on
  * it, so serialise them.  No part of the array has to start at zero. */

@@ -791,9 +791,8 @@ extern "C" int tsph_wcsph_rhs_noalloc(const tsph_wcsph_params* prm, const tsph_w
   void* scratch = nullptr;
   {
     // the first call on a device (and the first after its context changed)
-    // takes the array's device address; that call should come before any
-    // stream capture (when the context id cannot be read, the address is
-    // taken on every call)
+    // takes the array's device address (when the context id cannot be read,
+    // the address is taken on every call)
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     const unsigned long long ctx = current_context_id();
     scratch = g_noalloc_ptr[dev];
