@@ -599,6 +599,11 @@ typedef struct {
   int64_t density_renormalization;
   double lattice_kernel_sum;
   int64_t boundary_consistent_density;
+  /* adaptive_dt resumed from a checkpoint (kleefsman_obstacle_3d.py:598-626
+   * restores elapsed and dt): the simulated time at the start of step
+   * first_step and the step size next_dt gave it (<= 0: dt)                */
+  double start_elapsed;
+  double start_dt;
 } tsph_case_params;
 
 typedef struct tsph_engine tsph_engine; /* opaque host handle */
@@ -664,6 +669,12 @@ int tsph_engine_diag(tsph_engine* engine, int64_t case_id, double* out, int64_t 
  * non-finite state and TSPH_ERR_CAPACITY when a neighbour row overflowed. */
 int tsph_engine_status(tsph_engine* engine, int64_t case_id, int64_t* counters,
                        tsph_stream stream);
+/* The adaptive clock of one case after the steps run so far: the simulated
+ * time at the start of its next step and that step's size before the clamp
+ * to the target time (the `elapsed` and `dt` a checkpoint of the loop at
+ * kleefsman_obstacle_3d.py:636-640 stores) to the host; synchronises.
+ * `clock` holds 2 values. */
+int tsph_engine_clock(tsph_engine* engine, int64_t case_id, double* clock, tsph_stream stream);
 /* Threads per block of the pair kernels: 64, 128 (default) or 256.  A tuning
  * knob (results do not depend on it); the step graph is re-captured. */
 int tsph_engine_set_block(tsph_engine* engine, int64_t threads);

@@ -172,7 +172,8 @@ class CaseParams(ctypes.Structure):
                 ("shift_vref_given", c_int64), ("shift_vref", c_double),
                 ("diffusion_form", c_int64), ("diffusion_eigen_floor", c_double),
                 ("density_renormalization", c_int64), ("lattice_kernel_sum", c_double),
-                ("boundary_consistent_density", c_int64)]
+                ("boundary_consistent_density", c_int64),
+                ("start_elapsed", c_double), ("start_dt", c_double)]
 
 
 _SIGNATURES = {
@@ -252,6 +253,7 @@ _SIGNATURES = {
                                  c_void_p]),
     "tsph_engine_diag": (c_int, [c_void_p, c_int64, c_void_p, c_int64, c_int64, c_void_p]),
     "tsph_engine_status": (c_int, [c_void_p, c_int64, c_void_p, c_void_p]),
+    "tsph_engine_clock": (c_int, [c_void_p, c_int64, c_void_p, c_void_p]),
     "tsph_engine_usage": (c_int, [c_void_p, c_void_p]),
     "tsph_engine_row_entries": (c_int, [c_void_p, c_void_p, c_void_p]),
     "tsph_engine_graph_stats": (c_int, [c_void_p, c_void_p]),

@@ -2850,8 +2850,10 @@ bool case_params_ok(const tsph_case_params* p) {
   if (!p || (p->dim != 2 && p->dim != 3) || p->n_fluid <= 0 || p->n_wall < 0 || p->n_obstacle < 0 ||
       p->n_obstacle > p->n_wall || p->shift_every < 0 || p->first_step < 0)
     return false;
-  if (p->adaptive_dt && (p->first_step != 0 || !(p->courant_h > 0.0) || !(p->dt_limit > 0.0) ||
-                        !(p->dt_safety > 0.0) || !(p->target_time > 0.0) || !std::isfinite(p->dt_growth)))
+  if (p->adaptive_dt && (!(p->courant_h > 0.0) || !(p->dt_limit > 0.0) || !(p->dt_safety > 0.0) ||
+                        !(p->target_time > 0.0) || !std::isfinite(p->dt_growth) ||
+                        !(p->start_elapsed >= 0.0) || !std::isfinite(p->start_elapsed) ||
+                        !std::isfinite(p->start_dt)))
     return false;
   if (p->csf_curvature < 0 || p->csf_curvature > 2 || p->csf_delta_normalization < 0 ||
       p->csf_delta_normalization > 1 || p->csf_contact_model < 0 || p->csf_contact_model > 3 ||
@@ -3002,7 +3004,12 @@ int tsph_engine_add_case(tsph_engine* E, const tsph_case_params* p, const double
   ctl.active = 1;
   ctl.steps = static_cast<unsigned long long>(p->first_step);
   ctl.dt_now = p->dt;
-  ctl.dt_step = ctl.dt_int = p->dt;
+  if (p->adaptive_dt) {
+    // a run resumed from a checkpoint continues its clock and step size
+    ctl.elapsed = p->start_elapsed;
+    if (p->start_dt > 0.0) ctl.dt_now = p->start_dt;
+  }
+  ctl.dt_step = ctl.dt_int = ctl.dt_now;
   TSPH_CUDA_CHECK(cudaMemcpyAsync(d.ctl + slot, &ctl, sizeof(CaseCtl), cudaMemcpyHostToDevice, s));
   TSPH_CUDA_CHECK(cudaMemsetAsync(d.diag + static_cast<int64_t>(slot) * d.diag_ring * kDiag, 0,
                                   static_cast<size_t>(d.diag_ring) * kDiag * sizeof(double), s));
@@ -3283,6 +3290,18 @@ int tsph_engine_status(tsph_engine* E, int64_t case_id, int64_t* counters, tsph_
   counters[7] = t.final_step;
   if (t.status & 2) return TSPH_ERR_STATE;
   if (t.status & 1) return TSPH_ERR_CAPACITY;
+  return TSPH_OK;
+}
+
+int tsph_engine_clock(tsph_engine* E, int64_t case_id, double* clock, tsph_stream stream) {
+  if (!E || !clock) return TSPH_ERR_ARG;
+  if (!find_case(E, case_id)) return TSPH_ERR_ARG;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  CaseCtl t;
+  TSPH_CUDA_CHECK(cudaMemcpyAsync(&t, E->d.ctl + case_id, sizeof(CaseCtl), cudaMemcpyDeviceToHost, s));
+  TSPH_CUDA_CHECK(cudaStreamSynchronize(s));
+  clock[0] = t.elapsed;
+  clock[1] = t.dt_now;
   return TSPH_OK;
 }
 

@@ -144,7 +144,7 @@ class CaseSpec:
 
 
 def _case_params(*, dim, n_fluid, n_wall, n_obstacle, cfg, h, wall_mass, box_hi, lo, hi,
-                 shift_every=0, obstacle=None, first_step=0, adaptive=False):
+                 shift_every=0, obstacle=None, first_step=0, adaptive=False, start_clock=None):
     psi = cfg.density_diffusion > 0.0 and cfg.density_diffusion_form == "antuono"
     if psi and dim == 3:
         # rhs_3d's contract (dam_break_3d.py:330-336)
@@ -225,6 +225,9 @@ def _case_params(*, dim, n_fluid, n_wall, n_obstacle, cfg, h, wall_mass, box_hi,
                          capillary_dt_limit(cfg))
         p.dt_growth, p.dt_safety = float(cfg.dt_growth), float(cfg.dt_safety)
         p.target_time = cfg.steps * cfg.dt
+        if start_clock is not None:
+            # a resumed run: the time at the start of first_step and its step size
+            p.start_elapsed, p.start_dt = float(start_clock[0]), float(start_clock[1])
     p.shift_strength = getattr(cfg, "shift_strength", 1.0)
     p.shift_limit = getattr(cfg, "shift_limit", 0.25)
     p.shift_free_surface = 0.95
@@ -259,10 +262,12 @@ def dam_break_3d_host_state(cfg: DamBreak3DConfig, obstacle=None, seed=None):
 
 
 def dam_break_3d_case(cfg: DamBreak3DConfig, *, obstacle=None, shift_every: int = 0, seed=None,
-                      host_state=None, velocity=None, first_step: int = 0, label: str = "") -> CaseSpec:
+                      host_state=None, velocity=None, first_step: int = 0, start_clock=None,
+                      label: str = "") -> CaseSpec:
     """The 3-D dam break of ``tensorsph.dam_break_3d`` (optionally with the box
     obstacle of kleefsman_obstacle_3d.py) as a ``CaseSpec``; ``first_step``
-    numbers the first step of a resumed run."""
+    numbers the first step of a resumed run, and an adaptive run resumed from a
+    checkpoint starts from ``start_clock`` = (elapsed, dt) of that checkpoint."""
     if host_state is None:
         host_state = dam_break_3d_host_state(cfg, obstacle, seed)
     x, mass, wall, n_ob = host_state
@@ -275,7 +280,8 @@ def dam_break_3d_case(cfg: DamBreak3DConfig, *, obstacle=None, shift_every: int 
                      wall_mass=mass_3d(cfg.dx, cfg.h_factor, cfg.rho0, cfg.density_calibration),
                      box_hi=box, lo=allpos.min(dim=0).values.tolist(),
                      hi=allpos.max(dim=0).values.tolist(), shift_every=shift_every,
-                     obstacle=obstacle, first_step=first_step, adaptive=cfg.adaptive_dt)
+                     obstacle=obstacle, first_step=first_step, adaptive=cfg.adaptive_dt,
+                     start_clock=start_clock)
     v = torch.zeros_like(x) if velocity is None else velocity.double().contiguous()
     return CaseSpec(p, x, v, mass.double().contiguous(), wall, label or "dam_break_3d")
 
@@ -606,6 +612,15 @@ class BatchEngine:
         _lib.check(rc, "tsph_engine_status")
         return out
 
+    def clock(self, case_id: int) -> tuple[float, float]:
+        """(elapsed, dt) of an adaptive case after the steps run so far: the
+        time at the start of its next step and that step's size before the
+        clamp to the target time (synchronises the engine stream)."""
+        buf = (ctypes.c_double * 2)()
+        _lib.check(_lib.lib().tsph_engine_clock(self._handle, int(case_id), buf, self.stream.cuda_stream),
+                   "tsph_engine_clock")
+        return float(buf[0]), float(buf[1])
+
     def close(self) -> None:
         if self._handle is not None and self._handle.value:
             torch.cuda.synchronize(self.device)
@@ -676,9 +691,10 @@ class DamBreak3DEngine(BatchEngine):
     def __init__(self, cfg: DamBreak3DConfig, *, obstacle=None, shift_every: int = 0,
                  seed: int | None = None, max_neighbors: int = 160, diag_ring: int = 8192,
                  device: torch.device | None = None, host_state=None, velocity=None,
-                 first_step: int = 0):
+                 first_step: int = 0, start_clock=None):
         spec = dam_break_3d_case(cfg, obstacle=obstacle, shift_every=shift_every, seed=seed,
-                                 host_state=host_state, velocity=velocity, first_step=first_step)
+                                 host_state=host_state, velocity=velocity, first_step=first_step,
+                                 start_clock=start_clock)
         super().__init__(**capacity_for([spec], max_neighbors=max_neighbors, diag_ring=diag_ring),
                          device=device)
         self.cfg = cfg
@@ -939,10 +955,6 @@ def run_case(cfg: DamBreak3DConfig, pair_skin_factor: float | None = None, snaps
     if pair_skin_factor is not None:
         from dataclasses import replace
         cfg = replace(cfg, pair_skin_factor=pair_skin_factor)
-    if cfg.adaptive_dt:
-        if checkpoint_path is not None:
-            raise NotImplementedError("checkpoints with adaptive_dt are not supported by the device engine")
-        return _run_3d_adaptive(cfg, obstacle, shift_every, seed, max_neighbors, snapshot_times)
     host = dam_break_3d_host_state(cfg, obstacle, seed)
     prev = None
     if checkpoint_path is not None and resume and Path(checkpoint_path).exists():
@@ -952,8 +964,13 @@ def run_case(cfg: DamBreak3DConfig, pair_skin_factor: float | None = None, snaps
                              f"this configuration builds {tuple(host[0].shape)}")
         if "device_run" not in prev:
             raise ValueError("checkpoint carries no device run record; it was written by another driver")
-        if prev["step"] + 1 > cfg.steps:
+        if not cfg.adaptive_dt and prev["step"] + 1 > cfg.steps:
             raise ValueError(f"checkpoint step {prev['step']} is not below the run's {cfg.steps} steps")
+        if cfg.adaptive_dt and prev["elapsed"] >= cfg.steps * cfg.dt - 1.0e-12 * max(1.0, cfg.steps * cfg.dt):
+            raise ValueError(f"checkpoint time {prev['elapsed']} is not below the run's {cfg.steps * cfg.dt}")
+    if cfg.adaptive_dt:
+        return _run_3d_adaptive(cfg, obstacle, shift_every, seed, max_neighbors, snapshot_times, host=host,
+                                prev=prev, checkpoint_path=checkpoint_path, checkpoint_every=checkpoint_every)
     first = prev["step"] + 1 if prev else 0
     if prev:
         host = (prev["positions"].double(), host[1], host[2], host[3])
@@ -1026,36 +1043,112 @@ def run_case(cfg: DamBreak3DConfig, pair_skin_factor: float | None = None, snaps
     return run
 
 
-def _run_3d_adaptive(cfg, obstacle, shift_every: int, seed, max_neighbors: int, snapshot_times=None) -> DamBreak3DRun:
+class _AdaptiveRecord(_DeviceRecord):
+    """``_DeviceRecord`` of an adaptive run: its samples are the
+    output_every-th steps and the final one, their times read from the meter
+    rows (column 25, the time at the step's start), and its last integrated
+    step is the one before the final step (or ``upto`` while the run goes on)."""
+
+    def __init__(self, cfg, first: int, prev: dict | None, n_fluid: int, initial_energy: float):
+        super().__init__(cfg, [], first, prev, n_fluid, initial_energy)
+        self.base_cfg = cfg
+
+    def collect(self, rows, upto: int, final: int | None = None) -> dict:  # type: ignore[override]
+        from dataclasses import replace
+        rows_t = torch.as_tensor(rows)
+        every = max(1, int(self.base_cfg.output_every))
+        self.samples = [(k, float(rows_t[k - self.first, 25])) for k in range(self.first, upto + 1)
+                        if k % every == 0 or k == final]
+        self.cfg = replace(self.base_cfg, steps=final if final is not None else upto + 1)
+        out = super().collect(rows, upto)
+        seen = rows_t[:upto - self.first + 1]
+        dev = self.dev
+        # smallest and largest step before its clamp to the target time, and the
+        # acoustic Courant peak of the steps taken (dam_break.py:394-397)
+        h = self.base_cfg.h_factor * self.base_cfg.dx
+        lo = [float(seen[:, 27].min())] if seen.shape[0] else []
+        hi = [float(seen[:, 27].max())] if seen.shape[0] else []
+        cour = [float((seen[:, 26] * (self.base_cfg.sound_speed + seen[:, 1])).max()) / h] if seen.shape[0] else []
+        out["dt_min"] = min([float(dev["dt_min"])] + lo) if "dt_min" in dev else (lo[0] if lo else self.base_cfg.dt)
+        out["dt_max"] = max([float(dev["dt_max"])] + hi) if "dt_max" in dev else (hi[0] if hi else self.base_cfg.dt)
+        out["courant"] = max([float(dev.get("courant", 0.0))] + cour)
+        out["rebuilds"] = int(dev.get("rebuilds", 0)) + (int(seen[-1, 10]) if seen.shape[0] else 0)
+        return out
+
+    def payload(self, rows, step: int, dt: float) -> dict:  # type: ignore[override]
+        """What the checkpoint after the update of ``step`` stores; ``dt`` is
+        the size next_dt gave the step after it."""
+        r = self.collect(rows, step)
+        keep = ("kinetic_energy", "potential_energy", "speed_samples", "obstacle_force", "tvc_log", "rebuilds",
+                "dt_min", "dt_max", "courant")
+        extra = {"device_run": {**{k: r[k] for k in keep}, "initial_energy": self.initial_energy}}
+        return {**r, "dt": float(dt), "extra": extra}
+
+
+def _run_3d_adaptive(cfg, obstacle, shift_every: int, seed, max_neighbors: int, snapshot_times=None, *,
+                     host=None, prev=None, checkpoint_path=None, checkpoint_every: int = 0) -> DamBreak3DRun:
     """The 3-D loop with adaptive_dt (dam_break_3d.py:617-711): meters at
-    every output_every-th step and at the final one, times from the device."""
-    from dataclasses import replace
+    every output_every-th step and at the final one, times from the device.
+
+    With checkpoints (kleefsman_obstacle_3d.py:598-640) the state after the
+    update of every step k with ``k % checkpoint_every == 0`` is written with
+    the loop's clock (the time at the start of step k + 1 and next_dt's step
+    for it); a run resumed from ``prev`` starts its engine at step
+    ``prev["step"] + 1`` with that clock and continues the series."""
+    from pathlib import Path
+    from .checkpoint import CheckpointWriter
+    host = host if host is not None else dam_break_3d_host_state(cfg, obstacle, seed)
+    first = prev["step"] + 1 if prev else 0
+    if prev:
+        host = (prev["positions"].double(), host[1], host[2], host[3])
     eng = DamBreak3DEngine(cfg, obstacle=obstacle, shift_every=shift_every, seed=seed,
-                           max_neighbors=max_neighbors, diag_ring=4 * cfg.steps + 1100,
-                           host_state=dam_break_3d_host_state(cfg, obstacle, seed))
-    final, snapshots = _advance_adaptive(eng, eng.case_id, cfg, snapshot_times=snapshot_times or [])
-    with torch.cuda.stream(eng.stream):
-        x, v, _, _ = eng.state()
-        xs, vs = x.cpu(), v.cpu()
-        diag = eng.diagnostics(0, final + 1).cpu()
-    samples = [(k, float(diag[k, 25])) for k in range(final + 1) if k % cfg.output_every == 0 or k == final]
-    # the record of a fixed-step run of ``final`` steps, with these samples
-    rec = _DeviceRecord(replace(cfg, steps=final), samples, 0, None, eng.n_fluid, eng.initial_pe).collect(diag, final)
-    dts = diag[:, 27]
+                           max_neighbors=max_neighbors, diag_ring=4 * cfg.steps + 1100, host_state=host,
+                           velocity=prev["velocity"] if prev else None, first_step=first,
+                           start_clock=(prev["elapsed"], prev["dt"]) if prev else None)
+    record = _AdaptiveRecord(cfg, first, prev, eng.n_fluid, eng.initial_pe)
+    writer = None
+    if checkpoint_path is not None and checkpoint_every > 0:
+        writer = CheckpointWriter(eng, eng.case_id, checkpoint_path, cfg, obstacle=obstacle)
+
+    def checkpoint(k):
+        elapsed, dt = eng.clock(eng.case_id)
+        writer.take(k, elapsed, first, k - first + 1, lambda rows: record.payload(rows, k, dt))
+
+    try:
+        final, snapshots = _advance_adaptive(eng, eng.case_id, cfg, snapshot_times=snapshot_times or [],
+                                             first=first, start_time=prev["elapsed"] if prev else 0.0,
+                                             checkpoint_every=checkpoint_every if writer else 0,
+                                             on_checkpoint=checkpoint if writer else None)
+        with torch.cuda.stream(eng.stream):
+            x, v, _, _ = eng.state()
+            xs, vs = x.cpu(), v.cpu()
+            diag = eng.diagnostics(first, final + 1 - first).cpu()
+        if writer is not None:
+            writer.close()
+    finally:
+        if writer is not None and writer.thread is not None:
+            writer.thread.join()
+    rec = record.collect(diag, final, final=final)
     run = DamBreak3DRun(
         times=rec["times"], front=rec["front"], kinetic_energy=rec["kinetic_energy"],
         potential_energy=rec["potential_energy"], mass=eng.initial_mass, escaped=rec["escapes"],
-        rebuilds=int(diag[final, 10]), max_speed=rec["speeds"], max_density_compression=rec["compression"],
+        rebuilds=rec["rebuilds"], max_speed=rec["speeds"], max_density_compression=rec["compression"],
         initial_mass=eng.initial_mass, final_mass=eng.initial_mass, final_positions=xs,
-        initial_energy=eng.initial_pe, steps_taken=final, simulated_time=float(diag[final, 25]),
+        initial_energy=record.initial_energy, steps_taken=final, simulated_time=float(diag[final - first, 25]),
         obstacle_force=rec["obstacle_force"], obstacle_impulse=rec["sph_impulse"],
         clamp_impulse=rec["clamp_impulse"], obstacle_clamps=rec["clamps"], tvc_log=rec["tvc_log"],
-        snapshots=snapshots, dt_min=float(dts.min()), dt_max=float(dts.max()),
-        max_acoustic_courant=_max_courant(cfg, diag))
+        snapshots=snapshots, dt_min=rec["dt_min"], dt_max=rec["dt_max"],
+        max_acoustic_courant=rec["courant"], resumed=prev is not None)
     masses = eng.spec.mass
     run.final_energy = float(0.5 * (masses[:, None] * vs.square()).sum()
                              + (masses * cfg.gravity * xs[:, 1]).sum())
     eng.close()
+    if checkpoint_path is not None:
+        # a completed run must not be resumed by the next attempt
+        try:
+            Path(checkpoint_path).unlink()
+        except FileNotFoundError:
+            pass
     return run
 
 
@@ -1090,7 +1183,8 @@ def _max_courant(cfg, diag) -> float:
     return max(float(diag[k, 26]) * (cfg.sound_speed + float(diag[k, 1])) / h for k in range(diag.shape[0]))
 
 
-def _advance_adaptive(eng, cid, cfg, chunk: int = 64, snapshot_times=None):
+def _advance_adaptive(eng, cid, cfg, chunk: int = 64, snapshot_times=None, *, first: int = 0,
+                      start_time: float = 0.0, checkpoint_every: int = 0, on_checkpoint=None):
     """Step an adaptive case until it records its final meters (the step at
     which the simulated time reaches steps * dt); returns that step, and with
     ``snapshot_times`` also the snapshots.  Steps after the final one leave
@@ -1099,9 +1193,13 @@ def _advance_adaptive(eng, cid, cfg, chunk: int = 64, snapshot_times=None):
     A snapshot target is taken at the first sample step (every
     ``output_every``-th and the final one) whose starting time reaches it, as
     dam_break.py:409-414 does: the chunks then end on the sample steps, and
-    the time at the start of step k is read from the meter row of step k-1."""
+    the time at the start of step k is read from the meter row of step k-1.
+    A run resumed at step ``first`` (its clock at ``start_time``) skips the
+    targets before that time.  With ``checkpoint_every`` the chunks also end
+    after each integrated step k with ``k % checkpoint_every == 0``, where
+    ``on_checkpoint(k)`` is called."""
     max_steps = 4 * cfg.steps + 1000
-    targets = sorted(float(t) for t in (snapshot_times or []))
+    targets = sorted(float(t) for t in (snapshot_times or []) if first == 0 or float(t) >= start_time - 1.0e-12)
     snaps, nxt = [], 0
 
     def take(t):
@@ -1113,10 +1211,15 @@ def _advance_adaptive(eng, cid, cfg, chunk: int = 64, snapshot_times=None):
             nxt += 1
 
     every = max(1, int(cfg.output_every)) if targets else chunk
-    take(0.0)
-    done = 0
+    if first % every == 0:
+        take(start_time)
+    done = first
     while done <= max_steps:
         n = min(every - done % every, max_steps + 1 - done)
+        if checkpoint_every:
+            # end the chunk after the next checkpoint step k >= done
+            k = done + (-done) % checkpoint_every
+            n = min(n, k + 1 - done)
         eng.step(n)
         done += n
         st = BatchEngine.status(eng, cid)
@@ -1126,7 +1229,9 @@ def _advance_adaptive(eng, cid, cfg, chunk: int = 64, snapshot_times=None):
                 with torch.cuda.stream(eng.stream):
                     take(float(BatchEngine.diagnostics(eng, cid, final, 1).cpu()[0, 25]))
             return (final, snaps) if snapshot_times is not None else final
-        if nxt < len(targets):
+        if checkpoint_every and (done - 1) % checkpoint_every == 0:
+            on_checkpoint(done - 1)
+        if nxt < len(targets) and done % every == 0:
             with torch.cuda.stream(eng.stream):
                 row = BatchEngine.diagnostics(eng, cid, done - 1, 1).cpu()[0]
             take(float(row[25]) + float(row[26]))

@@ -13,6 +13,8 @@ obstacle clamp impulse they carry.
   round-off (the resumed engine rebuilds its lists at the resume step, so
   its FP32 sums run in another order: positions within 1e-8 m, meters and
   impulses within 1e-6 relative).
+* The same for an adaptive-step run, whose checkpoint also carries the
+  loop's clock.
 """
 import numpy as np
 import pytest
@@ -135,5 +137,64 @@ def test_resume_continues_an_interrupted_run(gpu, tmp_path, monkeypatch):
         1e-6 * max(np.abs(full.clamp_impulse).max(), 1e-12)
     assert run.obstacle_clamps == full.obstacle_clamps and run.escaped == full.escaped
     assert run.max_density_compression == pytest.approx(full.max_density_compression, rel=1e-6)
+    assert run.initial_energy == full.initial_energy
+    assert (run.final_positions - full.final_positions).abs().max() < 1e-8
+
+
+def _adaptive_cfg(steps):
+    from dataclasses import replace
+    cfg, _ = small_case()
+    return replace(cfg, steps=steps, output_every=4, max_courant=0.25, adaptive_dt=True)
+
+
+def test_adaptive_run_checkpoints_and_resumes(gpu, tmp_path, monkeypatch):
+    """adaptive_dt with checkpoints (kleefsman_obstacle_3d.py:598-640): the
+    file keeps the loop's clock, the time at the start of the next step and
+    the step next_dt chose for it, equal to the uninterrupted run's meter
+    rows; checkpointing leaves the run bit for bit unchanged; a run resumed
+    from it takes the same number of steps to the same time, its samples
+    before the checkpoint exact and the rest to round-off."""
+    import pathlib
+    from tensorsph_b200.checkpoint import load_checkpoint
+    from tensorsph_b200.engine import DamBreak3DEngine, _advance_adaptive, run_case
+    cfg = _adaptive_cfg(20)
+    full = run_case(cfg, obstacle=OBSTACLE)
+    eng = DamBreak3DEngine(cfg, obstacle=OBSTACLE, diag_ring=4 * cfg.steps + 1100)
+    final = _advance_adaptive(eng, eng.case_id, cfg)
+    with torch.cuda.stream(eng.stream):
+        diag = eng.diagnostics(0, final + 1).cpu().numpy()
+    eng.close()
+    assert final == full.steps_taken > cfg.steps and full.dt_min < cfg.dt
+    ck = run_case(cfg, obstacle=OBSTACLE, checkpoint_path=tmp_path / "kept.pt", checkpoint_every=5)
+    assert torch.equal(ck.final_positions, full.final_positions) and ck.times == full.times
+    assert not (tmp_path / "kept.pt").exists()
+
+    path = tmp_path / "state.pt"
+    # the first attempt ends at 12 dt and keeps its last checkpoint (after
+    # the update of step 10), as a process that died would
+    with monkeypatch.context() as m:
+        m.setattr(pathlib.Path, "unlink", lambda self, missing_ok=False: None)
+        run_case(_adaptive_cfg(12), obstacle=OBSTACLE, checkpoint_path=path, checkpoint_every=5)
+    state = load_checkpoint(path, cfg, OBSTACLE)
+    assert state["step"] == 10
+    assert state["elapsed"] == diag[11, 25] and state["dt"] == diag[11, 27]
+    assert state["times"] == full.times[:3] and state["front"] == full.front[:3]
+    run = run_case(cfg, obstacle=OBSTACLE, checkpoint_path=path, checkpoint_every=5)
+    assert run.resumed and not path.exists()
+    assert run.steps_taken == full.steps_taken
+    assert run.simulated_time == pytest.approx(full.simulated_time, rel=1e-12)
+    assert run.times[:3] == full.times[:3]
+    np.testing.assert_allclose(run.times, full.times, rtol=1e-9)
+    np.testing.assert_allclose(run.front, full.front, rtol=1e-9)
+    np.testing.assert_allclose(run.kinetic_energy, full.kinetic_energy, rtol=1e-6)
+    assert len(run.obstacle_force) == len(full.obstacle_force) == final
+    np.testing.assert_allclose(run.obstacle_force[:11], full.obstacle_force[:11], rtol=1e-12, atol=1e-12)
+    f = np.abs(np.array(full.obstacle_force)).max()
+    assert np.abs(np.array(run.obstacle_force) - np.array(full.obstacle_force)).max() <= 1e-6 * f
+    assert np.abs(np.array(run.obstacle_impulse) - np.array(full.obstacle_impulse)).max() <= \
+        1e-6 * np.abs(full.obstacle_impulse).max()
+    assert run.dt_min == pytest.approx(full.dt_min, rel=1e-6) and run.dt_max == full.dt_max
+    assert run.max_acoustic_courant == pytest.approx(full.max_acoustic_courant, rel=1e-6)
+    assert run.obstacle_clamps == full.obstacle_clamps and run.escaped == full.escaped
     assert run.initial_energy == full.initial_energy
     assert (run.final_positions - full.final_positions).abs().max() < 1e-8
