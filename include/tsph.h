@@ -604,6 +604,24 @@ typedef struct {
    * first_step and the step size next_dt gave it (<= 0: dt)                */
   double start_elapsed;
   double start_dt;
+  /* 2-D compression regularisation (droplet_impact.py:982-1028 with
+   * compression_regularization.py:96-187): the density is rule(S) rho0 with
+   * S = W(0) m_a / rho0 + Kref sum_b W_ab m_b / rho0; rule 0 "internal" (S),
+   * 1 "free_surface" (max(S, 1)); normalization 1 "reference_mean" (Kref the
+   * case's 1 / mean{S > 1} of the step before, 1 at admission), 0 "none"
+   * (Kref = 1).  Excludes density diffusion and renormalisation.            */
+  int64_t compression;
+  int64_t compression_rule;
+  int64_t compression_normalization;
+  /* free-surface pressure closure (droplet_impact.py:429-492, in rhs and
+   * rhs_3d): a fluid particle with rho < surface_threshold rho0 takes
+   * max(0, sum_b (p_b - g (y_a - y_b) rho_b) W_ab / sum_b W_ab) over its fluid
+   * neighbours; donors 0 the known ones ("interior", surface_layers Jacobi
+   * passes), 1 all ("all", one pass)                                        */
+  int64_t surface_closure;
+  double surface_threshold;
+  int64_t surface_donors;
+  int64_t surface_layers;
 } tsph_case_params;
 
 typedef struct tsph_engine tsph_engine; /* opaque host handle */
@@ -652,14 +670,16 @@ int tsph_engine_graph_kernels(tsph_engine* engine, int64_t* kernels);
  * FP64 (device, nullable). */
 int tsph_engine_read(tsph_engine* engine, int64_t case_id, double* x, double* v, double* rho,
                      double* p, tsph_stream stream);
-/* Copy `count` per-step meter rows of one case (28 doubles each: max rho,
+/* Copy `count` per-step meter rows of one case (30 doubles each: max rho,
  * max |v|, front x, obstacle force xyz, kinetic and potential energy,
  * escapes, clamps, rebuilds, longest row, step, status, obstacle impulse x,
  * c_ref, the step's transport-velocity correction: max |shift|,
  * sum |shift|, kept and clipped counts, obstacle impulse y and z, and the
  * obstacle clamp impulse xyz; both impulses through the step's update and
  * counted from the case's admission; the time at the step's start, the step
- * taken and the step before its clamp to the target time) starting at its
+ * taken and the step before its clamp to the target time; with the
+ * compression regularisation the step's 1 / mean{S > 1} and the number of
+ * particles with S > 1, else 0 and 0) starting at its
  * step `first` into `out` (device).  Row k of a ring of R rows is step k mod R. */
 int tsph_engine_diag(tsph_engine* engine, int64_t case_id, double* out, int64_t first,
                      int64_t count, tsph_stream stream);

@@ -173,7 +173,10 @@ class CaseParams(ctypes.Structure):
                 ("diffusion_form", c_int64), ("diffusion_eigen_floor", c_double),
                 ("density_renormalization", c_int64), ("lattice_kernel_sum", c_double),
                 ("boundary_consistent_density", c_int64),
-                ("start_elapsed", c_double), ("start_dt", c_double)]
+                ("start_elapsed", c_double), ("start_dt", c_double),
+                ("compression", c_int64), ("compression_rule", c_int64),
+                ("compression_normalization", c_int64), ("surface_closure", c_int64),
+                ("surface_threshold", c_double), ("surface_donors", c_int64), ("surface_layers", c_int64)]
 
 
 _SIGNATURES = {

@@ -47,7 +47,7 @@ namespace {
 
 constexpr int kBlock = 128;     // default threads per block of the pair kernels
 constexpr int kMaxBlock = 256;  // largest block the kernels are built for
-constexpr int kDiag = 28;
+constexpr int kDiag = 30;
 constexpr int kBatch = 4;
 constexpr int kCodeBits = 6;                               // cell-offset code bits of a row entry
 constexpr uint32_t kCodeMask = (1u << kCodeBits) - 1;
@@ -101,6 +101,13 @@ struct CaseDev {
   int renorm;              // Shepard renormalisation of the summation density
   float lattice_sum;       // its full-support kernel sum
   int bcd;                 // boundary-consistent density (a second wall pass)
+  int comp;                // compression regularisation (the density is rule(S) rho0)
+  int comp_fs;             // its rule: 1 "free_surface" max(S, 1), 0 "internal" S
+  int comp_norm;           // its normalisation: 1 "reference_mean", 0 "none" (Kref = 1)
+  int closure;             // free-surface pressure closure
+  int closure_all;         // its donors: 1 every fluid neighbour ("all"), 0 the known ones
+  int closure_passes;      // its Jacobi passes
+  float closure_thr;       // receivers: rho < closure_thr (threshold x rho0)
 };
 
 struct CaseCtl {
@@ -130,6 +137,9 @@ struct CaseCtl {
   double dt_int;        // this step's integration dt (0 on the final and after it)
   int finished;         // adaptive: the target time is reached (later steps are frozen)
   int final_step;       // adaptive: the step that recorded the final meters
+  double kref;          // compression: the inverse reference compression this step uses
+  double comp_written;  // compression: 1 / mean{S > 1} of this step (the next step's kref)
+  unsigned long long comp_counted;  // compression: particles with S > 1 this step
 };
 
 struct Dev {
@@ -174,6 +184,10 @@ struct Dev {
   int has_csf, maxfit;
   int has_psi;            // some case uses the psi diffusion form (one more gather)
   int has_bcd;            // some case uses the boundary-consistent density
+  int has_comp;           // some case uses the compression regularisation
+  int closure_passes;     // most passes of the pressure closure over the cases (0: none)
+  float* pbuf;            // closure: the other pressure buffer of its Jacobi passes
+  uint8_t* known;         // closure: [2][NF] known-pressure flags of the passes
   int has_tvc, tvc_late;  // tvc_late: the correction runs after the second list pass
   int csf_kinds;          // CSF options present in the batch: fits 1 quadratic, 2 circle,
                           // 16 quadratic + local_range, 32 circle + local_range; 4 local_range,
@@ -693,10 +707,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_density(const __grid_constant__ D
     const float4 la = e.lp[a];
     const float2 ncell = f2(-cellf), inv_h2 = f2(inv_h), sigma2 = f2(sigma);
     // the deviation rho - rho0, summed with compensation from -rho0
-    CSum<float> s, kt;
+    CSum<float> s, kt, nb;
     s.add(-C.rho0);
     s.add(la.w * sigma);
-    const bool renorm = C.renorm != 0;
+    const bool renorm = C.renorm != 0, comp = C.comp != 0;
     walk_row<KB>(e, a, [&](const uint32_t* ent) {
       float2 part = f2(0.f), wsum = f2(0.f);
 #pragma unroll
@@ -713,9 +727,20 @@ __global__ void __launch_bounds__(kMaxBlock) k_density(const __grid_constant__ D
       }
       s.add(part.x + part.y);
       if (renorm) kt.add(wsum.x + wsum.y);
+      if (comp) nb.add(part.x + part.y);
     });
     const float dfloor = floor_ - C.rho0;
     float d = s.value();
+    if (comp) {
+      // the compression regularisation (droplet_impact.py:1007-1028):
+      // rho0 (S - 1) = (m_a W(0) - rho0) + Kref sum_b m_b W_ab, with Kref the
+      // inverse reference compression the case carries from the step before;
+      // the raw value feeds this step's average, the rule gives the density
+      const float kref_m1 = static_cast<float>(e.ctl[kOne ? e.one_slot : e.cid[a]].kref - 1.0);
+      d = d + kref_m1 * nb.value();
+      e.dlt[a] = d;
+      if (C.comp_fs) d = d > 0.f ? d : 0.f;
+    }
     d = d > dfloor ? d : dfloor;
     if (renorm) {
       // rho S / T - rho0 = d S / T + rho0 (S - T) / T, T = W(0) + sum_b W_ab
@@ -731,6 +756,118 @@ __global__ void __launch_bounds__(kMaxBlock) k_density(const __grid_constant__ D
       d = d > dfloor ? d : dfloor;
     }
     e.rs[a] = make_float2(d, la.w / (C.rho0 + d));
+  }
+}
+
+// E1c (cases with the compression regularisation): AverageCompression
+// (compression_regularization.py:140-160), 1 / mean{S > 1} over the case's
+// fluid, 1 when no particle has S > 1.  One block per case reads its rows in
+// a fixed order, so the value does not depend on the rest of the batch.  It
+// is written after this step's density used the previous one, as the
+// reference's dynamics list does; with "reference_mean" the next step uses it.
+__global__ void __launch_bounds__(1024) k_compression_average(Dev e) {
+  __shared__ double part[32];
+  __shared__ unsigned long long cnt[32];
+  const int c = blockIdx.x;
+  CaseCtl& t = e.ctl[c];
+  if (!t.active) return;
+  const CaseDev& C = e.cases[c];
+  if (!C.comp) return;
+  const double inv_rho0 = 1.0 / static_cast<double>(C.rho0);
+  double sum = 0.0;  // sum of S - 1 over S > 1
+  unsigned long long n = 0;
+  for (int i = threadIdx.x; i < C.n_fluid; i += blockDim.x) {
+    const float v = e.dlt[C.fluid_begin + i];
+    if (v > 0.f) {
+      sum += static_cast<double>(v) * inv_rho0;
+      ++n;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    sum += __shfl_down_sync(0xffffffffu, sum, o);
+    n += __shfl_down_sync(0xffffffffu, n, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    part[threadIdx.x >> 5] = sum;
+    cnt[threadIdx.x >> 5] = n;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double total = 0.0;
+    unsigned long long count = 0;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) {
+      total += part[w];
+      count += cnt[w];
+    }
+    total += static_cast<double>(count);  // sum of S over S > 1
+    const bool ok = count > 0 && total > 0.0;
+    t.comp_written = ok ? static_cast<double>(count) / total : 1.0;
+    t.comp_counted = ok ? count : 0;
+    t.kref = C.comp_norm ? t.comp_written : 1.0;
+  }
+}
+
+// E2b (cases with the free-surface pressure closure, droplet_impact.py:429-492):
+// receivers rho < threshold rho0 take max(0, sum_b (p_b - g (y_a - y_b) rho_b)
+// W_ab / sum_b W_ab) over their fluid neighbours, the donors the particles
+// whose pressure is known ("interior", one Jacobi pass per layer, ping-ponged
+// between pr and pbuf) or all of them ("all", one pass); a receiver without a
+// donor keeps its pressure.  Rows of other cases (and of a case whose passes
+// are done) copy through.
+__global__ void k_closure_init(Dev e) {
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    const CaseDev& C = e.cases[e.cid[a]];
+    e.known[a] = (C.closure && e.rho[a] < C.closure_thr) ? 0 : 1;
+  }
+}
+
+template <bool kOne>
+__global__ void __launch_bounds__(kMaxBlock) k_closure_pass(const __grid_constant__ Dev e, int pass,
+                                                            const float* __restrict__ p_in,
+                                                            const uint8_t* __restrict__ known_in,
+                                                            float* __restrict__ p_out, uint8_t* __restrict__ known_out) {
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    const CaseDev& C = case_of<kOne>(e, a);
+    if (known_in[a] || pass >= C.closure_passes) {
+      p_out[a] = p_in[a];
+      known_out[a] = known_in[a];
+      continue;
+    }
+    const float4 la = e.lp[a];
+    const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, g = C.grav;
+    const int NF = e.NF, n = e.cnt[a];
+    const bool all = C.closure_all != 0;
+    CSum<float> num, den;
+    for (int k = 0; k < n; ++k) {
+      const uint32_t ent = ld_entry(e.nbr + a + static_cast<int64_t>(k) * e.rows);
+      const int b = static_cast<int>(ent >> kCodeBits);
+      if (b >= NF || !(all || known_in[b])) continue;
+      const float4 lb = e.lp[b];
+      const float3 d = sep(la, lb, ent, cellf);
+      const float r2 = fmaf(d.z, d.z, fmaf(d.y, d.y, d.x * d.x));
+      const float W = sigma * shape(radial(r2, inv_h).q);
+      num.add(W * (p_in[b] - g * d.y * e.rho[b]));
+      den.add(W);
+    }
+    const float dn = den.value();
+    if (dn > 1.0e-30f) {
+      const float v = num.value() / dn;
+      p_out[a] = v > 0.f ? v : 0.f;
+      known_out[a] = 1;
+    } else {
+      p_out[a] = p_in[a];
+      known_out[a] = 0;
+    }
+  }
+}
+
+// The closed pressure into pr and p / rho^2 of the closure cases.
+__global__ void k_closure_finish(Dev e, const float* __restrict__ p_final) {
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
+    if (!e.cases[e.cid[a]].closure) continue;
+    const float p = p_final[a], r = e.rho[a];
+    e.pr[a] = p;
+    e.pq[a] = p / (r * r);
   }
 }
 
@@ -1933,6 +2070,8 @@ __global__ void k_finalize(Dev e) {
   row[25] = t.elapsed;
   row[26] = t.dt_step;
   row[27] = C.adaptive ? t.dt_now : C.dt;
+  row[28] = C.comp ? t.comp_written : 0.0;
+  row[29] = C.comp ? static_cast<double>(t.comp_counted) : 0.0;
   t.elapsed += t.dt_int;
   if (C.adaptive && t.dt_int > 0.0) {
     // next_dt (droplet_impact.py:522-556) with the speed at the step's start
@@ -2461,6 +2600,8 @@ size_t carve(const tsph_engine_params& p, Dev* d, char* base, CaseDev** cases, c
   t.rs = static_cast<float2*>(take((N + 1) * sizeof(float2)));
   t.gg = static_cast<float4*>(take((N + 1) * sizeof(float4)));
   t.dlt = static_cast<float*>(take(NF * sizeof(float)));
+  t.pbuf = static_cast<float*>(take(NF * sizeof(float)));
+  t.known = static_cast<uint8_t*>(take(2 * NF * sizeof(uint8_t)));
   t.acc = static_cast<float4*>(take(NF * sizeof(float4)));
   t.conc = static_cast<float*>(take((N + 1) * sizeof(float)));
   t.gradc = static_cast<float4*>(take(NF * sizeof(float4)));
@@ -2540,12 +2681,16 @@ void batch_changed(tsph_engine* E) {
   d.has_tvc = 0;
   d.has_psi = 0;
   d.has_bcd = 0;
+  d.has_comp = 0;
+  d.closure_passes = 0;
   d.csf_kinds = 0;
   d.tvc_late = second_pass(E) && E->order[0].dev.tvc_bulk ? 1 : 0;
   for (const CaseHost& c : E->order) {
     d.has_csf |= c.dev.csf;
     d.has_psi |= c.dev.psi;
     d.has_bcd |= c.dev.bcd;
+    d.has_comp |= c.dev.comp;
+    if (c.dev.closure) d.closure_passes = std::max(d.closure_passes, c.dev.closure_passes);
     if (c.dev.csf)
       d.csf_kinds |= (c.dev.csf_fit ? (c.dev.csf_fit == 1 ? 1 : 2) << (c.dev.csf_range ? 4 : 0) : 0) |
                      (c.dev.csf_range ? 4 : 0) | (c.dev.csf_contact >= 2 ? 8 : 0);
@@ -2659,9 +2804,20 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr, b
   const bool deep = E->batch == 8;
 #define TSPH_PICK(K) (one ? (deep ? K<true, 8> : K<true, 4>) : (deep ? K<false, 8> : K<false, 4>))
   TSPH_PICK(k_density)<<<g, B, 0, s>>>(d);
+  if (d.has_comp) k_compression_average<<<d.n_slots, 1024, 0, s>>>(d);
   if (d.has_psi) TSPH_PICK(k_density_gradient)<<<g, B, 0, s>>>(d);
   mark();
   TSPH_PICK(k_diffusion_eos)<<<g, B, 0, s>>>(d);
+  if (d.closure_passes > 0) {
+    k_closure_init<<<g, B, 0, s>>>(d);
+    float* pres[2] = {d.pr, d.pbuf};
+    uint8_t* known[2] = {d.known, d.known + d.NF};
+    for (int k = 0; k < d.closure_passes; ++k)
+      (one ? k_closure_pass<true> : k_closure_pass<false>)<<<g, B, 0, s>>>(d, k, pres[k & 1], known[k & 1],
+                                                                           pres[(k + 1) & 1], known[(k + 1) & 1]);
+    k_closure_finish<<<g, B, 0, s>>>(d, pres[d.closure_passes & 1]);
+    TSPH_LAUNCH_CHECK();
+  }
   mark();
   if (d.nw) TSPH_PICK(k_walls)<<<grid_for(d.nw, B), B, 0, s>>>(d);
   if (d.has_bcd && d.nw) {
@@ -2805,6 +2961,13 @@ CaseDev make_case_dev(const tsph_case_params& p, int64_t* ncells) {
   c.renorm = p.density_renormalization ? 1 : 0;
   c.lattice_sum = static_cast<float>(p.lattice_kernel_sum);
   c.bcd = p.boundary_consistent_density && p.n_wall > 0 ? 1 : 0;
+  c.comp = p.compression && p.dim == 2 ? 1 : 0;
+  c.comp_fs = p.compression_rule == 1 ? 1 : 0;
+  c.comp_norm = p.compression_normalization == 1 ? 1 : 0;
+  c.closure = p.surface_closure ? 1 : 0;
+  c.closure_all = p.surface_donors == 1 ? 1 : 0;
+  c.closure_passes = c.closure ? (c.closure_all ? 1 : static_cast<int>(std::max<int64_t>(1, p.surface_layers))) : 0;
+  c.closure_thr = static_cast<float>(p.surface_threshold * p.rho0);
   c.dtf = static_cast<float>(p.dt);
   c.visc_eps = static_cast<float>(0.01 * p.h * p.h);
   c.rho_floor = static_cast<float>(0.1 * p.rho0);
@@ -2860,6 +3023,14 @@ bool case_params_ok(const tsph_case_params* p) {
       !std::isfinite(p->csf_contact_angle) ||
       (p->csf_contact_model == 1 && !(p->csf_contact_reach > 0.0 && p->csf_contact_reach <= 2.0)) ||
       (p->csf_contact_model >= 2 && !(p->csf_wall_area > 0.0 && std::isfinite(p->csf_traction_calibration))))
+    return false;
+  if (p->compression && (p->dim != 2 || p->compression_rule < 0 || p->compression_rule > 1 ||
+                         p->compression_normalization < 0 || p->compression_normalization > 1 ||
+                         p->density_renormalization || p->diffusion_scale > 0.0 ||
+                         p->boundary_consistent_density))
+    return false;
+  if (p->surface_closure && (!std::isfinite(p->surface_threshold) || p->surface_donors < 0 ||
+                             p->surface_donors > 1 || p->surface_layers < 1 || p->surface_layers > 64))
     return false;
   if (!(p->h > 0) || !(p->dt > 0) || !(p->skin >= 0) || !(p->rho0 > 0) || !(p->gamma > 0) ||
       !(p->sound_speed > 0))
@@ -3010,6 +3181,8 @@ int tsph_engine_add_case(tsph_engine* E, const tsph_case_params* p, const double
     if (p->start_dt > 0.0) ctl.dt_now = p->start_dt;
   }
   ctl.dt_step = ctl.dt_int = ctl.dt_now;
+  ctl.kref = 1.0;  // sv_compression_inv_ref_ starts at 1
+  ctl.comp_written = 1.0;
   TSPH_CUDA_CHECK(cudaMemcpyAsync(d.ctl + slot, &ctl, sizeof(CaseCtl), cudaMemcpyHostToDevice, s));
   TSPH_CUDA_CHECK(cudaMemsetAsync(d.diag + static_cast<int64_t>(slot) * d.diag_ring * kDiag, 0,
                                   static_cast<size_t>(d.diag_ring) * kDiag * sizeof(double), s));

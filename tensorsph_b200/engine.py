@@ -41,7 +41,8 @@ DIAG_FIELDS = ("rho_max", "speed_max", "front", "force_x", "force_y", "force_z",
                "potential", "escapes", "clamps", "rebuilds", "row_max", "step", "status",
                "impulse_x", "c_reference", "tvc_max_shift", "tvc_shift_sum", "tvc_kept",
                "tvc_clipped", "impulse_y", "impulse_z", "clamp_impulse_x", "clamp_impulse_y",
-               "clamp_impulse_z", "time", "dt", "dt_unclamped")
+               "clamp_impulse_z", "time", "dt", "dt_unclamped", "compression_inverse",
+               "compression_counted")
 
 
 def obstacle_lattice_3d(lo, hi, dx: float) -> torch.Tensor:
@@ -153,9 +154,32 @@ def _case_params(*, dim, n_fluid, n_wall, n_obstacle, cfg, h, wall_mass, box_hi,
     if dim == 3 and (cfg.density_renormalization or cfg.boundary_consistent_density):
         raise NotImplementedError("density_renormalization and boundary_consistent_density are "
                                   "options of the 2-D rhs")
-    if getattr(cfg, "density_regularization", "none") != "none" or getattr(cfg, "surface_pressure_closure", False):
-        raise NotImplementedError("density_regularization and surface_pressure_closure are options of the "
-                                  "rhs drop-ins, not of the device engine")
+    reg = getattr(cfg, "density_regularization", "none")
+    compression = dim == 2 and reg != "none"
+    if compression:
+        # the rhs's contract (droplet_impact.py:982-1006); rhs_3d has no regularisation
+        from .compression_regularization import NORMALIZATIONS, RULES
+        if reg != "compression":
+            raise ValueError(f"unknown density_regularization {reg!r}; expected 'none' or 'compression'")
+        if cfg.density_renormalization:
+            raise ValueError("density_regularization='compression' replaces the summation density; "
+                             "combining it with density_renormalization would normalise an "
+                             "already-normalised field")
+        if cfg.compression_regularization_rule not in RULES:
+            raise ValueError(f"unknown compression_regularization_rule "
+                             f"{cfg.compression_regularization_rule!r}; expected one of {RULES}")
+        if cfg.compression_normalization not in NORMALIZATIONS:
+            raise ValueError(f"unknown compression_normalization {cfg.compression_normalization!r}; "
+                             f"expected one of {NORMALIZATIONS}")
+        if cfg.density_diffusion > 0.0:
+            raise ValueError("density_regularization='compression' and density_diffusion are two "
+                             "different ways of obtaining the density; pick one")
+        if cfg.compression_regularization_rule == "free_stream":
+            # compression_regularization.py:164-184: the loop passes no indicator
+            raise ValueError("rule 'free_stream' needs an indicator array")
+        if cfg.boundary_consistent_density:
+            raise ValueError("boundary_consistent_density cannot be combined with "
+                             "density_regularization != 'none'")
     p = _lib.CaseParams()
     p.dim, p.n_fluid, p.n_wall, p.n_obstacle = dim, n_fluid, n_wall, n_obstacle
     p.shift_every = int(shift_every)
@@ -177,6 +201,16 @@ def _case_params(*, dim, n_fluid, n_wall, n_obstacle, cfg, h, wall_mass, box_hi,
         p.density_renormalization = 1
         p.lattice_kernel_sum = float(lattice_kernel_sum(h, cfg.dx))
     p.boundary_consistent_density = 1 if cfg.boundary_consistent_density else 0
+    if compression:
+        p.compression = 1
+        p.compression_rule = 1 if cfg.compression_regularization_rule == "free_surface" else 0
+        p.compression_normalization = 1 if cfg.compression_normalization == "reference_mean" else 0
+    if getattr(cfg, "surface_pressure_closure", False):
+        # droplet_impact.py:429-492 (rhs) and dam_break_3d.py:339-342 (rhs_3d)
+        p.surface_closure = 1
+        p.surface_threshold = float(cfg.surface_pressure_threshold)
+        p.surface_donors = 1 if cfg.surface_pressure_donors == "all" else 0
+        p.surface_layers = max(1, int(cfg.surface_pressure_layers))
     for k in range(3):
         p.box_hi[k] = box_hi[k]
     p.tolerance = 0.25 * cfg.dx

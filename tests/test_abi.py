@@ -88,7 +88,7 @@ def test_struct_sizes_match_header():
     assert ctypes.sizeof(_lib.ShiftParams) == 8 * 9
     assert ctypes.sizeof(_lib.ClampParams) == 8 * (3 + 3 + 3 + 1 + 1 + 3 + 3 + 1)
     assert ctypes.sizeof(_lib.EngineParams) == 8 * 8
-    assert ctypes.sizeof(_lib.CaseParams) == 8 * (6 + 11 + 3 + 1 + 3 + 3 + 1 + 4 + 3 + 3 + 2 + 4 + 1 + 3 + 2 + 5 + 6 + 2 + 2 + 3 + 2)
+    assert ctypes.sizeof(_lib.CaseParams) == 8 * (6 + 11 + 3 + 1 + 3 + 3 + 1 + 4 + 3 + 3 + 2 + 4 + 1 + 3 + 2 + 5 + 6 + 2 + 2 + 3 + 2 + 7)
     assert ctypes.sizeof(_lib.Csf3Params) == 8 * (3 + 3 + 4 + 1)
     assert ctypes.sizeof(_lib.Csf3IO) == 8 * 11
     assert ctypes.sizeof(_lib.TvcParams) == 8 * (8 + 8)

@@ -105,17 +105,31 @@ def test_step_limits_match_reference(golden):
     assert np.array_equal(np.asarray(rows), g)
 
 
-def test_engine_refuses_rhs_only_options():
-    """The compression regularisation and the free-surface closure are
-    options of the rhs drop-ins: a device case built with either is refused,
-    not run without it."""
+def test_engine_compression_and_closure_options():
+    """The compression regularisation (2-D, droplet_impact.py:982-1028) and
+    the free-surface closure (droplet_impact.py:429-492) become case
+    parameters; the combinations the rhs refuses raise its ValueErrors, and
+    3-D cases ignore the regularisation as rhs_3d does."""
     from tensorsph_b200.engine import dam_break_2d_case, droplet_impact_case
-    with pytest.raises(NotImplementedError):
-        dam_break_2d_case(_dam2d(surface_pressure_closure=True))
-    with pytest.raises(NotImplementedError):
-        dam_break_2d_case(_dam2d(density_regularization="compression"))
-    with pytest.raises(NotImplementedError):
-        droplet_impact_case(_drop(surface_pressure_closure=True))
+    p = dam_break_2d_case(_dam2d(density_diffusion=0.0, density_regularization="compression")).params
+    assert (p.compression, p.compression_rule, p.compression_normalization) == (1, 1, 1)
+    p = dam_break_2d_case(_dam2d(density_diffusion=0.0, density_regularization="compression",
+                                 compression_regularization_rule="internal",
+                                 compression_normalization="none")).params
+    assert (p.compression, p.compression_rule, p.compression_normalization) == (1, 0, 0)
+    p = dam_break_2d_case(_dam2d(surface_pressure_closure=True, surface_pressure_donors="all",
+                                 surface_pressure_threshold=0.98)).params
+    assert (p.surface_closure, p.surface_donors, p.surface_threshold) == (1, 1, 0.98)
+    p = droplet_impact_case(_drop(surface_pressure_closure=True, surface_pressure_layers=4)).params
+    assert (p.surface_closure, p.surface_donors, p.surface_layers) == (1, 0, 4)
+    for bad, msg in ((dict(density_diffusion=0.1, density_regularization="compression"), "pick one"),
+                     (dict(density_diffusion=0.0, density_regularization="compression",
+                           density_renormalization=True), "already-normalised"),
+                     (dict(density_diffusion=0.0, density_regularization="compression",
+                           compression_regularization_rule="free_stream"), "indicator"),
+                     (dict(density_diffusion=0.0, density_regularization="volume"), "unknown")):
+        with pytest.raises(ValueError, match=msg):
+            dam_break_2d_case(_dam2d(**bad))
 
 
 def test_dam_break_2d_shift_reference_speed_and_refusals():

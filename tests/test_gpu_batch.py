@@ -43,16 +43,24 @@ def small_3d(dx=0.02, obstacle=True):
     return cfg, ob
 
 
-def oracle_2d_steps(cfg, x, mass, wall, steps):
+def oracle_2d_steps(cfg, x, mass, wall, steps, ledger=None):
+    """``steps`` FP64 oracle steps; with ``ledger`` (a list) each step's
+    compression state (inverse reference written, particles counted) is
+    appended to it."""
     x = x.copy()
     v = np.zeros_like(x)
     out = []
     box = np.array([cfg.pool_width, cfg.tank_top()])
     tol = 0.25 * cfg.dx
+    state = {}
     for _ in range(steps):
         h = cfg.h_factor * cfg.dx
         pairs = cell_linked_pairs(np.concatenate((x, wall)), 2.0 * h)
-        rho, p, acc = op.rhs(x, v, mass, cfg, pairs=pairs, wall=wall, dt=cfg.dt)
+        # the loop's pair cache holds no wall-wall pairs (fluid_count, dam_break.py:335)
+        pairs = pairs[pairs[:, 0] < x.shape[0]]
+        rho, p, acc = op.rhs(x, v, mass, cfg, pairs=pairs, wall=wall, dt=cfg.dt, state=state)
+        if ledger is not None:
+            ledger.append((state.get("inverse_reference"), state.get("counted")))
         out.append((rho, p, acc))
         v = v + cfg.dt * acc
         x = x + cfg.dt * v
@@ -70,7 +78,13 @@ def engine_for(specs, **kw):
 OPTION_SETS = [dict(), dict(density_diffusion_form="antuono"), dict(density_renormalization=True),
                dict(boundary_consistent_density=True),
                dict(density_diffusion_form="antuono", boundary_consistent_density=True,
-                    density_diffusion_eigenvalue_floor=0.2)]
+                    density_diffusion_eigenvalue_floor=0.2),
+               dict(density_diffusion=0.0, density_regularization="compression"),
+               dict(density_diffusion=0.0, density_regularization="compression",
+                    compression_regularization_rule="internal", compression_normalization="none"),
+               dict(surface_pressure_closure=True),
+               dict(surface_pressure_closure=True, surface_pressure_donors="all", surface_pressure_threshold=0.995),
+               dict(surface_pressure_closure=True, surface_pressure_layers=3, density_diffusion_form="antuono")]
 
 
 @pytest.mark.parametrize("opts", OPTION_SETS)
@@ -78,7 +92,9 @@ def test_2d_case_matches_fp64_oracle(opts, gpu):
     """The 2-D dam break in the engine against the FP64 oracle's rhs + Euler
     + clamps, for the rhs options the engine runs: Molteni diffusion, the
     psi form with the renormalised density gradient, the Shepard density
-    renormalisation and the boundary-consistent density."""
+    renormalisation, the boundary-consistent density, the compression
+    regularisation (its carried 1 / mean{S > 1} and count against the
+    oracle's state after every step) and the free-surface pressure closure."""
     from dataclasses import replace
     from tensorsph_b200.engine import dam_break_2d_case
     cfg = replace(small_2d(), **opts)
@@ -87,7 +103,8 @@ def test_2d_case_matches_fp64_oracle(opts, gpu):
     cid = eng.add(spec)
     steps = 6
     x, m, w = spec.x.numpy(), spec.mass.numpy(), spec.wall.numpy()
-    ref, xr, vr = oracle_2d_steps(cfg, x, m, w, steps)
+    ledger = []
+    ref, xr, vr = oracle_2d_steps(cfg, x, m, w, steps, ledger)
     eng.step(1)
     ex, ev, erho, ep = [t.cpu().numpy() for t in eng.read(cid)]
     bulk = cfg.rho0 * cfg.sound_speed ** 2 / cfg.gamma
@@ -103,6 +120,16 @@ def test_2d_case_matches_fp64_oracle(opts, gpu):
     diag = eng.diagnostics(cid, 0, steps).cpu().numpy()
     for k in range(steps):
         assert diag[k, 0] == pytest.approx(ref[k][0].max(), rel=2e-6)
+        if cfg.density_regularization == "compression":
+            written, counted = ledger[k]
+            assert diag[k, 28] == pytest.approx(written, rel=1e-6)
+            assert abs(diag[k, 29] - counted) <= max(2, 0.01 * counted)
+        else:
+            assert diag[k, 28] == diag[k, 29] == 0.0
+    if cfg.surface_pressure_closure:
+        # the closure acted: surface particles below the threshold hold more
+        # than their Tait pressure
+        assert (ref[0][0] < cfg.surface_pressure_threshold * cfg.rho0).any()
     st = eng.status(cid)
     assert st["steps"] == steps and st["status"] == 0 and st["escapes"] == 0
     eng.close()

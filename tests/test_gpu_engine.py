@@ -63,9 +63,15 @@ def oracle_steps(cfg, obstacle, x, mass, wall, n_ob, steps):
     return out, x, v
 
 
-def test_engine_matches_fp64_oracle(gpu):
+@pytest.mark.parametrize("opts", [dict(), dict(surface_pressure_closure=True, surface_pressure_layers=3)])
+def test_engine_matches_fp64_oracle(opts, gpu):
+    """The 3-D obstacle case against the FP64 oracle (rhs_3d, Euler, box and
+    obstacle clamps), with and without rhs_3d's free-surface pressure closure
+    (dam_break_3d.py:339-342)."""
+    from dataclasses import replace
     from tensorsph_b200.engine import DamBreak3DEngine
     cfg, obstacle = small_case()
+    cfg = replace(cfg, **opts)
     x, mass, wall, n_ob = DamBreak3DEngine.build_host_state(cfg, obstacle)
     eng = DamBreak3DEngine(cfg, obstacle=obstacle, host_state=(x, mass, wall, n_ob), diag_ring=64)
     steps = 8
