@@ -81,6 +81,9 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=48)
     ap.add_argument("--serve-time-scale", type=float, default=0.05)
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
+    ap.add_argument("--serve-tight-gb", type=float, default=4.0,
+                    help="a second served run under this HBM budget, small enough that admissions "
+                         "wait for retirements (0: none)")
     ap.add_argument("--dplus-dx", type=float, default=0.0138,
                     help="lattice spacing of the 3-D delta-plus leg (0: no leg)")
     ap.add_argument("--dplus-steps", type=int, default=20)
@@ -681,6 +684,21 @@ def rhs2d_leg(args, dev):
         spairs = spairs[(spairs[:, 0] < sp.shape[0]) | (spairs[:, 1] < sp.shape[0])]
         op.rhs(sp, np.zeros_like(sp), smass.numpy(), scfg, pairs=spairs, wall=sw, dt=scfg.dt)
         t_cpu = time.perf_counter() - t0
+        # the timed path (FP32) on the oracle's column against the FP64 oracle
+        d_rho, d_p, d_acc = (t.double().cpu().numpy() for t in rhs(
+            spos.to(dev), torch.zeros_like(spos).to(dev), smass.to(dev), scfg,
+            pairs=torch.from_numpy(spairs).to(dev), wall=swall.to(dev), dt=scfg.dt))
+        f64 = np.float64
+        o_rho, o_p, o_acc = op.rhs(sp.astype(f64), np.zeros(sp.shape, f64), smass.numpy().astype(f64), scfg,
+                                   pairs=spairs, wall=sw.astype(f64), dt=scfg.dt)
+        bulk = scfg.rho0 * scfg.sound_speed ** 2 / scfg.gamma
+        at = int(np.argmax(o_rho))
+        errors = {"rho_over_rho0": float(np.abs(d_rho - o_rho).max() / scfg.rho0),
+                  "p_over_B": float(np.abs(d_p - o_p).max() / bulk),
+                  "acc_over_max_acc": float(np.abs(d_acc - o_acc).max() / np.abs(o_acc).max()),
+                  "oracle_rho_max_over_rho0": float(o_rho[at] / scfg.rho0),
+                  "oracle_rho_max_at": [float(v) for v in sp[at]],
+                  "sample": "dx=0.02 column (the CPU rate's), device FP32 vs oracle FP64"}
     finally:
         torch.set_default_dtype(saved)
     n = pos.shape[0]
@@ -689,6 +707,7 @@ def rhs2d_leg(args, dev):
             "fluid_particles": n, "wall_particles": int(wall.shape[0]), "pairs": int(pairs.shape[0]),
             "ms_per_call": ms, "fluid_particles_per_s": n / (ms / 1e3),
             "rho_max_over_rho0": float(rho.max()) / cfg.rho0,
+            "errors_vs_fp64": errors,
             "cpu_oracle": {"fluid_particles_per_s": sp.shape[0] / t_cpu, "fluid_particles": sp.shape[0],
                            "cores": 1, "seconds": t_cpu,
                            "sample": "dx=0.02 column: pairs + density, diffusion, walls, force"}}
