@@ -413,12 +413,18 @@ def droplet_impact_case(cfg, *, drop_speed: float = 0.0, label: str = "") -> Cas
 def shear_decay_case(n: int, *, box: float = 1.0, amplitude: float = 1.0e-3, nu: float = 1.0e-2,
                      sound_speed: float = 1.0, rho0: float = 1000.0, gamma: float = 7.0,
                      h_factor: float = 1.3, jitter: float = 0.01, seed: int = 0,
-                     skin_factor: float = 0.25, courant: float = 0.25, label: str = "") -> CaseSpec:
+                     skin_factor: float = 0.25, courant: float = 0.25, density_diffusion: float = 0.0,
+                     density_diffusion_form: str = "antuono", density_diffusion_eigenvalue_floor: float = 0.1,
+                     label: str = "") -> CaseSpec:
     """A triply periodic shear decay u_x = A sin(2 pi z / L) on an n^3 lattice
     with a seeded uniform jitter of +-jitter dx, as a ``CaseSpec`` of the batch
     engine (its WCSPH operators: Tait, Morris viscous Laplacian; no gravity, no
     walls).  dt is the smaller of acoustic CFL ``courant`` and 0.9 x the
-    viscous limit 0.125 h^2 / nu."""
+    viscous limit 0.125 h^2 / nu.  ``density_diffusion`` > 0 adds the density
+    diffusion of threed's ``accelerations`` (operators3.py:226-236, scale
+    2 delta c0 h), by default its psi form with the renormalised gradient."""
+    if density_diffusion_form not in ("antuono", "molteni"):
+        raise ValueError(f"unknown density_diffusion_form {density_diffusion_form!r}")
     dx = box / n
     h = h_factor * dx
     dt = min(courant * h / sound_speed, 0.9 * 0.125 * h * h / nu)
@@ -437,6 +443,10 @@ def shear_decay_case(n: int, *, box: float = 1.0, amplitude: float = 1.0e-3, nu:
     p.dim, p.n_fluid, p.n_wall, p.n_obstacle = 3, x.shape[0], 0, 0
     p.h, p.rho0, p.sound_speed, p.gamma = h, rho0, sound_speed, gamma
     p.gravity, p.viscosity, p.wall_friction, p.diffusion_scale = 0.0, nu, 0.0, 0.0
+    if density_diffusion > 0.0:
+        p.diffusion_scale = 2.0 * density_diffusion * sound_speed * h
+        p.diffusion_form = 1 if density_diffusion_form == "antuono" else 0
+        p.diffusion_eigen_floor = float(density_diffusion_eigenvalue_floor)
     p.dt, p.wall_mass, p.skin = dt, 0.0, skin_factor * h
     for kk in range(3):
         p.box_hi[kk] = box

@@ -584,3 +584,30 @@ def test_2d_shift_reference_speed(gpu):
     assert scale > 0.0
     assert np.abs(d2 - 2.0 * d1).max() < 1e-4 * scale
     assert np.abs(da - d1).max() > 1e-3 * scale
+
+
+@pytest.mark.parametrize("form", ["antuono", "molteni"])
+def test_periodic_shear_case_density_diffusion_matches_oracle(form, gpu):
+    """The periodic shear case with threed's density diffusion (the psi form
+    with the renormalised gradient and its eigenvalue floor, the default of
+    operators3.py:212-236, and the Molteni form) across the periodic wraps:
+    the density after the first step's diffusion against the oracle's
+    ``accelerations`` in FP64, to 1e-5 of rho0 (the FP32 bar)."""
+    from tensorsph_b200.engine import BatchEngine, capacity_for, shear_decay_case
+    from oracle.neighbors import periodic_pairs
+    spec = shear_decay_case(10, amplitude=1e-2, nu=1e-3, sound_speed=5.0, jitter=0.3, seed=3,
+                            density_diffusion=0.1, density_diffusion_form=form,
+                            density_diffusion_eigenvalue_floor=0.2)
+    eng = BatchEngine(**capacity_for([spec], max_neighbors=160, diag_ring=8))
+    cid = eng.add(spec)
+    eng.step(1)
+    _, _, rho, _ = (t.cpu().numpy() for t in eng.read(cid))
+    eng.close()
+    x, v, m = spec.x.numpy(), spec.v.numpy(), spec.mass.numpy()
+    h = float(spec.params.h)
+    pairs = periodic_pairs(x, 1.0, 2.0 * h)
+    _, want, _ = op.accelerations(x, v, m, h, pairs, rho0=1000.0, sound_speed=5.0, viscosity=1e-3, box=1.0,
+                                  density_diffusion=0.1, dt=spec.dt, density_diffusion_form=form,
+                                  density_diffusion_eigenvalue_floor=0.2)
+    assert np.abs(want - 1000.0).max() > 1.0   # the jitter makes density contrasts to diffuse
+    assert np.abs(rho - want).max() / 1000.0 < 1e-5
