@@ -172,6 +172,7 @@ struct Dev {
   float4* gradc;
   float4* lpv;       // shifting: local position + volume m/rho after the Euler update
   float* tmp_v;      // the volume carried through a rebuild's permutation
+  float2* tmp_rp;    // the last density and pressure carried through it (read back by id)
   double4* csA;      // CSF: colour, M00, M01, M11
   double4* csB;      // CSF: grad c x, y, |grad c|, |det M|
   double2* csN0;     // CSF: raw normal
@@ -472,6 +473,7 @@ __global__ void k_permute(Dev e) {
     st4(e.tmp4b, a, ld4(e.vel, s));
     e.tmp_id[a] = e.id[s];
     e.tmp_v[a] = e.vb[s].w;
+    e.tmp_rp[a] = make_float2(e.rho[s], e.pr[s]);
   }
 }
 
@@ -493,6 +495,11 @@ __global__ void k_permute_back(Dev e) {
     e.lp[a] = local_of(C, key - C.key_off, p.x, p.y, p.z, p.w);
     // the shifting passes after the Euler update read this step's volumes
     if (C.shift_every > 0 || C.tvc_bulk) e.lpv[a] = local_of(C, key - C.key_off, p.x, p.y, p.z, e.tmp_v[a]);
+    // the density and pressure of the step's evaluation stay with their
+    // particle: a rebuild of the second list pass comes after them
+    const float2 rp = e.tmp_rp[a];
+    e.rho[a] = rp.x;
+    e.pr[a] = rp.y;
   }
 }
 
@@ -2632,6 +2639,7 @@ size_t carve(const tsph_engine_params& p, Dev* d, char* base, CaseDev** cases, c
   t.tmp4b = static_cast<double4*>(take(nsort * sizeof(double4)));
   t.tmp_id = static_cast<int32_t*>(take(nsort * sizeof(int32_t)));
   t.tmp_v = static_cast<float*>(take(nsort * sizeof(float)));
+  t.tmp_rp = static_cast<float2*>(take(nsort * sizeof(float2)));
   t.ctl = static_cast<CaseCtl*>(take(p.max_cases * sizeof(CaseCtl)));
   t.diag = static_cast<double*>(take(static_cast<size_t>(p.max_cases) * p.diag_ring * kDiag * sizeof(double)));
   t.any_rebuild = static_cast<int*>(take(sizeof(int)));

@@ -154,7 +154,6 @@ def test_adaptive_run_checkpoints_and_resumes(gpu, tmp_path, monkeypatch):
     rows; checkpointing leaves the run bit for bit unchanged; a run resumed
     from it takes the same number of steps to the same time, its samples
     before the checkpoint exact and the rest to round-off."""
-    import pathlib
     from tensorsph_b200.checkpoint import load_checkpoint
     from tensorsph_b200.engine import DamBreak3DEngine, _advance_adaptive, run_case
     cfg = _adaptive_cfg(20)
@@ -170,11 +169,23 @@ def test_adaptive_run_checkpoints_and_resumes(gpu, tmp_path, monkeypatch):
     assert not (tmp_path / "kept.pt").exists()
 
     path = tmp_path / "state.pt"
-    # the first attempt ends at 12 dt and keeps its last checkpoint (after
-    # the update of step 10), as a process that died would
+    # the first attempt dies right after its checkpoint of step 10 is written
+    from tensorsph_b200.checkpoint import CheckpointWriter
+    take = CheckpointWriter.take
+
+    class Killed(Exception):
+        pass
+
+    def take_then_die(self, step, *a, **kw):
+        take(self, step, *a, **kw)
+        if step == 10:
+            self.wait()
+            raise Killed
+
     with monkeypatch.context() as m:
-        m.setattr(pathlib.Path, "unlink", lambda self, missing_ok=False: None)
-        run_case(_adaptive_cfg(12), obstacle=OBSTACLE, checkpoint_path=path, checkpoint_every=5)
+        m.setattr(CheckpointWriter, "take", take_then_die)
+        with pytest.raises(Killed):
+            run_case(cfg, obstacle=OBSTACLE, checkpoint_path=path, checkpoint_every=5)
     state = load_checkpoint(path, cfg, OBSTACLE)
     assert state["step"] == 10
     assert state["elapsed"] == diag[11, 25] and state["dt"] == diag[11, 27]
