@@ -1911,119 +1911,163 @@ __device__ __forceinline__ bool clamp_box(const CaseDev& C, double& px, double& 
   return ox || oy || oz;
 }
 
+// Meters of the integrated rows: kinetic and potential energy (sums), the
+// largest displacement since the list anchor, speed, front x and density.
+struct StepMeters {
+  double ke = 0, pe = 0, dmax = 0, vmax = 0, xmax = 0, rmax = 0;
+};
+
+// Euler update of row a with the box and obstacle clamps (dam_break_3d.py:
+// 429-452, kleefsman_obstacle_3d.py:208-266), its meters into m.
+__device__ __forceinline__ void integrate_row(const Dev& e, int a, const CaseDev& C, int c, StepMeters& s) {
+  const double4 x0 = ld4(e.pos, a);
+  const double4 v0 = ld4(e.vel, a);
+  const float4 ac = e.acc[a];
+  const double m = x0.w;
+  const double dt = C.adaptive ? e.ctl[c].dt_int : C.dt;
+  const double v2 = v0.x * v0.x + v0.y * v0.y + v0.z * v0.z;
+  s.ke += 0.5 * m * v2;
+  s.pe += m * C.gravity * x0.y;
+  s.vmax = fmax(s.vmax, sqrt(v2));
+  s.xmax = fmax(s.xmax, x0.x);
+  s.rmax = fmax(s.rmax, static_cast<double>(e.rho[a]));
+  double vx = v0.x + dt * static_cast<double>(ac.x), vy = v0.y + dt * static_cast<double>(ac.y),
+         vz = v0.z + dt * static_cast<double>(ac.z);
+  double px = x0.x + dt * vx, py = x0.y + dt * vy, pz = x0.z + dt * vz;
+  if (C.periodic) {
+    // remainder into [0, L)
+    const double L = C.pbox;
+    px -= L * floor(px / L);
+    py -= L * floor(py / L);
+    pz -= L * floor(pz / L);
+    px = px >= L ? px - L : px;
+    py = py >= L ? py - L : py;
+    pz = pz >= L ? pz - L : pz;
+  } else if (clamp_box(C, px, py, pz, vx, vy, vz)) {
+    atomicAdd(&e.ctl[c].escapes, 1ull);
+  }
+  if (C.has_ob && px > C.ob_lo[0] && px < C.ob_hi[0] && py > C.ob_lo[1] && py < C.ob_hi[1] &&
+      pz > C.ob_lo[2] && pz < C.ob_hi[2]) {
+    // exit through the nearest face (first minimum, as argmin)
+    const double dist[6] = {px - C.ob_lo[0], C.ob_hi[0] - px, py - C.ob_lo[1],
+                            C.ob_hi[1] - py, pz - C.ob_lo[2], C.ob_hi[2] - pz};
+    int which = 0;
+    double best = dist[0];
+#pragma unroll
+    for (int f = 1; f < 6; ++f) {
+      if (dist[f] < best) {
+        best = dist[f];
+        which = f;
+      }
+    }
+    const double to = (which & 1) ? C.ob_eps : -C.ob_eps;
+    const int axis = which >> 1;
+    double taken;
+    if (axis == 0) {
+      px = ((which & 1) ? C.ob_hi[0] : C.ob_lo[0]) + to;
+      taken = vx;
+      vx = 0.0;
+    } else if (axis == 1) {
+      py = ((which & 1) ? C.ob_hi[1] : C.ob_lo[1]) + to;
+      taken = vy;
+      vy = 0.0;
+    } else {
+      pz = ((which & 1) ? C.ob_hi[2] : C.ob_lo[2]) + to;
+      taken = vz;
+      vz = 0.0;
+    }
+    // the obstacle's share of the clamp (kleefsman_obstacle_3d.py:259-260);
+    // clamps are rare events, so one atomic each
+    atomicAdd(&e.ctl[c].clamp_impulse[axis], m * taken);
+    atomicAdd(&e.ctl[c].clamps, 1ull);
+  }
+  if (!isfinite(px) || !isfinite(py) || !isfinite(pz) || !isfinite(vx) || !isfinite(vy) || !isfinite(vz)) {
+    atomicOr(e.status, 2);
+    atomicOr(&e.ctl[c].status, 2);
+  }
+  st4(e.pos, a, make_double4(px, py, pz, m));
+  st4(e.vel, a, make_double4(vx, vy, vz, 0.0));
+  const float4 la = local_of(C, e.home[a] - C.key_off, px, py, pz, m);
+  e.lp[a] = la;
+  if (C.shift_every > 0 || C.tvc_bulk) e.lpv[a] = make_float4(la.x, la.y, la.z, e.vb[a].w);
+  const double4 an = ld4(e.anchor, a);
+  double ex = px - an.x, ey = py - an.y, ez = pz - an.z;
+  if (C.periodic) {
+    const double L = C.pbox;
+    ex -= L * rint(ex / L);
+    ey -= L * rint(ey / L);
+    ez -= L * rint(ez / L);
+  }
+  s.dmax = fmax(s.dmax, sqrt(ex * ex + ey * ey + ez * ez));
+}
+
+// The block's meters into one thread (thread 0): the two sums and four
+// maxima reduced together, one barrier.
+__device__ __forceinline__ void block_meters(StepMeters& s, double (*red)[kMaxBlock / 32]) {
+  double v[6] = {s.ke, s.pe, s.dmax, s.vmax, s.xmax, s.rmax};
+#pragma unroll
+  for (int k = 0; k < 6; ++k) v[k] = k < 2 ? warp_reduce_sum(v[k]) : warp_reduce_max(v[k]);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) red[k][w] = v[k];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int j = 1; j < static_cast<int>(blockDim.x >> 5); ++j) {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) v[k] = k < 2 ? v[k] + red[k][j] : fmax(v[k], red[k][j]);
+    }
+    s.ke = v[0];
+    s.pe = v[1];
+    s.dmax = v[2];
+    s.vmax = v[3];
+    s.xmax = v[4];
+    s.rmax = v[5];
+  }
+}
+
+__device__ __forceinline__ void add_meters(CaseCtl& t, const StepMeters& s) {
+  atomicAdd(&t.ke, s.ke);
+  atomicAdd(&t.pe, s.pe);
+  atomic_max_nonneg(&t.disp[0], s.dmax);
+  atomic_max_nonneg(&t.speed_max, s.vmax);
+  atomic_max_nonneg(&t.front_max, s.xmax);
+  atomic_max_nonneg(&t.rho_max, s.rmax);
+}
+
+// A batch of one runs a grid-stride loop over a few blocks per SM, so that
+// each block adds its meters to the case once (same-address atomics from
+// every block of a one-row-per-thread grid cost tens of microseconds on a
+// 2 M-row case).  A batch of several cases keeps one row per thread: a block
+// whose rows all belong to one case adds one total, a mixed block adds per
+// row.
 template <bool kOne>
 __global__ void __launch_bounds__(kMaxBlock) k_integrate(const __grid_constant__ Dev e) {
-  __shared__ double red[kMaxBlock / 32];
+  __shared__ double red[6][kMaxBlock / 32];
+  StepMeters s;
+  if (kOne) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x)
+      integrate_row(e, a, e.one, e.one_slot, s);
+    block_meters(s, red);
+    if (threadIdx.x == 0) add_meters(e.ctl[e.one_slot], s);
+    return;
+  }
   const int a0 = blockIdx.x * blockDim.x;
   if (a0 >= e.nf) return;
   const int a = a0 + threadIdx.x;
-  const int cb = kOne ? e.one_slot : e.cid[a0];
-  const bool uniform = kOne || cb == e.cid[min(a0 + static_cast<int>(blockDim.x), e.nf) - 1];
+  const int cb = e.cid[a0];
+  const bool uniform = cb == e.cid[min(a0 + static_cast<int>(blockDim.x), e.nf) - 1];
   int c = -1;
-  double ke = 0, pe = 0, dmax = 0, vmax = 0, xmax = 0, rmax = 0;
   if (a < e.nf) {
-    c = kOne ? cb : e.cid[a];
-    const CaseDev& C = case_of<kOne>(e, a);
-    const double4 x0 = ld4(e.pos, a);
-    const double4 v0 = ld4(e.vel, a);
-    const float4 ac = e.acc[a];
-    const double m = x0.w;
-    const double dt = C.adaptive ? e.ctl[c].dt_int : C.dt;
-    const double v2 = v0.x * v0.x + v0.y * v0.y + v0.z * v0.z;
-    ke = 0.5 * m * v2;
-    pe = m * C.gravity * x0.y;
-    vmax = sqrt(v2);
-    xmax = x0.x;
-    rmax = static_cast<double>(e.rho[a]);
-    double vx = v0.x + dt * static_cast<double>(ac.x), vy = v0.y + dt * static_cast<double>(ac.y),
-           vz = v0.z + dt * static_cast<double>(ac.z);
-    double px = x0.x + dt * vx, py = x0.y + dt * vy, pz = x0.z + dt * vz;
-    if (C.periodic) {
-      // remainder into [0, L)
-      const double L = C.pbox;
-      px -= L * floor(px / L);
-      py -= L * floor(py / L);
-      pz -= L * floor(pz / L);
-      px = px >= L ? px - L : px;
-      py = py >= L ? py - L : py;
-      pz = pz >= L ? pz - L : pz;
-    } else if (clamp_box(C, px, py, pz, vx, vy, vz)) {
-      atomicAdd(&e.ctl[c].escapes, 1ull);
-    }
-    if (C.has_ob && px > C.ob_lo[0] && px < C.ob_hi[0] && py > C.ob_lo[1] && py < C.ob_hi[1] &&
-        pz > C.ob_lo[2] && pz < C.ob_hi[2]) {
-      // exit through the nearest face (first minimum, as argmin)
-      const double dist[6] = {px - C.ob_lo[0], C.ob_hi[0] - px, py - C.ob_lo[1],
-                              C.ob_hi[1] - py, pz - C.ob_lo[2], C.ob_hi[2] - pz};
-      int which = 0;
-      double best = dist[0];
-#pragma unroll
-      for (int f = 1; f < 6; ++f) {
-        if (dist[f] < best) {
-          best = dist[f];
-          which = f;
-        }
-      }
-      const double to = (which & 1) ? C.ob_eps : -C.ob_eps;
-      const int axis = which >> 1;
-      double taken;
-      if (axis == 0) {
-        px = ((which & 1) ? C.ob_hi[0] : C.ob_lo[0]) + to;
-        taken = vx;
-        vx = 0.0;
-      } else if (axis == 1) {
-        py = ((which & 1) ? C.ob_hi[1] : C.ob_lo[1]) + to;
-        taken = vy;
-        vy = 0.0;
-      } else {
-        pz = ((which & 1) ? C.ob_hi[2] : C.ob_lo[2]) + to;
-        taken = vz;
-        vz = 0.0;
-      }
-      // the obstacle's share of the clamp (kleefsman_obstacle_3d.py:259-260);
-      // clamps are rare events, so one atomic each
-      atomicAdd(&e.ctl[c].clamp_impulse[axis], m * taken);
-      atomicAdd(&e.ctl[c].clamps, 1ull);
-    }
-    if (!isfinite(px) || !isfinite(py) || !isfinite(pz) || !isfinite(vx) || !isfinite(vy) || !isfinite(vz)) {
-      atomicOr(e.status, 2);
-      atomicOr(&e.ctl[c].status, 2);
-    }
-    const double x[3] = {px, py, pz};
-    const double v[3] = {vx, vy, vz};
-    st4(e.pos, a, make_double4(x[0], x[1], x[2], m));
-    st4(e.vel, a, make_double4(v[0], v[1], v[2], 0.0));
-    const float4 la = local_of(C, e.home[a] - C.key_off, x[0], x[1], x[2], m);
-    e.lp[a] = la;
-    if (C.shift_every > 0 || C.tvc_bulk) e.lpv[a] = make_float4(la.x, la.y, la.z, e.vb[a].w);
-    const double4 an = ld4(e.anchor, a);
-    double ex = x[0] - an.x, ey = x[1] - an.y, ez = x[2] - an.z;
-    if (C.periodic) {
-      const double L = C.pbox;
-      ex -= L * rint(ex / L);
-      ey -= L * rint(ey / L);
-      ez -= L * rint(ez / L);
-    }
-    dmax = sqrt(ex * ex + ey * ey + ez * ez);
+    c = e.cid[a];
+    integrate_row(e, a, e.cases[c], c, s);
   }
   if (uniform) {
-    ke = block_reduce<false>(ke, red);
-    pe = block_reduce<false>(pe, red);
-    dmax = block_reduce<true>(dmax, red);
-    vmax = block_reduce<true>(vmax, red);
-    xmax = block_reduce<true>(xmax, red);
-    rmax = block_reduce<true>(rmax, red);
+    block_meters(s, red);
     c = threadIdx.x == 0 ? cb : -1;
   }
-  if (c >= 0) {
-    CaseCtl& t = e.ctl[c];
-    atomicAdd(&t.ke, ke);
-    atomicAdd(&t.pe, pe);
-    atomic_max_nonneg(&t.disp[0], dmax);
-    atomic_max_nonneg(&t.speed_max, vmax);
-    atomic_max_nonneg(&t.front_max, xmax);
-    atomic_max_nonneg(&t.rho_max, rmax);
-  }
+  if (c >= 0) add_meters(e.ctl[c], s);
 }
 
 // Per-case meter row: max rho, max |v|, front x, obstacle force xyz, kinetic
@@ -2574,6 +2618,8 @@ struct tsph_engine {
   bool stale = false;          // the batch changed: the next step re-captures and updates exec
   int64_t instantiations = 0;  // step graphs instantiated
   int64_t updates = 0;         // batch changes absorbed by cudaGraphExecUpdate
+  int sms = 148;               // multiprocessors of the device (grid-stride launch caps)
+  int integrate_per_sm[3] = {1, 1, 1};  // resident k_integrate<true> blocks of 64, 128, 256 threads
 };
 
 namespace tsph {
@@ -2863,7 +2909,13 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr, b
   mark();
   if (d.n_ob) k_reaction<<<static_cast<unsigned>((d.n_ob + B - 1) / B), B, 0, s>>>(d);
   mark();
-  (one ? k_integrate<true> : k_integrate<false>)<<<static_cast<unsigned>((d.nf + B - 1) / B), B, 0, s>>>(d);
+  if (one) {
+    // one wave of resident blocks
+    const int per_sm = E->integrate_per_sm[B == 64 ? 0 : (B == 128 ? 1 : 2)];
+    k_integrate<true><<<grid_for(d.nf, B, static_cast<int64_t>(E->sms) * per_sm), B, 0, s>>>(d);
+  }
+  else
+    k_integrate<false><<<static_cast<unsigned>((d.nf + B - 1) / B), B, 0, s>>>(d);
   k_finalize<<<gc, 128, 0, s>>>(d);
   if (d.has_tvc && !d.tvc_late) {
     // the correction reads the rows of this step (the pass-0 lists)
@@ -2891,7 +2943,8 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr, b
     }
     k_select_finish<<<1, 32, 0, s>>>(d, pos - static_cast<double>(lo));
     mark();
-    if (shifting(E)) k_shift_apply<<<g, B, 0, s>>>(d);
+    // a grid-stride loop over a few blocks per SM: one displacement atomic per block
+    if (shifting(E)) k_shift_apply<<<grid_for(d.nf, B, static_cast<int64_t>(E->sms) * (1024 / B)), B, 0, s>>>(d);
     if (d.tvc_late) {
       // the bulk scope: the rows of the second pass, the mask of its percentile
       k_tvc_gradient<true><<<g, B, 0, s>>>(d);
@@ -3128,6 +3181,18 @@ int tsph_engine_create(const tsph_engine_params* prm, void* arena, int64_t arena
   }
   E->prm = *prm;
   E->arena = static_cast<char*>(arena);
+  {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && sms > 0)
+      E->sms = sms;
+    const int blocks[3] = {64, 128, 256};
+    for (int k = 0; k < 3; ++k) {
+      int n = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_integrate<true>, blocks[k], 0) == cudaSuccess && n > 0)
+        E->integrate_per_sm[k] = n;
+    }
+  }
   carve(*prm, &E->d, E->arena, &E->cases_dev, &E->radix_scratch);
   Dev& d = E->d;
   d.NF = static_cast<int>(prm->max_fluid);
