@@ -2613,6 +2613,8 @@ struct tsph_engine {
   cudaGraphExec_t exec = nullptr;
   cudaStream_t captured_on = nullptr;
   cudaStream_t aux = nullptr;  // captures the bodies of the step graph's conditional nodes
+  cudaStream_t side = nullptr; // the shifting percentile's branch beside the gradient pass
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   bool conditional = true;     // rebuilds in conditional nodes (off if the driver refuses them)
   int64_t rebuild_kernels = 0; // kernel nodes of one conditional rebuild body
   bool stale = false;          // the batch changed: the next step re-captures and updates exec
@@ -2706,6 +2708,15 @@ int key_bits(int64_t cells) {
   int bits = 1;
   while ((int64_t(1) << bits) < cells) ++bits;
   return bits;
+}
+
+void release_streams(tsph_engine* E) {
+  if (E->aux) cudaStreamDestroy(E->aux);
+  if (E->side) cudaStreamDestroy(E->side);
+  if (E->fork_ev) cudaEventDestroy(E->fork_ev);
+  if (E->join_ev) cudaEventDestroy(E->join_ev);
+  E->aux = E->side = nullptr;
+  E->fork_ev = E->join_ev = nullptr;
 }
 
 void invalidate_graph(tsph_engine* E) {
@@ -2931,17 +2942,33 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr, b
     mark();
     k_concentration<<<g, B, 0, s>>>(d);
     mark();
+    // In the step graph the percentile's select (small and partly one-block
+    // kernels) runs on a branch beside the gradient pass; both only read the
+    // concentration, and the shift waits for both.  Stage-timed steps keep
+    // them in sequence.
+    const bool fork = marks == nullptr;
+    cudaStream_t sel = s;
+    if (fork) {
+      TSPH_CUDA_CHECK(cudaEventRecord(E->fork_ev, s));
+      TSPH_CUDA_CHECK(cudaStreamWaitEvent(E->side, E->fork_ev, 0));
+      sel = E->side;
+    }
     if (shifting(E)) k_conc_gradient<<<g, B, 0, s>>>(d);
     mark();
     const double pos = 0.95 * static_cast<double>(d.nf - 1);
     const long long lo = static_cast<long long>(std::floor(pos)), hi = static_cast<long long>(std::ceil(pos));
-    const unsigned gs = grid_for(d.nf, 256, 148 * 4);
+    const unsigned gs = grid_for(d.nf, 256, static_cast<int64_t>(E->sms) * 4);
     const int widths[3] = {11, 11, 10}, shifts[3] = {21, 10, 0};
     for (int pass = 0; pass < 3; ++pass) {
-      k_select_hist<<<gs, 256, 0, s>>>(d, shifts[pass], widths[pass]);
-      k_select_pick<<<1, 1024, 0, s>>>(d, shifts[pass], widths[pass], lo, hi);
+      k_select_hist<<<gs, 256, 0, sel>>>(d, shifts[pass], widths[pass]);
+      k_select_pick<<<1, 1024, 0, sel>>>(d, shifts[pass], widths[pass], lo, hi);
     }
-    k_select_finish<<<1, 32, 0, s>>>(d, pos - static_cast<double>(lo));
+    k_select_finish<<<1, 32, 0, sel>>>(d, pos - static_cast<double>(lo));
+    TSPH_LAUNCH_CHECK();
+    if (fork) {
+      TSPH_CUDA_CHECK(cudaEventRecord(E->join_ev, E->side));
+      TSPH_CUDA_CHECK(cudaStreamWaitEvent(s, E->join_ev, 0));
+    }
     mark();
     // a grid-stride loop over a few blocks per SM: one displacement atomic per block
     if (shifting(E)) k_shift_apply<<<grid_for(d.nf, B, static_cast<int64_t>(E->sms) * (1024 / B)), B, 0, s>>>(d);
@@ -3179,6 +3206,13 @@ int tsph_engine_create(const tsph_engine_params* prm, void* arena, int64_t arena
     delete E;
     return TSPH_ERR_CUDA;
   }
+  if (cudaStreamCreateWithFlags(&E->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&E->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&E->join_ev, cudaEventDisableTiming) != cudaSuccess) {
+    release_streams(E);
+    delete E;
+    return TSPH_ERR_CUDA;
+  }
   E->prm = *prm;
   E->arena = static_cast<char*>(arena);
   {
@@ -3211,7 +3245,7 @@ int tsph_engine_create(const tsph_engine_params* prm, void* arena, int64_t arena
       cudaMemsetAsync(E->cases_dev, 0, prm->max_cases * sizeof(CaseDev), s) != cudaSuccess ||
       (k_null_row<<<1, 1, 0, s>>>(d), cudaGetLastError()) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess) {
-    cudaStreamDestroy(E->aux);
+    release_streams(E);
     delete E;
     return TSPH_ERR_CUDA;
   }
@@ -3603,7 +3637,7 @@ int tsph_engine_set_batch(tsph_engine* E, int64_t depth) {
 int tsph_engine_destroy(tsph_engine* E) {
   if (!E) return TSPH_OK;
   invalidate_graph(E);
-  if (E->aux) cudaStreamDestroy(E->aux);
+  release_streams(E);
   delete E;
   return TSPH_OK;
 }
