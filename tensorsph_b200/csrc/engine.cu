@@ -49,6 +49,7 @@ constexpr int kBlock = 128;     // default threads per block of the pair kernels
 constexpr int kMaxBlock = 256;  // largest block the kernels are built for
 constexpr int kDiag = 30;
 constexpr int kBatch = 4;
+constexpr int kConcBatch = 4;  // neighbour records in flight in the shifting passes
 constexpr int kCodeBits = 6;                               // cell-offset code bits of a row entry
 constexpr uint32_t kCodeMask = (1u << kCodeBits) - 1;
 constexpr uint32_t kSelfCode = 0x15u;                      // offset (0, 0, 0): fields (1, 1, 1)
@@ -2245,7 +2246,8 @@ __global__ void k_tvc_finish(Dev e) {
 // ------------------------------------------------------------- shifting ---
 // One case (slot e.shift_slot) owns every fluid row when shifting runs.
 
-__global__ void __launch_bounds__(kMaxBlock) k_concentration(Dev e) {
+template <int KB>
+__global__ void __launch_bounds__(kMaxBlock) k_concentration(const __grid_constant__ Dev e) {
   if (!e.ctl[e.shift_slot].conc_now) return;
   const CaseDev& C = e.cases[e.shift_slot];
   const float sig2d = C.sig2d, inv_h = C.inv_h, cellf = C.cellf;
@@ -2255,10 +2257,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_concentration(Dev e) {
     const float2 ncell = f2(-cellf), inv_h2 = f2(inv_h), sig2 = f2(sig2d);
     CSum<float> s;
     s.add(la.w * sig2d);
-    walk_row(e, a, [&](const uint32_t* ent) {
+    walk_row<KB>(e, a, [&](const uint32_t* ent) {
       float2 part = f2(0.f);
 #pragma unroll
-      for (int j = 0; j < kBatch; j += 2) {
+      for (int j = 0; j < KB; j += 2) {
         const uint32_t e0 = ent[j], e1 = ent[j + 1];
         const int c0 = static_cast<int>(e0 >> kCodeBits), c1 = static_cast<int>(e1 >> kCodeBits);
         const float4 l0 = e.lpv[c0 < NF ? c0 : e.null_row], l1 = e.lpv[c1 < NF ? c1 : e.null_row];
@@ -2275,7 +2277,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_concentration(Dev e) {
   }
 }
 
-__global__ void __launch_bounds__(kMaxBlock) k_conc_gradient(Dev e) {
+template <int KB>
+__global__ void __launch_bounds__(kMaxBlock) k_conc_gradient(const __grid_constant__ Dev e) {
   if (!e.ctl[e.shift_slot].shift_now) return;
   const CaseDev& C = e.cases[e.shift_slot];
   const float sig2d = C.sig2d, inv_h = C.inv_h, cellf = C.cellf;
@@ -2285,10 +2288,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_conc_gradient(Dev e) {
     const float ca = e.conc[a];
     const float2 ncell = f2(-cellf), inv_h2 = f2(inv_h), gscale = f2(sig2d * inv_h);
     CSum<float> gx, gy, gz;
-    walk_row(e, a, [&](const uint32_t* ent) {
+    walk_row<KB>(e, a, [&](const uint32_t* ent) {
       float2 px = f2(0.f), py = f2(0.f), pz = f2(0.f);
 #pragma unroll
-      for (int j = 0; j < kBatch; j += 2) {
+      for (int j = 0; j < KB; j += 2) {
         const uint32_t e0 = ent[j], e1 = ent[j + 1];
         const int c0 = static_cast<int>(e0 >> kCodeBits), c1 = static_cast<int>(e1 >> kCodeBits);
         const int b0 = c0 < NF ? c0 : e.null_row, b1 = c1 < NF ? c1 : e.null_row;
@@ -2940,7 +2943,7 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr, b
     rc = enqueue_rebuild(E, s, 1, graph);
     if (rc) return rc;
     mark();
-    k_concentration<<<g, B, 0, s>>>(d);
+    k_concentration<kConcBatch><<<g, B, 0, s>>>(d);
     mark();
     // In the step graph the percentile's select (small and partly one-block
     // kernels) runs on a branch beside the gradient pass; both only read the
@@ -2953,7 +2956,7 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr, b
       TSPH_CUDA_CHECK(cudaStreamWaitEvent(E->side, E->fork_ev, 0));
       sel = E->side;
     }
-    if (shifting(E)) k_conc_gradient<<<g, B, 0, s>>>(d);
+    if (shifting(E)) k_conc_gradient<kConcBatch><<<g, B, 0, s>>>(d);
     mark();
     const double pos = 0.95 * static_cast<double>(d.nf - 1);
     const long long lo = static_cast<long long>(std::floor(pos)), hi = static_cast<long long>(std::ceil(pos));
@@ -2970,8 +2973,7 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr, b
       TSPH_CUDA_CHECK(cudaStreamWaitEvent(s, E->join_ev, 0));
     }
     mark();
-    // a grid-stride loop over a few blocks per SM: one displacement atomic per block
-    if (shifting(E)) k_shift_apply<<<grid_for(d.nf, B, static_cast<int64_t>(E->sms) * (1024 / B)), B, 0, s>>>(d);
+    if (shifting(E)) k_shift_apply<<<g, B, 0, s>>>(d);
     if (d.tvc_late) {
       // the bulk scope: the rows of the second pass, the mask of its percentile
       k_tvc_gradient<true><<<g, B, 0, s>>>(d);
