@@ -13,6 +13,7 @@ from __future__ import annotations
 import ctypes
 from dataclasses import dataclass
 import math
+import weakref
 
 import torch
 
@@ -21,6 +22,31 @@ from .droplet_impact import symmetric_rows
 from .neighbor_search import grid_pairs
 
 __all__ = ["DeltaPlusStep", "delta_plus_step", "delta_plus_step3"]
+
+
+# The gather rows of the last pair list a step was given: a Verlet cache
+# (PairListCache) hands back the same tensor between rebuilds, so a caller
+# that steps with it pays for the check and the row build once per rebuild.
+# The rows are dropped with the pair list they were built from.
+_ROWS: dict = {"pairs": None, "version": None, "nrows": None, "rows": None}
+
+
+def _forget_rows(_ref=None) -> None:
+    _ROWS.update(pairs=None, version=None, nrows=None, rows=None)
+
+
+def _rows_of(pairs: torch.Tensor, dev, nrows: int):
+    ref = _ROWS["pairs"]
+    if (ref is not None and ref() is pairs and _ROWS["version"] == pairs._version
+            and _ROWS["nrows"] == nrows):
+        return _ROWS["rows"]
+    i, j = pairs.unbind(1)
+    if bool(((i < 0) | (i >= j) | (j >= nrows)).any()):
+        raise ValueError("each pair must have 0 <= i < j < number of particles")
+    _forget_rows()
+    rows = symmetric_rows(_lib.to_dev(pairs, dev), nrows)
+    _ROWS.update(pairs=weakref.ref(pairs, _forget_rows), version=pairs._version, nrows=nrows, rows=rows)
+    return rows
 
 
 @dataclass
@@ -107,20 +133,17 @@ def _delta_plus(dim, pos, velocity, density, mass, *, dx, sound_speed, reference
     dtype = pos.dtype
     P, V, R, M = (_lib.to_dev(t.detach(), dev, dtype).contiguous() for t in (pos, velocity, density, mass))
     W, WV, WN = (_lib.to_dev(t.detach(), dev, dtype).contiguous() for t in (wall, wall_velocity, wall_normal))
-    cloud = torch.cat((P, W)) if nw else P
     if pairs is None:
+        cloud = torch.cat((P, W)) if nw else P
         pairs_dev, _, _ = grid_pairs(cloud, 2 * h) if n + nw >= 2 else (
             torch.zeros((0, 2), dtype=torch.long, device=dev), 0, None)
+        rowptr, entries = symmetric_rows(pairs_dev, n + nw)
     else:
         if pairs.ndim != 2 or pairs.shape[1] != 2 or pairs.dtype != torch.long:
             raise ValueError("expected a (P, 2) long pair list")
         if pairs.device != pos.device:
             raise ValueError("pair list must share the device of the state")
-        i, j = pairs.unbind(1)
-        if bool(((i < 0) | (i >= j) | (j >= n + nw)).any()):
-            raise ValueError("each pair must have 0 <= i < j < number of particles")
-        pairs_dev = _lib.to_dev(pairs, dev)
-    rowptr, entries = symmetric_rows(pairs_dev, n + nw)
+        rowptr, entries = _rows_of(pairs, dev, n + nw)
     prm = _lib.DeltaPlusParams()
     prm.dtype, prm.n_fluid, prm.n_wall = _lib.dtype_code(dtype), n, nw
     prm.dx, prm.sound_speed, prm.reference_speed, prm.dt = float(dx), float(sound_speed), \
