@@ -214,14 +214,16 @@ int radix_sort_u64_i32(uint64_t* keys, int32_t* vals, uint64_t* keys_tmp, int32_
 
 // ---------------------------------------------------------- segmented sort ---
 
-constexpr int kShortRow = 256;    // one warp, rank sort in shared memory
-constexpr int kMediumRow = 8192;  // one block, bitonic in shared memory
+constexpr int kShortRow = 64;     // one warp, rank sort in shared memory
+constexpr int kMidRow = 1024;     // one 128-thread block, bitonic in shared memory
+constexpr int kMediumRow = 8192;  // one 512-thread block, bitonic in shared memory
 constexpr int kSortWarps = 8;
 
 struct SegsortLists {
   int64_t* medium;
   int64_t* long_rows;
-  int64_t* counts;  // [0] medium, [1] long
+  int64_t* mid;
+  int64_t* counts;  // [0] medium, [1] long, [2] mid
 };
 
 __global__ void segsort_short(uint32_t* __restrict__ vals, const int64_t* __restrict__ rowptr,
@@ -234,7 +236,9 @@ __global__ void segsort_short(uint32_t* __restrict__ vals, const int64_t* __rest
     if (len <= 1) continue;
     if (len > kShortRow) {
       if (lane == 0) {
-        if (len <= kMediumRow)
+        if (len <= kMidRow)
+          lists.mid[atomicAdd(reinterpret_cast<unsigned long long*>(&lists.counts[2]), 1ull)] = r;
+        else if (len <= kMediumRow)
           lists.medium[atomicAdd(reinterpret_cast<unsigned long long*>(&lists.counts[0]), 1ull)] = r;
         else
           lists.long_rows[atomicAdd(reinterpret_cast<unsigned long long*>(&lists.counts[1]), 1ull)] = r;
@@ -269,6 +273,26 @@ __device__ __forceinline__ void bitonic_smem(uint32_t* a, int p2) {
       }
       __syncthreads();
     }
+  }
+}
+
+// Rows of kShortRow + 1 .. kMidRow entries (the symmetric rows of a 3-D
+// pair list at h = 2 dx hold ~330): a small block per row, so that many rows
+// are in flight on every SM between the network's barriers.
+__global__ void __launch_bounds__(128) segsort_mid(uint32_t* __restrict__ vals, const int64_t* __restrict__ rowptr,
+                                                   SegsortLists lists) {
+  __shared__ uint32_t buf[kMidRow];
+  const int64_t count = lists.counts[2];
+  for (int64_t q = blockIdx.x; q < count; q += gridDim.x) {
+    const int64_t r = lists.mid[q];
+    const int64_t beg = rowptr[r], len = rowptr[r + 1] - beg;
+    int p2 = 1;
+    while (p2 < len) p2 <<= 1;
+    for (int t = threadIdx.x; t < p2; t += blockDim.x) buf[t] = t < len ? vals[beg + t] : 0xffffffffu;
+    __syncthreads();
+    bitonic_smem(buf, p2);
+    for (int t = threadIdx.x; t < len; t += blockDim.x) vals[beg + t] = buf[t];
+    __syncthreads();
   }
 }
 
@@ -323,7 +347,7 @@ __global__ void segsort_long(uint32_t* __restrict__ vals, const int64_t* __restr
 }
 
 size_t segsort_scratch_bytes(int64_t rows) {
-  return 2 * align_up(static_cast<size_t>(rows + 1) * sizeof(int64_t)) + 256;
+  return 3 * align_up(static_cast<size_t>(rows + 1) * sizeof(int64_t)) + 256;
 }
 
 int segmented_sort_u32(uint32_t* vals, const int64_t* rowptr, int64_t rows, void* scratch,
@@ -334,9 +358,12 @@ int segmented_sort_u32(uint32_t* vals, const int64_t* rowptr, int64_t rows, void
   lists.counts = reinterpret_cast<int64_t*>(sc);
   lists.medium = reinterpret_cast<int64_t*>(sc + 256);
   lists.long_rows = reinterpret_cast<int64_t*>(sc + 256 + align_up((rows + 1) * sizeof(int64_t)));
-  TSPH_CUDA_CHECK(cudaMemsetAsync(lists.counts, 0, 2 * sizeof(int64_t), s));
+  lists.mid = reinterpret_cast<int64_t*>(sc + 256 + 2 * align_up((rows + 1) * sizeof(int64_t)));
+  TSPH_CUDA_CHECK(cudaMemsetAsync(lists.counts, 0, 3 * sizeof(int64_t), s));
   unsigned g = grid_for(rows, kSortWarps, 148 * 16);
   segsort_short<<<g, kSortWarps * 32, 0, s>>>(vals, rowptr, rows, lists);
+  TSPH_LAUNCH_CHECK();
+  segsort_mid<<<148 * 12, 128, 0, s>>>(vals, rowptr, lists);
   TSPH_LAUNCH_CHECK();
   segsort_medium<<<148 * 2, 512, 0, s>>>(vals, rowptr, lists);
   TSPH_LAUNCH_CHECK();

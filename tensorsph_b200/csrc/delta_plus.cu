@@ -36,6 +36,20 @@ namespace {
 
 constexpr uint32_t kIdx = 0x7fffffffu;
 
+// Four values in one aligned load: the records the gathers read for each
+// neighbour (position + volume, velocity + pressure, ...), packed once per
+// step so that a neighbour costs one or two vector loads instead of a
+// scalar load per component.
+template <class T>
+struct alignas(4 * sizeof(T)) Q4 {
+  T x, y, z, w;
+};
+
+template <class T>
+__device__ __forceinline__ T comp(const Q4<T>& q, int k) {
+  return k == 0 ? q.x : (k == 1 ? q.y : q.z);
+}
+
 // packed symmetric D x D: 2-D (00, 01, 11), 3-D (00, 01, 02, 11, 12, 22)
 template <int D>
 struct Sym {
@@ -83,6 +97,15 @@ struct DPW {
   T* wrho;   // wall density
   T* wn;     // unit wall normals, D per station
   int* status;  // bit 0: nonpositive wall density, bit 1: nonpositive/non-finite density
+  // packed neighbour records (copies of the values above, so the results do
+  // not depend on them)
+  Q4<T>* pk;  // every row: position, V = m / rho (fluid) or 0 (station)
+  Q4<T>* fv;  // fluid: velocity, p
+  Q4<T>* u4;  // fluid: v' after P2, lambda
+  Q4<T>* g4;  // fluid: renormalised grad rho after P3, rho
+  Q4<T>* s4;  // fluid: m, rho, surface flag after P4
+  Q4<T>* wq;  // stations: unit normal, wall pressure
+  Q4<T>* wv;  // stations: velocity, wall density
 };
 
 template <class T, int D>
@@ -120,11 +143,22 @@ __device__ __forceinline__ T cross_norm(const T a[D], const T b[D]) {
   return sqrt(cx * cx + cy * cy + cz * cz);
 }
 
-template <class T>
+template <class T, int D>
 __global__ void p0_state(DPP<T> p, DPW<T> w) {
-  for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < p.n; a += gridDim.x * blockDim.x) {
-    w.vol[a] = w.mass[a] / w.rho[a];
-    w.p[a] = p.c2 * (w.rho[a] - p.rho0);
+  for (int64_t a = blockIdx.x * blockDim.x + threadIdx.x; a < p.n + p.nw; a += gridDim.x * blockDim.x) {
+    T x[D];
+    point<T, D>(p, w, a, x);
+    if (a < p.n) {
+      const T vol = w.mass[a] / w.rho[a];
+      const T pr = p.c2 * (w.rho[a] - p.rho0);
+      w.vol[a] = vol;
+      w.p[a] = pr;
+      w.pk[a] = Q4<T>{x[0], x[1], D == 3 ? x[D - 1] : T(0), vol};
+      const T* v = w.vel + D * a;
+      w.fv[a] = Q4<T>{v[0], v[1], D == 3 ? v[D - 1] : T(0), pr};
+    } else {
+      w.pk[a] = Q4<T>{x[0], x[1], D == 3 ? x[D - 1] : T(0), T(0)};
+    }
   }
 }
 
@@ -147,13 +181,14 @@ __global__ void p1_walls(DPP<T> p, DPW<T> w) {
     for (int64_t e = w.rowptr[r]; e < w.rowptr[r + 1]; ++e) {
       const int64_t f = w.ent[e] & kIdx;
       if (f >= p.n) continue;
+      const Q4<T> xf = w.pk[f];
       T d[D];  // x_f - x_w
 #pragma unroll
-      for (int k = 0; k < D; ++k) d[k] = w.pos[D * f + k] - xw[k];
+      for (int k = 0; k < D; ++k) d[k] = comp(xf, k) - xw[k];
       const T r2 = dot<T, D>(d, d);
       if (!(r2 < p.support2)) continue;
       const T W = p.k.w(sqrt(r2));
-      num.add(W * (w.p[f] + w.rho[f] * p.g * d[1]));
+      num.add(W * (w.fv[f].w + w.rho[f] * p.g * d[1]));
       den.add(W);
       ++pairs;
     }
@@ -164,15 +199,22 @@ __global__ void p1_walls(DPP<T> p, DPW<T> w) {
     w.wrho[s] = wr;
     if (pairs > 0 && !(wr > T(0))) atomicOr(w.status, 1);
     // reaction: minus the force this station exerts on each fluid pair
+    T wvel[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) wvel[k] = w.wall_vel[D * s + k];
+    w.wq[s] = Q4<T>{nv[0], nv[1], D == 3 ? nv[D - 1] : T(0), wp};
+    w.wv[s] = Q4<T>{wvel[0], wvel[1], D == 3 ? wvel[D - 1] : T(0), wr};
     CSum<T> rc[D];
     for (int64_t e = w.rowptr[r]; e < w.rowptr[r + 1]; ++e) {
       const int64_t f = w.ent[e] & kIdx;
       if (f >= p.n) continue;
+      const Q4<T> xf = w.pk[f];
       T d[D];
 #pragma unroll
-      for (int k = 0; k < D; ++k) d[k] = w.pos[D * f + k] - xw[k];
+      for (int k = 0; k < D; ++k) d[k] = comp(xf, k) - xw[k];
       const T r2 = dot<T, D>(d, d);
       if (!(r2 < p.support2)) continue;
+      const Q4<T> vf = w.fv[f];
       T W, gs;
       p.k.wg(sqrt(r2), W, gs);
       T gv[D], tv[D], rel[D];
@@ -182,12 +224,12 @@ __global__ void p1_walls(DPP<T> p, DPW<T> w) {
 #pragma unroll
       for (int k = 0; k < D; ++k) {
         tv[k] = nv[k] * sg;
-        rel[k] = w.vel[D * f + k] - w.wall_vel[D * s + k];
+        rel[k] = comp(vf, k) - wvel[k];
       }
       const T closing = dot<T, D>(rel, tv);
       const T ng = dot<T, D>(gv, tv);
-      const T twice = w.p[f] + wp + T(2) * w.rho[f] * p.c0 * closing;
-      const T c = -(w.vol[f] * p.dxd * twice) * ng;
+      const T twice = vf.w + wp + T(2) * w.rho[f] * p.c0 * closing;
+      const T c = -(xf.w * p.dxd * twice) * ng;
 #pragma unroll
       for (int k = 0; k < D; ++k) rc[k].add(-(c * tv[k]));
     }
@@ -210,10 +252,10 @@ __global__ void p2_force(DPP<T> p, DPW<T> w) {
     CSum<T> fc[D], mom[S::N];
     for (int64_t e = w.rowptr[a]; e < w.rowptr[a + 1]; ++e) {
       const int64_t b = w.ent[e] & kIdx;
-      T xb[D], d[D];
-      point<T, D>(p, w, b, xb);
+      const Q4<T> xb = w.pk[b];
+      T d[D];
 #pragma unroll
-      for (int k = 0; k < D; ++k) d[k] = xa[k] - xb[k];
+      for (int k = 0; k < D; ++k) d[k] = xa[k] - comp(xb, k);
       const T r2 = dot<T, D>(d, d);
       if (!(r2 < p.support2)) continue;
       T W, gs;
@@ -222,12 +264,13 @@ __global__ void p2_force(DPP<T> p, DPW<T> w) {
 #pragma unroll
       for (int k = 0; k < D; ++k) gv[k] = d[k] * gs;
       if (b < p.n) {
-        const T Vb = w.vol[b];
-        T c = -(Va * Vb * (pa + w.p[b]));
+        const Q4<T> vb = w.fv[b];
+        const T Vb = xb.w;
+        T c = -(Va * Vb * (pa + vb.w));
         if (p.rho0_nu != T(0)) {
           T dv[D];
 #pragma unroll
-          for (int k = 0; k < D; ++k) dv[k] = va[k] - w.vel[D * b + k];
+          for (int k = 0; k < D; ++k) dv[k] = va[k] - comp(vb, k);
           const T approach = dot<T, D>(dv, d);
           const T floor2 = T(1e-12) * p.h * p.h;
           const T pi = approach / (r2 > floor2 ? r2 : floor2);
@@ -242,29 +285,32 @@ __global__ void p2_force(DPP<T> p, DPW<T> w) {
           for (int j = i; j < D; ++j) mom[S::at(i, j)].add(Vb * -(d[i] * gv[j]));
       } else {
         const int64_t s = b - p.n;
+        const Q4<T> wq = w.wq[s], wv = w.wv[s];
         T nv[D], tv[D], rel[D];
 #pragma unroll
-        for (int k = 0; k < D; ++k) nv[k] = w.wn[D * s + k];
+        for (int k = 0; k < D; ++k) nv[k] = comp(wq, k);
         const T sg = sgn(dot<T, D>(gv, nv));
 #pragma unroll
         for (int k = 0; k < D; ++k) {
           tv[k] = nv[k] * sg;
-          rel[k] = va[k] - w.wall_vel[D * s + k];
+          rel[k] = va[k] - comp(wv, k);
         }
         const T closing = dot<T, D>(rel, tv);
         const T ng = dot<T, D>(gv, tv);
-        const T twice = pa + w.wp[s] + T(2) * ra * p.c0 * closing;
+        const T twice = pa + wq.w + T(2) * ra * p.c0 * closing;
         const T c = -(Va * p.dxd * twice) * ng;
 #pragma unroll
         for (int k = 0; k < D; ++k) fc[k].add(c * tv[k]);
       }
     }
     const T m = w.mass[a];
+    T un[D];
 #pragma unroll
     for (int k = 0; k < D; ++k) {
       const T ak = fc[k].value() / m - (k == 1 ? p.g : T(0));
       w.acc[D * a + k] = ak;
-      w.out_vel[D * a + k] = va[k] + p.dt * ak;
+      un[k] = va[k] + p.dt * ak;
+      w.out_vel[D * a + k] = un[k];
     }
     // eigenvalues and the eigen-floored inverse of M (delta_plus.py:39-42)
     double mm[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
@@ -301,6 +347,7 @@ __global__ void p2_force(DPP<T> p, DPW<T> w) {
         for (int j = i; j < D; ++j) inv[S::at(i, j)] += vec[k][i] * vec[k][j] / l;
     }
     w.lam[a] = static_cast<T>(lmin);
+    w.u4[a] = Q4<T>{un[0], un[1], D == 3 ? un[D - 1] : T(0), static_cast<T>(lmin)};
 #pragma unroll
     for (int q = 0; q < S::N; ++q) w.inv[S::N * a + q] = static_cast<T>(inv[q]);
   }
@@ -332,10 +379,10 @@ __global__ void p3_geometry(DPP<T> p, DPW<T> w) {
     CSum<T> div, gr[D], gl[D];
     for (int64_t e = w.rowptr[a]; e < w.rowptr[a + 1]; ++e) {
       const int64_t b = w.ent[e] & kIdx;
-      T xb[D], d[D];
-      point<T, D>(p, w, b, xb);
+      const Q4<T> xb = w.pk[b];
+      T d[D];
 #pragma unroll
-      for (int k = 0; k < D; ++k) d[k] = xa[k] - xb[k];
+      for (int k = 0; k < D; ++k) d[k] = xa[k] - comp(xb, k);
       const T r2 = dot<T, D>(d, d);
       if (!(r2 < p.support2)) continue;
       T W, gs;
@@ -344,12 +391,13 @@ __global__ void p3_geometry(DPP<T> p, DPW<T> w) {
 #pragma unroll
       for (int k = 0; k < D; ++k) gv[k] = d[k] * gs;
       if (b < p.n) {
-        const T Vb = w.vol[b];
+        const Q4<T> ub = w.u4[b];
+        const T Vb = xb.w;
         T du[D];
 #pragma unroll
-        for (int k = 0; k < D; ++k) du[k] = w.out_vel[D * b + k] - ua[k];
+        for (int k = 0; k < D; ++k) du[k] = comp(ub, k) - ua[k];
         div.add(Vb * dot<T, D>(du, gv));
-        const T dr = Vb * (w.rho[b] - ra), dl = Vb * (w.lam[b] - la);
+        const T dr = Vb * (w.rho[b] - ra), dl = Vb * (ub.w - la);
 #pragma unroll
         for (int k = 0; k < D; ++k) {
           gr[k].add(dr * gv[k]);
@@ -357,11 +405,12 @@ __global__ void p3_geometry(DPP<T> p, DPW<T> w) {
         }
       } else {
         const int64_t s = b - p.n;
+        const Q4<T> wq = w.wq[s], wv = w.wv[s];
         T nv[D], rel[D];
 #pragma unroll
         for (int k = 0; k < D; ++k) {
-          nv[k] = w.wn[D * s + k];
-          rel[k] = w.wall_vel[D * s + k] - ua[k];
+          nv[k] = comp(wq, k);
+          rel[k] = comp(wv, k) - ua[k];
         }
         const T ns = dot<T, D>(rel, nv);
         div.add(T(2) * p.dxd * ns * dot<T, D>(nv, gv));
@@ -383,6 +432,7 @@ __global__ void p3_geometry(DPP<T> p, DPW<T> w) {
       w.grho[D * a + k] = outr[k];
       w.nrm[D * a + k] = -outl[k] / den;
     }
+    w.g4[a] = Q4<T>{outr[0], outr[1], D == 3 ? outr[D - 1] : T(0), ra};
     w.str[a] = mag * p.h;
     w.rate[a] = -ra * div.value();
   }
@@ -417,36 +467,40 @@ __global__ void p4_density(DPP<T> p, DPW<T> w) {
     for (int64_t e = w.rowptr[a]; e < w.rowptr[a + 1]; ++e) {
       const int64_t b = w.ent[e] & kIdx;
       if (b >= p.n) continue;
+      const Q4<T> xb = w.pk[b];
       T d[D], ray[D];
 #pragma unroll
       for (int k = 0; k < D; ++k) {
-        d[k] = xa[k] - w.pos[D * b + k];
+        d[k] = xa[k] - comp(xb, k);
         ray[k] = -d[k];
       }
       const T r2 = dot<T, D>(d, d);
       if (!(r2 < p.support2)) continue;
       covered += occupied<T, D>(ray, na, p.h);
       if (p.dscale != T(0)) {
+        const Q4<T> gb = w.g4[b];
         T W, gs;
         p.k.wg(sqrt(r2), W, gs);
         T gdd[D], sg[D];
 #pragma unroll
         for (int k = 0; k < D; ++k) {
           gdd[k] = d[k] * gs;
-          sg[k] = ga[k] + w.grho[D * b + k];
+          sg[k] = ga[k] + comp(gb, k);
         }
         const T radial = -dot<T, D>(d, gdd);
         const T proj = T(0.5) * dot<T, D>(sg, d);
-        const T contrast = (ra - w.rho[b]) - proj;
+        const T contrast = (ra - gb.w) - proj;
         const T coupling = contrast * radial / (r2 + T(1e-12));
-        diff.add(-p.dscale * w.vol[b] * coupling);
+        diff.add(-p.dscale * xb.w * coupling);
       }
     }
     const T nr = ra + p.dt * (w.rate[a] + diff.value());
     w.out_rho[a] = nr;
     if (!(nr > T(0)) || !isfinite(nr)) atomicOr(w.status, 2);
     const T la = w.lam[a];
-    w.surf[a] = (la < T(0.2)) || (la < T(0.75) && covered == 0);
+    const int sf = (la < T(0.2)) || (la < T(0.75) && covered == 0);
+    w.surf[a] = sf;
+    w.s4[a] = Q4<T>{w.mass[a], ra, sf ? T(1) : T(0), T(0)};
   }
 }
 
@@ -464,10 +518,10 @@ __global__ void p5_shift(DPP<T> p, DPW<T> w) {
     int64_t first_wall = -1;
     for (int64_t e = w.rowptr[a]; e < w.rowptr[a + 1]; ++e) {
       const int64_t b = w.ent[e] & kIdx;
-      T xb[D], d[D];
-      point<T, D>(p, w, b, xb);
+      const Q4<T> xb = w.pk[b];
+      T d[D];
 #pragma unroll
-      for (int k = 0; k < D; ++k) d[k] = xa[k] - xb[k];
+      for (int k = 0; k < D; ++k) d[k] = xa[k] - comp(xb, k);
       const T r2 = dot<T, D>(d, d);
       if (!(r2 < p.support2)) continue;
       T W, gs;
@@ -476,13 +530,14 @@ __global__ void p5_shift(DPP<T> p, DPW<T> w) {
       const T r4 = ratio * ratio * ratio * ratio;
       const T rep = (T(1) + T(0.2) * r4) * gs;  // repulsion = rep * d
       if (b < p.n) {
-        band = band || (w.surf[b] != 0);
-        const T c = w.mass[b] * rep / (ra + w.rho[b]);
+        const Q4<T> sb = w.s4[b];
+        band = band || (sb.z != T(0));
+        const T c = sb.x * rep / (ra + sb.y);
 #pragma unroll
         for (int k = 0; k < D; ++k) sc[k].add(c * d[k]);
       } else {
         const int64_t s = b - p.n;
-        const T wr = w.wrho[s];
+        const T wr = w.wv[s].w;
         const T c = (wr * p.dxd / (ra + wr)) * rep;
 #pragma unroll
         for (int k = 0; k < D; ++k) sc[k].add(c * d[k]);
@@ -521,11 +576,12 @@ __global__ void p5_shift(DPP<T> p, DPW<T> w) {
         const int64_t b = w.ent[e] & kIdx;
         if (b < p.n) continue;
         const int64_t s = b - p.n;
+        const Q4<T> xs = w.pk[b], wq = w.wq[s];
         T d[D], ns[D];
 #pragma unroll
         for (int k = 0; k < D; ++k) {
-          d[k] = xa[k] - w.wall[D * s + k];
-          ns[k] = w.wn[D * s + k];
+          d[k] = xa[k] - comp(xs, k);
+          ns[k] = comp(wq, k);
         }
         if (dot<T, D>(d, d) != nearest) continue;
         pinned = absv(dot<T, D>(tv, ns)) > tol;
@@ -566,18 +622,20 @@ int dp_dim(const tsph_delta_plus_params& p) { return p.dim == 3 ? 3 : 2; }
 
 struct Layout {
   size_t total;
-  size_t off[14];
+  size_t off[21];
 };
 
 Layout dp_layout(const tsph_delta_plus_params& p) {
   const size_t ts = p.dtype == TSPH_F64 ? 8 : 4;
   const size_t D = static_cast<size_t>(dp_dim(p));
   const size_t n = static_cast<size_t>(p.n_fluid), nw = static_cast<size_t>(p.n_wall);
-  const size_t sizes[14] = {n * ts, n * ts, n * ts, D * (D + 1) / 2 * n * ts, D * n * ts, D * n * ts, n * ts,
-                            n * ts, n * sizeof(int), nw * ts, nw * ts, D * nw * ts, sizeof(int), 0};
+  const size_t q4 = 4 * ts;
+  const size_t sizes[21] = {n * ts, n * ts, n * ts, D * (D + 1) / 2 * n * ts, D * n * ts, D * n * ts, n * ts,
+                            n * ts, n * sizeof(int), nw * ts, nw * ts, D * nw * ts, sizeof(int), 0,
+                            (n + nw) * q4, n * q4, n * q4, n * q4, n * q4, nw * q4, nw * q4};
   Layout L{};
   size_t used = 0;
-  for (int k = 0; k < 14; ++k) {
+  for (int k = 0; k < 21; ++k) {
     L.off[k] = used;
     used += align_up(sizes[k] > 0 ? sizes[k] : 1);
   }
@@ -647,9 +705,16 @@ int run_dp(const tsph_delta_plus_params& prm, const tsph_delta_plus_io& io, char
   w.wrho = reinterpret_cast<T*>(ws + L.off[10]);
   w.wn = reinterpret_cast<T*>(ws + L.off[11]);
   w.status = reinterpret_cast<int*>(ws + L.off[12]);
+  w.pk = reinterpret_cast<Q4<T>*>(ws + L.off[14]);
+  w.fv = reinterpret_cast<Q4<T>*>(ws + L.off[15]);
+  w.u4 = reinterpret_cast<Q4<T>*>(ws + L.off[16]);
+  w.g4 = reinterpret_cast<Q4<T>*>(ws + L.off[17]);
+  w.s4 = reinterpret_cast<Q4<T>*>(ws + L.off[18]);
+  w.wq = reinterpret_cast<Q4<T>*>(ws + L.off[19]);
+  w.wv = reinterpret_cast<Q4<T>*>(ws + L.off[20]);
   TSPH_CUDA_CHECK(cudaMemsetAsync(w.status, 0, sizeof(int), s));
   const unsigned g = grid_for(p.n, 128);
-  p0_state<T><<<grid_for(p.n, 256), 256, 0, s>>>(p, w);
+  p0_state<T, D><<<grid_for(p.n + p.nw, 256), 256, 0, s>>>(p, w);
   if (p.nw) p1_walls<T, D><<<grid_for(p.nw, 128), 128, 0, s>>>(p, w);
   p2_force<T, D><<<g, 128, 0, s>>>(p, w);
   p3_geometry<T, D><<<g, 128, 0, s>>>(p, w);
