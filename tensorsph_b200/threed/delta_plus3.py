@@ -137,3 +137,28 @@ def run_delta_plus_3d(cfg: DamBreak3DConfig, steps: int, *, obstacle=None, dtype
     run.rebuilds = cache.rebuilds
     run.final_positions, run.final_velocity, run.final_density = pos, vel, rho
     return run
+
+
+def main(argv=None) -> None:
+    """``python -m tensorsph_b200.threed.delta_plus3 --dx 0.0138 --steps 20``:
+    the dam break with the obstacle advanced by delta-plus steps on the current
+    GPU (two untimed steps first), one line of timing and state."""
+    import argparse
+    from ..engine import obstacle_case
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--dx", type=float, default=0.0138)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--fp64", action="store_true")
+    args = ap.parse_args(argv)
+    dtype = torch.float64 if args.fp64 else torch.float32
+    cfg, ob = obstacle_case(dx=args.dx)
+    host = delta_plus_case_3d(cfg, ob, dtype)
+    run_delta_plus_3d(cfg, 2, obstacle=ob, dtype=dtype, host_state=host)
+    run = run_delta_plus_3d(cfg, args.steps, obstacle=ob, dtype=dtype, host_state=host)
+    print(f"fluid {run.n_fluid} stations {run.n_wall} steps {run.steps} "
+          f"ms/step {1e3 * run.seconds / run.steps:.3f} rebuilds {run.rebuilds} "
+          f"max |rho/rho0 - 1| {max(run.density_deviation):.4g} front {run.front[-1]:.6f}")
+
+
+if __name__ == "__main__":
+    main()
