@@ -778,6 +778,13 @@ def checkpoint_leg(args, dev, cfg, obstacle, host, tuning):
     return out
 
 
+def workload_config(args) -> dict:
+    """The workload both arms' lines name."""
+    return {"workload": "3-D dam break with box obstacle: 1.2x1.0x0.55 m fluid in a 3.2x1.0x1.0 m tank, "
+                        f"obstacle 0.16x0.16x0.4 m, dx={args.dx:g}",
+            "shift_every": args.shift_every, "density_diffusion": 0.1}
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -788,8 +795,8 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        workload = (f"3-D dam break with obstacle (headline geometry), the reference's own CPU step "
-                    f"loop on the dx={args.ref_dx:g} rung")
+        workload = (f"each step one solver step of the reference's own CPU loop on the dx={args.ref_dx:g} "
+                    "rung of the same case (a full-size step takes ~40 s on the host)")
         if reference_available():
             r = reference_loop(args.ref_dx, args.steps, max(args.warmup, 1), args.shift_every)
             kind = "reference"
@@ -816,7 +823,7 @@ def main():
                 "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
                 "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded lattice)",
-                "config": {"workload": workload},
+                "config": {**workload_config(args), "reference_sample": workload},
                 "cpu_baseline": {"value": value, "unit": "fluid particle-updates/s", "cores": cores,
                                  "kind": kind, "sample": sample},
                 "e2e": {"value": value, "unit": "fluid particle-updates/s",
@@ -1011,11 +1018,8 @@ def main():
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded lattice, no dataset)",
-            "config": {"workload": "3-D dam break with box obstacle: 1.2x1.0x0.55 m fluid in a "
-                                   "3.2x1.0x1.0 m tank, obstacle 0.16x0.16x0.4 m, dx="
-                                   f"{args.dx:g}", "fluid_particles": nf, "wall_particles": nw,
+            "config": {**workload_config(args), "fluid_particles": nf, "wall_particles": nw,
                        "solver_steps_per_step": chunk, "ms_per_solver_step": ms_solver,
-                       "shift_every": args.shift_every, "density_diffusion": 0.1,
                        "pair_skin_factor": cfg.pair_skin_factor,
                        "tuning": None if tuning is None else tuning["best"],
                        "pairs": "FP32 pair arithmetic, FP64 positions/velocities/meters",

@@ -19,8 +19,11 @@
 //                 (l_a - l_b) - (c_b - c_a) * cell, exact to the FP32 rounding
 //                 of the two local coordinates
 //   vb   float4   FP32 velocity + volume m/rho;  pr, rho, pq = p/rho^2
-//   nbr  uint32[maxnb][rows] k-major rows (thread a reads nbr[k*rows + a]),
-//        entry = row index << 6 | cell offset (dx+1) | (dy+1) << 2 | (dz+1) << 4
+//   nbr  uint32 rows in groups of four: entry k of row a at
+//        ((k >> 2) * rows + a) * 4 + (k & 3), so a thread reads four entries
+//        with one 16-byte load and a warp's loads of one group are contiguous;
+//        entry = row index << 6 | cell offset (dx+1) | (dy+1) << 2 | (dz+1) << 4,
+//        the last group of a row padded with null-row entries
 // Each case rebuilds its rows only when its own particles leave its own skin
 // and the order of its block depends on its own particles only, so a case
 // evolves bit for bit the same alone or batched with others.  Retiring a case
@@ -387,28 +390,54 @@ __device__ __forceinline__ uint32_t ld_entry(const uint32_t* p) {
   return v;
 }
 
+// Index of entry k of row a (groups of four entries per row).
+__host__ __device__ __forceinline__ int64_t entry_at(int64_t rows, int64_t a, int k) {
+  return ((static_cast<int64_t>(k >> 2) * rows + a) << 2) + (k & 3);
+}
+
+// The four entries of group g of row a, not allocated in L1.
+__device__ __forceinline__ uint4 ld_group(const uint32_t* nbr, int64_t rows, int64_t a, int g) {
+  const uint32_t* p = nbr + ((static_cast<int64_t>(g) * rows + a) << 2);
+  uint4 v;
+  asm volatile("ld.global.L1::no_allocate.v4.u32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(p));
+  return v;
+}
+
 // 1/x for the regularised pair denominators r^2 + eps (x >= eps > 0): the
 // hardware reciprocal, within 2 ulp.
 __device__ __forceinline__ float rcp_pair(float x) { return __fdividef(1.f, x); }
 
-// Walk row a in batches of KB entries (padded with null-row entries); the loads of a
-// batch are all issued before any use.  KB (the batch depth: neighbour
-// records in flight per thread) is a tuning parameter of the hot kernels.
+// Walk row a in batches of KB entries (KB a multiple of 4: whole groups; the
+// last group is padded with null-row entries by the builder, groups past the
+// row read as null-row entries); the loads of a batch are all issued before
+// any use.  KB (the batch depth: neighbour records in flight per thread) is
+// a tuning parameter of the hot kernels.
 template <int KB = kBatch, class Body>
 __device__ __forceinline__ void walk_row(const Dev& e, int64_t a, Body&& body) {
-  const int n = e.cnt[a];
-  const uint32_t* row = e.nbr + a;
+  static_assert(KB % 4 == 0, "batches of whole groups");
+  constexpr int G = KB / 4;
+  const int groups = (e.cnt[a] + 3) >> 2;
+  const uint4 padg = make_uint4(e.pad, e.pad, e.pad, e.pad);
   // the entries of the next batch are loaded while the current one is used
-  uint32_t cur[KB], nxt[KB];
+  uint4 cur[G], nxt[G];
 #pragma unroll
-  for (int j = 0; j < KB; ++j) cur[j] = j < n ? ld_entry(row + static_cast<int64_t>(j) * e.rows) : e.pad;
-  for (int k = 0; k < n; k += KB) {
+  for (int j = 0; j < G; ++j) cur[j] = j < groups ? ld_group(e.nbr, e.rows, a, j) : padg;
+  for (int g = 0; g < groups; g += G) {
 #pragma unroll
-    for (int j = 0; j < KB; ++j)
-      nxt[j] = (k + KB + j < n) ? ld_entry(row + static_cast<int64_t>(k + KB + j) * e.rows) : e.pad;
-    body(cur);
+    for (int j = 0; j < G; ++j) nxt[j] = (g + G + j < groups) ? ld_group(e.nbr, e.rows, a, g + G + j) : padg;
+    uint32_t ent[KB];
 #pragma unroll
-    for (int j = 0; j < KB; ++j) cur[j] = nxt[j];
+    for (int j = 0; j < G; ++j) {
+      ent[4 * j] = cur[j].x;
+      ent[4 * j + 1] = cur[j].y;
+      ent[4 * j + 2] = cur[j].z;
+      ent[4 * j + 3] = cur[j].w;
+    }
+    body(ent);
+#pragma unroll
+    for (int j = 0; j < G; ++j) cur[j] = nxt[j];
   }
 }
 
@@ -581,7 +610,7 @@ __global__ void k_rows(Dev e) {
                 }
                 if (b < fe && b != a && ddx * ddx + ddy * ddy + ddz * ddz <= rc2) {
                   if (count < e.maxnb)
-                    e.nbr[static_cast<int64_t>(count) * e.rows + a] = (static_cast<uint32_t>(b) << kCodeBits) | code;
+                    e.nbr[entry_at(e.rows, a, count)] = (static_cast<uint32_t>(b) << kCodeBits) | code;
                   ++count;
                 }
               }
@@ -601,7 +630,7 @@ __global__ void k_rows(Dev e) {
                   const double ddx = pa.x - pb[j].x, ddy = pa.y - pb[j].y, ddz = pa.z - pb[j].z;
                   if (w0 + j < we && ddx * ddx + ddy * ddy + ddz * ddz <= rc2) {
                     if (count < e.maxnb)
-                      e.nbr[static_cast<int64_t>(count) * e.rows + a] = (static_cast<uint32_t>(b) << kCodeBits) | code;
+                      e.nbr[entry_at(e.rows, a, count)] = (static_cast<uint32_t>(b) << kCodeBits) | code;
                     ++count;
                   }
                 }
@@ -616,6 +645,8 @@ __global__ void k_rows(Dev e) {
       atomicOr(&ctl.status, 1);
     }
     e.cnt[a] = count < e.maxnb ? count : e.maxnb;
+    // the rest of the last group: null-row entries (maxnb is a multiple of 4)
+    for (int k = count; k < e.maxnb && (k & 3); ++k) e.nbr[entry_at(e.rows, a, k)] = e.pad;
     atomicMax(&ctl.row_max, static_cast<unsigned long long>(count));
     if (fluid_row && C.csf) {
       // the CSF fit rows: fluid particles within 4h + skin
@@ -850,7 +881,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_closure_pass(const __grid_constan
     const bool all = C.closure_all != 0;
     CSum<float> num, den;
     for (int k = 0; k < n; ++k) {
-      const uint32_t ent = ld_entry(e.nbr + a + static_cast<int64_t>(k) * e.rows);
+      const uint32_t ent = ld_entry(e.nbr + entry_at(e.rows, a, k));
       const int b = static_cast<int>(ent >> kCodeBits);
       if (b >= NF || !(all || known_in[b])) continue;
       const float4 lb = e.lp[b];
@@ -1283,10 +1314,9 @@ struct KD {
 __device__ __forceinline__ bool row_nearest_wall(const Dev& e, int a, double ax, double ay, double& d2, double& nx,
                                                  double& ny) {
   const int n = e.cnt[a];
-  const uint32_t* row = e.nbr + a;
   bool any = false;
   for (int k = 0; k < n; ++k) {
-    const uint32_t b = ld_entry(row + static_cast<int64_t>(k) * e.rows) >> kCodeBits;
+    const uint32_t b = ld_entry(e.nbr + entry_at(e.rows, a, k)) >> kCodeBits;
     if (b < static_cast<uint32_t>(e.NF) || b >= static_cast<uint32_t>(e.null_row)) continue;
     const double2 pw = ld_xy(e.pos, static_cast<int>(b));
     const double dx = ax - pw.x, dy = ay - pw.y, r2 = dx * dx + dy * dy;
@@ -1314,20 +1344,18 @@ __device__ __forceinline__ KD kernel_d(double dx, double dy, const CaseDev& C) {
 // entries come with ok = false and b = a.
 template <class Body>
 __device__ __forceinline__ void fluid_row(const Dev& e, int a, Body&& body) {
-  const int n = e.cnt[a];
-  const uint32_t* row = e.nbr + a;
-  uint32_t nxt[4];
-#pragma unroll
-  for (int j = 0; j < 4; ++j) nxt[j] = j < n ? (ld_entry(row + static_cast<int64_t>(j) * e.rows) >> kCodeBits) : 0xffffffffu;
-  for (int k = 0; k < n; k += 4) {
+  const int groups = (e.cnt[a] + 3) >> 2;
+  uint4 nxt = groups > 0 ? ld_group(e.nbr, e.rows, a, 0) : make_uint4(e.pad, e.pad, e.pad, e.pad);
+  for (int g = 0; g < groups; ++g) {
+    const uint32_t v4[4] = {nxt.x, nxt.y, nxt.z, nxt.w};
+    nxt = g + 1 < groups ? ld_group(e.nbr, e.rows, a, g + 1) : make_uint4(e.pad, e.pad, e.pad, e.pad);
     int b[4];
     bool ok[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      const uint32_t v = nxt[j];
+      const uint32_t v = v4[j] >> kCodeBits;
       ok[j] = v < static_cast<uint32_t>(e.NF);
       b[j] = ok[j] ? static_cast<int>(v) : a;
-      nxt[j] = (k + 4 + j < n) ? (ld_entry(row + static_cast<int64_t>(k + 4 + j) * e.rows) >> kCodeBits) : 0xffffffffu;
     }
     body(b, ok);
   }
@@ -1846,7 +1874,7 @@ __global__ void k_csf_final(const __grid_constant__ Dev e) {
         double sw = 0.0;  // sum of W over the wall particles (all within 2h are in the row)
         const int cnt = e.cnt[a];
         for (int k = 0; k < cnt; ++k) {
-          const uint32_t b = ld_entry(e.nbr + a + static_cast<int64_t>(k) * e.rows) >> kCodeBits;
+          const uint32_t b = ld_entry(e.nbr + entry_at(e.rows, a, k)) >> kCodeBits;
           if (b < static_cast<uint32_t>(e.NF) || b >= static_cast<uint32_t>(e.null_row)) continue;
           const double2 pw = ld_xy(e.pos, static_cast<int>(b));
           sw += kernel_d(pa.x - pw.x, pa.y - pw.y, C).w;
@@ -2556,7 +2584,7 @@ __global__ void k_remap(Dev e, int fluid_from, int wall_from, int df, int dw, in
     e.home[a] -= dkeys;
     const int n = e.cnt[a];
     for (int k = 0; k < n; ++k) {
-      uint32_t& ent = e.nbr[static_cast<int64_t>(k) * e.rows + a];
+      uint32_t& ent = e.nbr[entry_at(e.rows, a, k)];
       const uint32_t b = ent >> kCodeBits;
       const uint32_t nb = b < static_cast<uint32_t>(e.NF) ? b - df : b - dw;
       ent = (nb << kCodeBits) | (ent & kCodeMask);
@@ -2633,6 +2661,9 @@ struct tsph_engine {
 namespace tsph {
 namespace {
 
+// Row capacity in whole groups of four entries.
+int64_t row_capacity(int64_t max_neighbors) { return (max_neighbors + 3) / 4 * 4; }
+
 // Carve the arena; with base == nullptr only the size is computed.
 size_t carve(const tsph_engine_params& p, Dev* d, char* base, CaseDev** cases, char** radix_scratch) {
   size_t used = 0;
@@ -2678,7 +2709,7 @@ size_t carve(const tsph_engine_params& p, Dev* d, char* base, CaseDev** cases, c
   t.csf_hist = static_cast<unsigned int*>(take(static_cast<size_t>(p.max_cases) * 256 * sizeof(unsigned int)));
   t.nbr4 = static_cast<uint32_t*>(take(static_cast<size_t>(p.max_fit_neighbors) * NF * sizeof(uint32_t)));
   t.cnt4 = static_cast<int32_t*>(take(NF * sizeof(int32_t)));
-  t.nbr = static_cast<uint32_t*>(take(static_cast<size_t>(p.max_neighbors) * N * sizeof(uint32_t)));
+  t.nbr = static_cast<uint32_t*>(take(static_cast<size_t>(row_capacity(p.max_neighbors)) * N * sizeof(uint32_t)));
   t.cnt = static_cast<int32_t*>(take(N * sizeof(int32_t)));
   t.ob_rows = static_cast<int32_t*>(take(std::max<int64_t>(p.max_obstacle, 1) * sizeof(int32_t)));
   t.fstart = static_cast<int32_t*>(take(p.max_cells * sizeof(int32_t)));
@@ -3237,7 +3268,7 @@ int tsph_engine_create(const tsph_engine_params* prm, void* arena, int64_t arena
   d.NF = static_cast<int>(prm->max_fluid);
   d.nf = d.nw = d.n_ob = 0;
   d.n_slots = static_cast<int>(prm->max_cases);
-  d.maxnb = static_cast<int>(prm->max_neighbors);
+  d.maxnb = static_cast<int>(row_capacity(prm->max_neighbors));
   d.maxfit = static_cast<int>(prm->max_fit_neighbors);
   d.diag_ring = static_cast<int>(prm->diag_ring);
   d.shift_slot = 0;
@@ -3365,10 +3396,10 @@ int tsph_engine_remove_case(tsph_engine* E, int64_t case_id, tsph_stream stream)
     if ((rc = move_down(a.p, a.e, fb, fe, ftail, stage, stage_bytes, s))) return rc;
   for (const Arr& a : wall_arrays)
     if ((rc = move_down(a.p, a.e, W0 + wb, W0 + we, wtail, stage, stage_bytes, s))) return rc;
-  for (int k = 0; k < d.maxnb; ++k) {
-    uint32_t* col = d.nbr + static_cast<int64_t>(k) * d.rows;
-    if ((rc = move_down(col, sizeof(uint32_t), fb, fe, ftail, stage, stage_bytes, s))) return rc;
-    if ((rc = move_down(col, sizeof(uint32_t), W0 + wb, W0 + we, wtail, stage, stage_bytes, s))) return rc;
+  for (int g = 0; g < d.maxnb / 4; ++g) {
+    uint4* col = reinterpret_cast<uint4*>(d.nbr) + static_cast<int64_t>(g) * d.rows;
+    if ((rc = move_down(col, sizeof(uint4), fb, fe, ftail, stage, stage_bytes, s))) return rc;
+    if ((rc = move_down(col, sizeof(uint4), W0 + wb, W0 + we, wtail, stage, stage_bytes, s))) return rc;
   }
   if (d.has_csf) {
     if ((rc = move_down(d.cnt4, sizeof(int32_t), fb, fe, ftail, stage, stage_bytes, s))) return rc;
