@@ -277,22 +277,69 @@ __device__ __forceinline__ void bitonic_smem(uint32_t* a, int p2) {
 }
 
 // Rows of kShortRow + 1 .. kMidRow entries (the symmetric rows of a 3-D
-// pair list at h = 2 dx hold ~330): a small block per row, so that many rows
-// are in flight on every SM between the network's barriers.
-__global__ void __launch_bounds__(128) segsort_mid(uint32_t* __restrict__ vals, const int64_t* __restrict__ rowptr,
+// pair list at h = 2 dx hold ~330): one warp per row, a bitonic network over
+// the row padded to p2 = 32 E entries held in registers, entry i = r * 32 +
+// lane in register r of its lane.  Stages at distances below 32 exchange
+// across lanes with shuffles, the others compare registers of one lane.
+template <int E>
+__device__ __forceinline__ void warp_bitonic(uint32_t* __restrict__ vals, int64_t beg, int64_t len) {
+  const int lane = threadIdx.x & 31;
+  uint32_t v[E];
+#pragma unroll
+  for (int r = 0; r < E; ++r) {
+    const int64_t i = static_cast<int64_t>(r) * 32 + lane;
+    v[r] = i < len ? vals[beg + i] : 0xffffffffu;
+  }
+#pragma unroll
+  for (int k = 2; k <= 32 * E; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j < 32) {
+        const bool lower = (lane & j) == 0;
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+          const int i = r * 32 + lane;
+          const bool asc = (i & k) == 0;
+          const uint32_t o = __shfl_xor_sync(0xffffffffu, v[r], j);
+          v[r] = (lower == asc) ? min(v[r], o) : max(v[r], o);
+        }
+      } else {
+        const int jr = j >> 5;
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+          if (r & jr) continue;
+          const int i = r * 32 + lane;
+          const bool asc = (i & k) == 0;
+          const uint32_t a = v[r], b = v[r | jr];
+          v[r] = asc ? min(a, b) : max(a, b);
+          v[r | jr] = asc ? max(a, b) : min(a, b);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < E; ++r) {
+    const int64_t i = static_cast<int64_t>(r) * 32 + lane;
+    if (i < len) vals[beg + i] = v[r];
+  }
+}
+
+__global__ void __launch_bounds__(256) segsort_mid(uint32_t* __restrict__ vals, const int64_t* __restrict__ rowptr,
                                                    SegsortLists lists) {
-  __shared__ uint32_t buf[kMidRow];
   const int64_t count = lists.counts[2];
-  for (int64_t q = blockIdx.x; q < count; q += gridDim.x) {
+  const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t q = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); q < count;
+       q += warps) {
     const int64_t r = lists.mid[q];
     const int64_t beg = rowptr[r], len = rowptr[r + 1] - beg;
-    int p2 = 1;
-    while (p2 < len) p2 <<= 1;
-    for (int t = threadIdx.x; t < p2; t += blockDim.x) buf[t] = t < len ? vals[beg + t] : 0xffffffffu;
-    __syncthreads();
-    bitonic_smem(buf, p2);
-    for (int t = threadIdx.x; t < len; t += blockDim.x) vals[beg + t] = buf[t];
-    __syncthreads();
+    if (len <= 128)
+      warp_bitonic<4>(vals, beg, len);
+    else if (len <= 256)
+      warp_bitonic<8>(vals, beg, len);
+    else if (len <= 512)
+      warp_bitonic<16>(vals, beg, len);
+    else
+      warp_bitonic<32>(vals, beg, len);
   }
 }
 
@@ -363,7 +410,7 @@ int segmented_sort_u32(uint32_t* vals, const int64_t* rowptr, int64_t rows, void
   unsigned g = grid_for(rows, kSortWarps, 148 * 16);
   segsort_short<<<g, kSortWarps * 32, 0, s>>>(vals, rowptr, rows, lists);
   TSPH_LAUNCH_CHECK();
-  segsort_mid<<<148 * 12, 128, 0, s>>>(vals, rowptr, lists);
+  segsort_mid<<<148 * 8, 256, 0, s>>>(vals, rowptr, lists);
   TSPH_LAUNCH_CHECK();
   segsort_medium<<<148 * 2, 512, 0, s>>>(vals, rowptr, lists);
   TSPH_LAUNCH_CHECK();
