@@ -698,8 +698,9 @@ int tsph_engine_clock(tsph_engine* engine, int64_t case_id, double* clock, tsph_
 /* Threads per block of the pair kernels: 64, 128 (default) or 256.  A tuning
  * knob (results do not depend on it); the step graph is re-captured. */
 int tsph_engine_set_block(tsph_engine* engine, int64_t threads);
-/* Neighbour records in flight per thread in the pair kernels: 4 (default) or
- * 8.  A tuning knob (results do not depend on it); the graph is re-captured. */
+/* Neighbour records in flight per thread in the pair kernels: 4 (default), 8
+ * or 16 (whole groups of row entries).  A tuning knob (results do not depend
+ * on it); the graph is re-captured. */
 int tsph_engine_set_batch(tsph_engine* engine, int64_t depth);
 /* Entries of the current neighbour rows: out[0] over the fluid rows, out[1]
  * over the wall rows (synchronises the stream).  The pair passes' work per

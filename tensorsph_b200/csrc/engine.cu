@@ -53,10 +53,10 @@ constexpr int kMaxBlock = 256;  // largest block the kernels are built for
 constexpr int kDiag = 30;
 constexpr int kBatch = 4;
 // Neighbour records in flight in the shifting passes, measured on the 2 M
-// case: depth 8 is the faster for both (concentration 0.272 against
-// 0.286 ms, gradient 0.369 against 0.416 ms before the rows were grouped)
-constexpr int kConcBatch = 8;
-constexpr int kGradBatch = 8;
+// case with grouped rows: concentration 0.260 ms at 16, 0.270 at 8, 0.286
+// at 4; gradient 0.317 at 16, 0.328 at 8
+constexpr int kConcBatch = 16;
+constexpr int kGradBatch = 16;
 constexpr int kCodeBits = 6;                               // cell-offset code bits of a row entry
 constexpr uint32_t kCodeMask = (1u << kCodeBits) - 1;
 constexpr uint32_t kSelfCode = 0x15u;                      // offset (0, 0, 0): fields (1, 1, 1)
@@ -2904,8 +2904,10 @@ int enqueue_step(tsph_engine* E, cudaStream_t s, cudaEvent_t* marks = nullptr, b
   const int B = E->block;
   const unsigned g = grid_for(d.nf, B);
   const bool one = E->order.size() == 1;
-  const bool deep = E->batch == 8;
-#define TSPH_PICK(K) (one ? (deep ? K<true, 8> : K<true, 4>) : (deep ? K<false, 8> : K<false, 4>))
+  const int depth = E->batch;
+#define TSPH_PICK(K)                                                                     \
+  (one ? (depth == 16 ? K<true, 16> : (depth == 8 ? K<true, 8> : K<true, 4>))            \
+       : (depth == 16 ? K<false, 16> : (depth == 8 ? K<false, 8> : K<false, 4>)))
   TSPH_PICK(k_density)<<<g, B, 0, s>>>(d);
   if (d.has_comp) k_compression_average<<<d.n_slots, 1024, 0, s>>>(d);
   if (d.has_psi) TSPH_PICK(k_density_gradient)<<<g, B, 0, s>>>(d);
@@ -3663,7 +3665,7 @@ int tsph_engine_set_block(tsph_engine* E, int64_t threads) {
 }
 
 int tsph_engine_set_batch(tsph_engine* E, int64_t depth) {
-  if (!E || (depth != 4 && depth != 8)) return TSPH_ERR_ARG;
+  if (!E || (depth != 4 && depth != 8 && depth != 16)) return TSPH_ERR_ARG;
   if (depth != E->batch) {
     E->batch = static_cast<int>(depth);
     invalidate_graph(E);

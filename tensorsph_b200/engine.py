@@ -574,7 +574,7 @@ class BatchEngine:
                    "tsph_engine_set_block")
 
     def set_batch(self, depth: int) -> None:
-        """Neighbour records in flight per thread (4 or 8): a tuning knob."""
+        """Neighbour records in flight per thread (4, 8 or 16): a tuning knob."""
         _lib.check(_lib.lib().tsph_engine_set_batch(self._handle, int(depth)),
                    "tsph_engine_set_batch")
 
@@ -767,7 +767,7 @@ class DamBreak3DEngine(BatchEngine):
 
 
 def tune_single_case(cfg: DamBreak3DConfig, *, obstacle=None, shift_every: int = 0, host_state=None,
-                     skins=(0.1, 0.15, 0.25), blocks=(128, 256), batches=(4, 8), steps: int = 60,
+                     skins=(0.1, 0.15, 0.25), blocks=(128, 256), batches=(4, 8, 16), steps: int = 60,
                      device=None, cache: bool = True) -> dict:
     """Autotune one 3-D case by timing: the Verlet skin (which sets the cell edge
     2h + skin and how often lists are rebuilt), the pair kernels' block size and

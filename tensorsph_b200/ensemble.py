@@ -112,7 +112,7 @@ def run_plain(specs, steps: int, *, warmup: int = 3, block: int = 128, batch: in
             "seconds": total_t, "updates_per_s": total_u / total_t}
 
 
-def autotune(draws, *, blocks=(64, 128, 256), batches=(4, 8), skins=(0.15, 0.25, 0.4),
+def autotune(draws, *, blocks=(64, 128, 256), batches=(4, 8, 16), skins=(0.15, 0.25, 0.4),
              steps: int = 30, warmup: int = 10, device=None, cache: bool = True) -> dict:
     """Time each (block, batch depth, skin) on the sample ``draws`` and return
     the fastest.
