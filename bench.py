@@ -74,6 +74,10 @@ def parse():
     ap.add_argument("--shift-every", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--skin", type=float, default=0.0,
+                    help="with --no-tune: the list skin in h (0: the configuration's 0.25)")
+    ap.add_argument("--block", type=int, default=0, help="with --no-tune: pair-kernel block size (0: 128)")
+    ap.add_argument("--batch", type=int, default=0, help="with --no-tune: batch depth 4, 8 or 16 (0: 4)")
     ap.add_argument("--cpu-sample-steps", type=int, default=6)
     ap.add_argument("--ensemble-cases", type=int, default=256)
     ap.add_argument("--ensemble-steps", type=int, default=100)
@@ -850,6 +854,12 @@ def main():
         from tensorsph_b200.engine import tune_single_case
         tuning = tune_single_case(cfg, obstacle=obstacle, shift_every=args.shift_every,
                                   host_state=host, device=dev)
+        cfg = replace(cfg, pair_skin_factor=tuning["best"]["skin_factor"])
+    elif args.skin or args.block or args.batch:
+        # a fixed choice (for profiling the tuned configuration without tuning)
+        from dataclasses import replace
+        tuning = {"best": {"skin_factor": args.skin or cfg.pair_skin_factor, "block": args.block or 128,
+                           "batch": args.batch or 4}, "trials": [], "cached": None, "fixed": True}
         cfg = replace(cfg, pair_skin_factor=tuning["best"]["skin_factor"])
     solver_steps = args.steps * chunk
     eng = DamBreak3DEngine(cfg, obstacle=obstacle, shift_every=args.shift_every, host_state=host,
