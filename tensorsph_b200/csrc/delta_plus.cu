@@ -50,6 +50,32 @@ __device__ __forceinline__ T comp(const Q4<T>& q, int k) {
   return k == 0 ? q.x : (k == 1 ? q.y : q.z);
 }
 
+// A row's sum.  FP64 adds term by term.  FP32 adds kChunk terms plainly into
+// a partial that then joins a compensated total (flush), so the compensation
+// is paid once per chunk instead of once per term; the passes flush all their
+// sums together every kChunk in-support neighbours and at the row's end.
+constexpr int kChunk = 8;
+
+template <class T>
+struct RowSum {
+  T s = T(0);
+  __device__ __forceinline__ void add(T x) { s += x; }
+  __device__ __forceinline__ void flush() {}
+  __device__ __forceinline__ T value() const { return s; }
+};
+
+template <>
+struct RowSum<float> {
+  CSum<float> c;
+  float p = 0.f;
+  __device__ __forceinline__ void add(float x) { p += x; }
+  __device__ __forceinline__ void flush() {
+    c.add(p);
+    p = 0.f;
+  }
+  __device__ __forceinline__ float value() const { return c.value(); }
+};
+
 // packed symmetric D x D: 2-D (00, 01, 11), 3-D (00, 01, 02, 11, 12, 22)
 template <int D>
 struct Sym {
@@ -176,7 +202,7 @@ __global__ void p1_walls(DPP<T> p, DPW<T> w) {
       nv[k] = nv[k] / nn;
       w.wn[D * s + k] = nv[k];
     }
-    CSum<T> num, den;
+    RowSum<T> num, den;
     int pairs = 0;
     for (int64_t e = w.rowptr[r]; e < w.rowptr[r + 1]; ++e) {
       const int64_t f = w.ent[e] & kIdx;
@@ -190,8 +216,13 @@ __global__ void p1_walls(DPP<T> p, DPW<T> w) {
       const T W = p.k.w(sqrt(r2));
       num.add(W * (w.fv[f].w + w.rho[f] * p.g * d[1]));
       den.add(W);
-      ++pairs;
+      if (++pairs % kChunk == 0) {
+        num.flush();
+        den.flush();
+      }
     }
+    num.flush();
+    den.flush();
     const T dd = den.value();
     const T wp = num.value() / (dd > p.tiny ? dd : p.tiny);
     const T wr = p.rho0 + wp / p.c2;
@@ -204,7 +235,8 @@ __global__ void p1_walls(DPP<T> p, DPW<T> w) {
     for (int k = 0; k < D; ++k) wvel[k] = w.wall_vel[D * s + k];
     w.wq[s] = Q4<T>{nv[0], nv[1], D == 3 ? nv[D - 1] : T(0), wp};
     w.wv[s] = Q4<T>{wvel[0], wvel[1], D == 3 ? wvel[D - 1] : T(0), wr};
-    CSum<T> rc[D];
+    RowSum<T> rc[D];
+    int pend = 0;
     for (int64_t e = w.rowptr[r]; e < w.rowptr[r + 1]; ++e) {
       const int64_t f = w.ent[e] & kIdx;
       if (f >= p.n) continue;
@@ -232,9 +264,17 @@ __global__ void p1_walls(DPP<T> p, DPW<T> w) {
       const T c = -(xf.w * p.dxd * twice) * ng;
 #pragma unroll
       for (int k = 0; k < D; ++k) rc[k].add(-(c * tv[k]));
+      if (++pend == kChunk) {
+#pragma unroll
+        for (int k = 0; k < D; ++k) rc[k].flush();
+        pend = 0;
+      }
     }
 #pragma unroll
-    for (int k = 0; k < D; ++k) w.reaction[D * s + k] = rc[k].value();
+    for (int k = 0; k < D; ++k) {
+      rc[k].flush();
+      w.reaction[D * s + k] = rc[k].value();
+    }
   }
 }
 
@@ -249,7 +289,8 @@ __global__ void p2_force(DPP<T> p, DPW<T> w) {
       va[k] = w.vel[D * a + k];
     }
     const T Va = w.vol[a], pa = w.p[a], ra = w.rho[a];
-    CSum<T> fc[D], mom[S::N];
+    RowSum<T> fc[D], mom[S::N];
+    int pend = 0;
     for (int64_t e = w.rowptr[a]; e < w.rowptr[a + 1]; ++e) {
       const int64_t b = w.ent[e] & kIdx;
       const Q4<T> xb = w.pk[b];
@@ -302,7 +343,18 @@ __global__ void p2_force(DPP<T> p, DPW<T> w) {
 #pragma unroll
         for (int k = 0; k < D; ++k) fc[k].add(c * tv[k]);
       }
+      if (++pend == kChunk) {
+#pragma unroll
+        for (int k = 0; k < D; ++k) fc[k].flush();
+#pragma unroll
+        for (int q = 0; q < S::N; ++q) mom[q].flush();
+        pend = 0;
+      }
     }
+#pragma unroll
+    for (int k = 0; k < D; ++k) fc[k].flush();
+#pragma unroll
+    for (int q = 0; q < S::N; ++q) mom[q].flush();
     const T m = w.mass[a];
     T un[D];
 #pragma unroll
@@ -376,7 +428,8 @@ __global__ void p3_geometry(DPP<T> p, DPW<T> w) {
       ua[k] = w.out_vel[D * a + k];
     }
     const T ra = w.rho[a], la = w.lam[a];
-    CSum<T> div, gr[D], gl[D];
+    RowSum<T> div, gr[D], gl[D];
+    int pend = 0;
     for (int64_t e = w.rowptr[a]; e < w.rowptr[a + 1]; ++e) {
       const int64_t b = w.ent[e] & kIdx;
       const Q4<T> xb = w.pk[b];
@@ -415,6 +468,21 @@ __global__ void p3_geometry(DPP<T> p, DPW<T> w) {
         const T ns = dot<T, D>(rel, nv);
         div.add(T(2) * p.dxd * ns * dot<T, D>(nv, gv));
       }
+      if (++pend == kChunk) {
+        div.flush();
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+          gr[k].flush();
+          gl[k].flush();
+        }
+        pend = 0;
+      }
+    }
+    div.flush();
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      gr[k].flush();
+      gl[k].flush();
     }
     const T* inv = w.inv + S::N * a;
     T sr[D], sl[D], outr[D], outl[D];
@@ -462,8 +530,8 @@ __global__ void p4_density(DPP<T> p, DPW<T> w) {
       na[k] = w.nrm[D * a + k];
     }
     const T ra = w.rho[a];
-    CSum<T> diff;
-    int covered = 0;
+    RowSum<T> diff;
+    int covered = 0, pend = 0;
     for (int64_t e = w.rowptr[a]; e < w.rowptr[a + 1]; ++e) {
       const int64_t b = w.ent[e] & kIdx;
       if (b >= p.n) continue;
@@ -492,8 +560,13 @@ __global__ void p4_density(DPP<T> p, DPW<T> w) {
         const T contrast = (ra - gb.w) - proj;
         const T coupling = contrast * radial / (r2 + T(1e-12));
         diff.add(-p.dscale * xb.w * coupling);
+        if (++pend == kChunk) {
+          diff.flush();
+          pend = 0;
+        }
       }
     }
+    diff.flush();
     const T nr = ra + p.dt * (w.rate[a] + diff.value());
     w.out_rho[a] = nr;
     if (!(nr > T(0)) || !isfinite(nr)) atomicOr(w.status, 2);
@@ -512,7 +585,8 @@ __global__ void p5_shift(DPP<T> p, DPW<T> w) {
     for (int k = 0; k < D; ++k) xa[k] = w.pos[D * a + k];
     const T ra = w.rho[a];
     bool band = w.surf[a] != 0;
-    CSum<T> sc[D];
+    RowSum<T> sc[D];
+    int pend = 0;
     T nearest = T(0);
     bool has_wall = false;
     int64_t first_wall = -1;
@@ -547,7 +621,14 @@ __global__ void p5_shift(DPP<T> p, DPW<T> w) {
         }
         has_wall = true;
       }
+      if (++pend == kChunk) {
+#pragma unroll
+        for (int k = 0; k < D; ++k) sc[k].flush();
+        pend = 0;
+      }
     }
+#pragma unroll
+    for (int k = 0; k < D; ++k) sc[k].flush();
     T raw[D], na[D], sh[D];
 #pragma unroll
     for (int k = 0; k < D; ++k) {
