@@ -171,3 +171,45 @@ def test_resumed_record_equals_uninterrupted_record():
     np.testing.assert_allclose(part["sph_impulse"], whole["sph_impulse"], rtol=1e-14)
     np.testing.assert_allclose(part["clamp_impulse"], whole["clamp_impulse"], rtol=1e-14)
     assert len(whole["obstacle_force"]) == 20 and len(whole["times"]) == 6
+
+
+def test_resumed_adaptive_record_equals_uninterrupted_record():
+    """The same for an adaptive run: samples are the output_every-th steps and
+    the final one with their times from the rows (column 25), the step range
+    from column 27 and the Courant peak from columns 26 and 1 over every row,
+    and a checkpoint carries them (and the rebuild count) into the resumed
+    record; its dt is next_dt's step after the checkpointed one."""
+    from dataclasses import replace
+    from tensorsph_b200.dam_break_3d import DamBreak3DConfig
+    from tensorsph_b200.engine import DIAG_FIELDS, _AdaptiveRecord
+    cfg = replace(DamBreak3DConfig(steps=12, output_every=4, dt=1e-3), adaptive_dt=True)
+    final = 17
+    g = torch.Generator().manual_seed(9)
+    rows = torch.rand((final + 1, len(DIAG_FIELDS)), generator=g, dtype=torch.float64)
+    cum = (8, 9, 10, 14, 20, 21, 22, 23, 24)
+    rows[:, [8, 9, 10]] = torch.randint(0, 3, (final + 1, 3), generator=g).double()
+    rows[:, cum] = rows[:, cum].cumsum(0)
+    rows[:, 26] = 0.9e-3 * (1.0 + 0.1 * torch.rand(final + 1, generator=g, dtype=torch.float64))
+    rows[:, 27] = rows[:, 26]
+    rows[:, 25] = torch.cat((torch.zeros(1, dtype=torch.float64), rows[:-1, 26].cumsum(0)))
+    whole = _AdaptiveRecord(cfg, 0, None, 100, 7.0).collect(rows, final, final=final)
+    assert [t for t in whole["times"]] == [float(rows[k, 25]) for k in (0, 4, 8, 12, 16, 17)]
+    assert whole["dt_min"] == float(rows[:, 27].min()) and whole["dt_max"] == float(rows[:, 27].max())
+    h = cfg.h_factor * cfg.dx
+    assert whole["courant"] == pytest.approx(float((rows[:, 26] * (cfg.sound_speed + rows[:, 1])).max()) / h,
+                                             rel=1e-15)
+    assert whole["rebuilds"] == int(rows[final, 10])
+    assert len(whole["obstacle_force"]) == final
+    saved = _AdaptiveRecord(cfg, 0, None, 100, 7.0).payload(rows[:11], 10, dt=4.5e-4)
+    assert saved["dt"] == 4.5e-4
+    prev = {k: v for k, v in saved.items() if k not in ("extra", "dt")}
+    prev.update(saved["extra"])
+    later = rows[11:].clone()
+    later[:, cum] -= rows[10, cum]
+    part = _AdaptiveRecord(cfg, 11, prev, 100, -1.0).collect(later, final, final=final)
+    for k in ("times", "front", "kinetic_energy", "potential_energy", "speed_samples", "escapes", "clamps",
+              "rebuilds", "speeds", "compression", "dt_min", "dt_max"):
+        assert part[k] == whole[k], k
+    assert part["courant"] == pytest.approx(whole["courant"], rel=1e-15)
+    np.testing.assert_allclose(part["obstacle_force"], whole["obstacle_force"], rtol=0, atol=0)
+    np.testing.assert_allclose(part["sph_impulse"], whole["sph_impulse"], rtol=1e-14)
