@@ -1155,10 +1155,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_walls(const __grid_constant__ Dev
   }
 }
 
-template <bool kOne, int KB>
 // At most 80 registers (three 256-thread blocks per SM): the depth-8 and -16
 // instances then keep one more block resident without spilling (measured on
 // the 2 M case: 0.530 -> 0.505 ms at depth 8, 0.516 -> 0.508 at 16).
+template <bool kOne, int KB>
 __global__ void __launch_bounds__(kMaxBlock, 3) k_force(const __grid_constant__ Dev e) {
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
     const CaseDev& C = case_of<kOne>(e, a);
