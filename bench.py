@@ -45,10 +45,11 @@ ALGO_BYTES_STEP = 244      # per fluid update, compulsory bytes of the whole ste
 ALGO_BYTES_WALL = 48       # per wall particle and step
 # FP32 operations per listed neighbour of each pair pass, counted from the
 # kernel source (an FMA counts 2, every other arithmetic instruction 1,
-# including rsqrt and reciprocals and the cell-offset decode; a packed FP32x2
-# instruction counts once per neighbour it serves).
-PAIR_FLOPS = {"density": 39, "diffusion": 62, "walls": 41, "force": 77, "concentration": 39,
-              "gradient": 63}
+# including rsqrt, reciprocals and the integer-to-FP32 conversion of the
+# fixed-point separation; a packed FP32x2 instruction counts once per
+# neighbour it serves).
+PAIR_FLOPS = {"density": 27, "diffusion": 50, "walls": 32, "force": 65, "concentration": 27,
+              "gradient": 51}
 # DRAM bytes of one force launch per fluid particle: ncu capture of the force
 # pass on the dx = 0.0138 rung (241,488 fluid) at skin 0.15 h and depth 8,
 # dram__bytes_read.sum + dram__bytes_write.sum divided by the fluid rows.

@@ -522,7 +522,7 @@ int tsph_internal_energy(const void* rho, int64_t n, int64_t dtype, double rho0,
 /* All calls on one engine must use one stream.                              */
 /* ------------------------------------------------------------------------ */
 typedef struct {
-  int64_t max_fluid, max_wall, max_obstacle; /* particle capacities (sum < 2^26)   */
+  int64_t max_fluid, max_wall, max_obstacle; /* particle capacities (sum < 2^31-2) */
   int64_t max_cells;                          /* cell capacity over all cases       */
   int64_t max_cases;                          /* case slots                         */
   int64_t max_neighbors;                      /* neighbour-row capacity             */

@@ -14,16 +14,16 @@
 //
 // Per particle (sorted order):
 //   pos  double4  x, y, z, mass -- FP64 state (integration, list builds)
-//   lp   float4   position relative to its home cell (its cell at its case's
-//                 last rebuild) + mass; a pair separation is
-//                 (l_a - l_b) - (c_b - c_a) * cell, exact to the FP32 rounding
-//                 of the two local coordinates
+//   lp   Rec      position in fixed point (units of the case's power-of-two
+//                 q from its origin, one 32-bit word per axis) + mass; a pair
+//                 separation is the integer difference of the words in FP32
+//                 times q, exact to the rounding of the two positions to q
 //   vb   float4   FP32 velocity + volume m/rho;  pr, rho, pq = p/rho^2
 //   nbr  uint32 rows in groups of four: entry k of row a at
 //        ((k >> 2) * rows + a) * 4 + (k & 3), so a thread reads four entries
 //        with one 16-byte load and a warp's loads of one group are contiguous;
-//        entry = row index << 6 | cell offset (dx+1) | (dy+1) << 2 | (dz+1) << 4,
-//        the last group of a row padded with null-row entries
+//        entry = the neighbour's row index, the last group of a row padded
+//        with null-row entries
 // Each case rebuilds its rows only when its own particles leave its own skin
 // and the order of its block depends on its own particles only, so a case
 // evolves bit for bit the same alone or batched with others.  Retiring a case
@@ -57,10 +57,19 @@ constexpr int kBatch = 4;
 // at 4; gradient 0.317 at 16, 0.328 at 8
 constexpr int kConcBatch = 16;
 constexpr int kGradBatch = 16;
-constexpr int kCodeBits = 6;                               // cell-offset code bits of a row entry
-constexpr uint32_t kCodeMask = (1u << kCodeBits) - 1;
-constexpr uint32_t kSelfCode = 0x15u;                      // offset (0, 0, 0): fields (1, 1, 1)
-constexpr int64_t kMaxRows = (int64_t(1) << 26) - 1;      // row index in the other 26 bits
+constexpr int64_t kMaxRows = (int64_t(1) << 31) - 2;      // a row entry is a particle index (int)
+
+// The position record every gather reads: the position in fixed point, one
+// unsigned 32-bit word per axis counting units of the case's q from its
+// origin (modulo 2^32), and the mass (or the volume) in the fourth word.  A
+// separation is the wrapped integer difference of two words converted to
+// FP32 and scaled by q: exact for a power-of-two q (every non-periodic case)
+// and, for a periodic cube of edge 2^32 q, the minimum image by the 2^32
+// wrap.  No cell offset has to be decoded per neighbour.
+struct __align__(16) Rec {
+  uint32_t x, y, z;
+  float w;
+};
 
 struct CaseDev {
   double origin[3];
@@ -73,6 +82,8 @@ struct CaseDev {
   int fluid_begin, n_fluid, wall_begin, n_wall;
   int ob_begin, n_ob, has_ob, shift_every;
   float cellf, inv_h, sigma, sig2d, rho0, bulk, gamma, inv_gamma;
+  float qf;                // the fixed-point unit of the position records, metres
+  double inv_q;            // 1 / q
   float grav, nu2, nu2f, dscale, dtf, visc_eps, rho_floor, wall_mass;
   int csf;                 // CSF surface tension on (2-D)
   int csf_fit;             // curvature fit: 0 none ("mls"), 1 quadratic, 2 circle
@@ -83,7 +94,7 @@ struct CaseDev {
   double ca_area_factor;   // traction: the wall delta's A / (1/2)
   double ca_c_sigma;       // traction: C sigma
   int periodic;            // triply periodic cube of edge pbox (3-D, no walls)
-  double pbox;             // the cube edge: n cells x the FP32 cell edge, exactly
+  double pbox;             // the cube edge: n cells x the FP32 cell edge, exactly (2^32 q)
   int stencil_cells;       // cells each side covering the 4h fit stencil
   double sigma_st, h_d, inv_h_d, sigma2d_d, vol_scale;  // CSF: sigma, h, 1/h, 10/(7 pi h^2), 1/rho0
   double stencil2;         // (4h)^2
@@ -153,9 +164,12 @@ struct CaseCtl {
 struct Dev {
   int nf, nw, NF, n_slots, maxnb, diag_ring, n_ob, shift_slot, one_slot, null_row;
   int64_t rows;  // NF + wall capacity: the row stride of nbr
-  // The null row (index rows) of every gathered array: far from every case,
-  // zero mass, volume, pressure and velocity, so that a pair with it adds
-  // exactly zero.  Rows are padded to whole batches with entries of it.
+  // The null row (index rows) of every gathered array: zero mass, volume,
+  // pressure and velocity, and its position record 2^30 units or more from
+  // every particle of a non-periodic case, so that a pair with it adds exactly
+  // zero (in a periodic cube, where no record is far from every other, every
+  // term of a pair carries the null row's zero mass or volume).  Rows are
+  // padded to whole batches with entries of it.
   uint32_t pad;
   CaseDev one;   // the case of a batch of one (kernel-parameter copy)
   const CaseDev* cases;
@@ -164,7 +178,7 @@ struct Dev {
   double4* pos;
   double4* vel;
   double4* anchor;
-  float4* lp;
+  Rec* lp;
   int32_t* home;
   int32_t* id;
   int32_t* cid;
@@ -178,7 +192,7 @@ struct Dev {
   float4* acc;
   float* conc;
   float4* gradc;
-  float4* lpv;       // shifting: local position + volume m/rho after the Euler update
+  Rec* lpv;          // shifting: position + volume m/rho after the Euler update
   float* tmp_v;      // the volume carried through a rebuild's permutation
   float2* tmp_rp;    // the last density and pressure carried through it (read back by id)
   double4* csA;      // CSF: colour, M00, M01, M11
@@ -283,39 +297,24 @@ __device__ __forceinline__ int local_cell(const CaseDev& c, double x, double y, 
   return (cx * c.ncy + cy) * c.ncz + cz;
 }
 
-// Position relative to the origin of the case's cell `local_key`; the cell
-// origin uses the FP32-rounded cell size so that (c_b - c_a) * cellf is exact.
-__device__ __forceinline__ float4 local_of(const CaseDev& c, int local_key, double x, double y, double z,
-                                           double m) {
-  const int cz = local_key % c.ncz;
-  const int cy = (local_key / c.ncz) % c.ncy;
-  const int cx = local_key / (c.ncz * c.ncy);
-  const double cs = static_cast<double>(c.cellf);
-  return make_float4(static_cast<float>(x - (c.origin[0] + cx * cs)),
-                     static_cast<float>(y - (c.origin[1] + cy * cs)),
-                     static_cast<float>(z - (c.origin[2] + cz * cs)), static_cast<float>(m));
+// One axis of a position in units of q from the case origin, rounded to
+// nearest and wrapped modulo 2^32.
+__device__ __forceinline__ uint32_t fixed_of(const CaseDev& c, int k, double x) {
+  return static_cast<uint32_t>(static_cast<unsigned long long>(__double2ll_rn((x - c.origin[k]) * c.inv_q)));
 }
 
-// Cell offset c_b - c_a of a row entry, 2 bits per axis (dx + 1 at bit 0,
-// dy + 1 at bit 2, dz + 1 at bit 4).  unit<S> places a field f in {0, 1, 2}
-// in the top two mantissa bits (21, 22) of 1.0f, giving 1 + f/4 in
-// {1, 1.25, 1.5}, then 4 v - 5 in {-1, 0, 1}, all exact: no table lookup per
-// neighbour.
-template <int kShift>
-__device__ __forceinline__ float unit(uint32_t ent) {
-  const uint32_t bits = ((ent << (21 - kShift)) & (3u << 21)) | 0x3f800000u;
-  return fmaf(4.f, __uint_as_float(bits), -5.f);
+__device__ __forceinline__ Rec rec_of(const CaseDev& c, double x, double y, double z, double w) {
+  return Rec{fixed_of(c, 0, x), fixed_of(c, 1, y), fixed_of(c, 2, z), static_cast<float>(w)};
 }
 
-__host__ __device__ constexpr uint32_t entry_code(int dx, int dy, int dz) {
-  return static_cast<uint32_t>((dx + 1) | ((dy + 1) << 2) | ((dz + 1) << 4));
+// Separation on one axis of records a and b in FP32 metres: the wrapped
+// difference of the words (|la - lb| < 2^24 units for a list pair, so the
+// conversion is exact) times q.
+__device__ __forceinline__ float sep1(uint32_t la, uint32_t lb, float q) {
+  return __int2float_rn(static_cast<int>(la - lb)) * q;
 }
-
-// The separation is (l_a - l_b) - u * cell with u * cell exact, so one FMA per
-// axis gives the same bits as a subtraction of a precomputed offset.
-__device__ __forceinline__ float3 sep(const float4& la, const float4& lb, uint32_t ent, float cellf) {
-  return make_float3(fmaf(-unit<0>(ent), cellf, la.x - lb.x), fmaf(-unit<2>(ent), cellf, la.y - lb.y),
-                     fmaf(-unit<4>(ent), cellf, la.z - lb.z));
+__device__ __forceinline__ float3 sep(const Rec& la, const Rec& lb, float q) {
+  return make_float3(sep1(la.x, lb.x, q), sep1(la.y, lb.y, q), sep1(la.z, lb.z, q));
 }
 
 // ------------------------------------------------- packed FP32 pairs ---
@@ -325,19 +324,10 @@ __device__ __forceinline__ float3 sep(const float4& la, const float4& lb, uint32
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, f2(-1.f), a); }
 
-// Cell offsets of two entries on one axis (see unit).
-template <int kShift>
-__device__ __forceinline__ float2 unit2(uint32_t e0, uint32_t e1) {
-  const uint32_t b0 = ((e0 << (21 - kShift)) & (3u << 21)) | 0x3f800000u;
-  const uint32_t b1 = ((e1 << (21 - kShift)) & (3u << 21)) | 0x3f800000u;
-  return __ffma2_rn(f2(4.f), make_float2(__uint_as_float(b0), __uint_as_float(b1)), f2(-5.f));
-}
-
-// Separations of two neighbours on one axis, (l_a - l_b) - u * cell: the same
-// bits as sep.  ncell = (-cell, -cell).
-template <int kShift>
-__device__ __forceinline__ float2 sep2(float la, float lb0, float lb1, uint32_t e0, uint32_t e1, float2 ncell) {
-  return __ffma2_rn(unit2<kShift>(e0, e1), ncell, sub2(f2(la), make_float2(lb0, lb1)));
+// Separations of two neighbours on one axis (see sep1).  q2 = (q, q).
+__device__ __forceinline__ float2 sep2(uint32_t la, uint32_t lb0, uint32_t lb1, float2 q2) {
+  return __fmul2_rn(make_float2(__int2float_rn(static_cast<int>(la - lb0)), __int2float_rn(static_cast<int>(la - lb1))),
+                    q2);
 }
 
 struct Radial2 {
@@ -526,9 +516,10 @@ __global__ void k_permute_back(Dev e) {
     st4(e.vel, a, ld4(e.tmp4b, a));
     e.id[a] = e.tmp_id[a];
     e.home[a] = key;
-    e.lp[a] = local_of(C, key - C.key_off, p.x, p.y, p.z, p.w);
+    const Rec r = rec_of(C, p.x, p.y, p.z, p.w);
+    e.lp[a] = r;
     // the shifting passes after the Euler update read this step's volumes
-    if (C.shift_every > 0 || C.tvc_bulk) e.lpv[a] = local_of(C, key - C.key_off, p.x, p.y, p.z, e.tmp_v[a]);
+    if (C.shift_every > 0 || C.tvc_bulk) e.lpv[a] = Rec{r.x, r.y, r.z, e.tmp_v[a]};
     // the density and pressure of the step's evaluation stay with their
     // particle: a rebuild of the second list pass comes after them
     const float2 rp = e.tmp_rp[a];
@@ -592,7 +583,6 @@ __global__ void k_rows(Dev e) {
           if (per) z = z < 0 ? z + C.ncz : (z >= C.ncz ? z - C.ncz : z);
           if (z < 0 || z >= C.ncz) continue;
           const int cell = C.key_off + (x * C.ncy + y) * C.ncz + z;
-          const uint32_t code = entry_code(dx, dy, dz);
           const int fs = e.fstart[cell];
           if (fs >= 0) {
             const int fe = e.fend[cell];
@@ -611,7 +601,7 @@ __global__ void k_rows(Dev e) {
                 }
                 if (b < fe && b != a && ddx * ddx + ddy * ddy + ddz * ddz <= rc2) {
                   if (count < e.maxnb)
-                    e.nbr[entry_at(e.rows, a, count)] = (static_cast<uint32_t>(b) << kCodeBits) | code;
+                    e.nbr[entry_at(e.rows, a, count)] = static_cast<uint32_t>(b);
                   ++count;
                 }
               }
@@ -631,7 +621,7 @@ __global__ void k_rows(Dev e) {
                   const double ddx = pa.x - pb[j].x, ddy = pa.y - pb[j].y, ddz = pa.z - pb[j].z;
                   if (w0 + j < we && ddx * ddx + ddy * ddy + ddz * ddz <= rc2) {
                     if (count < e.maxnb)
-                      e.nbr[entry_at(e.rows, a, count)] = (static_cast<uint32_t>(b) << kCodeBits) | code;
+                      e.nbr[entry_at(e.rows, a, count)] = static_cast<uint32_t>(b);
                     ++count;
                   }
                 }
@@ -672,7 +662,7 @@ __global__ void k_rows(Dev e) {
               const int b = b0 + j;
               const double ddx = pa.x - pb[j].x, ddy = pa.y - pb[j].y;
               if (b < fe && b != a && ddx * ddx + ddy * ddy <= C.fit_rc2) {
-                if (c4 < e.maxfit) e.nbr4[static_cast<int64_t>(c4) * e.NF + a] = static_cast<uint32_t>(b) << kCodeBits;
+                if (c4 < e.maxfit) e.nbr4[static_cast<int64_t>(c4) * e.NF + a] = static_cast<uint32_t>(b);
                 ++c4;
               }
             }
@@ -746,9 +736,9 @@ template <bool kOne, int KB>
 __global__ void __launch_bounds__(kMaxBlock) k_density(const __grid_constant__ Dev e) {
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
     const CaseDev& C = case_of<kOne>(e, a);
-    const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, floor_ = C.rho_floor;
-    const float4 la = e.lp[a];
-    const float2 ncell = f2(-cellf), inv_h2 = f2(inv_h), sigma2 = f2(sigma);
+    const float sigma = C.sigma, inv_h = C.inv_h, qf = C.qf, floor_ = C.rho_floor;
+    const Rec la = e.lp[a];
+    const float2 q2 = f2(qf), inv_h2 = f2(inv_h), sigma2 = f2(sigma);
     // the deviation rho - rho0, summed with compensation from -rho0
     CSum<float> s, kt, nb;
     s.add(-C.rho0);
@@ -759,10 +749,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_density(const __grid_constant__ D
 #pragma unroll
       for (int j = 0; j < KB; j += 2) {
         const uint32_t e0 = ent[j], e1 = ent[j + 1];
-        const float4 l0 = e.lp[e0 >> kCodeBits], l1 = e.lp[e1 >> kCodeBits];
-        const float2 dx = sep2<0>(la.x, l0.x, l1.x, e0, e1, ncell);
-        const float2 dy = sep2<2>(la.y, l0.y, l1.y, e0, e1, ncell);
-        const float2 dz = sep2<4>(la.z, l0.z, l1.z, e0, e1, ncell);
+        const Rec l0 = e.lp[e0], l1 = e.lp[e1];
+        const float2 dx = sep2(la.x, l0.x, l1.x, q2);
+        const float2 dy = sep2(la.y, l0.y, l1.y, q2);
+        const float2 dz = sep2(la.z, l0.z, l1.z, q2);
         const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
         const float2 W = __fmul2_rn(sigma2, shape2(radial2(r2, inv_h2).q));
         part = __ffma2_rn(make_float2(l0.w, l1.w), W, part);
@@ -876,17 +866,17 @@ __global__ void __launch_bounds__(kMaxBlock) k_closure_pass(const __grid_constan
       known_out[a] = known_in[a];
       continue;
     }
-    const float4 la = e.lp[a];
-    const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, g = C.grav;
+    const Rec la = e.lp[a];
+    const float sigma = C.sigma, inv_h = C.inv_h, qf = C.qf, g = C.grav;
     const int NF = e.NF, n = e.cnt[a];
     const bool all = C.closure_all != 0;
     CSum<float> num, den;
     for (int k = 0; k < n; ++k) {
       const uint32_t ent = ld_entry(e.nbr + entry_at(e.rows, a, k));
-      const int b = static_cast<int>(ent >> kCodeBits);
+      const int b = static_cast<int>(ent);
       if (b >= NF || !(all || known_in[b])) continue;
-      const float4 lb = e.lp[b];
-      const float3 d = sep(la, lb, ent, cellf);
+      const Rec lb = e.lp[b];
+      const float3 d = sep(la, lb, qf);
       const float r2 = fmaf(d.z, d.z, fmaf(d.y, d.y, d.x * d.x));
       const float W = sigma * shape(radial(r2, inv_h).q);
       num.add(W * (p_in[b] - g * d.y * e.rho[b]));
@@ -923,23 +913,23 @@ __global__ void __launch_bounds__(kMaxBlock) k_density_gradient(const __grid_con
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
     const CaseDev& C = case_of<kOne>(e, a);
     if (!C.psi) continue;
-    const float4 la = e.lp[a];
+    const Rec la = e.lp[a];
     const float2 ra = e.rs[a];
-    const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf;
+    const float sigma = C.sigma, inv_h = C.inv_h, qf = C.qf;
     const int NF = e.NF;
-    const float2 ncell = f2(-cellf), inv_h2 = f2(inv_h), gscale = f2(sigma * inv_h);
+    const float2 q2 = f2(qf), inv_h2 = f2(inv_h), gscale = f2(sigma * inv_h);
     CSum<float> gx, gy, gz, mxx, mxy, mxz, myy, myz, mzz;
     walk_row<KB>(e, a, [&](const uint32_t* ent) {
 #pragma unroll
       for (int j = 0; j < KB; j += 2) {
         const uint32_t e0 = ent[j], e1 = ent[j + 1];
-        const int c0 = static_cast<int>(e0 >> kCodeBits), c1 = static_cast<int>(e1 >> kCodeBits);
+        const int c0 = static_cast<int>(e0), c1 = static_cast<int>(e1);
         const int b0 = c0 < NF ? c0 : e.null_row, b1 = c1 < NF ? c1 : e.null_row;
-        const float4 l0 = e.lp[b0], l1 = e.lp[b1];
+        const Rec l0 = e.lp[b0], l1 = e.lp[b1];
         const float2 r0 = e.rs[b0], r1 = e.rs[b1];
-        const float2 dx = sep2<0>(la.x, l0.x, l1.x, e0, e1, ncell);
-        const float2 dy = sep2<2>(la.y, l0.y, l1.y, e0, e1, ncell);
-        const float2 dz = sep2<4>(la.z, l0.z, l1.z, e0, e1, ncell);
+        const float2 dx = sep2(la.x, l0.x, l1.x, q2);
+        const float2 dy = sep2(la.y, l0.y, l1.y, q2);
+        const float2 dz = sep2(la.z, l0.z, l1.z, q2);
         const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
         const Radial2 R = radial2(r2, inv_h2);
         const float2 gs = __fmul2_rn(__fmul2_rn(gscale, dshape2(R.q)), R.inv_r);
@@ -980,30 +970,30 @@ __global__ void __launch_bounds__(kMaxBlock) k_diffusion_eos(const __grid_consta
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
     const CaseDev& C = case_of<kOne>(e, a);
     const float2 ra = e.rs[a];  // (rho - rho0, m / rho)
-    const float4 la = e.lp[a];
+    const Rec la = e.lp[a];
     float d = ra.x;
     const float dscale = C.dscale;
     if (dscale > 0.f && C.psi) {
       // psi form (density_diffusion.py:145-172): the contrast
       // (rho_a - rho_b) - (<grad rho>_a + <grad rho>_b) . d / 2
       const float4 ga = e.gg[a];
-      const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf;
+      const float sigma = C.sigma, inv_h = C.inv_h, qf = C.qf;
       const int NF = e.NF;
-      const float2 ncell = f2(-cellf), inv_h2 = f2(inv_h), gscale = f2(-sigma * inv_h);
+      const float2 q2 = f2(qf), inv_h2 = f2(inv_h), gscale = f2(-sigma * inv_h);
       CSum<float> rate;
       walk_row<KB>(e, a, [&](const uint32_t* ent) {
         float2 part = f2(0.f);
 #pragma unroll
         for (int j = 0; j < KB; j += 2) {
           const uint32_t e0 = ent[j], e1 = ent[j + 1];
-          const int c0 = static_cast<int>(e0 >> kCodeBits), c1 = static_cast<int>(e1 >> kCodeBits);
+          const int c0 = static_cast<int>(e0), c1 = static_cast<int>(e1);
           const int b0 = c0 < NF ? c0 : e.null_row, b1 = c1 < NF ? c1 : e.null_row;
-          const float4 l0 = e.lp[b0], l1 = e.lp[b1];
+          const Rec l0 = e.lp[b0], l1 = e.lp[b1];
           const float2 r0 = e.rs[b0], r1 = e.rs[b1];
           const float4 g0 = e.gg[b0], g1 = e.gg[b1];
-          const float2 dx = sep2<0>(la.x, l0.x, l1.x, e0, e1, ncell);
-          const float2 dy = sep2<2>(la.y, l0.y, l1.y, e0, e1, ncell);
-          const float2 dz = sep2<4>(la.z, l0.z, l1.z, e0, e1, ncell);
+          const float2 dx = sep2(la.x, l0.x, l1.x, q2);
+          const float2 dy = sep2(la.y, l0.y, l1.y, q2);
+          const float2 dz = sep2(la.z, l0.z, l1.z, q2);
           const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
           const Radial2 R = radial2(r2, inv_h2);
           const float2 ngr = __fmul2_rn(__fmul2_rn(__fmul2_rn(gscale, dshape2(R.q)), R.inv_r), r2);
@@ -1024,9 +1014,9 @@ __global__ void __launch_bounds__(kMaxBlock) k_diffusion_eos(const __grid_consta
       d = ra.x + dtf * rate.value();
       d = d > dfloor ? d : dfloor;
     } else if (dscale > 0.f) {
-      const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf;
+      const float sigma = C.sigma, inv_h = C.inv_h, qf = C.qf;
       const int NF = e.NF;
-      const float2 ncell = f2(-cellf), inv_h2 = f2(inv_h), gscale = f2(-sigma * inv_h);
+      const float2 q2 = f2(qf), inv_h2 = f2(inv_h), gscale = f2(-sigma * inv_h);
       CSum<float> rate;
       walk_row<KB>(e, a, [&](const uint32_t* ent) {
         float2 part = f2(0.f);
@@ -1034,13 +1024,13 @@ __global__ void __launch_bounds__(kMaxBlock) k_diffusion_eos(const __grid_consta
         for (int j = 0; j < KB; j += 2) {
           // wall neighbours do not diffuse: they read the null row
           const uint32_t e0 = ent[j], e1 = ent[j + 1];
-          const int c0 = static_cast<int>(e0 >> kCodeBits), c1 = static_cast<int>(e1 >> kCodeBits);
+          const int c0 = static_cast<int>(e0), c1 = static_cast<int>(e1);
           const int b0 = c0 < NF ? c0 : e.null_row, b1 = c1 < NF ? c1 : e.null_row;
-          const float4 l0 = e.lp[b0], l1 = e.lp[b1];
+          const Rec l0 = e.lp[b0], l1 = e.lp[b1];
           const float2 r0 = e.rs[b0], r1 = e.rs[b1];
-          const float2 dx = sep2<0>(la.x, l0.x, l1.x, e0, e1, ncell);
-          const float2 dy = sep2<2>(la.y, l0.y, l1.y, e0, e1, ncell);
-          const float2 dz = sep2<4>(la.z, l0.z, l1.z, e0, e1, ncell);
+          const float2 dx = sep2(la.x, l0.x, l1.x, q2);
+          const float2 dy = sep2(la.y, l0.y, l1.y, q2);
+          const float2 dz = sep2(la.z, l0.z, l1.z, q2);
           const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
           const Radial2 R = radial2(r2, inv_h2);
           // -grad W . r = -sigma f'(q) r / h
@@ -1077,10 +1067,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_bcd(const __grid_constant__ Dev e
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
     const CaseDev& C = case_of<kOne>(e, a);
     if (!C.bcd) continue;
-    const float4 la = e.lp[a];
-    const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, inv_rho0 = 1.f / C.rho0;
+    const Rec la = e.lp[a];
+    const float sigma = C.sigma, inv_h = C.inv_h, qf = C.qf, inv_rho0 = 1.f / C.rho0;
     const int NF = e.NF;
-    const float2 ncell = f2(-cellf), inv_h2 = f2(inv_h), sigma2 = f2(sigma);
+    const float2 q2 = f2(qf), inv_h2 = f2(inv_h), sigma2 = f2(sigma);
     CSum<float> corr;
     walk_row<KB>(e, a, [&](const uint32_t* ent) {
       float2 part = f2(0.f);
@@ -1088,12 +1078,12 @@ __global__ void __launch_bounds__(kMaxBlock) k_bcd(const __grid_constant__ Dev e
       for (int j = 0; j < KB; j += 2) {
         // fluid neighbours read the null row (zero mass)
         const uint32_t e0 = ent[j], e1 = ent[j + 1];
-        const int c0 = static_cast<int>(e0 >> kCodeBits), c1 = static_cast<int>(e1 >> kCodeBits);
+        const int c0 = static_cast<int>(e0), c1 = static_cast<int>(e1);
         const int b0 = c0 >= NF ? c0 : e.null_row, b1 = c1 >= NF ? c1 : e.null_row;
-        const float4 l0 = e.lp[b0], l1 = e.lp[b1];
-        const float2 dx = sep2<0>(la.x, l0.x, l1.x, e0, e1, ncell);
-        const float2 dy = sep2<2>(la.y, l0.y, l1.y, e0, e1, ncell);
-        const float2 dz = sep2<4>(la.z, l0.z, l1.z, e0, e1, ncell);
+        const Rec l0 = e.lp[b0], l1 = e.lp[b1];
+        const float2 dx = sep2(la.x, l0.x, l1.x, q2);
+        const float2 dy = sep2(la.y, l0.y, l1.y, q2);
+        const float2 dz = sep2(la.z, l0.z, l1.z, q2);
         const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
         const float2 W = __fmul2_rn(sigma2, shape2(radial2(r2, inv_h2).q));
         const float2 dm = make_float2(l0.w * ((e.rho[b0] - C.rho0) * inv_rho0),
@@ -1121,18 +1111,18 @@ __global__ void __launch_bounds__(kMaxBlock) k_walls(const __grid_constant__ Dev
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < e.nw; t += gridDim.x * blockDim.x) {
     const int64_t a = e.NF + t;
     const CaseDev& C = case_of<kOne>(e, a);
-    const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, grav = C.grav;
+    const float sigma = C.sigma, inv_h = C.inv_h, qf = C.qf, grav = C.grav;
     const int f0 = C.fluid_begin;
-    const float4 la = e.lp[a];
+    const Rec la = e.lp[a];
     CSum<float> num, den;
     walk_row<KB>(e, a, [&](const uint32_t* ent) {
       float pn = 0.f, pd = 0.f;
 #pragma unroll
       for (int j = 0; j < KB; ++j) {
         const bool ok = ent[j] != e.pad;
-        const int f = ok ? static_cast<int>(ent[j] >> kCodeBits) : f0;
-        const float4 lf = e.lp[f];
-        const float3 d = sep(la, lf, ok ? ent[j] : kSelfCode, cellf);  // r_w - r_f
+        const int f = ok ? static_cast<int>(ent[j]) : f0;
+        const Rec lf = e.lp[f];
+        const float3 d = sep(la, lf, qf);  // r_w - r_f
         const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
         const float W = ok ? sigma * shape(radial(r2, inv_h).q) : 0.f;
         float src = e.pr[f];
@@ -1162,26 +1152,26 @@ template <bool kOne, int KB>
 __global__ void __launch_bounds__(kMaxBlock, 3) k_force(const __grid_constant__ Dev e) {
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
     const CaseDev& C = case_of<kOne>(e, a);
-    const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, nu2 = C.nu2, nu2f = C.nu2f,
+    const float sigma = C.sigma, inv_h = C.inv_h, qf = C.qf, nu2 = C.nu2, nu2f = C.nu2f,
                 eta2 = C.visc_eps;
     const int NF = e.NF;
-    const float4 la = e.lp[a];
+    const Rec la = e.lp[a];
     const float4 va = e.vb[a];
     const float Pa = e.pq[a];
-    const float2 ncell = f2(-cellf), inv_h2 = f2(inv_h), gscale = f2(sigma * inv_h);
+    const float2 q2 = f2(qf), inv_h2 = f2(inv_h), gscale = f2(sigma * inv_h);
     CSum<float> ax, ay, az;
     walk_row<KB>(e, a, [&](const uint32_t* ent) {
       float2 px = f2(0.f), py = f2(0.f), pz = f2(0.f);
 #pragma unroll
       for (int j = 0; j < KB; j += 2) {
         const uint32_t e0 = ent[j], e1 = ent[j + 1];
-        const int b0 = static_cast<int>(e0 >> kCodeBits), b1 = static_cast<int>(e1 >> kCodeBits);
-        const float4 l0 = e.lp[b0], l1 = e.lp[b1];
+        const int b0 = static_cast<int>(e0), b1 = static_cast<int>(e1);
+        const Rec l0 = e.lp[b0], l1 = e.lp[b1];
         const float4 v0 = e.vb[b0], v1 = e.vb[b1];
         const float2 Pb = make_float2(e.pq[b0], e.pq[b1]);
-        const float2 dx = sep2<0>(la.x, l0.x, l1.x, e0, e1, ncell);
-        const float2 dy = sep2<2>(la.y, l0.y, l1.y, e0, e1, ncell);
-        const float2 dz = sep2<4>(la.z, l0.z, l1.z, e0, e1, ncell);
+        const float2 dx = sep2(la.x, l0.x, l1.x, q2);
+        const float2 dy = sep2(la.y, l0.y, l1.y, q2);
+        const float2 dz = sep2(la.z, l0.z, l1.z, q2);
         const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
         const Radial2 R = radial2(r2, inv_h2);
         const float2 gs = __fmul2_rn(__fmul2_rn(gscale, dshape2(R.q)), R.inv_r);
@@ -1228,9 +1218,9 @@ __global__ void __launch_bounds__(kMaxBlock) k_reaction(Dev e) {
     const int64_t w = e.ob_rows[q];
     c = e.cid[w];
     const CaseDev& C = e.cases[c];
-    const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, nu2f = C.nu2f, eta2 = C.visc_eps;
+    const float sigma = C.sigma, inv_h = C.inv_h, qf = C.qf, nu2f = C.nu2f, eta2 = C.visc_eps;
     const int f0 = C.fluid_begin;
-    const float4 lw_ = e.lp[w];
+    const Rec lw_ = e.lp[w];
     const float Pw = e.pq[w];
     const float mw = lw_.w;
     const float Vw = e.vb[w].w;
@@ -1240,9 +1230,9 @@ __global__ void __launch_bounds__(kMaxBlock) k_reaction(Dev e) {
 #pragma unroll
       for (int j = 0; j < kBatch; ++j) {
         const bool ok = ent[j] != e.pad;
-        const int fi = ok ? static_cast<int>(ent[j] >> kCodeBits) : f0;
-        const float4 lf = e.lp[fi];
-        const float3 d = sep(lw_, lf, ok ? ent[j] : kSelfCode, cellf);
+        const int fi = ok ? static_cast<int>(ent[j]) : f0;
+        const Rec lf = e.lp[fi];
+        const float3 d = sep(lw_, lf, qf);
         const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
         const Radial R = radial(r2, inv_h);
         float gs = sigma * dshape(R.q) * inv_h * R.inv_r;
@@ -1320,7 +1310,7 @@ __device__ __forceinline__ bool row_nearest_wall(const Dev& e, int a, double ax,
   const int n = e.cnt[a];
   bool any = false;
   for (int k = 0; k < n; ++k) {
-    const uint32_t b = ld_entry(e.nbr + entry_at(e.rows, a, k)) >> kCodeBits;
+    const uint32_t b = ld_entry(e.nbr + entry_at(e.rows, a, k));
     if (b < static_cast<uint32_t>(e.NF) || b >= static_cast<uint32_t>(e.null_row)) continue;
     const double2 pw = ld_xy(e.pos, static_cast<int>(b));
     const double dx = ax - pw.x, dy = ay - pw.y, r2 = dx * dx + dy * dy;
@@ -1357,7 +1347,7 @@ __device__ __forceinline__ void fluid_row(const Dev& e, int a, Body&& body) {
     bool ok[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      const uint32_t v = v4[j] >> kCodeBits;
+      const uint32_t v = v4[j];
       ok[j] = v < static_cast<uint32_t>(e.NF);
       b[j] = ok[j] ? static_cast<int>(v) : a;
     }
@@ -1603,7 +1593,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_range(const __grid_constant__
         const double4 pa = ld4(e.pos, a);
         const int n4 = e.cnt4[a];
         for (int k = 0; k < n4; ++k) {
-          const int b = static_cast<int>(e.nbr4[static_cast<int64_t>(k) * e.NF + a] >> kCodeBits);
+          const int b = static_cast<int>(e.nbr4[static_cast<int64_t>(k) * e.NF + a]);
           const double2 pb = ld_xy(e.pos, b);
           const double dx = pa.x - pb.x, dy = pa.y - pb.y;
           if (!(dx * dx + dy * dy <= C.stencil2)) continue;
@@ -1751,14 +1741,14 @@ __global__ void __launch_bounds__(kMaxBlock) k_csf_fit(const __grid_constant__ D
       const int n4 = e.cnt4[a];
       int nb4[4];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) nb4[j] = j < n4 ? static_cast<int>(e.nbr4[static_cast<int64_t>(j) * e.NF + a] >> kCodeBits) : a;
+      for (int j = 0; j < 4; ++j) nb4[j] = j < n4 ? static_cast<int>(e.nbr4[static_cast<int64_t>(j) * e.NF + a]) : a;
       for (int k = 0; k < n4; k += 4) {
         int b[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
           b[j] = nb4[j];
           // prefetch the next batch's entries
-          nb4[j] = k + 4 + j < n4 ? static_cast<int>(e.nbr4[static_cast<int64_t>(k + 4 + j) * e.NF + a] >> kCodeBits) : a;
+          nb4[j] = k + 4 + j < n4 ? static_cast<int>(e.nbr4[static_cast<int64_t>(k + 4 + j) * e.NF + a]) : a;
         }
         double2 pb[4];
         double mg[4];
@@ -1878,7 +1868,7 @@ __global__ void k_csf_final(const __grid_constant__ Dev e) {
         double sw = 0.0;  // sum of W over the wall particles (all within 2h are in the row)
         const int cnt = e.cnt[a];
         for (int k = 0; k < cnt; ++k) {
-          const uint32_t b = ld_entry(e.nbr + entry_at(e.rows, a, k)) >> kCodeBits;
+          const uint32_t b = ld_entry(e.nbr + entry_at(e.rows, a, k));
           if (b < static_cast<uint32_t>(e.NF) || b >= static_cast<uint32_t>(e.null_row)) continue;
           const double2 pw = ld_xy(e.pos, static_cast<int>(b));
           sw += kernel_d(pa.x - pw.x, pa.y - pw.y, C).w;
@@ -2023,9 +2013,9 @@ __device__ __forceinline__ void integrate_row(const Dev& e, int a, const CaseDev
   }
   st4(e.pos, a, make_double4(px, py, pz, m));
   st4(e.vel, a, make_double4(vx, vy, vz, 0.0));
-  const float4 la = local_of(C, e.home[a] - C.key_off, px, py, pz, m);
+  const Rec la = rec_of(C, px, py, pz, m);
   e.lp[a] = la;
-  if (C.shift_every > 0 || C.tvc_bulk) e.lpv[a] = make_float4(la.x, la.y, la.z, e.vb[a].w);
+  if (C.shift_every > 0 || C.tvc_bulk) e.lpv[a] = Rec{la.x, la.y, la.z, e.vb[a].w};
   const double4 an = ld4(e.anchor, a);
   double ex = px - an.x, ey = py - an.y, ez = pz - an.z;
   if (C.periodic) {
@@ -2185,18 +2175,18 @@ __global__ void __launch_bounds__(kMaxBlock) k_tvc_gradient(Dev e) {
     const int c = e.cid[a];
     if (!e.ctl[c].tvc_now) continue;
     const CaseDev& C = e.cases[c];
-    const float sigma = C.sigma, inv_h = C.inv_h, cellf = C.cellf, wvol = C.tvc_wall_vol;
-    const float4 la = e.lp[a];
+    const float sigma = C.sigma, inv_h = C.inv_h, qf = C.qf, wvol = C.tvc_wall_vol;
+    const Rec la = e.lp[a];
     CSum<float> gx, gy, gz;
     walk_row(e, a, [&](const uint32_t* ent) {
       float px = 0.f, py = 0.f, pz = 0.f;
 #pragma unroll
       for (int j = 0; j < kBatch; ++j) {
-        const int b = static_cast<int>(ent[j] >> kCodeBits);
-        const float4 lb = e.lp[b];
+        const int b = static_cast<int>(ent[j]);
+        const Rec lb = e.lp[b];
         // fluid: this step's m / rho; wall: m_w / rho0; the null row: 0
         const float vb = b < NF ? (kLate ? e.lpv[b].w : e.vb[b].w) : (b < e.null_row ? wvol : 0.f);
-        const float3 d = sep(la, lb, ent[j], cellf);
+        const float3 d = sep(la, lb, qf);
         const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
         const Radial R = radial(r2, inv_h);
         const float w = 2.f * vb * (sigma * dshape(R.q) * inv_h * R.inv_r);
@@ -2252,7 +2242,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_tvc_apply(Dev e) {
     if (clamp_box(C, x.x, x.y, x.z, v.x, v.y, v.z)) atomicAdd(&t.escapes, 1ull);
     st4(e.pos, a, x);
     st4(e.vel, a, v);
-    e.lp[a] = local_of(C, e.home[a] - C.key_off, x.x, x.y, x.z, x.w);
+    e.lp[a] = rec_of(C, x.x, x.y, x.z, x.w);
     const double4 an = ld4(e.anchor, a);
     const double ex = x.x - an.x, ey = x.y - an.y, ez = x.z - an.z;
     atomic_max_nonneg(&t.disp[0], sqrt(ex * ex + ey * ey + ez * ez));
@@ -2285,11 +2275,11 @@ template <int KB>
 __global__ void __launch_bounds__(kMaxBlock) k_concentration(const __grid_constant__ Dev e) {
   if (!e.ctl[e.shift_slot].conc_now) return;
   const CaseDev& C = e.cases[e.shift_slot];
-  const float sig2d = C.sig2d, inv_h = C.inv_h, cellf = C.cellf;
+  const float sig2d = C.sig2d, inv_h = C.inv_h, qf = C.qf;
   const int NF = e.NF;
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
-    const float4 la = e.lpv[a];  // (x, y, z, V) after the Euler update
-    const float2 ncell = f2(-cellf), inv_h2 = f2(inv_h), sig2 = f2(sig2d);
+    const Rec la = e.lpv[a];  // (x, y, z, V) after the Euler update
+    const float2 q2 = f2(qf), inv_h2 = f2(inv_h), sig2 = f2(sig2d);
     CSum<float> s;
     s.add(la.w * sig2d);
     walk_row<KB>(e, a, [&](const uint32_t* ent) {
@@ -2297,11 +2287,11 @@ __global__ void __launch_bounds__(kMaxBlock) k_concentration(const __grid_consta
 #pragma unroll
       for (int j = 0; j < KB; j += 2) {
         const uint32_t e0 = ent[j], e1 = ent[j + 1];
-        const int c0 = static_cast<int>(e0 >> kCodeBits), c1 = static_cast<int>(e1 >> kCodeBits);
-        const float4 l0 = e.lpv[c0 < NF ? c0 : e.null_row], l1 = e.lpv[c1 < NF ? c1 : e.null_row];
-        const float2 dx = sep2<0>(la.x, l0.x, l1.x, e0, e1, ncell);
-        const float2 dy = sep2<2>(la.y, l0.y, l1.y, e0, e1, ncell);
-        const float2 dz = sep2<4>(la.z, l0.z, l1.z, e0, e1, ncell);
+        const int c0 = static_cast<int>(e0), c1 = static_cast<int>(e1);
+        const Rec l0 = e.lpv[c0 < NF ? c0 : e.null_row], l1 = e.lpv[c1 < NF ? c1 : e.null_row];
+        const float2 dx = sep2(la.x, l0.x, l1.x, q2);
+        const float2 dy = sep2(la.y, l0.y, l1.y, q2);
+        const float2 dz = sep2(la.z, l0.z, l1.z, q2);
         const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
         const float2 W = __fmul2_rn(sig2, shape2(radial2(r2, inv_h2).q));
         part = __ffma2_rn(make_float2(l0.w, l1.w), W, part);
@@ -2316,25 +2306,25 @@ template <int KB>
 __global__ void __launch_bounds__(kMaxBlock) k_conc_gradient(const __grid_constant__ Dev e) {
   if (!e.ctl[e.shift_slot].shift_now) return;
   const CaseDev& C = e.cases[e.shift_slot];
-  const float sig2d = C.sig2d, inv_h = C.inv_h, cellf = C.cellf;
+  const float sig2d = C.sig2d, inv_h = C.inv_h, qf = C.qf;
   const int NF = e.NF;
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < e.nf; a += gridDim.x * blockDim.x) {
-    const float4 la = e.lpv[a];
+    const Rec la = e.lpv[a];
     const float ca = e.conc[a];
-    const float2 ncell = f2(-cellf), inv_h2 = f2(inv_h), gscale = f2(sig2d * inv_h);
+    const float2 q2 = f2(qf), inv_h2 = f2(inv_h), gscale = f2(sig2d * inv_h);
     CSum<float> gx, gy, gz;
     walk_row<KB>(e, a, [&](const uint32_t* ent) {
       float2 px = f2(0.f), py = f2(0.f), pz = f2(0.f);
 #pragma unroll
       for (int j = 0; j < KB; j += 2) {
         const uint32_t e0 = ent[j], e1 = ent[j + 1];
-        const int c0 = static_cast<int>(e0 >> kCodeBits), c1 = static_cast<int>(e1 >> kCodeBits);
+        const int c0 = static_cast<int>(e0), c1 = static_cast<int>(e1);
         const int b0 = c0 < NF ? c0 : e.null_row, b1 = c1 < NF ? c1 : e.null_row;
-        const float4 l0 = e.lpv[b0], l1 = e.lpv[b1];
+        const Rec l0 = e.lpv[b0], l1 = e.lpv[b1];
         const float2 cb = make_float2(e.conc[b0], e.conc[b1]);
-        const float2 dx = sep2<0>(la.x, l0.x, l1.x, e0, e1, ncell);
-        const float2 dy = sep2<2>(la.y, l0.y, l1.y, e0, e1, ncell);
-        const float2 dz = sep2<4>(la.z, l0.z, l1.z, e0, e1, ncell);
+        const float2 dx = sep2(la.x, l0.x, l1.x, q2);
+        const float2 dy = sep2(la.y, l0.y, l1.y, q2);
+        const float2 dz = sep2(la.z, l0.z, l1.z, q2);
         const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
         const Radial2 R = radial2(r2, inv_h2);
         const float2 gs = __fmul2_rn(__fmul2_rn(gscale, dshape2(R.q)), R.inv_r);
@@ -2501,7 +2491,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_shift_apply(Dev e) {
     x.y += sy;
     x.z += sz;
     st4(e.pos, a, x);
-    e.lp[a] = local_of(C, e.home[a] - C.key_off, x.x, x.y, x.z, x.w);
+    e.lp[a] = rec_of(C, x.x, x.y, x.z, x.w);
     const double4 an = ld4(e.anchor, a);
     const double ex = x.x - an.x, ey = x.y - an.y, ez = x.z - an.z;
     dmax = fmax(dmax, sqrt(ex * ex + ey * ey + ez * ez));
@@ -2513,12 +2503,14 @@ __global__ void __launch_bounds__(kMaxBlock) k_shift_apply(Dev e) {
   }
 }
 
-// The null row: positions 1e4 m from every cell origin (pairs with it are
-// far outside the support, and every term is multiplied by its zero mass,
-// volume or weight), finite density.
+// The null row: position words 0xC0000000, 2^30 units or more (half the
+// record range of the case, at least twice the list cutoff) from every
+// particle of a non-periodic case, whose words lie in [0, 2^31), so that pairs
+// with it are far outside the support; every term is also multiplied by its
+// zero mass, volume or weight.  Finite density.
 __global__ void k_null_row(Dev e) {
   const int64_t n = e.null_row;
-  const float4 far = make_float4(1e4f, 1e4f, 1e4f, 0.f);
+  const Rec far{0xC0000000u, 0xC0000000u, 0xC0000000u, 0.f};
   e.lp[n] = far;
   e.lpv[n] = far;
   e.vb[n] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -2573,7 +2565,7 @@ __global__ void k_place_walls(Dev e, int begin, int n, int slot, int dim, const 
     e.home[a] = key;
     e.cid[a] = slot;
     e.cnt[a] = 0;
-    e.lp[a] = local_of(C, key - C.key_off, w[dim * o], w[dim * o + 1], z, m);
+    e.lp[a] = rec_of(C, w[dim * o], w[dim * o + 1], z, m);
     if (o >= n - n_ob) e.ob_rows[ob_begin + (o - (n - n_ob))] = static_cast<int>(a);
   }
 }
@@ -2589,15 +2581,13 @@ __global__ void k_remap(Dev e, int fluid_from, int wall_from, int df, int dw, in
     const int n = e.cnt[a];
     for (int k = 0; k < n; ++k) {
       uint32_t& ent = e.nbr[entry_at(e.rows, a, k)];
-      const uint32_t b = ent >> kCodeBits;
-      const uint32_t nb = b < static_cast<uint32_t>(e.NF) ? b - df : b - dw;
-      ent = (nb << kCodeBits) | (ent & kCodeMask);
+      ent = ent < static_cast<uint32_t>(e.NF) ? ent - df : ent - dw;
     }
     if (a < e.NF && e.cases[e.cid[a]].csf) {
       const int n4 = e.cnt4[a];
       for (int k = 0; k < n4; ++k) {
         uint32_t& ent = e.nbr4[static_cast<int64_t>(k) * e.NF + a];
-        ent = ((ent >> kCodeBits) - df) << kCodeBits;
+        ent -= df;
       }
     }
   }
@@ -2681,11 +2671,11 @@ size_t carve(const tsph_engine_params& p, Dev* d, char* base, CaseDev** cases, c
   Dev t{};
   t.rows = N;
   t.null_row = static_cast<int>(N);
-  t.pad = (static_cast<uint32_t>(N) << kCodeBits) | kSelfCode;
+  t.pad = static_cast<uint32_t>(N);
   t.pos = static_cast<double4*>(take(N * sizeof(double4)));
   t.vel = static_cast<double4*>(take(NF * sizeof(double4)));
   t.anchor = static_cast<double4*>(take(NF * sizeof(double4)));
-  t.lp = static_cast<float4*>(take((N + 1) * sizeof(float4)));
+  t.lp = static_cast<Rec*>(take((N + 1) * sizeof(Rec)));
   t.home = static_cast<int32_t*>(take(N * sizeof(int32_t)));
   t.id = static_cast<int32_t*>(take(NF * sizeof(int32_t)));
   t.cid = static_cast<int32_t*>(take(N * sizeof(int32_t)));
@@ -2701,7 +2691,7 @@ size_t carve(const tsph_engine_params& p, Dev* d, char* base, CaseDev** cases, c
   t.acc = static_cast<float4*>(take(NF * sizeof(float4)));
   t.conc = static_cast<float*>(take((N + 1) * sizeof(float)));
   t.gradc = static_cast<float4*>(take(NF * sizeof(float4)));
-  t.lpv = static_cast<float4*>(take((N + 1) * sizeof(float4)));
+  t.lpv = static_cast<Rec*>(take((N + 1) * sizeof(Rec)));
   t.csA = static_cast<double4*>(take(NF * sizeof(double4)));
   t.csB = static_cast<double4*>(take(NF * sizeof(double4)));
   t.csN0 = static_cast<double2*>(take(NF * sizeof(double2)));
@@ -3035,9 +3025,10 @@ CaseDev make_case_dev(const tsph_case_params& p, int64_t* ncells) {
   double cell = 2.0 * p.h + p.skin;
   int64_t nx, ny, nz;
   if (p.periodic_box > 0.0) {
-    // n cells of edge L/n >= the list cutoff per axis; the edge is rounded to
-    // FP32 and the box snapped to n times it, so that a separation across
-    // the wrap, (l_a - l_b) - u * cell, is as exact as any other
+    // n cells of edge L/n >= the list cutoff per axis (the edge rounded to
+    // FP32 and the box snapped to n times it); the position records count
+    // units of L / 2^32, so that the 2^32 wrap of their difference is the
+    // minimum image
     const int64_t n = std::max<int64_t>(3, static_cast<int64_t>(std::floor(p.periodic_box / (cell * (1.0 + 1e-6)))));
     c.cellf = static_cast<float>(p.periodic_box / static_cast<double>(n));
     cell = static_cast<double>(c.cellf);
@@ -3054,6 +3045,19 @@ CaseDev make_case_dev(const tsph_case_params& p, int64_t* ncells) {
     ny = static_cast<int64_t>(std::ceil((p.grid_hi[1] - p.grid_lo[1]) / cell)) + 1;
     nz = p.dim == 3 ? static_cast<int64_t>(std::ceil((p.grid_hi[2] - p.grid_lo[2]) / cell)) + 1 : 1;
     if (p.dim == 2) c.origin[2] = -0.5 * cell;
+  }
+  if (c.periodic) {
+    c.inv_q = 4294967296.0 / c.pbox;
+    c.qf = static_cast<float>(c.pbox / 4294967296.0);
+  } else {
+    // the smallest power of two q with 2^31 q >= the grid's extent (and >= 4
+    // cells): every record word lies in [0, 2^31), 2^30 units or more from the
+    // null row's
+    const double extent = std::max(4.0, static_cast<double>(std::max(nx, std::max(ny, nz)))) * cell;
+    int k = -60;
+    while (std::ldexp(1.0, k + 31) < extent) ++k;
+    c.inv_q = std::ldexp(1.0, -k);
+    c.qf = static_cast<float>(std::ldexp(1.0, k));
   }
   *ncells = nx * ny * nz;
   c.ncx = static_cast<int>(nx);
@@ -3394,11 +3398,11 @@ int tsph_engine_remove_case(tsph_engine* E, int64_t case_id, tsph_stream stream)
     size_t e;
   };
   const Arr fluid_arrays[] = {{d.pos, sizeof(double4)}, {d.vel, sizeof(double4)}, {d.anchor, sizeof(double4)},
-                              {d.lp, sizeof(float4)},   {d.home, sizeof(int32_t)}, {d.id, sizeof(int32_t)},
+                              {d.lp, sizeof(Rec)},   {d.home, sizeof(int32_t)}, {d.id, sizeof(int32_t)},
                               {d.cid, sizeof(int32_t)}, {d.vb, sizeof(float4)},    {d.pr, sizeof(float)},
                               {d.rho, sizeof(float)},   {d.pq, sizeof(float)},     {d.rs, sizeof(float2)},
                               {d.acc, sizeof(float4)},  {d.cnt, sizeof(int32_t)}};
-  const Arr wall_arrays[] = {{d.pos, sizeof(double4)}, {d.lp, sizeof(float4)}, {d.home, sizeof(int32_t)},
+  const Arr wall_arrays[] = {{d.pos, sizeof(double4)}, {d.lp, sizeof(Rec)}, {d.home, sizeof(int32_t)},
                              {d.cid, sizeof(int32_t)},  {d.vb, sizeof(float4)}, {d.pr, sizeof(float)},
                              {d.rho, sizeof(float)},    {d.pq, sizeof(float)},  {d.cnt, sizeof(int32_t)}};
   int rc = TSPH_OK;

@@ -34,7 +34,7 @@ __all__ = ["BatchEngine", "CaseSpec", "DamBreak3DEngine", "DamBreak3DRun", "dam_
            "dam_break_3d_case", "droplet_impact_case", "engine_bytes", "shear_decay_case", "obstacle_case", "obstacle_lattice_3d",
            "run_case", "run_dam_break_2d", "tune_single_case", "DIAG_FIELDS"]
 
-MAX_ROWS = (1 << 26) - 2   # fluid + wall rows of one engine (26-bit row index, one null row)
+MAX_ROWS = (1 << 26) - 2   # fluid + wall rows the host layer gives one engine (the engine takes < 2^31 - 1)
 FIT_NEIGHBORS = 128        # CSF curvature-fit row capacity (2-D, 4h + skin)
 
 DIAG_FIELDS = ("rho_max", "speed_max", "front", "force_x", "force_y", "force_z", "kinetic",

@@ -133,7 +133,7 @@ def capacities_for_budget(budget_bytes: float, *, max_cases: int = 64,
     per_c = (engine_bytes(max_fluid=1, max_wall=1, **dict(probe, max_cells=m)) - base) / m
     room = max(float(budget_bytes) - base, 0.0)
     max_fluid = int(room / (per_f + per_w / 2.0 + 2.0 * per_c))
-    max_fluid = min(max_fluid, (MAX_ROWS * 2) // 3)   # fluid + wall rows < 2^26
+    max_fluid = min(max_fluid, (MAX_ROWS * 2) // 3)   # fluid + wall rows <= MAX_ROWS
     return dict(max_fluid=max_fluid, max_wall=max(max_fluid // 2, 1), max_cells=2 * max_fluid,
                 max_cases=max_cases, max_neighbors=max_neighbors, diag_ring=4, max_obstacle=0)
 

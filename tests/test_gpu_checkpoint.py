@@ -195,8 +195,11 @@ def test_adaptive_run_checkpoints_and_resumes(gpu, tmp_path, monkeypatch):
     assert run.steps_taken == full.steps_taken
     assert run.simulated_time == pytest.approx(full.simulated_time, rel=1e-12)
     assert run.times[:3] == full.times[:3]
-    np.testing.assert_allclose(run.times, full.times, rtol=1e-9)
-    np.testing.assert_allclose(run.front, full.front, rtol=1e-9)
+    # the resumed run rebuilds its rows at the checkpoint, so its FP32 sums
+    # run in another order: later samples agree to the FP32 round-off of the
+    # steps next_dt chooses
+    np.testing.assert_allclose(run.times, full.times, rtol=1e-7)
+    np.testing.assert_allclose(run.front, full.front, rtol=1e-7)
     np.testing.assert_allclose(run.kinetic_energy, full.kinetic_energy, rtol=1e-6)
     assert len(run.obstacle_force) == len(full.obstacle_force) == final
     np.testing.assert_allclose(run.obstacle_force[:11], full.obstacle_force[:11], rtol=1e-12, atol=1e-12)
