@@ -53,7 +53,7 @@ PAIR_FLOPS = {"density": 27, "diffusion": 50, "walls": 32, "force": 65, "concent
 # DRAM bytes of one force launch per fluid particle: ncu capture of the force
 # pass on the dx = 0.0138 rung (241,488 fluid) at skin 0.15 h and depth 8,
 # dram__bytes_read.sum + dram__bytes_write.sum divided by the fluid rows.
-FORCE_TRAFFIC_PER_FLUID = 378.0
+FORCE_TRAFFIC_PER_FLUID = 373.0
 FORCE_TRAFFIC_RUNG = "dx=0.0138 (241,488 fluid), skin 0.15 h, depth 8, ncu capture scaled by fluid rows"
 MIN_TIMED_SOLVER_STEPS = 200
 
