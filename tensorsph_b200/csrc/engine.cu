@@ -206,6 +206,7 @@ struct Dev {
   float2* st;        // CSF: surface-tension acceleration
   unsigned int* csf_hist;  // [n_slots][256] median-select histograms
   int has_csf, maxfit;
+  int has_2d, has_3d;     // the batch holds 2-D, 3-D cases (which row builders run)
   int has_psi;            // some case uses the psi diffusion form (one more gather)
   int has_bcd;            // some case uses the boundary-consistent density
   int has_comp;           // some case uses the compression regularisation
@@ -585,6 +586,7 @@ __global__ void __launch_bounds__(128, 8) k_rows(Dev e, int n_cells) {
     CaseCtl& ctl = e.ctl[c];
     if (!ctl.rebuild) continue;
     const CaseDev& C = e.cases[c];
+    if (C.dim == 2) continue;  // k_rows_2d
     const int key_a = cell - C.key_off;
     const int cz = key_a % C.ncz, cy = (key_a / C.ncz) % C.ncy, cx = key_a / (C.ncz * C.ncy);
     const unsigned long long lim = C.rows_lim;
@@ -685,6 +687,70 @@ __global__ void __launch_bounds__(128, 8) k_rows(Dev e, int n_cells) {
       for (int o = 16; o > 0; o >>= 1) longest = max(longest, __shfl_xor_sync(0xffffffffu, longest, o));
       if (lane == 0) atomicMax(&ctl.row_max, static_cast<unsigned long long>(longest));
     }
+  }
+}
+
+// The rows of rebuilding 2-D cases, one thread per row: a 2-D cell holds
+// ~8 rows, too few for a warp per cell.  The same test and entry order as
+// k_rows: per column x + dx, the fluid rows of its cells y - 1 .. y + 1 (one
+// run of consecutive keys), then their wall rows.
+__global__ void k_rows_2d(Dev e) {
+  if (!*e.any_rebuild) return;
+  const int total = e.nf + e.nw;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const int64_t a = t < e.nf ? t : e.NF + (t - e.nf);
+    const int c = e.cid[a];
+    CaseCtl& ctl = e.ctl[c];
+    if (!ctl.rebuild) continue;
+    const CaseDev& C = e.cases[c];
+    if (C.dim != 2) continue;
+    const bool fluid_row = t < e.nf;
+    const Rec pa = e.lp[a];
+    const unsigned long long bound = C.rows_lim + 1;
+    const int key_a = e.home[a] - C.key_off;
+    const int cy = key_a % C.ncy, cx = key_a / C.ncy;
+    uint32_t* const row = e.nbr + entry_at(e.rows, a, 0);
+    const int64_t group_stride = e.rows * 4;
+    int count = 0;
+    auto scan = [&](int b0, int b1, int64_t off) {
+      for (int b = b0; b < b1; ++b) {
+        const uint32_t id = static_cast<uint32_t>(off + b);
+        if (dist2_units(pa, e.lp[off + b]) < bound && id != static_cast<uint32_t>(a)) {
+          if (count < e.maxnb) row[(count >> 2) * group_stride + (count & 3)] = id;
+          ++count;
+        }
+      }
+    };
+    const int y0 = cy > 0 ? cy - 1 : 0, y1 = cy + 1 < C.ncy ? cy + 1 : cy;
+    for (int dx = -1; dx <= 1; ++dx) {
+      const int x = cx + dx;
+      if (x < 0 || x >= C.ncx) continue;
+      const int column = C.key_off + x * C.ncy;
+      int f0 = -1, f1 = -1, w0 = -1, w1 = -1;
+      for (int y = y0; y <= y1; ++y) {
+        const int fsy = e.fstart[column + y];
+        if (fsy >= 0) {
+          if (f0 < 0) f0 = fsy;
+          f1 = e.fend[column + y];
+        }
+        if (fluid_row) {
+          const int wsy = e.wstart[column + y];
+          if (wsy >= 0) {
+            if (w0 < 0) w0 = wsy;
+            w1 = e.wend[column + y];
+          }
+        }
+      }
+      if (f0 >= 0) scan(f0, f1, 0);
+      if (w0 >= 0) scan(w0, w1, e.NF);
+    }
+    if (count > e.maxnb) {
+      atomicOr(e.status, 1);
+      atomicOr(&ctl.status, 1);
+    }
+    e.cnt[a] = count < e.maxnb ? count : e.maxnb;
+    for (int k = count; k < e.maxnb && (k & 3); ++k) e.nbr[entry_at(e.rows, a, k)] = e.pad;
+    atomicMax(&ctl.row_max, static_cast<unsigned long long>(count));
   }
 }
 
@@ -2834,6 +2900,8 @@ void batch_changed(tsph_engine* E) {
   Dev& d = E->d;
   d.shift_slot = second_pass(E) ? E->order[0].slot : 0;
   d.has_csf = 0;
+  d.has_2d = 0;
+  d.has_3d = 0;
   d.has_tvc = 0;
   d.has_psi = 0;
   d.has_bcd = 0;
@@ -2843,6 +2911,8 @@ void batch_changed(tsph_engine* E) {
   d.tvc_late = second_pass(E) && E->order[0].dev.tvc_bulk ? 1 : 0;
   for (const CaseHost& c : E->order) {
     d.has_csf |= c.dev.csf;
+    d.has_2d |= c.dev.dim == 2 ? 1 : 0;
+    d.has_3d |= c.dev.dim == 2 ? 0 : 1;
     d.has_psi |= c.dev.psi;
     d.has_bcd |= c.dev.bcd;
     d.has_comp |= c.dev.comp;
@@ -2876,7 +2946,8 @@ int enqueue_rebuild_body(tsph_engine* E, cudaStream_t s) {
   k_permute_back<<<g, kBlock, 0, s>>>(d);
   k_clear_table<<<grid_for(E->total_cells, 256), 256, 0, s>>>(d.fstart, d.fend, E->total_cells, d.any_rebuild);
   k_fill_table<<<g, kBlock, 0, s>>>(nullptr, d.keys, d.nf, d.fstart, d.fend, d.any_rebuild);
-  k_rows<<<grid_for(E->total_cells * 32, 128), 128, 0, s>>>(d, static_cast<int>(E->total_cells));
+  if (d.has_3d) k_rows<<<grid_for(E->total_cells * 32, 128), 128, 0, s>>>(d, static_cast<int>(E->total_cells));
+  if (d.has_2d) k_rows_2d<<<grid_for(d.nf + d.nw, kBlock), kBlock, 0, s>>>(d);
   if (d.has_csf) k_fit_rows<<<g, kBlock, 0, s>>>(d);
   k_rebuilt<<<gc, 128, 0, s>>>(d);
   TSPH_LAUNCH_CHECK();
