@@ -160,3 +160,16 @@ def test_tuning_cache_roundtrip(tmp_path, monkeypatch):
     tuning.store(k1, {"skin_factor": 0.15, "block": 128, "batch": 8})
     assert tuning.lookup(k2) == {"skin_factor": 0.15, "block": 128, "batch": 8}
     assert tuning.lookup(k3) is None
+
+
+def test_tuner_prefers_the_wider_skin_among_equal_trials():
+    """Trials from rest cannot see the rebuilds a wider skin saves later, so a
+    near-tie goes to the wider skin; a clear win by a narrower one stands."""
+    from tensorsph_b200.engine import pick_trial
+    trials = [{"skin_factor": 0.10, "batch": 4, "ms_per_step": 1.870},
+              {"skin_factor": 0.15, "batch": 8, "ms_per_step": 1.880},
+              {"skin_factor": 0.15, "batch": 4, "ms_per_step": 1.884},
+              {"skin_factor": 0.25, "batch": 8, "ms_per_step": 2.050}]
+    assert pick_trial(trials) == trials[1]
+    trials[0]["ms_per_step"] = 1.80
+    assert pick_trial(trials) == trials[0]
