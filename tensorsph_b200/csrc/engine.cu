@@ -65,7 +65,7 @@ constexpr int64_t kMaxRows = (int64_t(1) << 31) - 2;      // a row entry is a pa
 // separation is the wrapped integer difference of two words converted to
 // FP32 and scaled by q: exact for a power-of-two q (every non-periodic case)
 // and, for a periodic cube of edge 2^32 q, the minimum image by the 2^32
-// wrap.  No cell offset has to be decoded per neighbour.
+// wrap.  The row entry carries no cell offset.
 struct __align__(16) Rec {
   uint32_t x, y, z;
   float w;
@@ -81,7 +81,7 @@ struct CaseDev {
   int ncx, ncy, ncz, key_off;
   int fluid_begin, n_fluid, wall_begin, n_wall;
   int ob_begin, n_ob, has_ob, shift_every;
-  float cellf, inv_h, sigma, sig2d, rho0, bulk, gamma, inv_gamma;
+  float inv_h, sigma, sig2d, rho0, bulk, gamma, inv_gamma;
   float qf;                // the fixed-point unit of the position records, metres
   double inv_q;            // 1 / q
   float grav, nu2, nu2f, dscale, dtf, visc_eps, rho_floor, wall_mass;
@@ -3162,8 +3162,7 @@ CaseDev make_case_dev(const tsph_case_params& p, int64_t* ncells) {
     // units of L / 2^32, so that the 2^32 wrap of their difference is the
     // minimum image
     const int64_t n = std::max<int64_t>(3, static_cast<int64_t>(std::floor(p.periodic_box / (cell * (1.0 + 1e-6)))));
-    c.cellf = static_cast<float>(p.periodic_box / static_cast<double>(n));
-    cell = static_cast<double>(c.cellf);
+    cell = static_cast<double>(static_cast<float>(p.periodic_box / static_cast<double>(n)));
     c.periodic = 1;
     c.pbox = static_cast<double>(n) * cell;
     for (int k = 0; k < 3; ++k) c.origin[k] = 0.0;
@@ -3171,7 +3170,6 @@ CaseDev make_case_dev(const tsph_case_params& p, int64_t* ncells) {
     c.cell = cell;
   } else {
     c.cell = cell;
-    c.cellf = static_cast<float>(cell);
     for (int k = 0; k < 3; ++k) c.origin[k] = p.grid_lo[k];
     nx = static_cast<int64_t>(std::ceil((p.grid_hi[0] - p.grid_lo[0]) / cell)) + 1;
     ny = static_cast<int64_t>(std::ceil((p.grid_hi[1] - p.grid_lo[1]) / cell)) + 1;
