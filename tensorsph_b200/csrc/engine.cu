@@ -564,8 +564,8 @@ __device__ __forceinline__ unsigned long long dist2_units(const Rec& la, const R
 // Rows at the list cutoff (2h + skin), for the rows of rebuilding cases; wall
 // rows keep fluid neighbours only (they feed the Adami extrapolation and the
 // obstacle reaction).  One warp per home cell: the lanes take the cell's
-// rows (fluid, then wall) 32 at a time and walk the same 27 neighbour cells
-// in lockstep, so each candidate record is one broadcast load and no lane
+// rows (fluid, then wall) 32 at a time and walk the same neighbour cells in
+// lockstep, so each candidate record is one broadcast load and no lane
 // diverges.  The test is exact integer arithmetic on the fixed-point records
 // against (cutoff / q + 2)^2: every pair within the cutoff is listed (the
 // rounding of the two records moves a distance by under sqrt(3) units), plus
