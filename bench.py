@@ -55,6 +55,9 @@ PAIR_FLOPS = {"density": 27, "diffusion": 50, "walls": 32, "force": 65, "concent
 # dram__bytes_read.sum + dram__bytes_write.sum divided by the fluid rows.
 FORCE_TRAFFIC_PER_FLUID = 373.0
 FORCE_TRAFFIC_RUNG = "dx=0.0138 (241,488 fluid), skin 0.15 h, depth 8, ncu capture scaled by fluid rows"
+# What the same ncu capture shows limits the force pass (neither roof binds).
+FORCE_LIMITER = ("l1: l1tex throughput 90 % of peak, data pipe 74 % of elapsed cycles, long-scoreboard "
+                 "stalls 6.3 per issue; DRAM 13 %, FMA/ALU pipes 38-41 % (ncu capture on dx=0.0138)")
 MIN_TIMED_SOLVER_STEPS = 200
 
 
@@ -1040,6 +1043,7 @@ def main():
                          "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                          "traffic": FORCE_TRAFFIC_PER_FLUID * nf,
                          "traffic_source": f"from_profile: {FORCE_TRAFFIC_RUNG}",
+                         "limiter": FORCE_LIMITER,
                          "peak_source": hbm_src,
                          "algorithmic_bytes_per_launch": ALGO_BYTES_FORCE * nf,
                          "launch_ms": stage["force"],
