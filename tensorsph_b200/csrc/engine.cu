@@ -569,8 +569,8 @@ __device__ __forceinline__ unsigned long long dist2_units(const Rec& la, const R
 // diverges.  The test is exact integer arithmetic on the fixed-point records
 // against (cutoff / q + 2)^2: every pair within the cutoff is listed (the
 // rounding of the two records moves a distance by under sqrt(3) units), plus
-// the rare pair up to 2 units (a few nm) beyond it, where every kernel is
-// zero.  Entries follow the stencil: per column (dx, dy), the fluid rows of
+// the rare pair up to 2 + sqrt(3) units (7 nm here) beyond it, where every
+// kernel is zero.  Entries follow the stencil: per column (dx, dy), the fluid rows of
 // its cells z - 1 .. z + 1, then their wall rows.
 __global__ void __launch_bounds__(128, 8) k_rows(Dev e, int n_cells) {
   if (!*e.any_rebuild) return;

@@ -173,3 +173,31 @@ def test_tuner_prefers_the_wider_skin_among_equal_trials():
     assert pick_trial(trials) == trials[1]
     trials[0]["ms_per_step"] = 1.80
     assert pick_trial(trials) == trials[0]
+
+
+def test_fixed_point_row_test_lists_every_pair_within_the_cutoff():
+    """The row builder's criterion, restated: positions rounded to units of a
+    power-of-two q with 2^31 q >= the extent, squared integer distance against
+    ceil((cutoff / q + 2)^2).  It lists every pair within the cutoff (FP64) and
+    nothing beyond the cutoff plus (2 + sqrt(3)) q (seeded cloud with pairs
+    placed on the cutoff)."""
+    import math
+    import numpy as np
+    rng = np.random.default_rng(7)
+    extent, rc = 3.3, 0.0193
+    k = -60
+    while math.ldexp(1.0, k + 31) < extent:
+        k += 1
+    q = math.ldexp(1.0, k)
+    a = rng.uniform(0.0, extent, (4000, 3))
+    d = rng.normal(size=(4000, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    b = a + d * (rc + rng.uniform(-3 * q, 3 * q, (4000, 1)))   # pairs straddling the cutoff
+    r = np.linalg.norm(a - b, axis=1)
+    ia = np.rint(a / q).astype(np.int64)
+    ib = np.rint(b / q).astype(np.int64)
+    d2 = ((ia - ib) ** 2).sum(axis=1)
+    lim = math.ceil((rc / q + 2.0) ** 2)
+    listed = d2 <= lim
+    assert listed[r <= rc].all()
+    assert (r[listed] <= rc + (2.0 + math.sqrt(3.0)) * q * (1 + 1e-9)).all()
